@@ -1,0 +1,136 @@
+"""Flow-case parameters and the seeded synthetic cases the tests and the
+benchmark use.
+
+A case is a mesh (index sets, see mesh.py) plus the physics switches that
+the reference hard-codes in LBM_Manager's constructor
+(LBM_Manager.cpp:38-80) and in its compile-time constants
+(header/Constants.h:164-236).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from .lattice import directions, reference_units, weights
+from .mesh import Mesh, MeshSpec, Sphere, build_mesh
+
+COLLISIONS = {"LBGK": 0, "Cumulant": 1}
+IB_METHODS = {"DW": 0, "FH": 1}
+BC_MODES = {"neq": 0, "zouhe_outflow": 1}
+STREAM_CONVENTIONS = {"reference": 0, "textbook": 1}
+STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
+
+
+@dataclass
+class CaseParams:
+    q: int = 19
+    collision: str = "LBGK"
+    ib_method: str = "FH"
+    bc_mode: str = "neq"
+    stream_convention: str = "reference"
+    nu: float = 0.02                 # level-0 lattice viscosity
+    u_bc: tuple = (0.05, 0.0, 0.0)   # boundary velocity (lattice units)
+    u_ref: float = 0.05              # reference velocity of the unit conversion
+    rho0: float = 1.0
+    storage: str = "f64"
+    tau: list = field(default_factory=list)
+
+    def taus(self, max_level: int) -> list:
+        if self.tau:
+            return list(self.tau)
+        t, _, _ = reference_units(self.nu, self.u_ref, max_level,
+                                  collision="LBGK")
+        return t
+
+
+@dataclass
+class Case:
+    mesh: Mesh
+    params: CaseParams
+
+    @property
+    def max_level(self) -> int:
+        return self.mesh.spec.max_level
+
+    @property
+    def q(self) -> int:
+        return self.params.q
+
+
+def sphere_case(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1, refine=None, center=(16, 16, 16),
+                radius=4.0, u=0.05, re=20.0, boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow",
+                ib_method="FH") -> Case:
+    """Flow past a sphere; nu = u * 2R / Re in coarse units."""
+    if refine is None:
+        refine = [((4, 8, 8), (28, 24, 24))]
+    nu = u * 2.0 * radius / re
+    spec = MeshSpec(q=q, max_level=max_level, coarse=tuple(coarse), refine=list(refine), boundary=tuple(boundary),
+                    sphere=Sphere(tuple(center), radius))
+    p = CaseParams(q=q, collision=collision, ib_method=ib_method, bc_mode=bc_mode, nu=nu, u_bc=(u, 0.0, 0.0),
+                   u_ref=u)
+    return Case(build_mesh(spec), p)
+
+
+def uniform_box_case(q=19, n=(16, 16, 16), nu=1.0 / 30.0, boundary=("periodic",) * 3, collision="LBGK",
+                     u_ref=0.02, storage="f64", stream_convention="reference", empty_levels=0,
+                     u_bc=(0.0, 0.0, 0.0)) -> Case:
+    """Single populated level; `empty_levels` adds empty finer levels so the
+    reference harness (which needs at least two levels) can run it."""
+    spec = MeshSpec(q=q, max_level=empty_levels, coarse=tuple(n), refine=[None] * empty_levels,
+                    boundary=tuple(boundary))
+    p = CaseParams(q=q, collision=collision, nu=nu, u_bc=tuple(u_bc), u_ref=u_ref, bc_mode="neq",
+                   storage=storage, stream_convention=stream_convention)
+    return Case(build_mesh(spec), p)
+
+
+def taylor_green_fields(n, u0=0.02, rho_amp=True):
+    """TGV initial field on an n^3 periodic box with wavenumber 2 pi / n:
+    u = u0 sin kx cos ky cos kz, v = -u0 cos kx sin ky cos kz, w = 0, and the
+    matching pressure term in the density (c_s^2 = 1/3)."""
+    nx, ny, nz = n
+    k = 2.0 * np.pi / nx
+    x = (np.arange(nx) + 0.5) * k
+    y = (np.arange(ny) + 0.5) * (2.0 * np.pi / ny)
+    z = (np.arange(nz) + 0.5) * (2.0 * np.pi / nz)
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    u = u0 * np.sin(X) * np.cos(Y) * np.cos(Z)
+    v = -u0 * np.cos(X) * np.sin(Y) * np.cos(Z)
+    w = np.zeros_like(u)
+    rho = np.ones_like(u)
+    if rho_amp:
+        rho = rho + 3.0 * (u0 * u0 / 16.0) * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0)
+    return rho, u, v, w
+
+
+def equilibrium(q, rho, ux, uy, uz):
+    """BGK equilibrium, same expression order as LBM_Manager::calculateFeq
+    (LBM_Manager.cpp:137-169); arrays broadcast, output shape (Q, ...)."""
+    ex, ey, ez, _ = directions(q)
+    w = weights(q)
+    uu = ux * ux + uy * uy + uz * uz
+    out = []
+    for i in range(q):
+        euv = ex[i] * ux + ey[i] * uy + ez[i] * uz
+        out.append(rho * w[i] * (1. + 3. * euv + 4.5 * euv * euv - 1.5 * uu))
+    return np.stack(out)
+
+
+def perturbed_populations(case: Case, seed: int = 1234, amp: float = 0.02):
+    """Seeded near-equilibrium populations for every stored cell of every
+    level (f = feq(rho, u) * (1 + amp * noise), rho in [0.95, 1.05],
+    |u| < 0.05), keyed by the sorted cell keys.  Solid cells stay zero."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for l in range(case.max_level + 1):
+        keys = case.mesh.all_keys(l)
+        n = keys.size
+        rho = rng.uniform(0.95, 1.05, n)
+        u = rng.uniform(-0.03, 0.03, (3, n))
+        f = equilibrium(case.q, rho, u[0], u[1], u[2]) * (1.0 + amp * rng.uniform(-1, 1, (case.q, n)))
+        if l == case.max_level and case.mesh.levels[l]["lat_sf"].size:
+            sf = np.isin(keys, case.mesh.levels[l]["lat_sf"])
+            f[:, sf] = 0.0
+        out.append((keys, np.ascontiguousarray(f)))
+    return out

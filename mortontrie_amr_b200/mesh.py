@@ -1,0 +1,276 @@
+"""Box-refinement mesher that emits the reference's lattice index-set contract.
+
+The reference builds its per-level index sets in Lat_Manager::voxelize
+(Lat_Voxelize.cpp:17-733) from an STL-driven octree.  The LBM step only
+consumes the resulting sets (Lat_Manager.hpp:245-316):
+
+  lat_f[l]              cells that collide and stream
+  lat_overlap_F2C[l]    coarse cells under the fine region's outer shell:
+                        collide, receive f by coalescence, never stream
+  lat_overlap_C2F[l]    fine cells that are children of F2C[l-1]: their fcol
+                        is copied from f, then overwritten by explosion
+  ghost_overlap_C2F[l]  fine cells just outside the fine region that give
+                        C2F cells something to pull from
+  ghost_overlap_F2C[l]  coarse lat_f neighbours of F2C cells (explosion
+                        sources for ghost_overlap_C2F)
+  lat_sf                finest-level solid cells (f = fcol = 0 storage)
+  lat_bc[26]            level-0 boundary shell split into 6 faces, 12 edges,
+                        8 corners (Lat_Voxelize.cpp:242-288)
+  dis                   finest-level cells with at least one link that
+                        crosses the solid: normalised wall distance per
+                        direction q>=1, -1 where the link is free
+                        (Lat_Voxelize.cpp:1252-1285)
+
+This module re-creates that contract for nested refinement boxes and an
+analytic sphere, which is what the flow cases here need.  The sets it
+returns are plain sorted uint64 key arrays.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from .lattice import cell_key, directions
+
+SET_NAMES = ("lat_f", "overlap_F2C", "overlap_C2F", "ghost_overlap_C2F", "ghost_overlap_F2C", "lat_sf")
+
+# lat_bc index -> side of the box on each axis (-1 low, +1 high, 0 none);
+# the index order is the reference's Bdry_Type enum (D3Q19_BC_Manager.hpp:25-53).
+BC_SIDES = [
+    (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1),
+    (1, 1, 0), (-1, 1, 0), (-1, -1, 0), (1, -1, 0),
+    (0, 1, 1), (0, -1, 1), (0, 1, -1), (0, -1, -1),
+    (1, 0, 1), (-1, 0, 1), (1, 0, -1), (-1, 0, -1),
+    (1, 1, 1), (-1, 1, 1), (-1, -1, 1), (1, -1, 1),
+    (1, 1, -1), (-1, 1, -1), (-1, -1, -1), (1, -1, -1),
+]
+
+
+@dataclass
+class Sphere:
+    center: tuple  # coarse-cell units, measured from the box corner
+    radius: float  # coarse-cell units
+
+
+@dataclass
+class MeshSpec:
+    q: int
+    max_level: int
+    coarse: tuple                      # (nx, ny, nz) coarse cells
+    # per level l < L: ((lo), (hi)) in level-l cells, or None for an empty
+    # finer level (the reference cannot run with a single level: its
+    # LBM_Manager::defineRunOrder indexes past the level array when
+    # C_max_level == 0, LBM_Manager.cpp:105-128)
+    refine: list = field(default_factory=list)
+    boundary: tuple = ("bc", "bc", "bc")  # per axis: "bc" (level-0 boundary shell) or "periodic"
+    sphere: Optional[Sphere] = None
+
+
+@dataclass
+class Mesh:
+    spec: MeshSpec
+    levels: list          # per level: dict set name -> sorted uint64 keys
+    lat_bc: list          # 26 sorted uint64 key arrays (level 0)
+    dis_keys: np.ndarray  # sorted finest-level keys
+    dis_rows: np.ndarray  # (n, Q-1) float64
+    extent: list          # per level: (nx, ny, nz) in that level's cells
+
+    def all_keys(self, level: int) -> np.ndarray:
+        parts = [self.levels[level][s] for s in SET_NAMES]
+        if level == 0:
+            parts += list(self.lat_bc)
+        return np.unique(np.concatenate(parts)) if parts else np.zeros(0, np.uint64)
+
+    def n_cells(self) -> list:
+        return [int(self.all_keys(l).size) for l in range(self.spec.max_level + 1)]
+
+
+def _grid(lo, hi):
+    xs = np.arange(lo[0], hi[0], dtype=np.int64)
+    ys = np.arange(lo[1], hi[1], dtype=np.int64)
+    zs = np.arange(lo[2], hi[2], dtype=np.int64)
+    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+    return X.ravel(), Y.ravel(), Z.ravel()
+
+
+def _shell_mask(x, y, z, lo, hi, width):
+    return ((x < lo[0] + width) | (x >= hi[0] - width) | (y < lo[1] + width) | (y >= hi[1] - width)
+            | (z < lo[2] + width) | (z >= hi[2] - width))
+
+
+def _inside(x, y, z, lo, hi):
+    return ((x >= lo[0]) & (x < hi[0]) & (y >= lo[1]) & (y < hi[1]) & (z >= lo[2]) & (z < hi[2]))
+
+
+def _neighbours(x, y, z, q, extent, periodic):
+    """Q-1 neighbour coordinates, wrapped on periodic axes."""
+    ex, ey, ez, _ = directions(q)
+    out = []
+    for d in range(1, q):
+        nx_, ny_, nz_ = x + ex[d], y + ey[d], z + ez[d]
+        if periodic[0]:
+            nx_ = np.mod(nx_, extent[0])
+        if periodic[1]:
+            ny_ = np.mod(ny_, extent[1])
+        if periodic[2]:
+            nz_ = np.mod(nz_, extent[2])
+        out.append((nx_, ny_, nz_))
+    return out
+
+
+def _sorted_unique(a):
+    return np.unique(np.asarray(a, np.uint64))
+
+
+def build_mesh(spec: MeshSpec) -> Mesh:
+    L = spec.max_level
+    q = spec.q
+    if len(spec.refine) != L:
+        raise ValueError("need one refinement box per level below the maximum level")
+    periodic = tuple(b == "periodic" for b in spec.boundary)
+    nx, ny, nz = spec.coarse
+    levels = []
+    extents = []
+    lat_bc = [np.zeros(0, np.uint64) for _ in range(26)]
+
+    # domain of each level in its own cell units
+    dom_lo = [(0, 0, 0)]
+    dom_hi = [(nx, ny, nz)]
+    for l in range(L):
+        if spec.refine[l] is None or dom_hi[-1] == (0, 0, 0):
+            dom_lo.append((0, 0, 0))
+            dom_hi.append((0, 0, 0))
+            continue
+        lo, hi = spec.refine[l]
+        dom_lo.append(tuple(2 * v for v in lo))
+        dom_hi.append(tuple(2 * v for v in hi))
+    for l in range(L + 1):
+        extents.append(tuple((n << l) for n in (nx, ny, nz)))
+
+    for l in range(L + 1):
+        x, y, z = _grid(dom_lo[l], dom_hi[l])
+        sets = {}
+        stored = np.ones(x.size, bool)
+        is_bc = np.zeros(x.size, bool)
+        if l == 0:
+            side = np.zeros((x.size, 3), np.int64)
+            for a, (c, n) in enumerate(zip((x, y, z), (nx, ny, nz))):
+                if spec.boundary[a] == "bc":
+                    side[c == 0, a] = -1
+                    side[c == n - 1, a] = 1
+            is_bc = np.any(side != 0, axis=1)
+            for i, s in enumerate(BC_SIDES):
+                m = is_bc & (side[:, 0] == s[0]) & (side[:, 1] == s[1]) & (side[:, 2] == s[2])
+                lat_bc[i] = _sorted_unique(cell_key(L, 0, x[m], y[m], z[m]))
+        f2c = np.zeros(x.size, bool)
+        if l < L and dom_hi[l + 1] != (0, 0, 0):
+            lo, hi = spec.refine[l]
+            inside = _inside(x, y, z, lo, hi)
+            f2c = inside & _shell_mask(x, y, z, lo, hi, 1)
+            stored &= ~(inside & ~f2c)
+            if np.any(inside & is_bc):
+                raise ValueError("refinement box touches the boundary shell")
+        c2f = np.zeros(x.size, bool)
+        if l > 0:
+            c2f = _shell_mask(x, y, z, dom_lo[l], dom_hi[l], 2)
+            if np.any(c2f & f2c):
+                raise ValueError(f"level {l}: refinement box too close to the coarse/fine interface")
+        fluid = stored & ~is_bc & ~f2c & ~c2f
+        sets["overlap_F2C"] = _sorted_unique(cell_key(L, l, x[f2c], y[f2c], z[f2c]))
+        sets["overlap_C2F"] = _sorted_unique(cell_key(L, l, x[c2f], y[c2f], z[c2f]))
+        sets["lat_sf"] = np.zeros(0, np.uint64)
+        fx, fy, fz = x[fluid], y[fluid], z[fluid]
+        if l == L and spec.sphere is not None:
+            if L == 0:
+                raise ValueError("the solid boundary is only applied on a refined finest level")
+            s = 1 << L
+            cx, cy, cz = (c * s for c in spec.sphere.center)
+            r = spec.sphere.radius * s
+            px, py, pz = fx + 0.5, fy + 0.5, fz + 0.5
+            solid = (px - cx) ** 2 + (py - cy) ** 2 + (pz - cz) ** 2 < r * r
+            # every neighbour of the solid must be a plain fluid cell
+            sets["lat_sf"] = _sorted_unique(cell_key(L, l, fx[solid], fy[solid], fz[solid]))
+            fx, fy, fz = fx[~solid], fy[~solid], fz[~solid]
+        sets["lat_f"] = _sorted_unique(cell_key(L, l, fx, fy, fz))
+        levels.append(sets)
+
+    # ghost layers (Lat_Voxelize.cpp:676-733 semantics)
+    for l in range(L + 1):
+        sets = levels[l]
+        if l > 0:
+            cx_, cy_, cz_ = _coords_of(sets["overlap_C2F"], L, l)
+            cand = []
+            for (a, b, c) in _neighbours(cx_, cy_, cz_, q, extents[l], periodic):
+                ok = (a >= 0) & (b >= 0) & (c >= 0)
+                cand.append(cell_key(L, l, a[ok], b[ok], c[ok]))
+            cand = _sorted_unique(np.concatenate(cand)) if cand else np.zeros(0, np.uint64)
+            keep = ~np.isin(cand, sets["lat_f"]) & ~np.isin(cand, sets["overlap_C2F"])
+            sets["ghost_overlap_C2F"] = cand[keep]
+            bad = np.isin(sets["ghost_overlap_C2F"], sets["overlap_F2C"]) | np.isin(sets["ghost_overlap_C2F"], sets["lat_sf"])
+            if np.any(bad):
+                raise ValueError(f"level {l}: ghost layer overlaps the next interface or the solid")
+        else:
+            sets["ghost_overlap_C2F"] = np.zeros(0, np.uint64)
+        if l < L:
+            fx_, fy_, fz_ = _coords_of(sets["overlap_F2C"], L, l)
+            cand = []
+            for (a, b, c) in _neighbours(fx_, fy_, fz_, q, extents[l], periodic):
+                ok = (a >= 0) & (b >= 0) & (c >= 0)
+                cand.append(cell_key(L, l, a[ok], b[ok], c[ok]))
+            cand = _sorted_unique(np.concatenate(cand)) if cand else np.zeros(0, np.uint64)
+            sets["ghost_overlap_F2C"] = cand[np.isin(cand, sets["lat_f"])]
+        else:
+            sets["ghost_overlap_F2C"] = np.zeros(0, np.uint64)
+
+    dis_keys = np.zeros(0, np.uint64)
+    dis_rows = np.zeros((0, q - 1))
+    if spec.sphere is not None:
+        dis_keys, dis_rows = _sphere_links(spec, levels[L]["lat_f"])
+        sf_keys = levels[L]["lat_sf"]
+        # IB cells must be plain lat_f cells; the solid must stay clear of C2F.
+        sx, sy, sz = _coords_of(sf_keys, L, L)
+        for (a, b, c) in _neighbours(sx, sy, sz, q, extents[L], periodic):
+            k = cell_key(L, L, a, b, c)
+            if np.any(np.isin(k, levels[L]["overlap_C2F"])) or np.any(np.isin(k, levels[L]["ghost_overlap_C2F"])):
+                raise ValueError("solid too close to the coarse/fine interface")
+    return Mesh(spec=spec, levels=levels, lat_bc=lat_bc, dis_keys=dis_keys, dis_rows=dis_rows,
+                extent=extents)
+
+
+def _coords_of(keys, L, l):
+    from .lattice import cell_coords
+    return cell_coords(L, l, keys)
+
+
+def _sphere_links(spec: MeshSpec, fluid_keys: np.ndarray):
+    """Normalised distance from each finest-level fluid cell centre to the
+    sphere along every link (Lat_Voxelize.cpp:1252-1285 semantics: 0 at the
+    cell centre, 1 at the neighbour centre, -1 when the link is free)."""
+    L = spec.max_level
+    q = spec.q
+    ex, ey, ez, _ = directions(q)
+    s = 1 << L
+    cx, cy, cz = (c * s for c in spec.sphere.center)
+    r = spec.sphere.radius * s
+    x, y, z = _coords_of(fluid_keys, L, L)
+    px, py, pz = x + 0.5 - cx, y + 0.5 - cy, z + 0.5 - cz
+    c0 = px * px + py * py + pz * pz - r * r
+    rows = np.full((x.size, q - 1), -1.0)
+    for d in range(1, q):
+        a = float(ex[d] ** 2 + ey[d] ** 2 + ez[d] ** 2)
+        b = 2.0 * (px * ex[d] + py * ey[d] + pz * ez[d])
+        disc = b * b - 4.0 * a * c0
+        ok = disc >= 0.0
+        t = np.full(x.size, -1.0)
+        t[ok] = (-b[ok] - np.sqrt(disc[ok])) / (2.0 * a)
+        hit = ok & (t >= 0.0) & (t <= 1.0)
+        rows[hit, d - 1] = t[hit]
+    has = np.any(rows != -1.0, axis=1)
+    return fluid_keys[has].copy(), rows[has].copy()
+
+
+def cavity_or_box_spec(q, coarse, max_level=0, refine=None, boundary=("bc", "bc", "bc"), sphere=None):
+    return MeshSpec(q=q, max_level=max_level, coarse=tuple(coarse), refine=list(refine or []),
+                    boundary=tuple(boundary), sphere=sphere)

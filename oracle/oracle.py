@@ -1,0 +1,233 @@
+"""Python drivers for the CPU oracle (mt_oracle.c) and the reference harness.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline leg, never by the product package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SET_IDS = {"lat_f": 0, "overlap_F2C": 1, "overlap_C2F": 2, "ghost_overlap_C2F": 3, "ghost_overlap_F2C": 4,
+           "lat_sf": 5}
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        import build  # noqa: WPS433 (oracle/build.py, sibling module)
+        path = build.build_oracle_lib()
+        L = C.CDLL(path)
+        vp, i32, i64, dp, u64p = C.c_void_p, C.c_int, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_uint64)
+        L.oc_case_new.restype = vp
+        L.oc_case_new.argtypes = [i32, i32, i32, i32, i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int64), dp,
+                                  C.c_double, dp]
+        L.oc_case_free.argtypes = [vp]
+        L.oc_add_set.argtypes = [vp, i32, i32, u64p, i64]
+        L.oc_set_dis.argtypes = [vp, u64p, dp, i64]
+        L.oc_build.argtypes = [vp]
+        L.oc_init_equilibrium.argtypes = [vp, C.c_double, dp]
+        L.oc_level_size.restype = i64
+        L.oc_level_size.argtypes = [vp, i32]
+        L.oc_get_level.argtypes = [vp, i32, u64p, C.POINTER(C.c_uint32), dp, dp, dp, dp]
+        L.oc_set_level.argtypes = [vp, i32, dp, dp, dp, dp]
+        L.oc_get_force.argtypes = [vp, dp]
+        L.oc_reset_force.argtypes = [vp]
+        L.oc_step.argtypes = [vp, i32]
+        L.oc_neighbors.argtypes = [vp, i32, C.POINTER(C.c_int32)]
+        L.oc_neighbor_keys.argtypes = [vp, i32, u64p, i64, u64p]
+        L.oc_collide_cell.argtypes = [i32, i32, dp, C.c_double, dp, C.c_double, dp]
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class OracleCase:
+    """The CPU restatement of the reference step on one case."""
+
+    def __init__(self, case):
+        import sys
+        sys.path.insert(0, HERE)
+        from mortontrie_amr_b200.case import BC_MODES, COLLISIONS, IB_METHODS, STREAM_CONVENTIONS
+        self.case = case
+        p = case.params
+        m = case.mesh
+        self.q = p.q
+        self.L = m.spec.max_level
+        tau = np.array(p.taus(self.L), np.float64)
+        per = (C.c_int * 3)(*[int(b == "periodic") for b in m.spec.boundary])
+        ext = (C.c_int64 * 3)(*m.spec.coarse)
+        ubc = np.array(p.u_bc, np.float64)
+        self.h = lib().oc_case_new(p.q, self.L, COLLISIONS[p.collision], IB_METHODS[p.ib_method],
+                                   BC_MODES[p.bc_mode], STREAM_CONVENTIONS[p.stream_convention], per, ext,
+                                   _p(tau, C.c_double), p.rho0, _p(ubc, C.c_double))
+        if not self.h:
+            raise ValueError("oracle rejected the case parameters")
+        for l in range(self.L + 1):
+            for name, sid in SET_IDS.items():
+                k = np.ascontiguousarray(m.levels[l][name], np.uint64)
+                lib().oc_add_set(self.h, l, sid, _p(k, C.c_uint64), k.size)
+        for b in range(26):
+            k = np.ascontiguousarray(m.lat_bc[b], np.uint64)
+            lib().oc_add_set(self.h, 0, 16 + b, _p(k, C.c_uint64), k.size)
+        dk = np.ascontiguousarray(m.dis_keys, np.uint64)
+        dr = np.ascontiguousarray(m.dis_rows, np.float64)
+        if lib().oc_set_dis(self.h, _p(dk, C.c_uint64), _p(dr, C.c_double), dk.size) != 0:
+            raise ValueError("dis rows must be sorted by key")
+        if lib().oc_build(self.h) != 0:
+            raise ValueError("oracle build failed")
+        u0 = np.array(p.u_bc, np.float64)
+        lib().oc_init_equilibrium(self.h, p.rho0, _p(u0, C.c_double))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oc_case_free(self.h)
+            self.h = None
+
+    def size(self, l):
+        return int(lib().oc_level_size(self.h, l))
+
+    def get(self, l):
+        n = self.size(l)
+        keys = np.zeros(n, np.uint64)
+        tags = np.zeros(n, np.uint32)
+        f = np.zeros((self.q, n))
+        fcol = np.zeros((self.q, n))
+        rho = np.zeros(n)
+        u = np.zeros((n, 3))
+        lib().oc_get_level(self.h, l, _p(keys, C.c_uint64), _p(tags, C.c_uint32), _p(f, C.c_double),
+                           _p(fcol, C.c_double), _p(rho, C.c_double), _p(u, C.c_double))
+        return dict(keys=keys, tags=tags, f=f, fcol=fcol, rho=rho, u=u)
+
+    def set_populations(self, l, f, fcol=None):
+        f = np.ascontiguousarray(f, np.float64)
+        fc = f if fcol is None else np.ascontiguousarray(fcol, np.float64)
+        assert f.shape == (self.q, self.size(l))
+        lib().oc_set_level(self.h, l, _p(f, C.c_double), _p(fc, C.c_double), None, None)
+
+    def step(self, n=1):
+        rc = lib().oc_step(self.h, int(n))
+        if rc != 0:
+            raise RuntimeError(f"oracle step failed ({rc})")
+
+    def force(self):
+        out = np.zeros(4)
+        lib().oc_get_force(self.h, _p(out, C.c_double))
+        return out
+
+    def reset_force(self):
+        lib().oc_reset_force(self.h)
+
+    def neighbors(self, l):
+        n = self.size(l)
+        out = np.zeros((self.q - 1, n), np.int32)
+        lib().oc_neighbors(self.h, l, _p(out, C.c_int32))
+        return out
+
+    def neighbor_keys(self, l, keys):
+        keys = np.ascontiguousarray(keys, np.uint64)
+        out = np.zeros((keys.size, self.q), np.uint64)
+        lib().oc_neighbor_keys(self.h, l, _p(keys, C.c_uint64), keys.size, _p(out, C.c_uint64))
+        return out
+
+
+def collide_cell(q, collision, f, rho, u, tau):
+    f = np.ascontiguousarray(f, np.float64)
+    u = np.ascontiguousarray(u, np.float64)
+    out = np.zeros(q)
+    lib().oc_collide_cell(q, collision, _p(f, C.c_double), float(rho), _p(u, C.c_double), float(tau),
+                          _p(out, C.c_double))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# reference harness driver
+# ---------------------------------------------------------------------------
+def harness_input(case, nsteps, init=None) -> bytes:
+    """Serialise a case for oracle/refharness/harness.cpp (run_step)."""
+    from mortontrie_amr_b200.case import COLLISIONS, IB_METHODS
+    m = case.mesh
+    p = case.params
+    L = m.spec.max_level
+    b = bytearray()
+    b += struct.pack("<iiiii", p.q, L, COLLISIONS[p.collision], IB_METHODS[p.ib_method], nsteps)
+    b += struct.pack("<ddddd", p.nu, p.u_bc[0], p.u_bc[1], p.u_bc[2], p.u_ref)
+    for l in range(L + 1):
+        for name in SET_IDS:
+            k = np.ascontiguousarray(m.levels[l][name], np.uint64)
+            b += struct.pack("<q", k.size) + k.tobytes()
+    for i in range(26):
+        k = np.ascontiguousarray(m.lat_bc[i], np.uint64)
+        b += struct.pack("<q", k.size) + k.tobytes()
+    b += struct.pack("<q", m.dis_keys.size)
+    for k, row in zip(m.dis_keys, m.dis_rows):
+        b += struct.pack("<Q", int(k)) + np.ascontiguousarray(row, np.float64).tobytes()
+    if init is None:
+        b += struct.pack("<i", 0)
+    else:
+        b += struct.pack("<i", 1)
+        for (keys, f) in init:
+            b += struct.pack("<q", keys.size)
+            rec = np.zeros(keys.size, dtype=[("k", "<u8"), ("f", "<f8", (p.q,))])
+            rec["k"] = keys
+            rec["f"] = np.ascontiguousarray(f.T)
+            b += rec.tobytes()
+    return bytes(b)
+
+
+def parse_harness_output(data: bytes, q, L, nsteps):
+    off = 0
+    secs = struct.unpack_from("<d", data, off)[0]
+    off += 8
+    levels = []
+    for _ in range(L + 1):
+        n = struct.unpack_from("<q", data, off)[0]
+        off += 8
+        dt = np.dtype([("k", "<u8"), ("v", "<f8", (2 * q + 4,))])
+        rec = np.frombuffer(data, dt, n, off)
+        off += n * dt.itemsize
+        v = rec["v"]
+        levels.append(dict(keys=rec["k"].copy(), f=np.ascontiguousarray(v[:, :q].T), fcol=np.ascontiguousarray(v[:, q:2 * q].T),
+                           rho=v[:, 2 * q].copy(), u=v[:, 2 * q + 1:2 * q + 4].copy()))
+    nf = struct.unpack_from("<q", data, off)[0]
+    off += 8
+    force = np.frombuffer(data, "<f8", nf, off).reshape(-1, 4).copy()
+    off += nf * 8
+    tau = np.frombuffer(data, "<f8", L + 1, off).copy()
+    return dict(seconds=secs, levels=levels, force=force, tau=tau)
+
+
+def run_harness(case, nsteps, init=None, timeout=600):
+    import build
+    q, L = case.params.q, case.mesh.spec.max_level
+    exe = build.build_refharness(q, L)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as fh:
+            fh.write(harness_input(case, nsteps, init))
+        subprocess.run([exe, "step", fin, fout], check=True, timeout=timeout)
+        with open(fout, "rb") as fh:
+            return parse_harness_output(fh.read(), q, L, nsteps)
+
+
+def run_harness_morton(q, L, levels, keys, timeout=120):
+    import build
+    exe = build.build_refharness(q, L)
+    levels = np.ascontiguousarray(levels, np.int32)
+    keys = np.ascontiguousarray(keys, np.uint64)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as fh:
+            fh.write(struct.pack("<q", keys.size) + levels.tobytes() + keys.tobytes())
+        subprocess.run([exe, "morton", fin, fout], check=True, timeout=timeout)
+        return np.fromfile(fout, np.uint64).reshape(keys.size, q)

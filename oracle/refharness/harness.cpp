@@ -1,0 +1,257 @@
+/*
+ * harness.cpp -- drives the reference's own LBM translation units
+ * (LBM_Manager.cpp, LBM_Simulator.cpp, lbm_kernel/*, BC/*,
+ * ComplexBoundary_Manager.cpp, Morton_Assist.cpp) on index sets supplied in
+ * a binary file, and dumps the populations it produces.
+ *
+ * TEST INFRASTRUCTURE ONLY: it generates the golden vectors that pin the
+ * oracle and times the reference CPU path.  The reference mesher cannot
+ * produce box-refined meshes (Grid_Manager.cpp:99-102 leaves intermediate
+ * levels empty), so the harness fills Lat_Manager's public sets directly and
+ * sets dx[l] on every level (the reference only sets the finest one,
+ * Lat_Voxelize.cpp:422), then runs LBM_Manager::LBMkernel(0) followed by the
+ * all-level macroscopic update, i.e. the body of LBM_Manager::fluidSimulate
+ * (LBM_Simulator.cpp:8-18) without the diagnostics print and Tecplot output.
+ *
+ * usage: harness step  <in.bin> <out.bin>
+ *        harness morton <in.bin> <out.bin>     (neighbour-key known answers)
+ */
+#include <algorithm>
+#include <array>
+#include <bitset>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <set>
+#include <sstream>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <unordered_set>
+#include <vector>
+
+/* the harness reaches LBM_Manager's private stepping entry point and state */
+#define private public
+#define protected public
+#include "General.h"
+#include "Constants.h"
+#include "Morton_Assist.h"
+#include "Lat_Manager.hpp"
+#include "LBM_Manager.hpp"
+#include "IO_Manager.h"
+#include "lbm_kernel/Collision_Model_Factory.hpp"
+#include "lbm_kernel/Stream_Manager.hpp"
+#include "ComplexBoundary_Manager.hpp"
+#include "BC/D3Q19_BC_Manager.hpp"
+#undef private
+#undef protected
+
+/* static members whose definitions live in translation units the harness
+ * does not build (Grid_Manager.cpp, Lat_Manager.cpp, Obj_Manager.cpp ...) */
+Morton_Assist *Morton_Assist::pointer_me;
+std::array<D_morton, C_max_level + 1> Morton_Assist::ref_one;
+std::array<std::array<D_morton, 2>, C_max_level + 1> Morton_Assist::xmorton_ref;
+std::array<std::array<D_morton, 2>, C_max_level + 1> Morton_Assist::ymorton_ref;
+std::array<std::array<D_morton, 2>, C_max_level + 1> Morton_Assist::zmorton_ref;
+std::array<D_morton, C_max_level + 1> Morton_Assist::morton_xyz;
+std::array<D_morton, C_max_level + 1> Morton_Assist::morton_xyz_flip;
+D_morton Morton_Assist::mortonx_min, Morton_Assist::mortonx_max;
+D_morton Morton_Assist::mortony_min, Morton_Assist::mortony_max;
+D_morton Morton_Assist::mortonz_min, Morton_Assist::mortonz_max;
+Lat_Manager *Lat_Manager::pointer_me;
+LBM_Manager *LBM_Manager::pointer_me;
+IO_Manager *IO_Manager::pointer_me;
+std::ofstream *Log_function::logfile;
+void IO_Manager::writeFlow(const D_int) {}
+
+namespace {
+
+struct Reader {
+    FILE *fp;
+    template <class T> T get()
+    {
+        T v;
+        if (fread(&v, sizeof(T), 1, fp) != 1) throw std::runtime_error("short input");
+        return v;
+    }
+    template <class T> std::vector<T> vec(int64_t n)
+    {
+        std::vector<T> v((size_t)n);
+        if (n && fread(v.data(), sizeof(T), (size_t)n, fp) != (size_t)n) throw std::runtime_error("short input");
+        return v;
+    }
+};
+
+D_morton K(uint64_t k) { return D_morton(k); }
+
+void setup_morton(Morton_Assist &ma)
+{
+    Morton_Assist::pointer_me = &ma;
+    ma.morton_initial();
+    for (unsigned l = 0; l <= C_max_level; ++l) Morton_Assist::compute_ref(l);
+}
+
+int run_morton(Reader &in, FILE *out)
+{
+    Morton_Assist ma;
+    setup_morton(ma);
+    int64_t n = in.get<int64_t>();
+    auto lev = in.vec<int32_t>(n);
+    auto keys = in.vec<uint64_t>(n);
+    for (int64_t i = 0; i < n; ++i)
+        for (int q = 0; q < C_Q; ++q) {
+            uint64_t r = Morton_Assist::find_neighbor(K(keys[i]), (uint)lev[i], ex[q], ey[q], ez[q]).to_ullong();
+            fwrite(&r, 8, 1, out);
+        }
+    return 0;
+}
+
+int run_step(Reader &in, FILE *out)
+{
+    Morton_Assist ma;
+    setup_morton(ma);
+    int32_t q = in.get<int32_t>(), L = in.get<int32_t>();
+    if (q != C_Q || L != (int32_t)C_max_level) {
+        fprintf(stderr, "harness built for Q=%d L=%d, input has Q=%d L=%d\n", C_Q, (int)C_max_level, q, L);
+        return 2;
+    }
+    int32_t collision = in.get<int32_t>(), ib_fh = in.get<int32_t>(), nsteps = in.get<int32_t>();
+    sphere::U_kineViscosity = in.get<double>();
+    sphere::U_u0 = in.get<double>();
+    sphere::U_v0 = in.get<double>();
+    sphere::U_w0 = in.get<double>();
+    sphere::R_velocity = in.get<double>();
+    sphere::U_dynaViscosity = sphere::U_kineViscosity * U_rho0;
+    sphere::R_Re = sphere::R_velocity * R_length / sphere::U_kineViscosity;
+
+    Lat_Manager lm;
+    Lat_Manager::pointer_me = &lm;
+    std::array<D_mapLat, C_max_level + 1> *maps[5] = {&lm.lat_f, &lm.lat_overlap_F2C, &lm.lat_overlap_C2F,
+                                                     &lm.ghost_overlap_C2F, &lm.ghost_overlap_F2C};
+    const int flags[5] = {FLUID, OVERLAP_F2C, OVERLAP_C2F, OVERLAP_GHOST, OVERLAP_GHOST};
+    for (int l = 0; l <= L; ++l) {
+        for (int s = 0; s < 6; ++s) {
+            int64_t n = in.get<int64_t>();
+            auto keys = in.vec<uint64_t>(n);
+            for (auto k : keys) {
+                if (s < 5)
+                    (*maps[s])[l].insert(std::make_pair(K(k), Cell(flags[s])));
+                else
+                    lm.lat_sf.insert(std::make_pair(K(k), Cell(SOLID)));
+            }
+        }
+        lm.dx[l] = C_dx / (double)two_power_n(l);
+    }
+    for (int b = 0; b < 26; ++b) {
+        int64_t n = in.get<int64_t>();
+        auto keys = in.vec<uint64_t>(n);
+        for (auto k : keys) lm.lat_bc[b].insert(K(k));
+    }
+    {
+        int64_t n = in.get<int64_t>();
+        for (int64_t i = 0; i < n; ++i) {
+            uint64_t k = in.get<uint64_t>();
+            auto row = in.vec<double>(C_Q - 1);
+            std::array<D_real, C_Q - 1> a;
+            for (int j = 0; j < C_Q - 1; ++j) a[j] = row[j];
+            lm.dis.insert(std::make_pair(K(k), a));
+        }
+    }
+
+    LBM_Manager *mgr = new LBM_Manager();
+    if (collision == 1) mgr->collideModel = Collision_Model_Factory::createCollisionModel("Cumulant");
+    if (!ib_fh) mgr->solidBCModel = new SinglePointInterpolation(mgr->user, IB_Method::DISTANCE_WEIGHTED);
+    mgr->initialBC();
+
+    int32_t init_mode = in.get<int32_t>();
+    if (init_mode == 1) {
+        for (int l = 0; l <= L; ++l) {
+            int64_t n = in.get<int64_t>();
+            for (int64_t i = 0; i < n; ++i) {
+                uint64_t k = in.get<uint64_t>();
+                auto f = in.vec<double>(C_Q);
+                for (int j = 0; j < C_Q; ++j) {
+                    mgr->user[l].df.f[j].at(K(k)) = f[j];
+                    mgr->user[l].df.fcol[j].at(K(k)) = f[j];
+                }
+            }
+        }
+    }
+
+    std::vector<double> force;
+    auto t0 = std::chrono::steady_clock::now();
+    for (int s = 0; s < nsteps; ++s) {
+        mgr->LBMkernel(0);
+        mgr->calculateMacros();
+        force.push_back(mgr->m_ibFx_sum);
+        force.push_back(mgr->m_ibFy_sum);
+        force.push_back(mgr->m_ibFz_sum);
+        force.push_back((double)mgr->m_ibForce_count);
+        mgr->m_ibFx_sum = mgr->m_ibFy_sum = mgr->m_ibFz_sum = 0.0;
+        mgr->m_ibForce_count = 0;
+    }
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+
+    fwrite(&secs, 8, 1, out);
+    for (int l = 0; l <= L; ++l) {
+        std::vector<uint64_t> keys;
+        for (auto &kv : mgr->user[l].df.f[0]) keys.push_back(kv.first.to_ullong());
+        std::sort(keys.begin(), keys.end());
+        int64_t n = (int64_t)keys.size();
+        fwrite(&n, 8, 1, out);
+        for (auto k : keys) {
+            fwrite(&k, 8, 1, out);
+            double rec[2 * C_Q + 4];
+            for (int j = 0; j < C_Q; ++j) {
+                rec[j] = mgr->user[l].df.f[j].at(K(k));
+                rec[C_Q + j] = mgr->user[l].df.fcol[j].at(K(k));
+            }
+            auto d = mgr->user[l].density.find(K(k));
+            auto v = mgr->user[l].velocity.find(K(k));
+            rec[2 * C_Q] = d == mgr->user[l].density.end() ? NAN : d->second;
+            rec[2 * C_Q + 1] = v == mgr->user[l].velocity.end() ? NAN : v->second.x;
+            rec[2 * C_Q + 2] = v == mgr->user[l].velocity.end() ? NAN : v->second.y;
+            rec[2 * C_Q + 3] = v == mgr->user[l].velocity.end() ? NAN : v->second.z;
+            fwrite(rec, 8, 2 * C_Q + 4, out);
+        }
+    }
+    int64_t nf = (int64_t)force.size();
+    fwrite(&nf, 8, 1, out);
+    fwrite(force.data(), 8, force.size(), out);
+    double tau[C_max_level + 1];
+    for (unsigned l = 0; l <= C_max_level; ++l) tau[l] = mgr->tau[l];
+    fwrite(tau, 8, C_max_level + 1, out);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    if (argc != 4) {
+        fprintf(stderr, "usage: %s step|morton <in.bin> <out.bin>\n", argv[0]);
+        return 2;
+    }
+    std::ofstream devnull("/dev/null");
+    Log_function::logfile = &devnull;
+    if (!freopen("/dev/null", "w", stdout)) return 3;
+    FILE *fin = fopen(argv[2], "rb");
+    FILE *fout = fopen(argv[3], "wb");
+    if (!fin || !fout) return 3;
+    Reader rd{fin};
+    int rc;
+    try {
+        rc = std::string(argv[1]) == "morton" ? run_morton(rd, fout) : run_step(rd, fout);
+    } catch (const std::exception &e) {
+        fprintf(stderr, "harness: %s\n", e.what());
+        rc = 4;
+    }
+    fclose(fout);
+    fclose(fin);
+    return rc;
+}
