@@ -1,0 +1,369 @@
+"""Benchmark: uniform single-level roofline case of the LBM time step.
+
+Workload: D3Q19 LBGK on a 256^3 fully periodic Morton-ordered grid,
+Taylor-Green initial field (u0 = 0.02, wavenumber 2 pi / 256, rho = 1 plus
+the pressure term), tau = 0.6.  A step is one time step of the whole grid;
+the headline runs FP32 arithmetic on populations stored as FP16 deviations
+f - w_q (76 B per cell update), the FP64 / FP32 / BF16 storages are timed
+beside it.  Inputs stay resident in HBM (state 637 MB at FP16, larger than
+the 126 MB L2, so no flush between steps).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank runs its own replica of the case on its own GPU
+(the path has no exchange step; weak scaling, no collective on the data
+path); the time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_EDGE = 256
+Q = 19
+TAU = 0.6
+NU = (TAU - 0.5) / 3.0
+U0 = 0.02
+BYTES_PER_CELL = {"f64": 2 * Q * 8, "f32": 2 * Q * 4, "f16": 2 * Q * 2, "bf16": 2 * Q * 2}
+WORKLOAD = "uniform 256^3 periodic Taylor-Green, D3Q19 LBGK, tau=0.6, u0=0.02"
+
+
+def measured_hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic(key):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            return json.load(fh).get(key)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.1)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        # samples under load: clock above the idle floor
+        loaded = [v for v in sm if v > 0.5 * max(sm)] if sm else []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in rows for j in range(4) if r[5 + j].lower() == "active"})
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300),
+                                device_id=None)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def tgv_fields():
+    from mortontrie_amr_b200.case import taylor_green_fields
+    from mortontrie_amr_b200.lbm import morton_order_fields
+    rho, u, v, w = taylor_green_fields((N_EDGE,) * 3, U0)
+    return morton_order_fields(N_EDGE, rho, u, v, w)
+
+
+def make_case(storage):
+    from mortontrie_amr_b200.case import uniform_box_case
+    return uniform_box_case(q=Q, n=(N_EDGE,) * 3, nu=NU, storage=storage, u_ref=U0)
+
+
+def time_steps(ctx, dense, steps, warmup, world, torch):
+    """Device time of `steps` steps on the library's stream (= torch's
+    current stream), max over ranks; returns (seconds, launches)."""
+    stream = torch.cuda.current_stream()
+    dense.step(warmup)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = ctx.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dense.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    launches = ctx.launch_count() - l0
+    secs = e0.elapsed_time(e1) / 1e3
+    return max_over_ranks(secs, world), launches
+
+
+def run_ours(args):
+    import torch
+
+    from mortontrie_amr_b200.lbm import Context, DenseCase
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    fields = tgv_fields()
+    n_cells = N_EDGE ** 3
+    peak, peak_kind = measured_hbm_peak()
+
+    # headline: FP16 shifted storage
+    case = make_case("f16")
+    dense = DenseCase(ctx, case, "f16")
+    dense.init_fields(*fields)
+    sampler = ClockSampler(local)
+    if rank == 0:
+        sampler.start()
+    secs, launches = time_steps(ctx, dense, args.steps, args.warmup, world, torch)
+    clocks = sampler.stop() if rank == 0 else None
+    mlups = world * n_cells * args.steps / secs / 1e6
+    per_launch = secs / args.steps
+    achieved = BYTES_PER_CELL["f16"] * n_cells / per_launch / 1e9
+    red = dense.reduce()
+    del dense
+
+    # storage variants, same workload
+    variants = {}
+    for st in (() if args.quick else ("f64", "f32", "bf16")):
+        d = DenseCase(ctx, make_case(st), st)
+        d.init_fields(*fields)
+        s, _ = time_steps(ctx, d, args.steps, args.warmup, world, torch)
+        bw = BYTES_PER_CELL[st] * n_cells / (s / args.steps) / 1e9
+        variants[st] = {"mlups": round(world * n_cells * args.steps / s / 1e6, 1),
+                        "bytes_per_cell_update": BYTES_PER_CELL[st], "achieved_gbs": round(bw, 1),
+                        "frac": round(bw / peak, 4)}
+        del d
+
+    # end to end through the public API: pinned host fields -> device, the
+    # steps, density + velocity back to pinned host memory
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "edge": N_EDGE, "mlups": round(mlups, 1),
+                              "achieved_gbs": round(achieved, 1), "launches": int(launches)}), flush=True)
+        ctx.close()
+        return
+    host = [torch.from_numpy(f).pin_memory() for f in fields]
+    out_rho = torch.empty(n_cells, dtype=torch.float64).pin_memory()
+    out_u = torch.empty(3 * n_cells, dtype=torch.float64).pin_memory()
+    d = DenseCase(ctx, case, "f16")
+    stream = torch.cuda.current_stream()
+    d.init_fields_ptr(*[h.data_ptr() for h in host])
+    d.step(args.warmup)
+    d.macros_ptr(out_rho.data_ptr(), out_u.data_ptr())
+    torch.cuda.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    d.init_fields_ptr(*[h.data_ptr() for h in host])
+    d.step(args.steps)
+    d.macros_ptr(out_rho.data_ptr(), out_u.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    barrier(world)
+    e2e_secs = max_over_ranks(e0.elapsed_time(e1) / 1e3, world)
+    h2d = 4 * 8 * n_cells
+    d2h = 4 * 8 * n_cells
+    e2e = {"value": round(world * n_cells * args.steps / e2e_secs / 1e6, 1), "unit": "MLUPS",
+           "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
+           "h2d_bytes_per_solve": h2d, "d2h_bytes_per_solve": d2h, "steps_per_solve": args.steps,
+           "wall_s": round(wall, 4),
+           "path": "mt_case_init_fields (pinned FP64 rho,u) -> mt_step x K -> mt_case_get_macros (pinned)"}
+    del d
+
+    if rank == 0:
+        cpu = cpu_baseline_sample() if (world == 1 and not args.no_cpu_baseline) else None
+        traffic = committed_traffic("k_dense_q19_f16_256")
+        line = {
+            "metric": "fine-level MLUPS (uniform case), %HBM roofline",
+            "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * secs / args.steps, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": n_cells, "storage": "f16 deviations f - w_q",
+                       "bytes_per_cell_update": BYTES_PER_CELL["f16"], "levels": 1,
+                       "l2": "state 637 MB > 126 MB L2; no flush", "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "k_dense<19, half, LBGK, fused>",
+                         "algorithmic_bytes_per_launch": BYTES_PER_CELL["f16"] * n_cells},
+            "variants": variants,
+            "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+            "diagnostics": {"mass": red["mass"], "kinetic_energy": red["kinetic_energy"]},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def _reference_sample_case():
+    """Bounded CPU sample of the workload for the reference's own code: a
+    48^3 single populated level (the reference needs a second, empty level
+    and has no periodic wrap, so the box is closed by its non-equilibrium
+    extrapolation boundary), D3Q19 LBGK, tau 0.6."""
+    from mortontrie_amr_b200.case import uniform_box_case
+    return uniform_box_case(q=Q, n=(48, 48, 48), nu=NU, boundary=("bc", "bc", "bc"), empty_levels=1,
+                            u_bc=(U0, 0.0, 0.0), u_ref=U0)
+
+
+def cpu_reference_run(nprocs, steps, warmup):
+    """Run `nprocs` single-threaded reference harness processes at once (one
+    per core, the reference has no threading); returns (MLUPS, kind, cores,
+    sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    case = _reference_sample_case()
+    n_fluid = int(case.mesh.levels[0]["lat_f"].size)
+    try:
+        import oracle as O
+        import build as B
+        have_ref = os.path.exists(B.harness_path(Q, 1)) or os.path.isdir(B.REF)
+    except Exception:
+        have_ref = False
+    if have_ref:
+        with tempfile.TemporaryDirectory() as td:
+            procs = [O.start_harness(case, steps, td, i, nwarm=warmup) for i in range(nprocs)]
+            secs = []
+            for p, out in procs:
+                p.wait(timeout=3600)
+                if p.returncode != 0:
+                    raise RuntimeError("reference harness failed")
+                with open(out, "rb") as fh:
+                    secs.append(O.parse_harness_output(fh.read(), Q, 1, steps)["seconds"])
+        mlups = nprocs * n_fluid * steps / max(secs) / 1e6
+        kind = "reference"
+    else:
+        import oracle as O
+        oc = O.OracleCase(case)
+        oc.step(warmup)
+        t = time.perf_counter()
+        oc.step(steps)
+        mlups = n_fluid * steps / (time.perf_counter() - t) / 1e6
+        kind, nprocs = "port", 1
+    sample = (f"{nprocs} process(es) x {steps} steps of a 48^3 D3Q19 LBGK box ({n_fluid} stepped cells each), "
+              f"hash-map backend, 1 thread per process")
+    return mlups, kind, nprocs, sample
+
+
+def cpu_baseline_sample():
+    mlups, kind, cores, sample = cpu_reference_run(1, 12, 1)
+    return {"value": round(mlups, 4), "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    nprocs = max(1, min(os.cpu_count() or 1, 32))
+    # each bench step is one time step of every sample process
+    mlups, kind, cores, sample = cpu_reference_run(nprocs, max(1, args.steps // 25), max(0, min(args.warmup, 2)))
+    line = {
+        "impl": "reference", "metric": "fine-level MLUPS (uniform case), %HBM roofline", "value": round(mlups, 4),
+        "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": sample},
+        "cpu_baseline": {"value": round(mlups, 4), "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": round(mlups, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--edge", type=int, default=256, help="cube edge (power of two); 256 is the configuration")
+    ap.add_argument("--quick", action="store_true", help="headline kernel only (profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    global N_EDGE
+    N_EDGE = args.edge
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,151 @@
+/*
+ * mt_lbm.h -- C ABI of libmtlbm, the B200 (sm_100a) implementation of the
+ * multi-level lattice-Boltzmann time step of MortonTrieCode-CAD2025/
+ * mortonTrie_AMR.
+ *
+ * Every function returns an int status (MT_OK or a negative MT_ERR_* code);
+ * none aborts the process.  mt_last_error() gives a readable message for the
+ * last failure on a context.  Device memory is owned by the context; host
+ * buffers are owned by the caller.  Populations cross the boundary as FP64
+ * structure-of-arrays [Q][n], n cells of one level in ascending Morton-key
+ * order (the order mt_case_get_keys returns).
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   D_map_define<T>            header/Grid_Class.h:116-137, header/user.h:18-45
+ *   Lat_Manager index sets     header/Lat_Manager.hpp:245-316
+ *   LBM_Manager                header/LBM_Manager.hpp:25-119
+ *   Collision_Model::collide   header/lbm_kernel/Collision_Manager.hpp:73-97
+ *   Stream_Model::stream       header/lbm_kernel/Stream_Manager.hpp:12-37
+ *   ComplexBoundary_Model      header/ComplexBoundary_Manager.hpp:16-46
+ *   D3Q19_BC_Strategy/Manager  header/BC/D3Q19_BC_Manager.hpp:15-263
+ */
+#ifndef MT_LBM_H
+#define MT_LBM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MT_MAX_LEVELS 8
+
+/* status codes */
+#define MT_OK 0
+#define MT_ERR_ARG (-1)      /* bad argument or unsupported combination */
+#define MT_ERR_CUDA (-2)     /* a CUDA call failed */
+#define MT_ERR_STATE (-3)    /* call out of order (e.g. step before build) */
+#define MT_ERR_MESH (-4)     /* index sets violate the contract (missing child / neighbour) */
+#define MT_ERR_NONFINITE (-5) /* the device guard found a NaN/Inf population */
+
+/* lattice index sets, Lat_Manager.hpp:245-316 */
+#define MT_SET_LAT_F 0
+#define MT_SET_OVERLAP_F2C 1
+#define MT_SET_OVERLAP_C2F 2
+#define MT_SET_GHOST_C2F 3
+#define MT_SET_GHOST_F2C 4
+#define MT_SET_LAT_SF 5
+#define MT_SET_LAT_BC0 16 /* MT_SET_LAT_BC0 + b, b = 0..25 in Bdry_Type order (D3Q19_BC_Manager.hpp:25-53) */
+
+#define MT_COLL_LBGK 0     /* Collision_LBGK, lbm_kernel/Collision_Manager.cpp:13-53 */
+#define MT_COLL_CUMULANT 1 /* Collision_Cumulant, lbm_kernel/Collision_Cumulant.cpp:22-652 (Q = 27) */
+#define MT_IB_DW 0         /* SinglePointInterpolation, distance weighted */
+#define MT_IB_FH 1         /* SinglePointInterpolation, Filippova-Haenel */
+#define MT_BC_NEQ 0        /* nonEquilibrumExtrapolation_* (BC/NonEquilibrumExtrapolation.cpp) */
+#define MT_BC_ZOUHE_OUTFLOW 1 /* velocity inlet on West, zero-gradient outflow on East */
+#define MT_PULL_REFERENCE 0   /* f_q(x) = fcol_q(x + e_q), Stream_Manager.cpp:43-76 */
+#define MT_PULL_TEXTBOOK 1    /* f_q(x) = fcol_q(x - e_q) */
+#define MT_STORE_F64 0
+#define MT_STORE_F32 1  /* FP32 storage of f - w_q, FP32 arithmetic */
+#define MT_STORE_F16 2  /* FP16 storage of f - w_q, FP32 arithmetic */
+#define MT_STORE_BF16 3 /* BF16 storage of f - w_q, FP32 arithmetic */
+
+/* Case description: the switches the reference hard-codes in
+ * LBM_Manager::LBM_Manager (LBM_Manager.cpp:32-95) and its per-level
+ * relaxation times from LBM_Manager::setUnit (LBM_Manager.cpp:763-844). */
+typedef struct mt_case_desc {
+    int32_t q;                 /* 19 or 27 */
+    int32_t max_level;         /* C_max_level, 0 .. MT_MAX_LEVELS-1 */
+    int32_t collision;         /* MT_COLL_* */
+    int32_t ib_method;         /* MT_IB_* */
+    int32_t bc_mode;           /* MT_BC_* */
+    int32_t stream_convention; /* MT_PULL_* */
+    int32_t storage;           /* MT_STORE_* (the multi-level path supports MT_STORE_F64) */
+    int32_t periodic[3];       /* per axis: 1 wraps neighbours (no reference counterpart; BC/Periodic.cpp is dead code) */
+    int64_t extent0[3];        /* level-0 cells per axis */
+    double tau[MT_MAX_LEVELS]; /* LBM_Manager::tau */
+    double rho0;               /* U_rho0 / CF_Rho */
+    double u_bc[3];            /* boundary velocity in lattice units (input_v / CF_U) */
+} mt_case_desc;
+
+typedef struct mt_ctx mt_ctx;
+
+/* ---- context ---------------------------------------------------------- */
+int mt_create(int32_t device, mt_ctx **out);
+int mt_destroy(mt_ctx *ctx);
+const char *mt_last_error(const mt_ctx *ctx);
+/* run all work of this context on a caller-owned cudaStream_t (NULL: own stream) */
+int mt_set_stream(mt_ctx *ctx, void *cuda_stream);
+int mt_synchronize(mt_ctx *ctx);
+/* kernels launched by this context so far (graph replays count their nodes) */
+int mt_launch_count(const mt_ctx *ctx, int64_t *out);
+
+/* ---- case setup: LBM_Manager::LBM_Manager + allocMacrosAndDDF --------- */
+int mt_case_create(mt_ctx *ctx, const mt_case_desc *desc, int32_t *case_id);
+/* Dense periodic Morton cube (no counterpart in the reference): max_level 0,
+ * all axes periodic, equal power-of-two extents; every cell is lat_f and the
+ * key set is generated on the device. */
+int mt_case_create_dense(mt_ctx *ctx, const mt_case_desc *desc, int32_t *case_id);
+int mt_case_destroy(mt_ctx *ctx, int32_t case_id);
+/* add keys to one index set of one level (Lat_Manager::lat_f[l].insert ...) */
+int mt_case_add_set(mt_ctx *ctx, int32_t case_id, int32_t level, int32_t set_id, const uint64_t *keys, int64_t n);
+/* Lat_Manager::dis: finest-level keys (ascending) and Q-1 wall distances each */
+int mt_case_set_dis(mt_ctx *ctx, int32_t case_id, const uint64_t *keys, const double *rows, int64_t n);
+/* device build: radix sort + unique of the keys, set tags, neighbour table
+ * by binary search of the Morton neighbour keys (Morton_Assist::find_neighbor
+ * + D_map_define::find), explosion/coalescence child tables, IB list */
+int mt_case_build(mt_ctx *ctx, int32_t case_id);
+int mt_case_level_size(mt_ctx *ctx, int32_t case_id, int32_t level, int64_t *n);
+int mt_case_get_keys(mt_ctx *ctx, int32_t case_id, int32_t level, uint64_t *keys, uint32_t *tags);
+/* neighbour table [(Q-1)][n]: index of the cell at key + e_k, or -1 */
+int mt_case_get_neighbors(mt_ctx *ctx, int32_t case_id, int32_t level, int32_t *nbr);
+/* D_map_define::find in bulk: index of each key on the level, or -1 */
+int mt_find(mt_ctx *ctx, int32_t case_id, int32_t level, const uint64_t *keys, int64_t n, int64_t *idx);
+
+/* ---- state ------------------------------------------------------------ */
+/* reference initial state (LBM_Manager.cpp:482-592, 296-304): f = fcol =
+ * feq(rho0, u0) on every stored cell, zero on solid cells */
+int mt_case_init_equilibrium(mt_ctx *ctx, int32_t case_id, double rho0, const double *u0);
+/* f = fcol = feq(rho_i, u_i) per cell from host fields [n] (dense path) */
+int mt_case_init_fields(mt_ctx *ctx, int32_t case_id, const double *rho, const double *ux, const double *uy,
+                        const double *uz);
+int mt_case_set_populations(mt_ctx *ctx, int32_t case_id, int32_t level, const double *f, const double *fcol);
+int mt_case_get_populations(mt_ctx *ctx, int32_t case_id, int32_t level, double *f, double *fcol);
+/* density [n] and velocity [3][n] of a level (density/velocity maps of User) */
+int mt_case_get_macros(mt_ctx *ctx, int32_t case_id, int32_t level, double *rho, double *u);
+/* FP64 reductions over the stepped cells: mass, x/y/z momentum (dense path) */
+int mt_case_reduce(mt_ctx *ctx, int32_t case_id, double *out4);
+
+/* ---- the reference call surface --------------------------------------- */
+int mt_calculate_macros(mt_ctx *ctx, int32_t case_id, int32_t level); /* LBM_Manager::calculateMacros(level) */
+int mt_collide(mt_ctx *ctx, int32_t case_id, int32_t level);          /* Collision_Model::collide(level) */
+int mt_stream(mt_ctx *ctx, int32_t case_id, int32_t level);           /* ABPatternPull::stream(level) */
+int mt_explosion(mt_ctx *ctx, int32_t case_id, int32_t level);        /* LBM_Manager::AMR_transDDF_explosion */
+int mt_coalescence(mt_ctx *ctx, int32_t case_id, int32_t level);      /* LBM_Manager::AMR_transDDF_coalescence */
+int mt_apply_bc(mt_ctx *ctx, int32_t case_id);                        /* applyBoundaryCondition(face, "AfterStream") x 6 */
+int mt_ib_treat(mt_ctx *ctx, int32_t case_id);                        /* ComplexBoundary_Model::treat */
+int mt_lbm_kernel(mt_ctx *ctx, int32_t case_id, int32_t level);       /* LBM_Manager::LBMkernel(level) */
+/* n coarse steps of LBM_Manager::fluidSimulate (LBM_Simulator.cpp:11-17):
+ * LBMkernel(0) then calculateMacros() on every level, replayed from a CUDA
+ * graph; asynchronous on the context stream */
+int mt_step(mt_ctx *ctx, int32_t case_id, int32_t n_coarse_steps);
+/* accumulated momentum-exchange force of treat() calls: fx, fy, fz, count
+ * (LBM_Manager::accumIBForce, LBM_Manager.cpp:846-852) */
+int mt_get_force(mt_ctx *ctx, int32_t case_id, double *out4);
+int mt_reset_force(mt_ctx *ctx, int32_t case_id);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MT_LBM_H */

@@ -1,0 +1,590 @@
+// C ABI of libmtlbm (declarations and reference citations in include/mt_lbm.h).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+#include "mt_internal.hpp"
+
+extern template struct mt::DenseOps<double>;
+extern template struct mt::DenseOps<float>;
+extern template struct mt::DenseOps<__half>;
+extern template struct mt::DenseOps<__nv_bfloat16>;
+
+struct mt_ctx {
+    mt::Ctx c;
+};
+
+namespace mt {
+
+int set_err(Ctx &ctx, int code, const std::string &msg)
+{
+    ctx.last_error = msg;
+    return code;
+}
+
+namespace {
+
+enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT };
+
+int get_case(mt_ctx *h, int32_t id, Case **out)
+{
+    if (!h) return MT_ERR_ARG;
+    Ctx &ctx = h->c;
+    if (id < 0 || id >= (int32_t)ctx.cases.size() || !ctx.cases[id])
+        return set_err(ctx, MT_ERR_ARG, "unknown case id");
+    *out = ctx.cases[id];
+    return MT_OK;
+}
+
+int check_desc(Ctx &ctx, const mt_case_desc *d)
+{
+    if (!d) return set_err(ctx, MT_ERR_ARG, "null case description");
+    if (d->q != 19 && d->q != 27) return set_err(ctx, MT_ERR_ARG, "q must be 19 or 27");
+    if (d->max_level < 0 || d->max_level >= MT_MAX_LEVELS) return set_err(ctx, MT_ERR_ARG, "max_level out of range");
+    if (d->collision != MT_COLL_LBGK && d->collision != MT_COLL_CUMULANT)
+        return set_err(ctx, MT_ERR_ARG, "unknown collision model");
+    if (d->collision == MT_COLL_CUMULANT && d->q != 27)
+        return set_err(ctx, MT_ERR_ARG, "the cumulant collision needs D3Q27");
+    if (d->storage < MT_STORE_F64 || d->storage > MT_STORE_BF16) return set_err(ctx, MT_ERR_ARG, "unknown storage");
+    for (int l = 0; l <= d->max_level; ++l)
+        if (!(d->tau[l] > 0.5)) return set_err(ctx, MT_ERR_ARG, "tau must exceed 1/2 on every level");
+    for (int a = 0; a < 3; ++a)
+        if (d->extent0[a] <= 0 || d->extent0[a] > ((int64_t)1 << (21 - d->max_level)))
+            return set_err(ctx, MT_ERR_ARG, "extent does not fit the 21-bit Morton coordinate");
+    return MT_OK;
+}
+
+int add_case(Ctx &ctx, Case *c, int32_t *id)
+{
+    ctx.cases.push_back(c);
+    *id = (int32_t)ctx.cases.size() - 1;
+    return MT_OK;
+}
+
+template <class F> int dense_dispatch(Case &c, F &&fn)
+{
+    switch (c.d.storage) {
+    case MT_STORE_F64: return fn((double *)nullptr);
+    case MT_STORE_F32: return fn((float *)nullptr);
+    case MT_STORE_F16: return fn((__half *)nullptr);
+    default: return fn((__nv_bfloat16 *)nullptr);
+    }
+}
+
+size_t storage_bytes(int s) { return s == MT_STORE_F64 ? 8 : (s == MT_STORE_F32 ? 4 : 2); }
+
+int phase_call(mt_ctx *h, int32_t id, int phase, int level)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    if (c->dense) return set_err(h->c, MT_ERR_STATE, "per-phase calls need a multi-level case (use mt_step)");
+    if (!c->built) return set_err(h->c, MT_ERR_STATE, "case not built");
+    return amr_phase(h->c, *c, phase, level);
+}
+
+}  // namespace
+}  // namespace mt
+
+using namespace mt;
+
+extern "C" {
+
+int mt_create(int32_t device, mt_ctx **out)
+{
+    if (!out) return MT_ERR_ARG;
+    *out = nullptr;
+    mt_ctx *h = new (std::nothrow) mt_ctx();
+    if (!h) return MT_ERR_ARG;
+    h->c.device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->c.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete h;
+        return MT_ERR_CUDA;
+    }
+    h->c.own_stream = true;
+    *out = h;
+    return MT_OK;
+}
+
+int mt_destroy(mt_ctx *h)
+{
+    if (!h) return MT_ERR_ARG;
+    cudaSetDevice(h->c.device);
+    cudaStreamSynchronize(h->c.stream);
+    for (Case *c : h->c.cases)
+        if (c) {
+            amr_free(*c);
+            if (c->A) cudaFree(c->A);
+            if (c->B) cudaFree(c->B);
+            delete c;
+        }
+    if (h->c.own_stream) cudaStreamDestroy(h->c.stream);
+    delete h;
+    return MT_OK;
+}
+
+const char *mt_last_error(const mt_ctx *h) { return h ? h->c.last_error.c_str() : "null context"; }
+
+int mt_set_stream(mt_ctx *h, void *stream)
+{
+    if (!h) return MT_ERR_ARG;
+    Ctx &ctx = h->c;
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    if (ctx.own_stream) cudaStreamDestroy(ctx.stream);
+    if (stream) {
+        ctx.stream = (cudaStream_t)stream;
+        ctx.own_stream = false;
+    } else {
+        MT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking));
+        ctx.own_stream = true;
+    }
+    // captured graphs are launched on whatever stream is current; nothing to redo
+    return MT_OK;
+}
+
+int mt_synchronize(mt_ctx *h)
+{
+    if (!h) return MT_ERR_ARG;
+    MT_CUDA(h->c, cudaStreamSynchronize(h->c.stream));
+    return MT_OK;
+}
+
+int mt_launch_count(const mt_ctx *h, int64_t *out)
+{
+    if (!h || !out) return MT_ERR_ARG;
+    *out = h->c.launches;
+    return MT_OK;
+}
+
+int mt_case_create(mt_ctx *h, const mt_case_desc *d, int32_t *id)
+{
+    if (!h || !id) return MT_ERR_ARG;
+    Ctx &ctx = h->c;
+    int rc = check_desc(ctx, d);
+    if (rc) return rc;
+    if (d->storage != MT_STORE_F64)
+        return set_err(ctx, MT_ERR_ARG, "the multi-level path stores populations in FP64");
+    Case *c = new Case();
+    c->d = *d;
+    return add_case(ctx, c, id);
+}
+
+int mt_case_create_dense(mt_ctx *h, const mt_case_desc *d, int32_t *id)
+{
+    if (!h || !id) return MT_ERR_ARG;
+    Ctx &ctx = h->c;
+    int rc = check_desc(ctx, d);
+    if (rc) return rc;
+    if (d->max_level != 0) return set_err(ctx, MT_ERR_ARG, "the dense path has one level");
+    if (!d->periodic[0] || !d->periodic[1] || !d->periodic[2])
+        return set_err(ctx, MT_ERR_ARG, "the dense path is periodic on every axis");
+    const int64_t e = d->extent0[0];
+    if (e != d->extent0[1] || e != d->extent0[2] || (e & (e - 1)) != 0 || e < 2 || e > 1024)
+        return set_err(ctx, MT_ERR_ARG, "the dense path needs a cube of 2^b cells per edge, 2 <= 2^b <= 1024");
+    Case *c = new Case();
+    c->d = *d;
+    c->dense = true;
+    int bits = 0;
+    while (((int64_t)1 << bits) < e) ++bits;
+    c->bits = bits;
+    c->N = e * e * e;
+    const size_t bytes = storage_bytes(d->storage) * (size_t)d->q * (size_t)c->N;
+    cudaError_t ea = cudaMalloc(&c->A, bytes);
+    cudaError_t eb = ea == cudaSuccess ? cudaMalloc(&c->B, bytes) : ea;
+    if (eb != cudaSuccess) {
+        if (c->A) cudaFree(c->A);
+        delete c;
+        return set_err(ctx, MT_ERR_CUDA, std::string("dense allocation: ") + cudaGetErrorString(eb));
+    }
+    c->built = true;
+    rc = add_case(ctx, c, id);
+    if (rc) return rc;
+    const double u0[3] = {d->u_bc[0], d->u_bc[1], d->u_bc[2]};
+    return dense_dispatch(*c, [&](auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        return DenseOps<S>::init(ctx, *c, nullptr, nullptr, nullptr, nullptr, d->rho0, u0);
+    });
+}
+
+int mt_case_destroy(mt_ctx *h, int32_t id)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    cudaStreamSynchronize(h->c.stream);
+    amr_free(*c);
+    if (c->A) cudaFree(c->A);
+    if (c->B) cudaFree(c->B);
+    delete c;
+    h->c.cases[id] = nullptr;
+    return MT_OK;
+}
+
+int mt_case_add_set(mt_ctx *h, int32_t id, int32_t level, int32_t set_id, const uint64_t *keys, int64_t n)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || c->built) return set_err(ctx, MT_ERR_STATE, "sets can only be added before the build");
+    if (level < 0 || level > c->d.max_level) return set_err(ctx, MT_ERR_ARG, "level out of range");
+    if (n < 0 || (n > 0 && !keys)) return set_err(ctx, MT_ERR_ARG, "bad key array");
+    uint8_t s;
+    if (set_id >= MT_SET_LAT_BC0 && set_id < MT_SET_LAT_BC0 + 26) {
+        if (level != 0) return set_err(ctx, MT_ERR_ARG, "boundary sets live on level 0");
+        s = (uint8_t)(16 + set_id - MT_SET_LAT_BC0);
+    } else if (set_id >= 0 && set_id < kNumSets) {
+        s = (uint8_t)set_id;
+    } else {
+        return set_err(ctx, MT_ERR_ARG, "unknown set id");
+    }
+    Level &lv = c->lv[level];
+    lv.raw_keys.insert(lv.raw_keys.end(), keys, keys + n);
+    lv.raw_set.insert(lv.raw_set.end(), (size_t)n, s);
+    return MT_OK;
+}
+
+int mt_case_set_dis(mt_ctx *h, int32_t id, const uint64_t *keys, const double *rows, int64_t n)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || c->built) return set_err(ctx, MT_ERR_STATE, "dis can only be set before the build");
+    if (n < 0 || (n > 0 && (!keys || !rows))) return set_err(ctx, MT_ERR_ARG, "bad dis arrays");
+    for (int64_t i = 1; i < n; ++i)
+        if (keys[i] <= keys[i - 1]) return set_err(ctx, MT_ERR_ARG, "dis keys must be strictly ascending");
+    c->h_dis_key.assign(keys, keys + n);
+    c->h_dis.assign(rows, rows + n * (c->d.q - 1));
+    return MT_OK;
+}
+
+int mt_case_build(mt_ctx *h, int32_t id)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || c->built) return set_err(ctx, MT_ERR_STATE, "case already built");
+    MT_CUDA(ctx, cudaSetDevice(ctx.device));
+    rc = amr_build(ctx, *c);
+    if (rc) return rc;
+    const double u0[3] = {c->d.u_bc[0], c->d.u_bc[1], c->d.u_bc[2]};
+    rc = amr_init_equilibrium(ctx, *c, c->d.rho0, u0);
+    if (rc) return rc;
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
+int mt_case_level_size(mt_ctx *h, int32_t id, int32_t level, int64_t *n)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    if (!n || level < 0 || level > c->d.max_level) return set_err(h->c, MT_ERR_ARG, "bad level");
+    *n = c->dense ? c->N : c->lv[level].n;
+    return MT_OK;
+}
+
+int mt_case_get_keys(mt_ctx *h, int32_t id, int32_t level, uint64_t *keys, uint32_t *tags)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense) {
+        // the dense cube is every key 0 .. N-1 (level 0, Morton order), all lat_f
+        for (int64_t i = 0; i < c->N; ++i) {
+            if (keys) keys[i] = (uint64_t)i;
+            if (tags) tags[i] = TAG_LATF;
+        }
+        return MT_OK;
+    }
+    if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+    if (level < 0 || level > c->d.max_level) return set_err(ctx, MT_ERR_ARG, "bad level");
+    Level &lv = c->lv[level];
+    if (lv.n == 0) return MT_OK;
+    if (keys) MT_CUDA(ctx, cudaMemcpyAsync(keys, lv.key, 8 * lv.n, cudaMemcpyDeviceToHost, ctx.stream));
+    if (tags) MT_CUDA(ctx, cudaMemcpyAsync(tags, lv.tag, 4 * lv.n, cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
+int mt_case_get_neighbors(mt_ctx *h, int32_t id, int32_t level, int32_t *nbr)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "neighbour tables exist for built multi-level cases");
+    if (level < 0 || level > c->d.max_level || !nbr) return set_err(ctx, MT_ERR_ARG, "bad level");
+    Level &lv = c->lv[level];
+    if (lv.n == 0) return MT_OK;
+    MT_CUDA(ctx, cudaMemcpyAsync(nbr, lv.nbr, 4 * lv.n * (c->d.q - 1), cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
+int mt_find(mt_ctx *h, int32_t id, int32_t level, const uint64_t *keys, int64_t n, int64_t *idx)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (n < 0 || (n > 0 && (!keys || !idx))) return set_err(ctx, MT_ERR_ARG, "bad arrays");
+    if (c->dense) {
+        for (int64_t i = 0; i < n; ++i) idx[i] = keys[i] < (uint64_t)c->N ? (int64_t)keys[i] : -1;
+        return MT_OK;
+    }
+    if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+    if (level < 0 || level > c->d.max_level) return set_err(ctx, MT_ERR_ARG, "bad level");
+    return amr_find(ctx, *c, level, keys, n, idx);
+}
+
+int mt_case_init_equilibrium(mt_ctx *h, int32_t id, double rho0, const double *u0)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!u0) return set_err(ctx, MT_ERR_ARG, "null velocity");
+    if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+    if (c->dense)
+        return dense_dispatch(*c, [&](auto *tag) {
+            using S = std::remove_pointer_t<decltype(tag)>;
+            return DenseOps<S>::init(ctx, *c, nullptr, nullptr, nullptr, nullptr, rho0, u0);
+        });
+    return amr_init_equilibrium(ctx, *c, rho0, u0);
+}
+
+int mt_case_init_fields(mt_ctx *h, int32_t id, const double *rho, const double *ux, const double *uy,
+                        const double *uz)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!c->dense) return set_err(ctx, MT_ERR_STATE, "field initialisation is for the dense path");
+    if (!rho || !ux || !uy || !uz) return set_err(ctx, MT_ERR_ARG, "null field");
+    double *d = nullptr;
+    const size_t nb = sizeof(double) * c->N;
+    MT_CUDA(ctx, cudaMallocAsync(&d, 4 * nb, ctx.stream));
+    MT_CUDA(ctx, cudaMemcpyAsync(d, rho, nb, cudaMemcpyHostToDevice, ctx.stream));
+    MT_CUDA(ctx, cudaMemcpyAsync(d + c->N, ux, nb, cudaMemcpyHostToDevice, ctx.stream));
+    MT_CUDA(ctx, cudaMemcpyAsync(d + 2 * c->N, uy, nb, cudaMemcpyHostToDevice, ctx.stream));
+    MT_CUDA(ctx, cudaMemcpyAsync(d + 3 * c->N, uz, nb, cudaMemcpyHostToDevice, ctx.stream));
+    const double u0[3] = {0, 0, 0};
+    rc = dense_dispatch(*c, [&](auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        return DenseOps<S>::init(ctx, *c, d, d + c->N, d + 2 * c->N, d + 3 * c->N, 1.0, u0);
+    });
+    cudaFreeAsync(d, ctx.stream);
+    return rc;
+}
+
+int mt_case_set_populations(mt_ctx *h, int32_t id, int32_t level, const double *f, const double *fcol)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+    if (level < 0 || level > c->d.max_level) return set_err(ctx, MT_ERR_ARG, "bad level");
+    const int Q = c->d.q;
+    if (c->dense) {
+        if (!f) return set_err(ctx, MT_ERR_ARG, "null populations");
+        if (fcol && fcol != f && std::memcmp(f, fcol, sizeof(double) * Q * c->N) != 0)
+            return set_err(ctx, MT_ERR_ARG, "the dense path starts from f == fcol");
+        double *d = nullptr;
+        MT_CUDA(ctx, cudaMallocAsync(&d, sizeof(double) * Q * c->N, ctx.stream));
+        MT_CUDA(ctx, cudaMemcpyAsync(d, f, sizeof(double) * Q * c->N, cudaMemcpyHostToDevice, ctx.stream));
+        rc = dense_dispatch(*c, [&](auto *tag) {
+            using S = std::remove_pointer_t<decltype(tag)>;
+            return DenseOps<S>::set(ctx, *c, d);
+        });
+        cudaFreeAsync(d, ctx.stream);
+        return rc;
+    }
+    Level &lv = c->lv[level];
+    if (f) MT_CUDA(ctx, cudaMemcpyAsync(lv.f, f, sizeof(double) * Q * lv.n, cudaMemcpyHostToDevice, ctx.stream));
+    if (fcol) MT_CUDA(ctx, cudaMemcpyAsync(lv.fcol, fcol, sizeof(double) * Q * lv.n, cudaMemcpyHostToDevice, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
+int mt_case_get_populations(mt_ctx *h, int32_t id, int32_t level, double *f, double *fcol)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+    if (level < 0 || level > c->d.max_level) return set_err(ctx, MT_ERR_ARG, "bad level");
+    const int Q = c->d.q;
+    if (c->dense) {
+        double *d = nullptr;
+        const size_t nb = sizeof(double) * Q * c->N;
+        MT_CUDA(ctx, cudaMallocAsync(&d, nb, ctx.stream));
+        for (int which = 0; which < 2; ++which) {
+            double *dst = which == 0 ? f : fcol;
+            if (!dst) continue;
+            const int pull = (which == 0 && c->a_is_fcol) ? 1 : 0;
+            rc = dense_dispatch(*c, [&](auto *tag) {
+                using S = std::remove_pointer_t<decltype(tag)>;
+                return DenseOps<S>::get(ctx, *c, d, pull);
+            });
+            if (rc) break;
+            MT_CUDA(ctx, cudaMemcpyAsync(dst, d, nb, cudaMemcpyDeviceToHost, ctx.stream));
+        }
+        MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+        cudaFreeAsync(d, ctx.stream);
+        return rc;
+    }
+    Level &lv = c->lv[level];
+    if (f) MT_CUDA(ctx, cudaMemcpyAsync(f, lv.f, sizeof(double) * Q * lv.n, cudaMemcpyDeviceToHost, ctx.stream));
+    if (fcol) MT_CUDA(ctx, cudaMemcpyAsync(fcol, lv.fcol, sizeof(double) * Q * lv.n, cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
+int mt_case_get_macros(mt_ctx *h, int32_t id, int32_t level, double *rho, double *u)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+    if (level < 0 || level > c->d.max_level) return set_err(ctx, MT_ERR_ARG, "bad level");
+    if (c->dense) {
+        double *d = nullptr;
+        MT_CUDA(ctx, cudaMallocAsync(&d, sizeof(double) * 4 * c->N, ctx.stream));
+        rc = dense_dispatch(*c, [&](auto *tag) {
+            using S = std::remove_pointer_t<decltype(tag)>;
+            return DenseOps<S>::macros(ctx, *c, d, d + c->N);
+        });
+        if (!rc) {
+            if (rho) MT_CUDA(ctx, cudaMemcpyAsync(rho, d, sizeof(double) * c->N, cudaMemcpyDeviceToHost, ctx.stream));
+            if (u) MT_CUDA(ctx, cudaMemcpyAsync(u, d + c->N, sizeof(double) * 3 * c->N, cudaMemcpyDeviceToHost, ctx.stream));
+        }
+        MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+        cudaFreeAsync(d, ctx.stream);
+        return rc;
+    }
+    Level &lv = c->lv[level];
+    if (rho) MT_CUDA(ctx, cudaMemcpyAsync(rho, lv.rho, sizeof(double) * lv.n, cudaMemcpyDeviceToHost, ctx.stream));
+    if (u) MT_CUDA(ctx, cudaMemcpyAsync(u, lv.u, sizeof(double) * 3 * lv.n, cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
+int mt_case_reduce(mt_ctx *h, int32_t id, double *out)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!out) return set_err(ctx, MT_ERR_ARG, "null output");
+    if (!c->dense) return set_err(ctx, MT_ERR_STATE, "device reductions are implemented for the dense path");
+    double *d = nullptr;
+    MT_CUDA(ctx, cudaMallocAsync(&d, sizeof(double) * 5, ctx.stream));
+    rc = dense_dispatch(*c, [&](auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        return DenseOps<S>::reduce(ctx, *c, d);
+    });
+    if (!rc) MT_CUDA(ctx, cudaMemcpyAsync(out, d, sizeof(double) * 5, cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    cudaFreeAsync(d, ctx.stream);
+    return rc;
+}
+
+int mt_calculate_macros(mt_ctx *h, int32_t id, int32_t level) { return phase_call(h, id, PH_MACROS, level); }
+int mt_collide(mt_ctx *h, int32_t id, int32_t level) { return phase_call(h, id, PH_COLLIDE, level); }
+int mt_stream(mt_ctx *h, int32_t id, int32_t level) { return phase_call(h, id, PH_STREAM, level); }
+int mt_explosion(mt_ctx *h, int32_t id, int32_t level) { return phase_call(h, id, PH_EXPLOSION, level); }
+int mt_coalescence(mt_ctx *h, int32_t id, int32_t level) { return phase_call(h, id, PH_COALESCENCE, level); }
+int mt_apply_bc(mt_ctx *h, int32_t id)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    return phase_call(h, id, c->d.bc_mode == MT_BC_NEQ ? PH_BC : PH_BC_INOUT, 0);
+}
+int mt_ib_treat(mt_ctx *h, int32_t id)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    return phase_call(h, id, PH_IB, c->d.max_level);
+}
+
+int mt_lbm_kernel(mt_ctx *h, int32_t id, int32_t level)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "LBMkernel needs a built multi-level case");
+    if (level < 0 || level > c->d.max_level) return set_err(ctx, MT_ERR_ARG, "bad level");
+    return amr_lbm_kernel(ctx, *c, level);
+}
+
+int mt_step(mt_ctx *h, int32_t id, int32_t n)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+    if (n < 0) return set_err(ctx, MT_ERR_ARG, "negative step count");
+    if (n == 0) return MT_OK;
+    if (c->dense) {
+        return dense_dispatch(*c, [&](auto *tag) {
+            using S = std::remove_pointer_t<decltype(tag)>;
+            int r = MT_OK, left = n;
+            if (!c->a_is_fcol) {
+                r = DenseOps<S>::step(ctx, *c, 1);
+                if (r) return r;
+                c->a_is_fcol = true;
+                --left;
+            }
+            for (int s = 0; s < left && !r; ++s) r = DenseOps<S>::step(ctx, *c, 0);
+            return r;
+        });
+    }
+    rc = amr_step(ctx, *c, n);
+    if (rc) return rc;
+    return MT_OK;
+}
+
+int mt_get_force(mt_ctx *h, int32_t id, double *out4)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!out4) return set_err(ctx, MT_ERR_ARG, "null output");
+    if (c->dense || !c->force_acc) {
+        for (int i = 0; i < 4; ++i) out4[i] = 0;
+        return MT_OK;
+    }
+    MT_CUDA(ctx, cudaMemcpyAsync(out4, c->force_acc, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
+int mt_reset_force(mt_ctx *h, int32_t id)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->force_acc) MT_CUDA(ctx, cudaMemsetAsync(c->force_acc, 0, 4 * sizeof(double), ctx.stream));
+    return MT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,407 @@
+// Dense uniform path: a periodic Morton-ordered cube of 2^b cells per edge,
+// cell index = Morton interleave of (x, y, z).  Neighbour indices come from
+// masked increments of the dilated coordinates (the same carry trick as
+// Morton_Assist::find_x1/find_x0, Morton_Assist.h:229-259, wrapped at the cube
+// edge), so no neighbour table is read.
+//
+// State: one population array A of the storage type, [Q][N].  After
+// initialisation A holds f (post-stream, = fcol).  The first step collides in
+// place into B; every later step is one fused kernel that pulls the
+// post-collision populations of the previous step from the neighbours
+// (= the reference's stream), computes the moments and collides, writing B.
+// The reference's f after step n is the pull of A, its fcol is A itself.
+//
+// Storage: double (unshifted, reference operation order, compiled without FMA)
+// or float / half / bfloat16 holding the deviation f - w_q, with FP32
+// arithmetic on the deviations (rho - 1 = sum of deviations, momentum = sum
+// of e_q * deviation, since sum w = 1 and sum w e = 0).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "mt_internal.hpp"
+
+namespace mt {
+
+template <class S> struct Store;
+template <> struct Store<double> {
+    using C = double;
+    static constexpr bool shifted = false;
+    __device__ static __forceinline__ double ld(const double *p, int64_t i) { return __ldg(p + i); }
+    __device__ static __forceinline__ void st(double *p, int64_t i, double v) { p[i] = v; }
+};
+template <> struct Store<float> {
+    using C = float;
+    static constexpr bool shifted = true;
+    __device__ static __forceinline__ float ld(const float *p, int64_t i) { return __ldg(p + i); }
+    __device__ static __forceinline__ void st(float *p, int64_t i, float v) { p[i] = v; }
+};
+template <> struct Store<__half> {
+    using C = float;
+    static constexpr bool shifted = true;
+    __device__ static __forceinline__ float ld(const __half *p, int64_t i) { return __half2float(__ldg(p + i)); }
+    __device__ static __forceinline__ void st(__half *p, int64_t i, float v) { p[i] = __float2half_rn(v); }
+};
+template <> struct Store<__nv_bfloat16> {
+    using C = float;
+    static constexpr bool shifted = true;
+    __device__ static __forceinline__ float ld(const __nv_bfloat16 *p, int64_t i)
+    {
+        return __bfloat162float(__ldg(p + i));
+    }
+    __device__ static __forceinline__ void st(__nv_bfloat16 *p, int64_t i, float v) { p[i] = __float2bfloat16_rn(v); }
+};
+
+struct DenseGeom {
+    uint32_t m[3];  // per-axis bit masks within the 3b index bits
+    uint32_t lo[3]; // lowest bit of each axis (1, 2, 4)
+};
+
+__device__ __forceinline__ uint32_t dstep(uint32_t i, uint32_t m, uint32_t lo, int dir)
+{
+    return dir > 0 ? ((((i | ~m) + lo) & m) | (i & ~m)) : ((((i & m) - lo) & m) | (i & ~m));
+}
+// index of the cell at i + s * e_k
+__device__ __forceinline__ uint32_t dense_nbr(const DenseGeom &g, uint32_t i, int k, int s)
+{
+    uint32_t r = i;
+    if (ex(k)) r = dstep(r, g.m[0], g.lo[0], s * ex(k));
+    if (ey(k)) r = dstep(r, g.m[1], g.lo[1], s * ey(k));
+    if (ez(k)) r = dstep(r, g.m[2], g.lo[2], s * ez(k));
+    return r;
+}
+
+enum { DM_FUSED = 0, DM_COLLIDE = 1, DM_PULL = 2 };
+
+// FP32 LBGK on deviations s_k = f_k - w_k: fcol - w = s + omega (feq - f)
+template <int Q>
+__device__ __forceinline__ void lbgk_dev(float *s, float omega)
+{
+    float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        dr += s[k];
+        if (ex(k)) jx += ex(k) * s[k];
+        if (ey(k)) jy += ey(k) * s[k];
+        if (ez(k)) jz += ez(k) * s[k];
+    }
+    const float rho = 1.f + dr;
+    const float ir = 1.f / rho;
+    const float ux = jx * ir, uy = jy * ir, uz = jz * ir;
+    const float uu = 1.5f * (ux * ux + uy * uy + uz * uz);
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const float eu = ex(k) * ux + ey(k) * uy + ez(k) * uz;
+        const float wk = (float)w<Q>(k);
+        // feq - w = w (drho + rho (3 eu + 4.5 eu^2 - 1.5 u^2))
+        const float dfeq = wk * (dr + rho * (3.f * eu + 4.5f * eu * eu - uu));
+        s[k] = fmaf(omega, dfeq - s[k], s[k]);
+    }
+}
+
+template <int Q, class S, int COLL, int MODE>
+__global__ void __launch_bounds__(256) k_dense(const S *__restrict__ A, S *__restrict__ B, int64_t N, DenseGeom g,
+                                              int textbook, double tau)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int sgn = textbook ? -1 : 1;
+    C f[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const uint32_t src = (MODE == DM_COLLIDE || k == 0) ? i : dense_nbr(g, i, k, sgn);
+        f[k] = T::ld(A, (int64_t)k * N + src);
+    }
+    if (MODE != DM_PULL) {
+        if constexpr (!T::shifted) {
+            double r, x, y, z;
+            macros_ref<Q>(f, r, x, y, z);
+            if constexpr (COLL == MT_COLL_LBGK) {
+#pragma unroll
+                for (int k = 0; k < Q; ++k) f[k] = f[k] - (f[k] - feq_ref<Q>(k, r, x, y, z)) / tau;
+            } else {
+                double o[27];
+                cumulant_collide<double>(f, r, x, y, z, 1. / tau, o);
+#pragma unroll
+                for (int k = 0; k < 27; ++k) f[k] = o[k];
+            }
+        } else {
+            if constexpr (COLL == MT_COLL_LBGK) {
+                lbgk_dev<Q>(f, (float)(1.0 / tau));
+            } else {
+                float full[27], o[27];
+                float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+                for (int k = 0; k < 27; ++k) {
+                    full[k] = (float)w<27>(k) + f[k];
+                    dr += f[k];
+                    jx += ex(k) * f[k];
+                    jy += ey(k) * f[k];
+                    jz += ez(k) * f[k];
+                }
+                const float rho = 1.f + dr;
+                const float ir = 1.f / rho;
+                cumulant_collide<float>(full, rho, jx * ir, jy * ir, jz * ir, (float)(1.0 / tau), o);
+#pragma unroll
+                for (int k = 0; k < 27; ++k) f[k] = o[k] - (float)w<27>(k);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < Q; ++k) T::st(B, (int64_t)k * N + i, f[k]);
+}
+
+// populations from host doubles -> storage (shift applied), or equilibrium of fields
+template <int Q, class S>
+__global__ void k_dense_from_f64(const double *src, S *A, int64_t N)
+{
+    using T = Store<S>;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        double v = src[k * N + i];
+        if (T::shifted) v -= w<Q>(k);
+        T::st(A, k * N + i, (typename T::C)v);
+    }
+}
+
+template <int Q, class S>
+__global__ void k_dense_eq(const double *rho, const double *ux, const double *uy, const double *uz, double rho0,
+                           double u0x, double u0y, double u0z, S *A, int64_t N)
+{
+    using T = Store<S>;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double r = rho ? rho[i] : rho0, x = ux ? ux[i] : u0x, y = uy ? uy[i] : u0y, z = uz ? uz[i] : u0z;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        double v = feq_ref<Q>(k, r, x, y, z);
+        if (T::shifted) {
+            // deviation computed without forming feq first: w (rho - 1 + rho P)
+            const double uu = x * x + y * y + z * z;
+            const double eu = ex(k) * x + ey(k) * y + ez(k) * z;
+            v = w<Q>(k) * ((r - 1.0) + r * (3. * eu + 4.5 * eu * eu - 1.5 * uu));
+        }
+        T::st(A, k * N + i, (typename T::C)v);
+    }
+}
+
+// storage -> doubles, optionally pulled (post-stream f from post-collision A)
+template <int Q, class S>
+__global__ void k_dense_to_f64(const S *A, double *dst, int64_t N, DenseGeom g, int pull, int textbook)
+{
+    using T = Store<S>;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int sgn = textbook ? -1 : 1;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const uint32_t src = (pull && k) ? dense_nbr(g, i, k, sgn) : i;
+        double v = (double)T::ld(A, (int64_t)k * N + src);
+        if (T::shifted) v += w<Q>(k);
+        dst[k * N + i] = v;
+    }
+}
+
+// density and velocity of f (pulled from A when A holds post-collision values)
+template <int Q, class S>
+__global__ void k_dense_macros(const S *A, int64_t N, DenseGeom g, int pull, int textbook, double *rho, double *u)
+{
+    using T = Store<S>;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int sgn = textbook ? -1 : 1;
+    double d[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const uint32_t src = (pull && k) ? dense_nbr(g, i, k, sgn) : i;
+        double v = (double)T::ld(A, (int64_t)k * N + src);
+        if (T::shifted) v += w<Q>(k);
+        d[k] = v;
+    }
+    double r, x, y, z;
+    macros_ref<Q>(d, r, x, y, z);
+    rho[i] = r;
+    u[i] = x;
+    u[N + i] = y;
+    u[2 * N + i] = z;
+}
+
+// per-block FP64 partial sums of mass, momentum and kinetic energy of f
+template <int Q, class S>
+__global__ void k_dense_reduce(const S *A, int64_t N, DenseGeom g, int pull, int textbook, double *partial)
+{
+    using T = Store<S>;
+    __shared__ double sh[5][256];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double a[5] = {0, 0, 0, 0, 0};
+    if (i < N) {
+        const int sgn = textbook ? -1 : 1;
+        double r = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            const uint32_t src = (pull && k) ? dense_nbr(g, i, k, sgn) : i;
+            double v = (double)T::ld(A, (int64_t)k * N + src);
+            if (T::shifted) v += w<Q>(k);
+            r += v;
+            jx += v * ex(k);
+            jy += v * ey(k);
+            jz += v * ez(k);
+        }
+        a[0] = r;
+        a[1] = jx;
+        a[2] = jy;
+        a[3] = jz;
+        a[4] = 0.5 * (jx * jx + jy * jy + jz * jz) / r;
+    }
+    for (int c = 0; c < 5; ++c) sh[c][threadIdx.x] = a[c];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int c = 0; c < 5; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 5; ++c) partial[(int64_t)c * gridDim.x + blockIdx.x] = sh[c][0];
+}
+
+static __global__ void k_sum_partials(const double *partial, int64_t nb, double *out)
+{
+    __shared__ double sh[256];
+    for (int c = 0; c < 5; ++c) {
+        double a = 0;
+        for (int64_t j = threadIdx.x; j < nb; j += blockDim.x) a += partial[c * nb + j];
+        sh[threadIdx.x] = a;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[c] = sh[0];
+        __syncthreads();
+    }
+}
+
+inline DenseGeom dense_geom(int bits)
+{
+    DenseGeom g;
+    for (int a = 0; a < 3; ++a) {
+        uint32_t m = 0;
+        for (int b = 0; b < bits; ++b) m |= 1u << (3 * b + a);
+        g.m[a] = m;
+        g.lo[a] = 1u << a;
+    }
+    return g;
+}
+
+template <class S>
+int DenseOps<S>::step(Ctx &ctx, Case &c, int mode)
+{
+    const int B = 256;
+    const unsigned grid = grid_for(c.N, B);
+    const DenseGeom g = dense_geom(c.bits);
+    const S *A = (const S *)c.A;
+    S *Bp = (S *)c.B;
+    const int tb = c.d.stream_convention;
+    const double tau = c.d.tau[0];
+#define MT_DENSE_LAUNCH(QQ, CC)                                                                           \
+    do {                                                                                                  \
+        if (mode == DM_FUSED)                                                                             \
+            k_dense<QQ, S, CC, DM_FUSED><<<grid, B, 0, ctx.stream>>>(A, Bp, c.N, g, tb, tau);             \
+        else                                                                                              \
+            k_dense<QQ, S, CC, DM_COLLIDE><<<grid, B, 0, ctx.stream>>>(A, Bp, c.N, g, tb, tau);           \
+    } while (0)
+    if (c.d.q == 19)
+        MT_DENSE_LAUNCH(19, MT_COLL_LBGK);
+    else if (c.d.collision == MT_COLL_LBGK)
+        MT_DENSE_LAUNCH(27, MT_COLL_LBGK);
+    else
+        MT_DENSE_LAUNCH(27, MT_COLL_CUMULANT);
+#undef MT_DENSE_LAUNCH
+    MT_LAUNCHED(ctx);
+    std::swap(c.A, c.B);
+    return MT_OK;
+}
+
+template <class S>
+int DenseOps<S>::init(Ctx &ctx, Case &c, const double *rho, const double *ux, const double *uy, const double *uz,
+                      double rho0, const double *u0)
+{
+    const unsigned grid = grid_for(c.N, 256);
+    if (c.d.q == 19)
+        k_dense_eq<19, S><<<grid, 256, 0, ctx.stream>>>(rho, ux, uy, uz, rho0, u0[0], u0[1], u0[2], (S *)c.A, c.N);
+    else
+        k_dense_eq<27, S><<<grid, 256, 0, ctx.stream>>>(rho, ux, uy, uz, rho0, u0[0], u0[1], u0[2], (S *)c.A, c.N);
+    MT_LAUNCHED(ctx);
+    c.a_is_fcol = false;
+    return MT_OK;
+}
+
+template <class S>
+int DenseOps<S>::get(Ctx &ctx, Case &c, double *d_f, int pull)
+{
+    const unsigned grid = grid_for(c.N, 256);
+    const DenseGeom g = dense_geom(c.bits);
+    if (c.d.q == 19)
+        k_dense_to_f64<19, S><<<grid, 256, 0, ctx.stream>>>((const S *)c.A, d_f, c.N, g, pull, c.d.stream_convention);
+    else
+        k_dense_to_f64<27, S><<<grid, 256, 0, ctx.stream>>>((const S *)c.A, d_f, c.N, g, pull, c.d.stream_convention);
+    MT_LAUNCHED(ctx);
+    return MT_OK;
+}
+
+template <class S>
+int DenseOps<S>::set(Ctx &ctx, Case &c, const double *d_f)
+{
+    const unsigned grid = grid_for(c.N, 256);
+    if (c.d.q == 19)
+        k_dense_from_f64<19, S><<<grid, 256, 0, ctx.stream>>>(d_f, (S *)c.A, c.N);
+    else
+        k_dense_from_f64<27, S><<<grid, 256, 0, ctx.stream>>>(d_f, (S *)c.A, c.N);
+    MT_LAUNCHED(ctx);
+    c.a_is_fcol = false;
+    return MT_OK;
+}
+
+template <class S>
+int DenseOps<S>::macros(Ctx &ctx, Case &c, double *d_rho, double *d_u)
+{
+    const unsigned grid = grid_for(c.N, 256);
+    const DenseGeom g = dense_geom(c.bits);
+    const int pull = c.a_is_fcol ? 1 : 0;
+    if (c.d.q == 19)
+        k_dense_macros<19, S><<<grid, 256, 0, ctx.stream>>>((const S *)c.A, c.N, g, pull, c.d.stream_convention, d_rho,
+                                                            d_u);
+    else
+        k_dense_macros<27, S><<<grid, 256, 0, ctx.stream>>>((const S *)c.A, c.N, g, pull, c.d.stream_convention, d_rho,
+                                                            d_u);
+    MT_LAUNCHED(ctx);
+    return MT_OK;
+}
+
+template <class S>
+int DenseOps<S>::reduce(Ctx &ctx, Case &c, double *d_out)
+{
+    const unsigned grid = grid_for(c.N, 256);
+    const DenseGeom g = dense_geom(c.bits);
+    const int pull = c.a_is_fcol ? 1 : 0;
+    double *partial = nullptr;
+    MT_CUDA(ctx, cudaMallocAsync(&partial, sizeof(double) * 5 * grid, ctx.stream));
+    if (c.d.q == 19)
+        k_dense_reduce<19, S><<<grid, 256, 0, ctx.stream>>>((const S *)c.A, c.N, g, pull, c.d.stream_convention,
+                                                            partial);
+    else
+        k_dense_reduce<27, S><<<grid, 256, 0, ctx.stream>>>((const S *)c.A, c.N, g, pull, c.d.stream_convention,
+                                                            partial);
+    MT_LAUNCHED(ctx);
+    k_sum_partials<<<1, 256, 0, ctx.stream>>>(partial, grid, d_out);
+    MT_LAUNCHED(ctx);
+    cudaFreeAsync(partial, ctx.stream);
+    return MT_OK;
+}
+
+}  // namespace mt

@@ -1,0 +1,136 @@
+// Internal types of libmtlbm: context, per-case device state, launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mt_lbm.h"
+#include "mt_lattice.cuh"
+
+namespace mt {
+
+constexpr int kMaxLevels = MT_MAX_LEVELS;
+constexpr int kNumSets = 6;  // lat_f, F2C, C2F, ghost C2F, ghost F2C, solid
+
+// per-cell tag bits (which reference index sets the cell belongs to)
+enum : uint32_t {
+    TAG_LATF = 1u,
+    TAG_F2C = 2u,
+    TAG_C2F = 4u,
+    TAG_GC2F = 8u,
+    TAG_GF2C = 16u,
+    TAG_BC = 32u,
+    TAG_SF = 64u,
+    TAG_IB = 128u,
+};
+
+// device error flags raised by build / step kernels
+enum : int {
+    DEVERR_MISSING_CHILD = 1,     // a child of an interface cell is not stored (the reference's .at() throws)
+    DEVERR_MISSING_BC_NBR = 2,    // a boundary cell's reserved neighbour is not stored
+    DEVERR_DIS_NOT_FINEST = 4,    // a dis key is not a finest-level cell
+    DEVERR_NONFINITE = 8,         // NaN/Inf population found by the guard
+};
+
+struct Level {
+    int64_t n = 0;
+    uint64_t *key = nullptr;   // sorted unique Morton keys
+    uint32_t *tag = nullptr;
+    int8_t *bcidx = nullptr;   // lat_bc index or -1
+    int32_t *disrow = nullptr; // row in the dis table or -1
+    int32_t *nbr = nullptr;    // [(Q-1) * n]: index of the cell at key + e_k (k >= 1) or -1
+    double *f = nullptr, *fcol = nullptr;  // [Q * n] FP64 populations (general path)
+    double *rho = nullptr, *u = nullptr;   // [n], [3 * n] macroscopic fields
+    int32_t *list[kNumSets] = {};
+    int64_t nlist[kNumSets] = {};
+    int32_t *collide_list = nullptr; int64_t ncollide = 0;  // lat_f then F2C
+    int32_t *stream_list = nullptr;  int64_t nstream = 0;   // lat_f then C2F
+    int32_t *bclist[26] = {};
+    int64_t nbc[26] = {};
+    int32_t *iblist = nullptr; int64_t nib = 0;             // finest lat_f cells with dis rows
+    // explosion sources on the parent level (F2C then ghost F2C) and their children on this level
+    int32_t *expl_src = nullptr; int32_t *expl_child = nullptr; int64_t nexpl = 0, nexpl_f2c = 0;
+    // coalescence: F2C cells of this level and their children on the next level
+    int32_t *coal_child = nullptr;
+    // raw uploads, consumed by the build
+    std::vector<uint64_t> raw_keys;
+    std::vector<uint8_t> raw_set;  // 0..5 sets, 16 + b for lat_bc[b]
+};
+
+struct Case {
+    mt_case_desc d{};
+    bool dense = false;
+    bool built = false;
+    Level lv[kMaxLevels];
+    int64_t ndis = 0;
+    uint64_t *dis_key = nullptr;
+    double *dis = nullptr;
+    std::vector<uint64_t> h_dis_key;
+    std::vector<double> h_dis;
+    double *ib_force = nullptr;  // [3 * nib] per-cell force of the last treat()
+    double *force_acc = nullptr; // [4] fx, fy, fz, treat count
+    int *dev_err = nullptr;
+    MortonGeom geom{};
+    // dense uniform path
+    int bits = 0;        // log2 of the cube edge
+    int64_t N = 0;       // cells
+    void *A = nullptr, *B = nullptr;  // populations [Q * N] in the storage type
+    bool a_is_fcol = false;           // false: A holds post-stream f; true: A holds post-collision fcol
+    double *bc_tmp = nullptr;         // scratch of the boundary sweep
+    // captured coarse step
+    cudaGraphExec_t graph = nullptr;
+    int64_t graph_launches = 0;
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<Case *> cases;
+    std::string last_error;
+    int64_t launches = 0;  // kernels this library launched (graph nodes count per replay)
+};
+
+// kernel launchers implemented in the .cu files
+int amr_build(Ctx &ctx, Case &c);
+int amr_init_equilibrium(Ctx &ctx, Case &c, double rho0, const double *u0);
+int amr_lbm_kernel(Ctx &ctx, Case &c, int level);
+int amr_step(Ctx &ctx, Case &c, int n);
+int amr_phase(Ctx &ctx, Case &c, int phase, int level);
+int amr_find(Ctx &ctx, Case &c, int level, const uint64_t *h_keys, int64_t n, int64_t *h_idx);
+void amr_free(Case &c);
+
+// dense uniform path, one explicit instantiation per storage type
+// (mt_dense_f64.cu builds the FP64 one without FMA contraction)
+template <class S> struct DenseOps {
+    static int step(Ctx &ctx, Case &c, int mode);  // mode: 0 fused pull+collide, 1 collide in place
+    static int init(Ctx &ctx, Case &c, const double *rho, const double *ux, const double *uy, const double *uz,
+                    double rho0, const double *u0);
+    static int get(Ctx &ctx, Case &c, double *d_f, int pull);
+    static int set(Ctx &ctx, Case &c, const double *d_f);
+    static int macros(Ctx &ctx, Case &c, double *d_rho, double *d_u);
+    static int reduce(Ctx &ctx, Case &c, double *d_out);
+};
+
+// error helpers
+int set_err(Ctx &ctx, int code, const std::string &msg);
+#define MT_CUDA(ctx, call)                                                                          \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return ::mt::set_err((ctx), MT_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+#define MT_LAUNCHED(ctx)                                                                            \
+    do {                                                                                            \
+        cudaError_t e_ = cudaGetLastError();                                                        \
+        if (e_ != cudaSuccess)                                                                      \
+            return ::mt::set_err((ctx), MT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+        (ctx).launches++;                                                                           \
+    } while (0)
+
+inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
+
+}  // namespace mt

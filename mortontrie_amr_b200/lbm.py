@@ -1,0 +1,359 @@
+"""Python host mirror of the reference's LBM call surface over the C ABI.
+
+The class and method names follow the reference's interface
+(header/LBM_Manager.hpp:25-119, header/lbm_kernel/Collision_Manager.hpp:73-97,
+header/lbm_kernel/Stream_Manager.hpp:12-37, header/ComplexBoundary_Manager.hpp
+:16-46, header/BC/D3Q19_BC_Manager.hpp:201-263); every call goes through
+libmtlbm.so (include/mt_lbm.h).  There is no CPU fallback: importing this
+module raises if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .case import BC_MODES, COLLISIONS, IB_METHODS, STORAGE, STREAM_CONVENTIONS, Case
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmtlbm.so")
+
+MAX_LEVELS = 8
+SET_IDS = {"lat_f": 0, "overlap_F2C": 1, "overlap_C2F": 2, "ghost_overlap_C2F": 3, "ghost_overlap_F2C": 4,
+           "lat_sf": 5}
+SET_LAT_BC0 = 16
+ERRORS = {-1: "MT_ERR_ARG", -2: "MT_ERR_CUDA", -3: "MT_ERR_STATE", -4: "MT_ERR_MESH", -5: "MT_ERR_NONFINITE"}
+EXPORTS = [
+    "mt_create", "mt_destroy", "mt_last_error", "mt_set_stream", "mt_synchronize", "mt_launch_count",
+    "mt_case_create", "mt_case_create_dense", "mt_case_destroy", "mt_case_add_set", "mt_case_set_dis",
+    "mt_case_build", "mt_case_level_size", "mt_case_get_keys", "mt_case_get_neighbors", "mt_find",
+    "mt_case_init_equilibrium", "mt_case_init_fields", "mt_case_set_populations", "mt_case_get_populations",
+    "mt_case_get_macros", "mt_case_reduce", "mt_calculate_macros", "mt_collide", "mt_stream", "mt_explosion",
+    "mt_coalescence", "mt_apply_bc", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force", "mt_reset_force",
+]
+
+
+class MTError(RuntimeError):
+    pass
+
+
+class mt_case_desc(C.Structure):
+    _fields_ = [("q", C.c_int32), ("max_level", C.c_int32), ("collision", C.c_int32), ("ib_method", C.c_int32),
+                ("bc_mode", C.c_int32), ("stream_convention", C.c_int32), ("storage", C.c_int32),
+                ("periodic", C.c_int32 * 3), ("extent0", C.c_int64 * 3), ("tau", C.c_double * MAX_LEVELS),
+                ("rho0", C.c_double), ("u_bc", C.c_double * 3)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libmtlbm.so; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise MTError(f"{LIB_PATH} is missing: run mortontrie_amr_b200/build.py (or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+        u64p, i64p, i32p, u32p, dp = (C.POINTER(C.c_uint64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_uint32), C.POINTER(C.c_double))
+        sig = {
+            "mt_create": [i32, C.POINTER(vp)], "mt_destroy": [vp], "mt_set_stream": [vp, vp], "mt_synchronize": [vp],
+            "mt_launch_count": [vp, i64p], "mt_case_create": [vp, C.POINTER(mt_case_desc), i32p],
+            "mt_case_create_dense": [vp, C.POINTER(mt_case_desc), i32p], "mt_case_destroy": [vp, i32],
+            "mt_case_add_set": [vp, i32, i32, i32, u64p, i64], "mt_case_set_dis": [vp, i32, u64p, dp, i64],
+            "mt_case_build": [vp, i32], "mt_case_level_size": [vp, i32, i32, i64p],
+            "mt_case_get_keys": [vp, i32, i32, u64p, u32p], "mt_case_get_neighbors": [vp, i32, i32, i32p],
+            "mt_find": [vp, i32, i32, u64p, i64, i64p], "mt_case_init_equilibrium": [vp, i32, C.c_double, dp],
+            "mt_case_init_fields": [vp, i32, dp, dp, dp, dp], "mt_case_set_populations": [vp, i32, i32, dp, dp],
+            "mt_case_get_populations": [vp, i32, i32, dp, dp], "mt_case_get_macros": [vp, i32, i32, dp, dp],
+            "mt_case_reduce": [vp, i32, dp], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
+            "mt_apply_bc": [vp, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
+            "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.mt_last_error.argtypes = [vp]
+        L.mt_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class Context:
+    """One device context (mt_create); owns every case created on it."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        rc = lib().mt_create(device, C.byref(self.h))
+        if rc != 0:
+            raise MTError(f"mt_create failed ({ERRORS.get(rc, rc)})")
+
+    def check(self, rc, what=""):
+        if rc != 0:
+            msg = lib().mt_last_error(self.h).decode()
+            raise MTError(f"{what}: {ERRORS.get(rc, rc)}: {msg}")
+
+    def set_stream(self, cuda_stream_handle):
+        self.check(lib().mt_set_stream(self.h, C.c_void_p(cuda_stream_handle or 0)), "mt_set_stream")
+
+    def synchronize(self):
+        self.check(lib().mt_synchronize(self.h), "mt_synchronize")
+
+    def launch_count(self) -> int:
+        v = C.c_int64()
+        self.check(lib().mt_launch_count(self.h, C.byref(v)), "mt_launch_count")
+        return v.value
+
+    def close(self):
+        if self.h:
+            lib().mt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_desc(case: Case, storage: str = None) -> mt_case_desc:
+    p = case.params
+    m = case.mesh
+    d = mt_case_desc()
+    d.q = p.q
+    d.max_level = m.spec.max_level
+    d.collision = COLLISIONS[p.collision]
+    d.ib_method = IB_METHODS[p.ib_method]
+    d.bc_mode = BC_MODES[p.bc_mode]
+    d.stream_convention = STREAM_CONVENTIONS[p.stream_convention]
+    d.storage = STORAGE[storage or p.storage]
+    for a in range(3):
+        d.periodic[a] = int(m.spec.boundary[a] == "periodic")
+        d.extent0[a] = int(m.spec.coarse[a])
+        d.u_bc[a] = float(p.u_bc[a])
+    for l, t in enumerate(p.taus(m.spec.max_level)):
+        d.tau[l] = float(t)
+    d.rho0 = float(p.rho0)
+    return d
+
+
+class LBM_Manager:
+    """Multi-level case on the device: the reference's LBM_Manager with its
+    strategy objects (collide / stream / treat / boundary) as methods."""
+
+    def __init__(self, ctx: Context, case: Case):
+        self.ctx = ctx
+        self.case = case
+        self.q = case.params.q
+        self.L = case.mesh.spec.max_level
+        d = make_desc(case, "f64")
+        cid = C.c_int32()
+        ctx.check(lib().mt_case_create(ctx.h, C.byref(d), C.byref(cid)), "mt_case_create")
+        self.id = cid.value
+        m = case.mesh
+        for l in range(self.L + 1):
+            for name, sid in SET_IDS.items():
+                k = np.ascontiguousarray(m.levels[l][name], np.uint64)
+                ctx.check(lib().mt_case_add_set(ctx.h, self.id, l, sid, _ptr(k, C.c_uint64), k.size), "add_set")
+        for b in range(26):
+            k = np.ascontiguousarray(m.lat_bc[b], np.uint64)
+            ctx.check(lib().mt_case_add_set(ctx.h, self.id, 0, SET_LAT_BC0 + b, _ptr(k, C.c_uint64), k.size),
+                      "add_set")
+        dk = np.ascontiguousarray(m.dis_keys, np.uint64)
+        dr = np.ascontiguousarray(m.dis_rows, np.float64)
+        ctx.check(lib().mt_case_set_dis(ctx.h, self.id, _ptr(dk, C.c_uint64), _ptr(dr, C.c_double), dk.size),
+                  "set_dis")
+        ctx.check(lib().mt_case_build(ctx.h, self.id), "mt_case_build")
+
+    # ---- D_map_define-style access ------------------------------------
+    def size(self, level):
+        n = C.c_int64()
+        self.ctx.check(lib().mt_case_level_size(self.ctx.h, self.id, level, C.byref(n)), "level_size")
+        return n.value
+
+    def keys(self, level):
+        n = self.size(level)
+        k = np.zeros(n, np.uint64)
+        t = np.zeros(n, np.uint32)
+        self.ctx.check(lib().mt_case_get_keys(self.ctx.h, self.id, level, _ptr(k, C.c_uint64), _ptr(t, C.c_uint32)),
+                       "get_keys")
+        return k, t
+
+    def find(self, level, keys):
+        keys = np.ascontiguousarray(keys, np.uint64)
+        out = np.zeros(keys.size, np.int64)
+        self.ctx.check(lib().mt_find(self.ctx.h, self.id, level, _ptr(keys, C.c_uint64), keys.size,
+                                     _ptr(out, C.c_int64)), "mt_find")
+        return out
+
+    def neighbors(self, level):
+        n = self.size(level)
+        out = np.zeros((self.q - 1, n), np.int32)
+        self.ctx.check(lib().mt_case_get_neighbors(self.ctx.h, self.id, level, _ptr(out, C.c_int32)), "neighbors")
+        return out
+
+    # ---- state --------------------------------------------------------
+    def initial_equilibrium(self, rho0, u0):
+        u = np.ascontiguousarray(u0, np.float64)
+        self.ctx.check(lib().mt_case_init_equilibrium(self.ctx.h, self.id, float(rho0), _ptr(u, C.c_double)),
+                       "init_equilibrium")
+
+    def set_populations(self, level, f, fcol=None):
+        f = np.ascontiguousarray(f, np.float64)
+        fc = f if fcol is None else np.ascontiguousarray(fcol, np.float64)
+        self.ctx.check(lib().mt_case_set_populations(self.ctx.h, self.id, level, _ptr(f, C.c_double),
+                                                     _ptr(fc, C.c_double)), "set_populations")
+
+    def populations(self, level):
+        n = self.size(level)
+        f = np.zeros((self.q, n))
+        fc = np.zeros((self.q, n))
+        self.ctx.check(lib().mt_case_get_populations(self.ctx.h, self.id, level, _ptr(f, C.c_double),
+                                                     _ptr(fc, C.c_double)), "get_populations")
+        return f, fc
+
+    def macros(self, level):
+        n = self.size(level)
+        rho = np.zeros(n)
+        u = np.zeros((3, n))
+        self.ctx.check(lib().mt_case_get_macros(self.ctx.h, self.id, level, _ptr(rho, C.c_double),
+                                                _ptr(u, C.c_double)), "get_macros")
+        return rho, u
+
+    # ---- the reference call surface ------------------------------------
+    def calculateMacros(self, level=None):
+        levels = range(self.L + 1) if level is None else [level]
+        for l in levels:
+            self.ctx.check(lib().mt_calculate_macros(self.ctx.h, self.id, l), "calculateMacros")
+
+    def collide(self, level):
+        self.ctx.check(lib().mt_collide(self.ctx.h, self.id, level), "collide")
+
+    def stream(self, level):
+        self.ctx.check(lib().mt_stream(self.ctx.h, self.id, level), "stream")
+
+    def AMR_transDDF_explosion(self, level):
+        self.ctx.check(lib().mt_explosion(self.ctx.h, self.id, level), "explosion")
+
+    def AMR_transDDF_coalescence(self, level):
+        self.ctx.check(lib().mt_coalescence(self.ctx.h, self.id, level), "coalescence")
+
+    def applyBoundaryCondition(self):
+        self.ctx.check(lib().mt_apply_bc(self.ctx.h, self.id), "applyBoundaryCondition")
+
+    def treat(self):
+        self.ctx.check(lib().mt_ib_treat(self.ctx.h, self.id), "treat")
+
+    def LBMkernel(self, level=0):
+        self.ctx.check(lib().mt_lbm_kernel(self.ctx.h, self.id, level), "LBMkernel")
+
+    def fluidSimulate(self, n_coarse_steps):
+        """n coarse steps (graph-replayed); asynchronous on the context stream."""
+        self.ctx.check(lib().mt_step(self.ctx.h, self.id, int(n_coarse_steps)), "mt_step")
+
+    def close(self):
+        """Release the case's device memory (mt_case_destroy)."""
+        if getattr(self, "id", None) is not None and self.ctx.h:
+            lib().mt_case_destroy(self.ctx.h, self.id)
+        self.id = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def force(self):
+        out = np.zeros(4)
+        self.ctx.check(lib().mt_get_force(self.ctx.h, self.id, _ptr(out, C.c_double)), "get_force")
+        return out
+
+    def reset_force(self):
+        self.ctx.check(lib().mt_reset_force(self.ctx.h, self.id), "reset_force")
+
+
+class DenseCase:
+    """Dense periodic Morton cube (uniform single level), any storage."""
+
+    def __init__(self, ctx: Context, case: Case, storage: str = None):
+        self.ctx = ctx
+        self.case = case
+        self.q = case.params.q
+        d = make_desc(case, storage)
+        cid = C.c_int32()
+        ctx.check(lib().mt_case_create_dense(ctx.h, C.byref(d), C.byref(cid)), "mt_case_create_dense")
+        self.id = cid.value
+        n = C.c_int64()
+        ctx.check(lib().mt_case_level_size(ctx.h, self.id, 0, C.byref(n)), "level_size")
+        self.n = n.value
+
+    def init_fields(self, rho, ux, uy, uz):
+        arrs = [np.ascontiguousarray(a, np.float64).ravel() for a in (rho, ux, uy, uz)]
+        self.ctx.check(lib().mt_case_init_fields(self.ctx.h, self.id, *[_ptr(a, C.c_double) for a in arrs]),
+                       "init_fields")
+        return arrs
+
+    def init_fields_ptr(self, rho_ptr, ux_ptr, uy_ptr, uz_ptr):
+        """Same as init_fields from raw host pointers (pinned buffers)."""
+        cast = lambda p: C.cast(C.c_void_p(p), C.POINTER(C.c_double))  # noqa: E731
+        self.ctx.check(lib().mt_case_init_fields(self.ctx.h, self.id, cast(rho_ptr), cast(ux_ptr), cast(uy_ptr),
+                                                 cast(uz_ptr)), "init_fields")
+
+    def set_populations(self, f):
+        f = np.ascontiguousarray(f, np.float64)
+        self.ctx.check(lib().mt_case_set_populations(self.ctx.h, self.id, 0, _ptr(f, C.c_double), None),
+                       "set_populations")
+
+    def populations(self):
+        f = np.zeros((self.q, self.n))
+        fc = np.zeros((self.q, self.n))
+        self.ctx.check(lib().mt_case_get_populations(self.ctx.h, self.id, 0, _ptr(f, C.c_double),
+                                                     _ptr(fc, C.c_double)), "get_populations")
+        return f, fc
+
+    def macros(self):
+        rho = np.zeros(self.n)
+        u = np.zeros((3, self.n))
+        self.ctx.check(lib().mt_case_get_macros(self.ctx.h, self.id, 0, _ptr(rho, C.c_double), _ptr(u, C.c_double)),
+                       "get_macros")
+        return rho, u
+
+    def macros_ptr(self, rho_ptr, u_ptr):
+        cast = lambda p: C.cast(C.c_void_p(p), C.POINTER(C.c_double))  # noqa: E731
+        self.ctx.check(lib().mt_case_get_macros(self.ctx.h, self.id, 0, cast(rho_ptr), cast(u_ptr)), "get_macros")
+
+    def reduce(self):
+        out = np.zeros(5)
+        self.ctx.check(lib().mt_case_reduce(self.ctx.h, self.id, _ptr(out, C.c_double)), "reduce")
+        return dict(mass=out[0], momentum=out[1:4].copy(), kinetic_energy=out[4])
+
+    def step(self, n=1):
+        self.ctx.check(lib().mt_step(self.ctx.h, self.id, int(n)), "mt_step")
+
+    def close(self):
+        if getattr(self, "id", None) is not None and self.ctx.h:
+            lib().mt_case_destroy(self.ctx.h, self.id)
+        self.id = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def morton_order_fields(n_edge, *fields):
+    """Reorder (x, y, z)-indexed cube fields into Morton (sorted key) order."""
+    from .lattice import morton_encode
+    idx = np.arange(n_edge)
+    X, Y, Z = np.meshgrid(idx, idx, idx, indexing="ij")
+    order = np.argsort(morton_encode(X.ravel(), Y.ravel(), Z.ravel()), kind="stable")
+    return [np.ascontiguousarray(f.ravel()[order]) for f in fields]

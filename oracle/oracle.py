@@ -153,14 +153,14 @@ def collide_cell(q, collision, f, rho, u, tau):
 # ---------------------------------------------------------------------------
 # reference harness driver
 # ---------------------------------------------------------------------------
-def harness_input(case, nsteps, init=None) -> bytes:
+def harness_input(case, nsteps, init=None, nwarm=0) -> bytes:
     """Serialise a case for oracle/refharness/harness.cpp (run_step)."""
     from mortontrie_amr_b200.case import COLLISIONS, IB_METHODS
     m = case.mesh
     p = case.params
     L = m.spec.max_level
     b = bytearray()
-    b += struct.pack("<iiiii", p.q, L, COLLISIONS[p.collision], IB_METHODS[p.ib_method], nsteps)
+    b += struct.pack("<iiiiii", p.q, L, COLLISIONS[p.collision], IB_METHODS[p.ib_method], nsteps, nwarm)
     b += struct.pack("<ddddd", p.nu, p.u_bc[0], p.u_bc[1], p.u_bc[2], p.u_ref)
     for l in range(L + 1):
         for name in SET_IDS:
@@ -207,17 +207,31 @@ def parse_harness_output(data: bytes, q, L, nsteps):
     return dict(seconds=secs, levels=levels, force=force, tau=tau)
 
 
-def run_harness(case, nsteps, init=None, timeout=600):
+def run_harness(case, nsteps, init=None, timeout=600, nwarm=0):
     import build
     q, L = case.params.q, case.mesh.spec.max_level
     exe = build.build_refharness(q, L)
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         with open(fin, "wb") as fh:
-            fh.write(harness_input(case, nsteps, init))
+            fh.write(harness_input(case, nsteps, init, nwarm))
         subprocess.run([exe, "step", fin, fout], check=True, timeout=timeout)
         with open(fout, "rb") as fh:
             return parse_harness_output(fh.read(), q, L, nsteps)
+
+
+def start_harness(case, nsteps, workdir, tag, nwarm=0):
+    """Launch one harness process without waiting (CPU baseline runs several
+    in parallel, one per core); returns (Popen, output path)."""
+    import build
+    q, L = case.params.q, case.mesh.spec.max_level
+    exe = build.harness_path(q, L)
+    if not os.path.exists(exe):
+        exe = build.build_refharness(q, L)
+    fin, fout = os.path.join(workdir, f"in{tag}.bin"), os.path.join(workdir, f"out{tag}.bin")
+    with open(fin, "wb") as fh:
+        fh.write(harness_input(case, nsteps, None, nwarm))
+    return subprocess.Popen([exe, "step", fin, fout]), fout
 
 
 def run_harness_morton(q, L, levels, keys, timeout=120):

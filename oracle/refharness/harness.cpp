@@ -121,6 +121,7 @@ int run_step(Reader &in, FILE *out)
         return 2;
     }
     int32_t collision = in.get<int32_t>(), ib_fh = in.get<int32_t>(), nsteps = in.get<int32_t>();
+    int32_t nwarm = in.get<int32_t>();
     sphere::U_kineViscosity = in.get<double>();
     sphere::U_u0 = in.get<double>();
     sphere::U_v0 = in.get<double>();
@@ -184,6 +185,12 @@ int run_step(Reader &in, FILE *out)
     }
 
     std::vector<double> force;
+    for (int s = 0; s < nwarm; ++s) {
+        mgr->LBMkernel(0);
+        mgr->calculateMacros();
+    }
+    mgr->m_ibFx_sum = mgr->m_ibFy_sum = mgr->m_ibFz_sum = 0.0;
+    mgr->m_ibForce_count = 0;
     auto t0 = std::chrono::steady_clock::now();
     for (int s = 0; s < nsteps; ++s) {
         mgr->LBMkernel(0);

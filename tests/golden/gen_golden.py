@@ -1,0 +1,83 @@
+"""Generate the golden vectors under tests/golden/ by running the reference's
+own LBM translation units (oracle/refharness, built by oracle/build.py from
+the reference checkout) on seeded synthetic cases.
+
+Run here, where the reference checkout exists:
+    python tests/golden/gen_golden.py
+The outputs are small .npz files; the GPU box only reads them.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from mortontrie_amr_b200.case import perturbed_populations  # noqa: E402
+from golden_cases import GOLDEN_CASES, build_case  # noqa: E402
+
+
+def set_digest(case):
+    h = hashlib.sha256()
+    m = case.mesh
+    for l in range(m.spec.max_level + 1):
+        for name in sorted(m.levels[l]):
+            h.update(name.encode())
+            h.update(np.ascontiguousarray(m.levels[l][name], np.uint64).tobytes())
+    for b in m.lat_bc:
+        h.update(np.ascontiguousarray(b, np.uint64).tobytes())
+    h.update(np.ascontiguousarray(m.dis_keys, np.uint64).tobytes())
+    h.update(np.ascontiguousarray(m.dis_rows, np.float64).tobytes())
+    return h.hexdigest()
+
+
+def main():
+    import oracle as O
+    for name, spec in GOLDEN_CASES.items():
+        case = build_case(spec)
+        init = perturbed_populations(case, seed=spec["seed"]) if spec["init"] == "perturbed" else None
+        out = O.run_harness(case, spec["steps"], init)
+        arrays = {"tau": out["tau"], "force": out["force"]}
+        for l, lv in enumerate(out["levels"]):
+            arrays[f"keys{l}"] = lv["keys"]
+            arrays[f"f{l}"] = lv["f"]
+            # fcol is compared bit-for-bit, so its SHA-256 is as strict as the array
+            arrays[f"fcol_sha{l}"] = np.frombuffer(hashlib.sha256(np.ascontiguousarray(lv["fcol"]).tobytes()).digest(),
+                                                   np.uint8)
+        meta = dict(spec=spec, set_digest=set_digest(case))
+        arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), np.uint8)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **arrays)
+        print(name, os.path.getsize(path), "bytes", [lv["keys"].size for lv in out["levels"]])
+
+    # Morton neighbour-key known answers from Morton_Assist::find_neighbor
+    rng = np.random.default_rng(99)
+    from mortontrie_amr_b200.lattice import cell_key
+    for (q, L) in [(27, 2)]:
+        levels, keys = [], []
+        for l in range(L + 1):
+            n = 64 << l
+            x = rng.integers(0, n, 120)
+            y = rng.integers(0, n, 120)
+            z = rng.integers(0, n, 120)
+            # include the box corners, where the masked arithmetic wraps
+            x[:4], y[:4], z[:4] = [0, n - 1, 0, n - 1], [0, 0, n - 1, n - 1], [0, n - 1, n - 1, 0]
+            keys.append(cell_key(L, l, x, y, z))
+            levels.append(np.full(120, l, np.int32))
+        levels = np.concatenate(levels)
+        keys = np.concatenate(keys)
+        nb = O.run_harness_morton(q, L, levels, keys)
+        path = os.path.join(HERE, f"morton_kat_q{q}_l{L}.npz")
+        np.savez_compressed(path, levels=levels, keys=keys, neighbors=nb)
+        print("morton kat", os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()

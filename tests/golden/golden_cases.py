@@ -1,0 +1,41 @@
+"""Specifications of the cases whose reference outputs are stored as golden
+vectors.  Shared by gen_golden.py and the tests, so both rebuild the same
+index sets with the mesher."""
+from __future__ import annotations
+
+from mortontrie_amr_b200.case import Case, CaseParams
+from mortontrie_amr_b200.mesh import MeshSpec, Sphere, build_mesh
+
+GOLDEN_CASES = {
+    # single populated level in a non-equilibrium-extrapolation box (LBGK Q19)
+    "box_q19_neq": dict(q=19, collision="LBGK", coarse=(10, 8, 8), max_level=1, refine=[None], sphere=None,
+                        boundary=("bc", "bc", "bc"), nu=0.02, u=0.05, ib="FH", steps=6, seed=7, init="perturbed"),
+    # two levels with a sphere: explosion, coalescence, Filippova-Haenel links, clamp, MDF
+    "sphere_q19_fh": dict(q=19, collision="LBGK", coarse=(16, 12, 12), max_level=1, refine=[((4, 3, 3), (12, 9, 9))],
+                          sphere=((8.0, 6.0, 6.0), 1.4), boundary=("bc", "bc", "bc"), nu=0.015, u=0.05, ib="FH",
+                          steps=4, seed=11, init="perturbed"),
+    # the same from the reference's own initial state (f = feq(rho0, u_bc))
+    "sphere_q19_fh_refinit": dict(q=19, collision="LBGK", coarse=(16, 12, 12), max_level=1,
+                                  refine=[((4, 3, 3), (12, 9, 9))], sphere=((8.0, 6.0, 6.0), 1.4),
+                                  boundary=("bc", "bc", "bc"), nu=0.015, u=0.05, ib="FH", steps=5, seed=0,
+                                  init="reference"),
+    # D3Q27 cumulant across a refinement interface
+    "refined_q27_cumulant": dict(q=27, collision="Cumulant", coarse=(12, 10, 10), max_level=1,
+                                 refine=[((3, 3, 3), (9, 7, 7))], sphere=None, boundary=("bc", "bc", "bc"), nu=0.01,
+                                 u=0.04, ib="FH", steps=4, seed=5, init="perturbed"),
+    # three levels, distance-weighted links
+    "sphere_q19_dw_l2": dict(q=19, collision="LBGK", coarse=(14, 12, 12), max_level=2,
+                             refine=[((4, 3, 3), (10, 9, 9)), ((11, 9, 9), (17, 15, 15))],
+                             sphere=((7.0, 6.0, 6.0), 0.6), boundary=("bc", "bc", "bc"), nu=0.005, u=0.05, ib="DW",
+                             steps=2, seed=3, init="perturbed"),
+}
+
+
+def build_case(spec) -> Case:
+    sphere = Sphere(tuple(spec["sphere"][0]), spec["sphere"][1]) if spec["sphere"] else None
+    refine = [None if r is None else (tuple(r[0]), tuple(r[1])) for r in spec["refine"]]
+    ms = MeshSpec(q=spec["q"], max_level=spec["max_level"], coarse=tuple(spec["coarse"]), refine=refine,
+                  boundary=tuple(spec["boundary"]), sphere=sphere)
+    p = CaseParams(q=spec["q"], collision=spec["collision"], ib_method=spec["ib"], bc_mode="neq", nu=spec["nu"],
+                   u_bc=(spec["u"], 0.0, 0.0), u_ref=spec["u"])
+    return Case(build_mesh(ms), p)

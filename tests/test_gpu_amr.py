@@ -1,0 +1,130 @@
+"""Multi-level FP64 path on the GPU: bit-exact against the reference's golden
+vectors and against the CPU oracle, through the C ABI."""
+import numpy as np
+import pytest
+from golden_cases import GOLDEN_CASES
+from helpers import TAG_BC, init_of, load_golden, rel_err, run_oracle, sha
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from mortontrie_amr_b200.lbm import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def _device_case(ctx, case, init):
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    mgr = LBM_Manager(ctx, case)
+    if init is not None:
+        for l, (keys, f) in enumerate(init):
+            k, _ = mgr.keys(l)
+            assert np.array_equal(k, keys)
+            mgr.set_populations(l, f)
+    return mgr
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN_CASES))
+def test_gpu_matches_reference_goldens(ctx, name):
+    spec, case, z, _ = load_golden(name)
+    mgr = _device_case(ctx, case, init_of(case, spec))
+    mgr.fluidSimulate(spec["steps"])
+    ctx.synchronize()
+    for l in range(case.max_level + 1):
+        keys, tags = mgr.keys(l)
+        np.testing.assert_array_equal(keys, z[f"keys{l}"])
+        f, fcol = mgr.populations(l)
+        keep = (tags & TAG_BC) == 0
+        assert np.array_equal(f[:, keep], z[f"f{l}"][:, keep]), (name, l, float(np.abs(f[:, keep] - z[f"f{l}"][:, keep]).max()))
+        assert sha(fcol) == bytes(z[f"fcol_sha{l}"]), (name, l)
+    force = mgr.force()
+    ref = z["force"].sum(axis=0)
+    assert force[3] == ref[3]
+    if np.abs(ref[:3]).max() > 0:
+        assert rel_err(force[:3], ref[:3]) < 1e-12
+
+
+def test_neighbor_table_matches_oracle(ctx):
+    import oracle as O
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    spec, case, z, _ = load_golden("sphere_q19_dw_l2")
+    mgr = LBM_Manager(ctx, case)
+    oc = O.OracleCase(case)
+    for l in range(case.max_level + 1):
+        assert np.array_equal(mgr.neighbors(l), oc.neighbors(l)), l
+        keys, _ = mgr.keys(l)
+        probe = np.concatenate([keys[::7], keys[::11] + np.uint64(1), np.array([0, 2**63], np.uint64)])
+        idx = mgr.find(l, probe)
+        want = np.searchsorted(keys, probe)
+        want = np.where((want < keys.size) & (keys[np.minimum(want, keys.size - 1)] == probe), want, -1)
+        assert np.array_equal(idx, want)
+
+
+def _cfg1_small(**kw):
+    from mortontrie_amr_b200.case import sphere_case
+    return sphere_case(coarse=(32, 16, 16), refine=[((6, 4, 4), (18, 12, 12))], center=(12, 8, 8), radius=2.0, **kw)
+
+
+@pytest.mark.parametrize("steps", [1, 7])
+def test_zouhe_outflow_periodic_matches_oracle(ctx, steps):
+    """cfg1 boundary set (velocity inlet, outflow, periodic y/z): restated
+    boundaries, GPU vs oracle bit-exact."""
+    case = _cfg1_small()
+    mgr = _device_case(ctx, case, None)
+    mgr.fluidSimulate(steps)
+    ctx.synchronize()
+    oc = run_oracle(case, steps)
+    for l in range(2):
+        f, fcol = mgr.populations(l)
+        g = oc.get(l)
+        assert np.array_equal(f, g["f"]) and np.array_equal(fcol, g["fcol"]), l
+    assert rel_err(mgr.force()[:3], oc.force()[:3]) < 1e-12
+
+
+def test_phase_calls_equal_graph_step(ctx):
+    """The reference call surface (LBMkernel + calculateMacros issued one by
+    one) gives the same state as the graph-replayed coarse step."""
+    case = _cfg1_small()
+    a = _device_case(ctx, case, None)
+    b = _device_case(ctx, case, None)
+    a.fluidSimulate(3)
+    for _ in range(3):
+        b.LBMkernel(0)
+        b.calculateMacros()
+    ctx.synchronize()
+    for l in range(2):
+        fa, ca = a.populations(l)
+        fb, cb = b.populations(l)
+        assert np.array_equal(fa, fb) and np.array_equal(ca, cb)
+
+
+def test_cfg1_full_size_matches_oracle(ctx):
+    """cfg1 at its full size (64x32x32 coarse, 2 levels, sphere R=4) for 10
+    coarse steps."""
+    from mortontrie_amr_b200.case import sphere_case
+    case = sphere_case()
+    mgr = _device_case(ctx, case, None)
+    mgr.fluidSimulate(10)
+    ctx.synchronize()
+    oc = run_oracle(case, 10)
+    for l in range(2):
+        f, fcol = mgr.populations(l)
+        g = oc.get(l)
+        assert np.array_equal(f, g["f"]), (l, float(np.abs(f - g["f"]).max()))
+        assert np.array_equal(fcol, g["fcol"])
+    assert rel_err(mgr.force()[:3], oc.force()[:3]) < 1e-12
+
+
+def test_missing_child_is_reported(ctx):
+    """A contract violation (a coarse F2C cell whose children are not stored)
+    returns MT_ERR_MESH instead of faulting, like the reference's .at()
+    throwing std::out_of_range."""
+    from mortontrie_amr_b200.lbm import LBM_Manager, MTError
+    case = _cfg1_small()
+    lv1 = case.mesh.levels[1]
+    lv1["overlap_C2F"] = lv1["overlap_C2F"][5:]
+    with pytest.raises(MTError, match="MT_ERR_MESH"):
+        LBM_Manager(ctx, case)
