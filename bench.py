@@ -174,8 +174,11 @@ def run_ours(args):
     from mortontrie_amr_b200.lbm import Context, DenseCase
     world, rank, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
+    # a dedicated (non-default) stream shared by torch's events and the library
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
     ctx = Context(local)
-    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    ctx.set_stream(stream.cuda_stream)
     fields = tgv_fields()
     n_cells = N_EDGE ** 3
     peak, peak_kind = measured_hbm_peak()
@@ -184,6 +187,7 @@ def run_ours(args):
     case = make_case("f16")
     dense = DenseCase(ctx, case, "f16")
     dense.init_fields(*fields)
+    block, tune_ms = dense.tune()  # outside the timed region; leaves the state unchanged
     sampler = ClockSampler(local)
     if rank == 0:
         sampler.start()
@@ -193,26 +197,28 @@ def run_ours(args):
     per_launch = secs / args.steps
     achieved = BYTES_PER_CELL["f16"] * n_cells / per_launch / 1e9
     red = dense.reduce()
-    del dense
+    dense.close()
 
     # storage variants, same workload
     variants = {}
     for st in (() if args.quick else ("f64", "f32", "bf16")):
         d = DenseCase(ctx, make_case(st), st)
         d.init_fields(*fields)
+        vblock, _ = d.tune()
         s, _ = time_steps(ctx, d, args.steps, args.warmup, world, torch)
         bw = BYTES_PER_CELL[st] * n_cells / (s / args.steps) / 1e9
         variants[st] = {"mlups": round(world * n_cells * args.steps / s / 1e6, 1),
                         "bytes_per_cell_update": BYTES_PER_CELL[st], "achieved_gbs": round(bw, 1),
-                        "frac": round(bw / peak, 4)}
-        del d
+                        "frac": round(bw / peak, 4), "block": vblock}
+        d.close()
 
     # end to end through the public API: pinned host fields -> device, the
     # steps, density + velocity back to pinned host memory
     if args.quick:
         if rank == 0:
-            print(json.dumps({"quick": True, "edge": N_EDGE, "mlups": round(mlups, 1),
-                              "achieved_gbs": round(achieved, 1), "launches": int(launches)}), flush=True)
+            print(json.dumps({"quick": True, "edge": N_EDGE, "mlups": round(mlups, 1), "block": block,
+                              "tune_ms": tune_ms, "achieved_gbs": round(achieved, 1),
+                              "launches": int(launches)}), flush=True)
         ctx.close()
         return
     host = [torch.from_numpy(f).pin_memory() for f in fields]
@@ -221,6 +227,7 @@ def run_ours(args):
     d = DenseCase(ctx, case, "f16")
     stream = torch.cuda.current_stream()
     d.init_fields_ptr(*[h.data_ptr() for h in host])
+    d.tune()
     d.step(args.warmup)
     d.macros_ptr(out_rho.data_ptr(), out_u.data_ptr())
     torch.cuda.synchronize()
@@ -256,6 +263,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "cells": n_cells, "storage": "f16 deviations f - w_q",
                        "bytes_per_cell_update": BYTES_PER_CELL["f16"], "levels": 1,
+                       "block": block, "tune_ms_per_launch": tune_ms,
                        "l2": "state 637 MB > 126 MB L2; no flush", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,

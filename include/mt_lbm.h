@@ -133,12 +133,20 @@ int mt_stream(mt_ctx *ctx, int32_t case_id, int32_t level);           /* ABPatte
 int mt_explosion(mt_ctx *ctx, int32_t case_id, int32_t level);        /* LBM_Manager::AMR_transDDF_explosion */
 int mt_coalescence(mt_ctx *ctx, int32_t case_id, int32_t level);      /* LBM_Manager::AMR_transDDF_coalescence */
 int mt_apply_bc(mt_ctx *ctx, int32_t case_id);                        /* applyBoundaryCondition(face, "AfterStream") x 6 */
+/* one face group: 0 West, 1 East, 2 South, 3 North, 4 Bot, 5 Top
+ * (D3Q19_BoundaryCondtion_Manager::applyBoundaryCondition, D3Q19_BC_Manager.hpp:220-244) */
+int mt_apply_bc_face(mt_ctx *ctx, int32_t case_id, int32_t face);
 int mt_ib_treat(mt_ctx *ctx, int32_t case_id);                        /* ComplexBoundary_Model::treat */
 int mt_lbm_kernel(mt_ctx *ctx, int32_t case_id, int32_t level);       /* LBM_Manager::LBMkernel(level) */
 /* n coarse steps of LBM_Manager::fluidSimulate (LBM_Simulator.cpp:11-17):
  * LBMkernel(0) then calculateMacros() on every level, replayed from a CUDA
  * graph; asynchronous on the context stream */
 int mt_step(mt_ctx *ctx, int32_t case_id, int32_t n_coarse_steps);
+/* Autotuner of the dense path (no reference counterpart): times the fused
+ * kernel at 128, 256, 512 and 1024 threads per block on the case's own state
+ * (writing only the scratch array, so the state is unchanged) and keeps the
+ * fastest; ms_per_candidate (nullable) receives the 4 mean launch times. */
+int mt_case_tune(mt_ctx *ctx, int32_t case_id, int32_t *best_block, float *ms_per_candidate);
 /* accumulated momentum-exchange force of treat() calls: fx, fy, fz, count
  * (LBM_Manager::accumIBForce, LBM_Manager.cpp:846-852) */
 int mt_get_force(mt_ctx *ctx, int32_t case_id, double *out4);

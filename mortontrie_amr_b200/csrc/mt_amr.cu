@@ -755,7 +755,8 @@ int amr_init_equilibrium(Ctx &ctx, Case &c, double rho0, const double *u0)
     return MT_OK;
 }
 
-enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT };
+enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
+       PH_BC_FACE0 = 8 };
 
 template <int Q>
 static int phase_q(Ctx &ctx, Case &c, int phase, int l)
@@ -773,13 +774,16 @@ static int phase_q(Ctx &ctx, Case &c, int phase, int l)
         return MT_OK;
     case PH_COLLIDE:
         if (lv.ncollide) {
-            if (c.d.collision == MT_COLL_LBGK)
+            if (c.d.collision == MT_COLL_LBGK) {
                 k_collide<Q, MT_COLL_LBGK><<<grid_for(lv.ncollide, B), B, 0, s>>>(lv.collide_list, lv.ncollide, n,
                                                                                    c.d.tau[l], lv.f, lv.rho, lv.u,
                                                                                    lv.fcol);
-            else
-                k_collide<Q, MT_COLL_CUMULANT><<<grid_for(lv.ncollide, 64), 64, 0, s>>>(
-                    lv.collide_list, lv.ncollide, n, c.d.tau[l], lv.f, lv.rho, lv.u, lv.fcol);
+            } else {
+                // the cumulant model exists for D3Q27 only (checked at case creation)
+                if constexpr (Q == 27)
+                    k_collide<Q, MT_COLL_CUMULANT><<<grid_for(lv.ncollide, 64), 64, 0, s>>>(
+                        lv.collide_list, lv.ncollide, n, c.d.tau[l], lv.f, lv.rho, lv.u, lv.fcol);
+            }
             MT_LAUNCHED(ctx);
         }
         if (lv.nlist[2]) {
@@ -812,7 +816,11 @@ static int phase_q(Ctx &ctx, Case &c, int phase, int l)
         MT_LAUNCHED(ctx);
         return MT_OK;
     }
-    case PH_BC: {
+    case PH_BC:
+    case PH_BC_FACE0 + 0: case PH_BC_FACE0 + 1: case PH_BC_FACE0 + 2:
+    case PH_BC_FACE0 + 3: case PH_BC_FACE0 + 4: case PH_BC_FACE0 + 5: {
+        // all six face groups in the reference's order, or one of them
+        const int f0 = phase == PH_BC ? 0 : phase - PH_BC_FACE0, f1 = phase == PH_BC ? 6 : f0 + 1;
         Level &l0 = c.lv[0];
         static const int face_sets[6][9] = {
             {0, 7, 8, 15, 17, 19, 20, 23, 24}, {1, 6, 9, 14, 16, 18, 21, 22, 25},
@@ -820,7 +828,7 @@ static int phase_q(Ctx &ctx, Case &c, int phase, int l)
             {4, -1, -1, -1, -1, -1, -1, -1, -1}, {5, -1, -1, -1, -1, -1, -1, -1, -1}};
         double *tmp = c.bc_tmp;
         if (!tmp) return MT_OK;
-        for (int face = 0; face < 6; ++face)
+        for (int face = f0; face < f1; ++face)
             for (int g = 0; g < 9; ++g) {
                 const int b = face_sets[face][g];
                 if (b < 0) break;

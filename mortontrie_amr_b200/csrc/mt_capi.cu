@@ -27,7 +27,8 @@ int set_err(Ctx &ctx, int code, const std::string &msg)
 
 namespace {
 
-enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT };
+enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
+       PH_BC_FACE0 = 8 };
 
 int get_case(mt_ctx *h, int32_t id, Case **out)
 {
@@ -514,6 +515,16 @@ int mt_apply_bc(mt_ctx *h, int32_t id)
     if (rc) return rc;
     return phase_call(h, id, c->d.bc_mode == MT_BC_NEQ ? PH_BC : PH_BC_INOUT, 0);
 }
+int mt_apply_bc_face(mt_ctx *h, int32_t id, int32_t face)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    if (face < 0 || face > 5) return set_err(h->c, MT_ERR_ARG, "face must be 0..5 (West East South North Bot Top)");
+    if (c->d.bc_mode != MT_BC_NEQ) return set_err(h->c, MT_ERR_STATE, "per-face calls apply to the NEQ boundary");
+    return phase_call(h, id, PH_BC_FACE0 + face, 0);
+}
+
 int mt_ib_treat(mt_ctx *h, int32_t id)
 {
     Case *c;
@@ -558,6 +569,26 @@ int mt_step(mt_ctx *h, int32_t id, int32_t n)
     }
     rc = amr_step(ctx, *c, n);
     if (rc) return rc;
+    return MT_OK;
+}
+
+int mt_case_tune(mt_ctx *h, int32_t id, int32_t *best_block, float *ms_per_candidate)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!c->dense) return set_err(ctx, MT_ERR_STATE, "the tuner picks the block shape of the dense kernel");
+    float ms[8];
+    int blocks[8], n = 0;
+    rc = dense_dispatch(*c, [&](auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        return DenseOps<S>::tune(ctx, *c, ms, blocks, &n);
+    });
+    if (rc) return rc;
+    if (best_block) *best_block = c->dense_block;
+    if (ms_per_candidate)
+        for (int j = 0; j < n; ++j) ms_per_candidate[j] = ms[j];
     return MT_OK;
 }
 

@@ -24,33 +24,41 @@
 
 namespace mt {
 
+// index type I: uint32_t while the array fits 2^32 elements (one wide
+// multiply-add per address), int64_t beyond
 template <class S> struct Store;
 template <> struct Store<double> {
     using C = double;
     static constexpr bool shifted = false;
-    __device__ static __forceinline__ double ld(const double *p, int64_t i) { return __ldg(p + i); }
-    __device__ static __forceinline__ void st(double *p, int64_t i, double v) { p[i] = v; }
+    template <class I> __device__ static __forceinline__ double ld(const double *p, I i) { return __ldg(p + i); }
+    template <class I> __device__ static __forceinline__ void st(double *p, I i, double v) { p[i] = v; }
 };
 template <> struct Store<float> {
     using C = float;
     static constexpr bool shifted = true;
-    __device__ static __forceinline__ float ld(const float *p, int64_t i) { return __ldg(p + i); }
-    __device__ static __forceinline__ void st(float *p, int64_t i, float v) { p[i] = v; }
+    template <class I> __device__ static __forceinline__ float ld(const float *p, I i) { return __ldg(p + i); }
+    template <class I> __device__ static __forceinline__ void st(float *p, I i, float v) { p[i] = v; }
 };
 template <> struct Store<__half> {
     using C = float;
     static constexpr bool shifted = true;
-    __device__ static __forceinline__ float ld(const __half *p, int64_t i) { return __half2float(__ldg(p + i)); }
-    __device__ static __forceinline__ void st(__half *p, int64_t i, float v) { p[i] = __float2half_rn(v); }
+    template <class I> __device__ static __forceinline__ float ld(const __half *p, I i)
+    {
+        return __half2float(__ldg(p + i));
+    }
+    template <class I> __device__ static __forceinline__ void st(__half *p, I i, float v) { p[i] = __float2half_rn(v); }
 };
 template <> struct Store<__nv_bfloat16> {
     using C = float;
     static constexpr bool shifted = true;
-    __device__ static __forceinline__ float ld(const __nv_bfloat16 *p, int64_t i)
+    template <class I> __device__ static __forceinline__ float ld(const __nv_bfloat16 *p, I i)
     {
         return __bfloat162float(__ldg(p + i));
     }
-    __device__ static __forceinline__ void st(__nv_bfloat16 *p, int64_t i, float v) { p[i] = __float2bfloat16_rn(v); }
+    template <class I> __device__ static __forceinline__ void st(__nv_bfloat16 *p, I i, float v)
+    {
+        p[i] = __float2bfloat16_rn(v);
+    }
 };
 
 struct DenseGeom {
@@ -100,20 +108,73 @@ __device__ __forceinline__ void lbgk_dev(float *s, float omega)
     }
 }
 
-template <int Q, class S, int COLL, int MODE>
-__global__ void __launch_bounds__(256) k_dense(const S *__restrict__ A, S *__restrict__ B, int64_t N, DenseGeom g,
-                                              int textbook, double tau)
+// FP32 LBGK on deviations, opposite directions paired: for q and inv(q) the
+// equilibrium shares its even part w (drho + rho (4.5 eu^2 - 1.5 u^2)) and
+// flips the sign of its odd part 3 w rho eu (D3Q19/27 list q, q+1 as a pair
+// for every odd q).
+template <int Q>
+__device__ __forceinline__ void lbgk_dev_pairs(float *s, float omega)
+{
+    float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        dr += s[k];
+        if (ex(k)) jx += ex(k) > 0 ? s[k] : -s[k];
+        if (ey(k)) jy += ey(k) > 0 ? s[k] : -s[k];
+        if (ez(k)) jz += ez(k) > 0 ? s[k] : -s[k];
+    }
+    const float rho = 1.f + dr;
+    const float ir = __frcp_rn(rho);
+    const float ux = jx * ir, uy = jy * ir, uz = jz * ir;
+    const float uu = 1.5f * (ux * ux + uy * uy + uz * uz);
+    {
+        const float d0 = (float)w<Q>(0) * (dr - rho * uu);
+        s[0] = fmaf(omega, d0 - s[0], s[0]);
+    }
+#pragma unroll
+    for (int k = 1; k < Q; k += 2) {
+        float eu = 0.f;
+        if (ex(k)) eu += ex(k) > 0 ? ux : -ux;
+        if (ey(k)) eu += ey(k) > 0 ? uy : -uy;
+        if (ez(k)) eu += ez(k) > 0 ? uz : -uz;
+        const float wk = (float)w<Q>(k);
+        const float wr = wk * rho;
+        const float even = fmaf(wr, fmaf(4.5f * eu, eu, -uu), wk * dr);
+        const float odd = 3.f * wr * eu;
+        const float dp = even + odd, dm = even - odd;
+        s[k] = fmaf(omega, dp - s[k], s[k]);
+        s[k + 1] = fmaf(omega, dm - s[k + 1], s[k + 1]);
+    }
+}
+
+// One cell per thread.  The three dilated coordinate parts of each axis at
+// offsets -1, 0, +1 are formed once; the pull source of direction k is then
+// px | py | pz of the right offsets (CONV 0: from x + e_k as the reference
+// streams, 1: from x - e_k).  IDX is the offset type: 32-bit while Q*N fits.
+template <int Q, class S, int COLL, int MODE, int CONV, class IDX>
+__global__ void __launch_bounds__(1024) k_dense(const S *__restrict__ A, S *__restrict__ B, IDX N, DenseGeom g,
+                                              double tau)
 {
     using T = Store<S>;
     using C = typename T::C;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const int sgn = textbook ? -1 : 1;
+    if (i >= (uint32_t)N) return;
+    uint32_t p[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const uint32_t c = i & g.m[a];
+        p[a][1] = c;
+        p[a][2] = ((i | ~g.m[a]) + g.lo[a]) & g.m[a];
+        p[a][0] = (c - g.lo[a]) & g.m[a];
+    }
+    constexpr int sg = CONV ? -1 : 1;
     C f[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-        const uint32_t src = (MODE == DM_COLLIDE || k == 0) ? i : dense_nbr(g, i, k, sgn);
-        f[k] = T::ld(A, (int64_t)k * N + src);
+        const uint32_t src = (MODE == DM_COLLIDE || k == 0)
+                                 ? i
+                                 : (p[0][1 + sg * ex(k)] | p[1][1 + sg * ey(k)] | p[2][1 + sg * ez(k)]);
+        f[k] = T::ld(A, (IDX)k * N + (IDX)src);
     }
     if (MODE != DM_PULL) {
         if constexpr (!T::shifted) {
@@ -130,7 +191,7 @@ __global__ void __launch_bounds__(256) k_dense(const S *__restrict__ A, S *__res
             }
         } else {
             if constexpr (COLL == MT_COLL_LBGK) {
-                lbgk_dev<Q>(f, (float)(1.0 / tau));
+                lbgk_dev_pairs<Q>(f, (float)(1.0 / tau));
             } else {
                 float full[27], o[27];
                 float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
@@ -151,7 +212,7 @@ __global__ void __launch_bounds__(256) k_dense(const S *__restrict__ A, S *__res
         }
     }
 #pragma unroll
-    for (int k = 0; k < Q; ++k) T::st(B, (int64_t)k * N + i, f[k]);
+    for (int k = 0; k < Q; ++k) T::st(B, (IDX)k * N + (IDX)i, f[k]);
 }
 
 // populations from host doubles -> storage (shift applied), or equilibrium of fields
@@ -301,19 +362,30 @@ inline DenseGeom dense_geom(int bits)
 template <class S>
 int DenseOps<S>::step(Ctx &ctx, Case &c, int mode)
 {
-    const int B = 256;
+    const int B = c.dense_block;
     const unsigned grid = grid_for(c.N, B);
     const DenseGeom g = dense_geom(c.bits);
     const S *A = (const S *)c.A;
     S *Bp = (S *)c.B;
     const int tb = c.d.stream_convention;
     const double tau = c.d.tau[0];
-#define MT_DENSE_LAUNCH(QQ, CC)                                                                           \
-    do {                                                                                                  \
-        if (mode == DM_FUSED)                                                                             \
-            k_dense<QQ, S, CC, DM_FUSED><<<grid, B, 0, ctx.stream>>>(A, Bp, c.N, g, tb, tau);             \
-        else                                                                                              \
-            k_dense<QQ, S, CC, DM_COLLIDE><<<grid, B, 0, ctx.stream>>>(A, Bp, c.N, g, tb, tau);           \
+    const bool idx32 = (uint64_t)c.d.q * (uint64_t)c.N < (1ull << 32);
+#define MT_DENSE_LAUNCH_I(QQ, CC, IDX)                                                                     \
+    do {                                                                                                   \
+        const IDX n = (IDX)c.N;                                                                            \
+        if (mode == DM_COLLIDE)                                                                            \
+            k_dense<QQ, S, CC, DM_COLLIDE, 0, IDX><<<grid, B, 0, ctx.stream>>>(A, Bp, n, g, tau);          \
+        else if (tb)                                                                                       \
+            k_dense<QQ, S, CC, DM_FUSED, 1, IDX><<<grid, B, 0, ctx.stream>>>(A, Bp, n, g, tau);            \
+        else                                                                                               \
+            k_dense<QQ, S, CC, DM_FUSED, 0, IDX><<<grid, B, 0, ctx.stream>>>(A, Bp, n, g, tau);            \
+    } while (0)
+#define MT_DENSE_LAUNCH(QQ, CC)                      \
+    do {                                             \
+        if (idx32)                                   \
+            MT_DENSE_LAUNCH_I(QQ, CC, uint32_t);     \
+        else                                         \
+            MT_DENSE_LAUNCH_I(QQ, CC, int64_t);      \
     } while (0)
     if (c.d.q == 19)
         MT_DENSE_LAUNCH(19, MT_COLL_LBGK);
@@ -322,6 +394,7 @@ int DenseOps<S>::step(Ctx &ctx, Case &c, int mode)
     else
         MT_DENSE_LAUNCH(27, MT_COLL_CUMULANT);
 #undef MT_DENSE_LAUNCH
+#undef MT_DENSE_LAUNCH_I
     MT_LAUNCHED(ctx);
     std::swap(c.A, c.B);
     return MT_OK;
@@ -401,6 +474,49 @@ int DenseOps<S>::reduce(Ctx &ctx, Case &c, double *d_out)
     k_sum_partials<<<1, 256, 0, ctx.stream>>>(partial, grid, d_out);
     MT_LAUNCHED(ctx);
     cudaFreeAsync(partial, ctx.stream);
+    return MT_OK;
+}
+
+template <class S>
+int DenseOps<S>::tune(Ctx &ctx, Case &c, float *ms_out, int *blocks_out, int *n_out)
+{
+    static const int cand[] = {128, 256, 512, 1024};
+    const int nc = (int)(sizeof(cand) / sizeof(cand[0]));
+    cudaEvent_t e0, e1;
+    MT_CUDA(ctx, cudaEventCreate(&e0));
+    MT_CUDA(ctx, cudaEventCreate(&e1));
+    const int saved = c.dense_block;
+    int best = saved;
+    float best_ms = 1e30f;
+    for (int j = 0; j < nc; ++j) {
+        c.dense_block = cand[j];
+        // each launch writes B from A and swaps; two launches restore A as
+        // the input, so timing pairs of launches leaves the state where the
+        // last pair put it: run one extra swap-back pair outside the timing
+        float ms = 0.f;
+        for (int rep = 0; rep < 2; ++rep) {
+            MT_CUDA(ctx, cudaEventRecord(e0, ctx.stream));
+            for (int t = 0; t < 4; ++t) {
+                int rc = step(ctx, c, DM_FUSED);
+                if (rc) return rc;
+                std::swap(c.A, c.B);  // undo the swap: every timed launch reads the same A
+            }
+            MT_CUDA(ctx, cudaEventRecord(e1, ctx.stream));
+            MT_CUDA(ctx, cudaEventSynchronize(e1));
+            MT_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+        }
+        ms /= 4.f;
+        if (ms_out) ms_out[j] = ms;
+        if (blocks_out) blocks_out[j] = cand[j];
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = cand[j];
+        }
+    }
+    if (n_out) *n_out = nc;
+    c.dense_block = best;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     return MT_OK;
 }
 

@@ -80,6 +80,7 @@ struct Case {
     void *A = nullptr, *B = nullptr;  // populations [Q * N] in the storage type
     bool a_is_fcol = false;           // false: A holds post-stream f; true: A holds post-collision fcol
     double *bc_tmp = nullptr;         // scratch of the boundary sweep
+    int dense_block = 256;            // threads per block of the fused kernel (autotuned)
     // captured coarse step
     cudaGraphExec_t graph = nullptr;
     int64_t graph_launches = 0;
@@ -113,6 +114,9 @@ template <class S> struct DenseOps {
     static int set(Ctx &ctx, Case &c, const double *d_f);
     static int macros(Ctx &ctx, Case &c, double *d_rho, double *d_u);
     static int reduce(Ctx &ctx, Case &c, double *d_out);
+    // time the fused kernel at each candidate block size (A -> B, no swap:
+    // the state is untouched) and keep the fastest in c.dense_block
+    static int tune(Ctx &ctx, Case &c, float *ms_out, int *blocks_out, int *n_out);
 };
 
 // error helpers

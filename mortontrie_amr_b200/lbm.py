@@ -30,7 +30,8 @@ EXPORTS = [
     "mt_case_build", "mt_case_level_size", "mt_case_get_keys", "mt_case_get_neighbors", "mt_find",
     "mt_case_init_equilibrium", "mt_case_init_fields", "mt_case_set_populations", "mt_case_get_populations",
     "mt_case_get_macros", "mt_case_reduce", "mt_calculate_macros", "mt_collide", "mt_stream", "mt_explosion",
-    "mt_coalescence", "mt_apply_bc", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force", "mt_reset_force",
+    "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
+    "mt_reset_force", "mt_case_tune",
 ]
 
 
@@ -70,8 +71,9 @@ def lib():
             "mt_case_get_populations": [vp, i32, i32, dp, dp], "mt_case_get_macros": [vp, i32, i32, dp, dp],
             "mt_case_reduce": [vp, i32, dp], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
-            "mt_apply_bc": [vp, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
+            "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
+            "mt_case_tune": [vp, i32, i32p, C.POINTER(C.c_float)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -246,8 +248,16 @@ class LBM_Manager:
     def AMR_transDDF_coalescence(self, level):
         self.ctx.check(lib().mt_coalescence(self.ctx.h, self.id, level), "coalescence")
 
-    def applyBoundaryCondition(self):
-        self.ctx.check(lib().mt_apply_bc(self.ctx.h, self.id), "applyBoundaryCondition")
+    FACES = {"West": 0, "East": 1, "South": 2, "North": 3, "Bot": 4, "Top": 5}
+
+    def applyBoundaryCondition(self, face=None, position="AfterStream"):
+        """All faces in the reference's order, or one face by name."""
+        if position != "AfterStream":
+            raise MTError("only the AfterStream position exists on the live boundary path")
+        if face is None:
+            self.ctx.check(lib().mt_apply_bc(self.ctx.h, self.id), "applyBoundaryCondition")
+        else:
+            self.ctx.check(lib().mt_apply_bc_face(self.ctx.h, self.id, self.FACES[face]), "applyBoundaryCondition")
 
     def treat(self):
         self.ctx.check(lib().mt_ib_treat(self.ctx.h, self.id), "treat")
@@ -337,6 +347,14 @@ class DenseCase:
 
     def step(self, n=1):
         self.ctx.check(lib().mt_step(self.ctx.h, self.id, int(n)), "mt_step")
+
+    def tune(self):
+        """Pick the fused kernel's block size (state unchanged); returns
+        (block, {block: ms per launch})."""
+        best = C.c_int32()
+        ms = (C.c_float * 4)()
+        self.ctx.check(lib().mt_case_tune(self.ctx.h, self.id, C.byref(best), ms), "mt_case_tune")
+        return best.value, dict(zip((128, 256, 512, 1024), [round(float(v), 5) for v in ms]))
 
     def close(self):
         if getattr(self, "id", None) is not None and self.ctx.h:

@@ -88,6 +88,23 @@ def test_reduced_precision_vs_f64(ctx, storage):
     assert abs(m_lp - m_ref) / m_ref < (1e-6 if storage == "f32" else 1e-3)
 
 
+def test_tuner_leaves_state_unchanged(ctx):
+    """mt_case_tune times the fused kernel into the scratch array only: the
+    trajectory with tuning in the middle equals the one without."""
+    n = 32
+    case, fields = _tgv_case(n)
+    a = _dense(ctx, case, fields, "f64")
+    b = _dense(ctx, case, fields, "f64")
+    a.step(3)
+    b.step(3)
+    block, ms = b.tune()
+    assert block in (128, 256, 512, 1024) and all(v > 0 for v in ms.values())
+    a.step(4)
+    b.step(4)
+    ctx.synchronize()
+    assert np.array_equal(a.populations()[0], b.populations()[0])
+
+
 def test_mass_and_momentum_conserved_f64(ctx):
     n = 32
     case, fields = _tgv_case(n)
@@ -99,18 +116,26 @@ def test_mass_and_momentum_conserved_f64(ctx):
     assert np.abs(r1["momentum"] - r0["momentum"]).max() < 1e-10
 
 
-@pytest.mark.parametrize("storage", ["f64", "f16"])
-def test_taylor_green_decay(ctx, storage):
-    """Kinetic energy follows exp(-6 nu k^2 t) (Stokes limit) within 1%
-    for either pull convention."""
+def test_taylor_green_decay(ctx):
+    """Kinetic energy of the 64^3 TGV follows the Stokes-limit decay
+    exp(-6 nu k^2 t) within 2% after 400 steps (the flow is not in the Stokes
+    limit: Re = u0 / (nu k) = 6, so the nonlinear transfer adds ~1.4%
+    dissipation), identically for either pull convention; FP16 shifted
+    storage reproduces the FP64 decay within 1e-3."""
     n, steps = 64, 400
     nu = 1.0 / 30.0
     k = 2 * np.pi / n
-    for conv in ("reference", "textbook"):
-        case, fields = _tgv_case(n, conv=conv, storage=storage)
-        d = _dense(ctx, case, fields, storage)
-        e0 = d.reduce()["kinetic_energy"]
-        d.step(steps)
-        e1 = d.reduce()["kinetic_energy"]
-        want = np.exp(-6 * nu * k * k * steps)
-        assert abs(e1 / e0 - want) / want < 1e-2, (conv, e1 / e0, want)
+    want = np.exp(-6 * nu * k * k * steps)
+    ratios = {}
+    for storage in ("f64", "f16"):
+        for conv in ("reference", "textbook"):
+            case, fields = _tgv_case(n, conv=conv, storage=storage)
+            d = _dense(ctx, case, fields, storage)
+            e0 = d.reduce()["kinetic_energy"]
+            d.step(steps)
+            ratios[storage, conv] = d.reduce()["kinetic_energy"] / e0
+            d.close()
+    for key, r in ratios.items():
+        assert abs(r - want) / want < 2e-2, (key, r, want)
+    assert abs(ratios["f64", "reference"] - ratios["f64", "textbook"]) < 1e-12
+    assert abs(ratios["f16", "reference"] - ratios["f64", "reference"]) / ratios["f64", "reference"] < 1e-3
