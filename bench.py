@@ -126,13 +126,22 @@ def barrier(world):
 
 
 def max_over_ranks(value, world):
+    """Maximum of a per-rank scalar (the step time) over all ranks; the only
+    collective of the benchmark, outside the timed region."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_mlups(cells_per_rank, steps, secs_per_rank, world):
+    """Whole-job MLUPS of `world` independent replicas timed as the maximum
+    over ranks (weak scaling: every rank steps its own case)."""
+    return world * cells_per_rank * steps / max_over_ranks(secs_per_rank, world) / 1e6
 
 
 def tgv_fields():

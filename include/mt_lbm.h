@@ -142,6 +142,11 @@ int mt_lbm_kernel(mt_ctx *ctx, int32_t case_id, int32_t level);       /* LBM_Man
  * LBMkernel(0) then calculateMacros() on every level, replayed from a CUDA
  * graph; asynchronous on the context stream */
 int mt_step(mt_ctx *ctx, int32_t case_id, int32_t n_coarse_steps);
+/* Health check after a run of steps: scans every population for NaN/Inf
+ * (the reference prints NaN diagnostics each substep, LBM_Simulator.cpp:33-86)
+ * and reports errors the step kernels raised.  MT_OK, MT_ERR_NONFINITE or
+ * MT_ERR_MESH; synchronises the context stream. */
+int mt_case_status(mt_ctx *ctx, int32_t case_id);
 /* Autotuner of the dense path (no reference counterpart): times the fused
  * kernel at 128, 256, 512 and 1024 threads per block on the case's own state
  * (writing only the scratch array, so the state is unchanged) and keeps the

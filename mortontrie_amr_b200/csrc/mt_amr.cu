@@ -958,6 +958,32 @@ int amr_step(Ctx &ctx, Case &c, int n)
     return MT_OK;
 }
 
+// non-finite guard over f and fcol of one level: raises DEVERR_NONFINITE
+// (the reference only prints NaN diagnostics, LBM_Simulator.cpp:33-41)
+__global__ void k_guard(const double *f, const double *fcol, int64_t total, int *err)
+{
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool bad = false;
+    for (; j < total; j += (int64_t)gridDim.x * blockDim.x) bad |= !isfinite(f[j]) || !isfinite(fcol[j]);
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(err, DEVERR_NONFINITE);
+}
+
+int amr_guard(Ctx &ctx, Case &c, int *flags)
+{
+    MT_CUDA(ctx, cudaMemsetAsync(c.dev_err, 0, sizeof(int), ctx.stream));
+    for (int l = 0; l <= c.d.max_level; ++l) {
+        Level &lv = c.lv[l];
+        if (!lv.n) continue;
+        const int64_t total = lv.n * c.d.q;
+        k_guard<<<std::min<int64_t>(grid_for(total, 256), 148 * 16), 256, 0, ctx.stream>>>(lv.f, lv.fcol, total,
+                                                                                          c.dev_err);
+        MT_LAUNCHED(ctx);
+    }
+    MT_CUDA(ctx, cudaMemcpyAsync(flags, c.dev_err, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
 __global__ void k_find(const uint64_t *key, int64_t n, const uint64_t *q, int64_t nq, int64_t *out)
 {
     int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;

@@ -1,0 +1,702 @@
+// Per-phase kernels of the multi-level time step, templated on the
+// population storage type S (mt_store.cuh).  With S = double every
+// expression keeps the reference's operation order and, compiled without
+// FMA contraction (mt_amr_f64.cu), reproduces its results bit-for-bit; the
+// float / half / bfloat16 instantiations (mt_amr_lp.cu) store f - w_q and
+// compute in FP32.
+//
+// Macros are computed inside the collision kernel from the same f the
+// reference's calculateMacros(level) reads just before collide(level)
+// (LBM_Simulator.cpp:26-28), and written out for the solid boundary and the
+// domain boundary that read them later in the substep.
+#pragma once
+
+#include <algorithm>
+
+#include "mt_internal.hpp"
+#include "mt_store.cuh"
+
+namespace mt {
+
+enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
+       PH_BC_FACE0 = 8 };
+
+__constant__ int8_t c_bdry19[26][14];
+__constant__ int8_t c_bdry27[26][18];
+
+template <int Q, class S>
+__global__ void k_init_eq(int64_t n, const uint32_t *tag, double rho0, double ux, double uy, double uz, S *f, S *fcol,
+                          typename Store<S>::C *rho, typename Store<S>::C *u)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = tag[i];
+    const bool solid = (t & TAG_SF) && !(t & (TAG_LATF | TAG_F2C | TAG_C2F | TAG_GC2F | TAG_BC));
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const double v = solid ? 0. : feq_ref<Q>(k, rho0, ux, uy, uz);
+        const C s = (C)(T::shifted ? v - w<Q>(k) : v);
+        T::st(f, k * n + i, s);
+        T::st(fcol, k * n + i, s);
+    }
+    rho[i] = (C)(solid ? 1. : rho0);
+    u[i] = (C)(solid ? 0. : ux);
+    u[n + i] = (C)(solid ? 0. : uy);
+    u[2 * n + i] = (C)(solid ? 0. : uz);
+}
+
+// LBM_Manager::calculateMacros(level), LBM_Manager.cpp:1003-1050
+template <int Q, class S>
+__global__ void k_macros(const int32_t *list, int64_t nl, int64_t n, const S *f, typename Store<S>::C *rho,
+                         typename Store<S>::C *u)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    C d[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::ld(f, k * n + i), k);
+    C r, x, y, z;
+    macros_g<Q, C>(d, r, x, y, z);
+    rho[i] = r;
+    u[i] = x;
+    u[n + i] = y;
+    u[2 * n + i] = z;
+}
+
+// calculateMacros(level) + Collision_LBGK::collide / Collision_Cumulant::collide
+// on lat_f then overlap_F2C (Collision_Manager.cpp:13-53, Collision_Cumulant.cpp:22-159)
+template <int Q, class S, int COLL>
+__global__ void k_collide(const int32_t *list, int64_t nl, int64_t n, double tau, const S *f,
+                          typename Store<S>::C *rho, typename Store<S>::C *u, S *fcol)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    C d[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::ld(f, k * n + i), k);
+    C r, x, y, z;
+    macros_g<Q, C>(d, r, x, y, z);
+    rho[i] = r;
+    u[i] = x;
+    u[n + i] = y;
+    u[2 * n + i] = z;
+    if constexpr (COLL == MT_COLL_LBGK) {
+        if constexpr (!T::shifted) {
+#pragma unroll
+            for (int k = 0; k < Q; ++k) {
+                const double fk = d[k];
+                fcol[k * n + i] = fk - (fk - feq_ref<Q>(k, r, x, y, z)) / tau;
+            }
+        } else {
+            const float om = (float)(1.0 / tau);
+            const float uu = 1.5f * (x * x + y * y + z * z);
+#pragma unroll
+            for (int k = 0; k < Q; ++k) {
+                const float eu = ex(k) * x + ey(k) * y + ez(k) * z;
+                const float wk = (float)w<Q>(k);
+                // deviations: feq - w = w ((rho - 1) + rho (3 eu + 4.5 eu^2 - 1.5 u^2))
+                const float dfeq = wk * ((r - 1.f) + r * (3.f * eu + 4.5f * eu * eu - uu));
+                const float s = d[k] - wk;
+                T::st(fcol, k * n + i, fmaf(om, dfeq - s, s));
+            }
+        }
+    } else if constexpr (Q == 27) {
+        C o[27];
+        cumulant_collide<C>(d, r, x, y, z, (C)(1. / tau), o);
+#pragma unroll
+        for (int k = 0; k < 27; ++k) T::st(fcol, k * n + i, stored_of<S, 27>(o[k], k));
+    }
+}
+
+// fcol = f on overlap_C2F (Collision_Manager.cpp:45-52)
+template <int Q, class S>
+__global__ void k_copy_fcol(const int32_t *list, int64_t nl, int64_t n, const S *f, S *fcol)
+{
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) fcol[k * n + i] = f[k * n + i];
+}
+
+// ABPatternPull::stream (Stream_Manager.cpp:43-76): a missing neighbour keeps f
+template <int Q, class S>
+__global__ void k_stream(const int32_t *list, int64_t nl, int64_t n, int textbook, const int32_t *nbr, const S *fcol,
+                         S *f)
+{
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    f[i] = fcol[i];
+#pragma unroll
+    for (int k = 1; k < Q; ++k) {
+        const int kk = textbook ? inv(k) : k;
+        const int32_t s = nbr[(int64_t)(kk - 1) * n + i];
+        if (s >= 0) f[k * n + i] = fcol[k * n + s];
+    }
+}
+
+// AMR_transDDF_explosion (LBM_Manager.cpp:1059-1129)
+template <int Q, class S>
+__global__ void k_explosion(const int32_t *src, const int32_t *child, int64_t ns, int64_t nc, const S *cfcol,
+                            int64_t nf, S *ffcol, double scale)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    const int64_t i = src[j];
+    C d[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::ld(cfcol, k * nc + i), k);
+    C r, x, y, z;
+    macros_g<Q, C>(d, r, x, y, z);
+    int32_t ch[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) ch[m] = child[(int64_t)m * ns + j];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
+        const C v = stored_of<S, Q>(fe + (C)scale * (d[k] - fe), k);
+#pragma unroll
+        for (int m = 0; m < 8; ++m)
+            if (ch[m] >= 0) T::st(ffcol, k * nf + ch[m], v);
+    }
+}
+
+// AMR_transDDF_coalescence (LBM_Manager.cpp:1131-1169)
+template <int Q, class S>
+__global__ void k_coalescence(const int32_t *list, const int32_t *child, int64_t nl, int64_t nc, S *cf, const S *ff,
+                              int64_t nf, double scale)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    int32_t ch[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) ch[m] = child[(int64_t)m * nl + j];
+    C a[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        C s = 0;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) s += full_of<S, Q>(T::ld(ff, k * nf + ch[m]), k);
+        a[k] = s / (C)8.0;
+    }
+    C r, x, y, z;
+    macros_g<Q, C>(a, r, x, y, z);
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
+        T::st(cf, k * nc + i, stored_of<S, Q>(fe + (C)scale * (a[k] - fe), k));
+    }
+}
+
+// Non-equilibrium extrapolation ("eflow stable" form) on one boundary set:
+// f_k(b) = feq_k(rho_b, u_bc) + f_k(b + e_k) - feq_k(rho_n, u_n) over the
+// reserved directions (NonEquilibrumExtrapolation.cpp:33-71).  Boundary f
+// is read by nothing but this update: a Jacobi sweep (values first, then
+// writes) keeps it deterministic.
+template <int Q, class S>
+__global__ void k_bc_neq(const int32_t *list, int64_t nl, int b, int64_t n, const int32_t *nbr,
+                         const typename Store<S>::C *rho, const typename Store<S>::C *u, S *f, double ubx,
+                         double uby, double ubz, double *tmp, int phase, int *err)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    constexpr int W = Q == 19 ? 14 : 18;
+    for (int t = 0; t < W; ++t) {
+        const int k = Q == 19 ? c_bdry19[b][t] : c_bdry27[b][t];
+        if (k < 0) break;
+        if (phase == 0) {
+            const int32_t nb = k == 0 ? (int32_t)i : nbr[(int64_t)(k - 1) * n + i];
+            if (nb < 0) {
+                atomicOr(err, DEVERR_MISSING_BC_NBR);
+                tmp[t * nl + j] = (double)full_of<S, Q>(T::ld(f, k * n + i), k);
+                continue;
+            }
+            const C fw = feq_g<Q, C>(k, rho[i], (C)ubx, (C)uby, (C)ubz);
+            const C fn = feq_g<Q, C>(k, rho[nb], u[nb], u[n + nb], u[2 * n + nb]);
+            tmp[t * nl + j] = (double)(fw + full_of<S, Q>(T::ld(f, k * n + nb), k) - fn);
+        } else {
+            T::st(f, k * n + i, stored_of<S, Q>((C)tmp[t * nl + j], k));
+        }
+    }
+}
+
+// Restated inlet/outflow on the x faces: West wall cells hold
+// fcol = feq(rho_inner, u_bc), East wall cells copy the inner cell's fcol.
+template <int Q, class S>
+__global__ void k_bc_inout(const int32_t *list, int64_t nl, int east, int64_t n, const int32_t *nbr,
+                           const typename Store<S>::C *rho, S *f, S *fcol, double ubx, double uby, double ubz, int *err)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    const int32_t nb = nbr[(int64_t)((east ? 2 : 1) - 1) * n + i];
+    if (nb < 0) {
+        atomicOr(err, DEVERR_MISSING_BC_NBR);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        if (east) {
+            const S v = fcol[k * n + nb];
+            fcol[k * n + i] = v;
+            f[k * n + i] = v;
+        } else {
+            const C v = stored_of<S, Q>(feq_g<Q, C>(k, rho[nb], (C)ubx, (C)uby, (C)ubz), k);
+            T::st(fcol, k * n + i, v);
+            T::st(f, k * n + i, v);
+        }
+    }
+}
+
+// SinglePointInterpolation::treat (ComplexBoundary_Manager.cpp:43-225):
+// wall links by Filippova-Haenel or distance-weighted interpolation, free
+// links by plain pull, density clamp, eight multi-direct-forcing sweeps
+// (each cell only touches its own populations: the sweeps run in registers).
+template <int Q, int FH, class S>
+__global__ void k_ib_treat(const int32_t *list, int64_t nl, int64_t n, const int32_t *disrow, const double *dis,
+                           const int32_t *nbr, const S *fcol, const typename Store<S>::C *rho, S *f, double *force)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    const double *dr = dis + (int64_t)disrow[i] * (Q - 1);
+    const C rho_b = rho[i];
+    auto FC = [&](int k, int64_t idx) { return full_of<S, Q>(T::ld(fcol, k * n + idx), k); };
+    C g[Q];
+    g[0] = FC(0, i);
+    C fx = 0, fy = 0, fz = 0;
+#pragma unroll
+    for (int k = 1; k < Q; ++k) {
+        const C dd = (C)dr[inv(k) - 1];
+        if (dr[inv(k) - 1] != -1.) {
+            const C finc = FC(inv(k), i);
+            const int32_t si = nbr[(int64_t)(inv(k) - 1) * n + i];
+            const C fstr = si >= 0 ? FC(k, si) : finc;
+            C fnew;
+            if (FH) {
+                if (dd < (C)0.5) {
+                    fnew = ((C)1.0 - (C)2.0 * dd) * finc + (C)2.0 * dd * fstr;
+                } else {
+                    const C feqw = (C)w19z(inv(k)) * rho_b;
+                    const C inv2d = (C)1.0 / ((C)2.0 * dd);
+                    fnew = inv2d * fstr + ((C)1.0 - inv2d) * feqw;
+                }
+            } else {
+                fnew = ((C)1.0 - dd) * finc + dd * fstr;
+            }
+            g[k] = fnew;
+            const C mt = finc + fnew;
+            fx += -mt * ex(k);
+            fy += -mt * ey(k);
+            fz += -mt * ez(k);
+        } else {
+            const int32_t si = nbr[(int64_t)(k - 1) * n + i];
+            g[k] = si < 0 ? FC(inv(k), i) : FC(k, si);
+        }
+    }
+    C ra = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) ra += g[k];
+    if (ra < (C)0.3)
+        g[0] += (C)1.0 * ((C)0.3 - ra);
+    else if (ra < (C)0.5)
+        g[0] += (C)0.5 * ((C)0.5 - ra);
+    else if (ra > (C)3.0)
+        g[0] += (C)1.0 * ((C)3.0 - ra);
+    else if (ra > (C)2.0)
+        g[0] += (C)0.5 * ((C)2.0 - ra);
+    for (int it = 0; it < 8; ++it) {
+        C r = 0, ux = 0, uy = 0, uz = 0;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            r += g[k];
+            ux += g[k] * ex(k);
+            uy += g[k] * ey(k);
+            uz += g[k] * ez(k);
+        }
+        if (r <= (C)0.) continue;
+        ux = ux / r;
+        uy = uy / r;
+        uz = uz / r;
+        const C um = sqrt(ux * ux + uy * uy + uz * uz);
+        if (um < (C)1e-10) continue;
+        const C mx = (C)-0.5 * r * ux, my = (C)-0.5 * r * uy, mz = (C)-0.5 * r * uz;
+        C adj = 0;
+#pragma unroll
+        for (int k = 1; k < Q; ++k) {
+            if (dr[inv(k) - 1] == -1.) continue;
+            const C df = (C)w19z(k) * (C)3.0 * (ex(k) * mx + ey(k) * my + ez(k) * mz);
+            g[k] += df;
+            adj -= df;
+        }
+        g[0] += adj;
+    }
+#pragma unroll
+    for (int k = 0; k < Q; ++k) T::st(f, k * n + i, stored_of<S, Q>(g[k], k));
+    force[j] = (double)fx;
+    force[nl + j] = (double)fy;
+    force[2 * nl + j] = (double)fz;
+}
+
+// fixed-order reduction of the per-cell IB force into the accumulator
+// (LBM_Manager::accumIBForce, one call per treat)
+static __global__ void k_force_reduce(const double *force, int64_t nl, double *acc)
+{
+    __shared__ double s[3][256];
+    const int t = threadIdx.x;
+    double a[3] = {0., 0., 0.};
+    for (int64_t j = t; j < nl; j += blockDim.x)
+        for (int c = 0; c < 3; ++c) a[c] += force[c * nl + j];
+    for (int c = 0; c < 3; ++c) s[c][t] = a[c];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (t < w)
+            for (int c = 0; c < 3; ++c) s[c][t] += s[c][t + w];
+        __syncthreads();
+    }
+    if (t == 0) {
+        for (int c = 0; c < 3; ++c) acc[c] += s[c][0];
+        acc[3] += 1.0;
+    }
+}
+
+static __global__ void k_force_tick(double *acc) { acc[3] += 1.0; }
+
+template <int Q, class S>
+__global__ void k_to_f64(const S *src, double *dst, int64_t n)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) dst[k * n + i] = (double)full_of<S, Q>(Store<S>::ld(src, k * n + i), k);
+}
+template <int Q, class S>
+__global__ void k_from_f64(const double *src, S *dst, int64_t n)
+{
+    using C = typename Store<S>::C;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const double v = src[k * n + i];
+        Store<S>::st(dst, k * n + i, (C)(Store<S>::shifted ? v - w<Q>(k) : v));
+    }
+}
+template <class C>
+__global__ void k_macro_to_f64(const C *src, double *dst, int64_t m)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < m) dst[i] = (double)src[i];
+}
+template <class S>
+__global__ void k_guard(const S *f, const S *fcol, int64_t total, int *err)
+{
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool bad = false;
+    for (; j < total; j += (int64_t)gridDim.x * blockDim.x)
+        bad |= !isfinite((double)Store<S>::ld(f, j)) || !isfinite((double)Store<S>::ld(fcol, j));
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(err, DEVERR_NONFINITE);
+}
+
+// ----------------------------------------------------------------------------
+// host side
+// ----------------------------------------------------------------------------
+template <class S> struct AmrTyped {
+    using C = typename Store<S>::C;
+    static S *f(Level &lv) { return (S *)lv.f; }
+    static S *fcol(Level &lv) { return (S *)lv.fcol; }
+    static C *rho(Level &lv) { return (C *)lv.rho; }
+    static C *u(Level &lv) { return (C *)lv.u; }
+};
+
+inline int upload_bdry_tables(Ctx &ctx)
+{
+    static const int8_t b19[26][14] = {
+        {0, 1, 3, 4, 5, 6, 7, 9, 11, 13, 15, 16, 17, 18}, {0, 2, 3, 4, 5, 6, 8, 10, 12, 14, 15, 16, 17, 18},
+        {0, 1, 2, 3, 5, 6, 7, 10, 11, 12, 13, 14, 15, 17}, {0, 1, 2, 4, 5, 6, 8, 9, 11, 12, 13, 14, 16, 18},
+        {0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 14, 15, 18}, {0, 1, 2, 3, 4, 6, 7, 8, 9, 10, 12, 13, 16, 17},
+        {0, 2, 4, 5, 6, 8, 12, 14, 16, 18, -1, -1, -1, -1}, {0, 1, 4, 5, 6, 9, 11, 13, 16, 18, -1, -1, -1, -1},
+        {0, 1, 3, 5, 6, 7, 11, 13, 15, 17, -1, -1, -1, -1}, {0, 2, 3, 5, 6, 10, 12, 14, 15, 17, -1, -1, -1, -1},
+        {0, 1, 2, 4, 6, 8, 9, 12, 13, 16, -1, -1, -1, -1}, {0, 1, 2, 3, 6, 7, 10, 12, 13, 17, -1, -1, -1, -1},
+        {0, 1, 2, 4, 5, 8, 9, 11, 14, 18, -1, -1, -1, -1}, {0, 1, 2, 3, 5, 7, 10, 11, 14, 15, -1, -1, -1, -1},
+        {0, 2, 3, 4, 6, 8, 10, 12, 16, 17, -1, -1, -1, -1}, {0, 1, 3, 4, 6, 7, 9, 13, 16, 17, -1, -1, -1, -1},
+        {0, 2, 3, 4, 5, 8, 10, 14, 15, 18, -1, -1, -1, -1}, {0, 1, 3, 4, 5, 7, 9, 11, 15, 18, -1, -1, -1, -1},
+        {0, 2, 4, 6, 8, 12, 16, -1, -1, -1, -1, -1, -1, -1}, {0, 1, 4, 6, 9, 13, 16, -1, -1, -1, -1, -1, -1, -1},
+        {0, 1, 3, 6, 7, 13, 17, -1, -1, -1, -1, -1, -1, -1}, {0, 2, 3, 6, 10, 12, 17, -1, -1, -1, -1, -1, -1, -1},
+        {0, 2, 4, 5, 8, 14, 18, -1, -1, -1, -1, -1, -1, -1}, {0, 1, 4, 5, 9, 11, 18, -1, -1, -1, -1, -1, -1, -1},
+        {0, 1, 3, 5, 7, 11, 15, -1, -1, -1, -1, -1, -1, -1}, {0, 2, 3, 5, 10, 14, 15, -1, -1, -1, -1, -1, -1, -1}};
+    static const int8_t b27[26][18] = {
+        {0, 1, 3, 4, 5, 6, 7, 9, 11, 13, 15, 16, 17, 18, 19, 21, 24, 26},
+        {0, 2, 3, 4, 5, 6, 8, 10, 12, 14, 15, 16, 17, 18, 20, 22, 23, 25},
+        {0, 1, 2, 3, 5, 6, 7, 10, 11, 12, 13, 14, 15, 17, 19, 22, 24, 25},
+        {0, 1, 2, 4, 5, 6, 8, 9, 11, 12, 13, 14, 16, 18, 20, 21, 23, 26},
+        {0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 14, 15, 18, 19, 21, 23, 25},
+        {0, 1, 2, 3, 4, 6, 7, 8, 9, 10, 12, 13, 16, 17, 20, 22, 24, 26},
+        {0, 2, 4, 5, 6, 8, 12, 14, 16, 18, 20, 23, -1, -1, -1, -1, -1, -1},
+        {0, 1, 4, 5, 6, 9, 11, 13, 16, 18, 21, 26, -1, -1, -1, -1, -1, -1},
+        {0, 1, 3, 5, 6, 7, 11, 13, 15, 17, 19, 24, -1, -1, -1, -1, -1, -1},
+        {0, 2, 3, 5, 6, 10, 12, 14, 15, 17, 22, 25, -1, -1, -1, -1, -1, -1},
+        {0, 1, 2, 4, 6, 8, 9, 12, 13, 16, 20, 26, -1, -1, -1, -1, -1, -1},
+        {0, 1, 2, 3, 6, 7, 10, 12, 13, 17, 22, 24, -1, -1, -1, -1, -1, -1},
+        {0, 1, 2, 4, 5, 8, 9, 11, 14, 18, 21, 23, -1, -1, -1, -1, -1, -1},
+        {0, 1, 2, 3, 5, 7, 10, 11, 14, 15, 19, 25, -1, -1, -1, -1, -1, -1},
+        {0, 2, 3, 4, 6, 8, 10, 12, 16, 17, 20, 22, -1, -1, -1, -1, -1, -1},
+        {0, 1, 3, 4, 6, 7, 9, 13, 16, 17, 24, 26, -1, -1, -1, -1, -1, -1},
+        {0, 2, 3, 4, 5, 8, 10, 14, 15, 18, 23, 25, -1, -1, -1, -1, -1, -1},
+        {0, 1, 3, 4, 5, 7, 9, 11, 15, 18, 19, 21, -1, -1, -1, -1, -1, -1},
+        {0, 2, 4, 6, 8, 12, 16, 20, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1},
+        {0, 1, 4, 6, 9, 13, 16, 26, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1},
+        {0, 1, 3, 6, 7, 13, 17, 24, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1},
+        {0, 2, 3, 6, 10, 12, 17, 22, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1},
+        {0, 2, 4, 5, 8, 14, 18, 23, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1},
+        {0, 1, 4, 5, 9, 11, 18, 21, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1},
+        {0, 1, 3, 5, 7, 11, 15, 19, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1},
+        {0, 2, 3, 5, 10, 14, 15, 25, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1}};
+    MT_CUDA(ctx, cudaMemcpyToSymbol(c_bdry19, b19, sizeof(b19)));
+    MT_CUDA(ctx, cudaMemcpyToSymbol(c_bdry27, b27, sizeof(b27)));
+    return MT_OK;
+}
+
+template <class S, int Q>
+int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
+{
+    using A = AmrTyped<S>;
+    const int B = 128;
+    cudaStream_t s = ctx.stream;
+    Level &lv = c.lv[l];
+    const int64_t n = lv.n;
+    switch (phase) {
+    case PH_MACROS:
+        if (lv.ncollide) {
+            k_macros<Q, S><<<grid_for(lv.ncollide, B), B, 0, s>>>(lv.collide_list, lv.ncollide, n, A::f(lv),
+                                                                   A::rho(lv), A::u(lv));
+            MT_LAUNCHED(ctx);
+        }
+        return MT_OK;
+    case PH_COLLIDE:
+        if (lv.ncollide) {
+            if (c.d.collision == MT_COLL_LBGK) {
+                k_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.ncollide, B), B, 0, s>>>(
+                    lv.collide_list, lv.ncollide, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv));
+            } else {
+                // the cumulant model exists for D3Q27 only (checked at case creation)
+                if constexpr (Q == 27)
+                    k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.ncollide, 64), 64, 0, s>>>(
+                        lv.collide_list, lv.ncollide, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv));
+            }
+            MT_LAUNCHED(ctx);
+        }
+        if (lv.nlist[2]) {
+            k_copy_fcol<Q, S><<<grid_for(lv.nlist[2], B), B, 0, s>>>(lv.list[2], lv.nlist[2], n, A::f(lv),
+                                                                      A::fcol(lv));
+            MT_LAUNCHED(ctx);
+        }
+        return MT_OK;
+    case PH_STREAM:
+        if (lv.nstream) {
+            k_stream<Q, S><<<grid_for(lv.nstream, B), B, 0, s>>>(lv.stream_list, lv.nstream, n, c.d.stream_convention,
+                                                                  lv.nbr, A::fcol(lv), A::f(lv));
+            MT_LAUNCHED(ctx);
+        }
+        return MT_OK;
+    case PH_EXPLOSION: {
+        if (l < 1 || !lv.nexpl) return MT_OK;
+        Level &cl = c.lv[l - 1];
+        const double scale = (2.0 * c.d.tau[l]) / c.d.tau[l - 1];
+        k_explosion<Q, S><<<grid_for(lv.nexpl, B), B, 0, s>>>(lv.expl_src, lv.expl_child, lv.nexpl, cl.n, A::fcol(cl),
+                                                               n, A::fcol(lv), scale);
+        MT_LAUNCHED(ctx);
+        return MT_OK;
+    }
+    case PH_COALESCENCE: {
+        if (l >= c.d.max_level || !lv.nlist[1]) return MT_OK;
+        Level &fl = c.lv[l + 1];
+        const double scale = c.d.tau[l] / (2.0 * c.d.tau[l + 1]);
+        k_coalescence<Q, S><<<grid_for(lv.nlist[1], B), B, 0, s>>>(lv.list[1], lv.coal_child, lv.nlist[1], n,
+                                                                    A::f(lv), A::f(fl), fl.n, scale);
+        MT_LAUNCHED(ctx);
+        return MT_OK;
+    }
+    case PH_BC:
+    case PH_BC_FACE0 + 0: case PH_BC_FACE0 + 1: case PH_BC_FACE0 + 2:
+    case PH_BC_FACE0 + 3: case PH_BC_FACE0 + 4: case PH_BC_FACE0 + 5: {
+        // all six face groups in the reference's order (LBM_Simulator.cpp:90-95), or one
+        const int f0 = phase == PH_BC ? 0 : phase - PH_BC_FACE0, f1 = phase == PH_BC ? 6 : f0 + 1;
+        Level &l0 = c.lv[0];
+        static const int face_sets[6][9] = {
+            {0, 7, 8, 15, 17, 19, 20, 23, 24}, {1, 6, 9, 14, 16, 18, 21, 22, 25},
+            {2, 11, 13, -1, -1, -1, -1, -1, -1}, {3, 10, 12, -1, -1, -1, -1, -1, -1},
+            {4, -1, -1, -1, -1, -1, -1, -1, -1}, {5, -1, -1, -1, -1, -1, -1, -1, -1}};
+        double *tmp = c.bc_tmp;
+        if (!tmp) return MT_OK;
+        for (int face = f0; face < f1; ++face)
+            for (int g = 0; g < 9; ++g) {
+                const int b = face_sets[face][g];
+                if (b < 0) break;
+                if (!l0.nbc[b]) continue;
+                for (int ph = 0; ph < 2; ++ph) {
+                    k_bc_neq<Q, S><<<grid_for(l0.nbc[b], B), B, 0, s>>>(l0.bclist[b], l0.nbc[b], b, l0.n, l0.nbr,
+                                                                         A::rho(l0), A::u(l0), A::f(l0), c.d.u_bc[0],
+                                                                         c.d.u_bc[1], c.d.u_bc[2], tmp, ph, c.dev_err);
+                    MT_LAUNCHED(ctx);
+                }
+            }
+        return MT_OK;
+    }
+    case PH_BC_INOUT: {
+        Level &l0 = c.lv[0];
+        for (int face = 0; face < 2; ++face) {
+            if (!l0.nbc[face]) continue;
+            k_bc_inout<Q, S><<<grid_for(l0.nbc[face], B), B, 0, s>>>(l0.bclist[face], l0.nbc[face], face, l0.n, l0.nbr,
+                                                                      A::rho(l0), A::f(l0), A::fcol(l0), c.d.u_bc[0],
+                                                                      c.d.u_bc[1], c.d.u_bc[2], c.dev_err);
+            MT_LAUNCHED(ctx);
+        }
+        return MT_OK;
+    }
+    case PH_IB: {
+        Level &fl = c.lv[c.d.max_level];
+        if (!fl.nib) {
+            k_force_tick<<<1, 1, 0, s>>>(c.force_acc);
+            MT_LAUNCHED(ctx);
+            return MT_OK;
+        }
+        if (c.d.ib_method == MT_IB_FH)
+            k_ib_treat<Q, 1, S><<<grid_for(fl.nib, 64), 64, 0, s>>>(fl.iblist, fl.nib, fl.n, fl.disrow, c.dis, fl.nbr,
+                                                                     A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force);
+        else
+            k_ib_treat<Q, 0, S><<<grid_for(fl.nib, 64), 64, 0, s>>>(fl.iblist, fl.nib, fl.n, fl.disrow, c.dis, fl.nbr,
+                                                                     A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force);
+        MT_LAUNCHED(ctx);
+        k_force_reduce<<<1, 256, 0, s>>>(c.ib_force, fl.nib, c.force_acc);
+        MT_LAUNCHED(ctx);
+        return MT_OK;
+    }
+    }
+    return set_err(ctx, MT_ERR_ARG, "unknown phase");
+}
+
+template <class S>
+int AmrOps<S>::phase(Ctx &ctx, Case &c, int phase, int level)
+{
+    return c.d.q == 19 ? amr_phase_q<S, 19>(ctx, c, phase, level) : amr_phase_q<S, 27>(ctx, c, phase, level);
+}
+
+template <class S>
+int AmrOps<S>::upload_tables(Ctx &ctx)
+{
+    return upload_bdry_tables(ctx);
+}
+
+template <class S>
+int AmrOps<S>::alloc(Ctx &ctx, Case &c, int l)
+{
+    using C = typename Store<S>::C;
+    Level &lv = c.lv[l];
+    const int64_t n = lv.n, Q = c.d.q;
+    MT_CUDA(ctx, cudaMallocAsync(&lv.f, sizeof(S) * n * Q, ctx.stream));
+    MT_CUDA(ctx, cudaMallocAsync(&lv.fcol, sizeof(S) * n * Q, ctx.stream));
+    MT_CUDA(ctx, cudaMallocAsync(&lv.rho, sizeof(C) * n, ctx.stream));
+    MT_CUDA(ctx, cudaMallocAsync(&lv.u, sizeof(C) * 3 * n, ctx.stream));
+    MT_CUDA(ctx, cudaMemsetAsync(lv.f, 0, sizeof(S) * n * Q, ctx.stream));
+    MT_CUDA(ctx, cudaMemsetAsync(lv.fcol, 0, sizeof(S) * n * Q, ctx.stream));
+    MT_CUDA(ctx, cudaMemsetAsync(lv.rho, 0, sizeof(C) * n, ctx.stream));
+    MT_CUDA(ctx, cudaMemsetAsync(lv.u, 0, sizeof(C) * 3 * n, ctx.stream));
+    return MT_OK;
+}
+
+template <class S>
+int AmrOps<S>::init_eq(Ctx &ctx, Case &c, double rho0, const double *u0)
+{
+    using A = AmrTyped<S>;
+    for (int l = 0; l <= c.d.max_level; ++l) {
+        Level &lv = c.lv[l];
+        if (!lv.n) continue;
+        if (c.d.q == 19)
+            k_init_eq<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(lv.n, lv.tag, rho0, u0[0], u0[1], u0[2],
+                                                                           A::f(lv), A::fcol(lv), A::rho(lv), A::u(lv));
+        else
+            k_init_eq<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(lv.n, lv.tag, rho0, u0[0], u0[1], u0[2],
+                                                                           A::f(lv), A::fcol(lv), A::rho(lv), A::u(lv));
+        MT_LAUNCHED(ctx);
+    }
+    return MT_OK;
+}
+
+template <class S>
+int AmrOps<S>::get(Ctx &ctx, Case &c, int l, int which, double *d_out)
+{
+    Level &lv = c.lv[l];
+    const S *src = (const S *)(which == 0 ? lv.f : lv.fcol);
+    if (!lv.n) return MT_OK;
+    if (c.d.q == 19)
+        k_to_f64<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(src, d_out, lv.n);
+    else
+        k_to_f64<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(src, d_out, lv.n);
+    MT_LAUNCHED(ctx);
+    return MT_OK;
+}
+
+template <class S>
+int AmrOps<S>::set(Ctx &ctx, Case &c, int l, int which, const double *d_in)
+{
+    Level &lv = c.lv[l];
+    S *dst = (S *)(which == 0 ? lv.f : lv.fcol);
+    if (!lv.n) return MT_OK;
+    if (c.d.q == 19)
+        k_from_f64<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(d_in, dst, lv.n);
+    else
+        k_from_f64<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(d_in, dst, lv.n);
+    MT_LAUNCHED(ctx);
+    return MT_OK;
+}
+
+template <class S>
+int AmrOps<S>::macros_out(Ctx &ctx, Case &c, int l, double *d_rho, double *d_u)
+{
+    using C = typename Store<S>::C;
+    Level &lv = c.lv[l];
+    if (!lv.n) return MT_OK;
+    k_macro_to_f64<C><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>((const C *)lv.rho, d_rho, lv.n);
+    MT_LAUNCHED(ctx);
+    k_macro_to_f64<C><<<grid_for(3 * lv.n, 256), 256, 0, ctx.stream>>>((const C *)lv.u, d_u, 3 * lv.n);
+    MT_LAUNCHED(ctx);
+    return MT_OK;
+}
+
+template <class S>
+int AmrOps<S>::guard(Ctx &ctx, Case &c)
+{
+    for (int l = 0; l <= c.d.max_level; ++l) {
+        Level &lv = c.lv[l];
+        if (!lv.n) continue;
+        const int64_t total = lv.n * c.d.q;
+        k_guard<S><<<(unsigned)std::min<int64_t>(grid_for(total, 256), 148 * 16), 256, 0, ctx.stream>>>(
+            (const S *)lv.f, (const S *)lv.fcol, total, c.dev_err);
+        MT_LAUNCHED(ctx);
+    }
+    return MT_OK;
+}
+
+}  // namespace mt

@@ -572,6 +572,30 @@ int mt_step(mt_ctx *h, int32_t id, int32_t n)
     return MT_OK;
 }
 
+int mt_case_status(mt_ctx *h, int32_t id)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+    if (c->dense) {
+        double r[5];
+        rc = mt_case_reduce(h, id, r);
+        if (rc) return rc;
+        for (double v : r)
+            if (!std::isfinite(v)) return set_err(ctx, MT_ERR_NONFINITE, "non-finite population in the dense state");
+        return MT_OK;
+    }
+    int flags = 0;
+    rc = amr_guard(ctx, *c, &flags);
+    if (rc) return rc;
+    if (flags & DEVERR_NONFINITE) return set_err(ctx, MT_ERR_NONFINITE, "non-finite population found by the guard");
+    if (flags & DEVERR_MISSING_BC_NBR)
+        return set_err(ctx, MT_ERR_MESH, "a boundary cell's reserved neighbour is not stored");
+    return MT_OK;
+}
+
 int mt_case_tune(mt_ctx *h, int32_t id, int32_t *best_block, float *ms_per_candidate)
 {
     Case *c;

@@ -215,6 +215,90 @@ __global__ void __launch_bounds__(1024) k_dense(const S *__restrict__ A, S *__re
     for (int k = 0; k < Q; ++k) T::st(B, (IDX)k * N + (IDX)i, f[k]);
 }
 
+// Two x-adjacent cells per thread for 16-bit storage.  Cells i0 = 2p and
+// i0 + 1 differ only in x bit 0, which is index bit 0, so their populations
+// of one direction form an aligned 32-bit pair.  For e_x = 0 the two pull
+// sources are again an aligned pair (one load); for e_x = +-1 they straddle
+// two pairs (x0 + 1, x0 + 2 or x0 - 1, x0): two aligned loads and a byte
+// permute.  Stores and conversions are per pair.
+template <class S> struct Pair16;
+template <> struct Pair16<__half> {
+    using P = __half2;
+    __device__ static __forceinline__ float2 to_f2(P v) { return __half22float2(v); }
+    __device__ static __forceinline__ P from_f2(float2 v) { return __float22half2_rn(v); }
+};
+template <> struct Pair16<__nv_bfloat16> {
+    using P = __nv_bfloat162;
+    __device__ static __forceinline__ float2 to_f2(P v) { return __bfloat1622float2(v); }
+    __device__ static __forceinline__ P from_f2(float2 v) { return __float22bfloat162_rn(v); }
+};
+
+__device__ __forceinline__ uint32_t hi_lo(uint32_t a, uint32_t b) { return __byte_perm(a, b, 0x5432); }
+
+template <int Q, class S, int CONV>
+__global__ void __launch_bounds__(256) k_dense_pair(const S *__restrict__ A, S *__restrict__ B, uint32_t N,
+                                                   DenseGeom g, double tau)
+{
+    using P = typename Pair16<S>::P;
+    const uint32_t pidx = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i0 = pidx << 1;
+    if (i0 >= N) return;
+    // dilated parts: x at offsets -2, 0, +2 (pair aligned), y and z at -1, 0, +1
+    uint32_t px[3], py[3], pz[3];
+    {
+        const uint32_t mx = g.m[0], lx2 = g.lo[0] << 3;  // x bit 1 sits at index bit 3
+        const uint32_t c = i0 & mx;
+        px[1] = c;
+        px[2] = ((i0 | ~mx) + lx2) & mx;
+        px[0] = (c - lx2) & mx;
+        const uint32_t my = g.m[1], ly = g.lo[1], cy = i0 & my;
+        py[1] = cy;
+        py[2] = ((i0 | ~my) + ly) & my;
+        py[0] = (cy - ly) & my;
+        const uint32_t mz = g.m[2], lz = g.lo[2], cz = i0 & mz;
+        pz[1] = cz;
+        pz[2] = ((i0 | ~mz) + lz) & mz;
+        pz[0] = (cz - lz) & mz;
+    }
+    constexpr int sg = CONV ? -1 : 1;
+    float fa[Q], fb[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const int dx = sg * ex(k), dy = sg * ey(k), dz = sg * ez(k);
+        const uint32_t yz = py[1 + dy] | pz[1 + dz];
+        const S *base = A + (size_t)k * N;
+        uint32_t v;
+        if (dx == 0) {
+            v = __ldg((const unsigned int *)(base + (px[1] | yz)));
+        } else if (dx > 0) {
+            // (x0 + 1, x0 + 2): high half of pair x0, low half of pair x0 + 2
+            const uint32_t a = __ldg((const unsigned int *)(base + (px[1] | yz)));
+            const uint32_t b = __ldg((const unsigned int *)(base + (px[2] | yz)));
+            v = hi_lo(a, b);
+        } else {
+            // (x0 - 1, x0): high half of pair x0 - 2, low half of pair x0
+            const uint32_t a = __ldg((const unsigned int *)(base + (px[0] | yz)));
+            const uint32_t b = __ldg((const unsigned int *)(base + (px[1] | yz)));
+            v = hi_lo(a, b);
+        }
+        P pv;
+        memcpy(&pv, &v, 4);
+        const float2 f2 = Pair16<S>::to_f2(pv);
+        fa[k] = f2.x;
+        fb[k] = f2.y;
+    }
+    const float om = (float)(1.0 / tau);
+    lbgk_dev_pairs<Q>(fa, om);
+    lbgk_dev_pairs<Q>(fb, om);
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const P pv = Pair16<S>::from_f2(make_float2(fa[k], fb[k]));
+        uint32_t v;
+        memcpy(&v, &pv, 4);
+        *(unsigned int *)(B + (size_t)k * N + i0) = v;
+    }
+}
+
 // populations from host doubles -> storage (shift applied), or equilibrium of fields
 template <int Q, class S>
 __global__ void k_dense_from_f64(const double *src, S *A, int64_t N)
@@ -369,6 +453,27 @@ int DenseOps<S>::step(Ctx &ctx, Case &c, int mode)
     S *Bp = (S *)c.B;
     const int tb = c.d.stream_convention;
     const double tau = c.d.tau[0];
+    if constexpr (std::is_same<S, __half>::value || std::is_same<S, __nv_bfloat16>::value) {
+        // 16-bit storage, LBGK: two cells per thread with paired accesses
+        if (mode == DM_FUSED && c.d.collision == MT_COLL_LBGK && (uint64_t)c.d.q * c.N < (1ull << 32)) {
+            const unsigned pgrid = grid_for(c.N / 2, B);
+            const uint32_t n32 = (uint32_t)c.N;
+            if (c.d.q == 19) {
+                if (tb)
+                    k_dense_pair<19, S, 1><<<pgrid, B, 0, ctx.stream>>>(A, Bp, n32, g, tau);
+                else
+                    k_dense_pair<19, S, 0><<<pgrid, B, 0, ctx.stream>>>(A, Bp, n32, g, tau);
+            } else {
+                if (tb)
+                    k_dense_pair<27, S, 1><<<pgrid, B, 0, ctx.stream>>>(A, Bp, n32, g, tau);
+                else
+                    k_dense_pair<27, S, 0><<<pgrid, B, 0, ctx.stream>>>(A, Bp, n32, g, tau);
+            }
+            MT_LAUNCHED(ctx);
+            std::swap(c.A, c.B);
+            return MT_OK;
+        }
+    }
     const bool idx32 = (uint64_t)c.d.q * (uint64_t)c.N < (1ull << 32);
 #define MT_DENSE_LAUNCH_I(QQ, CC, IDX)                                                                     \
     do {                                                                                                   \
@@ -481,7 +586,10 @@ template <class S>
 int DenseOps<S>::tune(Ctx &ctx, Case &c, float *ms_out, int *blocks_out, int *n_out)
 {
     static const int cand[] = {128, 256, 512, 1024};
-    const int nc = (int)(sizeof(cand) / sizeof(cand[0]));
+    // the paired 16-bit kernel is built for at most 256 threads per block
+    const bool pair16 = (std::is_same<S, __half>::value || std::is_same<S, __nv_bfloat16>::value) &&
+                        c.d.collision == MT_COLL_LBGK;
+    const int nc = pair16 ? 2 : (int)(sizeof(cand) / sizeof(cand[0]));
     cudaEvent_t e0, e1;
     MT_CUDA(ctx, cudaEventCreate(&e0));
     MT_CUDA(ctx, cudaEventCreate(&e1));

@@ -102,6 +102,7 @@ int amr_lbm_kernel(Ctx &ctx, Case &c, int level);
 int amr_step(Ctx &ctx, Case &c, int n);
 int amr_phase(Ctx &ctx, Case &c, int phase, int level);
 int amr_find(Ctx &ctx, Case &c, int level, const uint64_t *h_keys, int64_t n, int64_t *h_idx);
+int amr_guard(Ctx &ctx, Case &c, int *flags);
 void amr_free(Case &c);
 
 // dense uniform path, one explicit instantiation per storage type

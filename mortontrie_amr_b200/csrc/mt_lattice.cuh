@@ -174,6 +174,38 @@ template <int Q> MT_HD double feq_heluo_ref(int i, double rho, double ux, double
 
 MT_HD double safe_irho_ref(double r) { return 1.0 / ((r > -1e-6 && r < 1e-6) ? ((r < 0.0) ? -1e-6 : 1e-6) : r); }
 
+// The same three functions for any real type R: with R = double they are
+// the reference-order versions above, with R = float the reduced-precision
+// path's arithmetic.
+template <int Q, class R> MT_HD void macros_g(const R *d, R &rho, R &ux, R &uy, R &uz)
+{
+    R r = d[0], vx = 0, vy = 0, vz = 0;
+#pragma unroll
+    for (int i = 1; i < Q; ++i) {
+        r += d[i];
+        vx += d[i] * ex(i);
+        vy += d[i] * ey(i);
+        vz += d[i] * ez(i);
+    }
+    const R s = (r > R(-1e-6) && r < R(1e-6)) ? ((r < R(0)) ? R(-1e-6) : R(1e-6)) : r;
+    rho = r;
+    ux = vx / s;
+    uy = vy / s;
+    uz = vz / s;
+}
+template <int Q, class R> MT_HD R feq_g(int i, R rho, R ux, R uy, R uz)
+{
+    const R uu = ux * ux + uy * uy + uz * uz;
+    const R euv = ex(i) * ux + ey(i) * uy + ez(i) * uz;
+    return rho * (R)w<Q>(i) * (R(1) + R(3) * euv + R(4.5) * euv * euv - R(1.5) * uu);
+}
+template <int Q, class R> MT_HD R feq_heluo_g(int i, R rho, R ux, R uy, R uz)
+{
+    const R uu = ux * ux + uy * uy + uz * uz;
+    const R euv = ex(i) * ux + ey(i) * uy + ez(i) * uz;
+    return (R)w<Q>(i) * (rho + R(1) * (R(3) * euv + R(4.5) * euv * euv - R(1.5) * uu));
+}
+
 template <class R>
 MT_HD void chim_back(R a0, R a1, R a2, R v, R v2, R &pn, R &pz, R &pp)
 {

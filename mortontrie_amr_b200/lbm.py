@@ -31,7 +31,7 @@ EXPORTS = [
     "mt_case_init_equilibrium", "mt_case_init_fields", "mt_case_set_populations", "mt_case_get_populations",
     "mt_case_get_macros", "mt_case_reduce", "mt_calculate_macros", "mt_collide", "mt_stream", "mt_explosion",
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
-    "mt_reset_force", "mt_case_tune",
+    "mt_reset_force", "mt_case_tune", "mt_case_status",
 ]
 
 
@@ -73,7 +73,7 @@ def lib():
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
-            "mt_case_tune": [vp, i32, i32p, C.POINTER(C.c_float)],
+            "mt_case_tune": [vp, i32, i32p, C.POINTER(C.c_float)], "mt_case_status": [vp, i32],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -288,6 +288,11 @@ class LBM_Manager:
 
     def reset_force(self):
         self.ctx.check(lib().mt_reset_force(self.ctx.h, self.id), "reset_force")
+
+    def status(self):
+        """Raise MTError (MT_ERR_NONFINITE / MT_ERR_MESH) if the device
+        guard finds a problem; returns None when healthy."""
+        self.ctx.check(lib().mt_case_status(self.ctx.h, self.id), "mt_case_status")
 
 
 class DenseCase:

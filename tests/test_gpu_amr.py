@@ -118,6 +118,26 @@ def test_cfg1_full_size_matches_oracle(ctx):
     assert rel_err(mgr.force()[:3], oc.force()[:3]) < 1e-12
 
 
+def test_nonfinite_guard(ctx):
+    """A NaN planted on the host in one population propagates through the
+    steps; the device guard reports it as MT_ERR_NONFINITE and the context
+    stays usable."""
+    from mortontrie_amr_b200.lbm import MTError
+    case = _cfg1_small()
+    mgr = _device_case(ctx, case, None)
+    mgr.fluidSimulate(2)
+    assert mgr.status() is None
+    f, fcol = mgr.populations(1)
+    f[3, 100] = np.nan
+    mgr.set_populations(1, f, fcol)
+    mgr.fluidSimulate(1)
+    with pytest.raises(MTError, match="MT_ERR_NONFINITE"):
+        mgr.status()
+    healthy = _device_case(ctx, case, None)
+    healthy.fluidSimulate(1)
+    assert healthy.status() is None
+
+
 def test_missing_child_is_reported(ctx):
     """A contract violation (a coarse F2C cell whose children are not stored)
     returns MT_ERR_MESH instead of faulting, like the reference's .at()

@@ -88,6 +88,26 @@ def test_reduced_precision_vs_f64(ctx, storage):
     assert abs(m_lp - m_ref) / m_ref < (1e-6 if storage == "f32" else 1e-3)
 
 
+@pytest.mark.parametrize("storage,q", [("f16", 19), ("bf16", 19), ("f16", 27), ("f32", 19)])
+def test_reduced_precision_few_steps_close_to_f64(ctx, storage, q):
+    """Three steps of the paired 16-bit kernel (and the FP32 kernel) against
+    FP64: deviations agree to the storage's rounding (FP16 ~1e-3, BF16 ~1e-2
+    of the largest non-equilibrium deviation; FP32 ~1e-6)."""
+    n = 32
+    case, fields = _tgv_case(n, q=q)
+    ref = _dense(ctx, case, fields, "f64")
+    lp = _dense(ctx, case, fields, storage)
+    ref.step(3)
+    lp.step(3)
+    ctx.synchronize()
+    fr, _ = ref.populations()
+    fl, _ = lp.populations()
+    from mortontrie_amr_b200.lattice import weights
+    dev = fr - weights(q)[:, None]
+    err = np.abs(fl - fr).max() / np.abs(dev).max()
+    assert err < {"f16": 2e-3, "bf16": 2e-2, "f32": 2e-6}[storage], err
+
+
 def test_tuner_leaves_state_unchanged(ctx):
     """mt_case_tune times the fused kernel into the scratch array only: the
     trajectory with tuning in the middle equals the one without."""
