@@ -260,7 +260,14 @@ def run_ours(args):
            "h2d_bytes_per_solve": h2d, "d2h_bytes_per_solve": d2h, "steps_per_solve": args.steps,
            "wall_s": round(wall, 4),
            "path": "mt_case_init_fields (pinned FP64 rho,u) -> mt_step x K -> mt_case_get_macros (pinned)"}
-    del d
+    d.close()
+
+    amr = None
+    if not args.no_amr:
+        try:
+            amr = amr_section(ctx, torch)
+        except Exception as exc:  # reported, not hidden: the line says why the section is missing
+            amr = {"error": repr(exc)}
 
     if rank == 0:
         cpu = cpu_baseline_sample() if (world == 1 and not args.no_cpu_baseline) else None
@@ -282,12 +289,63 @@ def run_ours(args):
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
             "diagnostics": {"mass": red["mass"], "kinetic_energy": red["kinetic_energy"]},
             "cpu_baseline": cpu,
+            "amr_cumulant_sphere": amr,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def amr_section(ctx, torch, steps=10, warmup=2):
+    """4-level D3Q27 cumulant sphere (192x96x96 coarse, R = 6 coarse = 48
+    finest cells, Re 200, u 0.04, nested boxes 4R / 2.5R / 1.75R): coarse
+    steps of the multi-level path in the reference's FP64 and with FP32 / FP16
+    storage.  Fine-level MLUPS = finest stepped cells x 2^L per coarse step;
+    total MLUPS sums every level's substeps.  Accuracy of the reduced storage
+    is stated against the FP64 run after the same steps."""
+    from mortontrie_amr_b200.case import nested_sphere_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    case = nested_sphere_case()
+    m = case.mesh
+    L = m.spec.max_level
+    stepped = [int(m.levels[l]["lat_f"].size + m.levels[l]["overlap_C2F"].size) for l in range(L + 1)]
+    per_coarse_total = sum(n << l for l, n in enumerate(stepped))
+    per_coarse_fine = stepped[L] << L
+    out = {"workload": "4-level D3Q27 cumulant sphere 192x96x96, R=6 (48 finest), Re=200, u=0.04",
+           "stepped_cells_per_level": stepped, "coarse_steps": steps}
+    stream = torch.cuda.current_stream()
+    res = {}
+    for st in ("f64", "f32", "f16"):
+        mgr = LBM_Manager(ctx, case, st)
+        mgr.fluidSimulate(warmup)
+        torch.cuda.synchronize()
+        mgr.reset_force()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        mgr.fluidSimulate(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        secs = e0.elapsed_time(e1) / 1e3
+        rho, u = mgr.macros(L)
+        keys, tags = mgr.keys(L)
+        fluid = (tags & 1) != 0
+        f = mgr.force()
+        res[st] = dict(secs=secs, u=u[:, fluid], rho=rho[fluid], fx=f[0] / max(f[3], 1.0))
+        out[st] = {"fine_mlups": round(per_coarse_fine * steps / secs / 1e6, 1),
+                   "total_mlups": round(per_coarse_total * steps / secs / 1e6, 1),
+                   "ms_per_coarse_step": round(1e3 * secs / steps, 3)}
+        mgr.close()
+    ref = res["f64"]
+    for st in ("f32", "f16"):
+        r = res[st]
+        out[st]["velocity_l2_vs_f64"] = float(np.linalg.norm(r["u"] - ref["u"]) / np.linalg.norm(ref["u"]))
+        out[st]["drag_rel_vs_f64"] = float(abs(r["fx"] - ref["fx"]) / max(abs(ref["fx"]), 1e-300))
+        out[st]["mass_drift_vs_f64"] = float(abs(r["rho"].sum() - ref["rho"].sum()) / ref["rho"].sum())
+        out[st]["speedup_vs_f64"] = round(res["f64"]["secs"] / r["secs"], 3)
+    return out
 
 
 def _reference_sample_case():
@@ -369,6 +427,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-amr", action="store_true", help="skip the 4-level cumulant sphere section")
+    ap.add_argument("--amr-only", action="store_true",
+                    help="only the 4-level cumulant sphere section (K coarse steps per storage; profiling runs)")
     ap.add_argument("--edge", type=int, default=256, help="cube edge (power of two); 256 is the configuration")
     ap.add_argument("--quick", action="store_true", help="headline kernel only (profiling runs)")
     args = ap.parse_args()
@@ -378,6 +439,16 @@ def main():
     N_EDGE = args.edge
     if args.impl == "reference":
         run_reference(args)
+    elif args.amr_only:
+        import torch
+
+        from mortontrie_amr_b200.lbm import Context
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx = Context(0)
+        ctx.set_stream(stream.cuda_stream)
+        print(json.dumps({"amr_cumulant_sphere": amr_section(ctx, torch, steps=args.steps, warmup=1)}), flush=True)
+        ctx.close()
     else:
         run_ours(args)
 

@@ -22,7 +22,9 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", 
                  "--expt-relaxed-constexpr"]
 SOURCES = {
     "mt_capi.cu": [],
-    "mt_amr.cu": ["--fmad=false"],
+    "mt_amr.cu": [],
+    "mt_amr_f64.cu": ["--fmad=false"],
+    "mt_amr_lp.cu": [],
     "mt_dense_f64.cu": ["--fmad=false"],
     "mt_dense_lp.cu": [],
 }

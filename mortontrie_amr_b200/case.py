@@ -73,6 +73,24 @@ def sphere_case(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1, refine
     return Case(build_mesh(spec), p)
 
 
+def nested_sphere_case(q=27, collision="Cumulant", coarse=(192, 96, 96), max_level=3, center=(64, 48, 48),
+                       radius=6.0, half_widths=(4.0, 2.5, 1.75), u=0.04, re=200.0,
+                       boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow", ib_method="FH") -> Case:
+    """Flow past a sphere refined in nested boxes centred on it: the box
+    refined from level l to l+1 has half-width half_widths[l] * radius in
+    coarse units (the defaults are the 4-level D3Q27 cumulant sphere case:
+    192x96x96 coarse cells, R = 6 coarse = 48 finest cells, Re 200,
+    inlet u 0.04, outflow, periodic lateral sides)."""
+    refine = []
+    for l in range(max_level):
+        s = 1 << l
+        hw = int(round(half_widths[l] * radius * s))
+        c = [int(round(ci * s)) for ci in center]
+        refine.append((tuple(ci - hw for ci in c), tuple(ci + hw for ci in c)))
+    return sphere_case(q=q, collision=collision, coarse=coarse, max_level=max_level, refine=refine, center=center,
+                       radius=radius, u=u, re=re, boundary=boundary, bc_mode=bc_mode, ib_method=ib_method)
+
+
 def uniform_box_case(q=19, n=(16, 16, 16), nu=1.0 / 30.0, boundary=("periodic",) * 3, collision="LBGK",
                      u_ref=0.02, storage="f64", stream_convention="reference", empty_levels=0,
                      u_bc=(0.0, 0.0, 0.0)) -> Case:

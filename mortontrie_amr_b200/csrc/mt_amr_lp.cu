@@ -1,0 +1,9 @@
+// Reduced-precision instantiations of the multi-level phases: FP32
+// arithmetic on populations stored as f - w_q in FP32, FP16 or BF16.
+#include "mt_amr_phases.cuh"
+
+namespace mt {
+template struct AmrOps<float>;
+template struct AmrOps<__half>;
+template struct AmrOps<__nv_bfloat16>;
+}

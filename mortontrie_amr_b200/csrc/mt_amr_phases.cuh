@@ -21,8 +21,10 @@ namespace mt {
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
        PH_BC_FACE0 = 8 };
 
-__constant__ int8_t c_bdry19[26][14];
-__constant__ int8_t c_bdry27[26][18];
+// reserved boundary directions; one copy per translation unit, uploaded by
+// AmrOps<S>::upload_tables when a case of that storage type is built
+static __constant__ int8_t c_bdry19[26][14];
+static __constant__ int8_t c_bdry27[26][18];
 
 template <int Q, class S>
 __global__ void k_init_eq(int64_t n, const uint32_t *tag, double rho0, double ux, double uy, double uz, S *f, S *fcol,
@@ -615,6 +617,10 @@ int AmrOps<S>::alloc(Ctx &ctx, Case &c, int l)
     using C = typename Store<S>::C;
     Level &lv = c.lv[l];
     const int64_t n = lv.n, Q = c.d.q;
+    if (l == 0) {
+        int rc = upload_bdry_tables(ctx);
+        if (rc) return rc;
+    }
     MT_CUDA(ctx, cudaMallocAsync(&lv.f, sizeof(S) * n * Q, ctx.stream));
     MT_CUDA(ctx, cudaMallocAsync(&lv.fcol, sizeof(S) * n * Q, ctx.stream));
     MT_CUDA(ctx, cudaMallocAsync(&lv.rho, sizeof(C) * n, ctx.stream));

@@ -168,8 +168,6 @@ int mt_case_create(mt_ctx *h, const mt_case_desc *d, int32_t *id)
     Ctx &ctx = h->c;
     int rc = check_desc(ctx, d);
     if (rc) return rc;
-    if (d->storage != MT_STORE_F64)
-        return set_err(ctx, MT_ERR_ARG, "the multi-level path stores populations in FP64");
     Case *c = new Case();
     c->d = *d;
     return add_case(ctx, c, id);
@@ -411,11 +409,7 @@ int mt_case_set_populations(mt_ctx *h, int32_t id, int32_t level, const double *
         cudaFreeAsync(d, ctx.stream);
         return rc;
     }
-    Level &lv = c->lv[level];
-    if (f) MT_CUDA(ctx, cudaMemcpyAsync(lv.f, f, sizeof(double) * Q * lv.n, cudaMemcpyHostToDevice, ctx.stream));
-    if (fcol) MT_CUDA(ctx, cudaMemcpyAsync(lv.fcol, fcol, sizeof(double) * Q * lv.n, cudaMemcpyHostToDevice, ctx.stream));
-    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
-    return MT_OK;
+    return amr_set(ctx, *c, level, f, fcol);
 }
 
 int mt_case_get_populations(mt_ctx *h, int32_t id, int32_t level, double *f, double *fcol)
@@ -446,11 +440,7 @@ int mt_case_get_populations(mt_ctx *h, int32_t id, int32_t level, double *f, dou
         cudaFreeAsync(d, ctx.stream);
         return rc;
     }
-    Level &lv = c->lv[level];
-    if (f) MT_CUDA(ctx, cudaMemcpyAsync(f, lv.f, sizeof(double) * Q * lv.n, cudaMemcpyDeviceToHost, ctx.stream));
-    if (fcol) MT_CUDA(ctx, cudaMemcpyAsync(fcol, lv.fcol, sizeof(double) * Q * lv.n, cudaMemcpyDeviceToHost, ctx.stream));
-    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
-    return MT_OK;
+    return amr_get(ctx, *c, level, f, fcol);
 }
 
 int mt_case_get_macros(mt_ctx *h, int32_t id, int32_t level, double *rho, double *u)
@@ -476,11 +466,7 @@ int mt_case_get_macros(mt_ctx *h, int32_t id, int32_t level, double *rho, double
         cudaFreeAsync(d, ctx.stream);
         return rc;
     }
-    Level &lv = c->lv[level];
-    if (rho) MT_CUDA(ctx, cudaMemcpyAsync(rho, lv.rho, sizeof(double) * lv.n, cudaMemcpyDeviceToHost, ctx.stream));
-    if (u) MT_CUDA(ctx, cudaMemcpyAsync(u, lv.u, sizeof(double) * 3 * lv.n, cudaMemcpyDeviceToHost, ctx.stream));
-    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
-    return MT_OK;
+    return amr_macros(ctx, *c, level, rho, u);
 }
 
 int mt_case_reduce(mt_ctx *h, int32_t id, double *out)

@@ -1,9 +1,12 @@
 // Internal types of libmtlbm: context, per-case device state, launch helpers.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -42,8 +45,8 @@ struct Level {
     int8_t *bcidx = nullptr;   // lat_bc index or -1
     int32_t *disrow = nullptr; // row in the dis table or -1
     int32_t *nbr = nullptr;    // [(Q-1) * n]: index of the cell at key + e_k (k >= 1) or -1
-    double *f = nullptr, *fcol = nullptr;  // [Q * n] FP64 populations (general path)
-    double *rho = nullptr, *u = nullptr;   // [n], [3 * n] macroscopic fields
+    void *f = nullptr, *fcol = nullptr;  // [Q * n] populations in the case's storage type
+    void *rho = nullptr, *u = nullptr;   // [n], [3 * n] macroscopic fields (double, or float for reduced storage)
     int32_t *list[kNumSets] = {};
     int64_t nlist[kNumSets] = {};
     int32_t *collide_list = nullptr; int64_t ncollide = 0;  // lat_f then F2C
@@ -103,6 +106,22 @@ int amr_step(Ctx &ctx, Case &c, int n);
 int amr_phase(Ctx &ctx, Case &c, int phase, int level);
 int amr_find(Ctx &ctx, Case &c, int level, const uint64_t *h_keys, int64_t n, int64_t *h_idx);
 int amr_guard(Ctx &ctx, Case &c, int *flags);
+int amr_get(Ctx &ctx, Case &c, int level, double *h_f, double *h_fcol);
+int amr_set(Ctx &ctx, Case &c, int level, const double *h_f, const double *h_fcol);
+int amr_macros(Ctx &ctx, Case &c, int level, double *h_rho, double *h_u);
+
+// multi-level phases, one explicit instantiation per storage type
+// (mt_amr_f64.cu builds the FP64 one without FMA contraction)
+template <class S> struct AmrOps {
+    static int phase(Ctx &ctx, Case &c, int phase, int level);
+    static int upload_tables(Ctx &ctx);
+    static int alloc(Ctx &ctx, Case &c, int level);
+    static int init_eq(Ctx &ctx, Case &c, double rho0, const double *u0);
+    static int get(Ctx &ctx, Case &c, int level, int which, double *d_out);      // which: 0 f, 1 fcol
+    static int set(Ctx &ctx, Case &c, int level, int which, const double *d_in);
+    static int macros_out(Ctx &ctx, Case &c, int level, double *d_rho, double *d_u);
+    static int guard(Ctx &ctx, Case &c);
+};
 void amr_free(Case &c);
 
 // dense uniform path, one explicit instantiation per storage type
@@ -119,6 +138,17 @@ template <class S> struct DenseOps {
     // the state is untouched) and keep the fastest in c.dense_block
     static int tune(Ctx &ctx, Case &c, float *ms_out, int *blocks_out, int *n_out);
 };
+
+// call fn with a null pointer of the multi-level case's storage type
+template <class F> int amr_dispatch(Case &c, F &&fn)
+{
+    switch (c.d.storage) {
+    case MT_STORE_F64: return fn((double *)nullptr);
+    case MT_STORE_F32: return fn((float *)nullptr);
+    case MT_STORE_F16: return fn((__half *)nullptr);
+    default: return fn((__nv_bfloat16 *)nullptr);
+    }
+}
 
 // error helpers
 int set_err(Ctx &ctx, int code, const std::string &msg);

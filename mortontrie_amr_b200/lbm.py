@@ -151,12 +151,14 @@ class LBM_Manager:
     """Multi-level case on the device: the reference's LBM_Manager with its
     strategy objects (collide / stream / treat / boundary) as methods."""
 
-    def __init__(self, ctx: Context, case: Case):
+    def __init__(self, ctx: Context, case: Case, storage: str = "f64"):
+        """storage: "f64" (the reference's precision, bit-exact) or "f32" /
+        "f16" / "bf16" (FP32 arithmetic on stored deviations f - w_q)."""
         self.ctx = ctx
         self.case = case
         self.q = case.params.q
         self.L = case.mesh.spec.max_level
-        d = make_desc(case, "f64")
+        d = make_desc(case, storage)
         cid = C.c_int32()
         ctx.check(lib().mt_case_create(ctx.h, C.byref(d), C.byref(cid)), "mt_case_create")
         self.id = cid.value

@@ -118,6 +118,40 @@ def test_cfg1_full_size_matches_oracle(ctx):
     assert rel_err(mgr.force()[:3], oc.force()[:3]) < 1e-12
 
 
+# relative L2 of the velocity on lat_f cells vs the FP64 path after 30 coarse steps
+TOL_AMR = {"f32": 1e-5, "f16": 1e-2, "bf16": 6e-2}
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("which", ["cfg1_q19", "cumulant_q27"])
+def test_multilevel_reduced_storage_vs_f64(ctx, storage, which):
+    """Multi-level path with FP32 arithmetic on FP32 / FP16 / BF16 stored
+    deviations against the FP64 path: velocity field (every level) and drag
+    within the stated tolerances."""
+    from mortontrie_amr_b200.case import nested_sphere_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    if which == "cfg1_q19":
+        case = _cfg1_small()
+    else:
+        case = nested_sphere_case(coarse=(48, 24, 24), max_level=2, center=(16, 12, 12), radius=2.0,
+                                  half_widths=(4.0, 2.5), re=50.0)
+    a = LBM_Manager(ctx, case, "f64")
+    b = LBM_Manager(ctx, case, storage)
+    a.fluidSimulate(30)
+    b.fluidSimulate(30)
+    ctx.synchronize()
+    for l in range(case.max_level + 1):
+        _, ua = a.macros(l)
+        _, ub = b.macros(l)
+        _, tags = a.keys(l)
+        fluid = (tags & 1) != 0
+        err = np.linalg.norm(ub[:, fluid] - ua[:, fluid]) / np.linalg.norm(ua[:, fluid])
+        assert err < TOL_AMR[storage], (which, storage, l, err)
+    fa, fb = a.force(), b.force()
+    assert fa[3] == fb[3]
+    assert abs(fb[0] - fa[0]) / abs(fa[0]) < 10 * TOL_AMR[storage], (fa, fb)
+
+
 def test_nonfinite_guard(ctx):
     """A NaN planted on the host in one population propagates through the
     steps; the device guard reports it as MT_ERR_NONFINITE and the context
