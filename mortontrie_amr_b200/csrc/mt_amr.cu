@@ -292,7 +292,9 @@ int amr_build(Ctx &ctx, Case &c)
         MT_LAUNCHED(ctx);
         int rc = select_indices(ctx, fl.n, IbLatf{fl.tag}, &fl.iblist, &fl.nib);
         if (rc) return rc;
-        if (fl.nib) MT_CUDA(ctx, cudaMallocAsync(&c.ib_force, 8 * 3 * fl.nib, ctx.stream));
+        // per-cell forces (3 * nib) and the 256-cell partial sums (3 * ceil(nib / 256))
+        if (fl.nib)
+            MT_CUDA(ctx, cudaMallocAsync(&c.ib_force, 8 * 3 * (fl.nib + grid_for(fl.nib, 256)), ctx.stream));
     }
     {
         int64_t maxn = 0;

@@ -240,10 +240,12 @@ __global__ void k_bc_neq(const int32_t *list, int64_t nl, int b, int64_t n, cons
 }
 
 // Restated inlet/outflow on the x faces: West wall cells hold
-// fcol = feq(rho_inner, u_bc), East wall cells copy the inner cell's fcol.
+// fcol = feq(rho0, u_bc) (BC/ZouHe_Velocity.cpp:62-115 writes the
+// equilibrium at the boundary cell's own, never-updated density), East wall
+// cells copy the inner cell's fcol (BC/Outflow.cpp:39-52).
 template <int Q, class S>
-__global__ void k_bc_inout(const int32_t *list, int64_t nl, int east, int64_t n, const int32_t *nbr,
-                           const typename Store<S>::C *rho, S *f, S *fcol, double ubx, double uby, double ubz, int *err)
+__global__ void k_bc_inout(const int32_t *list, int64_t nl, int east, int64_t n, const int32_t *nbr, double rho0,
+                           S *f, S *fcol, double ubx, double uby, double ubz, int *err)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -262,7 +264,7 @@ __global__ void k_bc_inout(const int32_t *list, int64_t nl, int east, int64_t n,
             fcol[k * n + i] = v;
             f[k * n + i] = v;
         } else {
-            const C v = stored_of<S, Q>(feq_g<Q, C>(k, rho[nb], (C)ubx, (C)uby, (C)ubz), k);
+            const C v = stored_of<S, Q>(feq_g<Q, C>(k, (C)rho0, (C)ubx, (C)uby, (C)ubz), k);
             T::st(fcol, k * n + i, v);
             T::st(f, k * n + i, v);
         }
@@ -362,7 +364,24 @@ __global__ void k_ib_treat(const int32_t *list, int64_t nl, int64_t n, const int
 }
 
 // fixed-order reduction of the per-cell IB force into the accumulator
-// (LBM_Manager::accumIBForce, one call per treat)
+// (LBM_Manager::accumIBForce, one call per treat): stage 1 sums 256-cell
+// chunks into partials, stage 2 sums the partials in order
+static __global__ void k_force_partial(const double *force, int64_t nl, double *partial)
+{
+    __shared__ double s[3][256];
+    const int t = threadIdx.x;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + t;
+    for (int c = 0; c < 3; ++c) s[c][t] = j < nl ? force[c * nl + j] : 0.0;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (t < w)
+            for (int c = 0; c < 3; ++c) s[c][t] += s[c][t + w];
+        __syncthreads();
+    }
+    if (t == 0)
+        for (int c = 0; c < 3; ++c) partial[c * gridDim.x + blockIdx.x] = s[c][0];
+}
+
 static __global__ void k_force_reduce(const double *force, int64_t nl, double *acc)
 {
     __shared__ double s[3][256];
@@ -571,7 +590,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         for (int face = 0; face < 2; ++face) {
             if (!l0.nbc[face]) continue;
             k_bc_inout<Q, S><<<grid_for(l0.nbc[face], B), B, 0, s>>>(l0.bclist[face], l0.nbc[face], face, l0.n, l0.nbr,
-                                                                      A::rho(l0), A::f(l0), A::fcol(l0), c.d.u_bc[0],
+                                                                      c.d.rho0, A::f(l0), A::fcol(l0), c.d.u_bc[0],
                                                                       c.d.u_bc[1], c.d.u_bc[2], c.dev_err);
             MT_LAUNCHED(ctx);
         }
@@ -591,7 +610,12 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             k_ib_treat<Q, 0, S><<<grid_for(fl.nib, 64), 64, 0, s>>>(fl.iblist, fl.nib, fl.n, fl.disrow, c.dis, fl.nbr,
                                                                      A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force);
         MT_LAUNCHED(ctx);
-        k_force_reduce<<<1, 256, 0, s>>>(c.ib_force, fl.nib, c.force_acc);
+        // ib_force holds 3 * nib per-cell values followed by room for the partials
+        const unsigned nb = grid_for(fl.nib, 256);
+        double *partial = c.ib_force + 3 * fl.nib;
+        k_force_partial<<<nb, 256, 0, s>>>(c.ib_force, fl.nib, partial);
+        MT_LAUNCHED(ctx);
+        k_force_reduce<<<1, 256, 0, s>>>(partial, nb, c.force_acc);
         MT_LAUNCHED(ctx);
         return MT_OK;
     }

@@ -375,6 +375,17 @@ class DenseCase:
             pass
 
 
+def drag_coefficient(force4, u_lattice, diameter_finest_cells, rho=1.0):
+    """Cd = 2 F / (rho U^2 pi d^2 / 4) with F the mean momentum-exchange
+    force per treat() call (force4 = fx, fy, fz, number of calls, as
+    mt_get_force returns it), U the boundary velocity in level-0 lattice
+    units and d the sphere diameter in finest cells -- the formula of
+    LBM_Manager::infoPrint (LBM_Manager.cpp:964-979)."""
+    fx = force4[0] / max(force4[3], 1.0)
+    area = np.pi * diameter_finest_cells * diameter_finest_cells / 4.0
+    return 2.0 * fx / (rho * u_lattice * u_lattice * area)
+
+
 def morton_order_fields(n_edge, *fields):
     """Reorder (x, y, z)-indexed cube fields into Morton (sorted key) order."""
     from .lattice import morton_encode

@@ -942,10 +942,11 @@ static void phase_ib(oc_case *c)
 /* Restated domain boundaries with no runnable reference code: a velocity
  * inlet on the West face and a zero-gradient outflow on the East face, both
  * on boundary-shell cells whose fcol the fluid pulls from.  The inlet keeps
- * fcol = feq(rho_neighbour, u_bc) on the wall cell (the West branch of
- * BC/ZouHe_Velocity.cpp:62-115 writes the equilibrium); the outflow copies
- * the inner neighbour's post-collision populations (BC/Outflow.cpp:39-52
- * copies the inward populations from the first interior layer). */
+ * fcol = feq(rho0, u_bc) on the wall cell (the West branch of
+ * BC/ZouHe_Velocity.cpp:62-115 writes the equilibrium at the boundary cell's
+ * own density, which nothing updates from rho0); the outflow copies the inner
+ * neighbour's post-collision populations (BC/Outflow.cpp:39-52 copies the
+ * populations that stream inward from the first interior layer). */
 static int phase_bc_inout(oc_case *c)
 {
     oc_level *lv = &c->lv[0];
@@ -960,7 +961,7 @@ static int phase_bc_inout(oc_case *c)
             int64_t nb = find_idx(lv, nk);
             if (nb < 0) return -6;
             if (face == 0) {
-                feq_bgk(q, lv->rho[nb], c->u_bc, feq);
+                feq_bgk(q, c->rho0, c->u_bc, feq);
                 for (int k = 0; k < q; ++k) {
                     lv->fcol[k * lv->n + i] = feq[k];
                     lv->f[k * lv->n + i] = feq[k];

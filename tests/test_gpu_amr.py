@@ -119,7 +119,7 @@ def test_cfg1_full_size_matches_oracle(ctx):
 
 
 # relative L2 of the velocity on lat_f cells vs the FP64 path after 30 coarse steps
-TOL_AMR = {"f32": 1e-5, "f16": 1e-2, "bf16": 6e-2}
+TOL_AMR = {"f32": 5e-5, "f16": 1e-2, "bf16": 6e-2}
 
 
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
@@ -153,16 +153,18 @@ def test_multilevel_reduced_storage_vs_f64(ctx, storage, which):
 
 
 def test_nonfinite_guard(ctx):
-    """A NaN planted on the host in one population propagates through the
-    steps; the device guard reports it as MT_ERR_NONFINITE and the context
-    stays usable."""
+    """A NaN planted on the host in one population of a lat_f cell (overlap
+    cells are rewritten every step) propagates through the steps; the device
+    guard reports it as MT_ERR_NONFINITE and the context stays usable."""
     from mortontrie_amr_b200.lbm import MTError
     case = _cfg1_small()
     mgr = _device_case(ctx, case, None)
     mgr.fluidSimulate(2)
     assert mgr.status() is None
     f, fcol = mgr.populations(1)
-    f[3, 100] = np.nan
+    _, tags = mgr.keys(1)
+    cell = int(np.flatnonzero((tags & 1) != 0)[len(tags) // 3])
+    f[3, cell] = np.nan
     mgr.set_populations(1, f, fcol)
     mgr.fluidSimulate(1)
     with pytest.raises(MTError, match="MT_ERR_NONFINITE"):
