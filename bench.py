@@ -283,7 +283,7 @@ def run_ours(args):
                        "l2": "state 637 MB > 126 MB L2; no flush", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "k_dense<19, half, LBGK, fused>",
+                         "kernel": "k_dense_pair<19, half, LBGK> (fused pull + collide)",
                          "algorithmic_bytes_per_launch": BYTES_PER_CELL["f16"] * n_cells},
             "variants": variants,
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,

@@ -123,8 +123,9 @@ int mt_case_set_populations(mt_ctx *ctx, int32_t case_id, int32_t level, const d
 int mt_case_get_populations(mt_ctx *ctx, int32_t case_id, int32_t level, double *f, double *fcol);
 /* density [n] and velocity [3][n] of a level (density/velocity maps of User) */
 int mt_case_get_macros(mt_ctx *ctx, int32_t case_id, int32_t level, double *rho, double *u);
-/* FP64 reductions over the stepped cells: mass, x/y/z momentum (dense path) */
-int mt_case_reduce(mt_ctx *ctx, int32_t case_id, double *out4);
+/* FP64 reductions over the stepped cells (dense path): out[5] = mass, x/y/z momentum,
+   kinetic energy sum of |j|^2 / (2 rho) */
+int mt_case_reduce(mt_ctx *ctx, int32_t case_id, double *out5);
 
 /* ---- the reference call surface --------------------------------------- */
 int mt_calculate_macros(mt_ctx *ctx, int32_t case_id, int32_t level); /* LBM_Manager::calculateMacros(level) */
