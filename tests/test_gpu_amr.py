@@ -163,7 +163,8 @@ def test_nonfinite_guard(ctx):
     assert mgr.status() is None
     f, fcol = mgr.populations(1)
     _, tags = mgr.keys(1)
-    cell = int(np.flatnonzero((tags & 1) != 0)[len(tags) // 3])
+    fluid = np.flatnonzero((tags & 1) != 0)
+    cell = int(fluid[len(fluid) // 3])
     f[3, cell] = np.nan
     mgr.set_populations(1, f, fcol)
     mgr.fluidSimulate(1)
