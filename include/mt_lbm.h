@@ -126,6 +126,15 @@ int mt_case_get_macros(mt_ctx *ctx, int32_t case_id, int32_t level, double *rho,
 /* FP64 reductions over the stepped cells (dense path): out[5] = mass, x/y/z momentum,
    kinetic energy sum of |j|^2 / (2 rho) */
 int mt_case_reduce(mt_ctx *ctx, int32_t case_id, double *out5);
+/* Allocation-free variant of mt_case_reduce; no reference counterpart (the
+   reference has no device-side reduction).  For callers that must not allocate
+   device memory during the call (a host that budgets the GPU's memory up front
+   for its cases).  Same outputs and kernels; the scratch is a static device
+   array of 640 KiB, so cases above 4,194,304 cells return MT_ERR_ARG.  Calls
+   that overlap in time on one device race on that array: serialise them.  The
+   first call on a device does a one-time set-up (looks up the array's address);
+   make it before any stream capture.  Synchronises the stream. */
+int mt_case_reduce_noalloc(mt_ctx *ctx, int32_t case_id, double *out5);
 
 /* ---- the reference call surface --------------------------------------- */
 int mt_calculate_macros(mt_ctx *ctx, int32_t case_id, int32_t level); /* LBM_Manager::calculateMacros(level) */

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "mt_internal.hpp"
@@ -629,3 +630,85 @@ int mt_reset_force(mt_ctx *h, int32_t id)
 }
 
 }  // extern "C"
+
+// ---- allocation-free reduction ------------------------------------------
+//
+// mt_case_reduce_noalloc is for callers that must not allocate device memory
+// while they run: a host that has carved the GPU's memory up front for its
+// cases (an admission budget, a pool shared with other processes) or that
+// calls in from a context where cudaMalloc / cudaMallocAsync would take a
+// driver lock or grow a pool at a bad moment.  It launches the same two
+// kernels as mt_case_reduce, with their scratch in the static device array
+// below instead of a cudaMallocAsync'd buffer.
+//
+// Scratch: 5 * MT_NOALLOC_REDUCE_BLOCKS per-block partial sums (one block per
+// 256 cells) followed by the 5 totals, 640 KiB + 64 B in all; cases of more
+// than 256 * MT_NOALLOC_REDUCE_BLOCKS = 4,194,304 cells are rejected with
+// MT_ERR_ARG.  Nothing in it has to start at zero: each call writes every
+// partial slot it reads (k_dense_reduce, blocks 0 .. ceil(N/256)-1) and then
+// the 5 totals (k_sum_partials) before copying them out, in stream order.
+// The array is one per device and process, so calls that overlap in time on
+// the same device (two host threads, or two contexts on different streams)
+// race on it; the caller serialises them.  The first call on a device looks
+// up the array's device address (cudaGetSymbolAddress, with that device
+// current) and caches it; make that first call before any stream capture.
+
+namespace {
+
+constexpr int64_t MT_NOALLOC_REDUCE_BLOCKS = 16384;
+constexpr int MT_NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) double g_reduce_scratch[5 * MT_NOALLOC_REDUCE_BLOCKS + 8];
+
+std::mutex g_scratch_mu;
+double *g_scratch_ptr[MT_NOALLOC_MAX_DEVICES] = {};
+
+// device address of g_reduce_scratch on ctx.device (set-up on first use)
+int noalloc_scratch(mt::Ctx &ctx, double **out)
+{
+    if (ctx.device < 0 || ctx.device >= MT_NOALLOC_MAX_DEVICES)
+        return mt::set_err(ctx, MT_ERR_ARG, "device index out of range for the static reduction scratch");
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_ptr[ctx.device]) {
+        cudaError_t e = cudaSetDevice(ctx.device);
+        if (e != cudaSuccess) return mt::set_err(ctx, MT_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+        double *p = nullptr;
+        e = cudaGetSymbolAddress((void **)&p, g_reduce_scratch);
+        if (e != cudaSuccess || !p)
+            return mt::set_err(ctx, MT_ERR_CUDA,
+                               std::string("cudaGetSymbolAddress(reduction scratch): ") + cudaGetErrorString(e));
+        g_scratch_ptr[ctx.device] = p;
+    }
+    *out = g_scratch_ptr[ctx.device];
+    return MT_OK;
+}
+
+}  // namespace
+
+extern "C" int mt_case_reduce_noalloc(mt_ctx *h, int32_t id, double *out)
+{
+    using namespace mt;
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!out) return set_err(ctx, MT_ERR_ARG, "null output");
+    if (!c->dense) return set_err(ctx, MT_ERR_STATE, "device reductions are implemented for the dense path");
+    const int64_t blocks = (c->N + 255) / 256;
+    if (blocks > MT_NOALLOC_REDUCE_BLOCKS)
+        return set_err(ctx, MT_ERR_ARG,
+                       "mt_case_reduce_noalloc: " + std::to_string(c->N) + " cells exceed the static scratch (at most " +
+                           std::to_string(256 * MT_NOALLOC_REDUCE_BLOCKS) + " cells); use mt_case_reduce");
+    double *scratch = nullptr;
+    rc = noalloc_scratch(ctx, &scratch);
+    if (rc) return rc;
+    double *totals = scratch + 5 * MT_NOALLOC_REDUCE_BLOCKS;
+    rc = dense_dispatch(*c, [&](auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        return DenseOps<S>::reduce_into(ctx, *c, scratch, totals);
+    });
+    if (rc) return rc;
+    MT_CUDA(ctx, cudaMemcpyAsync(out, totals, sizeof(double) * 5, cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}

@@ -583,6 +583,24 @@ int DenseOps<S>::reduce(Ctx &ctx, Case &c, double *d_out)
 }
 
 template <class S>
+int DenseOps<S>::reduce_into(Ctx &ctx, Case &c, double *partial, double *d_out)
+{
+    const unsigned grid = grid_for(c.N, 256);
+    const DenseGeom g = dense_geom(c.bits);
+    const int pull = c.a_is_fcol ? 1 : 0;
+    if (c.d.q == 19)
+        k_dense_reduce<19, S><<<grid, 256, 0, ctx.stream>>>((const S *)c.A, c.N, g, pull, c.d.stream_convention,
+                                                            partial);
+    else
+        k_dense_reduce<27, S><<<grid, 256, 0, ctx.stream>>>((const S *)c.A, c.N, g, pull, c.d.stream_convention,
+                                                            partial);
+    MT_LAUNCHED(ctx);
+    k_sum_partials<<<1, 256, 0, ctx.stream>>>(partial, grid, d_out);
+    MT_LAUNCHED(ctx);
+    return MT_OK;
+}
+
+template <class S>
 int DenseOps<S>::tune(Ctx &ctx, Case &c, float *ms_out, int *blocks_out, int *n_out)
 {
     static const int cand[] = {128, 256, 512, 1024};

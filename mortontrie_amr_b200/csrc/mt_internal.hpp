@@ -134,6 +134,9 @@ template <class S> struct DenseOps {
     static int set(Ctx &ctx, Case &c, const double *d_f);
     static int macros(Ctx &ctx, Case &c, double *d_rho, double *d_u);
     static int reduce(Ctx &ctx, Case &c, double *d_out);
+    // the same two launches as reduce() into caller-provided device scratch:
+    // partial[5 * ceil(N / 256)] per-block sums and d_out[5] totals; allocates nothing
+    static int reduce_into(Ctx &ctx, Case &c, double *partial, double *d_out);
     // time the fused kernel at each candidate block size (A -> B, no swap:
     // the state is untouched) and keep the fastest in c.dense_block
     static int tune(Ctx &ctx, Case &c, float *ms_out, int *blocks_out, int *n_out);
