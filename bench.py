@@ -298,7 +298,7 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def amr_section(ctx, torch, steps=10, warmup=2):
+def amr_section(ctx, torch, steps=10, warmup=2, only=None):
     """4-level D3Q27 cumulant sphere (192x96x96 coarse, R = 6 coarse = 48
     finest cells, Re 200, u 0.04, nested boxes 4R / 2.5R / 1.75R): coarse
     steps of the multi-level path in the reference's FP64 and with FP32 / FP16
@@ -317,8 +317,14 @@ def amr_section(ctx, torch, steps=10, warmup=2):
            "stepped_cells_per_level": stepped, "coarse_steps": steps}
     stream = torch.cuda.current_stream()
     res = {}
-    for st in ("f64", "f32", "f16"):
-        mgr = LBM_Manager(ctx, case, st)
+    # (label, storage, schedule): the plain form is FP64 in the reference's
+    # phase order; the reduced storages run the fused schedule
+    runs = [("f64", "f64", "phases"), ("f64_fused", "f64", "fused"), ("f32", "f32", "fused"),
+            ("f16", "f16", "fused"), ("bf16", "bf16", "fused"), ("f16_phases", "f16", "phases")]
+    if only:
+        runs = [r for r in runs if r[0] in only]
+    for st, storage, schedule in runs:
+        mgr = LBM_Manager(ctx, case, storage, schedule=schedule)
         mgr.fluidSimulate(warmup)
         torch.cuda.synchronize()
         mgr.reset_force()
@@ -334,12 +340,15 @@ def amr_section(ctx, torch, steps=10, warmup=2):
         fluid = (tags & 1) != 0
         f = mgr.force()
         res[st] = dict(secs=secs, u=u[:, fluid], rho=rho[fluid], fx=f[0] / max(f[3], 1.0))
-        out[st] = {"fine_mlups": round(per_coarse_fine * steps / secs / 1e6, 1),
+        out[st] = {"storage": storage, "schedule": schedule,
+                   "fine_mlups": round(per_coarse_fine * steps / secs / 1e6, 1),
                    "total_mlups": round(per_coarse_total * steps / secs / 1e6, 1),
                    "ms_per_coarse_step": round(1e3 * secs / steps, 3)}
         mgr.close()
-    ref = res["f64"]
-    for st in ("f32", "f16"):
+    ref = res.get("f64")
+    for st, _, _ in runs:
+        if ref is None or st == "f64":
+            continue
         r = res[st]
         out[st]["velocity_l2_vs_f64"] = float(np.linalg.norm(r["u"] - ref["u"]) / np.linalg.norm(ref["u"]))
         out[st]["drag_rel_vs_f64"] = float(abs(r["fx"] - ref["fx"]) / max(abs(ref["fx"]), 1e-300))
@@ -430,6 +439,9 @@ def main():
     ap.add_argument("--no-amr", action="store_true", help="skip the 4-level cumulant sphere section")
     ap.add_argument("--amr-only", action="store_true",
                     help="only the 4-level cumulant sphere section (K coarse steps per storage; profiling runs)")
+    ap.add_argument("--amr-variants", default=None,
+                    help="comma list of multi-level runs to time (default all: "
+                         "f64,f64_fused,f32,f16,bf16,f16_phases); profiling runs")
     ap.add_argument("--edge", type=int, default=256, help="cube edge (power of two); 256 is the configuration")
     ap.add_argument("--quick", action="store_true", help="headline kernel only (profiling runs)")
     args = ap.parse_args()
@@ -447,7 +459,9 @@ def main():
         torch.cuda.set_stream(stream)
         ctx = Context(0)
         ctx.set_stream(stream.cuda_stream)
-        print(json.dumps({"amr_cumulant_sphere": amr_section(ctx, torch, steps=args.steps, warmup=1)}), flush=True)
+        only = args.amr_variants.split(",") if args.amr_variants else None
+        print(json.dumps({"amr_cumulant_sphere": amr_section(ctx, torch, steps=args.steps, warmup=1, only=only)}),
+              flush=True)
         ctx.close()
     else:
         run_ours(args)

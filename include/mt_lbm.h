@@ -59,6 +59,9 @@ extern "C" {
 #define MT_STORE_F32 1  /* FP32 storage of f - w_q, FP32 arithmetic */
 #define MT_STORE_F16 2  /* FP16 storage of f - w_q, FP32 arithmetic */
 #define MT_STORE_BF16 3 /* BF16 storage of f - w_q, FP32 arithmetic */
+#define MT_SCHED_PHASES 0 /* the reference's phase order: collide, stream, ... as separate passes */
+#define MT_SCHED_FUSED 1  /* stream of one substep fused with the collision of the next (same results) */
+#define MT_SCHED_FUSED_LISTS 2 /* MT_SCHED_FUSED over cell lists and the neighbour table, no 4x4x4 bricks */
 
 /* Case description: the switches the reference hard-codes in
  * LBM_Manager::LBM_Manager (LBM_Manager.cpp:32-95) and its per-level
@@ -70,7 +73,7 @@ typedef struct mt_case_desc {
     int32_t ib_method;         /* MT_IB_* */
     int32_t bc_mode;           /* MT_BC_* */
     int32_t stream_convention; /* MT_PULL_* */
-    int32_t storage;           /* MT_STORE_* (the multi-level path supports MT_STORE_F64) */
+    int32_t storage;           /* MT_STORE_*; FP64 is the reference precision (bit-exact) */
     int32_t periodic[3];       /* per axis: 1 wraps neighbours (no reference counterpart; BC/Periodic.cpp is dead code) */
     int64_t extent0[3];        /* level-0 cells per axis */
     double tau[MT_MAX_LEVELS]; /* LBM_Manager::tau */
@@ -162,6 +165,16 @@ int mt_case_status(mt_ctx *ctx, int32_t case_id);
  * (writing only the scratch array, so the state is unchanged) and keeps the
  * fastest; ms_per_candidate (nullable) receives the 4 mean launch times. */
 int mt_case_tune(mt_ctx *ctx, int32_t case_id, int32_t *best_block, float *ms_per_candidate);
+/* Schedule of mt_step for a multi-level case (no reference counterpart):
+ * MT_SCHED_PHASES (default) issues the reference's phases one pass each;
+ * MT_SCHED_FUSED keeps a second post-collision buffer per level and streams
+ * each substep in the same pass as the next substep's macros + collision
+ * (LBM_Simulator.cpp:20-229 reordered: the state after every coarse step is
+ * the same).  Its fused pass walks 4x4x4 Morton bricks with neighbours
+ * computed in shared memory where a level allows it (periodic axes a multiple
+ * of 4 cells); MT_SCHED_FUSED_LISTS uses cell lists and the neighbour table
+ * everywhere.  The per-phase calls always act on the current buffers. */
+int mt_case_set_schedule(mt_ctx *ctx, int32_t case_id, int32_t schedule);
 /* accumulated momentum-exchange force of treat() calls: fx, fy, fz, count
  * (LBM_Manager::accumIBForce, LBM_Manager.cpp:846-852) */
 int mt_get_force(mt_ctx *ctx, int32_t case_id, double *out4);

@@ -8,6 +8,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <utility>
 #include <cstring>
 
 #include "mt_internal.hpp"
@@ -126,6 +127,57 @@ __global__ void k_coal_children(MortonGeom g, int fine, const int32_t *src, int6
     }
 }
 
+// ---- 4x4x4 bricks of a level (fused schedule) --------------------------------
+__global__ void k_brick_flags(const uint64_t *key, int64_t n, int shift, int32_t *flag)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    flag[i] = (i == 0 || (key[i] >> shift) != (key[i - 1] >> shift)) ? 1 : 0;
+}
+
+// cb = inclusive scan of the flags: brick of cell i is cb[i] - 1
+__global__ void k_brick_fill(const uint64_t *key, const uint32_t *tag, int64_t n, int shift, int low,
+                             const int32_t *cb, int ib_level, int32_t *bstart, uint64_t *bkey,
+                             unsigned long long *bmask, uint8_t *bcls)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t b = cb[i] - 1;
+    const int m = (int)((key[i] >> low) & 63);
+    if (i == 0 || cb[i] != cb[i - 1]) {
+        bstart[b] = (int32_t)i;
+        bkey[b] = key[i] >> shift;
+    }
+    atomicOr(bmask + b, 1ull << m);
+    const uint32_t t = tag[i];
+    // stream covers lat_f then overlap_C2F, and a C2F cell's fcol = f copy
+    // comes after the collision (Collision_Manager.cpp:45-52)
+    uint8_t cls = 0;
+    if (t & TAG_C2F)
+        cls = 2;
+    else if ((t & TAG_LATF) && !(ib_level && (t & TAG_IB)))
+        cls = 1;
+    bcls[64 * b + m] = cls;
+}
+
+// neighbour bricks: Morton_Assist::find_neighbor applied to the corner cell
+// of the brick that faces the offset, then a search of the brick keys
+__global__ void k_brick_nbrs(MortonGeom g, int level, const uint64_t *bkey, int64_t nb, int shift, int low,
+                             int32_t *bnbr)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= 27 * nb) return;
+    const int64_t b = t / 27;
+    const int s = (int)(t - 27 * b);
+    const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+    const int lx = dx > 0 ? 3 : 0, ly = dy > 0 ? 3 : 0, lz = dz > 0 ? 3 : 0;
+    const uint64_t m = (uint64_t)((lx & 1) | ((lx & 2) << 2) | ((ly & 1) << 1) | ((ly & 2) << 3) | ((lz & 1) << 2) |
+                                  ((lz & 2) << 4));
+    const uint64_t rep = (bkey[b] << shift) | (m << low);
+    const uint64_t nk = find_neighbor(g, rep, level, dx, dy, dz);
+    bnbr[t] = (int32_t)find_key(bkey, nb, nk >> shift);
+}
+
 struct TagHas {
     const uint32_t *tag;
     uint32_t bit;
@@ -135,6 +187,13 @@ struct BcIs {
     const int8_t *bc;
     int8_t b;
     __host__ __device__ bool operator()(const int32_t &i) const { return bc[i] == b; }
+};
+struct LatfNotIb {
+    const uint32_t *tag;
+    __host__ __device__ bool operator()(const int32_t &i) const
+    {
+        return (tag[i] & TAG_LATF) && !(tag[i] & TAG_IB);
+    }
 };
 struct IbLatf {
     const uint32_t *tag;
@@ -337,12 +396,35 @@ int amr_build(Ctx &ctx, Case &c)
     return MT_OK;
 }
 
+void amr_drop_fused(Case &c)
+{
+    for (int p = 0; p < 2; ++p) {
+        if (c.fgraph[p]) cudaGraphExecDestroy(c.fgraph[p]);
+        c.fgraph[p] = nullptr;
+    }
+    for (int l = 0; l < kMaxLevels; ++l) {
+        Level &lv = c.lv[l];
+        void *ptrs[] = {lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls};
+        for (void *p : ptrs)
+            if (p) cudaFree(p);
+        lv.fused_list = nullptr;
+        lv.nfused = 0;
+        lv.bstart = nullptr;
+        lv.bmask = nullptr;
+        lv.bnbr = nullptr;
+        lv.bcls = nullptr;
+        lv.nbrick = 0;
+        lv.bricks = false;
+    }
+}
+
 void amr_free(Case &c)
 {
     for (int l = 0; l < kMaxLevels; ++l) {
         Level &lv = c.lv[l];
         void *ptrs[] = {lv.key, lv.tag, lv.bcidx, lv.disrow, lv.nbr, lv.f, lv.fcol, lv.rho, lv.u,
-                        lv.collide_list, lv.stream_list, lv.iblist, lv.expl_src, lv.expl_child, lv.coal_child};
+                        lv.collide_list, lv.stream_list, lv.iblist, lv.expl_src, lv.expl_child, lv.coal_child,
+                        lv.fcol_alt, lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         for (int s = 0; s < kNumSets; ++s)
@@ -362,6 +444,15 @@ void amr_free(Case &c)
     c.dev_err = nullptr;
     if (c.graph) cudaGraphExecDestroy(c.graph);
     c.graph = nullptr;
+    for (int p = 0; p < 2; ++p) {
+        if (c.fgraph[p]) cudaGraphExecDestroy(c.fgraph[p]);
+        c.fgraph[p] = nullptr;
+    }
+    if (c.side) cudaStreamDestroy(c.side);
+    if (c.ev_fork) cudaEventDestroy(c.ev_fork);
+    if (c.ev_join) cudaEventDestroy(c.ev_join);
+    c.side = nullptr;
+    c.ev_fork = c.ev_join = nullptr;
 }
 
 // ----------------------------------------------------------------------------
@@ -370,7 +461,7 @@ void amr_free(Case &c)
 // mt_amr_lp.cu)
 // ----------------------------------------------------------------------------
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
-       PH_BC_FACE0 = 8 };
+       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME };
 
 int amr_phase(Ctx &ctx, Case &c, int phase, int level)
 {
@@ -430,29 +521,192 @@ static int record_step(Ctx &ctx, Case &c)
     return MT_OK;
 }
 
+static int capture(Ctx &ctx, Case &c, int (*record)(Ctx &, Case &), cudaGraphExec_t *out, int64_t *launches)
+{
+    const int64_t before = ctx.launches;
+    MT_CUDA(ctx, cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
+    int rc = record(ctx, c);
+    cudaGraph_t captured = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx.stream, &captured);
+    if (rc) {
+        if (captured) cudaGraphDestroy(captured);
+        return rc;
+    }
+    if (e != cudaSuccess) return set_err(ctx, MT_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    *launches = ctx.launches - before;
+    ctx.launches = before;
+    e = cudaGraphInstantiate(out, captured, 0);
+    cudaGraphDestroy(captured);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        return set_err(ctx, MT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    return MT_OK;
+}
+
+// ---- fused schedule ---------------------------------------------------------
+// Per substep of level l: swap the post-collision buffers (fcol now holds the
+// collision computed one substep ahead), collide the F2C cells (their f came
+// from coalescence), the inlet/outflow wall cells, the finer levels, the
+// explosion, then one pass that streams lat_f and C2F, treats the IB cells and
+// collides all of them into the other buffer for the next substep; then the
+// boundary sweep and coalescence, as in LBM_Simulator.cpp:20-229.
+static void swap_buffers(Case &c, int l)
+{
+    std::swap(c.lv[l].fcol, c.lv[l].fcol_alt);
+    if (l == 0) c.par0 ^= 1;
+}
+
+static int fused_lbm_kernel(Ctx &ctx, Case &c, int l)
+{
+    const int L = c.d.max_level;
+    int rc;
+#define RUN(ph, lev)                               \
+    do {                                           \
+        if ((rc = amr_phase(ctx, c, (ph), (lev)))) \
+            return rc;                             \
+    } while (0)
+    for (int sub = 0; sub < 2; ++sub) {
+        swap_buffers(c, l);
+        RUN(PH_F2C_COLLIDE, l);
+        if (l == 0 && c.d.bc_mode == MT_BC_ZOUHE_OUTFLOW) RUN(PH_BC_INOUT, 0);
+        if (l < L)
+            if ((rc = fused_lbm_kernel(ctx, c, l + 1))) return rc;
+        if (sub == 0 && l > 0) RUN(PH_EXPLOSION, l);
+        RUN(PH_PULL_COLLIDE, l);
+        if (l == 0 && c.d.bc_mode == MT_BC_NEQ) RUN(PH_BC, 0);
+        if (l < L) RUN(PH_COALESCENCE, l);
+        if (l == 0) break;
+    }
+#undef RUN
+    return MT_OK;
+}
+
+static int record_fused_step(Ctx &ctx, Case &c)
+{
+    int rc = fused_lbm_kernel(ctx, c, 0);
+    if (rc) return rc;
+    for (int l = 0; l <= c.d.max_level; ++l)
+        if ((rc = amr_phase(ctx, c, PH_MACROS, l))) return rc;
+    return MT_OK;
+}
+
+// Bricks of level l, when they reproduce the neighbour table exactly: every
+// periodic axis spans a multiple of 4 cells at this level (the wrap then
+// falls on a brick boundary).
+static int build_bricks(Ctx &ctx, Case &c, int l)
+{
+    Level &lv = c.lv[l];
+    const int L = c.d.max_level;
+    for (int a = 0; a < 3; ++a)
+        if (c.d.periodic[a] && ((c.d.extent0[a] << l) % 4) != 0) return MT_OK;
+    const int64_t n = lv.n;
+    if (n * c.d.q >= ((int64_t)1 << 32)) return MT_OK;  // the brick pass uses 32-bit element offsets
+    const int low = 3 * (L - l), shift = low + 6;
+    int32_t *flag = nullptr, *cb = nullptr;
+    MT_CUDA(ctx, cudaMallocAsync(&flag, 4 * n, ctx.stream));
+    MT_CUDA(ctx, cudaMallocAsync(&cb, 4 * n, ctx.stream));
+    k_brick_flags<<<grid_for(n, 256), 256, 0, ctx.stream>>>(lv.key, n, shift, flag);
+    MT_LAUNCHED(ctx);
+    size_t tb = 0;
+    MT_CUDA(ctx, cub::DeviceScan::InclusiveSum(nullptr, tb, flag, cb, (int)n, ctx.stream));
+    void *tmp = nullptr;
+    MT_CUDA(ctx, cudaMallocAsync(&tmp, tb, ctx.stream));
+    MT_CUDA(ctx, cub::DeviceScan::InclusiveSum(tmp, tb, flag, cb, (int)n, ctx.stream));
+    int32_t nb = 0;
+    MT_CUDA(ctx, cudaMemcpyAsync(&nb, cb + (n - 1), 4, cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    uint64_t *bkey = nullptr;
+    MT_CUDA(ctx, cudaMallocAsync(&lv.bstart, 4 * (size_t)nb, ctx.stream));
+    MT_CUDA(ctx, cudaMallocAsync(&lv.bmask, 8 * (size_t)nb, ctx.stream));
+    MT_CUDA(ctx, cudaMallocAsync(&lv.bnbr, 4 * 27 * (size_t)nb, ctx.stream));
+    MT_CUDA(ctx, cudaMallocAsync(&lv.bcls, 64 * (size_t)nb, ctx.stream));
+    MT_CUDA(ctx, cudaMallocAsync(&bkey, 8 * (size_t)nb, ctx.stream));
+    MT_CUDA(ctx, cudaMemsetAsync(lv.bmask, 0, 8 * (size_t)nb, ctx.stream));
+    MT_CUDA(ctx, cudaMemsetAsync(lv.bcls, 0, 64 * (size_t)nb, ctx.stream));
+    const int ib_level = (l == L && l > 0) ? 1 : 0;
+    k_brick_fill<<<grid_for(n, 256), 256, 0, ctx.stream>>>(lv.key, lv.tag, n, shift, low, cb, ib_level, lv.bstart,
+                                                           bkey, (unsigned long long *)lv.bmask, lv.bcls);
+    MT_LAUNCHED(ctx);
+    k_brick_nbrs<<<grid_for(27 * (int64_t)nb, 256), 256, 0, ctx.stream>>>(c.geom, l, bkey, nb, shift, low, lv.bnbr);
+    MT_LAUNCHED(ctx);
+    cudaFreeAsync(tmp, ctx.stream);
+    cudaFreeAsync(flag, ctx.stream);
+    cudaFreeAsync(cb, ctx.stream);
+    cudaFreeAsync(bkey, ctx.stream);
+    lv.nbrick = nb;
+    lv.bricks = true;
+    return MT_OK;
+}
+
+// second buffers, the fused cell lists, and the lookahead collision of the
+// current f on every level
+static int prime_fused(Ctx &ctx, Case &c)
+{
+    const int L = c.d.max_level;
+    if (!c.side && L > 0 && c.lv[L].nib) {
+        MT_CUDA(ctx, cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+        MT_CUDA(ctx, cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
+        MT_CUDA(ctx, cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
+    }
+    for (int l = 0; l <= L; ++l) {
+        Level &lv = c.lv[l];
+        if (!lv.n) continue;
+        if (!lv.fcol_alt) {
+            const size_t bytes = (size_t)c.d.q * (size_t)lv.n *
+                                 (c.d.storage == MT_STORE_F64 ? 8 : c.d.storage == MT_STORE_F32 ? 4 : 2);
+            MT_CUDA(ctx, cudaMallocAsync(&lv.fcol_alt, bytes, ctx.stream));
+        }
+        if (!lv.bricks && c.use_bricks) {
+            int rc = build_bricks(ctx, c, l);
+            if (rc) return rc;
+        }
+        if (!lv.bricks && !lv.fused_list && lv.nlist[0]) {
+            int rc = (l == L && l > 0) ? select_indices(ctx, lv.n, LatfNotIb{lv.tag}, &lv.fused_list, &lv.nfused)
+                                       : select_indices(ctx, lv.n, TagHas{lv.tag, TAG_LATF}, &lv.fused_list,
+                                                        &lv.nfused);
+            if (rc) return rc;
+        }
+        int rc = amr_phase(ctx, c, PH_PRIME, l);
+        if (rc) return rc;
+    }
+    c.primed = true;
+    return MT_OK;
+}
+
 // n coarse steps replayed from one captured graph (fluidSimulate loop body)
 int amr_step(Ctx &ctx, Case &c, int n)
 {
     int rc;
+    if (c.schedule == MT_SCHED_FUSED) {
+        if (!c.primed && (rc = prime_fused(ctx, c))) return rc;
+        for (int s = 0; s < n; ++s) {
+            const int p = c.par0;
+            if (!c.fgraph[p]) {
+                // recording swaps the host-side buffer pointers exactly as one
+                // replay does, so after it the state matches a launched step
+                if ((rc = capture(ctx, c, record_fused_step, &c.fgraph[p], &c.fgraph_launches[p]))) {
+                    c.primed = false;
+                    return rc;
+                }
+            } else {
+                // the host-side effect of one replay: level 0 swaps once,
+                // levels >= 1 an even number of times
+                swap_buffers(c, 0);
+            }
+            MT_CUDA(ctx, cudaGraphLaunch(c.fgraph[p], ctx.stream));
+            ctx.launches += c.fgraph_launches[p];
+        }
+        return MT_OK;
+    }
+    c.primed = false;
+    if (c.graph && c.graph_par0 != c.par0) {
+        cudaGraphExecDestroy(c.graph);
+        c.graph = nullptr;
+    }
     if (!c.graph) {
-        const int64_t before = ctx.launches;
-        MT_CUDA(ctx, cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
-        rc = record_step(ctx, c);
-        cudaGraph_t captured = nullptr;
-        cudaError_t e = cudaStreamEndCapture(ctx.stream, &captured);
-        if (rc) {
-            if (captured) cudaGraphDestroy(captured);
-            return rc;
-        }
-        if (e != cudaSuccess) return set_err(ctx, MT_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
-        c.graph_launches = ctx.launches - before;
-        ctx.launches = before;
-        e = cudaGraphInstantiate(&c.graph, captured, 0);
-        cudaGraphDestroy(captured);
-        if (e != cudaSuccess) {
-            c.graph = nullptr;
-            return set_err(ctx, MT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-        }
+        if ((rc = capture(ctx, c, record_step, &c.graph, &c.graph_launches))) return rc;
+        c.graph_par0 = c.par0;
     }
     for (int s = 0; s < n; ++s) {
         MT_CUDA(ctx, cudaGraphLaunch(c.graph, ctx.stream));

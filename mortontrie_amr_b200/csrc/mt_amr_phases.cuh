@@ -19,7 +19,7 @@
 namespace mt {
 
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
-       PH_BC_FACE0 = 8 };
+       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME };
 
 // reserved boundary directions; one copy per translation unit, uploaded by
 // AmrOps<S>::upload_tables when a case of that storage type is built
@@ -70,6 +70,46 @@ __global__ void k_macros(const int32_t *list, int64_t nl, int64_t n, const S *f,
     u[2 * n + i] = z;
 }
 
+// post-collision populations of one cell from its f (already in the compute
+// type C) and its macros: Collision_LBGK::collide (Collision_Manager.cpp:13-53)
+// or Collision_Cumulant::collide (Collision_Cumulant.cpp:22-159), stored into
+// fcol[k * n + i].  Shared by the phase kernel and the fused pull + collide
+// kernels so both schedules run the same arithmetic.
+template <int Q, class S, int COLL, class I = int64_t>
+__device__ __forceinline__ void collide_store(const typename Store<S>::C *d, typename Store<S>::C r,
+                                              typename Store<S>::C x, typename Store<S>::C y,
+                                              typename Store<S>::C z, double tau, S *fcol, I n, I i)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    if constexpr (COLL == MT_COLL_LBGK) {
+        if constexpr (!T::shifted) {
+#pragma unroll
+            for (int k = 0; k < Q; ++k) {
+                const double fk = d[k];
+                fcol[(I)k * n + i] = fk - (fk - feq_ref<Q>(k, r, x, y, z)) / tau;
+            }
+        } else {
+            const float om = (float)(1.0 / tau);
+            const float uu = 1.5f * (x * x + y * y + z * z);
+#pragma unroll
+            for (int k = 0; k < Q; ++k) {
+                const float eu = ex(k) * x + ey(k) * y + ez(k) * z;
+                const float wk = (float)w<Q>(k);
+                // deviations: feq - w = w ((rho - 1) + rho (3 eu + 4.5 eu^2 - 1.5 u^2))
+                const float dfeq = wk * ((r - 1.f) + r * (3.f * eu + 4.5f * eu * eu - uu));
+                const float s = d[k] - wk;
+                T::st(fcol, (I)k * n + i, fmaf(om, dfeq - s, s));
+            }
+        }
+    } else if constexpr (Q == 27) {
+        C o[27];
+        cumulant_collide<C>(d, r, x, y, z, (C)(1. / tau), o);
+#pragma unroll
+        for (int k = 0; k < 27; ++k) T::st(fcol, (I)k * n + i, stored_of<S, 27>(o[k], k));
+    }
+}
+
 // calculateMacros(level) + Collision_LBGK::collide / Collision_Cumulant::collide
 // on lat_f then overlap_F2C (Collision_Manager.cpp:13-53, Collision_Cumulant.cpp:22-159)
 template <int Q, class S, int COLL>
@@ -90,32 +130,7 @@ __global__ void k_collide(const int32_t *list, int64_t nl, int64_t n, double tau
     u[i] = x;
     u[n + i] = y;
     u[2 * n + i] = z;
-    if constexpr (COLL == MT_COLL_LBGK) {
-        if constexpr (!T::shifted) {
-#pragma unroll
-            for (int k = 0; k < Q; ++k) {
-                const double fk = d[k];
-                fcol[k * n + i] = fk - (fk - feq_ref<Q>(k, r, x, y, z)) / tau;
-            }
-        } else {
-            const float om = (float)(1.0 / tau);
-            const float uu = 1.5f * (x * x + y * y + z * z);
-#pragma unroll
-            for (int k = 0; k < Q; ++k) {
-                const float eu = ex(k) * x + ey(k) * y + ez(k) * z;
-                const float wk = (float)w<Q>(k);
-                // deviations: feq - w = w ((rho - 1) + rho (3 eu + 4.5 eu^2 - 1.5 u^2))
-                const float dfeq = wk * ((r - 1.f) + r * (3.f * eu + 4.5f * eu * eu - uu));
-                const float s = d[k] - wk;
-                T::st(fcol, k * n + i, fmaf(om, dfeq - s, s));
-            }
-        }
-    } else if constexpr (Q == 27) {
-        C o[27];
-        cumulant_collide<C>(d, r, x, y, z, (C)(1. / tau), o);
-#pragma unroll
-        for (int k = 0; k < 27; ++k) T::st(fcol, k * n + i, stored_of<S, 27>(o[k], k));
-    }
+    collide_store<Q, S, COLL>(d, r, x, y, z, tau, fcol, n, i);
 }
 
 // fcol = f on overlap_C2F (Collision_Manager.cpp:45-52)
@@ -146,31 +161,39 @@ __global__ void k_stream(const int32_t *list, int64_t nl, int64_t n, int textboo
     }
 }
 
-// AMR_transDDF_explosion (LBM_Manager.cpp:1059-1129)
+// AMR_transDDF_explosion (LBM_Manager.cpp:1059-1129), eight threads per
+// coarse source cell, one per child: each computes the (identical) rescaled
+// populations and writes its own child, so the eight children of a source
+// (consecutive in key order) take one contiguous store per direction.
+// With a second post-collision buffer (fused schedule) the children of ghost
+// F2C cells (sources from nf2c on) are written to both: nothing else writes
+// them, and the reference keeps them over the second substep.
 template <int Q, class S>
-__global__ void k_explosion(const int32_t *src, const int32_t *child, int64_t ns, int64_t nc, const S *cfcol,
-                            int64_t nf, S *ffcol, double scale)
+__global__ void k_explosion(const int32_t *__restrict__ src, const int32_t *__restrict__ child, int64_t ns,
+                            int64_t nc, const S *__restrict__ cfcol, int64_t nf, S *__restrict__ ffcol, double scale,
+                            S *__restrict__ ffcol2, int64_t nf2c)
 {
     using T = Store<S>;
     using C = typename T::C;
-    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t j = t >> 3;
+    const int m = (int)(t & 7);
     if (j >= ns) return;
+    const int32_t ch = child[(int64_t)m * ns + j];
+    if (ch < 0) return;
     const int64_t i = src[j];
     C d[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::ld(cfcol, k * nc + i), k);
     C r, x, y, z;
     macros_g<Q, C>(d, r, x, y, z);
-    int32_t ch[8];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) ch[m] = child[(int64_t)m * ns + j];
+    const bool both = ffcol2 && j >= nf2c;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
         const C v = stored_of<S, Q>(fe + (C)scale * (d[k] - fe), k);
-#pragma unroll
-        for (int m = 0; m < 8; ++m)
-            if (ch[m] >= 0) T::st(ffcol, k * nf + ch[m], v);
+        T::st(ffcol, k * nf + ch, v);
+        if (both) T::st(ffcol2, k * nf + ch, v);
     }
 }
 
@@ -271,25 +294,25 @@ __global__ void k_bc_inout(const int32_t *list, int64_t nl, int east, int64_t n,
     }
 }
 
-// SinglePointInterpolation::treat (ComplexBoundary_Manager.cpp:43-225):
-// wall links by Filippova-Haenel or distance-weighted interpolation, free
-// links by plain pull, density clamp, eight multi-direct-forcing sweeps
-// (each cell only touches its own populations: the sweeps run in registers).
+// SinglePointInterpolation::treat (ComplexBoundary_Manager.cpp:43-225) on
+// one cell: wall links by Filippova-Haenel or distance-weighted
+// interpolation, free links by plain pull, density clamp, eight
+// multi-direct-forcing sweeps (each cell only touches its own populations:
+// the sweeps run in registers).  g receives the new f, (fx, fy, fz) the
+// cell's momentum-exchange force.
 template <int Q, int FH, class S>
-__global__ void k_ib_treat(const int32_t *list, int64_t nl, int64_t n, const int32_t *disrow, const double *dis,
-                           const int32_t *nbr, const S *fcol, const typename Store<S>::C *rho, S *f, double *force)
+__device__ __forceinline__ void ib_cell(int64_t i, int64_t n, const double *dr, const int32_t *nbr, const S *fcol,
+                                        typename Store<S>::C rho_b, typename Store<S>::C *g,
+                                        typename Store<S>::C &fx, typename Store<S>::C &fy,
+                                        typename Store<S>::C &fz)
 {
     using T = Store<S>;
     using C = typename T::C;
-    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (j >= nl) return;
-    const int64_t i = list[j];
-    const double *dr = dis + (int64_t)disrow[i] * (Q - 1);
-    const C rho_b = rho[i];
     auto FC = [&](int k, int64_t idx) { return full_of<S, Q>(T::ld(fcol, k * n + idx), k); };
-    C g[Q];
     g[0] = FC(0, i);
-    C fx = 0, fy = 0, fz = 0;
+    fx = 0;
+    fy = 0;
+    fz = 0;
 #pragma unroll
     for (int k = 1; k < Q; ++k) {
         const C dd = (C)dr[inv(k) - 1];
@@ -356,11 +379,226 @@ __global__ void k_ib_treat(const int32_t *list, int64_t nl, int64_t n, const int
         }
         g[0] += adj;
     }
+}
+
+template <int Q, int FH, class S>
+__global__ void k_ib_treat(const int32_t *list, int64_t nl, int64_t n, const int32_t *disrow, const double *dis,
+                           const int32_t *nbr, const S *fcol, const typename Store<S>::C *rho, S *f, double *force)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    const double *dr = dis + (int64_t)disrow[i] * (Q - 1);
+    C g[Q], fx, fy, fz;
+    ib_cell<Q, FH, S>(i, n, dr, nbr, fcol, rho[i], g, fx, fy, fz);
 #pragma unroll
     for (int k = 0; k < Q; ++k) T::st(f, k * n + i, stored_of<S, Q>(g[k], k));
     force[j] = (double)fx;
     force[nl + j] = (double)fy;
     force[2 * nl + j] = (double)fz;
+}
+
+// ---- fused schedule ---------------------------------------------------------
+// The level keeps two post-collision buffers.  A substep streams from the
+// current one (fcol) and, in the same pass, runs the next substep's
+// calculateMacros + collide on the streamed f, writing fnext.  Between the
+// stream of one substep and the collision of the next the reference touches a
+// lat_f cell's f only through treat() (IB cells, fused below) and a C2F
+// cell's fcol only through the copy fcol = f, so the lookahead collision sees
+// the same f as the reference's and gives the same populations.
+
+// gather of one cell's streamed populations from the source indices src[k]
+// (k >= 1; -1 = no neighbour): every load is issued before any store (f and
+// fcol are distinct buffers), so the Q - 1 gathers overlap.  A missing
+// neighbour keeps f (read back from f, not written).
+template <int Q, class S>
+__device__ __forceinline__ void pull_src(int64_t i, int64_t n, const int32_t *src, const S *__restrict__ fcol,
+                                         S *__restrict__ f, S *v)
+{
+    v[0] = fcol[i];
+#pragma unroll
+    for (int k = 1; k < Q; ++k) v[k] = src[k] >= 0 ? fcol[k * n + src[k]] : f[k * n + i];
+    f[i] = v[0];
+#pragma unroll
+    for (int k = 1; k < Q; ++k)
+        if (src[k] >= 0) f[k * n + i] = v[k];
+}
+
+// pull_src with 32-bit element offsets (Q * n < 2^32)
+template <int Q, class S>
+__device__ __forceinline__ void pull_src32(uint32_t i, uint32_t n, const int32_t *src, const S *__restrict__ fcol,
+                                           S *__restrict__ f, S *v)
+{
+    v[0] = fcol[i];
+#pragma unroll
+    for (int k = 1; k < Q; ++k)
+        v[k] = src[k] >= 0 ? fcol[(uint32_t)k * n + (uint32_t)src[k]] : f[(uint32_t)k * n + i];
+    f[i] = v[0];
+#pragma unroll
+    for (int k = 1; k < Q; ++k)
+        if (src[k] >= 0) f[(uint32_t)k * n + i] = v[k];
+}
+
+template <int Q, class S>
+__device__ __forceinline__ void pull_cell(int64_t i, int64_t n, int textbook, const int32_t *__restrict__ nbr,
+                                          const S *__restrict__ fcol, S *__restrict__ f, S *v)
+{
+    int32_t src[Q];
+#pragma unroll
+    for (int k = 1; k < Q; ++k) src[k] = __ldg(nbr + (int64_t)((textbook ? inv(k) : k) - 1) * n + i);
+    pull_src<Q, S>(i, n, src, fcol, f, v);
+}
+
+// ABPatternPull::stream then the next collide, on lat_f cells that are not IB
+// cells.
+template <int Q, class S, int COLL>
+__global__ void k_pull_collide(const int32_t *__restrict__ list, int64_t nl, int64_t n, int textbook,
+                               const int32_t *__restrict__ nbr, const S *__restrict__ fcol, S *__restrict__ f,
+                               S *__restrict__ fnext, double tau)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    C d[Q];
+    {
+        S v[Q];
+        pull_cell<Q, S>(i, n, textbook, nbr, fcol, f, v);
+#pragma unroll
+        for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::cv(v[k]), k);
+    }
+    C r, x, y, z;
+    macros_g<Q, C>(d, r, x, y, z);
+    collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i);
+}
+
+// stream on overlap_C2F cells and their next collision, fcol = f
+// (Collision_Manager.cpp:45-52)
+template <int Q, class S>
+__global__ void k_pull_copy(const int32_t *__restrict__ list, int64_t nl, int64_t n, int textbook,
+                            const int32_t *__restrict__ nbr, const S *__restrict__ fcol, S *__restrict__ f,
+                            S *__restrict__ fnext)
+{
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    S v[Q];
+    pull_cell<Q, S>(i, n, textbook, nbr, fcol, f, v);
+#pragma unroll
+    for (int k = 0; k < Q; ++k) fnext[k * n + i] = v[k];
+}
+
+// The fused pass over 4x4x4 bricks (one brick per 64 threads, two per
+// block).  The block first resolves the cell index of every position of each
+// brick's 6x6x6 neighbourhood into shared memory (from the start and
+// occupancy mask of the brick and its 26 neighbours), so a cell's Q - 1
+// source indices are shared-memory reads at fixed offsets instead of rows of
+// the neighbour table.  The brick neighbours come from
+// Morton_Assist::find_neighbor on a corner cell, so each computed neighbour
+// is the one the reference's find() returns.
+template <int Q, class S, int COLL>
+__global__ void __launch_bounds__(128) k_brick_step(int64_t nb, const int32_t *__restrict__ bstart,
+                                                    const uint64_t *__restrict__ bmask,
+                                                    const int32_t *__restrict__ bnbr,
+                                                    const uint8_t *__restrict__ bcls, int64_t n, int textbook,
+                                                    const S *__restrict__ fcol, S *__restrict__ f,
+                                                    S *__restrict__ fnext, double tau)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    __shared__ int32_t s_start[2][27];
+    __shared__ uint64_t s_mask[2][27];
+    __shared__ int32_t s_idx[2][216];
+    if (threadIdx.x < 54) {
+        const int bb = threadIdx.x / 27, sl = threadIdx.x - 27 * bb;
+        const int64_t b = 2 * (int64_t)blockIdx.x + bb;
+        const int32_t nbk = b < nb ? __ldg(bnbr + 27 * b + sl) : -1;
+        s_start[bb][sl] = nbk >= 0 ? __ldg(bstart + nbk) : 0;
+        s_mask[bb][sl] = nbk >= 0 ? __ldg(bmask + nbk) : 0ull;
+    }
+    __syncthreads();
+    const int lb = threadIdx.x >> 6, m = threadIdx.x & 63;
+    // halo position h = hx + 6 hy + 36 hz holds the cell at local (hx-1, hy-1, hz-1)
+    for (int h = m; h < 216; h += 64) {
+        const int nx = h % 6 - 1, ny = (h / 6) % 6 - 1, nz = h / 36 - 1;
+        const int sl = ((nx >> 2) + 1) + 3 * ((ny >> 2) + 1) + 9 * ((nz >> 2) + 1);
+        const int ax = nx & 3, ay = ny & 3, az = nz & 3;
+        const int mm = (ax & 1) | ((ax & 2) << 2) | ((ay & 1) << 1) | ((ay & 2) << 3) | ((az & 1) << 2) |
+                       ((az & 2) << 4);
+        const uint64_t nm = s_mask[lb][sl];
+        s_idx[lb][h] = ((nm >> mm) & 1ull) ? s_start[lb][sl] + __popcll(nm & ((1ull << mm) - 1ull)) : -1;
+    }
+    __syncthreads();
+    const int64_t b = 2 * (int64_t)blockIdx.x + lb;
+    if (b >= nb) return;
+    const int lx = (m & 1) | ((m >> 2) & 2), ly = ((m >> 1) & 1) | ((m >> 3) & 2),
+              lz = ((m >> 2) & 1) | ((m >> 4) & 2);
+    const int base = (lx + 1) + 6 * (ly + 1) + 36 * (lz + 1);
+    const int32_t i = s_idx[lb][base];
+    if (i < 0) return;
+    const int cls = __ldg(bcls + 64 * b + m);
+    if (!cls) return;
+    int32_t src[Q];
+#pragma unroll
+    for (int k = 1; k < Q; ++k) {
+        const int off = ex(k) + 6 * ey(k) + 36 * ez(k);
+        src[k] = s_idx[lb][base + (textbook ? -off : off)];
+    }
+    const uint32_t n32 = (uint32_t)n, i32 = (uint32_t)i;
+    S v[Q];
+    pull_src32<Q, S>(i32, n32, src, fcol, f, v);
+    if (cls == 2) {
+#pragma unroll
+        for (int k = 0; k < Q; ++k) fnext[(uint32_t)k * n32 + i32] = v[k];
+        return;
+    }
+    C d[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::cv(v[k]), k);
+    C r, x, y, z;
+    macros_g<Q, C>(d, r, x, y, z);
+    collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n32, i32);
+}
+
+// treat() on the IB cells of the finest level, then their next collision.
+// rho_b is the density calculateMacros(level) gives at the start of the
+// substep: the macros of the cell's f before this treat.
+template <int Q, int FH, class S, int COLL>
+__global__ void k_ib_collide(const int32_t *list, int64_t nl, int64_t n, const int32_t *disrow, const double *dis,
+                             const int32_t *nbr, const S *fcol, S *f, S *fnext, double tau, double *force)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    const double *dr = dis + (int64_t)disrow[i] * (Q - 1);
+    C g[Q], fx, fy, fz;
+    {
+#pragma unroll
+        for (int k = 0; k < Q; ++k) g[k] = full_of<S, Q>(T::ld(f, k * n + i), k);
+        C r, x, y, z;
+        macros_g<Q, C>(g, r, x, y, z);
+        ib_cell<Q, FH, S>(i, n, dr, nbr, fcol, r, g, fx, fy, fz);
+    }
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const C st = stored_of<S, Q>(g[k], k);
+        T::st(f, k * n + i, st);
+        // the next collision reads the stored value
+        S sv;
+        T::st(&sv, 0, st);
+        g[k] = full_of<S, Q>(T::cv(sv), k);
+    }
+    force[j] = (double)fx;
+    force[nl + j] = (double)fy;
+    force[2 * nl + j] = (double)fz;
+    C r, x, y, z;
+    macros_g<Q, C>(g, r, x, y, z);
+    collide_store<Q, S, COLL>(g, r, x, y, z, tau, fnext, n, i);
 }
 
 // fixed-order reduction of the per-cell IB force into the accumulator
@@ -545,8 +783,9 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         if (l < 1 || !lv.nexpl) return MT_OK;
         Level &cl = c.lv[l - 1];
         const double scale = (2.0 * c.d.tau[l]) / c.d.tau[l - 1];
-        k_explosion<Q, S><<<grid_for(lv.nexpl, B), B, 0, s>>>(lv.expl_src, lv.expl_child, lv.nexpl, cl.n, A::fcol(cl),
-                                                               n, A::fcol(lv), scale);
+        k_explosion<Q, S><<<grid_for(8 * lv.nexpl, B), B, 0, s>>>(lv.expl_src, lv.expl_child, lv.nexpl, cl.n, A::fcol(cl),
+                                                               n, A::fcol(lv), scale, (S *)lv.fcol_alt,
+                                                               lv.nexpl_f2c);
         MT_LAUNCHED(ctx);
         return MT_OK;
     }
@@ -617,6 +856,128 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         MT_LAUNCHED(ctx);
         k_force_reduce<<<1, 256, 0, s>>>(partial, nb, c.force_acc);
         MT_LAUNCHED(ctx);
+        return MT_OK;
+    }
+    case PH_F2C_COLLIDE:
+        // the F2C share of collide(level) in the fused schedule: their f comes from coalescence
+        if (lv.nlist[1]) {
+            if (c.d.collision == MT_COLL_LBGK) {
+                k_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nlist[1], B), B, 0, s>>>(
+                    lv.list[1], lv.nlist[1], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv));
+            } else {
+                if constexpr (Q == 27)
+                    k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nlist[1], 64), 64, 0, s>>>(
+                        lv.list[1], lv.nlist[1], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv));
+            }
+            MT_LAUNCHED(ctx);
+        }
+        return MT_OK;
+    case PH_PRIME:
+        // lookahead of the fused schedule from the current f: the second
+        // buffer gets every cell's fcol, then the collision of lat_f and the
+        // copy of C2F (the first collide(level) of the next substep)
+        if (!n) return MT_OK;
+        MT_CUDA(ctx, cudaMemcpyAsync(lv.fcol_alt, lv.fcol, sizeof(S) * Q * n, cudaMemcpyDeviceToDevice, s));
+        if (lv.nlist[0]) {
+            if (c.d.collision == MT_COLL_LBGK) {
+                k_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nlist[0], B), B, 0, s>>>(
+                    lv.list[0], lv.nlist[0], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt);
+            } else {
+                if constexpr (Q == 27)
+                    k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nlist[0], 64), 64, 0, s>>>(
+                        lv.list[0], lv.nlist[0], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt);
+            }
+            MT_LAUNCHED(ctx);
+        }
+        if (lv.nlist[2]) {
+            k_copy_fcol<Q, S><<<grid_for(lv.nlist[2], B), B, 0, s>>>(lv.list[2], lv.nlist[2], n, A::f(lv),
+                                                                      (S *)lv.fcol_alt);
+            MT_LAUNCHED(ctx);
+        }
+        return MT_OK;
+    case PH_PULL_COLLIDE: {
+        // stream(level) of this substep fused with collide(level) of the next,
+        // reading fcol and writing f and fcol_alt; treat() on the finest level
+        // (its cells are disjoint from the fused pass: on the side stream when
+        // the case has one, overlapping the pass)
+        const int L = c.d.max_level;
+        const bool ib_level = l == L && l > 0;
+        const int tb = c.d.stream_convention;
+        cudaStream_t is = s;
+        if (ib_level && lv.nib && c.side) {
+            MT_CUDA(ctx, cudaEventRecord(c.ev_fork, s));
+            MT_CUDA(ctx, cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+            is = c.side;
+        }
+        if (ib_level) {
+            if (!lv.nib) {
+                k_force_tick<<<1, 1, 0, s>>>(c.force_acc);
+                MT_LAUNCHED(ctx);
+            } else {
+                const double tau = c.d.tau[l];
+                auto ib = [&](auto fh, auto coll) {
+                    constexpr int FH = decltype(fh)::value, COLL = decltype(coll)::value;
+                    k_ib_collide<Q, FH, S, COLL><<<grid_for(lv.nib, 64), 64, 0, is>>>(
+                        lv.iblist, lv.nib, n, lv.disrow, c.dis, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt, tau,
+                        c.ib_force);
+                };
+                using I0 = std::integral_constant<int, 0>;
+                using I1 = std::integral_constant<int, 1>;
+                using LB = std::integral_constant<int, MT_COLL_LBGK>;
+                using CU = std::integral_constant<int, MT_COLL_CUMULANT>;
+                if (c.d.collision == MT_COLL_LBGK) {
+                    if (c.d.ib_method == MT_IB_FH) ib(I1{}, LB{}); else ib(I0{}, LB{});
+                } else {
+                    if constexpr (Q == 27) {
+                        if (c.d.ib_method == MT_IB_FH) ib(I1{}, CU{}); else ib(I0{}, CU{});
+                    }
+                }
+                MT_LAUNCHED(ctx);
+                const unsigned nb = grid_for(lv.nib, 256);
+                double *partial = c.ib_force + 3 * lv.nib;
+                k_force_partial<<<nb, 256, 0, is>>>(c.ib_force, lv.nib, partial);
+                MT_LAUNCHED(ctx);
+                k_force_reduce<<<1, 256, 0, is>>>(partial, nb, c.force_acc);
+                MT_LAUNCHED(ctx);
+            }
+        }
+        if (lv.bricks) {
+            const unsigned g = grid_for(lv.nbrick, 2);
+            if (c.d.collision == MT_COLL_LBGK) {
+                k_brick_step<Q, S, MT_COLL_LBGK><<<g, 128, 0, s>>>(lv.nbrick, lv.bstart, lv.bmask, lv.bnbr, lv.bcls,
+                                                                   n, tb, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
+                                                                   c.d.tau[l]);
+            } else {
+                if constexpr (Q == 27)
+                    k_brick_step<Q, S, MT_COLL_CUMULANT><<<g, 128, 0, s>>>(lv.nbrick, lv.bstart, lv.bmask, lv.bnbr,
+                                                                           lv.bcls, n, tb, A::fcol(lv), A::f(lv),
+                                                                           (S *)lv.fcol_alt, c.d.tau[l]);
+            }
+            MT_LAUNCHED(ctx);
+        } else {
+            if (lv.nfused) {
+                if (c.d.collision == MT_COLL_LBGK) {
+                    k_pull_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nfused, B), B, 0, s>>>(
+                        lv.fused_list, lv.nfused, n, tb, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
+                        c.d.tau[l]);
+                } else {
+                    if constexpr (Q == 27)
+                        k_pull_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nfused, 64), 64, 0, s>>>(
+                            lv.fused_list, lv.nfused, n, tb, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
+                            c.d.tau[l]);
+                }
+                MT_LAUNCHED(ctx);
+            }
+            if (lv.nlist[2]) {
+                k_pull_copy<Q, S><<<grid_for(lv.nlist[2], B), B, 0, s>>>(lv.list[2], lv.nlist[2], n, tb, lv.nbr,
+                                                                          A::fcol(lv), A::f(lv), (S *)lv.fcol_alt);
+                MT_LAUNCHED(ctx);
+            }
+        }
+        if (is != s) {
+            MT_CUDA(ctx, cudaEventRecord(c.ev_join, is));
+            MT_CUDA(ctx, cudaStreamWaitEvent(s, c.ev_join, 0));
+        }
         return MT_OK;
     }
     }

@@ -85,6 +85,7 @@ int phase_call(mt_ctx *h, int32_t id, int phase, int level)
     if (rc) return rc;
     if (c->dense) return set_err(h->c, MT_ERR_STATE, "per-phase calls need a multi-level case (use mt_step)");
     if (!c->built) return set_err(h->c, MT_ERR_STATE, "case not built");
+    c->primed = false;  // the fused schedule's lookahead no longer matches f
     return amr_phase(h->c, *c, phase, level);
 }
 
@@ -359,6 +360,7 @@ int mt_case_init_equilibrium(mt_ctx *h, int32_t id, double rho0, const double *u
             using S = std::remove_pointer_t<decltype(tag)>;
             return DenseOps<S>::init(ctx, *c, nullptr, nullptr, nullptr, nullptr, rho0, u0);
         });
+    c->primed = false;
     return amr_init_equilibrium(ctx, *c, rho0, u0);
 }
 
@@ -410,6 +412,7 @@ int mt_case_set_populations(mt_ctx *h, int32_t id, int32_t level, const double *
         cudaFreeAsync(d, ctx.stream);
         return rc;
     }
+    c->primed = false;
     return amr_set(ctx, *c, level, f, fcol);
 }
 
@@ -528,6 +531,7 @@ int mt_lbm_kernel(mt_ctx *h, int32_t id, int32_t level)
     Ctx &ctx = h->c;
     if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "LBMkernel needs a built multi-level case");
     if (level < 0 || level > c->d.max_level) return set_err(ctx, MT_ERR_ARG, "bad level");
+    c->primed = false;
     return amr_lbm_kernel(ctx, *c, level);
 }
 
@@ -556,6 +560,31 @@ int mt_step(mt_ctx *h, int32_t id, int32_t n)
     }
     rc = amr_step(ctx, *c, n);
     if (rc) return rc;
+    return MT_OK;
+}
+
+int mt_case_set_schedule(mt_ctx *h, int32_t id, int32_t schedule)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense) return set_err(ctx, MT_ERR_STATE, "the dense path has a single (fused) schedule");
+    if (schedule != MT_SCHED_PHASES && schedule != MT_SCHED_FUSED && schedule != MT_SCHED_FUSED_LISTS)
+        return set_err(ctx, MT_ERR_ARG, "schedule must be MT_SCHED_PHASES, MT_SCHED_FUSED or MT_SCHED_FUSED_LISTS");
+    const bool bricks = schedule == MT_SCHED_FUSED;
+    if (schedule == MT_SCHED_PHASES) {
+        c->primed = false;
+        c->schedule = MT_SCHED_PHASES;
+        return MT_OK;
+    }
+    if (c->schedule == MT_SCHED_PHASES || bricks != c->use_bricks) {
+        c->primed = false;
+        // the fused graphs bake in the pass each level uses
+        amr_drop_fused(*c);
+    }
+    c->use_bricks = bricks;
+    c->schedule = MT_SCHED_FUSED;
     return MT_OK;
 }
 

@@ -46,6 +46,23 @@ struct Level {
     int32_t *disrow = nullptr; // row in the dis table or -1
     int32_t *nbr = nullptr;    // [(Q-1) * n]: index of the cell at key + e_k (k >= 1) or -1
     void *f = nullptr, *fcol = nullptr;  // [Q * n] populations in the case's storage type
+    // fused schedule: the second post-collision buffer (the next substep's fcol,
+    // swapped with fcol at each substep) and the lat_f cells it collides (IB
+    // cells of the finest level excluded, they have their own kernel)
+    void *fcol_alt = nullptr;
+    int32_t *fused_list = nullptr; int64_t nfused = 0;
+    // 4x4x4 Morton bricks of the level's key set (fused schedule): a brick's
+    // cells are contiguous in key order, so a cell at local Morton index m is
+    // stored iff bit m of the brick's mask is set, at index
+    // start + popcount(mask & (2^m - 1)).  bnbr[27 * b + s] is the brick at
+    // offset (s % 3 - 1, s / 3 % 3 - 1, s / 9 - 1) or -1; bcls[64 * b + m] is
+    // the cell's work in the fused pass (0 none, 1 stream + collide, 2 stream + copy).
+    bool bricks = false;
+    int64_t nbrick = 0;
+    int32_t *bstart = nullptr;
+    uint64_t *bmask = nullptr;
+    int32_t *bnbr = nullptr;
+    uint8_t *bcls = nullptr;
     void *rho = nullptr, *u = nullptr;   // [n], [3 * n] macroscopic fields (double, or float for reduced storage)
     int32_t *list[kNumSets] = {};
     int64_t nlist[kNumSets] = {};
@@ -84,9 +101,24 @@ struct Case {
     bool a_is_fcol = false;           // false: A holds post-stream f; true: A holds post-collision fcol
     double *bc_tmp = nullptr;         // scratch of the boundary sweep
     int dense_block = 256;            // threads per block of the fused kernel (autotuned)
-    // captured coarse step
+    // captured coarse step of the phase schedule (recorded with level 0's
+    // post-collision buffer in parity graph_par0)
     cudaGraphExec_t graph = nullptr;
     int64_t graph_launches = 0;
+    int graph_par0 = 0;
+    // fused schedule: one graph per parity of level 0's buffers (levels >= 1
+    // swap an even number of times per coarse step), and whether the
+    // lookahead buffers hold the collision of the current f
+    int schedule = MT_SCHED_PHASES;
+    bool use_bricks = true;  // fused pass over 4x4x4 bricks where a level allows it (else cell lists)
+    bool primed = false;
+    int par0 = 0;
+    cudaGraphExec_t fgraph[2] = {nullptr, nullptr};
+    int64_t fgraph_launches[2] = {0, 0};
+    // second stream of the fused schedule: the IB cells' treat + collision
+    // overlaps the finest level's fused pass (disjoint cells)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 struct Ctx {
@@ -123,6 +155,8 @@ template <class S> struct AmrOps {
     static int guard(Ctx &ctx, Case &c);
 };
 void amr_free(Case &c);
+// forget the fused schedule's graphs and brick tables (rebuilt at the next fused step)
+void amr_drop_fused(Case &c);
 
 // dense uniform path, one explicit instantiation per storage type
 // (mt_dense_f64.cu builds the FP64 one without FMA contraction)

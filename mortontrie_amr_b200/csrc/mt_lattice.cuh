@@ -10,6 +10,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #ifndef MT_HD
 #define MT_HD __host__ __device__ __forceinline__
@@ -189,9 +190,16 @@ template <int Q, class R> MT_HD void macros_g(const R *d, R &rho, R &ux, R &uy, 
     }
     const R s = (r > R(-1e-6) && r < R(1e-6)) ? ((r < R(0)) ? R(-1e-6) : R(1e-6)) : r;
     rho = r;
-    ux = vx / s;
-    uy = vy / s;
-    uz = vz / s;
+    if constexpr (std::is_same<R, double>::value) {
+        ux = vx / s;
+        uy = vy / s;
+        uz = vz / s;
+    } else {
+        const R is = R(1) / s;
+        ux = vx * is;
+        uy = vy * is;
+        uz = vz * is;
+    }
 }
 template <int Q, class R> MT_HD R feq_g(int i, R rho, R ux, R uy, R uz)
 {
@@ -209,9 +217,20 @@ template <int Q, class R> MT_HD R feq_heluo_g(int i, R rho, R ux, R uy, R uz)
 template <class R>
 MT_HD void chim_back(R a0, R a1, R a2, R v, R v2, R &pn, R &pz, R &pp)
 {
-    pz = a0 * (1 - v2) - a1 * 2 * v - a2;
-    pn = (a0 * (v2 - v) + a1 * (2 * v - 1) + a2) * R(0.5);
-    pp = (a0 * (v2 + v) + a1 * (2 * v + 1) + a2) * R(0.5);
+    if constexpr (std::is_same<R, double>::value) {
+        // the reference's expression order (Collision_Cumulant.cpp:486-651)
+        pz = a0 * (1 - v2) - a1 * 2 * v - a2;
+        pn = (a0 * (v2 - v) + a1 * (2 * v - 1) + a2) * R(0.5);
+        pp = (a0 * (v2 + v) + a1 * (2 * v + 1) + a2) * R(0.5);
+    } else {
+        // the same polynomials with shared terms: t = a0 v^2 + 2 v a1 + a2,
+        // h = (a0 v + a1) / 2; pz = a0 - t, pp = t / 2 + h, pn = t / 2 - h
+        const R t = a0 * v2 + (2 * v * a1 + a2);
+        const R h = R(0.5) * (a0 * v + a1);
+        pz = a0 - t;
+        pp = R(0.5) * t + h;
+        pn = R(0.5) * t - h;
+    }
 }
 
 // D3Q27 cumulant collision (Collision_Cumulant.cpp:320-652): central moments
@@ -226,9 +245,35 @@ template <class R>
 MT_HD void cumulant_collide(const R *f, R rho, R ux, R uy, R uz, R omega1, R *out)
 {
     R m[27];
+#define MM(a, b, c) m[(a) + 3 * (b) + 9 * (c)]
+    if constexpr (!std::is_same<R, double>::value) {
+        // reduced precision: the same central moments by three chimera passes
+        // (x, then y, then z lines of three), a quarter of the operations
+        R g[27];
+#pragma unroll
+        for (int i = 0; i < 27; ++i) g[(ex(i) + 1) + 3 * (ey(i) + 1) + 9 * (ez(i) + 1)] = f[i];
+        const R v[3] = {ux, uy, uz};
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            const int st = ax == 0 ? 1 : (ax == 1 ? 3 : 9);
+            const R u = v[ax], u2 = u * u;
+#pragma unroll
+            for (int line = 0; line < 9; ++line) {
+                // base index of the line: the two other axes' positions
+                const int o1 = line % 3, o2 = line / 3;
+                const int bidx = ax == 0 ? 3 * o1 + 9 * o2 : (ax == 1 ? o1 + 9 * o2 : o1 + 3 * o2);
+                const R fm = g[bidx], f0 = g[bidx + st], fp = g[bidx + 2 * st];
+                const R k0 = fm + f0 + fp, d1 = fp - fm, s1 = fp + fm;
+                g[bidx] = k0;
+                g[bidx + st] = d1 - u * k0;
+                g[bidx + 2 * st] = s1 - 2 * u * d1 + u2 * k0;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 27; ++i) m[i] = g[i];
+    } else {
 #pragma unroll
     for (int i = 0; i < 27; ++i) m[i] = 0;
-#define MM(a, b, c) m[(a) + 3 * (b) + 9 * (c)]
 #pragma unroll
     for (int i = 0; i < 27; ++i) {
         const R cx = ex(i) - ux, cy = ey(i) - uy, cz = ez(i) - uz, fi = f[i];
@@ -259,6 +304,7 @@ MT_HD void cumulant_collide(const R *f, R rho, R ux, R uy, R uz, R omega1, R *ou
         MM(2, 1, 2) += cx * cx * cy * cz * cz * fi;
         MM(1, 2, 2) += cx * cy * cy * cz * cz * fi;
         MM(2, 2, 2) += cx * cx * cy * cy * cz * cz * fi;
+    }
     }
     R c200 = MM(2, 0, 0), c020 = MM(0, 2, 0), c002 = MM(0, 0, 2);
     R c110 = MM(1, 1, 0), c101 = MM(1, 0, 1), c011 = MM(0, 1, 1);

@@ -2,6 +2,7 @@
 //
 // double: unshifted populations, FP64 arithmetic (the reference's precision).
 // float / half / bfloat16: the deviation f - w_q is stored, arithmetic is FP32.
+// cv converts one stored value to the compute type.
 // Index type I of ld/st: uint32_t while an array fits 2^32 elements (one wide
 // multiply-add per address), int64_t beyond.
 #pragma once
@@ -19,6 +20,7 @@ template <> struct Store<double> {
     static constexpr bool shifted = false;
     static constexpr int bytes = 8;
     template <class I> __device__ static __forceinline__ double ld(const double *p, I i) { return __ldg(p + i); }
+    __device__ static __forceinline__ double cv(double v) { return v; }
     template <class I> __device__ static __forceinline__ void st(double *p, I i, double v) { p[i] = v; }
 };
 template <> struct Store<float> {
@@ -26,6 +28,7 @@ template <> struct Store<float> {
     static constexpr bool shifted = true;
     static constexpr int bytes = 4;
     template <class I> __device__ static __forceinline__ float ld(const float *p, I i) { return __ldg(p + i); }
+    __device__ static __forceinline__ float cv(float v) { return v; }
     template <class I> __device__ static __forceinline__ void st(float *p, I i, float v) { p[i] = v; }
 };
 template <> struct Store<__half> {
@@ -36,6 +39,7 @@ template <> struct Store<__half> {
     {
         return __half2float(__ldg(p + i));
     }
+    __device__ static __forceinline__ float cv(__half v) { return __half2float(v); }
     template <class I> __device__ static __forceinline__ void st(__half *p, I i, float v) { p[i] = __float2half_rn(v); }
 };
 template <> struct Store<__nv_bfloat16> {
@@ -46,6 +50,7 @@ template <> struct Store<__nv_bfloat16> {
     {
         return __bfloat162float(__ldg(p + i));
     }
+    __device__ static __forceinline__ float cv(__nv_bfloat16 v) { return __bfloat162float(v); }
     template <class I> __device__ static __forceinline__ void st(__nv_bfloat16 *p, I i, float v)
     {
         p[i] = __float2bfloat16_rn(v);

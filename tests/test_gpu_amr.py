@@ -16,9 +16,9 @@ def ctx():
     c.close()
 
 
-def _device_case(ctx, case, init):
+def _device_case(ctx, case, init, schedule="phases"):
     from mortontrie_amr_b200.lbm import LBM_Manager
-    mgr = LBM_Manager(ctx, case)
+    mgr = LBM_Manager(ctx, case, schedule=schedule)
     if init is not None:
         for l, (keys, f) in enumerate(init):
             k, _ = mgr.keys(l)
@@ -185,3 +185,123 @@ def test_missing_child_is_reported(ctx):
     lv1["overlap_C2F"] = lv1["overlap_C2F"][5:]
     with pytest.raises(MTError, match="MT_ERR_MESH"):
         LBM_Manager(ctx, case)
+
+
+def _nested_small():
+    from mortontrie_amr_b200.case import nested_sphere_case
+    return nested_sphere_case(coarse=(48, 24, 24), max_level=2, center=(16, 12, 12), radius=2.0,
+                              half_widths=(4.0, 2.5), re=50.0)
+
+
+def _same_state(a, b, L):
+    for l in range(L + 1):
+        fa, ca = a.populations(l)
+        fb, cb = b.populations(l)
+        assert np.array_equal(fa, fb), (l, float(np.abs(fa - fb).max()))
+        assert np.array_equal(ca, cb), (l, float(np.abs(ca - cb).max()))
+        ra, ua = a.macros(l)
+        rb, ub = b.macros(l)
+        assert np.array_equal(ra, rb) and np.array_equal(ua, ub), l
+
+
+@pytest.mark.parametrize("schedule", ["fused", "fused_lists"])
+@pytest.mark.parametrize("which", ["cfg1_q19", "cumulant_q27", "golden_dw"])
+@pytest.mark.parametrize("steps", [1, 2, 5])
+def test_fused_schedule_fp64_equals_phases(ctx, which, steps, schedule):
+    """The fused schedule (stream of a substep in the same pass as the next
+    substep's collision, two post-collision buffers per level) leaves the
+    same FP64 state as the reference's phase order after every coarse step:
+    populations, macros and the IB force, bit for bit."""
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    if which == "cfg1_q19":
+        case = _cfg1_small()
+    elif which == "cumulant_q27":
+        case = _nested_small()
+    else:
+        _, case, _, _ = load_golden("sphere_q19_dw_l2")
+    a = LBM_Manager(ctx, case, "f64")
+    b = LBM_Manager(ctx, case, "f64", schedule=schedule)
+    a.fluidSimulate(steps)
+    b.fluidSimulate(steps)
+    ctx.synchronize()
+    _same_state(a, b, case.max_level)
+    fa, fb = a.force(), b.force()
+    assert fa[3] == fb[3] and np.array_equal(fa[:3], fb[:3]), (fa, fb)
+    # continue from the same state across a level-0 buffer parity change
+    a.fluidSimulate(3)
+    b.fluidSimulate(3)
+    ctx.synchronize()
+    _same_state(a, b, case.max_level)
+
+
+@pytest.mark.parametrize("schedule", ["fused", "fused_lists"])
+@pytest.mark.parametrize("name", sorted(GOLDEN_CASES))
+def test_fused_schedule_matches_goldens(ctx, name, schedule):
+    """The reference's golden populations through the fused schedule."""
+    spec, case, z, _ = load_golden(name)
+    mgr = _device_case(ctx, case, init_of(case, spec), schedule=schedule)
+    mgr.fluidSimulate(spec["steps"])
+    ctx.synchronize()
+    for l in range(case.max_level + 1):
+        _, tags = mgr.keys(l)
+        f, fcol = mgr.populations(l)
+        keep = (tags & TAG_BC) == 0
+        assert np.array_equal(f[:, keep], z[f"f{l}"][:, keep]), (name, l)
+        assert sha(fcol) == bytes(z[f"fcol_sha{l}"]), (name, l)
+    force = mgr.force()
+    ref = z["force"].sum(axis=0)
+    assert force[3] == ref[3]
+    if np.abs(ref[:3]).max() > 0:
+        assert rel_err(force[:3], ref[:3]) < 1e-12
+
+
+def test_fused_schedule_interleaved_with_phase_calls(ctx):
+    """Per-phase calls and population writes between fused steps act on the
+    current buffers; the next fused step recomputes its lookahead."""
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    case = _cfg1_small()
+    a = LBM_Manager(ctx, case, "f64")
+    b = LBM_Manager(ctx, case, "f64", schedule="fused")
+    for m in (a, b):
+        m.fluidSimulate(3)
+        m.LBMkernel(0)
+        m.calculateMacros()
+        m.fluidSimulate(2)
+    ctx.synchronize()
+    _same_state(a, b, case.max_level)
+    f, fcol = a.populations(1)
+    f = f * (1.0 + 1e-3)
+    for m in (a, b):
+        m.set_populations(1, f, fcol)
+        m.fluidSimulate(2)
+    ctx.synchronize()
+    _same_state(a, b, case.max_level)
+    for sched in ("fused_lists", "phases", "fused"):
+        b.set_schedule(sched)
+        a.fluidSimulate(2)
+        b.fluidSimulate(2)
+        ctx.synchronize()
+        _same_state(a, b, case.max_level)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+def test_fused_schedule_reduced_storage_vs_f64(ctx, storage):
+    """FP32 arithmetic on stored deviations under the fused schedule, against
+    the FP64 phase schedule: same tolerances as the phase schedule."""
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    case = _nested_small()
+    a = LBM_Manager(ctx, case, "f64")
+    b = LBM_Manager(ctx, case, storage, schedule="fused")
+    a.fluidSimulate(30)
+    b.fluidSimulate(30)
+    ctx.synchronize()
+    for l in range(case.max_level + 1):
+        _, ua = a.macros(l)
+        _, ub = b.macros(l)
+        _, tags = a.keys(l)
+        fluid = (tags & 1) != 0
+        err = np.linalg.norm(ub[:, fluid] - ua[:, fluid]) / np.linalg.norm(ua[:, fluid])
+        assert err < TOL_AMR[storage], (storage, l, err)
+    fa, fb = a.force(), b.force()
+    assert fa[3] == fb[3]
+    assert abs(fb[0] - fa[0]) / abs(fa[0]) < 10 * TOL_AMR[storage], (fa, fb)
