@@ -135,6 +135,28 @@ __global__ void k_brick_flags(const uint64_t *key, int64_t n, int shift, int32_t
     flag[i] = (i == 0 || (key[i] >> shift) != (key[i - 1] >> shift)) ? 1 : 0;
 }
 
+// cell index at position h of brick b's 6x6x6 neighbourhood (local
+// coordinates h % 6 - 1, h / 6 % 6 - 1, h / 36 - 1), or -1
+__global__ void k_brick_halo(int64_t nb, const int32_t *bstart, const unsigned long long *bmask,
+                             const int32_t *bnbr, int32_t *halo)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= 216 * nb) return;
+    const int64_t b = t / 216;
+    const int h = (int)(t - 216 * b);
+    const int nx = h % 6 - 1, ny = (h / 6) % 6 - 1, nz = h / 36 - 1;
+    const int sl = ((nx >> 2) + 1) + 3 * ((ny >> 2) + 1) + 9 * ((nz >> 2) + 1);
+    const int ax = nx & 3, ay = ny & 3, az = nz & 3;
+    const int mm = (ax & 1) | ((ax & 2) << 2) | ((ay & 1) << 1) | ((ay & 2) << 3) | ((az & 1) << 2) | ((az & 2) << 4);
+    const int32_t s = bnbr[27 * b + sl];
+    int32_t out = -1;
+    if (s >= 0) {
+        const unsigned long long nm = bmask[s];
+        if ((nm >> mm) & 1ull) out = bstart[s] + __popcll(nm & ((1ull << mm) - 1ull));
+    }
+    halo[t] = out;
+}
+
 // cb = inclusive scan of the flags: brick of cell i is cb[i] - 1
 __global__ void k_brick_fill(const uint64_t *key, const uint32_t *tag, int64_t n, int shift, int low,
                              const int32_t *cb, int ib_level, int32_t *bstart, uint64_t *bkey,
@@ -404,7 +426,7 @@ void amr_drop_fused(Case &c)
     }
     for (int l = 0; l < kMaxLevels; ++l) {
         Level &lv = c.lv[l];
-        void *ptrs[] = {lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls};
+        void *ptrs[] = {lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls, lv.bhalo};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         lv.fused_list = nullptr;
@@ -413,6 +435,7 @@ void amr_drop_fused(Case &c)
         lv.bmask = nullptr;
         lv.bnbr = nullptr;
         lv.bcls = nullptr;
+        lv.bhalo = nullptr;
         lv.nbrick = 0;
         lv.bricks = false;
     }
@@ -424,7 +447,7 @@ void amr_free(Case &c)
         Level &lv = c.lv[l];
         void *ptrs[] = {lv.key, lv.tag, lv.bcidx, lv.disrow, lv.nbr, lv.f, lv.fcol, lv.rho, lv.u,
                         lv.collide_list, lv.stream_list, lv.iblist, lv.expl_src, lv.expl_child, lv.coal_child,
-                        lv.fcol_alt, lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls};
+                        lv.fcol_alt, lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls, lv.bhalo};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         for (int s = 0; s < kNumSets; ++s)
@@ -461,7 +484,7 @@ void amr_free(Case &c)
 // mt_amr_lp.cu)
 // ----------------------------------------------------------------------------
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
-       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME };
+       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE };
 
 int amr_phase(Ctx &ctx, Case &c, int phase, int level)
 {
@@ -546,18 +569,22 @@ static int capture(Ctx &ctx, Case &c, int (*record)(Ctx &, Case &), cudaGraphExe
 
 // ---- fused schedule ---------------------------------------------------------
 // Per substep of level l: swap the post-collision buffers (fcol now holds the
-// collision computed one substep ahead), collide the F2C cells (their f came
-// from coalescence), the inlet/outflow wall cells, the finer levels, the
-// explosion, then one pass that streams lat_f and C2F, treats the IB cells and
-// collides all of them into the other buffer for the next substep; then the
-// boundary sweep and coalescence, as in LBM_Simulator.cpp:20-229.
+// collision computed one substep ahead, F2C cells included), the
+// inlet/outflow wall cells, the finer levels, the explosion, then one pass
+// that streams lat_f and C2F, treats the IB cells and collides all of them
+// into the other buffer for the next substep; then the boundary sweep, and
+// coalescence followed by the F2C cells' next collision, as in
+// LBM_Simulator.cpp:20-229.  On each level's last substep of the coarse step
+// the passes also write the macros of the f they leave (the all-level
+// calculateMacros of LBM_Simulator.cpp:11-17), except on level 0 under the
+// non-equilibrium boundary, whose sweep reads the substep's earlier macros.
 static void swap_buffers(Case &c, int l)
 {
     std::swap(c.lv[l].fcol, c.lv[l].fcol_alt);
     if (l == 0) c.par0 ^= 1;
 }
 
-static int fused_lbm_kernel(Ctx &ctx, Case &c, int l)
+static int fused_lbm_kernel(Ctx &ctx, Case &c, int l, bool last_parent)
 {
     const int L = c.d.max_level;
     int rc;
@@ -567,15 +594,17 @@ static int fused_lbm_kernel(Ctx &ctx, Case &c, int l)
             return rc;                             \
     } while (0)
     for (int sub = 0; sub < 2; ++sub) {
+        const bool last = last_parent && (l == 0 || sub == 1);
         swap_buffers(c, l);
-        RUN(PH_F2C_COLLIDE, l);
         if (l == 0 && c.d.bc_mode == MT_BC_ZOUHE_OUTFLOW) RUN(PH_BC_INOUT, 0);
         if (l < L)
-            if ((rc = fused_lbm_kernel(ctx, c, l + 1))) return rc;
+            if ((rc = fused_lbm_kernel(ctx, c, l + 1, last))) return rc;
         if (sub == 0 && l > 0) RUN(PH_EXPLOSION, l);
+        c.macros_now = last && !(l == 0 && c.d.bc_mode == MT_BC_NEQ);
         RUN(PH_PULL_COLLIDE, l);
         if (l == 0 && c.d.bc_mode == MT_BC_NEQ) RUN(PH_BC, 0);
-        if (l < L) RUN(PH_COALESCENCE, l);
+        if (l < L) RUN(PH_COAL_COLLIDE, l);
+        c.macros_now = 0;
         if (l == 0) break;
     }
 #undef RUN
@@ -584,10 +613,10 @@ static int fused_lbm_kernel(Ctx &ctx, Case &c, int l)
 
 static int record_fused_step(Ctx &ctx, Case &c)
 {
-    int rc = fused_lbm_kernel(ctx, c, 0);
+    int rc = fused_lbm_kernel(ctx, c, 0, true);
     if (rc) return rc;
-    for (int l = 0; l <= c.d.max_level; ++l)
-        if ((rc = amr_phase(ctx, c, PH_MACROS, l))) return rc;
+    if (c.d.bc_mode == MT_BC_NEQ)
+        if ((rc = amr_phase(ctx, c, PH_MACROS, 0))) return rc;
     return MT_OK;
 }
 
@@ -629,6 +658,11 @@ static int build_bricks(Ctx &ctx, Case &c, int l)
                                                            bkey, (unsigned long long *)lv.bmask, lv.bcls);
     MT_LAUNCHED(ctx);
     k_brick_nbrs<<<grid_for(27 * (int64_t)nb, 256), 256, 0, ctx.stream>>>(c.geom, l, bkey, nb, shift, low, lv.bnbr);
+    MT_LAUNCHED(ctx);
+    MT_CUDA(ctx, cudaMallocAsync(&lv.bhalo, 4 * 216 * (size_t)nb, ctx.stream));
+    k_brick_halo<<<grid_for(216 * (int64_t)nb, 256), 256, 0, ctx.stream>>>(nb, lv.bstart,
+                                                                          (const unsigned long long *)lv.bmask,
+                                                                          lv.bnbr, lv.bhalo);
     MT_LAUNCHED(ctx);
     cudaFreeAsync(tmp, ctx.stream);
     cudaFreeAsync(flag, ctx.stream);

@@ -19,7 +19,7 @@
 namespace mt {
 
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
-       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME };
+       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE };
 
 // reserved boundary directions; one copy per translation unit, uploaded by
 // AmrOps<S>::upload_tables when a case of that storage type is built
@@ -225,6 +225,54 @@ __global__ void k_coalescence(const int32_t *list, const int32_t *child, int64_t
         const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
         T::st(cf, k * nc + i, stored_of<S, Q>(fe + (C)scale * (a[k] - fe), k));
     }
+}
+
+// Fused schedule: coalescence onto the F2C cells, then (the cells' f being
+// untouched until the next substep's collide) their next collision into
+// fnext, from the stored f as the reference's collide would read it; the
+// macros of that f are written when `macros` is set (the level's last
+// substep of the coarse step: calculateMacros of every level follows).
+template <int Q, class S, int COLL>
+__global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *__restrict__ child, int64_t nl,
+                               int64_t nc, S *__restrict__ cf, const S *__restrict__ ff, int64_t nf, double scale,
+                               double tau, S *__restrict__ cfnext, typename Store<S>::C *__restrict__ rho,
+                               typename Store<S>::C *__restrict__ u, int macros)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    int32_t ch[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) ch[m] = child[(int64_t)m * nl + j];
+    C a[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        C s = 0;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) s += full_of<S, Q>(T::ld(ff, k * nf + ch[m]), k);
+        a[k] = s / (C)8.0;
+    }
+    C r, x, y, z;
+    macros_g<Q, C>(a, r, x, y, z);
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
+        const C st = stored_of<S, Q>(fe + (C)scale * (a[k] - fe), k);
+        T::st(cf, k * nc + i, st);
+        S sv;
+        T::st(&sv, 0, st);
+        a[k] = full_of<S, Q>(T::cv(sv), k);
+    }
+    macros_g<Q, C>(a, r, x, y, z);
+    if (macros) {
+        rho[i] = r;
+        u[i] = x;
+        u[nc + i] = y;
+        u[2 * nc + i] = z;
+    }
+    collide_store<Q, S, COLL>(a, r, x, y, z, tau, cfnext, nc, i);
 }
 
 // Non-equilibrium extrapolation ("eflow stable" form) on one boundary set:
@@ -456,7 +504,8 @@ __device__ __forceinline__ void pull_cell(int64_t i, int64_t n, int textbook, co
 template <int Q, class S, int COLL>
 __global__ void k_pull_collide(const int32_t *__restrict__ list, int64_t nl, int64_t n, int textbook,
                                const int32_t *__restrict__ nbr, const S *__restrict__ fcol, S *__restrict__ f,
-                               S *__restrict__ fnext, double tau)
+                               S *__restrict__ fnext, double tau, typename Store<S>::C *__restrict__ rho,
+                               typename Store<S>::C *__restrict__ u, int macros)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -472,6 +521,12 @@ __global__ void k_pull_collide(const int32_t *__restrict__ list, int64_t nl, int
     }
     C r, x, y, z;
     macros_g<Q, C>(d, r, x, y, z);
+    if (macros) {
+        rho[i] = r;
+        u[i] = x;
+        u[n + i] = y;
+        u[2 * n + i] = z;
+    }
     collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i);
 }
 
@@ -491,76 +546,71 @@ __global__ void k_pull_copy(const int32_t *__restrict__ list, int64_t nl, int64_
     for (int k = 0; k < Q; ++k) fnext[k * n + i] = v[k];
 }
 
-// The fused pass over 4x4x4 bricks (one brick per 64 threads, two per
-// block).  The block first resolves the cell index of every position of each
-// brick's 6x6x6 neighbourhood into shared memory (from the start and
-// occupancy mask of the brick and its 26 neighbours), so a cell's Q - 1
-// source indices are shared-memory reads at fixed offsets instead of rows of
-// the neighbour table.  The brick neighbours come from
-// Morton_Assist::find_neighbor on a corner cell, so each computed neighbour
-// is the one the reference's find() returns.
+// The fused pass over 4x4x4 bricks, one brick per warp (two cells per lane,
+// local Morton index lane and lane + 32).  halo[216 * b + h] holds the cell
+// index of position h = hx + 6 hy + 36 hz of the brick's 6x6x6 neighbourhood
+// (local coordinates hx - 1, hy - 1, hz - 1; -1 = no cell), resolved once
+// from the bricks' starts and occupancy masks; the warp stages it in shared
+// memory, so a cell's Q - 1 source indices are shared-memory reads at fixed
+// offsets.  The brick neighbours come from Morton_Assist::find_neighbor on a
+// corner cell, so each source is the cell the reference's find() returns.
+// When `macros` is set (the level's last substep of the coarse step) the
+// macros of the streamed f are written too: they are what the all-level
+// calculateMacros at the end of the coarse step computes.
 template <int Q, class S, int COLL>
-__global__ void __launch_bounds__(128) k_brick_step(int64_t nb, const int32_t *__restrict__ bstart,
-                                                    const uint64_t *__restrict__ bmask,
-                                                    const int32_t *__restrict__ bnbr,
-                                                    const uint8_t *__restrict__ bcls, int64_t n, int textbook,
+__global__ void __launch_bounds__(128) k_brick_step(int64_t nb, const int32_t *__restrict__ halo,
+                                                    const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
                                                     const S *__restrict__ fcol, S *__restrict__ f,
-                                                    S *__restrict__ fnext, double tau)
+                                                    S *__restrict__ fnext, double tau,
+                                                    typename Store<S>::C *__restrict__ rho,
+                                                    typename Store<S>::C *__restrict__ u, int macros)
 {
     using T = Store<S>;
     using C = typename T::C;
-    __shared__ int32_t s_start[2][27];
-    __shared__ uint64_t s_mask[2][27];
-    __shared__ int32_t s_idx[2][216];
-    if (threadIdx.x < 54) {
-        const int bb = threadIdx.x / 27, sl = threadIdx.x - 27 * bb;
-        const int64_t b = 2 * (int64_t)blockIdx.x + bb;
-        const int32_t nbk = b < nb ? __ldg(bnbr + 27 * b + sl) : -1;
-        s_start[bb][sl] = nbk >= 0 ? __ldg(bstart + nbk) : 0;
-        s_mask[bb][sl] = nbk >= 0 ? __ldg(bmask + nbk) : 0ull;
-    }
-    __syncthreads();
-    const int lb = threadIdx.x >> 6, m = threadIdx.x & 63;
-    // halo position h = hx + 6 hy + 36 hz holds the cell at local (hx-1, hy-1, hz-1)
-    for (int h = m; h < 216; h += 64) {
-        const int nx = h % 6 - 1, ny = (h / 6) % 6 - 1, nz = h / 36 - 1;
-        const int sl = ((nx >> 2) + 1) + 3 * ((ny >> 2) + 1) + 9 * ((nz >> 2) + 1);
-        const int ax = nx & 3, ay = ny & 3, az = nz & 3;
-        const int mm = (ax & 1) | ((ax & 2) << 2) | ((ay & 1) << 1) | ((ay & 2) << 3) | ((az & 1) << 2) |
-                       ((az & 2) << 4);
-        const uint64_t nm = s_mask[lb][sl];
-        s_idx[lb][h] = ((nm >> mm) & 1ull) ? s_start[lb][sl] + __popcll(nm & ((1ull << mm) - 1ull)) : -1;
-    }
-    __syncthreads();
-    const int64_t b = 2 * (int64_t)blockIdx.x + lb;
+    __shared__ int32_t s_idx[4][216];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t b = 4 * (int64_t)blockIdx.x + w;
     if (b >= nb) return;
-    const int lx = (m & 1) | ((m >> 2) & 2), ly = ((m >> 1) & 1) | ((m >> 3) & 2),
-              lz = ((m >> 2) & 1) | ((m >> 4) & 2);
-    const int base = (lx + 1) + 6 * (ly + 1) + 36 * (lz + 1);
-    const int32_t i = s_idx[lb][base];
-    if (i < 0) return;
-    const int cls = __ldg(bcls + 64 * b + m);
-    if (!cls) return;
-    int32_t src[Q];
+    const int32_t *hb = halo + 216 * b;
+    for (int h = lane; h < 216; h += 32) s_idx[w][h] = __ldg(hb + h);
+    __syncwarp();
+#pragma unroll 1
+    for (int part = 0; part < 2; ++part) {
+        const int m = lane + 32 * part;
+        const int lx = (m & 1) | ((m >> 2) & 2), ly = ((m >> 1) & 1) | ((m >> 3) & 2),
+                  lz = ((m >> 2) & 1) | ((m >> 4) & 2);
+        const int base = (lx + 1) + 6 * (ly + 1) + 36 * (lz + 1);
+        const int32_t ii = s_idx[w][base];
+        if (ii < 0) continue;
+        const int cls = __ldg(bcls + 64 * b + m);
+        if (!cls) continue;
+        const uint32_t i = (uint32_t)ii;
+        int32_t src[Q];
 #pragma unroll
-    for (int k = 1; k < Q; ++k) {
-        const int off = ex(k) + 6 * ey(k) + 36 * ez(k);
-        src[k] = s_idx[lb][base + (textbook ? -off : off)];
+        for (int k = 1; k < Q; ++k) {
+            const int off = ex(k) + 6 * ey(k) + 36 * ez(k);
+            src[k] = s_idx[w][base + (textbook ? -off : off)];
+        }
+        S v[Q];
+        pull_src32<Q, S>(i, n, src, fcol, f, v);
+        if (cls == 2) {
+#pragma unroll
+            for (int k = 0; k < Q; ++k) fnext[(uint32_t)k * n + i] = v[k];
+            continue;
+        }
+        C d[Q];
+#pragma unroll
+        for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::cv(v[k]), k);
+        C r, x, y, z;
+        macros_g<Q, C>(d, r, x, y, z);
+        if (macros) {
+            rho[i] = r;
+            u[i] = x;
+            u[n + i] = y;
+            u[2 * n + i] = z;
+        }
+        collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i);
     }
-    const uint32_t n32 = (uint32_t)n, i32 = (uint32_t)i;
-    S v[Q];
-    pull_src32<Q, S>(i32, n32, src, fcol, f, v);
-    if (cls == 2) {
-#pragma unroll
-        for (int k = 0; k < Q; ++k) fnext[(uint32_t)k * n32 + i32] = v[k];
-        return;
-    }
-    C d[Q];
-#pragma unroll
-    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::cv(v[k]), k);
-    C r, x, y, z;
-    macros_g<Q, C>(d, r, x, y, z);
-    collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n32, i32);
 }
 
 // treat() on the IB cells of the finest level, then their next collision.
@@ -568,7 +618,8 @@ __global__ void __launch_bounds__(128) k_brick_step(int64_t nb, const int32_t *_
 // substep: the macros of the cell's f before this treat.
 template <int Q, int FH, class S, int COLL>
 __global__ void k_ib_collide(const int32_t *list, int64_t nl, int64_t n, const int32_t *disrow, const double *dis,
-                             const int32_t *nbr, const S *fcol, S *f, S *fnext, double tau, double *force)
+                             const int32_t *nbr, const S *fcol, S *f, S *fnext, double tau, double *force,
+                             typename Store<S>::C *rho, typename Store<S>::C *u, int macros)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -598,6 +649,12 @@ __global__ void k_ib_collide(const int32_t *list, int64_t nl, int64_t n, const i
     force[2 * nl + j] = (double)fz;
     C r, x, y, z;
     macros_g<Q, C>(g, r, x, y, z);
+    if (macros) {
+        rho[i] = r;
+        u[i] = x;
+        u[n + i] = y;
+        u[2 * n + i] = z;
+    }
     collide_store<Q, S, COLL>(g, r, x, y, z, tau, fnext, n, i);
 }
 
@@ -872,20 +929,38 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
+    case PH_COAL_COLLIDE: {
+        if (l >= c.d.max_level || !lv.nlist[1]) return MT_OK;
+        Level &fl = c.lv[l + 1];
+        const double scale = c.d.tau[l] / (2.0 * c.d.tau[l + 1]);
+        if (c.d.collision == MT_COLL_LBGK) {
+            k_coal_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nlist[1], 64), 64, 0, s>>>(
+                lv.list[1], lv.coal_child, lv.nlist[1], n, A::f(lv), A::f(fl), fl.n, scale, c.d.tau[l],
+                (S *)lv.fcol_alt, A::rho(lv), A::u(lv), c.macros_now);
+        } else {
+            if constexpr (Q == 27)
+                k_coal_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nlist[1], 64), 64, 0, s>>>(
+                    lv.list[1], lv.coal_child, lv.nlist[1], n, A::f(lv), A::f(fl), fl.n, scale, c.d.tau[l],
+                    (S *)lv.fcol_alt, A::rho(lv), A::u(lv), c.macros_now);
+        }
+        MT_LAUNCHED(ctx);
+        return MT_OK;
+    }
     case PH_PRIME:
         // lookahead of the fused schedule from the current f: the second
-        // buffer gets every cell's fcol, then the collision of lat_f and the
-        // copy of C2F (the first collide(level) of the next substep)
+        // buffer gets every cell's fcol, then the collision of lat_f and F2C
+        // and the copy of C2F (the first collide(level) of the next substep)
         if (!n) return MT_OK;
         MT_CUDA(ctx, cudaMemcpyAsync(lv.fcol_alt, lv.fcol, sizeof(S) * Q * n, cudaMemcpyDeviceToDevice, s));
-        if (lv.nlist[0]) {
+        if (lv.ncollide) {
             if (c.d.collision == MT_COLL_LBGK) {
-                k_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nlist[0], B), B, 0, s>>>(
-                    lv.list[0], lv.nlist[0], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt);
+                k_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.ncollide, B), B, 0, s>>>(
+                    lv.collide_list, lv.ncollide, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt);
             } else {
                 if constexpr (Q == 27)
-                    k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nlist[0], 64), 64, 0, s>>>(
-                        lv.list[0], lv.nlist[0], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt);
+                    k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.ncollide, 64), 64, 0, s>>>(
+                        lv.collide_list, lv.ncollide, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv),
+                        (S *)lv.fcol_alt);
             }
             MT_LAUNCHED(ctx);
         }
@@ -903,6 +978,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         const int L = c.d.max_level;
         const bool ib_level = l == L && l > 0;
         const int tb = c.d.stream_convention;
+        const int mac = c.macros_now;
         cudaStream_t is = s;
         if (ib_level && lv.nib && c.side) {
             MT_CUDA(ctx, cudaEventRecord(c.ev_fork, s));
@@ -919,7 +995,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
                     constexpr int FH = decltype(fh)::value, COLL = decltype(coll)::value;
                     k_ib_collide<Q, FH, S, COLL><<<grid_for(lv.nib, 64), 64, 0, is>>>(
                         lv.iblist, lv.nib, n, lv.disrow, c.dis, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt, tau,
-                        c.ib_force);
+                        c.ib_force, A::rho(lv), A::u(lv), mac);
                 };
                 using I0 = std::integral_constant<int, 0>;
                 using I1 = std::integral_constant<int, 1>;
@@ -942,16 +1018,17 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             }
         }
         if (lv.bricks) {
-            const unsigned g = grid_for(lv.nbrick, 2);
+            const unsigned g = grid_for(lv.nbrick, 4);
+            const uint32_t n32 = (uint32_t)n;
             if (c.d.collision == MT_COLL_LBGK) {
-                k_brick_step<Q, S, MT_COLL_LBGK><<<g, 128, 0, s>>>(lv.nbrick, lv.bstart, lv.bmask, lv.bnbr, lv.bcls,
-                                                                   n, tb, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
-                                                                   c.d.tau[l]);
+                k_brick_step<Q, S, MT_COLL_LBGK><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb, A::fcol(lv),
+                                                                   A::f(lv), (S *)lv.fcol_alt, c.d.tau[l],
+                                                                   A::rho(lv), A::u(lv), mac);
             } else {
                 if constexpr (Q == 27)
-                    k_brick_step<Q, S, MT_COLL_CUMULANT><<<g, 128, 0, s>>>(lv.nbrick, lv.bstart, lv.bmask, lv.bnbr,
-                                                                           lv.bcls, n, tb, A::fcol(lv), A::f(lv),
-                                                                           (S *)lv.fcol_alt, c.d.tau[l]);
+                    k_brick_step<Q, S, MT_COLL_CUMULANT><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb,
+                                                                           A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
+                                                                           c.d.tau[l], A::rho(lv), A::u(lv), mac);
             }
             MT_LAUNCHED(ctx);
         } else {
@@ -959,12 +1036,12 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
                 if (c.d.collision == MT_COLL_LBGK) {
                     k_pull_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nfused, B), B, 0, s>>>(
                         lv.fused_list, lv.nfused, n, tb, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
-                        c.d.tau[l]);
+                        c.d.tau[l], A::rho(lv), A::u(lv), mac);
                 } else {
                     if constexpr (Q == 27)
                         k_pull_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nfused, 64), 64, 0, s>>>(
                             lv.fused_list, lv.nfused, n, tb, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
-                            c.d.tau[l]);
+                            c.d.tau[l], A::rho(lv), A::u(lv), mac);
                 }
                 MT_LAUNCHED(ctx);
             }

@@ -55,7 +55,8 @@ struct Level {
     // cells are contiguous in key order, so a cell at local Morton index m is
     // stored iff bit m of the brick's mask is set, at index
     // start + popcount(mask & (2^m - 1)).  bnbr[27 * b + s] is the brick at
-    // offset (s % 3 - 1, s / 3 % 3 - 1, s / 9 - 1) or -1; bcls[64 * b + m] is
+    // offset (s % 3 - 1, s / 3 % 3 - 1, s / 9 - 1) or -1; bhalo resolves them per
+    // position of the 6x6x6 neighbourhood; bcls[64 * b + m] is
     // the cell's work in the fused pass (0 none, 1 stream + collide, 2 stream + copy).
     bool bricks = false;
     int64_t nbrick = 0;
@@ -63,6 +64,7 @@ struct Level {
     uint64_t *bmask = nullptr;
     int32_t *bnbr = nullptr;
     uint8_t *bcls = nullptr;
+    int32_t *bhalo = nullptr;  // [216 * b]: cell index at each position of the brick's 6x6x6 neighbourhood, or -1
     void *rho = nullptr, *u = nullptr;   // [n], [3 * n] macroscopic fields (double, or float for reduced storage)
     int32_t *list[kNumSets] = {};
     int64_t nlist[kNumSets] = {};
@@ -117,6 +119,7 @@ struct Case {
     int64_t fgraph_launches[2] = {0, 0};
     // second stream of the fused schedule: the IB cells' treat + collision
     // overlaps the finest level's fused pass (disjoint cells)
+    int macros_now = 0;  // set while recording a level's last substep of the coarse step
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
