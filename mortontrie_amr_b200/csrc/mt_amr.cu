@@ -182,6 +182,20 @@ __global__ void k_brick_fill(const uint64_t *key, const uint32_t *tag, int64_t n
     bcls[64 * b + m] = cls;
 }
 
+// cells whose streamed f a coarser level's coalescence reads: stream +
+// collide with f stored (class 3)
+__global__ void k_brick_mark(const int32_t *child, int64_t count, const int32_t *cb, const uint64_t *key, int low,
+                             uint8_t *bcls)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int32_t ci = child[t];
+    if (ci < 0) return;
+    const int64_t b = cb[ci] - 1;
+    const int m = (int)((key[ci] >> low) & 63);
+    if (bcls[64 * b + m] == 1) bcls[64 * b + m] = 3;
+}
+
 // neighbour bricks: Morton_Assist::find_neighbor applied to the corner cell
 // of the brick that faces the offset, then a search of the brick keys
 __global__ void k_brick_nbrs(MortonGeom g, int level, const uint64_t *bkey, int64_t nb, int shift, int low,
@@ -484,7 +498,8 @@ void amr_free(Case &c)
 // mt_amr_lp.cu)
 // ----------------------------------------------------------------------------
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
-       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE };
+       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
+       PH_SYNC_F };
 
 int amr_phase(Ctx &ctx, Case &c, int phase, int level)
 {
@@ -657,6 +672,12 @@ static int build_bricks(Ctx &ctx, Case &c, int l)
     k_brick_fill<<<grid_for(n, 256), 256, 0, ctx.stream>>>(lv.key, lv.tag, n, shift, low, cb, ib_level, lv.bstart,
                                                            bkey, (unsigned long long *)lv.bmask, lv.bcls);
     MT_LAUNCHED(ctx);
+    if (l > 0 && c.lv[l - 1].coal_child && c.lv[l - 1].nlist[1]) {
+        const int64_t cnt = 8 * c.lv[l - 1].nlist[1];
+        k_brick_mark<<<grid_for(cnt, 256), 256, 0, ctx.stream>>>(c.lv[l - 1].coal_child, cnt, cb, lv.key, low,
+                                                                 lv.bcls);
+        MT_LAUNCHED(ctx);
+    }
     k_brick_nbrs<<<grid_for(27 * (int64_t)nb, 256), 256, 0, ctx.stream>>>(c.geom, l, bkey, nb, shift, low, lv.bnbr);
     MT_LAUNCHED(ctx);
     MT_CUDA(ctx, cudaMallocAsync(&lv.bhalo, 4 * 216 * (size_t)nb, ctx.stream));
@@ -708,6 +729,19 @@ static int prime_fused(Ctx &ctx, Case &c)
     return MT_OK;
 }
 
+// the streamed f the fused passes left unstored (class-1 brick cells), for
+// every reader outside the fused schedule
+int amr_sync_f(Ctx &ctx, Case &c)
+{
+    if (!c.f_stale) return MT_OK;
+    for (int l = 0; l <= c.d.max_level; ++l) {
+        int rc = amr_phase(ctx, c, PH_SYNC_F, l);
+        if (rc) return rc;
+    }
+    c.f_stale = false;
+    return MT_OK;
+}
+
 // n coarse steps replayed from one captured graph (fluidSimulate loop body)
 int amr_step(Ctx &ctx, Case &c, int n)
 {
@@ -730,9 +764,11 @@ int amr_step(Ctx &ctx, Case &c, int n)
             }
             MT_CUDA(ctx, cudaGraphLaunch(c.fgraph[p], ctx.stream));
             ctx.launches += c.fgraph_launches[p];
+            for (int l = 0; l <= c.d.max_level; ++l) c.f_stale |= c.lv[l].bricks;
         }
         return MT_OK;
     }
+    if ((rc = amr_sync_f(ctx, c))) return rc;
     c.primed = false;
     if (c.graph && c.graph_par0 != c.par0) {
         cudaGraphExecDestroy(c.graph);
@@ -751,6 +787,7 @@ int amr_step(Ctx &ctx, Case &c, int n)
 
 int amr_guard(Ctx &ctx, Case &c, int *flags)
 {
+    if (int rc = amr_sync_f(ctx, c)) return rc;
     MT_CUDA(ctx, cudaMemsetAsync(c.dev_err, 0, sizeof(int), ctx.stream));
     int rc = amr_dispatch(c, [&](auto *tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
@@ -765,6 +802,7 @@ int amr_guard(Ctx &ctx, Case &c, int *flags)
 // populations of one level as FP64 [Q][n] (host buffers), in either direction
 int amr_get(Ctx &ctx, Case &c, int level, double *h_f, double *h_fcol)
 {
+    if (int rc = amr_sync_f(ctx, c)) return rc;
     Level &lv = c.lv[level];
     if (!lv.n) return MT_OK;
     const size_t nb = sizeof(double) * (size_t)c.d.q * (size_t)lv.n;
@@ -787,6 +825,7 @@ int amr_get(Ctx &ctx, Case &c, int level, double *h_f, double *h_fcol)
 
 int amr_set(Ctx &ctx, Case &c, int level, const double *h_f, const double *h_fcol)
 {
+    if (int rc = amr_sync_f(ctx, c)) return rc;
     Level &lv = c.lv[level];
     if (!lv.n) return MT_OK;
     const size_t nb = sizeof(double) * (size_t)c.d.q * (size_t)lv.n;

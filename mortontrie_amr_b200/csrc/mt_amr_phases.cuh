@@ -19,7 +19,8 @@
 namespace mt {
 
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
-       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE };
+       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
+       PH_SYNC_F };
 
 // reserved boundary directions; one copy per translation unit, uploaded by
 // AmrOps<S>::upload_tables when a case of that storage type is built
@@ -554,16 +555,23 @@ __global__ void k_pull_copy(const int32_t *__restrict__ list, int64_t nl, int64_
 // memory, so a cell's Q - 1 source indices are shared-memory reads at fixed
 // offsets.  The brick neighbours come from Morton_Assist::find_neighbor on a
 // corner cell, so each source is the cell the reference's find() returns.
+// 16-bit storage runs six blocks per SM (85 registers, a few spilled); the
+// wider types keep their registers.
+// bcls: 1 stream + collide, 3 the same with the streamed f stored, 2 stream
+// (f stored) + copy.  The streamed f of class-1 cells is read by nothing in
+// the coarse step (their next collision is computed here, a missing link's
+// f never changes), so it is stored only when `fall` is set or when the
+// state leaves the fused schedule (k_brick_pull).
 // When `macros` is set (the level's last substep of the coarse step) the
 // macros of the streamed f are written too: they are what the all-level
 // calculateMacros at the end of the coarse step computes.
 template <int Q, class S, int COLL>
-__global__ void __launch_bounds__(128) k_brick_step(int64_t nb, const int32_t *__restrict__ halo,
+__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? 6 : 1) k_brick_step(int64_t nb, const int32_t *__restrict__ halo,
                                                     const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
                                                     const S *__restrict__ fcol, S *__restrict__ f,
                                                     S *__restrict__ fnext, double tau,
                                                     typename Store<S>::C *__restrict__ rho,
-                                                    typename Store<S>::C *__restrict__ u, int macros)
+                                                    typename Store<S>::C *__restrict__ u, int macros, int fall)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -592,7 +600,16 @@ __global__ void __launch_bounds__(128) k_brick_step(int64_t nb, const int32_t *_
             src[k] = s_idx[w][base + (textbook ? -off : off)];
         }
         S v[Q];
-        pull_src32<Q, S>(i, n, src, fcol, f, v);
+        v[0] = fcol[i];
+#pragma unroll
+        for (int k = 1; k < Q; ++k)
+            v[k] = src[k] >= 0 ? fcol[(uint32_t)k * n + (uint32_t)src[k]] : f[(uint32_t)k * n + i];
+        if (cls != 1 || fall) {
+            f[i] = v[0];
+#pragma unroll
+            for (int k = 1; k < Q; ++k)
+                if (src[k] >= 0) f[(uint32_t)k * n + i] = v[k];
+        }
         if (cls == 2) {
 #pragma unroll
             for (int k = 0; k < Q; ++k) fnext[(uint32_t)k * n + i] = v[k];
@@ -610,6 +627,38 @@ __global__ void __launch_bounds__(128) k_brick_step(int64_t nb, const int32_t *_
             u[2 * n + i] = z;
         }
         collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i);
+    }
+}
+
+// The streamed f of the class-1 cells, from the buffer the last fused pass
+// read (the values that pass would have stored).
+template <int Q, class S>
+__global__ void __launch_bounds__(128) k_brick_pull(int64_t nb, const int32_t *__restrict__ halo,
+                                                    const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
+                                                    const S *__restrict__ fcol, S *__restrict__ f)
+{
+    __shared__ int32_t s_idx[4][216];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t b = 4 * (int64_t)blockIdx.x + w;
+    if (b >= nb) return;
+    const int32_t *hb = halo + 216 * b;
+    for (int h = lane; h < 216; h += 32) s_idx[w][h] = __ldg(hb + h);
+    __syncwarp();
+    for (int part = 0; part < 2; ++part) {
+        const int m = lane + 32 * part;
+        const int lx = (m & 1) | ((m >> 2) & 2), ly = ((m >> 1) & 1) | ((m >> 3) & 2),
+                  lz = ((m >> 2) & 1) | ((m >> 4) & 2);
+        const int base = (lx + 1) + 6 * (ly + 1) + 36 * (lz + 1);
+        const int32_t ii = s_idx[w][base];
+        if (ii < 0 || __ldg(bcls + 64 * b + m) != 1) continue;
+        int32_t src[Q];
+#pragma unroll
+        for (int k = 1; k < Q; ++k) {
+            const int off = ex(k) + 6 * ey(k) + 36 * ez(k);
+            src[k] = s_idx[w][base + (textbook ? -off : off)];
+        }
+        S v[Q];
+        pull_src32<Q, S>((uint32_t)ii, n, src, fcol, f, v);
     }
 }
 
@@ -946,6 +995,13 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         MT_LAUNCHED(ctx);
         return MT_OK;
     }
+    case PH_SYNC_F:
+        if (lv.bricks) {
+            k_brick_pull<Q, S><<<grid_for(lv.nbrick, 4), 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, (uint32_t)n,
+                                                                       c.d.stream_convention, A::fcol(lv), A::f(lv));
+            MT_LAUNCHED(ctx);
+        }
+        return MT_OK;
     case PH_PRIME:
         // lookahead of the fused schedule from the current f: the second
         // buffer gets every cell's fcol, then the collision of lat_f and F2C
@@ -979,6 +1035,8 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         const bool ib_level = l == L && l > 0;
         const int tb = c.d.stream_convention;
         const int mac = c.macros_now;
+        // level 0's boundary sweep reads the streamed f of inner cells
+        const int fall = (l == 0 && c.d.bc_mode == MT_BC_NEQ) ? 1 : 0;
         cudaStream_t is = s;
         if (ib_level && lv.nib && c.side) {
             MT_CUDA(ctx, cudaEventRecord(c.ev_fork, s));
@@ -1023,12 +1081,13 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             if (c.d.collision == MT_COLL_LBGK) {
                 k_brick_step<Q, S, MT_COLL_LBGK><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb, A::fcol(lv),
                                                                    A::f(lv), (S *)lv.fcol_alt, c.d.tau[l],
-                                                                   A::rho(lv), A::u(lv), mac);
+                                                                   A::rho(lv), A::u(lv), mac, fall);
             } else {
                 if constexpr (Q == 27)
                     k_brick_step<Q, S, MT_COLL_CUMULANT><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb,
                                                                            A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
-                                                                           c.d.tau[l], A::rho(lv), A::u(lv), mac);
+                                                                           c.d.tau[l], A::rho(lv), A::u(lv), mac,
+                                                                           fall);
             }
             MT_LAUNCHED(ctx);
         } else {

@@ -85,6 +85,7 @@ int phase_call(mt_ctx *h, int32_t id, int phase, int level)
     if (rc) return rc;
     if (c->dense) return set_err(h->c, MT_ERR_STATE, "per-phase calls need a multi-level case (use mt_step)");
     if (!c->built) return set_err(h->c, MT_ERR_STATE, "case not built");
+    if ((rc = amr_sync_f(h->c, *c))) return rc;
     c->primed = false;  // the fused schedule's lookahead no longer matches f
     return amr_phase(h->c, *c, phase, level);
 }
@@ -361,6 +362,7 @@ int mt_case_init_equilibrium(mt_ctx *h, int32_t id, double rho0, const double *u
             return DenseOps<S>::init(ctx, *c, nullptr, nullptr, nullptr, nullptr, rho0, u0);
         });
     c->primed = false;
+    c->f_stale = false;  // every f is rewritten
     return amr_init_equilibrium(ctx, *c, rho0, u0);
 }
 
@@ -531,6 +533,7 @@ int mt_lbm_kernel(mt_ctx *h, int32_t id, int32_t level)
     Ctx &ctx = h->c;
     if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "LBMkernel needs a built multi-level case");
     if (level < 0 || level > c->d.max_level) return set_err(ctx, MT_ERR_ARG, "bad level");
+    if ((rc = amr_sync_f(ctx, *c))) return rc;
     c->primed = false;
     return amr_lbm_kernel(ctx, *c, level);
 }
@@ -573,6 +576,7 @@ int mt_case_set_schedule(mt_ctx *h, int32_t id, int32_t schedule)
     if (schedule != MT_SCHED_PHASES && schedule != MT_SCHED_FUSED && schedule != MT_SCHED_FUSED_LISTS)
         return set_err(ctx, MT_ERR_ARG, "schedule must be MT_SCHED_PHASES, MT_SCHED_FUSED or MT_SCHED_FUSED_LISTS");
     const bool bricks = schedule == MT_SCHED_FUSED;
+    if (!c->dense && c->built && (rc = amr_sync_f(ctx, *c))) return rc;
     if (schedule == MT_SCHED_PHASES) {
         c->primed = false;
         c->schedule = MT_SCHED_PHASES;

@@ -120,6 +120,7 @@ struct Case {
     // second stream of the fused schedule: the IB cells' treat + collision
     // overlaps the finest level's fused pass (disjoint cells)
     int macros_now = 0;  // set while recording a level's last substep of the coarse step
+    bool f_stale = false; // fused passes left class-1 brick cells' streamed f unstored (amr_sync_f)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
@@ -144,6 +145,7 @@ int amr_guard(Ctx &ctx, Case &c, int *flags);
 int amr_get(Ctx &ctx, Case &c, int level, double *h_f, double *h_fcol);
 int amr_set(Ctx &ctx, Case &c, int level, const double *h_f, const double *h_fcol);
 int amr_macros(Ctx &ctx, Case &c, int level, double *h_rho, double *h_u);
+int amr_sync_f(Ctx &ctx, Case &c);
 
 // multi-level phases, one explicit instantiation per storage type
 // (mt_amr_f64.cu builds the FP64 one without FMA contraction)

@@ -152,13 +152,14 @@ def test_multilevel_reduced_storage_vs_f64(ctx, storage, which):
     assert abs(fb[0] - fa[0]) / abs(fa[0]) < 10 * TOL_AMR[storage], (fa, fb)
 
 
-def test_nonfinite_guard(ctx):
+@pytest.mark.parametrize("schedule", ["phases", "fused"])
+def test_nonfinite_guard(ctx, schedule):
     """A NaN planted on the host in one population of a lat_f cell (overlap
     cells are rewritten every step) propagates through the steps; the device
     guard reports it as MT_ERR_NONFINITE and the context stays usable."""
     from mortontrie_amr_b200.lbm import MTError
     case = _cfg1_small()
-    mgr = _device_case(ctx, case, None)
+    mgr = _device_case(ctx, case, None, schedule=schedule)
     mgr.fluidSimulate(2)
     assert mgr.status() is None
     f, fcol = mgr.populations(1)
