@@ -357,6 +357,70 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
     return out
 
 
+ACCURACY_CASES = {
+    "cfg3": "4-level D3Q27 cumulant sphere 192x96x96, R=6, Re=200, u=0.04",
+    "cfg3_re20": "4-level D3Q27 cumulant sphere 192x96x96, R=6, Re=20, u=0.04",
+    "cfg1": "2-level D3Q19 LBGK sphere 64x32x32, R=4, Re=20, u=0.05",
+}
+
+
+def _accuracy_case(name):
+    from mortontrie_amr_b200.case import nested_sphere_case, sphere_case
+    if name == "cfg1":
+        return sphere_case()
+    return nested_sphere_case(re=20.0 if name == "cfg3_re20" else 200.0)
+
+
+def amr_accuracy(ctx, torch, steps=2500, case_name="cfg3", scaling="reference"):
+    """Long-run accuracy of the reduced storages (fused schedule) against the
+    FP64 phase schedule on a sphere case: after `steps` coarse steps, the
+    drag coefficient averaged over the last tenth of the run, the velocity
+    field of every level's lat_f cells (relative L2), the total mass, and
+    whether every population stayed finite."""
+    from mortontrie_amr_b200.lbm import LBM_Manager, MTError, drag_coefficient
+    case = _accuracy_case(case_name)
+    m = case.mesh
+    L = m.spec.max_level
+    d_fine = 2.0 * m.spec.sphere.radius * (1 << L) if m.spec.sphere else 0.0
+    u_in = float(case.params.u_bc[0])
+    tail = max(steps // 10, 1)
+    res = {}
+    for st, storage, schedule in [("f64", "f64", "phases"), ("f32", "f32", "fused"), ("f16", "f16", "fused"),
+                                  ("bf16", "bf16", "fused")]:
+        mgr = LBM_Manager(ctx, case, storage, schedule=schedule, scaling=scaling)
+        t0 = time.time()
+        mgr.fluidSimulate(steps - tail)
+        mgr.reset_force()
+        mgr.fluidSimulate(tail)
+        torch.cuda.synchronize()
+        try:
+            mgr.status()
+            finite = True
+        except MTError:
+            finite = False
+        u_all, mass = [], 0.0
+        for l in range(L + 1):
+            rho, u = mgr.macros(l)
+            _, tags = mgr.keys(l)
+            fl = (tags & 1) != 0
+            u_all.append(u[:, fl])
+            mass += float(rho[fl].sum())
+        res[st] = dict(u=np.concatenate(u_all, axis=1), mass=mass, cd=drag_coefficient(mgr.force(), u_in, d_fine),
+                       wall_s=round(time.time() - t0, 2), finite=finite)
+        mgr.close()
+    ref = res["f64"]
+    out = {"case": ACCURACY_CASES[case_name], "interface_scaling": scaling, "coarse_steps": steps,
+           "finest_steps": steps << L, "drag_window_coarse_steps": tail, "cd_f64": ref["cd"],
+           "f64_finite": ref["finite"]}
+    for st in ("f32", "f16", "bf16"):
+        r = res[st]
+        out[st] = {"cd": r["cd"], "drag_rel_vs_f64": abs(r["cd"] - ref["cd"]) / abs(ref["cd"]),
+                   "velocity_l2_vs_f64": float(np.linalg.norm(r["u"] - ref["u"]) / np.linalg.norm(ref["u"])),
+                   "mass_drift_vs_f64": abs(r["mass"] - ref["mass"]) / ref["mass"], "wall_s": r["wall_s"],
+                   "finite": r["finite"]}
+    return out
+
+
 def _reference_sample_case():
     """Bounded CPU sample of the workload for the reference's own code: a
     48^3 single populated level (the reference needs a second, empty level
@@ -442,6 +506,11 @@ def main():
     ap.add_argument("--amr-variants", default=None,
                     help="comma list of multi-level runs to time (default all: "
                          "f64,f64_fused,f32,f16,bf16,f16_phases); profiling runs")
+    ap.add_argument("--amr-accuracy", type=int, default=0, metavar="N",
+                    help="only the long-run accuracy of the reduced storages on the 4-level sphere (N coarse steps)")
+    ap.add_argument("--accuracy-case", default="cfg3", choices=sorted(ACCURACY_CASES))
+    ap.add_argument("--scaling", default="reference", choices=["reference", "standard"],
+                    help="interface rescaling of the accuracy run")
     ap.add_argument("--edge", type=int, default=256, help="cube edge (power of two); 256 is the configuration")
     ap.add_argument("--quick", action="store_true", help="headline kernel only (profiling runs)")
     args = ap.parse_args()
@@ -451,6 +520,17 @@ def main():
     N_EDGE = args.edge
     if args.impl == "reference":
         run_reference(args)
+    elif args.amr_accuracy:
+        import torch
+
+        from mortontrie_amr_b200.lbm import Context
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx = Context(0)
+        ctx.set_stream(stream.cuda_stream)
+        print(json.dumps({"amr_accuracy": amr_accuracy(ctx, torch, args.amr_accuracy, args.accuracy_case,
+                                                       args.scaling)}), flush=True)
+        ctx.close()
     elif args.amr_only:
         import torch
 

@@ -62,6 +62,8 @@ extern "C" {
 #define MT_SCHED_PHASES 0 /* the reference's phase order: collide, stream, ... as separate passes */
 #define MT_SCHED_FUSED 1  /* stream of one substep fused with the collision of the next (same results) */
 #define MT_SCHED_FUSED_LISTS 2 /* MT_SCHED_FUSED over cell lists and the neighbour table, no 4x4x4 bricks */
+#define MT_SCALE_REFERENCE 0 /* explosion x 2 tau_f / tau_c, coalescence x tau_c / (2 tau_f): LBM_Manager.cpp:1065, 1137 */
+#define MT_SCALE_STANDARD 1  /* stress-continuous rescaling: fneq_f = tau_f / (2 tau_c) fneq_c and its inverse */
 
 /* Case description: the switches the reference hard-codes in
  * LBM_Manager::LBM_Manager (LBM_Manager.cpp:32-95) and its per-level
@@ -175,6 +177,12 @@ int mt_case_tune(mt_ctx *ctx, int32_t case_id, int32_t *best_block, float *ms_pe
  * of 4 cells); MT_SCHED_FUSED_LISTS uses cell lists and the neighbour table
  * everywhere.  The per-phase calls always act on the current buffers. */
 int mt_case_set_schedule(mt_ctx *ctx, int32_t case_id, int32_t schedule);
+/* Interface rescaling of a multi-level case (no reference counterpart; the
+ * reference hard-codes MT_SCALE_REFERENCE, the default).  MT_SCALE_STANDARD
+ * is the rescaling that keeps the viscous stress continuous across a 2:1
+ * level interface; with the reference's factors the non-equilibrium part is
+ * amplified 4x from coarse to fine and flows near tau = 0.5 go unstable. */
+int mt_case_set_interface_scaling(mt_ctx *ctx, int32_t case_id, int32_t scaling);
 /* accumulated momentum-exchange force of treat() calls: fx, fy, fz, count
  * (LBM_Manager::accumIBForce, LBM_Manager.cpp:846-852) */
 int mt_get_force(mt_ctx *ctx, int32_t case_id, double *out4);

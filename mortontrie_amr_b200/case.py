@@ -61,7 +61,7 @@ class Case:
 
 def sphere_case(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1, refine=None, center=(16, 16, 16),
                 radius=4.0, u=0.05, re=20.0, boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow",
-                ib_method="FH") -> Case:
+                ib_method="FH", stream_convention="reference") -> Case:
     """Flow past a sphere; nu = u * 2R / Re in coarse units."""
     if refine is None:
         refine = [((4, 8, 8), (28, 24, 24))]
@@ -69,13 +69,14 @@ def sphere_case(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1, refine
     spec = MeshSpec(q=q, max_level=max_level, coarse=tuple(coarse), refine=list(refine), boundary=tuple(boundary),
                     sphere=Sphere(tuple(center), radius))
     p = CaseParams(q=q, collision=collision, ib_method=ib_method, bc_mode=bc_mode, nu=nu, u_bc=(u, 0.0, 0.0),
-                   u_ref=u)
+                   u_ref=u, stream_convention=stream_convention)
     return Case(build_mesh(spec), p)
 
 
 def nested_sphere_case(q=27, collision="Cumulant", coarse=(192, 96, 96), max_level=3, center=(64, 48, 48),
                        radius=6.0, half_widths=(4.0, 2.5, 1.75), u=0.04, re=200.0,
-                       boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow", ib_method="FH") -> Case:
+                       boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow", ib_method="FH",
+                       stream_convention="reference") -> Case:
     """Flow past a sphere refined in nested boxes centred on it: the box
     refined from level l to l+1 has half-width half_widths[l] * radius in
     coarse units (the defaults are the 4-level D3Q27 cumulant sphere case:
@@ -88,7 +89,8 @@ def nested_sphere_case(q=27, collision="Cumulant", coarse=(192, 96, 96), max_lev
         c = [int(round(ci * s)) for ci in center]
         refine.append((tuple(ci - hw for ci in c), tuple(ci + hw for ci in c)))
     return sphere_case(q=q, collision=collision, coarse=coarse, max_level=max_level, refine=refine, center=center,
-                       radius=radius, u=u, re=re, boundary=boundary, bc_mode=bc_mode, ib_method=ib_method)
+                       radius=radius, u=u, re=re, boundary=boundary, bc_mode=bc_mode, ib_method=ib_method,
+                       stream_convention=stream_convention)
 
 
 def uniform_box_case(q=19, n=(16, 16, 16), nu=1.0 / 30.0, boundary=("periodic",) * 3, collision="LBGK",

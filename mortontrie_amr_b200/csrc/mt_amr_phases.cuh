@@ -843,6 +843,24 @@ inline int upload_bdry_tables(Ctx &ctx)
     return MT_OK;
 }
 
+// Rescaling of the non-equilibrium part across a level interface.  The
+// reference's factors (LBM_Manager.cpp:1065, 1137): 2 tau_f / tau_c onto the
+// fine post-collision populations and tau_c / (2 tau_f) onto the coarse
+// post-stream ones.  MT_SCALE_STANDARD uses the rescaling that keeps the
+// physical viscous stress continuous under 2:1 convective scaling (Dupuis &
+// Chopard 2003): fneq_f = tau_f / (2 tau_c) fneq_c, written for post-collision
+// populations as (tau_f - 1) / (2 (tau_c - 1)), and fneq_c = 2 tau_c / tau_f fneq_f.
+inline double c2f_scale(const Case &c, int fine)
+{
+    const double tf = c.d.tau[fine], tc = c.d.tau[fine - 1];
+    return c.scaling == MT_SCALE_STANDARD ? (tf - 1.0) / (2.0 * (tc - 1.0)) : (2.0 * tf) / tc;
+}
+inline double f2c_scale(const Case &c, int coarse)
+{
+    const double tc = c.d.tau[coarse], tf = c.d.tau[coarse + 1];
+    return c.scaling == MT_SCALE_STANDARD ? (2.0 * tc) / tf : tc / (2.0 * tf);
+}
+
 template <class S, int Q>
 int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
 {
@@ -888,7 +906,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
     case PH_EXPLOSION: {
         if (l < 1 || !lv.nexpl) return MT_OK;
         Level &cl = c.lv[l - 1];
-        const double scale = (2.0 * c.d.tau[l]) / c.d.tau[l - 1];
+        const double scale = c2f_scale(c, l);
         k_explosion<Q, S><<<grid_for(8 * lv.nexpl, B), B, 0, s>>>(lv.expl_src, lv.expl_child, lv.nexpl, cl.n, A::fcol(cl),
                                                                n, A::fcol(lv), scale, (S *)lv.fcol_alt,
                                                                lv.nexpl_f2c);
@@ -898,7 +916,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
     case PH_COALESCENCE: {
         if (l >= c.d.max_level || !lv.nlist[1]) return MT_OK;
         Level &fl = c.lv[l + 1];
-        const double scale = c.d.tau[l] / (2.0 * c.d.tau[l + 1]);
+        const double scale = f2c_scale(c, l);
         k_coalescence<Q, S><<<grid_for(lv.nlist[1], B), B, 0, s>>>(lv.list[1], lv.coal_child, lv.nlist[1], n,
                                                                     A::f(lv), A::f(fl), fl.n, scale);
         MT_LAUNCHED(ctx);
@@ -981,7 +999,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
     case PH_COAL_COLLIDE: {
         if (l >= c.d.max_level || !lv.nlist[1]) return MT_OK;
         Level &fl = c.lv[l + 1];
-        const double scale = c.d.tau[l] / (2.0 * c.d.tau[l + 1]);
+        const double scale = f2c_scale(c, l);
         if (c.d.collision == MT_COLL_LBGK) {
             k_coal_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nlist[1], 64), 64, 0, s>>>(
                 lv.list[1], lv.coal_child, lv.nlist[1], n, A::f(lv), A::f(fl), fl.n, scale, c.d.tau[l],

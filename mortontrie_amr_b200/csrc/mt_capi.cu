@@ -592,6 +592,28 @@ int mt_case_set_schedule(mt_ctx *h, int32_t id, int32_t schedule)
     return MT_OK;
 }
 
+int mt_case_set_interface_scaling(mt_ctx *h, int32_t id, int32_t scaling)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense) return set_err(ctx, MT_ERR_STATE, "the dense path has no level interface");
+    if (scaling != MT_SCALE_REFERENCE && scaling != MT_SCALE_STANDARD)
+        return set_err(ctx, MT_ERR_ARG, "scaling must be MT_SCALE_REFERENCE or MT_SCALE_STANDARD");
+    if (scaling != c->scaling) {
+        // the captured steps bake the factors in
+        if (c->graph) cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+        for (int p = 0; p < 2; ++p) {
+            if (c->fgraph[p]) cudaGraphExecDestroy(c->fgraph[p]);
+            c->fgraph[p] = nullptr;
+        }
+    }
+    c->scaling = scaling;
+    return MT_OK;
+}
+
 int mt_case_status(mt_ctx *h, int32_t id)
 {
     Case *c;

@@ -112,6 +112,7 @@ struct Case {
     // swap an even number of times per coarse step), and whether the
     // lookahead buffers hold the collision of the current f
     int schedule = MT_SCHED_PHASES;
+    int scaling = MT_SCALE_REFERENCE;  // interface rescaling of the non-equilibrium part
     bool use_bricks = true;  // fused pass over 4x4x4 bricks where a level allows it (else cell lists)
     bool primed = false;
     int par0 = 0;

@@ -31,11 +31,12 @@ EXPORTS = [
     "mt_case_init_equilibrium", "mt_case_init_fields", "mt_case_set_populations", "mt_case_get_populations",
     "mt_case_get_macros", "mt_case_reduce", "mt_calculate_macros", "mt_collide", "mt_stream", "mt_explosion",
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
-    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule",
+    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling",
 ]
 
 
 SCHEDULES = {"phases": 0, "fused": 1, "fused_lists": 2}
+SCALINGS = {"reference": 0, "standard": 1}
 
 
 class MTError(RuntimeError):
@@ -72,7 +73,7 @@ def lib():
             "mt_find": [vp, i32, i32, u64p, i64, i64p], "mt_case_init_equilibrium": [vp, i32, C.c_double, dp],
             "mt_case_init_fields": [vp, i32, dp, dp, dp, dp], "mt_case_set_populations": [vp, i32, i32, dp, dp],
             "mt_case_get_populations": [vp, i32, i32, dp, dp], "mt_case_get_macros": [vp, i32, i32, dp, dp],
-            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -154,7 +155,8 @@ class LBM_Manager:
     """Multi-level case on the device: the reference's LBM_Manager with its
     strategy objects (collide / stream / treat / boundary) as methods."""
 
-    def __init__(self, ctx: Context, case: Case, storage: str = "f64", schedule: str = "phases"):
+    def __init__(self, ctx: Context, case: Case, storage: str = "f64", schedule: str = "phases",
+                 scaling: str = "reference"):
         """storage: "f64" (the reference's precision, bit-exact) or "f32" /
         "f16" / "bf16" (FP32 arithmetic on stored deviations f - w_q).
         schedule: "phases" (the reference's passes) or "fused" (stream fused
@@ -182,6 +184,12 @@ class LBM_Manager:
                   "set_dis")
         ctx.check(lib().mt_case_build(ctx.h, self.id), "mt_case_build")
         self.set_schedule(schedule)
+        self.set_interface_scaling(scaling)
+
+    def set_interface_scaling(self, scaling: str):
+        """"reference" (the reference's factors) or "standard" (stress-continuous)."""
+        self.ctx.check(lib().mt_case_set_interface_scaling(self.ctx.h, self.id, SCALINGS[scaling]), "set_scaling")
+        self.scaling = scaling
 
     def set_schedule(self, schedule: str):
         self.ctx.check(lib().mt_case_set_schedule(self.ctx.h, self.id, SCHEDULES[schedule]), "set_schedule")
