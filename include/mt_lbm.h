@@ -183,6 +183,32 @@ int mt_case_set_schedule(mt_ctx *ctx, int32_t case_id, int32_t schedule);
  * level interface; with the reference's factors the non-equilibrium part is
  * amplified 4x from coarse to fine and flows near tau = 0.5 go unstable. */
 int mt_case_set_interface_scaling(mt_ctx *ctx, int32_t case_id, int32_t scaling);
+/* Velocity of one face strategy (face 0..5 = West East South North Bot Top),
+ * the input_v each nonEquilibrumExtrapolation_<face> / inlet strategy is
+ * constructed with (NonEquilibrumExtrapolation.hpp:37-100; LBM_Manager.cpp:53-61
+ * passes the same u0 to all six).  The face's boundary cells are reset to
+ * f = fcol = feq(rho0, u), as D3Q19_BC_Strategy::initial_Feq does from the
+ * velocity map (D3Q19_BC_Manager.hpp:157-167): boundary cells never collide,
+ * so this is the velocity the fluid sees (a moving lid). */
+int mt_case_set_face_velocity(mt_ctx *ctx, int32_t case_id, int32_t face, const double *u);
+
+/* ---- batches (no reference counterpart) --------------------------------
+ * Independent multi-level cases stepped together: every substep of every
+ * level runs one batched brick pass per model family (Q, collision, storage)
+ * over all members that have that level, driven from a work list of their
+ * 4x4x4 bricks; the members' other phases run on parallel graph branches.
+ * Each coarse step of the batch is one captured CUDA graph (re-captured when
+ * the membership changes).  A member ends every step in the state it would
+ * reach stepped alone with MT_SCHED_FUSED (bit-identical: the same kernels
+ * on the same cells).  Adding a case switches it to MT_SCHED_FUSED; a member
+ * is stepped only through its batch (mt_step returns MT_ERR_STATE). */
+int mt_batch_create(mt_ctx *ctx, int32_t *batch_id);
+int mt_batch_destroy(mt_ctx *ctx, int32_t batch_id);
+int mt_batch_add(mt_ctx *ctx, int32_t batch_id, int32_t case_id);
+int mt_batch_remove(mt_ctx *ctx, int32_t batch_id, int32_t case_id);
+int mt_batch_size(mt_ctx *ctx, int32_t batch_id, int32_t *n_cases);
+/* n coarse steps of every member; asynchronous on the context stream */
+int mt_batch_step(mt_ctx *ctx, int32_t batch_id, int32_t n_coarse_steps);
 /* accumulated momentum-exchange force of treat() calls: fx, fy, fz, count
  * (LBM_Manager::accumIBForce, LBM_Manager.cpp:846-852) */
 int mt_get_force(mt_ctx *ctx, int32_t case_id, double *out4);

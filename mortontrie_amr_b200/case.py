@@ -36,6 +36,7 @@ class CaseParams:
     rho0: float = 1.0
     storage: str = "f64"
     tau: list = field(default_factory=list)
+    face_u: dict = field(default_factory=dict)  # face (0..5 = W E S N B T) -> boundary velocity, else u_bc
 
     def taus(self, max_level: int) -> list:
         if self.tau:
@@ -91,6 +92,32 @@ def nested_sphere_case(q=27, collision="Cumulant", coarse=(192, 96, 96), max_lev
     return sphere_case(q=q, collision=collision, coarse=coarse, max_level=max_level, refine=refine, center=center,
                        radius=radius, u=u, re=re, boundary=boundary, bc_mode=bc_mode, ib_method=ib_method,
                        stream_convention=stream_convention)
+
+
+def cavity_case(q=19, collision="LBGK", coarse=(32, 32, 32), max_level=1, re=100.0, u_lid=0.05,
+                refine=None, ib_method="FH") -> Case:
+    """Lid-driven cavity: walls on every face (non-equilibrium boundary),
+    the Top face moving at u_lid along x; nu = u_lid * nz / Re in coarse
+    units.  With max_level > 0 the levels refine nested boxes under the lid
+    (default: 2 coarse cells clear of the side walls, the upper quarter of
+    the cavity, each finer box 2 coarse cells inside the previous one)."""
+    nx, ny, nz = coarse
+    nu = u_lid * nz / re
+    if refine is None:
+        refine = []
+        lo, hi = [2, 2, nz - nz // 4 - 2], [nx - 2, ny - 2, nz - 2]
+        for l in range(max_level):
+            s = 1 << l
+            refine.append((tuple(v * s for v in lo), tuple(v * s for v in hi)))
+            lo = [v + 2 for v in lo]
+            hi = [v - 2 for v in hi]
+    spec = MeshSpec(q=q, max_level=max_level, coarse=tuple(coarse), refine=list(refine) if max_level else [None],
+                    boundary=("bc", "bc", "bc"), sphere=None)
+    if max_level == 0:
+        spec = MeshSpec(q=q, max_level=1, coarse=tuple(coarse), refine=[None], boundary=("bc", "bc", "bc"))
+    p = CaseParams(q=q, collision=collision, ib_method=ib_method, bc_mode="neq", nu=nu, u_bc=(0.0, 0.0, 0.0),
+                   u_ref=u_lid, face_u={5: (u_lid, 0.0, 0.0)})
+    return Case(build_mesh(spec), p)
 
 
 def uniform_box_case(q=19, n=(16, 16, 16), nu=1.0 / 30.0, boundary=("periodic",) * 3, collision="LBGK",

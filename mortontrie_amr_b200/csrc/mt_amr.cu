@@ -356,6 +356,8 @@ static int build_level(Ctx &ctx, Case &c, int l)
 
 int amr_build(Ctx &ctx, Case &c)
 {
+    for (int f = 0; f < 6; ++f)
+        for (int a = 0; a < 3; ++a) c.face_u[f][a] = c.d.u_bc[a];
     const int L = c.d.max_level;
     c.geom.L = L;
     for (int a = 0; a < 3; ++a) {
@@ -499,7 +501,7 @@ void amr_free(Case &c)
 // ----------------------------------------------------------------------------
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
        PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
-       PH_SYNC_F };
+       PH_SYNC_F, PH_FACE_EQ0 = 24 };
 
 int amr_phase(Ctx &ctx, Case &c, int phase, int level)
 {
@@ -742,6 +744,22 @@ int amr_sync_f(Ctx &ctx, Case &c)
     return MT_OK;
 }
 
+// a face strategy's velocity: its boundary cells restart from feq(rho0, u)
+// and its non-equilibrium sweep (or the West inlet) uses u from now on
+int amr_set_face(Ctx &ctx, Case &c, int face, const double *u)
+{
+    if (int rc = amr_sync_f(ctx, c)) return rc;
+    for (int a = 0; a < 3; ++a) c.face_u[face][a] = u[a];
+    if (c.graph) cudaGraphExecDestroy(c.graph);
+    c.graph = nullptr;
+    for (int p = 0; p < 2; ++p) {
+        if (c.fgraph[p]) cudaGraphExecDestroy(c.fgraph[p]);
+        c.fgraph[p] = nullptr;
+    }
+    c.primed = false;
+    return amr_phase(ctx, c, PH_FACE_EQ0 + face, 0);
+}
+
 // n coarse steps replayed from one captured graph (fluidSimulate loop body)
 int amr_step(Ctx &ctx, Case &c, int n)
 {
@@ -781,6 +799,271 @@ int amr_step(Ctx &ctx, Case &c, int n)
     for (int s = 0; s < n; ++s) {
         MT_CUDA(ctx, cudaGraphLaunch(c.graph, ctx.stream));
         ctx.launches += c.graph_launches;
+    }
+    return MT_OK;
+}
+
+int amr_prime(Ctx &ctx, Case &c)
+{
+    return c.primed ? MT_OK : prime_fused(ctx, c);
+}
+
+// ---- batches ------------------------------------------------------------------
+// Every member takes the fused schedule's steps in lockstep: the recursion
+// below visits each level with all members that have it, in the order each
+// member alone would take (members never interact, so this is the same
+// computation as stepping them one by one).  The streamed + collided pass
+// of brick levels is one batched kernel per model family; a member's other
+// phases run on a pool of streams (parallel graph branches).
+namespace {
+
+struct BatchRec {
+    Batch *b;
+    std::vector<BrickBatch> hdesc;
+    int64_t cap = 0;
+};
+
+template <class Pred, class F>
+int fork_cases(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cs, Pred &&has, F &&fn)
+{
+    std::vector<Case *> work;
+    for (Case *c : cs)
+        if (has(*c)) work.push_back(c);
+    if (work.empty()) return MT_OK;
+    Batch &B = *R.b;
+    cudaStream_t main = ctx.stream;
+    const int P = (int)std::min<size_t>(B.pool.size(), work.size());
+    MT_CUDA(ctx, cudaEventRecord(B.ev_fork, main));
+    for (int p = 0; p < P; ++p) MT_CUDA(ctx, cudaStreamWaitEvent(B.pool[p], B.ev_fork, 0));
+    int rc = MT_OK;
+    for (size_t i = 0; i < work.size() && !rc; ++i) {
+        ctx.stream = B.pool[i % P];
+        rc = fn(*work[i]);
+    }
+    ctx.stream = main;
+    for (int p = 0; p < P; ++p) {
+        MT_CUDA(ctx, cudaEventRecord(B.ev_join[p], B.pool[p]));
+        MT_CUDA(ctx, cudaStreamWaitEvent(main, B.ev_join[p], 0));
+    }
+    return rc;
+}
+
+int storage_code(const Case &c) { return c.d.storage; }
+
+// batched brick passes of level l over the members in cs (brick levels only)
+int batch_bricks(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cs, int l, const BrickBatch **first_desc)
+{
+    // group by (q, collision, storage): one kernel instantiation each
+    std::vector<std::vector<Case *>> groups;
+    for (Case *c : cs) {
+        if (!c->lv[l].bricks) continue;
+        bool placed = false;
+        for (auto &g : groups)
+            if (g[0]->d.q == c->d.q && g[0]->d.collision == c->d.collision &&
+                storage_code(*g[0]) == storage_code(*c)) {
+                g.push_back(c);
+                placed = true;
+                break;
+            }
+        if (!placed) groups.push_back({c});
+    }
+    (void)first_desc;
+    for (auto &g : groups) {
+        for (size_t c0 = 0; c0 < g.size(); c0 += kMaxBatchSlots) {
+            if ((int64_t)R.hdesc.size() >= R.cap) return set_err(ctx, MT_ERR_STATE, "batch descriptor capacity");
+            BrickBatch d;
+            const size_t c1 = std::min(g.size(), c0 + kMaxBatchSlots);
+            for (size_t k = c0; k < c1; ++k) {
+                Case &c = *g[k];
+                Level &lv = c.lv[l];
+                BrickSlot &sl = d.slot[d.nslots];
+                sl.halo = lv.bhalo;
+                sl.cls = lv.bcls;
+                sl.fcol = lv.fcol;
+                sl.f = lv.f;
+                sl.fnext = lv.fcol_alt;
+                sl.rho = lv.rho;
+                sl.u = lv.u;
+                sl.tau = c.d.tau[l];
+                sl.n = (uint32_t)lv.n;
+                sl.textbook = c.d.stream_convention;
+                sl.fall = (l == 0 && c.d.bc_mode == MT_BC_NEQ) ? 1 : 0;
+                sl.macros = c.macros_now;
+                d.off[d.nslots + 1] = d.off[d.nslots] + lv.nbrick;
+                ++d.nslots;
+            }
+            d.total = d.off[d.nslots];
+            const BrickBatch *dev = R.b->ddesc[R.b->par] + R.hdesc.size();
+            R.hdesc.push_back(d);
+            Case &c = *g[0];
+            int rc = amr_dispatch(c, [&](auto *tag) {
+                using S = std::remove_pointer_t<decltype(tag)>;
+                return AmrOps<S>::batch_pass(ctx, c.d.q, c.d.collision, dev, d.total);
+            });
+            if (rc) return rc;
+        }
+    }
+    return MT_OK;
+}
+
+int batch_lbm_kernel(Ctx &ctx, BatchRec &R, const std::vector<Case *> &all, int l, bool last_parent)
+{
+    std::vector<Case *> cs;
+    for (Case *c : all)
+        if (c->d.max_level >= l && c->lv[l].n) cs.push_back(c);
+    if (cs.empty()) return MT_OK;
+    int rc;
+    for (int sub = 0; sub < 2; ++sub) {
+        const bool last = last_parent && (l == 0 || sub == 1);
+        for (Case *c : cs) swap_buffers(*c, l);
+        if (l == 0)
+            if ((rc = fork_cases(ctx, R, cs, [](Case &c) { return c.d.bc_mode == MT_BC_ZOUHE_OUTFLOW; },
+                                 [&](Case &c) { return amr_phase(ctx, c, PH_BC_INOUT, 0); })))
+                return rc;
+        if ((rc = batch_lbm_kernel(ctx, R, cs, l + 1, last))) return rc;
+        if (sub == 0 && l > 0)
+            if ((rc = fork_cases(ctx, R, cs, [](Case &) { return true; },
+                                 [&](Case &c) { return amr_phase(ctx, c, PH_EXPLOSION, l); })))
+                return rc;
+        for (Case *c : cs) c->macros_now = last && !(l == 0 && c->d.bc_mode == MT_BC_NEQ);
+        // members' own pull work (IB cells; levels without bricks) beside the batched brick pass
+        {
+            Batch &B = *R.b;
+            cudaStream_t main = ctx.stream;
+            std::vector<Case *> own;
+            for (Case *c : cs)
+                if (!c->lv[l].bricks || (l == c->d.max_level && l > 0)) own.push_back(c);
+            const int P = (int)std::min<size_t>(B.pool.size(), own.size());
+            if (P) {
+                MT_CUDA(ctx, cudaEventRecord(B.ev_fork, main));
+                for (int p = 0; p < P; ++p) MT_CUDA(ctx, cudaStreamWaitEvent(B.pool[p], B.ev_fork, 0));
+                for (size_t i = 0; i < own.size(); ++i) {
+                    Case &c = *own[i];
+                    ctx.stream = B.pool[i % P];
+                    c.pull_mode = c.lv[l].bricks ? 1 : 0;
+                    rc = amr_phase(ctx, c, PH_PULL_COLLIDE, l);
+                    c.pull_mode = 0;
+                    if (rc) {
+                        ctx.stream = main;
+                        return rc;
+                    }
+                }
+                ctx.stream = main;
+            }
+            if ((rc = batch_bricks(ctx, R, cs, l, nullptr))) return rc;
+            for (int p = 0; p < P; ++p) {
+                MT_CUDA(ctx, cudaEventRecord(B.ev_join[p], B.pool[p]));
+                MT_CUDA(ctx, cudaStreamWaitEvent(main, B.ev_join[p], 0));
+            }
+        }
+        if ((rc = fork_cases(ctx, R, cs,
+                             [&](Case &c) { return (l == 0 && c.d.bc_mode == MT_BC_NEQ) || l < c.d.max_level; },
+                             [&](Case &c) {
+                                 int r = MT_OK;
+                                 if (l == 0 && c.d.bc_mode == MT_BC_NEQ) r = amr_phase(ctx, c, PH_BC, 0);
+                                 if (!r && l < c.d.max_level) r = amr_phase(ctx, c, PH_COAL_COLLIDE, l);
+                                 return r;
+                             })))
+            return rc;
+        for (Case *c : cs) c->macros_now = 0;
+        if (l == 0) break;
+    }
+    return MT_OK;
+}
+
+int record_batch_step(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cases)
+{
+    int rc = batch_lbm_kernel(ctx, R, cases, 0, true);
+    if (rc) return rc;
+    return fork_cases(ctx, R, cases, [](Case &c) { return c.d.bc_mode == MT_BC_NEQ; },
+                      [&](Case &c) { return amr_phase(ctx, c, PH_MACROS, 0); });
+}
+
+}  // namespace
+
+void batch_drop(Batch &b)
+{
+    for (int p = 0; p < 2; ++p) {
+        if (b.graph[p]) cudaGraphExecDestroy(b.graph[p]);
+        b.graph[p] = nullptr;
+        if (b.ddesc[p]) cudaFree(b.ddesc[p]);
+        b.ddesc[p] = nullptr;
+    }
+    b.par = 0;
+}
+
+void batch_free(Batch &b)
+{
+    batch_drop(b);
+    for (cudaStream_t s : b.pool) cudaStreamDestroy(s);
+    for (cudaEvent_t e : b.ev_join) cudaEventDestroy(e);
+    if (b.ev_fork) cudaEventDestroy(b.ev_fork);
+    b.pool.clear();
+    b.ev_join.clear();
+    b.ev_fork = nullptr;
+}
+
+int batch_step(Ctx &ctx, Batch &B, const std::vector<Case *> &cases, int n)
+{
+    if (cases.empty() || n <= 0) return MT_OK;
+    int rc;
+    for (Case *c : cases) {
+        if ((rc = amr_sync_f(ctx, *c))) return rc;
+        if (!c->primed && (rc = prime_fused(ctx, *c))) return rc;
+    }
+    if (B.pool.empty()) {
+        const int P = (int)std::min<size_t>(8, cases.size());
+        for (int p = 0; p < P; ++p) {
+            cudaStream_t s;
+            cudaEvent_t e;
+            MT_CUDA(ctx, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+            MT_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            B.pool.push_back(s);
+            B.ev_join.push_back(e);
+        }
+        MT_CUDA(ctx, cudaEventCreateWithFlags(&B.ev_fork, cudaEventDisableTiming));
+    }
+    int Lmax = 0;
+    for (Case *c : cases) Lmax = std::max(Lmax, c->d.max_level);
+    for (int s = 0; s < n; ++s) {
+        const int p = B.par;
+        if (!B.graph[p]) {
+            BatchRec R;
+            R.b = &B;
+            // at most one descriptor per family (3 models x 4 storages) and chunk for every substep
+            R.cap = (int64_t)((2 << Lmax) * 12) * (int64_t)((cases.size() + kMaxBatchSlots - 1) / kMaxBatchSlots);
+            MT_CUDA(ctx, cudaMalloc(&B.ddesc[p], sizeof(BrickBatch) * R.cap));
+            for (Case *c : cases) c->no_side = true;
+            const int64_t before = ctx.launches;
+            cudaGraph_t captured = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return set_err(ctx, MT_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+            rc = record_batch_step(ctx, R, cases);
+            e = cudaStreamEndCapture(ctx.stream, &captured);
+            for (Case *c : cases) c->no_side = false;
+            if (rc || e != cudaSuccess) {
+                if (captured) cudaGraphDestroy(captured);
+                batch_drop(B);
+                return rc ? rc : set_err(ctx, MT_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+            }
+            B.graph_launches[p] = ctx.launches - before;
+            ctx.launches = before;
+            e = cudaGraphInstantiate(&B.graph[p], captured, 0);
+            cudaGraphDestroy(captured);
+            if (e != cudaSuccess) {
+                B.graph[p] = nullptr;
+                return set_err(ctx, MT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            }
+            MT_CUDA(ctx, cudaMemcpy(B.ddesc[p], R.hdesc.data(), sizeof(BrickBatch) * R.hdesc.size(),
+                                    cudaMemcpyHostToDevice));
+        } else {
+            for (Case *c : cases) swap_buffers(*c, 0);
+        }
+        MT_CUDA(ctx, cudaGraphLaunch(B.graph[p], ctx.stream));
+        ctx.launches += B.graph_launches[p];
+        B.par ^= 1;
+        for (Case *c : cases)
+            for (int l = 0; l <= c->d.max_level; ++l) c->f_stale |= c->lv[l].bricks;
     }
     return MT_OK;
 }

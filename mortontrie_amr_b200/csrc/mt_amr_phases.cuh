@@ -20,7 +20,7 @@ namespace mt {
 
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
        PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
-       PH_SYNC_F };
+       PH_SYNC_F, PH_FACE_EQ0 = 24 };
 
 // reserved boundary directions; one copy per translation unit, uploaded by
 // AmrOps<S>::upload_tables when a case of that storage type is built
@@ -343,6 +343,26 @@ __global__ void k_bc_inout(const int32_t *list, int64_t nl, int east, int64_t n,
     }
 }
 
+// D3Q19_BC_Strategy::initial_Feq (D3Q19_BC_Manager.hpp:157-167) on one
+// boundary set: f = fcol = feq(rho0, u) with the face's velocity
+template <int Q, class S>
+__global__ void k_bc_set_eq(const int32_t *list, int64_t nl, int64_t n, double rho0, double ux, double uy, double uz,
+                            S *f, S *fcol)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const double v = feq_ref<Q>(k, rho0, ux, uy, uz);
+        const C st = (C)(T::shifted ? v - w<Q>(k) : v);
+        T::st(f, k * n + i, st);
+        T::st(fcol, k * n + i, st);
+    }
+}
+
 // SinglePointInterpolation::treat (ComplexBoundary_Manager.cpp:43-225) on
 // one cell: wall links by Filippova-Haenel or distance-weighted
 // interpolation, free links by plain pull, density clamp, eight
@@ -565,22 +585,18 @@ __global__ void k_pull_copy(const int32_t *__restrict__ list, int64_t nl, int64_
 // When `macros` is set (the level's last substep of the coarse step) the
 // macros of the streamed f are written too: they are what the all-level
 // calculateMacros at the end of the coarse step computes.
+// one warp's brick b (see above); s_idx is the warp's 216-entry shared table
 template <int Q, class S, int COLL>
-__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? 6 : 1) k_brick_step(int64_t nb, const int32_t *__restrict__ halo,
-                                                    const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
-                                                    const S *__restrict__ fcol, S *__restrict__ f,
-                                                    S *__restrict__ fnext, double tau,
-                                                    typename Store<S>::C *__restrict__ rho,
-                                                    typename Store<S>::C *__restrict__ u, int macros, int fall)
+__device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, const int32_t *__restrict__ halo,
+                                           const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
+                                           const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext,
+                                           double tau, typename Store<S>::C *__restrict__ rho,
+                                           typename Store<S>::C *__restrict__ u, int macros, int fall)
 {
     using T = Store<S>;
     using C = typename T::C;
-    __shared__ int32_t s_idx[4][216];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t b = 4 * (int64_t)blockIdx.x + w;
-    if (b >= nb) return;
     const int32_t *hb = halo + 216 * b;
-    for (int h = lane; h < 216; h += 32) s_idx[w][h] = __ldg(hb + h);
+    for (int h = lane; h < 216; h += 32) s_idx[h] = __ldg(hb + h);
     __syncwarp();
 #pragma unroll 1
     for (int part = 0; part < 2; ++part) {
@@ -588,7 +604,7 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? 6 : 1) k_brick_ste
         const int lx = (m & 1) | ((m >> 2) & 2), ly = ((m >> 1) & 1) | ((m >> 3) & 2),
                   lz = ((m >> 2) & 1) | ((m >> 4) & 2);
         const int base = (lx + 1) + 6 * (ly + 1) + 36 * (lz + 1);
-        const int32_t ii = s_idx[w][base];
+        const int32_t ii = s_idx[base];
         if (ii < 0) continue;
         const int cls = __ldg(bcls + 64 * b + m);
         if (!cls) continue;
@@ -597,7 +613,7 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? 6 : 1) k_brick_ste
 #pragma unroll
         for (int k = 1; k < Q; ++k) {
             const int off = ex(k) + 6 * ey(k) + 36 * ez(k);
-            src[k] = s_idx[w][base + (textbook ? -off : off)];
+            src[k] = s_idx[base + (textbook ? -off : off)];
         }
         S v[Q];
         v[0] = fcol[i];
@@ -628,6 +644,43 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? 6 : 1) k_brick_ste
         }
         collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i);
     }
+}
+
+template <int Q, class S, int COLL>
+__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? 6 : 1) k_brick_step(
+    int64_t nb, const int32_t *__restrict__ halo, const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
+    const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext, double tau,
+    typename Store<S>::C *__restrict__ rho, typename Store<S>::C *__restrict__ u, int macros, int fall)
+{
+    __shared__ int32_t s_idx[4][216];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t b = 4 * (int64_t)blockIdx.x + w;
+    if (b >= nb) return;
+    brick_warp<Q, S, COLL>(b, lane, s_idx[w], halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros, fall);
+}
+
+// The same pass over the bricks of many cases (a batch): brick b of the work
+// list belongs to the slot whose [off[s], off[s + 1]) range holds it; each
+// slot carries one case level's tables, buffers and relaxation time.
+template <int Q, class S, int COLL>
+__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? 6 : 1) k_brick_step_batch(const BrickBatch *__restrict__ bb)
+{
+    __shared__ int32_t s_idx[4][216];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t b = 4 * (int64_t)blockIdx.x + w;
+    if (b >= bb->total) return;
+    int lo = 0, hi = bb->nslots;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (bb->off[mid] <= b)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    const BrickSlot &sl = bb->slot[lo];
+    using C = typename Store<S>::C;
+    brick_warp<Q, S, COLL>(b - bb->off[lo], lane, s_idx[w], sl.halo, sl.cls, sl.n, sl.textbook, (const S *)sl.fcol,
+                           (S *)sl.f, (S *)sl.fnext, sl.tau, (C *)sl.rho, (C *)sl.u, sl.macros, sl.fall);
 }
 
 // The streamed f of the class-1 cells, from the buffer the last fused pass
@@ -843,6 +896,14 @@ inline int upload_bdry_tables(Ctx &ctx)
     return MT_OK;
 }
 
+// boundary sets of each face strategy (West, East, South, North, Bot, Top):
+// the face, its edges and corners as NonEquilibrumExtrapolation.hpp:24-110
+// registers them
+static const int kFaceSets[6][9] = {
+    {0, 7, 8, 15, 17, 19, 20, 23, 24}, {1, 6, 9, 14, 16, 18, 21, 22, 25},
+    {2, 11, 13, -1, -1, -1, -1, -1, -1}, {3, 10, 12, -1, -1, -1, -1, -1, -1},
+    {4, -1, -1, -1, -1, -1, -1, -1, -1}, {5, -1, -1, -1, -1, -1, -1, -1, -1}};
+
 // Rescaling of the non-equilibrium part across a level interface.  The
 // reference's factors (LBM_Manager.cpp:1065, 1137): 2 tau_f / tau_c onto the
 // fine post-collision populations and tau_c / (2 tau_f) onto the coarse
@@ -928,21 +989,17 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         // all six face groups in the reference's order (LBM_Simulator.cpp:90-95), or one
         const int f0 = phase == PH_BC ? 0 : phase - PH_BC_FACE0, f1 = phase == PH_BC ? 6 : f0 + 1;
         Level &l0 = c.lv[0];
-        static const int face_sets[6][9] = {
-            {0, 7, 8, 15, 17, 19, 20, 23, 24}, {1, 6, 9, 14, 16, 18, 21, 22, 25},
-            {2, 11, 13, -1, -1, -1, -1, -1, -1}, {3, 10, 12, -1, -1, -1, -1, -1, -1},
-            {4, -1, -1, -1, -1, -1, -1, -1, -1}, {5, -1, -1, -1, -1, -1, -1, -1, -1}};
         double *tmp = c.bc_tmp;
         if (!tmp) return MT_OK;
         for (int face = f0; face < f1; ++face)
             for (int g = 0; g < 9; ++g) {
-                const int b = face_sets[face][g];
+                const int b = kFaceSets[face][g];
                 if (b < 0) break;
                 if (!l0.nbc[b]) continue;
                 for (int ph = 0; ph < 2; ++ph) {
-                    k_bc_neq<Q, S><<<grid_for(l0.nbc[b], B), B, 0, s>>>(l0.bclist[b], l0.nbc[b], b, l0.n, l0.nbr,
-                                                                         A::rho(l0), A::u(l0), A::f(l0), c.d.u_bc[0],
-                                                                         c.d.u_bc[1], c.d.u_bc[2], tmp, ph, c.dev_err);
+                    k_bc_neq<Q, S><<<grid_for(l0.nbc[b], B), B, 0, s>>>(
+                        l0.bclist[b], l0.nbc[b], b, l0.n, l0.nbr, A::rho(l0), A::u(l0), A::f(l0), c.face_u[face][0],
+                        c.face_u[face][1], c.face_u[face][2], tmp, ph, c.dev_err);
                     MT_LAUNCHED(ctx);
                 }
             }
@@ -953,8 +1010,8 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         for (int face = 0; face < 2; ++face) {
             if (!l0.nbc[face]) continue;
             k_bc_inout<Q, S><<<grid_for(l0.nbc[face], B), B, 0, s>>>(l0.bclist[face], l0.nbc[face], face, l0.n, l0.nbr,
-                                                                      c.d.rho0, A::f(l0), A::fcol(l0), c.d.u_bc[0],
-                                                                      c.d.u_bc[1], c.d.u_bc[2], c.dev_err);
+                                                                      c.d.rho0, A::f(l0), A::fcol(l0), c.face_u[0][0],
+                                                                      c.face_u[0][1], c.face_u[0][2], c.dev_err);
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
@@ -1013,6 +1070,21 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         MT_LAUNCHED(ctx);
         return MT_OK;
     }
+    case PH_FACE_EQ0 + 0: case PH_FACE_EQ0 + 1: case PH_FACE_EQ0 + 2:
+    case PH_FACE_EQ0 + 3: case PH_FACE_EQ0 + 4: case PH_FACE_EQ0 + 5: {
+        const int face = phase - PH_FACE_EQ0;
+        Level &l0 = c.lv[0];
+        for (int g = 0; g < 9; ++g) {
+            const int b = kFaceSets[face][g];
+            if (b < 0) break;
+            if (!l0.nbc[b]) continue;
+            k_bc_set_eq<Q, S><<<grid_for(l0.nbc[b], B), B, 0, s>>>(l0.bclist[b], l0.nbc[b], l0.n, c.d.rho0,
+                                                                    c.face_u[face][0], c.face_u[face][1],
+                                                                    c.face_u[face][2], A::f(l0), A::fcol(l0));
+            MT_LAUNCHED(ctx);
+        }
+        return MT_OK;
+    }
     case PH_SYNC_F:
         if (lv.bricks) {
             k_brick_pull<Q, S><<<grid_for(lv.nbrick, 4), 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, (uint32_t)n,
@@ -1056,7 +1128,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         // level 0's boundary sweep reads the streamed f of inner cells
         const int fall = (l == 0 && c.d.bc_mode == MT_BC_NEQ) ? 1 : 0;
         cudaStream_t is = s;
-        if (ib_level && lv.nib && c.side) {
+        if (ib_level && lv.nib && c.side && !c.no_side) {
             MT_CUDA(ctx, cudaEventRecord(c.ev_fork, s));
             MT_CUDA(ctx, cudaStreamWaitEvent(c.side, c.ev_fork, 0));
             is = c.side;
@@ -1093,7 +1165,9 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
                 MT_LAUNCHED(ctx);
             }
         }
-        if (lv.bricks) {
+        if (c.pull_mode == 1) {
+            // the batch runs this level's bricks
+        } else if (lv.bricks) {
             const unsigned g = grid_for(lv.nbrick, 4);
             const uint32_t n32 = (uint32_t)n;
             if (c.d.collision == MT_COLL_LBGK) {
@@ -1226,6 +1300,21 @@ int AmrOps<S>::macros_out(Ctx &ctx, Case &c, int l, double *d_rho, double *d_u)
     k_macro_to_f64<C><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>((const C *)lv.rho, d_rho, lv.n);
     MT_LAUNCHED(ctx);
     k_macro_to_f64<C><<<grid_for(3 * lv.n, 256), 256, 0, ctx.stream>>>((const C *)lv.u, d_u, 3 * lv.n);
+    MT_LAUNCHED(ctx);
+    return MT_OK;
+}
+
+template <class S>
+int AmrOps<S>::batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total)
+{
+    const unsigned g = grid_for(total, 4);
+    if (!g) return MT_OK;
+    if (q == 19)
+        k_brick_step_batch<19, S, MT_COLL_LBGK><<<g, 128, 0, ctx.stream>>>(d_desc);
+    else if (coll == MT_COLL_LBGK)
+        k_brick_step_batch<27, S, MT_COLL_LBGK><<<g, 128, 0, ctx.stream>>>(d_desc);
+    else
+        k_brick_step_batch<27, S, MT_COLL_CUMULANT><<<g, 128, 0, ctx.stream>>>(d_desc);
     MT_LAUNCHED(ctx);
     return MT_OK;
 }

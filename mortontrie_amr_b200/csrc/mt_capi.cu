@@ -120,6 +120,11 @@ int mt_destroy(mt_ctx *h)
     if (!h) return MT_ERR_ARG;
     cudaSetDevice(h->c.device);
     cudaStreamSynchronize(h->c.stream);
+    for (Batch *b : h->c.batches)
+        if (b) {
+            batch_free(*b);
+            delete b;
+        }
     for (Case *c : h->c.cases)
         if (c) {
             amr_free(*c);
@@ -219,6 +224,15 @@ int mt_case_destroy(mt_ctx *h, int32_t id)
     int rc = get_case(h, id, &c);
     if (rc) return rc;
     cudaStreamSynchronize(h->c.stream);
+    // leave every batch that holds the case
+    for (Batch *b : h->c.batches)
+        if (b)
+            for (size_t k = 0; k < b->ids.size(); ++k)
+                if (b->ids[k] == id) {
+                    b->ids.erase(b->ids.begin() + k);
+                    batch_drop(*b);
+                    break;
+                }
     amr_free(*c);
     if (c->A) cudaFree(c->A);
     if (c->B) cudaFree(c->B);
@@ -561,6 +575,7 @@ int mt_step(mt_ctx *h, int32_t id, int32_t n)
             return r;
         });
     }
+    if (c->in_batch) return set_err(ctx, MT_ERR_STATE, "the case belongs to a batch: step it with mt_batch_step");
     rc = amr_step(ctx, *c, n);
     if (rc) return rc;
     return MT_OK;
@@ -612,6 +627,118 @@ int mt_case_set_interface_scaling(mt_ctx *h, int32_t id, int32_t scaling)
     }
     c->scaling = scaling;
     return MT_OK;
+}
+
+int mt_case_set_face_velocity(mt_ctx *h, int32_t id, int32_t face, const double *u)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "face velocities need a built multi-level case");
+    if (face < 0 || face > 5) return set_err(ctx, MT_ERR_ARG, "face must be 0..5 (West East South North Bot Top)");
+    if (!u) return set_err(ctx, MT_ERR_ARG, "null velocity");
+    return amr_set_face(ctx, *c, face, u);
+}
+
+// ---- batches ------------------------------------------------------------------
+namespace {
+int get_batch(mt_ctx *h, int32_t id, Batch **out)
+{
+    if (!h) return MT_ERR_ARG;
+    if (id < 0 || id >= (int32_t)h->c.batches.size() || !h->c.batches[id])
+        return set_err(h->c, MT_ERR_ARG, "no such batch");
+    *out = h->c.batches[id];
+    return MT_OK;
+}
+}  // namespace
+
+int mt_batch_create(mt_ctx *h, int32_t *id)
+{
+    if (!h || !id) return MT_ERR_ARG;
+    h->c.batches.push_back(new Batch());
+    *id = (int32_t)h->c.batches.size() - 1;
+    return MT_OK;
+}
+
+int mt_batch_destroy(mt_ctx *h, int32_t id)
+{
+    Batch *b;
+    int rc = get_batch(h, id, &b);
+    if (rc) return rc;
+    for (int32_t cid : b->ids) {
+        Case *c;
+        if (!get_case(h, cid, &c)) c->in_batch--;
+    }
+    cudaStreamSynchronize(h->c.stream);
+    batch_free(*b);
+    delete b;
+    h->c.batches[id] = nullptr;
+    return MT_OK;
+}
+
+int mt_batch_add(mt_ctx *h, int32_t id, int32_t case_id)
+{
+    Batch *b;
+    int rc = get_batch(h, id, &b);
+    if (rc) return rc;
+    Case *c;
+    if ((rc = get_case(h, case_id, &c))) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "batches hold built multi-level cases");
+    for (int32_t x : b->ids)
+        if (x == case_id) return set_err(ctx, MT_ERR_ARG, "the case is already in the batch");
+    if ((rc = amr_sync_f(ctx, *c))) return rc;
+    if (c->schedule != MT_SCHED_FUSED) {
+        c->schedule = MT_SCHED_FUSED;
+        c->primed = false;
+    }
+    if ((rc = amr_prime(ctx, *c))) return rc;
+    b->ids.push_back(case_id);
+    c->in_batch++;
+    batch_drop(*b);
+    return MT_OK;
+}
+
+int mt_batch_remove(mt_ctx *h, int32_t id, int32_t case_id)
+{
+    Batch *b;
+    int rc = get_batch(h, id, &b);
+    if (rc) return rc;
+    for (size_t k = 0; k < b->ids.size(); ++k)
+        if (b->ids[k] == case_id) {
+            b->ids.erase(b->ids.begin() + k);
+            Case *c;
+            if (!get_case(h, case_id, &c)) c->in_batch--;
+            batch_drop(*b);
+            return MT_OK;
+        }
+    return set_err(h->c, MT_ERR_ARG, "the case is not in the batch");
+}
+
+int mt_batch_size(mt_ctx *h, int32_t id, int32_t *n)
+{
+    Batch *b;
+    int rc = get_batch(h, id, &b);
+    if (rc) return rc;
+    if (!n) return set_err(h->c, MT_ERR_ARG, "null output");
+    *n = (int32_t)b->ids.size();
+    return MT_OK;
+}
+
+int mt_batch_step(mt_ctx *h, int32_t id, int32_t n)
+{
+    Batch *b;
+    int rc = get_batch(h, id, &b);
+    if (rc) return rc;
+    if (n < 0) return set_err(h->c, MT_ERR_ARG, "negative step count");
+    std::vector<Case *> cs;
+    for (int32_t cid : b->ids) {
+        Case *c;
+        if ((rc = get_case(h, cid, &c))) return rc;
+        cs.push_back(c);
+    }
+    return batch_step(h->c, *b, cs, n);
 }
 
 int mt_case_status(mt_ctx *h, int32_t id)

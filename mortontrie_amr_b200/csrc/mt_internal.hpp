@@ -82,6 +82,26 @@ struct Level {
     std::vector<uint8_t> raw_set;  // 0..5 sets, 16 + b for lat_bc[b]
 };
 
+// one case level in a batched brick pass
+struct BrickSlot {
+    const int32_t *halo = nullptr;
+    const uint8_t *cls = nullptr;
+    const void *fcol = nullptr;  // current post-collision buffer
+    void *f = nullptr, *fnext = nullptr, *rho = nullptr, *u = nullptr;
+    double tau = 1.0;
+    uint32_t n = 0;
+    int32_t textbook = 0, fall = 0, macros = 0;
+};
+constexpr int kMaxBatchSlots = 128;
+// a batched brick pass: slots and the prefix offsets of their bricks
+struct BrickBatch {
+    int32_t nslots = 0;
+    int32_t pad = 0;
+    int64_t total = 0;
+    int64_t off[kMaxBatchSlots + 1] = {};
+    BrickSlot slot[kMaxBatchSlots];
+};
+
 struct Case {
     mt_case_desc d{};
     bool dense = false;
@@ -113,6 +133,7 @@ struct Case {
     // lookahead buffers hold the collision of the current f
     int schedule = MT_SCHED_PHASES;
     int scaling = MT_SCALE_REFERENCE;  // interface rescaling of the non-equilibrium part
+    double face_u[6][3] = {};          // bc_velocity of each face's strategy (u_bc unless set)
     bool use_bricks = true;  // fused pass over 4x4x4 bricks where a level allows it (else cell lists)
     bool primed = false;
     int par0 = 0;
@@ -121,9 +142,27 @@ struct Case {
     // second stream of the fused schedule: the IB cells' treat + collision
     // overlaps the finest level's fused pass (disjoint cells)
     int macros_now = 0;  // set while recording a level's last substep of the coarse step
+    int pull_mode = 0;   // PH_PULL_COLLIDE: 0 every cell, 1 the IB cells only (a batch runs the bricks)
+    bool no_side = false; // IB on the calling stream (batch recording)
+    int in_batch = 0;     // batches holding the case
     bool f_stale = false; // fused passes left class-1 brick cells' streamed f unstored (amr_sync_f)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+};
+
+// Cases stepped together (mt_batch_*): one batched brick pass per level,
+// substep and model family over all of them, their other phases on parallel
+// graph branches.  Level 0 of every member swaps buffers once per coarse
+// step, so two captured graphs alternate (par).
+struct Batch {
+    std::vector<int32_t> ids;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int64_t graph_launches[2] = {0, 0};
+    BrickBatch *ddesc[2] = {nullptr, nullptr};
+    int par = 0;
+    std::vector<cudaStream_t> pool;
+    std::vector<cudaEvent_t> ev_join;
+    cudaEvent_t ev_fork = nullptr;
 };
 
 struct Ctx {
@@ -131,6 +170,7 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::vector<Case *> cases;
+    std::vector<Batch *> batches;
     std::string last_error;
     int64_t launches = 0;  // kernels this library launched (graph nodes count per replay)
 };
@@ -147,6 +187,11 @@ int amr_get(Ctx &ctx, Case &c, int level, double *h_f, double *h_fcol);
 int amr_set(Ctx &ctx, Case &c, int level, const double *h_f, const double *h_fcol);
 int amr_macros(Ctx &ctx, Case &c, int level, double *h_rho, double *h_u);
 int amr_sync_f(Ctx &ctx, Case &c);
+int amr_set_face(Ctx &ctx, Case &c, int face, const double *u);
+int amr_prime(Ctx &ctx, Case &c);
+int batch_step(Ctx &ctx, Batch &b, const std::vector<Case *> &cases, int n);
+void batch_drop(Batch &b);
+void batch_free(Batch &b);
 
 // multi-level phases, one explicit instantiation per storage type
 // (mt_amr_f64.cu builds the FP64 one without FMA contraction)
@@ -159,6 +204,8 @@ template <class S> struct AmrOps {
     static int set(Ctx &ctx, Case &c, int level, int which, const double *d_in);
     static int macros_out(Ctx &ctx, Case &c, int level, double *d_rho, double *d_u);
     static int guard(Ctx &ctx, Case &c);
+    // batched brick pass (descriptor in device memory, total bricks known on the host)
+    static int batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total);
 };
 void amr_free(Case &c);
 // forget the fused schedule's graphs and brick tables (rebuilt at the next fused step)

@@ -31,7 +31,8 @@ EXPORTS = [
     "mt_case_init_equilibrium", "mt_case_init_fields", "mt_case_set_populations", "mt_case_get_populations",
     "mt_case_get_macros", "mt_case_reduce", "mt_calculate_macros", "mt_collide", "mt_stream", "mt_explosion",
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
-    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling",
+    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_face_velocity",
+    "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step",
 ]
 
 
@@ -73,7 +74,9 @@ def lib():
             "mt_find": [vp, i32, i32, u64p, i64, i64p], "mt_case_init_equilibrium": [vp, i32, C.c_double, dp],
             "mt_case_init_fields": [vp, i32, dp, dp, dp, dp], "mt_case_set_populations": [vp, i32, i32, dp, dp],
             "mt_case_get_populations": [vp, i32, i32, dp, dp], "mt_case_get_macros": [vp, i32, i32, dp, dp],
-            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp],
+            "mt_batch_create": [vp, i32p], "mt_batch_destroy": [vp, i32], "mt_batch_add": [vp, i32, i32],
+            "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -185,6 +188,15 @@ class LBM_Manager:
         ctx.check(lib().mt_case_build(ctx.h, self.id), "mt_case_build")
         self.set_schedule(schedule)
         self.set_interface_scaling(scaling)
+        for face, u in sorted(getattr(case.params, "face_u", {}).items()):
+            self.set_face_velocity(face, u)
+
+    def set_face_velocity(self, face: int, u):
+        """Velocity of boundary face `face` (0..5 = West East South North Bot
+        Top); resets that face's boundary cells to feq(rho0, u)."""
+        u = np.ascontiguousarray(u, np.float64)
+        self.ctx.check(lib().mt_case_set_face_velocity(self.ctx.h, self.id, int(face), _ptr(u, C.c_double)),
+                       "set_face_velocity")
 
     def set_interface_scaling(self, scaling: str):
         """"reference" (the reference's factors) or "standard" (stress-continuous)."""
@@ -313,6 +325,43 @@ class LBM_Manager:
         """Raise MTError (MT_ERR_NONFINITE / MT_ERR_MESH) if the device
         guard finds a problem; returns None when healthy."""
         self.ctx.check(lib().mt_case_status(self.ctx.h, self.id), "mt_case_status")
+
+
+class Batch:
+    """Independent multi-level cases stepped together (mt_batch_*): one
+    batched brick pass per level, substep and model family; each member ends
+    a step exactly where it would stepped alone under the fused schedule."""
+
+    def __init__(self, ctx: Context, managers=()):
+        self.ctx = ctx
+        bid = C.c_int32()
+        ctx.check(lib().mt_batch_create(ctx.h, C.byref(bid)), "mt_batch_create")
+        self.id = bid.value
+        self.members = []
+        for m in managers:
+            self.add(m)
+
+    def add(self, mgr):
+        self.ctx.check(lib().mt_batch_add(self.ctx.h, self.id, mgr.id), "mt_batch_add")
+        mgr.schedule = "fused"
+        self.members.append(mgr)
+
+    def remove(self, mgr):
+        self.ctx.check(lib().mt_batch_remove(self.ctx.h, self.id, mgr.id), "mt_batch_remove")
+        self.members.remove(mgr)
+
+    def __len__(self):
+        n = C.c_int32()
+        self.ctx.check(lib().mt_batch_size(self.ctx.h, self.id, C.byref(n)), "mt_batch_size")
+        return n.value
+
+    def step(self, n=1):
+        self.ctx.check(lib().mt_batch_step(self.ctx.h, self.id, int(n)), "mt_batch_step")
+
+    def close(self):
+        if getattr(self, "id", None) is not None and self.ctx.h:
+            lib().mt_batch_destroy(self.ctx.h, self.id)
+        self.id = None
 
 
 class DenseCase:

@@ -123,6 +123,7 @@ typedef struct {
     int64_t extent0[3];
     double tau[OC_MAXL];
     double rho0, u_bc[3];
+    double face_u[6][3]; /* bc_velocity of each face strategy */
     oc_level lv[OC_MAXL];
     int64_t ndis;
     uint64_t *dis_key;
@@ -480,6 +481,7 @@ void *oc_case_new(int q, int max_level, int collision, int ib_method, int bc_mod
         c->periodic[a] = periodic[a];
         c->extent0[a] = extent0[a];
         c->u_bc[a] = u_bc[a];
+        for (int f = 0; f < 6; ++f) c->face_u[f][a] = u_bc[a];
     }
     for (int l = 0; l <= max_level; ++l) c->tau[l] = tau[l];
     c->rho0 = rho0;
@@ -830,7 +832,7 @@ static int phase_bc_neq(oc_case *c)
                     uint64_t nk = find_neighbor(c, lv->key[i], 0, EX[k], EY[k], EZ[k]);
                     int64_t nb = find_idx(lv, nk);
                     if (nb < 0) return -5;
-                    double fw = feq_bgk_one(q, lv->rho[i], c->u_bc, k);
+                    double fw = feq_bgk_one(q, lv->rho[i], c->face_u[face], k);
                     double fn = feq_bgk_one(q, lv->rho[nb], &lv->u[3 * nb], k);
                     lv->f[k * lv->n + i] = fw + lv->f[k * lv->n + nb] - fn;
                 }
@@ -961,7 +963,7 @@ static int phase_bc_inout(oc_case *c)
             int64_t nb = find_idx(lv, nk);
             if (nb < 0) return -6;
             if (face == 0) {
-                feq_bgk(q, c->rho0, c->u_bc, feq);
+                feq_bgk(q, c->rho0, c->face_u[0], feq);
                 for (int k = 0; k < q; ++k) {
                     lv->fcol[k * lv->n + i] = feq[k];
                     lv->f[k * lv->n + i] = feq[k];
@@ -971,6 +973,32 @@ static int phase_bc_inout(oc_case *c)
                     lv->fcol[k * lv->n + i] = lv->fcol[k * lv->n + nb];
                     lv->f[k * lv->n + i] = lv->fcol[k * lv->n + nb];
                 }
+            }
+        }
+    }
+    return 0;
+}
+
+/* Velocity of one face strategy (the input_v of
+ * nonEquilibrumExtrapolation_<face>, NonEquilibrumExtrapolation.hpp:37-100)
+ * and the face's boundary cells reset to f = fcol = feq(rho0, u) as
+ * D3Q19_BC_Strategy::initial_Feq does (D3Q19_BC_Manager.hpp:157-167). */
+int oc_set_face_velocity(void *h, int face, const double *u)
+{
+    oc_case *c = (oc_case *)h;
+    if (face < 0 || face > 5) return -1;
+    oc_level *lv = &c->lv[0];
+    double feq[27];
+    for (int a = 0; a < 3; ++a) c->face_u[face][a] = u[a];
+    feq_bgk(c->q, c->rho0, u, feq);
+    for (int g = 0; g < 9; ++g) {
+        int b = FACE_SETS[face][g];
+        if (b < 0) break;
+        for (int64_t j = 0; j < lv->nbc[b]; ++j) {
+            int64_t i = lv->bclist[b][j];
+            for (int k = 0; k < c->q; ++k) {
+                lv->f[k * lv->n + i] = feq[k];
+                lv->fcol[k * lv->n + i] = feq[k];
             }
         }
     }

@@ -44,6 +44,7 @@ def lib():
         L.oc_neighbors.argtypes = [vp, i32, C.POINTER(C.c_int32)]
         L.oc_neighbor_keys.argtypes = [vp, i32, u64p, i64, u64p]
         L.oc_collide_cell.argtypes = [i32, i32, dp, C.c_double, dp, C.c_double, dp]
+        L.oc_set_face_velocity.argtypes = [vp, i32, dp]
         _lib = L
     return _lib
 
@@ -88,6 +89,9 @@ class OracleCase:
             raise ValueError("oracle build failed")
         u0 = np.array(p.u_bc, np.float64)
         lib().oc_init_equilibrium(self.h, p.rho0, _p(u0, C.c_double))
+        for face, u in sorted(getattr(p, "face_u", {}).items()):
+            uf = np.array(u, np.float64)
+            lib().oc_set_face_velocity(self.h, int(face), _p(uf, C.c_double))
 
     def __del__(self):
         if getattr(self, "h", None):
