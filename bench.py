@@ -268,6 +268,12 @@ def run_ours(args):
             amr = amr_section(ctx, torch)
         except Exception as exc:  # reported, not hidden: the line says why the section is missing
             amr = {"error": repr(exc)}
+    batched = None
+    if not args.no_batched and world == 1:
+        try:
+            batched = batched_section(ctx, torch)
+        except Exception as exc:
+            batched = {"error": repr(exc)}
 
     if rank == 0:
         cpu = cpu_baseline_sample() if (world == 1 and not args.no_cpu_baseline) else None
@@ -290,6 +296,7 @@ def run_ours(args):
             "diagnostics": {"mass": red["mass"], "kinetic_energy": red["kinetic_energy"]},
             "cpu_baseline": cpu,
             "amr_cumulant_sphere": amr,
+            "batched_uneven": batched,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -355,6 +362,121 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
         out[st]["mass_drift_vs_f64"] = float(abs(r["rho"].sum() - ref["rho"].sum()) / ref["rho"].sum())
         out[st]["speedup_vs_f64"] = round(res["f64"]["secs"] / r["secs"], 3)
     return out
+
+
+def _build_specs(specs):
+    """Host meshes of many cases, built in parallel worker processes (spawned:
+    the parent already holds a CUDA context)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    workers = max(1, min(len(specs), (os.cpu_count() or 2) - 1, 32))
+    from mortontrie_amr_b200.workloads import build_spec
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(build_spec, specs))
+
+
+def batched_section(ctx, torch, steps=20, warmup=2, solve_steps=2000, n_cases=64, seed=4):
+    """Batched uneven instances: 64 seeded cases (cavities and spheres, 4
+    domain sizes, 1-3 refinement levels, Re 10-200, D3Q19 LBGK or D3Q27
+    cumulant, stress-continuous interface factors).  All cases in one batch
+    (FP16 storage, fused schedule, one batched brick pass per level, substep
+    and model) against the same cases solved one at a time in the plain form
+    (FP64, phase order) and one at a time with FP16 storage.  Cases/h assume
+    `solve_steps` coarse steps per case at the measured per-step times;
+    accuracy compares the batched FP16 state with plain FP64 after the same
+    number of coarse steps."""
+    from mortontrie_amr_b200.lbm import Batch, LBM_Manager, drag_coefficient
+    from mortontrie_amr_b200.workloads import batched_uneven_cases
+    specs = batched_uneven_cases(seed, n_cases)
+    t0 = time.time()
+    cases = _build_specs(specs)
+    build_s = time.time() - t0
+    stream = torch.cuda.current_stream()
+    upd = []
+    for c in cases:
+        m = c.mesh
+        L = m.spec.max_level
+        upd.append(sum((int(m.levels[l]["lat_f"].size + m.levels[l]["overlap_C2F"].size) << l) for l in range(L + 1)))
+    total_steps = warmup + steps
+
+    def timed(fn, k):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn(k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    # batched, FP16
+    t0 = time.time()
+    members = [LBM_Manager(ctx, c, "f16", schedule="fused", scaling="standard") for c in cases]
+    batch = Batch(ctx, members)
+    batch.step(warmup)
+    torch.cuda.synchronize()
+    setup_b = time.time() - t0
+    tb = timed(batch.step, steps) / steps
+    res_b = [_case_result(m, c) for m, c in zip(members, cases)]
+    batch.close()
+    for m in members:
+        m.close()
+    # one at a time: plain FP64, and FP16 fused
+    out_single = {}
+    res_p = None
+    for label, storage, schedule in (("plain_f64", "f64", "phases"), ("f16_one_at_a_time", "f16", "fused")):
+        per = []
+        res = []
+        for c in cases:
+            mgr = LBM_Manager(ctx, c, storage, schedule=schedule, scaling="standard")
+            mgr.fluidSimulate(warmup)
+            per.append(timed(mgr.fluidSimulate, steps) / steps)
+            if label == "plain_f64":
+                res.append(_case_result(mgr, c))
+            mgr.close()
+        if label == "plain_f64":
+            res_p = res
+        solve = solve_steps * sum(per)
+        out_single[label] = {"ms_per_coarse_step_all_cases": round(1e3 * sum(per), 3),
+                             "cases_per_hour": round(len(cases) * 3600.0 / solve, 1),
+                             "mlups": round(sum(upd) / sum(per) / 1e6, 1)}
+    solve_b = solve_steps * tb
+    l2 = [float(np.linalg.norm(b["u"] - p["u"]) / max(np.linalg.norm(p["u"]), 1e-300)) for b, p in zip(res_b, res_p)]
+    finite = [bool(np.isfinite(b["u"]).all() and np.isfinite(p["u"]).all()) for b, p in zip(res_b, res_p)]
+    drag = [abs(b["cd"] - p["cd"]) / abs(p["cd"]) for b, p, c in zip(res_b, res_p, cases)
+            if c.mesh.spec.sphere is not None and np.isfinite(p["cd"]) and abs(p["cd"]) > 1e-6]
+    fin_l2 = [x for x, f in zip(l2, finite) if f]
+    return {
+        "workload": f"{len(cases)} seeded cases (seed {seed}): cavity/sphere, 32^3..128x64x64, 1-3 levels, "
+                    "Re 10-200, D3Q19 LBGK / D3Q27 cumulant, stress-continuous interface factors",
+        "cell_updates_per_coarse_step": int(sum(upd)), "host_mesh_build_s": round(build_s, 1),
+        "batch_setup_s": round(setup_b, 2), "coarse_steps_timed": steps, "solve_coarse_steps": solve_steps,
+        "batched_f16": {"ms_per_coarse_step_all_cases": round(1e3 * tb, 3),
+                        "cases_per_hour": round(len(cases) * 3600.0 / solve_b, 1),
+                        "mlups": round(sum(upd) / tb / 1e6, 1)},
+        **out_single,
+        "speedup_vs_plain_one_at_a_time": round(out_single["plain_f64"]["ms_per_coarse_step_all_cases"] /
+                                                (1e3 * tb), 2),
+        "accuracy_after_steps": total_steps,
+        "finite_cases": int(sum(finite)),
+        "velocity_l2_vs_plain_f64": {"median": float(np.median(fin_l2)) if fin_l2 else None,
+                                     "max": float(np.max(fin_l2)) if fin_l2 else None},
+        "drag_rel_vs_plain_f64": {"median": float(np.median(drag)) if drag else None,
+                                  "max": float(np.max(drag)) if drag else None, "sphere_cases": len(drag)},
+    }
+
+
+def _case_result(mgr, case):
+    from mortontrie_amr_b200.lbm import drag_coefficient
+    L = case.mesh.spec.max_level
+    us = []
+    for l in range(L + 1):
+        _, u = mgr.macros(l)
+        _, tags = mgr.keys(l)
+        us.append(u[:, (tags & 1) != 0])
+    cd = float("nan")
+    if case.mesh.spec.sphere is not None:
+        cd = drag_coefficient(mgr.force(), float(case.params.u_bc[0]), 2.0 * case.mesh.spec.sphere.radius * (1 << L))
+    return {"u": np.concatenate(us, axis=1), "cd": cd}
 
 
 ACCURACY_CASES = {
@@ -503,6 +625,8 @@ def main():
     ap.add_argument("--no-amr", action="store_true", help="skip the 4-level cumulant sphere section")
     ap.add_argument("--amr-only", action="store_true",
                     help="only the 4-level cumulant sphere section (K coarse steps per storage; profiling runs)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven instances section")
+    ap.add_argument("--batched-only", action="store_true", help="only the batched uneven instances section")
     ap.add_argument("--amr-variants", default=None,
                     help="comma list of multi-level runs to time (default all: "
                          "f64,f64_fused,f32,f16,bf16,f16_phases); profiling runs")
@@ -520,6 +644,16 @@ def main():
     N_EDGE = args.edge
     if args.impl == "reference":
         run_reference(args)
+    elif args.batched_only:
+        import torch
+
+        from mortontrie_amr_b200.lbm import Context
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx = Context(0)
+        ctx.set_stream(stream.cuda_stream)
+        print(json.dumps({"batched_uneven": batched_section(ctx, torch, steps=args.steps)}), flush=True)
+        ctx.close()
     elif args.amr_accuracy:
         import torch
 

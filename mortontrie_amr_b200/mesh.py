@@ -81,7 +81,7 @@ class Mesh:
         parts = [self.levels[level][s] for s in SET_NAMES]
         if level == 0:
             parts += list(self.lat_bc)
-        return np.unique(np.concatenate(parts)) if parts else np.zeros(0, np.uint64)
+        return _sorted_unique(np.concatenate(parts)) if parts else np.zeros(0, np.uint64)
 
     def n_cells(self) -> list:
         return [int(self.all_keys(l).size) for l in range(self.spec.max_level + 1)]
@@ -121,7 +121,23 @@ def _neighbours(x, y, z, q, extent, periodic):
 
 
 def _sorted_unique(a):
-    return np.unique(np.asarray(a, np.uint64))
+    a = np.sort(np.asarray(a, np.uint64))
+    if a.size < 2:
+        return a
+    keep = np.empty(a.size, bool)
+    keep[0] = True
+    np.not_equal(a[1:], a[:-1], out=keep[1:])
+    return a[keep]
+
+
+def _in_sorted(a, sorted_b):
+    """Membership of each key of a in the sorted unique array sorted_b."""
+    a = np.asarray(a, np.uint64)
+    if sorted_b.size == 0 or a.size == 0:
+        return np.zeros(a.size, bool)
+    idx = np.searchsorted(sorted_b, a)
+    np.minimum(idx, sorted_b.size - 1, out=idx)
+    return sorted_b[idx] == a
 
 
 def build_mesh(spec: MeshSpec) -> Mesh:
@@ -206,9 +222,10 @@ def build_mesh(spec: MeshSpec) -> Mesh:
                 ok = (a >= 0) & (b >= 0) & (c >= 0)
                 cand.append(cell_key(L, l, a[ok], b[ok], c[ok]))
             cand = _sorted_unique(np.concatenate(cand)) if cand else np.zeros(0, np.uint64)
-            keep = ~np.isin(cand, sets["lat_f"]) & ~np.isin(cand, sets["overlap_C2F"])
+            keep = ~_in_sorted(cand, sets["lat_f"]) & ~_in_sorted(cand, sets["overlap_C2F"])
             sets["ghost_overlap_C2F"] = cand[keep]
-            bad = np.isin(sets["ghost_overlap_C2F"], sets["overlap_F2C"]) | np.isin(sets["ghost_overlap_C2F"], sets["lat_sf"])
+            bad = (_in_sorted(sets["ghost_overlap_C2F"], sets["overlap_F2C"])
+                   | _in_sorted(sets["ghost_overlap_C2F"], sets["lat_sf"]))
             if np.any(bad):
                 raise ValueError(f"level {l}: ghost layer overlaps the next interface or the solid")
         else:
@@ -220,7 +237,7 @@ def build_mesh(spec: MeshSpec) -> Mesh:
                 ok = (a >= 0) & (b >= 0) & (c >= 0)
                 cand.append(cell_key(L, l, a[ok], b[ok], c[ok]))
             cand = _sorted_unique(np.concatenate(cand)) if cand else np.zeros(0, np.uint64)
-            sets["ghost_overlap_F2C"] = cand[np.isin(cand, sets["lat_f"])]
+            sets["ghost_overlap_F2C"] = cand[_in_sorted(cand, sets["lat_f"])]
         else:
             sets["ghost_overlap_F2C"] = np.zeros(0, np.uint64)
 
@@ -233,7 +250,7 @@ def build_mesh(spec: MeshSpec) -> Mesh:
         sx, sy, sz = _coords_of(sf_keys, L, L)
         for (a, b, c) in _neighbours(sx, sy, sz, q, extents[L], periodic):
             k = cell_key(L, L, a, b, c)
-            if np.any(np.isin(k, levels[L]["overlap_C2F"])) or np.any(np.isin(k, levels[L]["ghost_overlap_C2F"])):
+            if np.any(_in_sorted(k, levels[L]["overlap_C2F"])) or np.any(_in_sorted(k, levels[L]["ghost_overlap_C2F"])):
                 raise ValueError("solid too close to the coarse/fine interface")
     return Mesh(spec=spec, levels=levels, lat_bc=lat_bc, dis_keys=dis_keys, dis_rows=dis_rows,
                 extent=extents)
