@@ -45,12 +45,14 @@ extern "C" {
 #define MT_SET_GHOST_C2F 3
 #define MT_SET_GHOST_F2C 4
 #define MT_SET_LAT_SF 5
+#define MT_SET_IB_BAND 6  /* finest-level cells the markers' forcing can reach (MT_IB_DF; no reference counterpart) */
 #define MT_SET_LAT_BC0 16 /* MT_SET_LAT_BC0 + b, b = 0..25 in Bdry_Type order (D3Q19_BC_Manager.hpp:25-53) */
 
 #define MT_COLL_LBGK 0     /* Collision_LBGK, lbm_kernel/Collision_Manager.cpp:13-53 */
 #define MT_COLL_CUMULANT 1 /* Collision_Cumulant, lbm_kernel/Collision_Cumulant.cpp:22-652 (Q = 27) */
 #define MT_IB_DW 0         /* SinglePointInterpolation, distance weighted */
 #define MT_IB_FH 1         /* SinglePointInterpolation, Filippova-Haenel */
+#define MT_IB_DF 2         /* direct forcing on Lagrangian markers (no reference counterpart) */
 #define MT_BC_NEQ 0        /* nonEquilibrumExtrapolation_* (BC/NonEquilibrumExtrapolation.cpp) */
 #define MT_BC_ZOUHE_OUTFLOW 1 /* velocity inlet on West, zero-gradient outflow on East */
 #define MT_PULL_REFERENCE 0   /* f_q(x) = fcol_q(x + e_q), Stream_Manager.cpp:43-76 */
@@ -191,6 +193,18 @@ int mt_case_set_interface_scaling(mt_ctx *ctx, int32_t case_id, int32_t scaling)
  * velocity map (D3Q19_BC_Manager.hpp:157-167): boundary cells never collide,
  * so this is the velocity the fluid sees (a moving lid). */
 int mt_case_set_face_velocity(mt_ctx *ctx, int32_t case_id, int32_t face, const double *u);
+
+/* Lagrangian markers of a direct-forcing sphere (MT_IB_DF, no reference
+ * counterpart; after mt_case_build).  ref[3][nm]: marker offsets from the
+ * centre and dv[nm] their volume weights, in finest-level cells; center[3]
+ * in finest-level cells; path[period][6]: the centre's displacement and
+ * velocity at finest substep t (row t % period).  Each finest substep the
+ * velocity at a marker is interpolated with the 3-point kernel of Roma,
+ * Peskin & Berger, the force 2 rho (U - u) is spread back onto the
+ * MT_SET_IB_BAND cells (exact int64 fixed-point sums), and the band cells
+ * collide with Guo forcing; mt_get_force accumulates the force on the body. */
+int mt_case_set_markers(mt_ctx *ctx, int32_t case_id, int64_t nm, const double *ref, const double *dv,
+                        const double *center, int64_t period, const double *path);
 
 /* ---- batches (no reference counterpart) --------------------------------
  * Independent multi-level cases stepped together: every substep of every

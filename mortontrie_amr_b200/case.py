@@ -17,7 +17,7 @@ from .lattice import directions, reference_units, weights
 from .mesh import Mesh, MeshSpec, Sphere, build_mesh
 
 COLLISIONS = {"LBGK": 0, "Cumulant": 1}
-IB_METHODS = {"DW": 0, "FH": 1}
+IB_METHODS = {"DW": 0, "FH": 1, "DF": 2}
 BC_MODES = {"neq": 0, "zouhe_outflow": 1}
 STREAM_CONVENTIONS = {"reference": 0, "textbook": 1}
 STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
@@ -117,6 +117,40 @@ def cavity_case(q=19, collision="LBGK", coarse=(32, 32, 32), max_level=1, re=100
         spec = MeshSpec(q=q, max_level=1, coarse=tuple(coarse), refine=[None], boundary=("bc", "bc", "bc"))
     p = CaseParams(q=q, collision=collision, ib_method=ib_method, bc_mode="neq", nu=nu, u_bc=(0.0, 0.0, 0.0),
                    u_ref=u_lid, face_u={5: (u_lid, 0.0, 0.0)})
+    return Case(build_mesh(spec), p)
+
+
+def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q=19, period=2000,
+                   amplitude=0.5) -> Case:
+    """Flow past a sphere represented by direct-forcing Lagrangian markers
+    (one per finest cell^2 of surface, 3-point kernel): coarse channel
+    16R x 8R x 8R, inlet on West, outflow on East, periodic sides, centre at
+    (4R, 4R, 4R), nested refinement boxes around the sphere and its path
+    (transverse oscillation of `amplitude` R along y with `period` finest
+    steps when oscillating), nu = u 2R / Re in coarse units, D3Q19 LBGK."""
+    r = int(radius)
+    nx, ny, nz = 16 * r, 8 * r, 8 * r
+    c = (4 * r, 4 * r, 4 * r)
+    amp = amplitude * r if oscillating else 0.0
+    # finest box: the band (2.7 finest cells) plus the C2F shell and a margin
+    mg = max(0.5 * r, 6.0 / (1 << max_level) + 0.5)
+    hw = [r + mg, r + amp + mg, r + mg]
+    boxes = []
+    for _ in range(max_level):
+        boxes.append(list(hw))
+        hw = [hw[0] + max(2.0, 0.5 * r), min(hw[1] + max(2.0, 0.5 * r), 4 * r - 1.0), min(hw[2] + max(2.0, 0.5 * r), 4 * r - 1.0)]
+    boxes = boxes[::-1]  # level 0 box first
+    refine = []
+    for l, b in enumerate(boxes):
+        s = 1 << l
+        refine.append((tuple(int(np.floor((c[a] - b[a]) * s)) for a in range(3)),
+                       tuple(int(np.ceil((c[a] + b[a]) * s)) for a in range(3))))
+    nu = u * 2.0 * r / re
+    spec = MeshSpec(q=q, max_level=max_level, coarse=(nx, ny, nz), refine=refine,
+                    boundary=("bc", "periodic", "periodic"), sphere=Sphere(c, float(r)), ib="markers",
+                    oscillation=(amp, period) if oscillating else None)
+    p = CaseParams(q=q, collision="LBGK", ib_method="DF", bc_mode="zouhe_outflow", nu=nu, u_bc=(u, 0.0, 0.0),
+                   u_ref=u)
     return Case(build_mesh(spec), p)
 
 

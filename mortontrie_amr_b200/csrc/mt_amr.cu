@@ -30,6 +30,8 @@ __global__ void k_tag_cells(const uint64_t *raw, const uint8_t *set, int64_t nra
     if (s >= 16) {
         bit = TAG_BC;
         bcidx[i] = (int8_t)(s - 16);
+    } else if (s == MT_SET_IB_BAND) {
+        bit = TAG_BAND;
     } else {
         const uint32_t bits[kNumSets] = {TAG_LATF, TAG_F2C, TAG_C2F, TAG_GC2F, TAG_GF2C, TAG_SF};
         bit = bits[s];
@@ -177,6 +179,8 @@ __global__ void k_brick_fill(const uint64_t *key, const uint32_t *tag, int64_t n
     uint8_t cls = 0;
     if (t & TAG_C2F)
         cls = 2;
+    else if ((t & TAG_LATF) && (t & TAG_BAND))
+        cls = 4;  // direct-forcing band: stream only, collided after the forcing
     else if ((t & TAG_LATF) && !(ib_level && (t & TAG_IB)))
         cls = 1;
     bcls[64 * b + m] = cls;
@@ -223,6 +227,13 @@ struct BcIs {
     const int8_t *bc;
     int8_t b;
     __host__ __device__ bool operator()(const int32_t &i) const { return bc[i] == b; }
+};
+struct LatfNotBand {
+    const uint32_t *tag;
+    __host__ __device__ bool operator()(const int32_t &i) const
+    {
+        return (tag[i] & TAG_LATF) && !(tag[i] & TAG_BAND);
+    }
 };
 struct LatfNotIb {
     const uint32_t *tag;
@@ -398,6 +409,27 @@ int amr_build(Ctx &ctx, Case &c)
         for (int b = 0; b < 26; ++b) maxn = std::max(maxn, c.lv[0].nbc[b]);
         if (maxn) MT_CUDA(ctx, cudaMallocAsync(&c.bc_tmp, sizeof(double) * 18 * maxn, ctx.stream));
     }
+    // direct-forcing band of the finest level and its collide list without the band
+    {
+        Level &fl = c.lv[L];
+        if (fl.n) {
+            int rc = select_indices(ctx, fl.n, TagHas{fl.tag, TAG_BAND}, &fl.band, &fl.nband);
+            if (rc) return rc;
+            if (fl.nband) {
+                int32_t *lat = nullptr;
+                int64_t nlat = 0;
+                rc = select_indices(ctx, fl.n, LatfNotBand{fl.tag}, &lat, &nlat);
+                if (rc) return rc;
+                rc = concat_lists(ctx, lat, nlat, fl.list[1], fl.nlist[1], &fl.collide_nb, &fl.ncollide_nb);
+                cudaFreeAsync(lat, ctx.stream);
+                if (rc) return rc;
+                MT_CUDA(ctx, cudaMallocAsync(&c.acc, sizeof(long long) * 3 * fl.n, ctx.stream));
+                MT_CUDA(ctx, cudaMemsetAsync(c.acc, 0, sizeof(long long) * 3 * fl.n, ctx.stream));
+                MT_CUDA(ctx, cudaMallocAsync(&c.tstep, sizeof(long long), ctx.stream));
+                MT_CUDA(ctx, cudaMemsetAsync(c.tstep, 0, sizeof(long long), ctx.stream));
+            }
+        }
+    }
     // cross-level child tables
     for (int l = 1; l <= L; ++l) {
         Level &cl = c.lv[l - 1], &fl = c.lv[l];
@@ -463,7 +495,8 @@ void amr_free(Case &c)
         Level &lv = c.lv[l];
         void *ptrs[] = {lv.key, lv.tag, lv.bcidx, lv.disrow, lv.nbr, lv.f, lv.fcol, lv.rho, lv.u,
                         lv.collide_list, lv.stream_list, lv.iblist, lv.expl_src, lv.expl_child, lv.coal_child,
-                        lv.fcol_alt, lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls, lv.bhalo};
+                        lv.fcol_alt, lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls, lv.bhalo,
+                        lv.band, lv.collide_nb};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         for (int s = 0; s < kNumSets; ++s)
@@ -472,7 +505,8 @@ void amr_free(Case &c)
             if (lv.bclist[b]) cudaFree(lv.bclist[b]);
         lv = Level();
     }
-    void *ptrs[] = {c.dis_key, c.dis, c.ib_force, c.force_acc, c.dev_err, c.bc_tmp};
+    void *ptrs[] = {c.dis_key, c.dis, c.ib_force, c.force_acc, c.dev_err, c.bc_tmp,
+                    c.mref, c.mdv, c.path, c.mforce, c.tstep, c.acc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     c.bc_tmp = nullptr;
@@ -481,6 +515,10 @@ void amr_free(Case &c)
     c.ib_force = nullptr;
     c.force_acc = nullptr;
     c.dev_err = nullptr;
+    c.mref = c.mdv = c.path = c.mforce = nullptr;
+    c.tstep = nullptr;
+    c.acc = nullptr;
+    c.nm = 0;
     if (c.graph) cudaGraphExecDestroy(c.graph);
     c.graph = nullptr;
     for (int p = 0; p < 2; ++p) {
@@ -501,7 +539,7 @@ void amr_free(Case &c)
 // ----------------------------------------------------------------------------
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
        PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
-       PH_SYNC_F, PH_FACE_EQ0 = 24 };
+       PH_SYNC_F, PH_DF, PH_FACE_EQ0 = 24 };
 
 int amr_phase(Ctx &ctx, Case &c, int phase, int level)
 {
@@ -619,6 +657,7 @@ static int fused_lbm_kernel(Ctx &ctx, Case &c, int l, bool last_parent)
         if (sub == 0 && l > 0) RUN(PH_EXPLOSION, l);
         c.macros_now = last && !(l == 0 && c.d.bc_mode == MT_BC_NEQ);
         RUN(PH_PULL_COLLIDE, l);
+        if (l == L && c.lv[l].nband) RUN(PH_DF, l);
         if (l == 0 && c.d.bc_mode == MT_BC_NEQ) RUN(PH_BC, 0);
         if (l < L) RUN(PH_COAL_COLLIDE, l);
         c.macros_now = 0;
@@ -719,9 +758,10 @@ static int prime_fused(Ctx &ctx, Case &c)
             if (rc) return rc;
         }
         if (!lv.bricks && !lv.fused_list && lv.nlist[0]) {
-            int rc = (l == L && l > 0) ? select_indices(ctx, lv.n, LatfNotIb{lv.tag}, &lv.fused_list, &lv.nfused)
-                                       : select_indices(ctx, lv.n, TagHas{lv.tag, TAG_LATF}, &lv.fused_list,
-                                                        &lv.nfused);
+            int rc = lv.nband ? select_indices(ctx, lv.n, LatfNotBand{lv.tag}, &lv.fused_list, &lv.nfused)
+                     : (l == L && l > 0) ? select_indices(ctx, lv.n, LatfNotIb{lv.tag}, &lv.fused_list, &lv.nfused)
+                                         : select_indices(ctx, lv.n, TagHas{lv.tag, TAG_LATF}, &lv.fused_list,
+                                                          &lv.nfused);
             if (rc) return rc;
         }
         int rc = amr_phase(ctx, c, PH_PRIME, l);
@@ -956,6 +996,9 @@ int batch_lbm_kernel(Ctx &ctx, BatchRec &R, const std::vector<Case *> &all, int 
                 MT_CUDA(ctx, cudaStreamWaitEvent(main, B.ev_join[p], 0));
             }
         }
+        if ((rc = fork_cases(ctx, R, cs, [&](Case &c) { return l == c.d.max_level && c.lv[l].nband > 0; },
+                             [&](Case &c) { return amr_phase(ctx, c, PH_DF, l); })))
+            return rc;
         if ((rc = fork_cases(ctx, R, cs,
                              [&](Case &c) { return (l == 0 && c.d.bc_mode == MT_BC_NEQ) || l < c.d.max_level; },
                              [&](Case &c) {

@@ -20,7 +20,7 @@ namespace mt {
 
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
        PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
-       PH_SYNC_F, PH_FACE_EQ0 = 24 };
+       PH_SYNC_F, PH_DF, PH_FACE_EQ0 = 24 };
 
 // reserved boundary directions; one copy per translation unit, uploaded by
 // AmrOps<S>::upload_tables when a case of that storage type is built
@@ -631,6 +631,7 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
             for (int k = 0; k < Q; ++k) fnext[(uint32_t)k * n + i] = v[k];
             continue;
         }
+        if (cls == 4) continue;  // direct-forcing band: collided after the forcing
         C d[Q];
 #pragma unroll
         for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::cv(v[k]), k);
@@ -758,6 +759,148 @@ __global__ void k_ib_collide(const int32_t *list, int64_t nl, int64_t n, const i
         u[2 * n + i] = z;
     }
     collide_store<Q, S, COLL>(g, r, x, y, z, tau, fnext, n, i);
+}
+
+// ---- direct-forcing immersed boundary (Lagrangian markers) --------------------
+// No reference counterpart: a rigid sphere represented by surface markers on
+// the finest level, explicit direct forcing (Uhlmann 2005) with the 3-point
+// kernel of Roma, Peskin & Berger (1999) and Guo forcing in the collision.
+// The Eulerian force of a substep is spread into int64 fixed point (2^-32),
+// so the atomic sums are exact and independent of the order of arrival.
+constexpr double kForceScale = 4294967296.0;  // 2^32
+
+__host__ __device__ __forceinline__ double roma3(double r)
+{
+    r = fabs(r);
+    if (r <= 0.5) return (1.0 + sqrt(1.0 - 3.0 * r * r)) / 3.0;
+    if (r <= 1.5) {
+        const double a = 1.0 - r;
+        return (5.0 - 3.0 * r - sqrt(1.0 - 3.0 * a * a)) / 6.0;
+    }
+    return 0.0;
+}
+
+// rho and the unforced velocity of the band cells from their streamed f
+template <int Q, class S>
+__global__ void k_band_macros(const int32_t *band, int64_t nb, int64_t n, const S *f, typename Store<S>::C *rho,
+                              typename Store<S>::C *u)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nb) return;
+    const int64_t i = band[j];
+    C d[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::ld(f, k * n + i), k);
+    C r, x, y, z;
+    macros_g<Q, C>(d, r, x, y, z);
+    rho[i] = r;
+    u[i] = x;
+    u[n + i] = y;
+    u[2 * n + i] = z;
+}
+
+static __global__ void k_band_clear(const int32_t *band, int64_t nb, int64_t n, long long *acc)
+{
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nb) return;
+    const int64_t i = band[j];
+    acc[i] = 0;
+    acc[n + i] = 0;
+    acc[2 * n + i] = 0;
+}
+
+// one marker: interpolate rho and u at X(t), force F = 2 rho (U - u), spread
+// F dv phi into the band cells; fk receives -F dv (the force on the body)
+template <class C>
+__global__ void k_df_markers(int64_t nm, const double *ref, const double *dv, double cx, double cy, double cz,
+                             const double *path, int64_t period, const long long *tstep, const uint64_t *key,
+                             const uint32_t *tag, int64_t n, const C *rho, const C *u, long long *acc, double *fk)
+{
+    const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (m >= nm) return;
+    const int64_t ph = *tstep % period;
+    const double *pp = path + 6 * ph;
+    const double X = cx + pp[0] + ref[m], Y = cy + pp[1] + ref[nm + m], Z = cz + pp[2] + ref[2 * nm + m];
+    const double ubx = pp[3], uby = pp[4], ubz = pp[5];
+    const int64_t ix = (int64_t)floor(X), iy = (int64_t)floor(Y), iz = (int64_t)floor(Z);
+    int32_t idx[27];
+    double wgt[27];
+    double r = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
+    for (int c = 0; c < 27; ++c) {
+        const int64_t x = ix + c % 3 - 1, y = iy + (c / 3) % 3 - 1, z = iz + c / 9 - 1;
+        const double wv = roma3((double)x + 0.5 - X) * roma3((double)y + 0.5 - Y) * roma3((double)z + 0.5 - Z);
+        int32_t i = -1;
+        if (x >= 0 && y >= 0 && z >= 0) {
+            const uint64_t k = dilate3((uint64_t)x) | (dilate3((uint64_t)y) << 1) | (dilate3((uint64_t)z) << 2);
+            i = (int32_t)find_key(key, n, k);
+            if (i >= 0 && !(tag[i] & TAG_BAND)) i = -1;
+        }
+        idx[c] = i;
+        wgt[c] = wv;
+        if (i >= 0) {
+            r += wv * (double)rho[i];
+            vx += wv * (double)u[i];
+            vy += wv * (double)u[n + i];
+            vz += wv * (double)u[2 * n + i];
+        }
+    }
+    const double fx = 2.0 * r * (ubx - vx), fy = 2.0 * r * (uby - vy), fz = 2.0 * r * (ubz - vz);
+    const double d = dv[m];
+    for (int c = 0; c < 27; ++c) {
+        const int32_t i = idx[c];
+        if (i < 0) continue;
+        const double s = wgt[c] * d;
+        atomicAdd((unsigned long long *)(acc + i), (unsigned long long)__double2ll_rn(fx * s * kForceScale));
+        atomicAdd((unsigned long long *)(acc + n + i), (unsigned long long)__double2ll_rn(fy * s * kForceScale));
+        atomicAdd((unsigned long long *)(acc + 2 * n + i), (unsigned long long)__double2ll_rn(fz * s * kForceScale));
+    }
+    fk[m] = -fx * d;
+    fk[nm + m] = -fy * d;
+    fk[2 * nm + m] = -fz * d;
+}
+
+static __global__ void k_df_tick(long long *tstep) { *tstep += 1; }
+
+// LBGK collision with Guo forcing on the band cells: u = (j + g / 2) / rho,
+// fcol = f - (f - feq(rho, u)) / tau + (1 - 1 / (2 tau)) w [3 (e - u) + 9 (e.u) e].g
+// (the band's rho and unforced velocity are written by k_band_macros)
+template <int Q, class S>
+__global__ void k_band_collide(const int32_t *band, int64_t nb, int64_t n, double tau, const S *f,
+                               const long long *acc, S *fcol)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nb) return;
+    const int64_t i = band[j];
+    C d[Q];
+    C r = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        d[k] = full_of<S, Q>(T::ld(f, k * n + i), k);
+        r += d[k];
+        jx += d[k] * ex(k);
+        jy += d[k] * ey(k);
+        jz += d[k] * ez(k);
+    }
+    const C gx = (C)((double)acc[i] / kForceScale), gy = (C)((double)acc[n + i] / kForceScale),
+            gz = (C)((double)acc[2 * n + i] / kForceScale);
+    const C rs = (r > C(-1e-6) && r < C(1e-6)) ? ((r < C(0)) ? C(-1e-6) : C(1e-6)) : r;
+    const C x = (jx + gx * C(0.5)) / rs, y = (jy + gy * C(0.5)) / rs, z = (jz + gz * C(0.5)) / rs;
+    const C om = C(1) / C(tau);
+    const C fpre = C(1) - C(0.5) * om;
+    const C uu = x * x + y * y + z * z;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        const C eu = ex(k) * x + ey(k) * y + ez(k) * z;
+        const C feq = r * (C)w<Q>(k) * (C(1) + C(3) * eu + C(4.5) * eu * eu - C(1.5) * uu);
+        const C ge = (C(3) * (ex(k) - x) + C(9) * eu * ex(k)) * gx + (C(3) * (ey(k) - y) + C(9) * eu * ey(k)) * gy +
+                     (C(3) * (ez(k) - z) + C(9) * eu * ez(k)) * gz;
+        const C out = d[k] - (d[k] - feq) * om + fpre * (C)w<Q>(k) * ge;
+        T::st(fcol, k * n + i, stored_of<S, Q>(out, k));
+    }
 }
 
 // fixed-order reduction of the per-cell IB force into the accumulator
@@ -922,6 +1065,53 @@ inline double f2c_scale(const Case &c, int coarse)
     return c.scaling == MT_SCALE_STANDARD ? (2.0 * tc) / tf : tc / (2.0 * tf);
 }
 
+// the direct-forcing step on level l (after its stream): band macros, the
+// markers' interpolation and spreading, the body force
+template <class S, int Q>
+int df_force(Ctx &ctx, Case &c, int l)
+{
+    using A = AmrTyped<S>;
+    using C = typename Store<S>::C;
+    cudaStream_t s = ctx.stream;
+    Level &lv = c.lv[l];
+    if (!lv.nband) return MT_OK;
+    k_band_macros<Q, S><<<grid_for(lv.nband, 128), 128, 0, s>>>(lv.band, lv.nband, lv.n, A::f(lv), A::rho(lv),
+                                                                 A::u(lv));
+    MT_LAUNCHED(ctx);
+    k_band_clear<<<grid_for(lv.nband, 256), 256, 0, s>>>(lv.band, lv.nband, lv.n, c.acc);
+    MT_LAUNCHED(ctx);
+    if (!c.nm) {
+        k_force_tick<<<1, 1, 0, s>>>(c.force_acc);
+        MT_LAUNCHED(ctx);
+        return MT_OK;
+    }
+    k_df_markers<C><<<grid_for(c.nm, 64), 64, 0, s>>>(c.nm, c.mref, c.mdv, c.center[0], c.center[1], c.center[2],
+                                                       c.path, c.period, c.tstep, lv.key, lv.tag, lv.n,
+                                                       (const C *)A::rho(lv), (const C *)A::u(lv), c.acc, c.mforce);
+    MT_LAUNCHED(ctx);
+    k_df_tick<<<1, 1, 0, s>>>(c.tstep);
+    MT_LAUNCHED(ctx);
+    const unsigned nb = grid_for(c.nm, 256);
+    double *partial = c.mforce + 3 * c.nm;
+    k_force_partial<<<nb, 256, 0, s>>>(c.mforce, c.nm, partial);
+    MT_LAUNCHED(ctx);
+    k_force_reduce<<<1, 256, 0, s>>>(partial, nb, c.force_acc);
+    MT_LAUNCHED(ctx);
+    return MT_OK;
+}
+
+template <class S, int Q>
+int band_collide(Ctx &ctx, Case &c, int l, void *out)
+{
+    using A = AmrTyped<S>;
+    Level &lv = c.lv[l];
+    if (!lv.nband) return MT_OK;
+    k_band_collide<Q, S><<<grid_for(lv.nband, 64), 64, 0, ctx.stream>>>(lv.band, lv.nband, lv.n, c.d.tau[l],
+                                                                         A::f(lv), c.acc, (S *)out);
+    MT_LAUNCHED(ctx);
+    return MT_OK;
+}
+
 template <class S, int Q>
 int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
 {
@@ -938,25 +1128,30 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
-    case PH_COLLIDE:
-        if (lv.ncollide) {
+    case PH_COLLIDE: {
+        // the direct-forcing band collides with its force (band_collide)
+        const int32_t *cl = lv.nband ? lv.collide_nb : lv.collide_list;
+        const int64_t ncl = lv.nband ? lv.ncollide_nb : lv.ncollide;
+        if (ncl) {
             if (c.d.collision == MT_COLL_LBGK) {
-                k_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.ncollide, B), B, 0, s>>>(
-                    lv.collide_list, lv.ncollide, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv));
+                k_collide<Q, S, MT_COLL_LBGK><<<grid_for(ncl, B), B, 0, s>>>(cl, ncl, n, c.d.tau[l], A::f(lv),
+                                                                             A::rho(lv), A::u(lv), A::fcol(lv));
             } else {
                 // the cumulant model exists for D3Q27 only (checked at case creation)
                 if constexpr (Q == 27)
-                    k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.ncollide, 64), 64, 0, s>>>(
-                        lv.collide_list, lv.ncollide, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv));
+                    k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(ncl, 64), 64, 0, s>>>(
+                        cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv));
             }
             MT_LAUNCHED(ctx);
         }
+        if (int rc = band_collide<S, Q>(ctx, c, l, A::fcol(lv))) return rc;
         if (lv.nlist[2]) {
             k_copy_fcol<Q, S><<<grid_for(lv.nlist[2], B), B, 0, s>>>(lv.list[2], lv.nlist[2], n, A::f(lv),
                                                                       A::fcol(lv));
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
+    }
     case PH_STREAM:
         if (lv.nstream) {
             k_stream<Q, S><<<grid_for(lv.nstream, B), B, 0, s>>>(lv.stream_list, lv.nstream, n, c.d.stream_convention,
@@ -1017,6 +1212,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         return MT_OK;
     }
     case PH_IB: {
+        if (c.d.ib_method == MT_IB_DF) return df_force<S, Q>(ctx, c, c.d.max_level);
         Level &fl = c.lv[c.d.max_level];
         if (!fl.nib) {
             k_force_tick<<<1, 1, 0, s>>>(c.force_acc);
@@ -1085,6 +1281,10 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         }
         return MT_OK;
     }
+    case PH_DF: {
+        if (int rc = df_force<S, Q>(ctx, c, l)) return rc;
+        return band_collide<S, Q>(ctx, c, l, lv.fcol_alt);
+    }
     case PH_SYNC_F:
         if (lv.bricks) {
             k_brick_pull<Q, S><<<grid_for(lv.nbrick, 4), 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, (uint32_t)n,
@@ -1098,17 +1298,21 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         // and the copy of C2F (the first collide(level) of the next substep)
         if (!n) return MT_OK;
         MT_CUDA(ctx, cudaMemcpyAsync(lv.fcol_alt, lv.fcol, sizeof(S) * Q * n, cudaMemcpyDeviceToDevice, s));
-        if (lv.ncollide) {
-            if (c.d.collision == MT_COLL_LBGK) {
-                k_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.ncollide, B), B, 0, s>>>(
-                    lv.collide_list, lv.ncollide, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt);
-            } else {
-                if constexpr (Q == 27)
-                    k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.ncollide, 64), 64, 0, s>>>(
-                        lv.collide_list, lv.ncollide, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv),
-                        (S *)lv.fcol_alt);
+        {
+            const int32_t *cl = lv.nband ? lv.collide_nb : lv.collide_list;
+            const int64_t ncl = lv.nband ? lv.ncollide_nb : lv.ncollide;
+            if (ncl) {
+                if (c.d.collision == MT_COLL_LBGK) {
+                    k_collide<Q, S, MT_COLL_LBGK><<<grid_for(ncl, B), B, 0, s>>>(
+                        cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt);
+                } else {
+                    if constexpr (Q == 27)
+                        k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(ncl, 64), 64, 0, s>>>(
+                            cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt);
+                }
+                MT_LAUNCHED(ctx);
             }
-            MT_LAUNCHED(ctx);
+            if (int rc = band_collide<S, Q>(ctx, c, l, lv.fcol_alt)) return rc;
         }
         if (lv.nlist[2]) {
             k_copy_fcol<Q, S><<<grid_for(lv.nlist[2], B), B, 0, s>>>(lv.list[2], lv.nlist[2], n, A::f(lv),
@@ -1122,7 +1326,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         // (its cells are disjoint from the fused pass: on the side stream when
         // the case has one, overlapping the pass)
         const int L = c.d.max_level;
-        const bool ib_level = l == L && l > 0;
+        const bool ib_level = l == L && l > 0 && c.d.ib_method != MT_IB_DF;
         const int tb = c.d.stream_convention;
         const int mac = c.macros_now;
         // level 0's boundary sweep reads the streamed f of inner cells
@@ -1199,6 +1403,11 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             if (lv.nlist[2]) {
                 k_pull_copy<Q, S><<<grid_for(lv.nlist[2], B), B, 0, s>>>(lv.list[2], lv.nlist[2], n, tb, lv.nbr,
                                                                           A::fcol(lv), A::f(lv), (S *)lv.fcol_alt);
+                MT_LAUNCHED(ctx);
+            }
+            if (lv.nband) {
+                k_stream<Q, S><<<grid_for(lv.nband, B), B, 0, s>>>(lv.band, lv.nband, n, tb, lv.nbr, A::fcol(lv),
+                                                                    A::f(lv));
                 MT_LAUNCHED(ctx);
             }
         }

@@ -51,6 +51,10 @@ int check_desc(Ctx &ctx, const mt_case_desc *d)
     if (d->collision == MT_COLL_CUMULANT && d->q != 27)
         return set_err(ctx, MT_ERR_ARG, "the cumulant collision needs D3Q27");
     if (d->storage < MT_STORE_F64 || d->storage > MT_STORE_BF16) return set_err(ctx, MT_ERR_ARG, "unknown storage");
+    if (d->ib_method != MT_IB_DW && d->ib_method != MT_IB_FH && d->ib_method != MT_IB_DF)
+        return set_err(ctx, MT_ERR_ARG, "unknown immersed-boundary method");
+    if (d->ib_method == MT_IB_DF && d->collision != MT_COLL_LBGK)
+        return set_err(ctx, MT_ERR_ARG, "direct forcing is implemented with the LBGK collision");
     for (int l = 0; l <= d->max_level; ++l)
         if (!(d->tau[l] > 0.5)) return set_err(ctx, MT_ERR_ARG, "tau must exceed 1/2 on every level");
     for (int a = 0; a < 3; ++a)
@@ -256,6 +260,9 @@ int mt_case_add_set(mt_ctx *h, int32_t id, int32_t level, int32_t set_id, const 
         s = (uint8_t)(16 + set_id - MT_SET_LAT_BC0);
     } else if (set_id >= 0 && set_id < kNumSets) {
         s = (uint8_t)set_id;
+    } else if (set_id == MT_SET_IB_BAND) {
+        if (level != c->d.max_level) return set_err(ctx, MT_ERR_ARG, "the forcing band lives on the finest level");
+        s = (uint8_t)MT_SET_IB_BAND;
     } else {
         return set_err(ctx, MT_ERR_ARG, "unknown set id");
     }
@@ -639,6 +646,50 @@ int mt_case_set_face_velocity(mt_ctx *h, int32_t id, int32_t face, const double 
     if (face < 0 || face > 5) return set_err(ctx, MT_ERR_ARG, "face must be 0..5 (West East South North Bot Top)");
     if (!u) return set_err(ctx, MT_ERR_ARG, "null velocity");
     return amr_set_face(ctx, *c, face, u);
+}
+
+int mt_case_set_markers(mt_ctx *h, int32_t id, int64_t nm, const double *ref, const double *dv, const double *center,
+                        int64_t period, const double *path)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "markers need a built multi-level case");
+    if (c->d.ib_method != MT_IB_DF) return set_err(ctx, MT_ERR_STATE, "markers need ib_method MT_IB_DF");
+    if (!c->lv[c->d.max_level].nband) return set_err(ctx, MT_ERR_MESH, "no MT_SET_IB_BAND cells on the finest level");
+    if (nm < 0 || period < 1 || (nm && (!ref || !dv)) || !center || !path)
+        return set_err(ctx, MT_ERR_ARG, "bad marker arrays");
+    void *old[] = {c->mref, c->mdv, c->path, c->mforce};
+    for (void *p : old)
+        if (p) cudaFree(p);
+    c->mref = c->mdv = c->path = c->mforce = nullptr;
+    c->nm = nm;
+    c->period = period;
+    for (int a = 0; a < 3; ++a) c->center[a] = center[a];
+    MT_CUDA(ctx, cudaMalloc(&c->path, sizeof(double) * 6 * period));
+    MT_CUDA(ctx, cudaMemcpy(c->path, path, sizeof(double) * 6 * period, cudaMemcpyHostToDevice));
+    if (nm) {
+        MT_CUDA(ctx, cudaMalloc(&c->mref, sizeof(double) * 3 * nm));
+        MT_CUDA(ctx, cudaMalloc(&c->mdv, sizeof(double) * nm));
+        MT_CUDA(ctx, cudaMalloc(&c->mforce, sizeof(double) * 3 * (nm + (nm + 255) / 256)));
+        MT_CUDA(ctx, cudaMemcpy(c->mref, ref, sizeof(double) * 3 * nm, cudaMemcpyHostToDevice));
+        MT_CUDA(ctx, cudaMemcpy(c->mdv, dv, sizeof(double) * nm, cudaMemcpyHostToDevice));
+    }
+    MT_CUDA(ctx, cudaMemsetAsync(c->tstep, 0, sizeof(long long), ctx.stream));
+    // the captured steps bake the marker arrays in
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+    for (int p = 0; p < 2; ++p) {
+        if (c->fgraph[p]) cudaGraphExecDestroy(c->fgraph[p]);
+        c->fgraph[p] = nullptr;
+    }
+    for (Batch *b : ctx.batches)
+        if (b)
+            for (int32_t x : b->ids)
+                if (x == id) batch_drop(*b);
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
 }
 
 // ---- batches ------------------------------------------------------------------

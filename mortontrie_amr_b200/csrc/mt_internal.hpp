@@ -28,6 +28,7 @@ enum : uint32_t {
     TAG_BC = 32u,
     TAG_SF = 64u,
     TAG_IB = 128u,
+    TAG_BAND = 256u,  // direct-forcing band
 };
 
 // device error flags raised by build / step kernels
@@ -73,6 +74,8 @@ struct Level {
     int32_t *bclist[26] = {};
     int64_t nbc[26] = {};
     int32_t *iblist = nullptr; int64_t nib = 0;             // finest lat_f cells with dis rows
+    int32_t *band = nullptr; int64_t nband = 0;             // direct-forcing band (finest level)
+    int32_t *collide_nb = nullptr; int64_t ncollide_nb = 0; // lat_f (not band) then F2C
     // explosion sources on the parent level (F2C then ghost F2C) and their children on this level
     int32_t *expl_src = nullptr; int32_t *expl_child = nullptr; int64_t nexpl = 0, nexpl_f2c = 0;
     // coalescence: F2C cells of this level and their children on the next level
@@ -134,6 +137,13 @@ struct Case {
     int schedule = MT_SCHED_PHASES;
     int scaling = MT_SCALE_REFERENCE;  // interface rescaling of the non-equilibrium part
     double face_u[6][3] = {};          // bc_velocity of each face's strategy (u_bc unless set)
+    // direct-forcing markers (MT_IB_DF)
+    int64_t nm = 0;
+    double *mref = nullptr, *mdv = nullptr, *path = nullptr, *mforce = nullptr;
+    double center[3] = {0, 0, 0};
+    int64_t period = 1;
+    long long *tstep = nullptr;
+    long long *acc = nullptr;  // [3][n_L] Eulerian force, fixed point
     bool use_bricks = true;  // fused pass over 4x4x4 bricks where a level allows it (else cell lists)
     bool primed = false;
     int par0 = 0;

@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "libmtlbm.so")
 
 MAX_LEVELS = 8
 SET_IDS = {"lat_f": 0, "overlap_F2C": 1, "overlap_C2F": 2, "ghost_overlap_C2F": 3, "ghost_overlap_F2C": 4,
-           "lat_sf": 5}
+           "lat_sf": 5, "ib_band": 6}
 SET_LAT_BC0 = 16
 ERRORS = {-1: "MT_ERR_ARG", -2: "MT_ERR_CUDA", -3: "MT_ERR_STATE", -4: "MT_ERR_MESH", -5: "MT_ERR_NONFINITE"}
 EXPORTS = [
@@ -31,7 +31,7 @@ EXPORTS = [
     "mt_case_init_equilibrium", "mt_case_init_fields", "mt_case_set_populations", "mt_case_get_populations",
     "mt_case_get_macros", "mt_case_reduce", "mt_calculate_macros", "mt_collide", "mt_stream", "mt_explosion",
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
-    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_face_velocity",
+    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step",
 ]
 
@@ -74,7 +74,7 @@ def lib():
             "mt_find": [vp, i32, i32, u64p, i64, i64p], "mt_case_init_equilibrium": [vp, i32, C.c_double, dp],
             "mt_case_init_fields": [vp, i32, dp, dp, dp, dp], "mt_case_set_populations": [vp, i32, i32, dp, dp],
             "mt_case_get_populations": [vp, i32, i32, dp, dp], "mt_case_get_macros": [vp, i32, i32, dp, dp],
-            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp],
+            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
             "mt_batch_create": [vp, i32p], "mt_batch_destroy": [vp, i32], "mt_batch_add": [vp, i32, i32],
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
@@ -175,7 +175,9 @@ class LBM_Manager:
         m = case.mesh
         for l in range(self.L + 1):
             for name, sid in SET_IDS.items():
-                k = np.ascontiguousarray(m.levels[l][name], np.uint64)
+                k = np.ascontiguousarray(m.levels[l].get(name, np.zeros(0, np.uint64)), np.uint64)
+                if sid == 6 and not k.size:
+                    continue
                 ctx.check(lib().mt_case_add_set(ctx.h, self.id, l, sid, _ptr(k, C.c_uint64), k.size), "add_set")
         for b in range(26):
             k = np.ascontiguousarray(m.lat_bc[b], np.uint64)
@@ -186,10 +188,22 @@ class LBM_Manager:
         ctx.check(lib().mt_case_set_dis(ctx.h, self.id, _ptr(dk, C.c_uint64), _ptr(dr, C.c_double), dk.size),
                   "set_dis")
         ctx.check(lib().mt_case_build(ctx.h, self.id), "mt_case_build")
+        if m.markers is not None:
+            self.set_markers(m.markers)
         self.set_schedule(schedule)
         self.set_interface_scaling(scaling)
         for face, u in sorted(getattr(case.params, "face_u", {}).items()):
             self.set_face_velocity(face, u)
+
+    def set_markers(self, mk):
+        """Upload the Lagrangian markers of a direct-forcing sphere (Markers)."""
+        ref = np.ascontiguousarray(mk.ref, np.float64)
+        dv = np.ascontiguousarray(mk.dv, np.float64)
+        ctr = np.ascontiguousarray(mk.center, np.float64)
+        path = np.ascontiguousarray(mk.path, np.float64)
+        self.ctx.check(lib().mt_case_set_markers(self.ctx.h, self.id, dv.size, _ptr(ref, C.c_double),
+                                                 _ptr(dv, C.c_double), _ptr(ctr, C.c_double), path.shape[0],
+                                                 _ptr(path, C.c_double)), "set_markers")
 
     def set_face_velocity(self, face: int, u):
         """Velocity of boundary face `face` (0..5 = West East South North Bot

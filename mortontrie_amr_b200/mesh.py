@@ -66,6 +66,47 @@ class MeshSpec:
     refine: list = field(default_factory=list)
     boundary: tuple = ("bc", "bc", "bc")  # per axis: "bc" (level-0 boundary shell) or "periodic"
     sphere: Optional[Sphere] = None
+    # "links": voxelised solid + wall distances (the reference's
+    # SinglePointInterpolation); "markers": direct forcing on Lagrangian
+    # surface markers, fluid inside the sphere and a forcing band
+    ib: str = "links"
+    # transverse oscillation of a marker sphere: (amplitude in coarse cells,
+    # period in finest steps), along y
+    oscillation: Optional[tuple] = None
+
+
+@dataclass
+class Markers:
+    """Lagrangian markers of a direct-forcing sphere, finest-level cell units."""
+    ref: np.ndarray     # (3, nm) offsets from the centre
+    dv: np.ndarray      # (nm,) volume weight of each marker
+    center: tuple       # initial centre
+    path: np.ndarray    # (period, 6): centre displacement and velocity at substep t % period
+
+
+def sphere_markers(spec: "MeshSpec") -> Markers:
+    """One marker per finest cell^2 of surface on a Fibonacci lattice; the
+    path samples y(t) = A sin(2 pi t / T) and its velocity per finest step."""
+    L = spec.max_level
+    s = 1 << L
+    r = spec.sphere.radius * s
+    nm = max(1, int(round(4.0 * np.pi * r * r)))
+    i = np.arange(nm) + 0.5
+    zc = 1.0 - 2.0 * i / nm
+    rc = np.sqrt(np.maximum(0.0, 1.0 - zc * zc))
+    phi = i * (np.pi * (3.0 - np.sqrt(5.0)))
+    ref = np.stack([r * rc * np.cos(phi), r * rc * np.sin(phi), r * zc])
+    dv = np.full(nm, 4.0 * np.pi * r * r / nm)
+    center = tuple(float(c * s) for c in spec.sphere.center)
+    if spec.oscillation:
+        amp, period = spec.oscillation[0] * s, int(spec.oscillation[1])
+        t = np.arange(period)
+        path = np.zeros((period, 6))
+        path[:, 1] = amp * np.sin(2.0 * np.pi * t / period)
+        path[:, 4] = amp * (2.0 * np.pi / period) * np.cos(2.0 * np.pi * t / period)
+    else:
+        path = np.zeros((1, 6))
+    return Markers(ref=np.ascontiguousarray(ref), dv=dv, center=center, path=np.ascontiguousarray(path))
 
 
 @dataclass
@@ -76,6 +117,7 @@ class Mesh:
     dis_keys: np.ndarray  # sorted finest-level keys
     dis_rows: np.ndarray  # (n, Q-1) float64
     extent: list          # per level: (nx, ny, nz) in that level's cells
+    markers: Optional["Markers"] = None
 
     def all_keys(self, level: int) -> np.ndarray:
         parts = [self.levels[level][s] for s in SET_NAMES]
@@ -198,7 +240,21 @@ def build_mesh(spec: MeshSpec) -> Mesh:
         sets["overlap_C2F"] = _sorted_unique(cell_key(L, l, x[c2f], y[c2f], z[c2f]))
         sets["lat_sf"] = np.zeros(0, np.uint64)
         fx, fy, fz = x[fluid], y[fluid], z[fluid]
-        if l == L and spec.sphere is not None:
+        if l == L and spec.sphere is not None and spec.ib == "markers":
+            # every cell a marker's 3x3x3 stencil can reach over the whole path:
+            # within 1.5 sqrt(3) of the surface of some position of the sphere
+            s = 1 << L
+            cx, cy, cz = (c * s for c in spec.sphere.center)
+            r = spec.sphere.radius * s
+            amp = spec.oscillation[0] * s if spec.oscillation else 0.0
+            px, py, pz = fx + 0.5 - cx, fy + 0.5 - cy, fz + 0.5 - cz
+            qy = np.clip(py, -amp, amp)
+            dmin = np.sqrt(px * px + (py - qy) ** 2 + pz * pz)
+            dmax = np.sqrt(px * px + (np.abs(py) + amp) ** 2 + pz * pz)
+            m = 2.7
+            band = (dmin <= r + m) & (dmax >= r - m)
+            sets["ib_band"] = _sorted_unique(cell_key(L, l, fx[band], fy[band], fz[band]))
+        elif l == L and spec.sphere is not None:
             if L == 0:
                 raise ValueError("the solid boundary is only applied on a refined finest level")
             s = 1 << L
@@ -243,7 +299,18 @@ def build_mesh(spec: MeshSpec) -> Mesh:
 
     dis_keys = np.zeros(0, np.uint64)
     dis_rows = np.zeros((0, q - 1))
-    if spec.sphere is not None:
+    markers = None
+    if spec.sphere is not None and spec.ib == "markers":
+        band = levels[L].get("ib_band", np.zeros(0, np.uint64))
+        if np.any(_in_sorted(band, levels[L]["overlap_C2F"])) or np.any(_in_sorted(band, levels[L]["ghost_overlap_C2F"])):
+            raise ValueError("the forcing band reaches the coarse/fine interface")
+        bx, by, bz = _coords_of(band, L, L)
+        for (a, b, c) in _neighbours(bx, by, bz, q, extents[L], periodic):
+            k = cell_key(L, L, a, b, c)
+            if np.any(_in_sorted(k, levels[L]["overlap_C2F"])):
+                raise ValueError("the forcing band is too close to the coarse/fine interface")
+        markers = sphere_markers(spec)
+    elif spec.sphere is not None:
         dis_keys, dis_rows = _sphere_links(spec, levels[L]["lat_f"])
         sf_keys = levels[L]["lat_sf"]
         # IB cells must be plain lat_f cells; the solid must stay clear of C2F.
@@ -253,7 +320,7 @@ def build_mesh(spec: MeshSpec) -> Mesh:
             if np.any(_in_sorted(k, levels[L]["overlap_C2F"])) or np.any(_in_sorted(k, levels[L]["ghost_overlap_C2F"])):
                 raise ValueError("solid too close to the coarse/fine interface")
     return Mesh(spec=spec, levels=levels, lat_bc=lat_bc, dis_keys=dis_keys, dis_rows=dis_rows,
-                extent=extents)
+                extent=extents, markers=markers)
 
 
 def _coords_of(keys, L, l):

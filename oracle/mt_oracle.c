@@ -27,10 +27,10 @@
 #define OC_MAXL 8
 #define OC_NSETS 6
 
-enum { S_LATF = 0, S_F2C = 1, S_C2F = 2, S_GC2F = 3, S_GF2C = 4, S_SF = 5, S_BC0 = 16 };
-enum { T_LATF = 1, T_F2C = 2, T_C2F = 4, T_GC2F = 8, T_GF2C = 16, T_BC = 32, T_SF = 64, T_IB = 128 };
+enum { S_LATF = 0, S_F2C = 1, S_C2F = 2, S_GC2F = 3, S_GF2C = 4, S_SF = 5, S_BAND = 6, S_BC0 = 16 };
+enum { T_LATF = 1, T_F2C = 2, T_C2F = 4, T_GC2F = 8, T_GF2C = 16, T_BC = 32, T_SF = 64, T_IB = 128, T_BAND = 256 };
 enum { COLL_LBGK = 0, COLL_CUMULANT = 1 };
-enum { IB_DW = 0, IB_FH = 1 };
+enum { IB_DW = 0, IB_FH = 1, IB_DF = 2 };
 /* domain boundary treatment on the x faces (the y/z faces follow the same
  * rule when they are not periodic) */
 enum { BC_NEQ = 0, BC_ZOUHE_OUTFLOW = 1 };
@@ -115,6 +115,9 @@ typedef struct {
     int64_t *bclist[26];
     keyvec raw[OC_NSETS];
     keyvec rawbc[26];
+    keyvec rawband;
+    int64_t nband;
+    int64_t *band;
 } oc_level;
 
 typedef struct {
@@ -131,6 +134,10 @@ typedef struct {
     double fx, fy, fz;
     int64_t nforce;
     int built;
+    /* direct-forcing markers (finest-level cell units) */
+    int64_t nm, period, tstep;
+    double *mref, *mdv, *path, center[3];
+    int64_t *acc; /* [3][n_L] Eulerian force in fixed point 2^-32 */
 } oc_case;
 
 /* ------------------------------------------------------------------ */
@@ -498,8 +505,10 @@ void oc_case_free(void *h)
         free(lv->f); free(lv->fcol); free(lv->rho); free(lv->u);
         for (int s = 0; s < OC_NSETS; ++s) { free(lv->list[s]); free(lv->raw[s].keys); }
         for (int b = 0; b < 26; ++b) { free(lv->bclist[b]); free(lv->rawbc[b].keys); }
+        free(lv->band); free(lv->rawband.keys);
     }
     free(c->dis_key); free(c->dis);
+    free(c->mref); free(c->mdv); free(c->path); free(c->acc);
     free(c);
 }
 
@@ -510,6 +519,11 @@ int oc_add_set(void *h, int level, int set_id, const uint64_t *keys, int64_t n)
     if (set_id >= S_BC0 && set_id < S_BC0 + 26) {
         if (level != 0) return -1;
         kv_push(&c->lv[0].rawbc[set_id - S_BC0], keys, n);
+        return 0;
+    }
+    if (set_id == S_BAND) {
+        if (level != c->L) return -1;
+        kv_push(&c->lv[level].rawband, keys, n);
         return 0;
     }
     if (set_id < 0 || set_id >= OC_NSETS) return -1;
@@ -576,6 +590,8 @@ int oc_build(void *h)
         lv->u = (double *)calloc((size_t)n * 3, sizeof(double));
     }
     oc_level *fl = &c->lv[c->L];
+    fl->band = index_list(fl, &fl->rawband, &fl->nband, T_BAND);
+    if (fl->nband) c->acc = (int64_t *)calloc((size_t)fl->n * 3, sizeof(int64_t));
     for (int64_t r = 0; r < c->ndis; ++r) {
         int64_t i = find_idx(fl, c->dis_key[r]);
         if (i < 0) return -2;
@@ -684,6 +700,8 @@ static void phase_macros(oc_case *c, int l)
 
 /* Collision_LBGK::collide / Collision_Cumulant::collide
  * (Collision_Manager.cpp:13-53, Collision_Cumulant.cpp:22-159) */
+static void band_collide(oc_case *c, int l, int64_t i);
+
 static void phase_collide(oc_case *c, int l)
 {
     oc_level *lv = &c->lv[l];
@@ -695,6 +713,10 @@ static void phase_collide(oc_case *c, int l)
         int64_t *li = lv->list[s == 0 ? S_LATF : S_F2C];
         for (int64_t j = 0; j < nl; ++j) {
             int64_t i = li[j];
+            if (lv->tag[i] & T_BAND) {
+                band_collide(c, l, i);
+                continue;
+            }
             if (c->collision == COLL_LBGK) {
                 feq_bgk(q, lv->rho[i], &lv->u[3 * i], feq);
                 for (int k = 0; k < q; ++k) {
@@ -842,6 +864,141 @@ static int phase_bc_neq(oc_case *c)
     return 0;
 }
 
+/* ---- direct forcing on Lagrangian markers (no reference counterpart) ----
+ * Restated from Uhlmann (2005) and Roma, Peskin & Berger (1999): the 3-point
+ * kernel, marker force 2 rho (U - u) from the interpolated unforced
+ * velocity, spreading into int64 fixed point (2^-32), Guo forcing in the
+ * collision of the band cells.  Same expression order as the device code. */
+#define OC_FSCALE 4294967296.0
+
+static double roma3(double r)
+{
+    r = fabs(r);
+    if (r <= 0.5) return (1.0 + sqrt(1.0 - 3.0 * r * r)) / 3.0;
+    if (r <= 1.5) {
+        double a = 1.0 - r;
+        return (5.0 - 3.0 * r - sqrt(1.0 - 3.0 * a * a)) / 6.0;
+    }
+    return 0.0;
+}
+
+static void band_collide(oc_case *c, int l, int64_t i)
+{
+    oc_level *lv = &c->lv[l];
+    int q = c->q;
+    int64_t n = lv->n;
+    double d[27], r = 0., jx = 0., jy = 0., jz = 0.;
+    for (int k = 0; k < q; ++k) {
+        d[k] = lv->f[k * n + i];
+        r += d[k];
+        jx += d[k] * EX[k];
+        jy += d[k] * EY[k];
+        jz += d[k] * EZ[k];
+    }
+    double gx = (double)c->acc[i] / OC_FSCALE, gy = (double)c->acc[n + i] / OC_FSCALE,
+           gz = (double)c->acc[2 * n + i] / OC_FSCALE;
+    double rs = (r > -1e-6 && r < 1e-6) ? ((r < 0.) ? -1e-6 : 1e-6) : r;
+    double x = (jx + gx * 0.5) / rs, y = (jy + gy * 0.5) / rs, z = (jz + gz * 0.5) / rs;
+    double om = 1.0 / c->tau[l];
+    double fpre = 1.0 - 0.5 * om;
+    double uu = x * x + y * y + z * z;
+    for (int k = 0; k < q; ++k) {
+        double eu = EX[k] * x + EY[k] * y + EZ[k] * z;
+        double wk = wq(q, k);
+        double feq = r * wk * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu);
+        double ge = (3.0 * (EX[k] - x) + 9.0 * eu * EX[k]) * gx + (3.0 * (EY[k] - y) + 9.0 * eu * EY[k]) * gy +
+                    (3.0 * (EZ[k] - z) + 9.0 * eu * EZ[k]) * gz;
+        lv->fcol[k * n + i] = d[k] - (d[k] - feq) * om + fpre * wk * ge;
+    }
+}
+
+static void phase_df(oc_case *c)
+{
+    int L = c->L, q = c->q;
+    oc_level *lv = &c->lv[L];
+    int64_t n = lv->n;
+    double d[27];
+    for (int64_t j = 0; j < lv->nband; ++j) {
+        int64_t i = lv->band[j];
+        for (int k = 0; k < q; ++k) d[k] = lv->f[k * n + i];
+        macros_of(q, d, &lv->rho[i], &lv->u[3 * i]);
+        c->acc[i] = 0;
+        c->acc[n + i] = 0;
+        c->acc[2 * n + i] = 0;
+    }
+    if (!c->nm) {
+        c->nforce += 1;
+        return;
+    }
+    const double *pp = c->path + 6 * (c->tstep % c->period);
+    double sx = 0., sy = 0., sz = 0.;
+    for (int64_t m = 0; m < c->nm; ++m) {
+        double X = c->center[0] + pp[0] + c->mref[m];
+        double Y = c->center[1] + pp[1] + c->mref[c->nm + m];
+        double Z = c->center[2] + pp[2] + c->mref[2 * c->nm + m];
+        int64_t ix = (int64_t)floor(X), iy = (int64_t)floor(Y), iz = (int64_t)floor(Z);
+        int64_t idx[27];
+        double wgt[27], r = 0., vx = 0., vy = 0., vz = 0.;
+        for (int cc = 0; cc < 27; ++cc) {
+            int64_t x = ix + cc % 3 - 1, y = iy + (cc / 3) % 3 - 1, z = iz + cc / 9 - 1;
+            double wv = roma3((double)x + 0.5 - X) * roma3((double)y + 0.5 - Y) * roma3((double)z + 0.5 - Z);
+            int64_t i = -1;
+            if (x >= 0 && y >= 0 && z >= 0) {
+                uint64_t k = dilate3((uint64_t)x) | (dilate3((uint64_t)y) << 1) | (dilate3((uint64_t)z) << 2);
+                i = find_idx(lv, k);
+                if (i >= 0 && !(lv->tag[i] & T_BAND)) i = -1;
+            }
+            idx[cc] = i;
+            wgt[cc] = wv;
+            if (i >= 0) {
+                r += wv * lv->rho[i];
+                vx += wv * lv->u[3 * i];
+                vy += wv * lv->u[3 * i + 1];
+                vz += wv * lv->u[3 * i + 2];
+            }
+        }
+        double fx = 2.0 * r * (pp[3] - vx), fy = 2.0 * r * (pp[4] - vy), fz = 2.0 * r * (pp[5] - vz);
+        double dv = c->mdv[m];
+        for (int cc = 0; cc < 27; ++cc) {
+            int64_t i = idx[cc];
+            if (i < 0) continue;
+            double sw = wgt[cc] * dv;
+            c->acc[i] += (int64_t)llrint(fx * sw * OC_FSCALE);
+            c->acc[n + i] += (int64_t)llrint(fy * sw * OC_FSCALE);
+            c->acc[2 * n + i] += (int64_t)llrint(fz * sw * OC_FSCALE);
+        }
+        sx += -fx * dv;
+        sy += -fy * dv;
+        sz += -fz * dv;
+    }
+    c->tstep += 1;
+    c->fx += sx;
+    c->fy += sy;
+    c->fz += sz;
+    c->nforce += 1;
+}
+
+int oc_set_markers(void *h, int64_t nm, const double *ref, const double *dv, const double *center, int64_t period,
+                   const double *path)
+{
+    oc_case *c = (oc_case *)h;
+    if (!c->built || !c->acc || period < 1) return -1;
+    free(c->mref);
+    free(c->mdv);
+    free(c->path);
+    c->nm = nm;
+    c->period = period;
+    c->tstep = 0;
+    c->mref = (double *)malloc((size_t)(3 * nm + 1) * sizeof(double));
+    c->mdv = (double *)malloc((size_t)(nm + 1) * sizeof(double));
+    c->path = (double *)malloc((size_t)(6 * period) * sizeof(double));
+    memcpy(c->mref, ref, (size_t)(3 * nm) * sizeof(double));
+    memcpy(c->mdv, dv, (size_t)nm * sizeof(double));
+    memcpy(c->path, path, (size_t)(6 * period) * sizeof(double));
+    for (int a = 0; a < 3; ++a) c->center[a] = center[a];
+    return 0;
+}
+
 /* SinglePointInterpolation::treat (ComplexBoundary_Manager.cpp:43-225):
  * interpolated bounce-back on wall links (Filippova-Haenel or distance
  * weighted), plain pull on free links, density clamp, then eight
@@ -849,6 +1006,10 @@ static int phase_bc_neq(oc_case *c)
  * every Q (the remaining D3Q27 weights are zero). */
 static void phase_ib(oc_case *c)
 {
+    if (c->ib_method == IB_DF) {
+        phase_df(c);
+        return;
+    }
     int L = c->L, q = c->q;
     oc_level *lv = &c->lv[L];
     static const double W19[19] = {1. / 3., 1. / 18., 1. / 18., 1. / 18., 1. / 18., 1. / 18., 1. / 18.,

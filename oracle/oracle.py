@@ -45,6 +45,7 @@ def lib():
         L.oc_neighbor_keys.argtypes = [vp, i32, u64p, i64, u64p]
         L.oc_collide_cell.argtypes = [i32, i32, dp, C.c_double, dp, C.c_double, dp]
         L.oc_set_face_velocity.argtypes = [vp, i32, dp]
+        L.oc_set_markers.argtypes = [vp, i64, dp, dp, dp, i64, dp]
         _lib = L
     return _lib
 
@@ -81,6 +82,10 @@ class OracleCase:
         for b in range(26):
             k = np.ascontiguousarray(m.lat_bc[b], np.uint64)
             lib().oc_add_set(self.h, 0, 16 + b, _p(k, C.c_uint64), k.size)
+        band = m.levels[self.L].get("ib_band")
+        if band is not None and band.size:
+            k = np.ascontiguousarray(band, np.uint64)
+            lib().oc_add_set(self.h, self.L, 6, _p(k, C.c_uint64), k.size)
         dk = np.ascontiguousarray(m.dis_keys, np.uint64)
         dr = np.ascontiguousarray(m.dis_rows, np.float64)
         if lib().oc_set_dis(self.h, _p(dk, C.c_uint64), _p(dr, C.c_double), dk.size) != 0:
@@ -89,6 +94,15 @@ class OracleCase:
             raise ValueError("oracle build failed")
         u0 = np.array(p.u_bc, np.float64)
         lib().oc_init_equilibrium(self.h, p.rho0, _p(u0, C.c_double))
+        if m.markers is not None:
+            mk = m.markers
+            ref = np.ascontiguousarray(mk.ref, np.float64)
+            dv = np.ascontiguousarray(mk.dv, np.float64)
+            ctr = np.ascontiguousarray(mk.center, np.float64)
+            path = np.ascontiguousarray(mk.path, np.float64)
+            if lib().oc_set_markers(self.h, dv.size, _p(ref, C.c_double), _p(dv, C.c_double), _p(ctr, C.c_double),
+                                    path.shape[0], _p(path, C.c_double)) != 0:
+                raise ValueError("oracle rejected the markers")
         for face, u in sorted(getattr(p, "face_u", {}).items()):
             uf = np.array(u, np.float64)
             lib().oc_set_face_velocity(self.h, int(face), _p(uf, C.c_double))

@@ -332,3 +332,50 @@ def test_cavity_matches_oracle(ctx, q, collision, L, schedule):
     # under the reference's streaming direction; either way they move
     _, u = mgr.macros(0)
     assert np.abs(u[0]).max() > 1e-3
+
+
+@pytest.mark.parametrize("schedule", ["phases", "fused", "fused_lists"])
+@pytest.mark.parametrize("oscillating", [False, True])
+def test_direct_forcing_matches_oracle(ctx, schedule, oscillating):
+    """Direct-forcing sphere (Lagrangian markers, 3-point kernel, Guo forcing
+    on the band): GPU FP64 vs the oracle, bit-exact populations and macros,
+    the same body force up to the order of its FP64 sum."""
+    from mortontrie_amr_b200.case import df_sphere_case
+    case = df_sphere_case(radius=3, max_level=1, re=50.0, oscillating=oscillating, period=60)
+    mgr = _device_case(ctx, case, None, schedule=schedule)
+    mgr.fluidSimulate(7)
+    ctx.synchronize()
+    oc = run_oracle(case, 7)
+    for l in range(case.max_level + 1):
+        f, fcol = mgr.populations(l)
+        _, tags = mgr.keys(l)
+        g = oc.get(l)
+        keep = (tags & TAG_BC) == 0
+        assert np.array_equal(f[:, keep], g["f"][:, keep]), (l, float(np.abs(f - g["f"])[:, keep].max()))
+        assert np.array_equal(fcol, g["fcol"]), (l, float(np.abs(fcol - g["fcol"]).max()))
+        rho, u = mgr.macros(l)
+        assert np.array_equal(rho[keep], g["rho"][keep]), l
+    fg, fo = mgr.force(), oc.force()
+    assert fg[3] == fo[3] == 14
+    assert rel_err(fg[:3], fo[:3]) < 1e-12, (fg, fo)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_direct_forcing_reduced_storage(ctx, storage):
+    from mortontrie_amr_b200.case import df_sphere_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    case = df_sphere_case(radius=3, max_level=2, re=50.0, oscillating=True, period=200)
+    a = LBM_Manager(ctx, case, "f64")
+    b = LBM_Manager(ctx, case, storage, schedule="fused")
+    a.fluidSimulate(30)
+    b.fluidSimulate(30)
+    ctx.synchronize()
+    L = case.max_level
+    _, ua = a.macros(L)
+    _, ub = b.macros(L)
+    _, tags = a.keys(L)
+    fl = (tags & 1) != 0
+    err = np.linalg.norm(ub[:, fl] - ua[:, fl]) / np.linalg.norm(ua[:, fl])
+    assert err < TOL_AMR[storage], err
+    fa, fb = a.force(), b.force()
+    assert abs(fb[0] - fa[0]) / abs(fa[0]) < 10 * TOL_AMR[storage], (fa, fb)

@@ -17,7 +17,7 @@ def ctx():
 
 
 def _mix():
-    from mortontrie_amr_b200.case import cavity_case, nested_sphere_case, sphere_case
+    from mortontrie_amr_b200.case import cavity_case, df_sphere_case, nested_sphere_case, sphere_case
     return [
         sphere_case(coarse=(32, 16, 16), refine=[((6, 4, 4), (18, 12, 12))], center=(12, 8, 8), radius=2.0),
         nested_sphere_case(coarse=(48, 24, 24), max_level=2, center=(16, 12, 12), radius=2.0, half_widths=(4.0, 2.5),
@@ -26,6 +26,8 @@ def _mix():
         cavity_case(q=27, collision="Cumulant", coarse=(24, 24, 24), max_level=2, re=60.0),
         # periodic extent 18 is not a multiple of 4: level 0 runs from cell lists
         sphere_case(coarse=(30, 18, 18), refine=[((6, 5, 5), (18, 13, 13))], center=(12, 9, 9), radius=2.0),
+        # direct-forcing oscillating sphere (Lagrangian markers)
+        df_sphere_case(radius=3, max_level=2, re=60.0, oscillating=True, period=100),
     ]
 
 
