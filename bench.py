@@ -268,6 +268,12 @@ def run_ours(args):
             amr = amr_section(ctx, torch)
         except Exception as exc:  # reported, not hidden: the line says why the section is missing
             amr = {"error": repr(exc)}
+    served = None
+    if not args.no_served and world == 1:
+        try:
+            served = served_section(ctx, torch)
+        except Exception as exc:
+            served = {"error": repr(exc)}
     batched = None
     if not args.no_batched and world == 1:
         try:
@@ -297,6 +303,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "amr_cumulant_sphere": amr,
             "batched_uneven": batched,
+            "served_mix": served,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -479,6 +486,47 @@ def _case_result(mgr, case):
     return {"u": np.concatenate(us, axis=1), "cd": cd}
 
 
+def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=16):
+    """Served mix: a seeded Poisson stream (rate 20/s for `duration` s) of
+    direct-forcing sphere flows (R in [3, 8], 16R x 8R x 8R, 1-3 refinement
+    levels, Re in [20, 300], D3Q19 LBGK, half oscillating with amplitude R/2
+    and period 2000 finest steps), each solved for 2000 finest steps, served
+    by continuous batching in FP16 under a 150 GB budget.  Cases/h and the
+    p50/p99 time-to-solution come from the wall clock of the request loop;
+    the one-at-a-time rate solves every request of the stream alone (FP16,
+    fused schedule, back to back); the drag error compares served results
+    with FP64 solves (phase schedule) of the lowest-Re requests whose served
+    result is finite."""
+    from mortontrie_amr_b200.serving import Server, TemplateCache, poisson_requests, solve_alone
+    reqs = poisson_requests(seed=seed, rate=rate, duration=duration)
+    cache = TemplateCache(workers=max(1, min(16, (os.cpu_count() or 2) - 1)))
+    t0 = time.time()
+    cache.prepare(reqs)
+    prep = time.time() - t0
+    # warm the kernels and the batch path on one small request (not timed)
+    Server(ctx, cache, storage="f16", chunk=chunk).run(reqs[:1], realtime=False)
+    stats = Server(ctx, cache, storage="f16", budget_gb=150.0, chunk=chunk).run(reqs, realtime=True)
+    served = stats.summary()
+    t_alone = [solve_alone(ctx, cache, r, storage="f16")[2] for r in reqs]
+    alone_rate = 3600.0 * len(reqs) / float(np.sum(t_alone))
+    res = {r.rid: r for r in stats.results}
+    finite = [r for r in stats.results if np.isfinite(r.cd)]
+    errs = []
+    for r in sorted(finite, key=lambda x: next(q.re for q in reqs if q.rid == x.rid))[:n_fp64]:
+        cd64 = solve_alone(ctx, cache, next(q for q in reqs if q.rid == r.rid), storage="f64")[0]
+        if np.isfinite(cd64) and abs(cd64) > 1e-6:
+            errs.append(abs(res[r.rid].cd - cd64) / abs(cd64))
+    return {"workload": f"{len(reqs)} Poisson requests ({rate:g}/s over {duration:g} s, seed {seed}): DF sphere "
+                        "R 3-8, 1-3 levels, Re 20-300, half oscillating, 2000 finest steps each, FP16",
+            "template_build_s": round(prep, 1), "templates": len(cache.meshes), **served,
+            "finite_results": len(finite),
+            "one_at_a_time_cases_per_hour": round(alone_rate, 1),
+            "one_at_a_time_wall_s": round(float(np.sum(t_alone)), 2),
+            "served_vs_one_at_a_time": round(served["cases_per_hour"] / alone_rate, 2),
+            "drag_rel_vs_fp64": {"median": float(np.median(errs)) if errs else None,
+                                 "max": float(np.max(errs)) if errs else None, "sample": len(errs)}}
+
+
 ACCURACY_CASES = {
     "cfg3": "4-level D3Q27 cumulant sphere 192x96x96, R=6, Re=200, u=0.04",
     "cfg3_re20": "4-level D3Q27 cumulant sphere 192x96x96, R=6, Re=20, u=0.04",
@@ -626,6 +674,9 @@ def main():
     ap.add_argument("--amr-only", action="store_true",
                     help="only the 4-level cumulant sphere section (K coarse steps per storage; profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven instances section")
+    ap.add_argument("--no-served", action="store_true", help="skip the served mix section")
+    ap.add_argument("--served-only", type=float, default=0.0, metavar="SECONDS",
+                    help="only the served mix, with SECONDS of Poisson arrivals")
     ap.add_argument("--batched-only", action="store_true", help="only the batched uneven instances section")
     ap.add_argument("--amr-variants", default=None,
                     help="comma list of multi-level runs to time (default all: "
@@ -644,6 +695,16 @@ def main():
     N_EDGE = args.edge
     if args.impl == "reference":
         run_reference(args)
+    elif args.served_only:
+        import torch
+
+        from mortontrie_amr_b200.lbm import Context
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx = Context(0)
+        ctx.set_stream(stream.cuda_stream)
+        print(json.dumps({"served_mix": served_section(ctx, torch, duration=args.served_only)}), flush=True)
+        ctx.close()
     elif args.batched_only:
         import torch
 

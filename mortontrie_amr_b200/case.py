@@ -121,7 +121,7 @@ def cavity_case(q=19, collision="LBGK", coarse=(32, 32, 32), max_level=1, re=100
 
 
 def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q=19, period=2000,
-                   amplitude=0.5) -> Case:
+                   amplitude=0.5, band_slack=0.0) -> Case:
     """Flow past a sphere represented by direct-forcing Lagrangian markers
     (one per finest cell^2 of surface, 3-point kernel): coarse channel
     16R x 8R x 8R, inlet on West, outflow on East, periodic sides, centre at
@@ -148,7 +148,7 @@ def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q
     nu = u * 2.0 * r / re
     spec = MeshSpec(q=q, max_level=max_level, coarse=(nx, ny, nz), refine=refine,
                     boundary=("bc", "periodic", "periodic"), sphere=Sphere(c, float(r)), ib="markers",
-                    oscillation=(amp, period) if oscillating else None)
+                    oscillation=(amp, period) if oscillating else None, band_slack=band_slack)
     p = CaseParams(q=q, collision="LBGK", ib_method="DF", bc_mode="zouhe_outflow", nu=nu, u_bc=(u, 0.0, 0.0),
                    u_ref=u)
     return Case(build_mesh(spec), p)

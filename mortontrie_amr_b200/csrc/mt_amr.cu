@@ -506,7 +506,7 @@ void amr_free(Case &c)
         lv = Level();
     }
     void *ptrs[] = {c.dis_key, c.dis, c.ib_force, c.force_acc, c.dev_err, c.bc_tmp,
-                    c.mref, c.mdv, c.path, c.mforce, c.tstep, c.acc};
+                    c.mref, c.mdv, c.path, c.mforce, c.tstep, c.acc, c.mgrid};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     c.bc_tmp = nullptr;
@@ -518,6 +518,7 @@ void amr_free(Case &c)
     c.mref = c.mdv = c.path = c.mforce = nullptr;
     c.tstep = nullptr;
     c.acc = nullptr;
+    c.mgrid = nullptr;
     c.nm = 0;
     if (c.graph) cudaGraphExecDestroy(c.graph);
     c.graph = nullptr;
@@ -537,9 +538,6 @@ void amr_free(Case &c)
 // storage type (mt_amr_phases.cuh, instantiated in mt_amr_f64.cu and
 // mt_amr_lp.cu)
 // ----------------------------------------------------------------------------
-enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
-       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
-       PH_SYNC_F, PH_DF, PH_FACE_EQ0 = 24 };
 
 int amr_phase(Ctx &ctx, Case &c, int phase, int level)
 {
@@ -859,7 +857,8 @@ namespace {
 
 struct BatchRec {
     Batch *b;
-    std::vector<BrickBatch> hdesc;
+    std::vector<BrickBatch> *hdesc;
+    BrickBatch *dbase = nullptr;
     int64_t cap = 0;
 };
 
@@ -910,7 +909,7 @@ int batch_bricks(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cs, int l, co
     (void)first_desc;
     for (auto &g : groups) {
         for (size_t c0 = 0; c0 < g.size(); c0 += kMaxBatchSlots) {
-            if ((int64_t)R.hdesc.size() >= R.cap) return set_err(ctx, MT_ERR_STATE, "batch descriptor capacity");
+            if ((int64_t)R.hdesc->size() >= R.cap) return set_err(ctx, MT_ERR_STATE, "batch descriptor capacity");
             BrickBatch d;
             const size_t c1 = std::min(g.size(), c0 + kMaxBatchSlots);
             for (size_t k = c0; k < c1; ++k) {
@@ -933,8 +932,8 @@ int batch_bricks(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cs, int l, co
                 ++d.nslots;
             }
             d.total = d.off[d.nslots];
-            const BrickBatch *dev = R.b->ddesc[R.b->par] + R.hdesc.size();
-            R.hdesc.push_back(d);
+            const BrickBatch *dev = R.dbase + R.hdesc->size();
+            R.hdesc->push_back(d);
             Case &c = *g[0];
             int rc = amr_dispatch(c, [&](auto *tag) {
                 using S = std::remove_pointer_t<decltype(tag)>;
@@ -1026,11 +1025,12 @@ int record_batch_step(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cases)
 
 void batch_drop(Batch &b)
 {
-    for (int p = 0; p < 2; ++p) {
+    for (int p = 0; p < 3; ++p) {
         if (b.graph[p]) cudaGraphExecDestroy(b.graph[p]);
         b.graph[p] = nullptr;
         if (b.ddesc[p]) cudaFree(b.ddesc[p]);
         b.ddesc[p] = nullptr;
+        b.hdesc[p].clear();
     }
     b.par = 0;
 }
@@ -1055,7 +1055,7 @@ int batch_step(Ctx &ctx, Batch &B, const std::vector<Case *> &cases, int n)
         if (!c->primed && (rc = prime_fused(ctx, *c))) return rc;
     }
     if (B.pool.empty()) {
-        const int P = (int)std::min<size_t>(8, cases.size());
+        const int P = 8;
         for (int p = 0; p < P; ++p) {
             cudaStream_t s;
             cudaEvent_t e;
@@ -1068,43 +1068,61 @@ int batch_step(Ctx &ctx, Batch &B, const std::vector<Case *> &cases, int n)
     }
     int Lmax = 0;
     for (Case *c : cases) Lmax = std::max(Lmax, c->d.max_level);
-    for (int s = 0; s < n; ++s) {
-        const int p = B.par;
-        if (!B.graph[p]) {
-            BatchRec R;
-            R.b = &B;
-            // at most one descriptor per family (3 models x 4 storages) and chunk for every substep
-            R.cap = (int64_t)((2 << Lmax) * 12) * (int64_t)((cases.size() + kMaxBatchSlots - 1) / kMaxBatchSlots);
-            MT_CUDA(ctx, cudaMalloc(&B.ddesc[p], sizeof(BrickBatch) * R.cap));
-            for (Case *c : cases) c->no_side = true;
-            const int64_t before = ctx.launches;
-            cudaGraph_t captured = nullptr;
-            cudaError_t e = cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal);
-            if (e != cudaSuccess) return set_err(ctx, MT_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
-            rc = record_batch_step(ctx, R, cases);
-            e = cudaStreamEndCapture(ctx.stream, &captured);
-            for (Case *c : cases) c->no_side = false;
-            if (rc || e != cudaSuccess) {
-                if (captured) cudaGraphDestroy(captured);
-                batch_drop(B);
-                return rc ? rc : set_err(ctx, MT_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
-            }
-            B.graph_launches[p] = ctx.launches - before;
-            ctx.launches = before;
-            e = cudaGraphInstantiate(&B.graph[p], captured, 0);
-            cudaGraphDestroy(captured);
-            if (e != cudaSuccess) {
-                B.graph[p] = nullptr;
-                return set_err(ctx, MT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-            }
-            MT_CUDA(ctx, cudaMemcpy(B.ddesc[p], R.hdesc.data(), sizeof(BrickBatch) * R.hdesc.size(),
-                                    cudaMemcpyHostToDevice));
-        } else {
-            for (Case *c : cases) swap_buffers(*c, 0);
+    // capture graph g (0/1: one step from that parity, 2: two steps)
+    auto record = [&](int g) -> int {
+        const int steps = g == 2 ? 2 : 1;
+        BatchRec R;
+        R.b = &B;
+        R.hdesc = &B.hdesc[g];
+        R.hdesc->clear();
+        // at most one descriptor per family (3 models x 4 storages) and chunk for every substep
+        R.cap = (int64_t)((2 << Lmax) * 12 * steps) *
+                (int64_t)((cases.size() + kMaxBatchSlots - 1) / kMaxBatchSlots);
+        MT_CUDA(ctx, cudaMallocAsync(&B.ddesc[g], sizeof(BrickBatch) * R.cap, ctx.stream));
+        R.dbase = B.ddesc[g];
+        for (Case *c : cases) c->no_side = true;
+        const int64_t before = ctx.launches;
+        cudaGraph_t captured = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return set_err(ctx, MT_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+        int r = MT_OK;
+        for (int k = 0; k < steps && !r; ++k) r = record_batch_step(ctx, R, cases);
+        e = cudaStreamEndCapture(ctx.stream, &captured);
+        for (Case *c : cases) c->no_side = false;
+        if (r || e != cudaSuccess) {
+            if (captured) cudaGraphDestroy(captured);
+            batch_drop(B);
+            return r ? r : set_err(ctx, MT_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
         }
-        MT_CUDA(ctx, cudaGraphLaunch(B.graph[p], ctx.stream));
-        ctx.launches += B.graph_launches[p];
-        B.par ^= 1;
+        B.graph_launches[g] = ctx.launches - before;
+        ctx.launches = before;
+        e = cudaGraphInstantiate(&B.graph[g], captured, 0);
+        cudaGraphDestroy(captured);
+        if (e != cudaSuccess) {
+            B.graph[g] = nullptr;
+            return set_err(ctx, MT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+        // stream-ordered upload: it lands before the graph's first launch
+        MT_CUDA(ctx, cudaMemcpyAsync(B.ddesc[g], R.hdesc->data(), sizeof(BrickBatch) * R.hdesc->size(),
+                                     cudaMemcpyHostToDevice, ctx.stream));
+        // recording swapped the members' buffers as executing does; undo it
+        // so that the caller applies one consistent host-side update per launch
+        for (int k = 0; k < steps; ++k)
+            for (Case *c : cases) swap_buffers(*c, 0);
+        return MT_OK;
+    };
+    int s = 0;
+    while (s < n) {
+        const int g = (n - s >= 2) ? 2 : B.par;
+        if (!B.graph[g] && (rc = record(g))) return rc;
+        MT_CUDA(ctx, cudaGraphLaunch(B.graph[g], ctx.stream));
+        ctx.launches += B.graph_launches[g];
+        const int steps = g == 2 ? 2 : 1;
+        for (int k = 0; k < steps; ++k) {
+            for (Case *c : cases) swap_buffers(*c, 0);
+            B.par ^= 1;
+        }
+        s += steps;
         for (Case *c : cases)
             for (int l = 0; l <= c->d.max_level; ++l) c->f_stale |= c->lv[l].bricks;
     }

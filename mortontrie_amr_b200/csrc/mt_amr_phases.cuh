@@ -18,9 +18,6 @@
 
 namespace mt {
 
-enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
-       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
-       PH_SYNC_F, PH_DF, PH_FACE_EQ0 = 24 };
 
 // reserved boundary directions; one copy per translation unit, uploaded by
 // AmrOps<S>::upload_tables when a case of that storage type is built
@@ -780,10 +777,11 @@ __host__ __device__ __forceinline__ double roma3(double r)
     return 0.0;
 }
 
-// rho and the unforced velocity of the band cells from their streamed f
+// rho and the unforced velocity of the band cells from their streamed f; the
+// band's force accumulator restarts from zero
 template <int Q, class S>
 __global__ void k_band_macros(const int32_t *band, int64_t nb, int64_t n, const S *f, typename Store<S>::C *rho,
-                              typename Store<S>::C *u)
+                              typename Store<S>::C *u, long long *acc)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -799,13 +797,6 @@ __global__ void k_band_macros(const int32_t *band, int64_t nb, int64_t n, const 
     u[i] = x;
     u[n + i] = y;
     u[2 * n + i] = z;
-}
-
-static __global__ void k_band_clear(const int32_t *band, int64_t nb, int64_t n, long long *acc)
-{
-    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (j >= nb) return;
-    const int64_t i = band[j];
     acc[i] = 0;
     acc[n + i] = 0;
     acc[2 * n + i] = 0;
@@ -813,10 +804,24 @@ static __global__ void k_band_clear(const int32_t *band, int64_t nb, int64_t n, 
 
 // one marker: interpolate rho and u at X(t), force F = 2 rho (U - u), spread
 // F dv phi into the band cells; fk receives -F dv (the force on the body)
+// grid[(x - lo) + dx ((y - lo) + dy (z - lo))] = index of band cell (x, y, z) or -1
+static __global__ void k_band_grid(const int32_t *band, int64_t nb, const uint64_t *key, int64_t lx, int64_t ly,
+                            int64_t lz, int64_t dx, int64_t dy, int64_t dz, int32_t *grid)
+{
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nb) return;
+    const int32_t i = band[j];
+    const uint64_t k = key[i];
+    const int64_t x = (int64_t)compact3(k) - lx, y = (int64_t)compact3(k >> 1) - ly, z = (int64_t)compact3(k >> 2) - lz;
+    if (x < 0 || y < 0 || z < 0 || x >= dx || y >= dy || z >= dz) return;
+    grid[x + dx * (y + dy * z)] = i;
+}
+
 template <class C>
 __global__ void k_df_markers(int64_t nm, const double *ref, const double *dv, double cx, double cy, double cz,
-                             const double *path, int64_t period, const long long *tstep, const uint64_t *key,
-                             const uint32_t *tag, int64_t n, const C *rho, const C *u, long long *acc, double *fk)
+                             const double *path, int64_t period, const long long *tstep, const int32_t *grid,
+                             int64_t lx, int64_t ly, int64_t lz, int64_t dx, int64_t dy, int64_t dz, int64_t n,
+                             const C *rho, const C *u, long long *acc, double *fk)
 {
     const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (m >= nm) return;
@@ -831,12 +836,11 @@ __global__ void k_df_markers(int64_t nm, const double *ref, const double *dv, do
     for (int c = 0; c < 27; ++c) {
         const int64_t x = ix + c % 3 - 1, y = iy + (c / 3) % 3 - 1, z = iz + c / 9 - 1;
         const double wv = roma3((double)x + 0.5 - X) * roma3((double)y + 0.5 - Y) * roma3((double)z + 0.5 - Z);
-        int32_t i = -1;
-        if (x >= 0 && y >= 0 && z >= 0) {
-            const uint64_t k = dilate3((uint64_t)x) | (dilate3((uint64_t)y) << 1) | (dilate3((uint64_t)z) << 2);
-            i = (int32_t)find_key(key, n, k);
-            if (i >= 0 && !(tag[i] & TAG_BAND)) i = -1;
-        }
+        // only band cells take force; they all lie in the grid's box
+        const int64_t gx = x - lx, gy = y - ly, gz = z - lz;
+        const int32_t i = (gx >= 0 && gy >= 0 && gz >= 0 && gx < dx && gy < dy && gz < dz)
+                              ? __ldg(grid + gx + dx * (gy + dy * gz))
+                              : -1;
         idx[c] = i;
         wgt[c] = wv;
         if (i >= 0) {
@@ -861,7 +865,28 @@ __global__ void k_df_markers(int64_t nm, const double *ref, const double *dv, do
     fk[2 * nm + m] = -fz * d;
 }
 
-static __global__ void k_df_tick(long long *tstep) { *tstep += 1; }
+// the body force of one forcing step: a fixed-order sum of the markers'
+// forces into the accumulator (fx, fy, fz, count), then the substep count
+static __global__ void k_df_sum(const double *fk, int64_t nm, double *acc, long long *tstep)
+{
+    __shared__ double s[3][1024];
+    const int t = threadIdx.x;
+    double a[3] = {0., 0., 0.};
+    for (int64_t j = t; j < nm; j += blockDim.x)
+        for (int c = 0; c < 3; ++c) a[c] += fk[c * nm + j];
+    for (int c = 0; c < 3; ++c) s[c][t] = a[c];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (t < w)
+            for (int c = 0; c < 3; ++c) s[c][t] += s[c][t + w];
+        __syncthreads();
+    }
+    if (t == 0) {
+        for (int c = 0; c < 3; ++c) acc[c] += s[c][0];
+        acc[3] += 1.0;
+        *tstep += 1;
+    }
+}
 
 // LBGK collision with Guo forcing on the band cells: u = (j + g / 2) / rho,
 // fcol = f - (f - feq(rho, u)) / tau + (1 - 1 / (2 tau)) w [3 (e - u) + 9 (e.u) e].g
@@ -1076,26 +1101,19 @@ int df_force(Ctx &ctx, Case &c, int l)
     Level &lv = c.lv[l];
     if (!lv.nband) return MT_OK;
     k_band_macros<Q, S><<<grid_for(lv.nband, 128), 128, 0, s>>>(lv.band, lv.nband, lv.n, A::f(lv), A::rho(lv),
-                                                                 A::u(lv));
-    MT_LAUNCHED(ctx);
-    k_band_clear<<<grid_for(lv.nband, 256), 256, 0, s>>>(lv.band, lv.nband, lv.n, c.acc);
+                                                                 A::u(lv), c.acc);
     MT_LAUNCHED(ctx);
     if (!c.nm) {
         k_force_tick<<<1, 1, 0, s>>>(c.force_acc);
         MT_LAUNCHED(ctx);
         return MT_OK;
     }
-    k_df_markers<C><<<grid_for(c.nm, 64), 64, 0, s>>>(c.nm, c.mref, c.mdv, c.center[0], c.center[1], c.center[2],
-                                                       c.path, c.period, c.tstep, lv.key, lv.tag, lv.n,
-                                                       (const C *)A::rho(lv), (const C *)A::u(lv), c.acc, c.mforce);
+    k_df_markers<C><<<grid_for(c.nm, 64), 64, 0, s>>>(
+        c.nm, c.mref, c.mdv, c.center[0], c.center[1], c.center[2], c.path, c.period, c.tstep, c.mgrid, c.mlo[0],
+        c.mlo[1], c.mlo[2], c.mdim[0], c.mdim[1], c.mdim[2], lv.n, (const C *)A::rho(lv), (const C *)A::u(lv), c.acc,
+        c.mforce);
     MT_LAUNCHED(ctx);
-    k_df_tick<<<1, 1, 0, s>>>(c.tstep);
-    MT_LAUNCHED(ctx);
-    const unsigned nb = grid_for(c.nm, 256);
-    double *partial = c.mforce + 3 * c.nm;
-    k_force_partial<<<nb, 256, 0, s>>>(c.mforce, c.nm, partial);
-    MT_LAUNCHED(ctx);
-    k_force_reduce<<<1, 256, 0, s>>>(partial, nb, c.force_acc);
+    k_df_sum<<<1, 1024, 0, s>>>(c.mforce, c.nm, c.force_acc, c.tstep);
     MT_LAUNCHED(ctx);
     return MT_OK;
 }
@@ -1285,6 +1303,13 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         if (int rc = df_force<S, Q>(ctx, c, l)) return rc;
         return band_collide<S, Q>(ctx, c, l, lv.fcol_alt);
     }
+    case PH_BAND_GRID:
+        if (lv.nband && c.mgrid) {
+            k_band_grid<<<grid_for(lv.nband, 256), 256, 0, s>>>(lv.band, lv.nband, lv.key, c.mlo[0], c.mlo[1], c.mlo[2],
+                                                                c.mdim[0], c.mdim[1], c.mdim[2], c.mgrid);
+            MT_LAUNCHED(ctx);
+        }
+        return MT_OK;
     case PH_SYNC_F:
         if (lv.bricks) {
             k_brick_pull<Q, S><<<grid_for(lv.nbrick, 4), 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, (uint32_t)n,

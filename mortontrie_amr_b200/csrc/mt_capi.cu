@@ -3,6 +3,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -28,8 +29,6 @@ int set_err(Ctx &ctx, int code, const std::string &msg)
 
 namespace {
 
-enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
-       PH_BC_FACE0 = 8 };
 
 int get_case(mt_ctx *h, int32_t id, Case **out)
 {
@@ -660,10 +659,11 @@ int mt_case_set_markers(mt_ctx *h, int32_t id, int64_t nm, const double *ref, co
     if (!c->lv[c->d.max_level].nband) return set_err(ctx, MT_ERR_MESH, "no MT_SET_IB_BAND cells on the finest level");
     if (nm < 0 || period < 1 || (nm && (!ref || !dv)) || !center || !path)
         return set_err(ctx, MT_ERR_ARG, "bad marker arrays");
-    void *old[] = {c->mref, c->mdv, c->path, c->mforce};
+    void *old[] = {c->mref, c->mdv, c->path, c->mforce, c->mgrid};
     for (void *p : old)
         if (p) cudaFree(p);
     c->mref = c->mdv = c->path = c->mforce = nullptr;
+    c->mgrid = nullptr;
     c->nm = nm;
     c->period = period;
     for (int a = 0; a < 3; ++a) c->center[a] = center[a];
@@ -677,6 +677,31 @@ int mt_case_set_markers(mt_ctx *h, int32_t id, int64_t nm, const double *ref, co
         MT_CUDA(ctx, cudaMemcpy(c->mdv, dv, sizeof(double) * nm, cudaMemcpyHostToDevice));
     }
     MT_CUDA(ctx, cudaMemsetAsync(c->tstep, 0, sizeof(long long), ctx.stream));
+    if (nm) {
+        // the box every marker stencil can reach over the path: centre + path
+        // extent +- (largest marker offset + 2.5 cells)
+        double rmax = 0.0, pmin[3] = {0, 0, 0}, pmax[3] = {0, 0, 0};
+        for (int64_t m = 0; m < nm; ++m) {
+            const double r2 = ref[m] * ref[m] + ref[nm + m] * ref[nm + m] + ref[2 * nm + m] * ref[2 * nm + m];
+            rmax = std::max(rmax, std::sqrt(r2));
+        }
+        for (int64_t t = 0; t < period; ++t)
+            for (int a = 0; a < 3; ++a) {
+                pmin[a] = std::min(pmin[a], path[6 * t + a]);
+                pmax[a] = std::max(pmax[a], path[6 * t + a]);
+            }
+        int64_t total = 1;
+        for (int a = 0; a < 3; ++a) {
+            const int64_t lo = std::max<int64_t>(0, (int64_t)std::floor(center[a] + pmin[a] - rmax - 3.0));
+            const int64_t hi = (int64_t)std::ceil(center[a] + pmax[a] + rmax + 3.0);
+            c->mlo[a] = lo;
+            c->mdim[a] = std::max<int64_t>(1, hi - lo);
+            total *= c->mdim[a];
+        }
+        MT_CUDA(ctx, cudaMalloc(&c->mgrid, sizeof(int32_t) * total));
+        MT_CUDA(ctx, cudaMemsetAsync(c->mgrid, 0xff, sizeof(int32_t) * total, ctx.stream));
+        if ((rc = amr_phase(ctx, *c, PH_BAND_GRID, c->d.max_level))) return rc;
+    }
     // the captured steps bake the marker arrays in
     if (c->graph) cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;

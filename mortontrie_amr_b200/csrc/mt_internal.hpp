@@ -18,6 +18,12 @@ namespace mt {
 constexpr int kMaxLevels = MT_MAX_LEVELS;
 constexpr int kNumSets = 6;  // lat_f, F2C, C2F, ghost C2F, ghost F2C, solid
 
+// phases of the multi-level step (amr_phase): the reference's strategy calls,
+// then the fused schedule's own passes
+enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
+       PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
+       PH_SYNC_F, PH_DF, PH_BAND_GRID, PH_FACE_EQ0 = 24 };
+
 // per-cell tag bits (which reference index sets the cell belongs to)
 enum : uint32_t {
     TAG_LATF = 1u,
@@ -144,6 +150,9 @@ struct Case {
     int64_t period = 1;
     long long *tstep = nullptr;
     long long *acc = nullptr;  // [3][n_L] Eulerian force, fixed point
+    // dense index of the band cells over the box the markers' stencils can reach
+    int32_t *mgrid = nullptr;
+    int64_t mlo[3] = {0, 0, 0}, mdim[3] = {0, 0, 0};
     bool use_bricks = true;  // fused pass over 4x4x4 bricks where a level allows it (else cell lists)
     bool primed = false;
     int par0 = 0;
@@ -166,9 +175,12 @@ struct Case {
 // step, so two captured graphs alternate (par).
 struct Batch {
     std::vector<int32_t> ids;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int64_t graph_launches[2] = {0, 0};
-    BrickBatch *ddesc[2] = {nullptr, nullptr};
+    // [0], [1]: one coarse step from level-0 parity 0 / 1; [2]: two coarse
+    // steps (back to the same parity, valid from either)
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+    int64_t graph_launches[3] = {0, 0, 0};
+    BrickBatch *ddesc[3] = {nullptr, nullptr, nullptr};
+    std::vector<BrickBatch> hdesc[3];  // host copies (kept alive for the asynchronous upload)
     int par = 0;
     std::vector<cudaStream_t> pool;
     std::vector<cudaEvent_t> ev_join;

@@ -73,6 +73,9 @@ class MeshSpec:
     # transverse oscillation of a marker sphere: (amplitude in coarse cells,
     # period in finest steps), along y
     oscillation: Optional[tuple] = None
+    # extra inner depth of the forcing band in coarse cells, so that one mesh
+    # serves marker spheres of radius in [radius - band_slack, radius]
+    band_slack: float = 0.0
 
 
 @dataclass
@@ -84,12 +87,13 @@ class Markers:
     path: np.ndarray    # (period, 6): centre displacement and velocity at substep t % period
 
 
-def sphere_markers(spec: "MeshSpec") -> Markers:
+def sphere_markers(spec: "MeshSpec", radius: Optional[float] = None) -> Markers:
     """One marker per finest cell^2 of surface on a Fibonacci lattice; the
-    path samples y(t) = A sin(2 pi t / T) and its velocity per finest step."""
+    path samples y(t) = A sin(2 pi t / T) and its velocity per finest step.
+    radius (coarse cells) defaults to the mesh's sphere radius."""
     L = spec.max_level
     s = 1 << L
-    r = spec.sphere.radius * s
+    r = (spec.sphere.radius if radius is None else radius) * s
     nm = max(1, int(round(4.0 * np.pi * r * r)))
     i = np.arange(nm) + 0.5
     zc = 1.0 - 2.0 * i / nm
@@ -252,7 +256,7 @@ def build_mesh(spec: MeshSpec) -> Mesh:
             dmin = np.sqrt(px * px + (py - qy) ** 2 + pz * pz)
             dmax = np.sqrt(px * px + (np.abs(py) + amp) ** 2 + pz * pz)
             m = 2.7
-            band = (dmin <= r + m) & (dmax >= r - m)
+            band = (dmin <= r + m) & (dmax >= r - m - spec.band_slack * s)
             sets["ib_band"] = _sorted_unique(cell_key(L, l, fx[band], fy[band], fz[band]))
         elif l == L and spec.sphere is not None:
             if L == 0:

@@ -1,0 +1,283 @@
+"""Request loop for served sphere-flow cases (continuous batching).
+
+Each request is a flow past a direct-forcing sphere (Lagrangian markers,
+3-point kernel): radius R coarse cells, coarse channel 16R x 8R x 8R, 1 to 3
+refinement levels, Reynolds number Re, D3Q19 LBGK, optionally oscillating
+transversely with amplitude R/2 and a period of 2000 finest steps.  A
+request is solved when its case has advanced `finest_steps` finest-level
+steps (one oscillation period by default); its result is the mean drag and
+lift coefficients over the run.
+
+The server keeps every admitted case resident on the device and steps all
+of them together in one batch (mt_batch_*): a request that arrives while
+others are running is admitted as soon as the HBM budget allows and joins
+the batch at the next chunk boundary; a finished case leaves it and frees
+its memory.  Host meshes come from a cache of templates keyed by the grid
+radius ceil(R), the level count and whether the sphere oscillates (the
+forcing band of a template covers any radius in [ceil(R) - 1, ceil(R)]);
+the markers are made per request for its exact radius.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from .case import CaseParams, df_sphere_case
+from .mesh import Markers
+
+PERIOD = 2000          # finest steps of one oscillation
+AMPLITUDE = 0.5        # oscillation amplitude in sphere radii
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float         # seconds after the start of the stream
+    radius: float          # coarse cells
+    levels: int            # refinement levels (max_level)
+    re: float
+    oscillating: bool
+    finest_steps: int = PERIOD
+
+    @property
+    def grid_radius(self) -> int:
+        return int(math.ceil(self.radius))
+
+    def coarse_steps(self) -> int:
+        return max(1, self.finest_steps >> self.levels)
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    admitted: float
+    finished: float
+    cd: float
+    cl: float
+    coarse_steps: int
+    storage: str
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def poisson_requests(seed: int = 5, rate: float = 20.0, duration: float = 300.0, radius=(3.0, 8.0),
+                     levels=(1, 3), re=(20.0, 300.0), p_osc: float = 0.5,
+                     finest_steps: int = PERIOD) -> list:
+    """Seeded Poisson stream: exponential inter-arrival times of mean 1/rate
+    over `duration` seconds; R, Re uniform, levels uniform in [levels[0],
+    levels[1]], oscillating with probability p_osc."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t > duration:
+            break
+        out.append(Request(rid=len(out), arrival=t, radius=float(rng.uniform(*radius)),
+                           levels=int(rng.integers(levels[0], levels[1] + 1)), re=float(rng.uniform(*re)),
+                           oscillating=bool(rng.random() < p_osc), finest_steps=finest_steps))
+    return out
+
+
+def template_key(req: Request) -> tuple:
+    return (req.grid_radius, req.levels, req.oscillating)
+
+
+def build_template(key: tuple):
+    """Host mesh of a template (picklable for worker processes)."""
+    r, levels, osc = key
+    return df_sphere_case(radius=r, max_level=levels, re=100.0, oscillating=osc, period=PERIOD,
+                          amplitude=AMPLITUDE, band_slack=1.0).mesh
+
+
+def request_case(req: Request, mesh):
+    """The case of one request on a template mesh: its own viscosity and
+    markers (exact radius and oscillation amplitude)."""
+    from .case import Case
+    s = 1 << req.levels
+    r = req.radius * s
+    nm = max(1, int(round(4.0 * np.pi * r * r)))
+    i = np.arange(nm) + 0.5
+    zc = 1.0 - 2.0 * i / nm
+    rc = np.sqrt(np.maximum(0.0, 1.0 - zc * zc))
+    phi = i * (np.pi * (3.0 - np.sqrt(5.0)))
+    ref = np.ascontiguousarray(np.stack([r * rc * np.cos(phi), r * rc * np.sin(phi), r * zc]))
+    dv = np.full(nm, 4.0 * np.pi * r * r / nm)
+    if req.oscillating:
+        amp = AMPLITUDE * r
+        t = np.arange(PERIOD)
+        path = np.zeros((PERIOD, 6))
+        path[:, 1] = amp * np.sin(2.0 * np.pi * t / PERIOD)
+        path[:, 4] = amp * (2.0 * np.pi / PERIOD) * np.cos(2.0 * np.pi * t / PERIOD)
+    else:
+        path = np.zeros((1, 6))
+    center = tuple(float(c * s) for c in mesh.spec.sphere.center)
+    mk = Markers(ref=ref, dv=dv, center=center, path=np.ascontiguousarray(path))
+    u = 0.05
+    params = CaseParams(q=19, collision="LBGK", ib_method="DF", bc_mode="zouhe_outflow",
+                        nu=u * 2.0 * req.radius / req.re, u_bc=(u, 0.0, 0.0), u_ref=u)
+    return Case(dataclasses.replace(mesh, markers=mk), params)
+
+
+def footprint_bytes(case, storage: str) -> int:
+    """Device memory of a resident case: three population buffers, the
+    neighbour table, macros, tags and lists, bricks and halo tables."""
+    sb = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}[storage]
+    q = case.params.q
+    total = 0
+    for lv in case.mesh.levels:
+        n = sum(int(v.size) for v in lv.values())
+        total += n * (3 * q * sb + 4 * (q - 1) + 4 * 4 + 8 + 4 + 16 + 8 + 20)
+    total += int(case.mesh.markers.dv.size) * 80 if case.mesh.markers is not None else 0
+    return total + (8 << 20)
+
+
+def drag_lift(mgr, req: Request) -> tuple:
+    f = mgr.force()
+    n = max(f[3], 1.0)
+    u = 0.05
+    d = 2.0 * req.radius * (1 << req.levels)
+    area = np.pi * d * d / 4.0
+    return 2.0 * f[0] / n / (u * u * area), 2.0 * f[1] / n / (u * u * area)
+
+
+class TemplateCache:
+    def __init__(self, workers: int = 0):
+        self.meshes = {}
+        self.workers = workers
+
+    def prepare(self, requests):
+        """Build every template the requests need (in worker processes)."""
+        keys = sorted({template_key(r) for r in requests} - set(self.meshes))
+        if not keys:
+            return
+        if self.workers > 1 and len(keys) > 1:
+            import multiprocessing as mp
+            from concurrent.futures import ProcessPoolExecutor
+            with ProcessPoolExecutor(max_workers=min(self.workers, len(keys)),
+                                     mp_context=mp.get_context("spawn")) as ex:
+                for k, m in zip(keys, ex.map(build_template, keys)):
+                    self.meshes[k] = m
+        else:
+            for k in keys:
+                self.meshes[k] = build_template(k)
+
+    def get(self, req: Request):
+        k = template_key(req)
+        if k not in self.meshes:
+            self.meshes[k] = build_template(k)
+        return self.meshes[k]
+
+
+@dataclass
+class ServerStats:
+    results: list = field(default_factory=list)
+    wall_s: float = 0.0
+    max_resident: int = 0
+    max_bytes: int = 0
+    chunks: int = 0
+    admit_s: float = 0.0    # host time creating and building admitted cases
+    step_s: float = 0.0     # host time issuing batch steps (graph capture included)
+    drain_s: float = 0.0    # host time waiting for finished cases and reading results
+
+    def summary(self) -> dict:
+        lat = np.array([r.latency for r in self.results]) if self.results else np.zeros(1)
+        return {"completed": len(self.results), "wall_s": round(self.wall_s, 2),
+                "cases_per_hour": round(3600.0 * len(self.results) / max(self.wall_s, 1e-9), 1),
+                "p50_s": round(float(np.percentile(lat, 50)), 3), "p99_s": round(float(np.percentile(lat, 99)), 3),
+                "max_resident_cases": self.max_resident, "max_resident_gb": round(self.max_bytes / 1e9, 2),
+                "chunks": self.chunks, "admit_s": round(self.admit_s, 2), "step_s": round(self.step_s, 2),
+                "drain_s": round(self.drain_s, 2)}
+
+
+class Server:
+    """Continuous-batching request loop on one device context."""
+
+    def __init__(self, ctx, cache: TemplateCache, storage: str = "f16", budget_gb: float = 150.0,
+                 chunk: int = 16, scaling: str = "standard"):
+        self.ctx = ctx
+        self.cache = cache
+        self.storage = storage
+        self.budget = int(budget_gb * 1e9)
+        self.chunk = chunk
+        self.scaling = scaling
+
+    def run(self, requests, realtime: bool = True, clock=None) -> ServerStats:
+        from .lbm import Batch, LBM_Manager
+        stats = ServerStats()
+        pending = sorted(requests, key=lambda r: r.arrival)
+        batch = Batch(self.ctx)
+        live = {}    # rid -> [mgr, req, remaining, admitted, bytes]
+        used = 0
+        t0 = time.perf_counter() if clock is None else clock()
+        now = (lambda: time.perf_counter() - t0) if clock is None else (lambda: clock() - t0)
+        qi = 0
+        while qi < len(pending) or live:
+            t = now() if realtime else float("inf")
+            # admit arrivals as memory frees up (oldest first)
+            while qi < len(pending) and pending[qi].arrival <= t:
+                req = pending[qi]
+                case = request_case(req, self.cache.get(req))
+                need = footprint_bytes(case, self.storage)
+                if live and used + need > self.budget:
+                    break
+                ta = time.perf_counter()
+                mgr = LBM_Manager(self.ctx, case, self.storage, schedule="fused", scaling=self.scaling)
+                batch.add(mgr)
+                stats.admit_s += time.perf_counter() - ta
+                live[req.rid] = [mgr, req, req.coarse_steps(), now(), need]
+                used += need
+                qi += 1
+            stats.max_resident = max(stats.max_resident, len(live))
+            stats.max_bytes = max(stats.max_bytes, used)
+            if not live:
+                if qi < len(pending) and realtime:
+                    time.sleep(max(0.0, min(pending[qi].arrival - now(), 0.05)))
+                continue
+            k = min(self.chunk, min(v[2] for v in live.values()))
+            ts = time.perf_counter()
+            batch.step(k)
+            stats.step_s += time.perf_counter() - ts
+            stats.chunks += 1
+            for v in live.values():
+                v[2] -= k
+            done = [rid for rid, v in live.items() if v[2] == 0]
+            if done:
+                td = time.perf_counter()
+                self.ctx.synchronize()
+                for rid in done:
+                    mgr, req, _, adm, need = live.pop(rid)
+                    cd, cl = drag_lift(mgr, req)
+                    stats.results.append(Result(rid=rid, arrival=req.arrival, admitted=adm, finished=now(), cd=cd,
+                                                cl=cl, coarse_steps=req.coarse_steps(), storage=self.storage))
+                    batch.remove(mgr)
+                    mgr.close()
+                    used -= need
+                stats.drain_s += time.perf_counter() - td
+        self.ctx.synchronize()
+        stats.wall_s = now()
+        batch.close()
+        return stats
+
+
+def solve_alone(ctx, cache: TemplateCache, req: Request, storage: str = "f16", scaling: str = "standard",
+                schedule: Optional[str] = None) -> tuple:
+    """One request by itself (no batch); returns (cd, cl, seconds)."""
+    from .lbm import LBM_Manager
+    case = request_case(req, cache.get(req))
+    t = time.perf_counter()
+    mgr = LBM_Manager(ctx, case, storage, schedule=schedule or ("phases" if storage == "f64" else "fused"),
+                      scaling=scaling)
+    mgr.fluidSimulate(req.coarse_steps())
+    ctx.synchronize()
+    cd, cl = drag_lift(mgr, req)
+    dt = time.perf_counter() - t
+    mgr.close()
+    return cd, cl, dt
