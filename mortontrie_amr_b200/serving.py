@@ -32,6 +32,7 @@ from .mesh import Markers
 
 PERIOD = 2000          # finest steps of one oscillation
 AMPLITUDE = 0.5        # oscillation amplitude in sphere radii
+U_INLET = 0.05         # inlet velocity, lattice units of level 0
 
 
 @dataclass
@@ -120,7 +121,7 @@ def request_case(req: Request, mesh):
         path = np.zeros((1, 6))
     center = tuple(float(c * s) for c in mesh.spec.sphere.center)
     mk = Markers(ref=ref, dv=dv, center=center, path=np.ascontiguousarray(path))
-    u = 0.05
+    u = U_INLET
     params = CaseParams(q=19, collision="LBGK", ib_method="DF", bc_mode="zouhe_outflow",
                         nu=u * 2.0 * req.radius / req.re, u_bc=(u, 0.0, 0.0), u_ref=u)
     return Case(dataclasses.replace(mesh, markers=mk), params)
@@ -142,7 +143,7 @@ def footprint_bytes(case, storage: str) -> int:
 def drag_lift(mgr, req: Request) -> tuple:
     f = mgr.force()
     n = max(f[3], 1.0)
-    u = 0.05
+    u = U_INLET
     d = 2.0 * req.radius * (1 << req.levels)
     area = np.pi * d * d / 4.0
     return 2.0 * f[0] / n / (u * u * area), 2.0 * f[1] / n / (u * u * area)
