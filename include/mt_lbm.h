@@ -223,6 +223,14 @@ int mt_batch_remove(mt_ctx *ctx, int32_t batch_id, int32_t case_id);
 int mt_batch_size(mt_ctx *ctx, int32_t batch_id, int32_t *n_cases);
 /* n coarse steps of every member; asynchronous on the context stream */
 int mt_batch_step(mt_ctx *ctx, int32_t batch_id, int32_t n_coarse_steps);
+/* Admission helpers for a request loop (no reference counterpart): switch a
+ * case to MT_SCHED_FUSED and build its fused-schedule tables (bricks, second
+ * buffers, lookahead) now, synchronising only this context's stream; then
+ * move the case to another context on the same device (a serving context
+ * whose stream keeps running its batch meanwhile).  The case gets a new id
+ * in dst; it must not be in a batch. */
+int mt_case_prepare(mt_ctx *ctx, int32_t case_id);
+int mt_case_transfer(mt_ctx *src, int32_t case_id, mt_ctx *dst, int32_t *new_id);
 /* accumulated momentum-exchange force of treat() calls: fx, fy, fz, count
  * (LBM_Manager::accumIBForce, LBM_Manager.cpp:846-852) */
 int mt_get_force(mt_ctx *ctx, int32_t case_id, double *out4);

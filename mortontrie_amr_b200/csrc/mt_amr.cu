@@ -1028,7 +1028,8 @@ void batch_drop(Batch &b)
     for (int p = 0; p < 3; ++p) {
         if (b.graph[p]) cudaGraphExecDestroy(b.graph[p]);
         b.graph[p] = nullptr;
-        if (b.ddesc[p]) cudaFree(b.ddesc[p]);
+        // stream-ordered: no device-wide synchronisation on a membership change
+        if (b.ddesc[p]) cudaFreeAsync(b.ddesc[p], b.free_stream);
         b.ddesc[p] = nullptr;
         b.hdesc[p].clear();
     }
@@ -1054,6 +1055,7 @@ int batch_step(Ctx &ctx, Batch &B, const std::vector<Case *> &cases, int n)
         if ((rc = amr_sync_f(ctx, *c))) return rc;
         if (!c->primed && (rc = prime_fused(ctx, *c))) return rc;
     }
+    B.free_stream = ctx.stream;
     if (B.pool.empty()) {
         const int P = 8;
         for (int p = 0; p < P; ++p) {

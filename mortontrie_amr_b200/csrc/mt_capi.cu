@@ -717,6 +717,38 @@ int mt_case_set_markers(mt_ctx *h, int32_t id, int64_t nm, const double *ref, co
     return MT_OK;
 }
 
+int mt_case_prepare(mt_ctx *h, int32_t id)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "prepare needs a built multi-level case");
+    if ((rc = amr_sync_f(ctx, *c))) return rc;
+    if (c->schedule != MT_SCHED_FUSED) {
+        c->schedule = MT_SCHED_FUSED;
+        c->primed = false;
+    }
+    if ((rc = amr_prime(ctx, *c))) return rc;
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
+int mt_case_transfer(mt_ctx *src, int32_t id, mt_ctx *dst, int32_t *new_id)
+{
+    Case *c;
+    int rc = get_case(src, id, &c);
+    if (rc) return rc;
+    if (!dst || !new_id) return set_err(src->c, MT_ERR_ARG, "null destination");
+    if (dst->c.device != src->c.device) return set_err(src->c, MT_ERR_ARG, "contexts on different devices");
+    if (c->in_batch) return set_err(src->c, MT_ERR_STATE, "remove the case from its batches first");
+    MT_CUDA(src->c, cudaStreamSynchronize(src->c.stream));
+    src->c.cases[id] = nullptr;
+    dst->c.cases.push_back(c);
+    *new_id = (int32_t)dst->c.cases.size() - 1;
+    return MT_OK;
+}
+
 // ---- batches ------------------------------------------------------------------
 namespace {
 int get_batch(mt_ctx *h, int32_t id, Batch **out)

@@ -185,6 +185,7 @@ struct Batch {
     std::vector<cudaStream_t> pool;
     std::vector<cudaEvent_t> ev_join;
     cudaEvent_t ev_fork = nullptr;
+    cudaStream_t free_stream = nullptr;  // the stream the batch last ran on
 };
 
 struct Ctx {

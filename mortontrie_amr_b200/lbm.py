@@ -32,7 +32,7 @@ EXPORTS = [
     "mt_case_get_macros", "mt_case_reduce", "mt_calculate_macros", "mt_collide", "mt_stream", "mt_explosion",
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
     "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_face_velocity", "mt_case_set_markers",
-    "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step",
+    "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
 ]
 
 
@@ -76,7 +76,7 @@ def lib():
             "mt_case_get_populations": [vp, i32, i32, dp, dp], "mt_case_get_macros": [vp, i32, i32, dp, dp],
             "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
             "mt_batch_create": [vp, i32p], "mt_batch_destroy": [vp, i32], "mt_batch_add": [vp, i32, i32],
-            "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -100,6 +100,7 @@ class Context:
     """One device context (mt_create); owns every case created on it."""
 
     def __init__(self, device: int = 0):
+        self.device = device
         self.h = C.c_void_p()
         rc = lib().mt_create(device, C.byref(self.h))
         if rc != 0:
@@ -194,6 +195,18 @@ class LBM_Manager:
         self.set_interface_scaling(scaling)
         for face, u in sorted(getattr(case.params, "face_u", {}).items()):
             self.set_face_velocity(face, u)
+
+    def prepare(self):
+        """Switch to the fused schedule and build its tables now."""
+        self.ctx.check(lib().mt_case_prepare(self.ctx.h, self.id), "mt_case_prepare")
+        self.schedule = "fused"
+
+    def transfer(self, dst: Context):
+        """Move this case to another context on the same device."""
+        nid = C.c_int32()
+        self.ctx.check(lib().mt_case_transfer(self.ctx.h, self.id, dst.h, C.byref(nid)), "mt_case_transfer")
+        self.ctx = dst
+        self.id = nid.value
 
     def set_markers(self, mk):
         """Upload the Lagrangian markers of a direct-forcing sphere (Markers)."""

@@ -211,8 +211,11 @@ class Server:
         self.scaling = scaling
 
     def run(self, requests, realtime: bool = True, clock=None) -> ServerStats:
-        from .lbm import Batch, LBM_Manager
+        from .lbm import Batch, Context, LBM_Manager
         stats = ServerStats()
+        # admitted cases are built on a context of their own, so that the
+        # build's synchronisations do not wait for the batch's queued steps
+        builder = Context(self.ctx.device)
         pending = sorted(requests, key=lambda r: r.arrival)
         batch = Batch(self.ctx)
         live = {}    # rid -> [mgr, req, remaining, admitted, bytes]
@@ -230,7 +233,9 @@ class Server:
                 if live and used + need > self.budget:
                     break
                 ta = time.perf_counter()
-                mgr = LBM_Manager(self.ctx, case, self.storage, schedule="fused", scaling=self.scaling)
+                mgr = LBM_Manager(builder, case, self.storage, schedule="fused", scaling=self.scaling)
+                mgr.prepare()
+                mgr.transfer(self.ctx)
                 batch.add(mgr)
                 stats.admit_s += time.perf_counter() - ta
                 live[req.rid] = [mgr, req, req.coarse_steps(), now(), need]
@@ -265,6 +270,7 @@ class Server:
         self.ctx.synchronize()
         stats.wall_s = now()
         batch.close()
+        builder.close()
         return stats
 
 
