@@ -408,6 +408,24 @@ int amr_build(Ctx &ctx, Case &c)
         int64_t maxn = 0;
         for (int b = 0; b < 26; ++b) maxn = std::max(maxn, c.lv[0].nbc[b]);
         if (maxn) MT_CUDA(ctx, cudaMallocAsync(&c.bc_tmp, sizeof(double) * 18 * maxn, ctx.stream));
+        // the concatenated list of all 26 sets for the one-pass sweep
+        int64_t tot = 0;
+        for (int b = 0; b < 26; ++b) tot += c.lv[0].nbc[b];
+        if (tot) {
+            c.nbc_all = tot;
+            MT_CUDA(ctx, cudaMallocAsync(&c.bc_all, sizeof(int32_t) * tot, ctx.stream));
+            MT_CUDA(ctx, cudaMallocAsync(&c.bc_setb, tot, ctx.stream));
+            MT_CUDA(ctx, cudaMallocAsync(&c.bc_tmp_all, sizeof(double) * 18 * tot, ctx.stream));
+            int64_t off = 0;
+            for (int b = 0; b < 26; ++b) {
+                const int64_t nb = c.lv[0].nbc[b];
+                if (!nb) continue;
+                MT_CUDA(ctx, cudaMemcpyAsync(c.bc_all + off, c.lv[0].bclist[b], sizeof(int32_t) * nb,
+                                             cudaMemcpyDeviceToDevice, ctx.stream));
+                MT_CUDA(ctx, cudaMemsetAsync(c.bc_setb + off, b, nb, ctx.stream));
+                off += nb;
+            }
+        }
     }
     // direct-forcing band of the finest level and its collide list without the band
     {
@@ -505,11 +523,15 @@ void amr_free(Case &c)
             if (lv.bclist[b]) cudaFree(lv.bclist[b]);
         lv = Level();
     }
-    void *ptrs[] = {c.dis_key, c.dis, c.ib_force, c.force_acc, c.dev_err, c.bc_tmp,
+    void *ptrs[] = {c.dis_key, c.dis, c.ib_force, c.force_acc, c.dev_err, c.bc_tmp, c.bc_all, c.bc_setb, c.bc_tmp_all,
                     c.mref, c.mdv, c.path, c.mforce, c.tstep, c.acc, c.mgrid};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     c.bc_tmp = nullptr;
+    c.bc_all = nullptr;
+    c.bc_setb = nullptr;
+    c.bc_tmp_all = nullptr;
+    c.nbc_all = 0;
     c.dis_key = nullptr;
     c.dis = nullptr;
     c.ib_force = nullptr;

@@ -308,6 +308,42 @@ __global__ void k_bc_neq(const int32_t *list, int64_t nl, int b, int64_t n, cons
     }
 }
 
+// the same sweep over every boundary set at once (one Jacobi pass: all values,
+// then all writes); setb gives each cell's set, ub its face's velocity
+struct BcVel {
+    double u[26][3];
+};
+template <int Q, class S>
+__global__ void k_bc_neq_all(const int32_t *list, const int8_t *setb, int64_t nl, int64_t n, const int32_t *nbr,
+                             const typename Store<S>::C *rho, const typename Store<S>::C *u, S *f, BcVel ub,
+                             double *tmp, int phase, int *err)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    const int b = setb[j];
+    constexpr int W = Q == 19 ? 14 : 18;
+    for (int t = 0; t < W; ++t) {
+        const int k = Q == 19 ? c_bdry19[b][t] : c_bdry27[b][t];
+        if (k < 0) break;
+        if (phase == 0) {
+            const int32_t nb = k == 0 ? (int32_t)i : nbr[(int64_t)(k - 1) * n + i];
+            if (nb < 0) {
+                atomicOr(err, DEVERR_MISSING_BC_NBR);
+                tmp[t * nl + j] = (double)full_of<S, Q>(T::ld(f, k * n + i), k);
+                continue;
+            }
+            const C fw = feq_g<Q, C>(k, rho[i], (C)ub.u[b][0], (C)ub.u[b][1], (C)ub.u[b][2]);
+            const C fn = feq_g<Q, C>(k, rho[nb], u[nb], u[n + nb], u[2 * n + nb]);
+            tmp[t * nl + j] = (double)(fw + full_of<S, Q>(T::ld(f, k * n + nb), k) - fn);
+        } else {
+            T::st(f, k * n + i, stored_of<S, Q>((C)tmp[t * nl + j], k));
+        }
+    }
+}
+
 // Restated inlet/outflow on the x faces: West wall cells hold
 // fcol = feq(rho0, u_bc) (BC/ZouHe_Velocity.cpp:62-115 writes the
 // equilibrium at the boundary cell's own, never-updated density), East wall
@@ -1202,6 +1238,22 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         // all six face groups in the reference's order (LBM_Simulator.cpp:90-95), or one
         const int f0 = phase == PH_BC ? 0 : phase - PH_BC_FACE0, f1 = phase == PH_BC ? 6 : f0 + 1;
         Level &l0 = c.lv[0];
+        if (phase == PH_BC && c.bc_all && c.nbc_all) {
+            BcVel ub;
+            for (int face = 0; face < 6; ++face)
+                for (int g = 0; g < 9; ++g) {
+                    const int b = kFaceSets[face][g];
+                    if (b < 0) break;
+                    for (int a = 0; a < 3; ++a) ub.u[b][a] = c.face_u[face][a];
+                }
+            for (int ph = 0; ph < 2; ++ph) {
+                k_bc_neq_all<Q, S><<<grid_for(c.nbc_all, B), B, 0, s>>>(c.bc_all, c.bc_setb, c.nbc_all, l0.n, l0.nbr,
+                                                                         A::rho(l0), A::u(l0), A::f(l0), ub,
+                                                                         c.bc_tmp_all, ph, c.dev_err);
+                MT_LAUNCHED(ctx);
+            }
+            return MT_OK;
+        }
         double *tmp = c.bc_tmp;
         if (!tmp) return MT_OK;
         for (int face = f0; face < f1; ++face)

@@ -130,7 +130,12 @@ struct Case {
     int64_t N = 0;       // cells
     void *A = nullptr, *B = nullptr;  // populations [Q * N] in the storage type
     bool a_is_fcol = false;           // false: A holds post-stream f; true: A holds post-collision fcol
-    double *bc_tmp = nullptr;         // scratch of the boundary sweep
+    double *bc_tmp = nullptr;         // scratch of the boundary sweep (per set)
+    // every boundary set at once: cells, their set, scratch [18][n]
+    int32_t *bc_all = nullptr;
+    int8_t *bc_setb = nullptr;
+    double *bc_tmp_all = nullptr;
+    int64_t nbc_all = 0;
     int dense_block = 256;            // threads per block of the fused kernel (autotuned)
     // captured coarse step of the phase schedule (recorded with level 0's
     // post-collision buffer in parity graph_par0)
