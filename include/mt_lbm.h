@@ -108,6 +108,33 @@ int mt_case_destroy(mt_ctx *ctx, int32_t case_id);
 int mt_case_add_set(mt_ctx *ctx, int32_t case_id, int32_t level, int32_t set_id, const uint64_t *keys, int64_t n);
 /* Lat_Manager::dis: finest-level keys (ascending) and Q-1 wall distances each */
 int mt_case_set_dis(mt_ctx *ctx, int32_t case_id, const uint64_t *keys, const double *rows, int64_t n);
+/* Box-and-sphere lattice classified on the device (no reference counterpart:
+ * the reference voxelises an STL in Lat_Manager::voxelize, Lat_Voxelize.cpp
+ * :17-733).  Produces the index-set contract of Lat_Manager.hpp:245-316 for
+ * nested refinement boxes: the level-0 boundary shell split into the 26
+ * lat_bc sets (Lat_Voxelize.cpp:242-288), F2C = the 1-cell shell of each
+ * refinement box, C2F = the 2-cell shell of each refined level, the ghost
+ * layers from the Q neighbours (Lat_Voxelize.cpp:676-733), and for a sphere
+ * either the voxelised solid with its wall distances (Lat_Voxelize.cpp
+ * :1252-1285) or the direct-forcing band. */
+typedef struct mt_mesh_spec {
+    int64_t coarse[3];                   /* level-0 cells per axis (the case's extent0) */
+    int32_t boundary_bc[3];              /* 1: boundary shell on this axis, 0: periodic (the case's periodic[] inverted) */
+    int32_t has_refine[MT_MAX_LEVELS];   /* level l < max_level holds a refinement box */
+    int64_t refine_lo[MT_MAX_LEVELS][3]; /* the box [lo, hi) in level-l cells */
+    int64_t refine_hi[MT_MAX_LEVELS][3];
+    int32_t sphere;                      /* 0 none, 1 solid + wall distances, 2 forcing band (MT_IB_DF) */
+    int32_t pad;
+    double center[3];                    /* coarse-cell units from the box corner */
+    double radius;                       /* coarse cells */
+    double osc_amplitude;                /* band of a sphere oscillating along y: amplitude in coarse cells */
+    double band_slack;                   /* extra inner band depth in coarse cells */
+} mt_mesh_spec;
+
+/* generate the case's sets from spec and build it (replaces mt_case_add_set,
+ * mt_case_set_dis and mt_case_build); MT_ERR_MESH with the host mesher's
+ * messages when the boxes or the sphere break the contract */
+int mt_case_generate(mt_ctx *ctx, int32_t case_id, const mt_mesh_spec *spec);
 /* device build: radix sort + unique of the keys, set tags, neighbour table
  * by binary search of the Morton neighbour keys (Morton_Assist::find_neighbor
  * + D_map_define::find), explosion/coalescence child tables, IB list */

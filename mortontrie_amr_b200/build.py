@@ -1,7 +1,8 @@
 """Build libmtlbm.so (sm_100a) in-tree with nvcc.
 
-The FP64 translation units (multi-level path and the FP64 dense kernel) are
-compiled with --fmad=false so that their arithmetic keeps the reference's
+The FP64 translation units (multi-level path, the FP64 dense kernel and the
+lattice classification, whose wall distances must equal the host mesher's)
+are compiled with --fmad=false so that their arithmetic keeps the reference's
 rounding; the reduced-precision dense kernels use FMA.
 """
 from __future__ import annotations
@@ -27,6 +28,7 @@ SOURCES = {
     "mt_amr_lp.cu": [],
     "mt_dense_f64.cu": ["--fmad=false"],
     "mt_dense_lp.cu": [],
+    "mt_mesh.cu": ["--fmad=false"],
 }
 
 

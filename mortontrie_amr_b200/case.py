@@ -14,7 +14,7 @@ from typing import Optional
 import numpy as np
 
 from .lattice import directions, reference_units, weights
-from .mesh import Mesh, MeshSpec, Sphere, build_mesh
+from .mesh import Mesh, MeshSpec, Sphere, build_mesh, spec_mesh
 
 COLLISIONS = {"LBGK": 0, "Cumulant": 1}
 IB_METHODS = {"DW": 0, "FH": 1, "DF": 2}
@@ -60,9 +60,19 @@ class Case:
         return self.params.q
 
 
+def _mesh(spec: MeshSpec, where: str):
+    """The host mesher's sets ("host") or the spec alone, classified on the
+    device when the case is created ("device")."""
+    if where == "host":
+        return build_mesh(spec)
+    if where == "device":
+        return spec_mesh(spec)
+    raise ValueError(f"mesh must be 'host' or 'device', not {where!r}")
+
+
 def sphere_case(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1, refine=None, center=(16, 16, 16),
                 radius=4.0, u=0.05, re=20.0, boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow",
-                ib_method="FH", stream_convention="reference") -> Case:
+                ib_method="FH", stream_convention="reference", mesh="host") -> Case:
     """Flow past a sphere; nu = u * 2R / Re in coarse units."""
     if refine is None:
         refine = [((4, 8, 8), (28, 24, 24))]
@@ -71,13 +81,13 @@ def sphere_case(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1, refine
                     sphere=Sphere(tuple(center), radius))
     p = CaseParams(q=q, collision=collision, ib_method=ib_method, bc_mode=bc_mode, nu=nu, u_bc=(u, 0.0, 0.0),
                    u_ref=u, stream_convention=stream_convention)
-    return Case(build_mesh(spec), p)
+    return Case(_mesh(spec, mesh), p)
 
 
 def nested_sphere_case(q=27, collision="Cumulant", coarse=(192, 96, 96), max_level=3, center=(64, 48, 48),
                        radius=6.0, half_widths=(4.0, 2.5, 1.75), u=0.04, re=200.0,
                        boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow", ib_method="FH",
-                       stream_convention="reference") -> Case:
+                       stream_convention="reference", mesh="host") -> Case:
     """Flow past a sphere refined in nested boxes centred on it: the box
     refined from level l to l+1 has half-width half_widths[l] * radius in
     coarse units (the defaults are the 4-level D3Q27 cumulant sphere case:
@@ -91,11 +101,11 @@ def nested_sphere_case(q=27, collision="Cumulant", coarse=(192, 96, 96), max_lev
         refine.append((tuple(ci - hw for ci in c), tuple(ci + hw for ci in c)))
     return sphere_case(q=q, collision=collision, coarse=coarse, max_level=max_level, refine=refine, center=center,
                        radius=radius, u=u, re=re, boundary=boundary, bc_mode=bc_mode, ib_method=ib_method,
-                       stream_convention=stream_convention)
+                       stream_convention=stream_convention, mesh=mesh)
 
 
 def cavity_case(q=19, collision="LBGK", coarse=(32, 32, 32), max_level=1, re=100.0, u_lid=0.05,
-                refine=None, ib_method="FH") -> Case:
+                refine=None, ib_method="FH", mesh="host") -> Case:
     """Lid-driven cavity: walls on every face (non-equilibrium boundary),
     the Top face moving at u_lid along x; nu = u_lid * nz / Re in coarse
     units.  With max_level > 0 the levels refine nested boxes under the lid
@@ -117,11 +127,11 @@ def cavity_case(q=19, collision="LBGK", coarse=(32, 32, 32), max_level=1, re=100
         spec = MeshSpec(q=q, max_level=1, coarse=tuple(coarse), refine=[None], boundary=("bc", "bc", "bc"))
     p = CaseParams(q=q, collision=collision, ib_method=ib_method, bc_mode="neq", nu=nu, u_bc=(0.0, 0.0, 0.0),
                    u_ref=u_lid, face_u={5: (u_lid, 0.0, 0.0)})
-    return Case(build_mesh(spec), p)
+    return Case(_mesh(spec, mesh), p)
 
 
 def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q=19, period=2000,
-                   amplitude=0.5, band_slack=0.0) -> Case:
+                   amplitude=0.5, band_slack=0.0, mesh="host") -> Case:
     """Flow past a sphere represented by direct-forcing Lagrangian markers
     (one per finest cell^2 of surface, 3-point kernel): coarse channel
     16R x 8R x 8R, inlet on West, outflow on East, periodic sides, centre at
@@ -151,19 +161,19 @@ def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q
                     oscillation=(amp, period) if oscillating else None, band_slack=band_slack)
     p = CaseParams(q=q, collision="LBGK", ib_method="DF", bc_mode="zouhe_outflow", nu=nu, u_bc=(u, 0.0, 0.0),
                    u_ref=u)
-    return Case(build_mesh(spec), p)
+    return Case(_mesh(spec, mesh), p)
 
 
 def uniform_box_case(q=19, n=(16, 16, 16), nu=1.0 / 30.0, boundary=("periodic",) * 3, collision="LBGK",
                      u_ref=0.02, storage="f64", stream_convention="reference", empty_levels=0,
-                     u_bc=(0.0, 0.0, 0.0)) -> Case:
+                     u_bc=(0.0, 0.0, 0.0), mesh="host") -> Case:
     """Single populated level; `empty_levels` adds empty finer levels so the
     reference harness (which needs at least two levels) can run it."""
     spec = MeshSpec(q=q, max_level=empty_levels, coarse=tuple(n), refine=[None] * empty_levels,
                     boundary=tuple(boundary))
     p = CaseParams(q=q, collision=collision, nu=nu, u_bc=tuple(u_bc), u_ref=u_ref, bc_mode="neq",
                    storage=storage, stream_convention=stream_convention)
-    return Case(build_mesh(spec), p)
+    return Case(_mesh(spec, mesh), p)
 
 
 def taylor_green_fields(n, u0=0.02, rho_amp=True):

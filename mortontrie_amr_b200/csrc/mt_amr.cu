@@ -296,18 +296,27 @@ static int build_level(Ctx &ctx, Case &c, int l)
 {
     Level &lv = c.lv[l];
     const int Q = c.d.q;
-    const int64_t nraw = (int64_t)lv.raw_keys.size();
+    const bool on_dev = lv.draw_keys != nullptr;
+    const int64_t nraw = on_dev ? lv.ndraw : (int64_t)lv.raw_keys.size();
     lv.n = 0;
     if (nraw > 0) {
         uint64_t *d_raw = nullptr, *d_sorted = nullptr;
         uint8_t *d_set = nullptr;
         int *d_num = nullptr;
-        MT_CUDA(ctx, cudaMallocAsync(&d_raw, 8 * nraw, ctx.stream));
+        if (on_dev) {
+            d_raw = lv.draw_keys;
+            d_set = lv.draw_set;
+            lv.draw_keys = nullptr;
+            lv.draw_set = nullptr;
+            lv.ndraw = 0;
+        } else {
+            MT_CUDA(ctx, cudaMallocAsync(&d_raw, 8 * nraw, ctx.stream));
+            MT_CUDA(ctx, cudaMallocAsync(&d_set, nraw, ctx.stream));
+            MT_CUDA(ctx, cudaMemcpyAsync(d_raw, lv.raw_keys.data(), 8 * nraw, cudaMemcpyHostToDevice, ctx.stream));
+            MT_CUDA(ctx, cudaMemcpyAsync(d_set, lv.raw_set.data(), nraw, cudaMemcpyHostToDevice, ctx.stream));
+        }
         MT_CUDA(ctx, cudaMallocAsync(&d_sorted, 8 * nraw, ctx.stream));
-        MT_CUDA(ctx, cudaMallocAsync(&d_set, nraw, ctx.stream));
         MT_CUDA(ctx, cudaMallocAsync(&d_num, sizeof(int), ctx.stream));
-        MT_CUDA(ctx, cudaMemcpyAsync(d_raw, lv.raw_keys.data(), 8 * nraw, cudaMemcpyHostToDevice, ctx.stream));
-        MT_CUDA(ctx, cudaMemcpyAsync(d_set, lv.raw_set.data(), nraw, cudaMemcpyHostToDevice, ctx.stream));
         size_t t1 = 0, t2 = 0;
         MT_CUDA(ctx, cub::DeviceRadixSort::SortKeys(nullptr, t1, d_raw, d_sorted, (int)nraw, 0, 64, ctx.stream));
         MT_CUDA(ctx, cudaMallocAsync(&lv.key, 8 * nraw, ctx.stream));
@@ -384,13 +393,16 @@ int amr_build(Ctx &ctx, Case &c)
         if (rc) return rc;
     }
     // dis rows and the IB cell list on the finest level
-    c.ndis = (int64_t)c.h_dis_key.size();
+    if (!c.dis_on_device) c.ndis = (int64_t)c.h_dis_key.size();
     const int W = c.d.q - 1;
     if (c.ndis > 0) {
-        MT_CUDA(ctx, cudaMallocAsync(&c.dis_key, 8 * c.ndis, ctx.stream));
-        MT_CUDA(ctx, cudaMallocAsync(&c.dis, 8 * c.ndis * W, ctx.stream));
-        MT_CUDA(ctx, cudaMemcpyAsync(c.dis_key, c.h_dis_key.data(), 8 * c.ndis, cudaMemcpyHostToDevice, ctx.stream));
-        MT_CUDA(ctx, cudaMemcpyAsync(c.dis, c.h_dis.data(), 8 * c.ndis * W, cudaMemcpyHostToDevice, ctx.stream));
+        if (!c.dis_on_device) {
+            MT_CUDA(ctx, cudaMallocAsync(&c.dis_key, 8 * c.ndis, ctx.stream));
+            MT_CUDA(ctx, cudaMallocAsync(&c.dis, 8 * c.ndis * W, ctx.stream));
+            MT_CUDA(ctx, cudaMemcpyAsync(c.dis_key, c.h_dis_key.data(), 8 * c.ndis, cudaMemcpyHostToDevice,
+                                         ctx.stream));
+            MT_CUDA(ctx, cudaMemcpyAsync(c.dis, c.h_dis.data(), 8 * c.ndis * W, cudaMemcpyHostToDevice, ctx.stream));
+        }
         Level &fl = c.lv[L];
         if (fl.n > 0) {
             k_dis_rows<<<grid_for(fl.n, 256), 256, 0, ctx.stream>>>(fl.key, fl.n, c.dis_key, c.ndis, fl.disrow, fl.tag);
@@ -514,7 +526,7 @@ void amr_free(Case &c)
         void *ptrs[] = {lv.key, lv.tag, lv.bcidx, lv.disrow, lv.nbr, lv.f, lv.fcol, lv.rho, lv.u,
                         lv.collide_list, lv.stream_list, lv.iblist, lv.expl_src, lv.expl_child, lv.coal_child,
                         lv.fcol_alt, lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls, lv.bhalo,
-                        lv.band, lv.collide_nb};
+                        lv.band, lv.collide_nb, lv.draw_keys, lv.draw_set};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         for (int s = 0; s < kNumSets; ++s)

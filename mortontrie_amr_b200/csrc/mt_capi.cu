@@ -303,6 +303,74 @@ int mt_case_build(mt_ctx *h, int32_t id)
     return MT_OK;
 }
 
+int mt_case_generate(mt_ctx *h, int32_t id, const mt_mesh_spec *sp)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || c->built) return set_err(ctx, MT_ERR_STATE, "case already built");
+    if (!sp) return set_err(ctx, MT_ERR_ARG, "null mesh spec");
+    for (int l = 0; l <= c->d.max_level; ++l)
+        if (!c->lv[l].raw_keys.empty()) return set_err(ctx, MT_ERR_STATE, "sets were already added to the case");
+    if (!c->h_dis_key.empty()) return set_err(ctx, MT_ERR_STATE, "dis was already set");
+    const int L = c->d.max_level;
+    for (int a = 0; a < 3; ++a) {
+        if (sp->coarse[a] != c->d.extent0[a]) return set_err(ctx, MT_ERR_ARG, "spec extent differs from the case's");
+        if ((sp->boundary_bc[a] != 0) == (c->d.periodic[a] != 0))
+            return set_err(ctx, MT_ERR_ARG, "spec boundary differs from the case's periodic axes");
+        if (sp->coarse[a] < 1 || (sp->coarse[a] << L) > (int64_t(1) << 21))
+            return set_err(ctx, MT_ERR_ARG, "extent out of the 21-bit Morton range");
+    }
+    if (sp->sphere < 0 || sp->sphere > 2) return set_err(ctx, MT_ERR_ARG, "sphere must be 0, 1 or 2");
+    if (sp->sphere == 2 && c->d.ib_method != MT_IB_DF)
+        return set_err(ctx, MT_ERR_ARG, "a forcing band needs ib_method MT_IB_DF");
+    if (sp->sphere && !(sp->radius > 0.0)) return set_err(ctx, MT_ERR_ARG, "sphere radius must be positive");
+    {
+        int64_t lo[3] = {0, 0, 0}, hi[3] = {sp->coarse[0], sp->coarse[1], sp->coarse[2]};
+        for (int l = 0; l < L; ++l) {
+            if (!sp->has_refine[l]) break;
+            for (int a = 0; a < 3; ++a) {
+                if (sp->refine_lo[l][a] < lo[a] || sp->refine_hi[l][a] > hi[a] ||
+                    sp->refine_hi[l][a] - sp->refine_lo[l][a] < 1)
+                    return set_err(ctx, MT_ERR_ARG, "refinement box outside its level's domain");
+                lo[a] = 2 * sp->refine_lo[l][a];
+                hi[a] = 2 * sp->refine_hi[l][a];
+            }
+            if ((hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]) > INT32_MAX)
+                return set_err(ctx, MT_ERR_ARG, "a level box above 2^31 cells");
+        }
+        if (sp->coarse[0] * sp->coarse[1] * sp->coarse[2] > INT32_MAX)
+            return set_err(ctx, MT_ERR_ARG, "a level box above 2^31 cells");
+    }
+    MT_CUDA(ctx, cudaSetDevice(ctx.device));
+    rc = amr_generate(ctx, *c, *sp);
+    if (rc) {
+        for (int l = 0; l <= L; ++l) {
+            Level &lv = c->lv[l];
+            if (lv.draw_keys) cudaFreeAsync(lv.draw_keys, ctx.stream);
+            if (lv.draw_set) cudaFreeAsync(lv.draw_set, ctx.stream);
+            lv.draw_keys = nullptr;
+            lv.draw_set = nullptr;
+            lv.ndraw = 0;
+        }
+        if (c->dis_key) cudaFreeAsync(c->dis_key, ctx.stream);
+        if (c->dis) cudaFreeAsync(c->dis, ctx.stream);
+        c->dis_key = nullptr;
+        c->dis = nullptr;
+        c->ndis = 0;
+        c->dis_on_device = false;
+        return rc;
+    }
+    rc = amr_build(ctx, *c);
+    if (rc) return rc;
+    const double u0[3] = {c->d.u_bc[0], c->d.u_bc[1], c->d.u_bc[2]};
+    rc = amr_init_equilibrium(ctx, *c, c->d.rho0, u0);
+    if (rc) return rc;
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
 int mt_case_level_size(mt_ctx *h, int32_t id, int32_t level, int64_t *n)
 {
     Case *c;

@@ -89,6 +89,10 @@ struct Level {
     // raw uploads, consumed by the build
     std::vector<uint64_t> raw_keys;
     std::vector<uint8_t> raw_set;  // 0..5 sets, 16 + b for lat_bc[b]
+    // the same pairs generated on the device (mt_case_generate), used instead
+    uint64_t *draw_keys = nullptr;
+    uint8_t *draw_set = nullptr;
+    int64_t ndraw = 0;
 };
 
 // one case level in a batched brick pass
@@ -121,6 +125,7 @@ struct Case {
     double *dis = nullptr;
     std::vector<uint64_t> h_dis_key;
     std::vector<double> h_dis;
+    bool dis_on_device = false;  // dis_key / dis generated on the device (ndis set)
     double *ib_force = nullptr;  // [3 * nib] per-cell force of the last treat()
     double *force_acc = nullptr; // [4] fx, fy, fz, treat count
     int *dev_err = nullptr;
@@ -205,6 +210,8 @@ struct Ctx {
 
 // kernel launchers implemented in the .cu files
 int amr_build(Ctx &ctx, Case &c);
+// device lattice classification: raw sets of every level and the dis table
+int amr_generate(Ctx &ctx, Case &c, const mt_mesh_spec &spec);
 int amr_init_equilibrium(Ctx &ctx, Case &c, double rho0, const double *u0);
 int amr_lbm_kernel(Ctx &ctx, Case &c, int level);
 int amr_step(Ctx &ctx, Case &c, int n);

@@ -1,0 +1,538 @@
+// Lattice classification on the device: the per-level index sets of
+// Lat_Manager (Lat_Manager.hpp:245-316) for nested refinement boxes and an
+// analytic sphere, generated directly as raw (key, set) pairs for the build
+// (mt_case_generate).  It restates, set for set, what the host mesher
+// (mortontrie_amr_b200/mesh.py) produces -- boundary shell split into the 26
+// lat_bc sets, F2C = 1-cell shell of each refinement box, C2F = 2-cell shell
+// of each refined level, ghost layers from Q-neighbours, the voxelised solid
+// with its wall distances (Lat_Voxelize.cpp:1252-1285 semantics) or the
+// direct-forcing band -- and raises the same contract errors.  Compiled
+// without FMA contraction so the wall distances equal the host's.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "mt_internal.hpp"
+
+namespace mt {
+
+namespace {
+
+// payload byte 0: the build's set code (0 lat_f, 1 F2C, 2 C2F, 5 solid,
+// 16 + b lat_bc[b]); bit 8: in the forcing band; 0xff: not stored
+enum : uint32_t { P_LATF = 0, P_F2C = 1, P_C2F = 2, P_SF = 5, P_NONE = 0xffu, P_BAND = 0x100u };
+enum : int { MERR_BOX_BC = 1, MERR_BOX_C2F = 2, MERR_GHOST = 4, MERR_SOLID = 8, MERR_BAND = 16 };
+
+struct Box {
+    int64_t lo[3], hi[3];
+    MT_HD int64_t n() const { return (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]); }
+};
+
+struct LevelGen {
+    int level, L, q;
+    int64_t ext[3];  // level extent in its own cells
+    int bc[3];       // boundary shell on this axis (level 0)
+    int per[3];      // periodic axis
+    Box dom;         // cells of this level
+    int has_ref;     // refinement box of this level present
+    Box ref;         // in this level's cells
+    int sphere;      // 0 none, 1 solid + links, 2 band (finest level only)
+    double cx, cy, cz, r, amp, slack;  // finest-level units
+    int8_t side_bc[27];                // lat_bc index of a (-1, 0, 1)^3 side combination
+};
+
+MT_HD uint64_t level_key(int L, int l, int64_t x, int64_t y, int64_t z)
+{
+    const int sh = L - l;
+    return dilate3((uint64_t)x << sh) | (dilate3((uint64_t)y << sh) << 1) | (dilate3((uint64_t)z << sh) << 2);
+}
+
+// every cell of the level's box: its key (~0 when not stored) and payload
+__global__ void k_classify(LevelGen g, uint64_t *key, uint32_t *pay, int *err)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nx = g.dom.hi[0] - g.dom.lo[0], ny = g.dom.hi[1] - g.dom.lo[1];
+    if (t >= g.dom.n()) return;
+    const int64_t x = g.dom.lo[0] + t % nx, y = g.dom.lo[1] + (t / nx) % ny, z = g.dom.lo[2] + t / (nx * ny);
+    const int64_t c[3] = {x, y, z};
+    int bcb = -1;
+    if (g.level == 0) {
+        int side[3] = {0, 0, 0};
+        for (int a = 0; a < 3; ++a)
+            if (g.bc[a]) side[a] = c[a] == 0 ? -1 : (c[a] == g.ext[a] - 1 ? 1 : 0);
+        if (side[0] || side[1] || side[2]) bcb = g.side_bc[(side[0] + 1) + 3 * (side[1] + 1) + 9 * (side[2] + 1)];
+    }
+    bool f2c = false, removed = false;
+    if (g.has_ref) {
+        bool inside = true, shell = false;
+        for (int a = 0; a < 3; ++a) {
+            inside &= c[a] >= g.ref.lo[a] && c[a] < g.ref.hi[a];
+            shell |= c[a] < g.ref.lo[a] + 1 || c[a] >= g.ref.hi[a] - 1;
+        }
+        f2c = inside && shell;
+        removed = inside && !shell;
+        if (inside && bcb >= 0) atomicOr(err, MERR_BOX_BC);
+    }
+    bool c2f = false;
+    if (g.level > 0)
+        for (int a = 0; a < 3; ++a) c2f |= c[a] < g.dom.lo[a] + 2 || c[a] >= g.dom.hi[a] - 2;
+    if (c2f && f2c) atomicOr(err, MERR_BOX_C2F);
+    uint32_t p;
+    if (removed)
+        p = P_NONE;
+    else if (bcb >= 0)
+        p = 16u + (uint32_t)bcb;
+    else if (f2c)
+        p = P_F2C;
+    else if (c2f)
+        p = P_C2F;
+    else
+        p = P_LATF;
+    if (p == P_LATF && g.sphere && g.level == g.L) {
+        const double px = (double)x + 0.5 - g.cx, py = (double)y + 0.5 - g.cy, pz = (double)z + 0.5 - g.cz;
+        if (g.sphere == 1) {
+            if (px * px + py * py + pz * pz < g.r * g.r) p = P_SF;
+        } else {
+            const double qy = fmin(fmax(py, -g.amp), g.amp);
+            const double dmin = sqrt(px * px + (py - qy) * (py - qy) + pz * pz);
+            const double ay = fabs(py) + g.amp;
+            const double dmax = sqrt(px * px + ay * ay + pz * pz);
+            if ((dmin <= g.r + 2.7) && (dmax >= g.r - 2.7 - g.slack)) p |= P_BAND;
+        }
+    }
+    key[t] = p == P_NONE ? ~0ull : level_key(g.L, g.level, x, y, z);
+    pay[t] = p;
+}
+
+// flags of the payloads: mode 0 set code == v, 1 band bit
+__global__ void k_flags(const uint32_t *pay, int64_t n, int mode, uint32_t v, uint8_t *flag)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    flag[t] = mode == 0 ? ((pay[t] & 0xffu) == v) : ((pay[t] & P_BAND) != 0);
+}
+
+// neighbour keys (Q - 1 per source cell), periodic axes wrapped; ~0 when a
+// coordinate falls below zero (the host mesher's filter)
+template <int Q>
+__global__ void k_nbr_keys(const uint64_t *src, int64_t ns, LevelGen g, uint64_t *out)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= ns * (Q - 1)) return;
+    const int64_t j = t / (Q - 1);
+    const int k = (int)(t - j * (Q - 1)) + 1;
+    const uint64_t key = src[j];
+    const int sh = g.L - g.level;
+    int64_t c[3] = {(int64_t)(compact3(key) >> sh), (int64_t)(compact3(key >> 1) >> sh),
+                    (int64_t)(compact3(key >> 2) >> sh)};
+    const int e[3] = {ex(k), ey(k), ez(k)};
+    bool ok = true;
+    for (int a = 0; a < 3; ++a) {
+        int64_t v = c[a] + e[a];
+        if (g.per[a]) v = ((v % g.ext[a]) + g.ext[a]) % g.ext[a];
+        if (v < 0) ok = false;
+        c[a] = v;
+    }
+    out[t] = ok ? level_key(g.L, g.level, c[0], c[1], c[2]) : ~0ull;
+}
+
+// flag[t]: key valid and (mode 0) in neither a nor b, (mode 1) in a
+__global__ void k_member(const uint64_t *keys, int64_t n, const uint64_t *a, int64_t na, const uint64_t *b,
+                         int64_t nb, int mode, uint8_t *flag)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint64_t k = keys[t];
+    bool f = false;
+    if (k != ~0ull) {
+        const bool ia = na && find_key(a, na, k) >= 0;
+        const bool ib = nb && find_key(b, nb, k) >= 0;
+        f = mode == 0 ? (!ia && !ib) : ia;
+    }
+    flag[t] = f;
+}
+
+__global__ void k_check_in(const uint64_t *keys, int64_t n, const uint64_t *a, int64_t na, const uint64_t *b,
+                           int64_t nb, int flag, int *err)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint64_t k = keys[t];
+    if (k == ~0ull) return;
+    if ((na && find_key(a, na, k) >= 0) || (nb && find_key(b, nb, k) >= 0)) atomicOr(err, flag);
+}
+
+// wall distances of the finest fluid cells (mesh.py _sphere_links, same
+// operation order); hit[j] = 1 when some link crosses the sphere
+template <int Q>
+__global__ void k_links(const uint64_t *keys, int64_t n, double cx, double cy, double cz, double r, double *rows,
+                        uint8_t *hit)
+{
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint64_t key = keys[j];
+    const double px = (double)(int64_t)compact3(key) + 0.5 - cx;
+    const double py = (double)(int64_t)compact3(key >> 1) + 0.5 - cy;
+    const double pz = (double)(int64_t)compact3(key >> 2) + 0.5 - cz;
+    const double c0 = px * px + py * py + pz * pz - r * r;
+    bool any = false;
+    for (int d = 1; d < Q; ++d) {
+        const double a = (double)(ex(d) * ex(d) + ey(d) * ey(d) + ez(d) * ez(d));
+        const double b = 2.0 * (px * ex(d) + py * ey(d) + pz * ez(d));
+        const double disc = b * b - 4.0 * a * c0;
+        double t = -1.0;
+        if (disc >= 0.0) {
+            const double tt = (-b - sqrt(disc)) / (2.0 * a);
+            if (tt >= 0.0 && tt <= 1.0) t = tt;
+        }
+        rows[j * (Q - 1) + (d - 1)] = t;
+        any |= t != -1.0;
+    }
+    hit[j] = any ? 1 : 0;
+}
+
+__global__ void k_gather_rows(const int64_t *idx, int64_t nd, const double *rows, const uint64_t *keys, int w,
+                              double *out, uint64_t *okey)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nd * w) return;
+    const int64_t j = t / w;
+    out[t] = rows[idx[j] * w + (t - j * w)];
+    if (t - j * w == 0) okey[j] = keys[idx[j]];
+}
+
+__global__ void k_codes(const uint32_t *pay, int64_t n, uint8_t *code)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) code[t] = (uint8_t)(pay[t] & 0xffu);
+}
+
+__global__ void k_fill_u8(uint8_t *p, int64_t n, uint8_t v)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < n) p[t] = v;
+}
+
+// device buffer with stream-ordered allocation and release
+template <class T> struct DBuf {
+    T *p = nullptr;
+    int64_t n = 0;
+    cudaStream_t s = nullptr;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    int alloc(Ctx &ctx, int64_t count)
+    {
+        if (p) cudaFreeAsync(p, s);
+        s = ctx.stream;
+        n = count;
+        MT_CUDA(ctx, cudaMallocAsync(&p, sizeof(T) * std::max<int64_t>(count, 1), s));
+        return MT_OK;
+    }
+    ~DBuf()
+    {
+        if (p) cudaFreeAsync(p, s);
+    }
+    T *release()
+    {
+        T *q = p;
+        p = nullptr;
+        return q;
+    }
+};
+
+// keys[flag] in order -> out (count on the host)
+int select_flagged(Ctx &ctx, const uint64_t *keys, const uint8_t *flag, int64_t n, DBuf<uint64_t> &out)
+{
+    if (int rc = out.alloc(ctx, n)) return rc;
+    if (!n) {
+        out.n = 0;
+        return MT_OK;
+    }
+    DBuf<int> cnt;
+    if (int rc = cnt.alloc(ctx, 1)) return rc;
+    size_t tb = 0;
+    MT_CUDA(ctx, cub::DeviceSelect::Flagged(nullptr, tb, keys, flag, out.p, cnt.p, (int)n, ctx.stream));
+    DBuf<char> tmp;
+    if (int rc = tmp.alloc(ctx, (int64_t)tb)) return rc;
+    MT_CUDA(ctx, cub::DeviceSelect::Flagged(tmp.p, tb, keys, flag, out.p, cnt.p, (int)n, ctx.stream));
+    int h = 0;
+    MT_CUDA(ctx, cudaMemcpyAsync(&h, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    out.n = h;
+    return MT_OK;
+}
+
+// sorted unique keys of an unsorted array (sentinels sort last and are kept once)
+int sort_unique(Ctx &ctx, const uint64_t *keys, int64_t n, DBuf<uint64_t> &out)
+{
+    if (int rc = out.alloc(ctx, n)) return rc;
+    if (!n) {
+        out.n = 0;
+        return MT_OK;
+    }
+    DBuf<uint64_t> sorted;
+    if (int rc = sorted.alloc(ctx, n)) return rc;
+    DBuf<int> cnt;
+    if (int rc = cnt.alloc(ctx, 1)) return rc;
+    size_t t1 = 0, t2 = 0;
+    MT_CUDA(ctx, cub::DeviceRadixSort::SortKeys(nullptr, t1, keys, sorted.p, (int)n, 0, 64, ctx.stream));
+    MT_CUDA(ctx, cub::DeviceSelect::Unique(nullptr, t2, sorted.p, out.p, cnt.p, (int)n, ctx.stream));
+    DBuf<char> tmp;
+    if (int rc = tmp.alloc(ctx, (int64_t)std::max(t1, t2))) return rc;
+    MT_CUDA(ctx, cub::DeviceRadixSort::SortKeys(tmp.p, t1, keys, sorted.p, (int)n, 0, 64, ctx.stream));
+    MT_CUDA(ctx, cub::DeviceSelect::Unique(tmp.p, t2, sorted.p, out.p, cnt.p, (int)n, ctx.stream));
+    int h = 0;
+    MT_CUDA(ctx, cudaMemcpyAsync(&h, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    out.n = h;
+    return MT_OK;
+}
+
+int nbr_keys(Ctx &ctx, const LevelGen &g, const uint64_t *src, int64_t ns, DBuf<uint64_t> &out)
+{
+    const int64_t m = ns * (g.q - 1);
+    if (int rc = out.alloc(ctx, m)) return rc;
+    if (!m) return MT_OK;
+    if (g.q == 19)
+        k_nbr_keys<19><<<grid_for(m, 256), 256, 0, ctx.stream>>>(src, ns, g, out.p);
+    else
+        k_nbr_keys<27><<<grid_for(m, 256), 256, 0, ctx.stream>>>(src, ns, g, out.p);
+    MT_LAUNCHED(ctx);
+    return MT_OK;
+}
+
+// the sorted keys of one set code among the level's sorted stored cells
+int set_keys(Ctx &ctx, const uint64_t *skey, const uint32_t *spay, int64_t ns, int mode, uint32_t v,
+             DBuf<uint64_t> &out)
+{
+    DBuf<uint8_t> flag;
+    if (int rc = flag.alloc(ctx, ns)) return rc;
+    if (ns) {
+        k_flags<<<grid_for(ns, 256), 256, 0, ctx.stream>>>(spay, ns, mode, v, flag.p);
+        MT_LAUNCHED(ctx);
+    }
+    return select_flagged(ctx, skey, flag.p, ns, out);
+}
+
+}  // namespace
+
+// raw sets of every level, the dis table or the band, then the build
+int amr_generate(Ctx &ctx, Case &c, const mt_mesh_spec &sp)
+{
+    const int L = c.d.max_level;
+    const int q = c.d.q;
+    static const int8_t sides[26][3] = {
+        {-1, 0, 0}, {1, 0, 0},   {0, -1, 0},  {0, 1, 0},   {0, 0, -1},  {0, 0, 1},   {1, 1, 0},
+        {-1, 1, 0}, {-1, -1, 0}, {1, -1, 0},  {0, 1, 1},   {0, -1, 1},  {0, 1, -1},  {0, -1, -1},
+        {1, 0, 1},  {-1, 0, 1},  {1, 0, -1},  {-1, 0, -1}, {1, 1, 1},   {-1, 1, 1},  {-1, -1, 1},
+        {1, -1, 1}, {1, 1, -1},  {-1, 1, -1}, {-1, -1, -1}, {1, -1, -1}};
+    DBuf<int> derr;
+    if (int rc = derr.alloc(ctx, 1)) return rc;
+    MT_CUDA(ctx, cudaMemsetAsync(derr.p, 0, sizeof(int), ctx.stream));
+    Box dom{{0, 0, 0}, {sp.coarse[0], sp.coarse[1], sp.coarse[2]}};
+    for (int l = 0; l <= L; ++l) {
+        LevelGen g{};
+        g.level = l;
+        g.L = L;
+        g.q = q;
+        for (int a = 0; a < 3; ++a) {
+            g.ext[a] = sp.coarse[a] << l;
+            g.bc[a] = sp.boundary_bc[a];
+            g.per[a] = !sp.boundary_bc[a];
+        }
+        for (int i = 0; i < 27; ++i) g.side_bc[i] = -1;
+        for (int b = 0; b < 26; ++b)
+            g.side_bc[(sides[b][0] + 1) + 3 * (sides[b][1] + 1) + 9 * (sides[b][2] + 1)] = (int8_t)b;
+        g.dom = dom;
+        g.has_ref = l < L && sp.has_refine[l] && dom.n() > 0;
+        if (g.has_ref)
+            for (int a = 0; a < 3; ++a) {
+                g.ref.lo[a] = sp.refine_lo[l][a];
+                g.ref.hi[a] = sp.refine_hi[l][a];
+            }
+        g.sphere = (l == L) ? sp.sphere : 0;
+        const double s = (double)(1 << L);
+        g.cx = sp.center[0] * s;
+        g.cy = sp.center[1] * s;
+        g.cz = sp.center[2] * s;
+        g.r = sp.radius * s;
+        g.amp = sp.osc_amplitude * s;
+        g.slack = sp.band_slack * s;
+        if (g.sphere == 1 && L == 0)
+            return set_err(ctx, MT_ERR_MESH, "the solid boundary is only applied on a refined finest level");
+        Level &lv = c.lv[l];
+        const int64_t nbox = dom.n();
+        // next level's domain: the refinement box doubled
+        Box next{{0, 0, 0}, {0, 0, 0}};
+        if (g.has_ref)
+            for (int a = 0; a < 3; ++a) {
+                next.lo[a] = 2 * g.ref.lo[a];
+                next.hi[a] = 2 * g.ref.hi[a];
+            }
+        dom = next;
+        if (nbox <= 0) continue;
+        // classify and sort the stored cells by key (not stored: ~0, last)
+        DBuf<uint64_t> key, skey;
+        DBuf<uint32_t> pay, spay;
+        if (int rc = key.alloc(ctx, nbox)) return rc;
+        if (int rc = pay.alloc(ctx, nbox)) return rc;
+        if (int rc = skey.alloc(ctx, nbox)) return rc;
+        if (int rc = spay.alloc(ctx, nbox)) return rc;
+        k_classify<<<grid_for(nbox, 256), 256, 0, ctx.stream>>>(g, key.p, pay.p, derr.p);
+        MT_LAUNCHED(ctx);
+        {
+            size_t tb = 0;
+            MT_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tb, key.p, skey.p, pay.p, spay.p, (int)nbox, 0, 64,
+                                                         ctx.stream));
+            DBuf<char> tmp;
+            if (int rc = tmp.alloc(ctx, (int64_t)tb)) return rc;
+            MT_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.p, skey.p, pay.p, spay.p, (int)nbox, 0, 64,
+                                                         ctx.stream));
+        }
+        // stored cells = keys below the sentinel
+        int64_t ns = 0;
+        {
+            DBuf<uint64_t> all;
+            DBuf<uint8_t> flag;
+            if (int rc = flag.alloc(ctx, nbox)) return rc;
+            k_member<<<grid_for(nbox, 256), 256, 0, ctx.stream>>>(skey.p, nbox, nullptr, 0, nullptr, 0, 0, flag.p);
+            MT_LAUNCHED(ctx);
+            if (int rc = select_flagged(ctx, skey.p, flag.p, nbox, all)) return rc;
+            ns = all.n;
+        }
+        DBuf<uint64_t> latf, f2c, c2f, sf, band, gc2f, gf2c;
+        if (int rc = set_keys(ctx, skey.p, spay.p, ns, 0, P_LATF, latf)) return rc;
+        if (int rc = set_keys(ctx, skey.p, spay.p, ns, 0, P_F2C, f2c)) return rc;
+        if (int rc = set_keys(ctx, skey.p, spay.p, ns, 0, P_C2F, c2f)) return rc;
+        if (int rc = set_keys(ctx, skey.p, spay.p, ns, 0, P_SF, sf)) return rc;
+        if (int rc = set_keys(ctx, skey.p, spay.p, ns, 1, 0, band)) return rc;
+        if (l > 0 && c2f.n) {
+            DBuf<uint64_t> cand, uniq;
+            if (int rc = nbr_keys(ctx, g, c2f.p, c2f.n, cand)) return rc;
+            if (int rc = sort_unique(ctx, cand.p, cand.n, uniq)) return rc;
+            DBuf<uint8_t> flag;
+            if (int rc = flag.alloc(ctx, uniq.n)) return rc;
+            if (uniq.n) {
+                k_member<<<grid_for(uniq.n, 256), 256, 0, ctx.stream>>>(uniq.p, uniq.n, latf.p, latf.n, c2f.p, c2f.n,
+                                                                       0, flag.p);
+                MT_LAUNCHED(ctx);
+            }
+            if (int rc = select_flagged(ctx, uniq.p, flag.p, uniq.n, gc2f)) return rc;
+            if (gc2f.n) {
+                k_check_in<<<grid_for(gc2f.n, 256), 256, 0, ctx.stream>>>(gc2f.p, gc2f.n, f2c.p, f2c.n, sf.p, sf.n,
+                                                                         MERR_GHOST, derr.p);
+                MT_LAUNCHED(ctx);
+            }
+        }
+        if (l < L && f2c.n) {
+            DBuf<uint64_t> cand, uniq;
+            if (int rc = nbr_keys(ctx, g, f2c.p, f2c.n, cand)) return rc;
+            if (int rc = sort_unique(ctx, cand.p, cand.n, uniq)) return rc;
+            DBuf<uint8_t> flag;
+            if (int rc = flag.alloc(ctx, uniq.n)) return rc;
+            if (uniq.n) {
+                k_member<<<grid_for(uniq.n, 256), 256, 0, ctx.stream>>>(uniq.p, uniq.n, latf.p, latf.n, nullptr, 0, 1,
+                                                                       flag.p);
+                MT_LAUNCHED(ctx);
+            }
+            if (int rc = select_flagged(ctx, uniq.p, flag.p, uniq.n, gf2c)) return rc;
+        }
+        if (l == L && g.sphere == 1) {
+            // wall distances of the fluid cells; the solid must stay clear of C2F
+            const int w = q - 1;
+            DBuf<double> rows;
+            DBuf<uint8_t> hit;
+            if (int rc = rows.alloc(ctx, latf.n * w)) return rc;
+            if (int rc = hit.alloc(ctx, latf.n)) return rc;
+            if (latf.n) {
+                if (q == 19)
+                    k_links<19><<<grid_for(latf.n, 128), 128, 0, ctx.stream>>>(latf.p, latf.n, g.cx, g.cy, g.cz, g.r,
+                                                                              rows.p, hit.p);
+                else
+                    k_links<27><<<grid_for(latf.n, 128), 128, 0, ctx.stream>>>(latf.p, latf.n, g.cx, g.cy, g.cz, g.r,
+                                                                              rows.p, hit.p);
+                MT_LAUNCHED(ctx);
+            }
+            // indices of the hit cells, in key order
+            DBuf<int64_t> idx;
+            DBuf<int> cnt;
+            if (int rc = idx.alloc(ctx, latf.n)) return rc;
+            if (int rc = cnt.alloc(ctx, 1)) return rc;
+            int nd = 0;
+            if (latf.n) {
+                size_t tb = 0;
+                cub::CountingInputIterator<int64_t> it(0);
+                MT_CUDA(ctx, cub::DeviceSelect::Flagged(nullptr, tb, it, hit.p, idx.p, cnt.p, (int)latf.n, ctx.stream));
+                DBuf<char> tmp;
+                if (int rc = tmp.alloc(ctx, (int64_t)tb)) return rc;
+                MT_CUDA(ctx, cub::DeviceSelect::Flagged(tmp.p, tb, it, hit.p, idx.p, cnt.p, (int)latf.n, ctx.stream));
+                MT_CUDA(ctx, cudaMemcpyAsync(&nd, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+                MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+            }
+            c.ndis = nd;
+            if (nd) {
+                MT_CUDA(ctx, cudaMallocAsync(&c.dis_key, 8 * (size_t)nd, ctx.stream));
+                MT_CUDA(ctx, cudaMallocAsync(&c.dis, 8 * (size_t)nd * w, ctx.stream));
+                k_gather_rows<<<grid_for((int64_t)nd * w, 256), 256, 0, ctx.stream>>>(idx.p, nd, rows.p, latf.p, w,
+                                                                                      c.dis, c.dis_key);
+                MT_LAUNCHED(ctx);
+            }
+            if (sf.n) {
+                DBuf<uint64_t> nk;
+                if (int rc = nbr_keys(ctx, g, sf.p, sf.n, nk)) return rc;
+                k_check_in<<<grid_for(nk.n, 256), 256, 0, ctx.stream>>>(nk.p, nk.n, c2f.p, c2f.n, gc2f.p, gc2f.n,
+                                                                       MERR_SOLID, derr.p);
+                MT_LAUNCHED(ctx);
+            }
+        }
+        if (l == L && g.sphere == 2 && band.n) {
+            DBuf<uint64_t> nk;
+            if (int rc = nbr_keys(ctx, g, band.p, band.n, nk)) return rc;
+            k_check_in<<<grid_for(nk.n, 256), 256, 0, ctx.stream>>>(nk.p, nk.n, c2f.p, c2f.n, nullptr, 0, MERR_BAND,
+                                                                   derr.p);
+            MT_LAUNCHED(ctx);
+        }
+        // raw (key, set) pairs for the build: stored cells, the ghost layers, the band
+        const int64_t nraw = ns + gc2f.n + gf2c.n + band.n;
+        uint64_t *rk = nullptr;
+        uint8_t *rs = nullptr;
+        MT_CUDA(ctx, cudaMallocAsync(&rk, 8 * (size_t)std::max<int64_t>(nraw, 1), ctx.stream));
+        MT_CUDA(ctx, cudaMallocAsync(&rs, (size_t)std::max<int64_t>(nraw, 1), ctx.stream));
+        int64_t off = 0;
+        if (ns) {
+            MT_CUDA(ctx, cudaMemcpyAsync(rk, skey.p, 8 * ns, cudaMemcpyDeviceToDevice, ctx.stream));
+            k_codes<<<grid_for(ns, 256), 256, 0, ctx.stream>>>(spay.p, ns, rs);
+            MT_LAUNCHED(ctx);
+            off = ns;
+        }
+        const DBuf<uint64_t> *extra[3] = {&gc2f, &gf2c, &band};
+        const uint8_t codes[3] = {3, 4, (uint8_t)MT_SET_IB_BAND};
+        for (int e = 0; e < 3; ++e) {
+            const int64_t m = extra[e]->n;
+            if (!m) continue;
+            MT_CUDA(ctx, cudaMemcpyAsync(rk + off, extra[e]->p, 8 * m, cudaMemcpyDeviceToDevice, ctx.stream));
+            k_fill_u8<<<grid_for(m, 256), 256, 0, ctx.stream>>>(rs + off, m, codes[e]);
+            MT_LAUNCHED(ctx);
+            off += m;
+        }
+        lv.draw_keys = rk;
+        lv.draw_set = rs;
+        lv.ndraw = nraw;
+    }
+    int herr = 0;
+    MT_CUDA(ctx, cudaMemcpyAsync(&herr, derr.p, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    if (herr & MERR_BOX_BC) return set_err(ctx, MT_ERR_MESH, "refinement box touches the boundary shell");
+    if (herr & MERR_BOX_C2F) return set_err(ctx, MT_ERR_MESH, "refinement box too close to the coarse/fine interface");
+    if (herr & MERR_GHOST) return set_err(ctx, MT_ERR_MESH, "ghost layer overlaps the next interface or the solid");
+    if (herr & MERR_SOLID) return set_err(ctx, MT_ERR_MESH, "solid too close to the coarse/fine interface");
+    if (herr & MERR_BAND) return set_err(ctx, MT_ERR_MESH, "the forcing band is too close to the coarse/fine interface");
+    c.dis_on_device = true;
+    return MT_OK;
+}
+
+}  // namespace mt

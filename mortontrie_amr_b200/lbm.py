@@ -15,6 +15,7 @@ import os
 import numpy as np
 
 from .case import BC_MODES, COLLISIONS, IB_METHODS, STORAGE, STREAM_CONVENTIONS, Case
+from .mesh import SpecMesh
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmtlbm.so")
@@ -33,6 +34,7 @@ EXPORTS = [
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
     "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
+    "mt_case_generate",
 ]
 
 
@@ -49,6 +51,41 @@ class mt_case_desc(C.Structure):
                 ("bc_mode", C.c_int32), ("stream_convention", C.c_int32), ("storage", C.c_int32),
                 ("periodic", C.c_int32 * 3), ("extent0", C.c_int64 * 3), ("tau", C.c_double * MAX_LEVELS),
                 ("rho0", C.c_double), ("u_bc", C.c_double * 3)]
+
+
+class mt_mesh_spec(C.Structure):
+    _fields_ = [("coarse", C.c_int64 * 3), ("boundary_bc", C.c_int32 * 3), ("has_refine", C.c_int32 * MAX_LEVELS),
+                ("refine_lo", (C.c_int64 * 3) * MAX_LEVELS), ("refine_hi", (C.c_int64 * 3) * MAX_LEVELS),
+                ("sphere", C.c_int32), ("pad", C.c_int32), ("center", C.c_double * 3), ("radius", C.c_double),
+                ("osc_amplitude", C.c_double), ("band_slack", C.c_double)]
+
+
+def make_mesh_spec(spec) -> mt_mesh_spec:
+    """mt_mesh_spec of a MeshSpec (mesh.py): the device classification
+    produces the sets build_mesh(spec) would."""
+    if len(spec.refine) != spec.max_level:
+        raise ValueError("need one refinement box per level below the maximum level")
+    if spec.max_level >= MAX_LEVELS:
+        raise ValueError("too many levels")
+    m = mt_mesh_spec()
+    for a in range(3):
+        m.coarse[a] = int(spec.coarse[a])
+        m.boundary_bc[a] = int(spec.boundary[a] == "bc")
+    for l, box in enumerate(spec.refine):
+        if box is None:
+            break
+        m.has_refine[l] = 1
+        for a in range(3):
+            m.refine_lo[l][a] = int(box[0][a])
+            m.refine_hi[l][a] = int(box[1][a])
+    if spec.sphere is not None:
+        m.sphere = 2 if spec.ib == "markers" else 1
+        for a in range(3):
+            m.center[a] = float(spec.sphere.center[a])
+        m.radius = float(spec.sphere.radius)
+        m.osc_amplitude = float(spec.oscillation[0]) if (spec.ib == "markers" and spec.oscillation) else 0.0
+        m.band_slack = float(spec.band_slack)
+    return m
 
 
 _lib = None
@@ -76,7 +113,8 @@ def lib():
             "mt_case_get_populations": [vp, i32, i32, dp, dp], "mt_case_get_macros": [vp, i32, i32, dp, dp],
             "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
             "mt_batch_create": [vp, i32p], "mt_batch_destroy": [vp, i32], "mt_batch_add": [vp, i32, i32],
-            "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
+            "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -160,11 +198,14 @@ class LBM_Manager:
     strategy objects (collide / stream / treat / boundary) as methods."""
 
     def __init__(self, ctx: Context, case: Case, storage: str = "f64", schedule: str = "phases",
-                 scaling: str = "reference"):
+                 scaling: str = "reference", generate: bool = False):
         """storage: "f64" (the reference's precision, bit-exact) or "f32" /
         "f16" / "bf16" (FP32 arithmetic on stored deviations f - w_q).
         schedule: "phases" (the reference's passes) or "fused" (stream fused
-        with the next collision; same state after every coarse step)."""
+        with the next collision; same state after every coarse step).
+        generate: classify the lattice on the device from the mesh spec
+        (mt_case_generate) instead of uploading the host mesher's sets; a
+        SpecMesh (no host sets) is always generated."""
         self.ctx = ctx
         self.case = case
         self.q = case.params.q
@@ -174,6 +215,11 @@ class LBM_Manager:
         ctx.check(lib().mt_case_create(ctx.h, C.byref(d), C.byref(cid)), "mt_case_create")
         self.id = cid.value
         m = case.mesh
+        if generate or isinstance(m, SpecMesh):
+            ms = make_mesh_spec(m.spec)
+            ctx.check(lib().mt_case_generate(ctx.h, self.id, C.byref(ms)), "mt_case_generate")
+            self._finish(m, schedule, scaling)
+            return
         for l in range(self.L + 1):
             for name, sid in SET_IDS.items():
                 k = np.ascontiguousarray(m.levels[l].get(name, np.zeros(0, np.uint64)), np.uint64)
@@ -189,11 +235,14 @@ class LBM_Manager:
         ctx.check(lib().mt_case_set_dis(ctx.h, self.id, _ptr(dk, C.c_uint64), _ptr(dr, C.c_double), dk.size),
                   "set_dis")
         ctx.check(lib().mt_case_build(ctx.h, self.id), "mt_case_build")
+        self._finish(m, schedule, scaling)
+
+    def _finish(self, m, schedule, scaling):
         if m.markers is not None:
             self.set_markers(m.markers)
         self.set_schedule(schedule)
         self.set_interface_scaling(scaling)
-        for face, u in sorted(getattr(case.params, "face_u", {}).items()):
+        for face, u in sorted(getattr(self.case.params, "face_u", {}).items()):
             self.set_face_velocity(face, u)
 
     def prepare(self):

@@ -133,6 +133,22 @@ class Mesh:
         return [int(self.all_keys(l).size) for l in range(self.spec.max_level + 1)]
 
 
+@dataclass
+class SpecMesh:
+    """A mesh known by its spec only: the device classifies the lattice when
+    the case is created (mt_case_generate), producing the sets build_mesh
+    would; the markers of a direct-forcing sphere are made on the host."""
+    spec: MeshSpec
+    markers: Optional["Markers"] = None
+
+
+def spec_mesh(spec: MeshSpec) -> SpecMesh:
+    if len(spec.refine) != spec.max_level:
+        raise ValueError("need one refinement box per level below the maximum level")
+    mk = sphere_markers(spec) if (spec.sphere is not None and spec.ib == "markers") else None
+    return SpecMesh(spec=spec, markers=mk)
+
+
 def _grid(lo, hi):
     xs = np.arange(lo[0], hi[0], dtype=np.int64)
     ys = np.arange(lo[1], hi[1], dtype=np.int64)

@@ -1,0 +1,112 @@
+"""Lattice classification on the device (mt_case_generate) against the host
+mesher: the same keys, set tags and neighbour tables on every level, and
+bit-identical populations and forces after stepping both builds."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from mortontrie_amr_b200.lbm import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def _cases():
+    from mortontrie_amr_b200.case import (cavity_case, df_sphere_case, nested_sphere_case, sphere_case,
+                                          uniform_box_case)
+    return {
+        "sphere_q19_fh": sphere_case(coarse=(32, 16, 16), refine=[((6, 4, 4), (18, 12, 12))], center=(12, 8, 8),
+                                     radius=2.0),
+        "sphere_q27_dw": sphere_case(q=27, ib_method="DW", coarse=(30, 18, 18), refine=[((6, 5, 5), (18, 13, 13))],
+                                     center=(12, 9, 9), radius=2.0),
+        "nested_q27_cumulant_l3": nested_sphere_case(coarse=(64, 32, 32), max_level=3, center=(20, 16, 16),
+                                                     radius=2.0, half_widths=(5.0, 3.5, 2.5), re=50.0),
+        "cavity_q19_l2": cavity_case(q=19, coarse=(24, 24, 24), max_level=2, re=100.0),
+        "cavity_q27_l0": cavity_case(q=27, collision="Cumulant", coarse=(16, 16, 16), max_level=0),
+        "df_osc_l2": df_sphere_case(radius=3, max_level=2, re=60.0, oscillating=True, period=100),
+        "df_slack_l1": df_sphere_case(radius=4, max_level=1, re=80.0, band_slack=1.0),
+        "box_periodic_empty": uniform_box_case(q=19, n=(16, 12, 8), empty_levels=1),
+    }
+
+
+CASES = sorted(_cases())
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_generated_sets_match_host_mesher(ctx, name):
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    case = _cases()[name]
+    a = LBM_Manager(ctx, case, schedule="fused")
+    b = LBM_Manager(ctx, case, schedule="fused", generate=True)
+    for l in range(case.max_level + 1):
+        ka, ta = a.keys(l)
+        kb, tb = b.keys(l)
+        assert np.array_equal(ka, kb), (name, l, ka.size, kb.size)
+        assert np.array_equal(ta, tb), (name, l, int((ta != tb).sum()))
+        assert np.array_equal(a.neighbors(l), b.neighbors(l)), (name, l)
+    a.fluidSimulate(3)
+    b.fluidSimulate(3)
+    ctx.synchronize()
+    for l in range(case.max_level + 1):
+        fa, ca = a.populations(l)
+        fb, cb = b.populations(l)
+        assert np.array_equal(fa, fb) and np.array_equal(ca, cb), (name, l)
+    assert np.array_equal(a.force(), b.force()), name
+    a.close()
+    b.close()
+
+
+def test_spec_mesh_case_runs_without_host_sets(ctx):
+    """A case made with mesh="device" has no host sets at all and matches
+    the host-mesher build step for step."""
+    from mortontrie_amr_b200.case import df_sphere_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    from mortontrie_amr_b200.mesh import SpecMesh
+    host = df_sphere_case(radius=3, max_level=1, re=50.0, oscillating=True, period=60)
+    dev = df_sphere_case(radius=3, max_level=1, re=50.0, oscillating=True, period=60, mesh="device")
+    assert isinstance(dev.mesh, SpecMesh)
+    a = LBM_Manager(ctx, host, storage="f16", schedule="fused")
+    b = LBM_Manager(ctx, dev, storage="f16", schedule="fused")
+    a.fluidSimulate(4)
+    b.fluidSimulate(4)
+    ctx.synchronize()
+    for l in range(2):
+        assert np.array_equal(a.populations(l)[0], b.populations(l)[0]), l
+    assert np.array_equal(a.force(), b.force())
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("bad", ["box_touches_bc", "box_near_interface", "solid_near_interface",
+                                 "band_near_interface"])
+def test_generated_contract_errors_match_host_mesher(ctx, bad):
+    """The device raises MT_ERR_MESH where the host mesher raises, with the
+    same message."""
+    from mortontrie_amr_b200.case import CaseParams, Case
+    from mortontrie_amr_b200.lbm import LBM_Manager, MTError
+    from mortontrie_amr_b200.mesh import MeshSpec, Sphere, SpecMesh, build_mesh
+    sp = {
+        "box_touches_bc": MeshSpec(q=19, max_level=1, coarse=(16, 16, 16), refine=[((0, 4, 4), (8, 12, 12))],
+                                   boundary=("bc", "bc", "bc")),
+        "box_near_interface": MeshSpec(q=19, max_level=2, coarse=(24, 16, 16),
+                                       refine=[((4, 4, 4), (16, 12, 12)), ((8, 8, 8), (20, 16, 16))],
+                                       boundary=("bc", "periodic", "periodic")),
+        "solid_near_interface": MeshSpec(q=19, max_level=1, coarse=(32, 16, 16), refine=[((6, 4, 4), (18, 12, 12))],
+                                         boundary=("bc", "periodic", "periodic"), sphere=Sphere((12, 8, 8), 3.6)),
+        "band_near_interface": MeshSpec(q=19, max_level=1, coarse=(32, 16, 16), refine=[((6, 4, 4), (18, 12, 12))],
+                                        boundary=("bc", "periodic", "periodic"), sphere=Sphere((12, 8, 8), 2.5),
+                                        ib="markers"),
+    }[bad]
+    with pytest.raises(ValueError) as host_err:
+        build_mesh(sp)
+    ib = "DF" if sp.ib == "markers" else "FH"
+    case = Case(SpecMesh(spec=sp), CaseParams(q=19, ib_method=ib, bc_mode="zouhe_outflow"))
+    with pytest.raises(MTError) as dev_err:
+        LBM_Manager(ctx, case)
+    assert "MT_ERR_MESH" in str(dev_err.value)
+    host_msg = str(host_err.value).split(": ", 1)[-1]
+    assert host_msg in str(dev_err.value), (str(host_err.value), str(dev_err.value))
