@@ -321,7 +321,9 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
     is stated against the FP64 run after the same steps."""
     from mortontrie_amr_b200.case import nested_sphere_case
     from mortontrie_amr_b200.lbm import LBM_Manager
+    t0 = time.time()
     case = nested_sphere_case()
+    host_mesh_s = time.time() - t0
     m = case.mesh
     L = m.spec.max_level
     stepped = [int(m.levels[l]["lat_f"].size + m.levels[l]["overlap_C2F"].size) for l in range(L + 1)]
@@ -368,18 +370,30 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
         out[st]["drag_rel_vs_f64"] = float(abs(r["fx"] - ref["fx"]) / max(abs(ref["fx"]), 1e-300))
         out[st]["mass_drift_vs_f64"] = float(abs(r["rho"].sum() - ref["rho"].sum()) / ref["rho"].sum())
         out[st]["speedup_vs_f64"] = round(res["f64"]["secs"] / r["secs"], 3)
+    # case set-up: the host mesher vs classification on the device (same
+    # sets); one small case first loads the classification kernels
+    LBM_Manager(ctx, nested_sphere_case(coarse=(48, 24, 24), max_level=2, center=(16, 12, 12), radius=2.0,
+                                        half_widths=(4.0, 2.5), mesh="device"), "f16", schedule="fused").close()
+    torch.cuda.synchronize()
+    t0 = time.time()
+    mgr = LBM_Manager(ctx, nested_sphere_case(mesh="device"), "f16", schedule="fused")
+    torch.cuda.synchronize()
+    dev_s = time.time() - t0
+    same = all(np.array_equal(mgr.keys(l)[0], m.all_keys(l)) for l in range(L + 1))
+    mgr.close()
+    out["case_setup_s"] = {"host_mesher": round(host_mesh_s, 2), "device_classification_and_build": round(dev_s, 3),
+                           "same_keys": bool(same)}
     return out
 
 
-def _build_specs(specs):
-    """Host meshes of many cases, built in parallel worker processes (spawned:
-    the parent already holds a CUDA context)."""
-    import multiprocessing as mp
-    from concurrent.futures import ProcessPoolExecutor
-    workers = max(1, min(len(specs), (os.cpu_count() or 2) - 1, 32))
-    from mortontrie_amr_b200.workloads import build_spec
-    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
-        return list(ex.map(build_spec, specs))
+def _stepped_updates(mgr):
+    """Cell updates of one coarse step: the stepped cells (lat_f and C2F
+    tags) of every level times its 2^l substeps, read from the device build."""
+    total = 0
+    for l in range(mgr.L + 1):
+        _, tags = mgr.keys(l)
+        total += int(np.count_nonzero(tags & 5)) << l
+    return total
 
 
 def batched_section(ctx, torch, steps=20, warmup=2, solve_steps=2000, n_cases=64, seed=4):
@@ -395,15 +409,9 @@ def batched_section(ctx, torch, steps=20, warmup=2, solve_steps=2000, n_cases=64
     from mortontrie_amr_b200.lbm import Batch, LBM_Manager, drag_coefficient
     from mortontrie_amr_b200.workloads import batched_uneven_cases
     specs = batched_uneven_cases(seed, n_cases)
-    t0 = time.time()
-    cases = _build_specs(specs)
-    build_s = time.time() - t0
+    # meshes classified on the device when each case is created
+    cases = [s.build(mesh="device") for s in specs]
     stream = torch.cuda.current_stream()
-    upd = []
-    for c in cases:
-        m = c.mesh
-        L = m.spec.max_level
-        upd.append(sum((int(m.levels[l]["lat_f"].size + m.levels[l]["overlap_C2F"].size) << l) for l in range(L + 1)))
     total_steps = warmup + steps
 
     def timed(fn, k):
@@ -418,6 +426,10 @@ def batched_section(ctx, torch, steps=20, warmup=2, solve_steps=2000, n_cases=64
     # batched, FP16
     t0 = time.time()
     members = [LBM_Manager(ctx, c, "f16", schedule="fused", scaling="standard") for c in cases]
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    upd = [_stepped_updates(m) for m in members]
+    t0 = time.time()
     batch = Batch(ctx, members)
     batch.step(warmup)
     torch.cuda.synchronize()
@@ -455,7 +467,7 @@ def batched_section(ctx, torch, steps=20, warmup=2, solve_steps=2000, n_cases=64
     return {
         "workload": f"{len(cases)} seeded cases (seed {seed}): cavity/sphere, 32^3..128x64x64, 1-3 levels, "
                     "Re 10-200, D3Q19 LBGK / D3Q27 cumulant, stress-continuous interface factors",
-        "cell_updates_per_coarse_step": int(sum(upd)), "host_mesh_build_s": round(build_s, 1),
+        "cell_updates_per_coarse_step": int(sum(upd)), "device_mesh_build_s": round(build_s, 2),
         "batch_setup_s": round(setup_b, 2), "coarse_steps_timed": steps, "solve_coarse_steps": solve_steps,
         "batched_f16": {"ms_per_coarse_step_all_cases": round(1e3 * tb, 3),
                         "cases_per_hour": round(len(cases) * 3600.0 / solve_b, 1),

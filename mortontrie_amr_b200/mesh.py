@@ -76,6 +76,9 @@ class MeshSpec:
     # extra inner depth of the forcing band in coarse cells, so that one mesh
     # serves marker spheres of radius in [radius - band_slack, radius]
     band_slack: float = 0.0
+    # closed triangulated solid surface (n, 3, 3) in coarse-cell units,
+    # voxelised on the finest level instead of a sphere (links mode)
+    surface: Optional[np.ndarray] = None
 
 
 @dataclass
@@ -147,6 +150,31 @@ def spec_mesh(spec: MeshSpec) -> SpecMesh:
         raise ValueError("need one refinement box per level below the maximum level")
     mk = sphere_markers(spec) if (spec.sphere is not None and spec.ib == "markers") else None
     return SpecMesh(spec=spec, markers=mk)
+
+
+def estimate_cells(spec: MeshSpec) -> list:
+    """Upper bound of the stored cells per level from the boxes alone (no
+    classification): the level's box minus the interior under the next
+    refinement box, plus a one-cell layer outside the box (ghost C2F) and
+    outside the refinement box (ghost F2C)."""
+    def vol(lo, hi, g=0):
+        return int(np.prod([max(0, h - l + 2 * g) for l, h in zip(lo, hi)]))
+    out = []
+    lo, hi = (0, 0, 0), tuple(spec.coarse)
+    for l in range(spec.max_level + 1):
+        if vol(lo, hi) == 0:
+            out.append(0)
+            continue
+        n = vol(lo, hi) + (vol(lo, hi, 1) - vol(lo, hi) if l > 0 else 0)
+        box = spec.refine[l] if l < spec.max_level else None
+        if box is not None:
+            n -= vol(box[0], box[1], -1)
+            n += vol(box[0], box[1], 1) - vol(box[0], box[1])
+            lo, hi = tuple(2 * v for v in box[0]), tuple(2 * v for v in box[1])
+        else:
+            lo, hi = (0, 0, 0), (0, 0, 0)
+        out.append(n)
+    return out
 
 
 def _grid(lo, hi):
@@ -274,6 +302,12 @@ def build_mesh(spec: MeshSpec) -> Mesh:
             m = 2.7
             band = (dmin <= r + m) & (dmax >= r - m - spec.band_slack * s)
             sets["ib_band"] = _sorted_unique(cell_key(L, l, fx[band], fy[band], fz[band]))
+        elif l == L and spec.surface is not None:
+            if L == 0:
+                raise ValueError("the solid boundary is only applied on a refined finest level")
+            solid = surface_inside(np.asarray(spec.surface, np.float64) * float(1 << L), fx, fy, fz)
+            sets["lat_sf"] = _sorted_unique(cell_key(L, l, fx[solid], fy[solid], fz[solid]))
+            fx, fy, fz = fx[~solid], fy[~solid], fz[~solid]
         elif l == L and spec.sphere is not None:
             if L == 0:
                 raise ValueError("the solid boundary is only applied on a refined finest level")
@@ -330,8 +364,12 @@ def build_mesh(spec: MeshSpec) -> Mesh:
             if np.any(_in_sorted(k, levels[L]["overlap_C2F"])):
                 raise ValueError("the forcing band is too close to the coarse/fine interface")
         markers = sphere_markers(spec)
-    elif spec.sphere is not None:
-        dis_keys, dis_rows = _sphere_links(spec, levels[L]["lat_f"])
+    elif spec.sphere is not None or spec.surface is not None:
+        if spec.surface is not None:
+            dis_keys, dis_rows = surface_links(np.asarray(spec.surface, np.float64) * float(1 << L), q,
+                                               levels[L]["lat_f"], L)
+        else:
+            dis_keys, dis_rows = _sphere_links(spec, levels[L]["lat_f"])
         sf_keys = levels[L]["lat_sf"]
         # IB cells must be plain lat_f cells; the solid must stay clear of C2F.
         sx, sy, sz = _coords_of(sf_keys, L, L)
@@ -341,6 +379,156 @@ def build_mesh(spec: MeshSpec) -> Mesh:
                 raise ValueError("solid too close to the coarse/fine interface")
     return Mesh(spec=spec, levels=levels, lat_bc=lat_bc, dis_keys=dis_keys, dis_rows=dis_rows,
                 extent=extents, markers=markers)
+
+
+def _edge_orient(u, v, py, pz):
+    """Orientation of (py, pz) against the directed edge u -> v in the (y, z)
+    plane, evaluated with the endpoints in lexicographic order and negated
+    when swapped, so that the two traversals of an edge give exactly
+    opposite values."""
+    swap = (u[0] > v[0]) | ((u[0] == v[0]) & (u[1] > v[1]))
+    P0 = np.where(swap, v[0], u[0]), np.where(swap, v[1], u[1])
+    R0 = np.where(swap, u[0], v[0]), np.where(swap, u[1], v[1])
+    o = (R0[0] - P0[0]) * (pz - P0[1]) - (R0[1] - P0[1]) * (py - P0[0])
+    return np.where(swap, -o, o)
+
+
+def column_crossings(tri, ys, zs):
+    """Crossings of the lines {(t, ys + 0.5, zs + 0.5)} with one triangle
+    (finest-cell units): (inside mask, x of the crossing).  The projected
+    triangle is taken counter-clockwise in (y, z); a line through an edge or
+    a vertex belongs to the triangle when the edge is a top or left edge
+    (z decreasing, or z constant and y decreasing along the counter-clockwise
+    traversal), so a line through a shared edge crosses exactly one of two
+    adjacent triangles and touches a silhouette edge zero or two times."""
+    a, b, c = tri[0], tri[1], tri[2]
+    area = (b[1] - a[1]) * (c[2] - a[2]) - (b[2] - a[2]) * (c[1] - a[1])
+    py, pz = ys + 0.5, zs + 0.5
+    if area == 0.0:
+        return np.zeros(py.shape, bool), np.zeros(py.shape)
+    verts = (a, b, c) if area > 0.0 else (a, c, b)
+    inside = np.ones(py.shape, bool)
+    for i in range(3):
+        u, v = verts[i], verts[(i + 1) % 3]
+        o = _edge_orient((u[1], u[2]), (v[1], v[2]), py, pz)
+        dy, dz = v[1] - u[1], v[2] - u[2]
+        top_left = (dz < 0.0) or (dz == 0.0 and dy < 0.0)
+        inside &= (o > 0.0) | ((o == 0.0) & top_left)
+    ny = (b[2] - a[2]) * (c[0] - a[0]) - (b[0] - a[0]) * (c[2] - a[2])
+    nz = (b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0])
+    x = a[0] - (ny * (py - a[1]) + nz * (pz - a[2])) / area
+    return inside, x
+
+
+def _tri_columns(tri):
+    """Finest-level (y, z) columns whose centre lines may cross the triangle."""
+    lo, hi = tri.min(axis=0), tri.max(axis=0)
+    y0, y1 = int(np.ceil(lo[1] - 0.5)), int(np.floor(hi[1] - 0.5))
+    z0, z1 = int(np.ceil(lo[2] - 0.5)), int(np.floor(hi[2] - 0.5))
+    return y0, y1, z0, z1
+
+
+def surface_inside(tris, fx, fy, fz):
+    """Cells whose centre lies inside the closed surface (finest-cell units):
+    an odd number of crossings of the +x ray from the centre (crossing x
+    strictly above the centre's x)."""
+    fx, fy, fz = (np.asarray(v, np.int64) for v in (fx, fy, fz))
+    cols = {}
+    for tri in tris:
+        y0, y1, z0, z1 = _tri_columns(tri)
+        if y1 < y0 or z1 < z0:
+            continue
+        Y, Z = np.meshgrid(np.arange(y0, y1 + 1), np.arange(z0, z1 + 1), indexing="ij")
+        ins, x = column_crossings(tri, Y.ravel().astype(np.float64), Z.ravel().astype(np.float64))
+        for yy, zz, xx in zip(Y.ravel()[ins].tolist(), Z.ravel()[ins].tolist(), x[ins].tolist()):
+            cols.setdefault((yy, zz), []).append(xx)
+    solid = np.zeros(fx.size, bool)
+    if not cols:
+        return solid
+    key = fy * (1 << 21) + fz
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    for (yy, zz), xs in cols.items():
+        k = yy * (1 << 21) + zz
+        i0, i1 = np.searchsorted(ks, k, "left"), np.searchsorted(ks, k, "right")
+        if i0 == i1:
+            continue
+        idx = order[i0:i1]
+        xs = np.sort(np.array(xs))
+        above = xs.size - np.searchsorted(xs, fx[idx] + 0.5, "right")
+        solid[idx] = (above & 1) == 1
+    return solid
+
+
+LINK_EPS = 1e-10
+
+
+def link_hits(tri, px, py, pz, q):
+    """Normalised wall distance of the links of cells with centres (px, py,
+    pz) across one triangle (ComplexBoundary's dis convention: 0 at the cell
+    centre, 1 at the neighbour's), -1 where the link misses it.  The
+    intersection is Shape::intersect_line_with_triangle (Shape.cpp:809-843:
+    Moller-Trumbore on the unit link direction, the crossing point rebuilt
+    from its barycentric coordinates and measured from the centre) and the
+    [0, 1] filter of Lat_Manager::compute_distance (Lat_Voxelize.cpp
+    :1252-1285); the barycentric bounds include the edges (>= -1e-10) so that
+    a link through an edge shared by two triangles is not missed."""
+    ex, ey, ez, _ = directions(q)
+    v1, v2, v3 = tri[0], tri[1], tri[2]
+    e1 = (v2[0] - v1[0], v2[1] - v1[1], v2[2] - v1[2])
+    e2 = (v3[0] - v1[0], v3[1] - v1[1], v3[2] - v1[2])
+    sx, sy, sz = px - v1[0], py - v1[1], pz - v1[2]
+    out = np.full((px.size, q - 1), -1.0)
+    for k in range(1, q):
+        gx, gy, gz = float(ex[k]), float(ey[k]), float(ez[k])
+        mag = np.sqrt(gx * gx + gy * gy + gz * gz)
+        dx, dy, dz = gx / mag, gy / mag, gz / mag
+        s1 = (dy * e2[2] - dz * e2[1], dz * e2[0] - dx * e2[2], dx * e2[1] - dy * e2[0])
+        s2 = (sy * e1[2] - sz * e1[1], sz * e1[0] - sx * e1[2], sx * e1[1] - sy * e1[0])
+        s1e1 = s1[0] * e1[0] + s1[1] * e1[1] + s1[2] * e1[2]
+        if s1e1 == 0.0:
+            continue
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t = (s2[0] * e2[0] + s2[1] * e2[1] + s2[2] * e2[2]) / s1e1
+            b1 = (s1[0] * sx + s1[1] * sy + s1[2] * sz) / s1e1
+            b2 = (s2[0] * dx + s2[1] * dy + s2[2] * dz) / s1e1
+        b0 = 1.0 - b1 - b2
+        ok = (t >= LINK_EPS) & (b1 >= -LINK_EPS) & (b2 >= -LINK_EPS) & (b0 >= -LINK_EPS)
+        ix = b0 * v1[0] + b1 * v2[0] + b2 * v3[0]
+        iy = b0 * v1[1] + b1 * v2[1] + b2 * v3[1]
+        iz = b0 * v1[2] + b1 * v2[2] + b2 * v3[2]
+        dist = np.sqrt((ix - px) * (ix - px) + (iy - py) * (iy - py) + (iz - pz) * (iz - pz))
+        nrm = dist / mag
+        ok &= (nrm >= 0.0) & (nrm <= 1.0)
+        out[ok, k - 1] = nrm[ok]
+    return out
+
+
+def surface_links(tris, q, fluid_keys, L):
+    """dis rows of the finest fluid cells whose links cross the surface: per
+    link the smallest normalised distance over the triangles."""
+    x, y, z = _coords_of(fluid_keys, L, L)
+    rows = np.full((x.size, q - 1), -1.0)
+    key = (x * (1 << 21) + y) * (1 << 21) + z
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    for tri in tris:
+        lo, hi = tri.min(axis=0), tri.max(axis=0)
+        rng = [np.arange(int(np.ceil(lo[a] - 1.5)), int(np.floor(hi[a] + 0.5)) + 1) for a in range(3)]
+        X, Y, Z = np.meshgrid(*rng, indexing="ij")
+        ck = (X.ravel() * (1 << 21) + Y.ravel()) * (1 << 21) + Z.ravel()
+        pos = np.searchsorted(ks, ck)
+        pos = np.minimum(pos, max(ks.size - 1, 0))
+        hit = ks[pos] == ck if ks.size else np.zeros(ck.size, bool)
+        idx = order[pos[hit]]
+        if idx.size == 0:
+            continue
+        d = link_hits(tri, x[idx] + 0.5, y[idx] + 0.5, z[idx] + 0.5, q)
+        cur = rows[idx]
+        better = (d != -1.0) & ((cur == -1.0) | (d < cur))
+        rows[idx] = np.where(better, d, cur)
+    has = np.any(rows != -1.0, axis=1)
+    return fluid_keys[has].copy(), rows[has].copy()
 
 
 def _coords_of(keys, L, l):

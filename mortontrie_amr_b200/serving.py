@@ -12,10 +12,13 @@ The server keeps every admitted case resident on the device and steps all
 of them together in one batch (mt_batch_*): a request that arrives while
 others are running is admitted as soon as the HBM budget allows and joins
 the batch at the next chunk boundary; a finished case leaves it and frees
-its memory.  Host meshes come from a cache of templates keyed by the grid
-radius ceil(R), the level count and whether the sphere oscillates (the
-forcing band of a template covers any radius in [ceil(R) - 1, ceil(R)]);
-the markers are made per request for its exact radius.
+its memory.  Meshes come from templates keyed by the grid radius ceil(R),
+the level count and whether the sphere oscillates (domain and refinement
+boxes).  By default the lattice is classified on the device per request
+(mt_case_generate, tens of milliseconds), with the forcing band fitted to the
+request's exact radius and amplitude; with host meshes the template's band
+covers any radius in [ceil(R) - 1, ceil(R)] and the cache keeps the sets.
+The markers are made per request for its exact radius.
 """
 from __future__ import annotations
 
@@ -28,7 +31,7 @@ from typing import Optional
 import numpy as np
 
 from .case import CaseParams, df_sphere_case
-from .mesh import Markers
+from .mesh import Markers, SpecMesh, Sphere, estimate_cells
 
 PERIOD = 2000          # finest steps of one oscillation
 AMPLITUDE = 0.5        # oscillation amplitude in sphere radii
@@ -91,11 +94,16 @@ def template_key(req: Request) -> tuple:
     return (req.grid_radius, req.levels, req.oscillating)
 
 
-def build_template(key: tuple):
-    """Host mesh of a template (picklable for worker processes)."""
+def build_template(key: tuple, mesh: str = "host"):
+    """Mesh of a template: the host mesher's sets ("host", picklable for
+    worker processes) or the spec alone ("device")."""
     r, levels, osc = key
     return df_sphere_case(radius=r, max_level=levels, re=100.0, oscillating=osc, period=PERIOD,
-                          amplitude=AMPLITUDE, band_slack=1.0).mesh
+                          amplitude=AMPLITUDE, band_slack=1.0, mesh=mesh).mesh
+
+
+def _build_host_template(key: tuple):
+    return build_template(key, "host")
 
 
 def request_case(req: Request, mesh):
@@ -124,6 +132,11 @@ def request_case(req: Request, mesh):
     u = U_INLET
     params = CaseParams(q=19, collision="LBGK", ib_method="DF", bc_mode="zouhe_outflow",
                         nu=u * 2.0 * req.radius / req.re, u_bc=(u, 0.0, 0.0), u_ref=u)
+    if isinstance(mesh, SpecMesh):
+        # the band of this request's own sphere and path
+        spec = dataclasses.replace(mesh.spec, sphere=Sphere(mesh.spec.sphere.center, req.radius), band_slack=0.0,
+                                   oscillation=(AMPLITUDE * req.radius, PERIOD) if req.oscillating else None)
+        return Case(SpecMesh(spec=spec, markers=mk), params)
     return Case(dataclasses.replace(mesh, markers=mk), params)
 
 
@@ -133,8 +146,11 @@ def footprint_bytes(case, storage: str) -> int:
     sb = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}[storage]
     q = case.params.q
     total = 0
-    for lv in case.mesh.levels:
-        n = sum(int(v.size) for v in lv.values())
+    if isinstance(case.mesh, SpecMesh):
+        cells = estimate_cells(case.mesh.spec)
+    else:
+        cells = [sum(int(v.size) for v in lv.values()) for lv in case.mesh.levels]
+    for n in cells:
         total += n * (3 * q * sb + 4 * (q - 1) + 4 * 4 + 8 + 4 + 16 + 8 + 20)
     total += int(case.mesh.markers.dv.size) * 80 if case.mesh.markers is not None else 0
     return total + (8 << 20)
@@ -150,30 +166,34 @@ def drag_lift(mgr, req: Request) -> tuple:
 
 
 class TemplateCache:
-    def __init__(self, workers: int = 0):
+    """Templates by key; mesh "device" keeps specs only (the lattice is
+    classified on the device per request), "host" the host mesher's sets."""
+
+    def __init__(self, workers: int = 0, mesh: str = "device"):
         self.meshes = {}
         self.workers = workers
+        self.mesh = mesh
 
     def prepare(self, requests):
-        """Build every template the requests need (in worker processes)."""
+        """Build every template the requests need (host sets in worker processes)."""
         keys = sorted({template_key(r) for r in requests} - set(self.meshes))
         if not keys:
             return
-        if self.workers > 1 and len(keys) > 1:
+        if self.mesh == "host" and self.workers > 1 and len(keys) > 1:
             import multiprocessing as mp
             from concurrent.futures import ProcessPoolExecutor
             with ProcessPoolExecutor(max_workers=min(self.workers, len(keys)),
                                      mp_context=mp.get_context("spawn")) as ex:
-                for k, m in zip(keys, ex.map(build_template, keys)):
+                for k, m in zip(keys, ex.map(_build_host_template, keys)):
                     self.meshes[k] = m
         else:
             for k in keys:
-                self.meshes[k] = build_template(k)
+                self.meshes[k] = build_template(k, self.mesh)
 
     def get(self, req: Request):
         k = template_key(req)
         if k not in self.meshes:
-            self.meshes[k] = build_template(k)
+            self.meshes[k] = build_template(k, self.mesh)
         return self.meshes[k]
 
 

@@ -26,7 +26,7 @@ class CaseSpec:
     q: int
     collision: str
 
-    def build(self) -> Case:
+    def build(self, mesh: str = "host") -> Case:
         if self.kind == "cavity":
             nx, ny, nz = self.coarse
             lo, hi = [2, 2, nz // 2], [nx - 2, ny - 2, nz - 2]
@@ -37,14 +37,14 @@ class CaseSpec:
                 lo = [lo[0] + 2, lo[1] + 2, lo[2] + 2]
                 hi = [hi[0] - 2, hi[1] - 2, hi[2] - 2]
             return cavity_case(q=self.q, collision=self.collision, coarse=self.coarse, max_level=self.levels,
-                               re=self.re, u_lid=0.05, refine=refine)
+                               re=self.re, u_lid=0.05, refine=refine, mesh=mesh)
         nx, ny, nz = self.coarse
         r = max(2, ny // 10)
         hw = (3.0, 2.0, 1.4)[: self.levels]
         cx = max(nx // 4, int(np.ceil(hw[0] * r)) + 2)
         return nested_sphere_case(q=self.q, collision=self.collision, coarse=self.coarse, max_level=self.levels,
                                   center=(cx, ny // 2, nz // 2), radius=float(r), half_widths=hw, u=0.05,
-                                  re=self.re)
+                                  re=self.re, mesh=mesh)
 
     def label(self) -> str:
         return (f"{self.kind} {'x'.join(map(str, self.coarse))} L{self.levels} Re{self.re:.0f} "

@@ -110,3 +110,33 @@ def test_generated_contract_errors_match_host_mesher(ctx, bad):
     assert "MT_ERR_MESH" in str(dev_err.value)
     host_msg = str(host_err.value).split(": ", 1)[-1]
     assert host_msg in str(dev_err.value), (str(host_err.value), str(dev_err.value))
+
+
+def test_flow_output_of_a_stepped_case(ctx, tmp_path):
+    """write_flow writes the device's velocity of every lat_f and F2C cell
+    (tecplot.cpp:16-176 layout) after a few steps."""
+    from mortontrie_amr_b200.case import sphere_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    from mortontrie_amr_b200.tecplot import write_flow
+    case = sphere_case(coarse=(32, 16, 16), refine=[((6, 4, 4), (18, 12, 12))], center=(12, 8, 8), radius=2.0,
+                       mesh="device")
+    mgr = LBM_Manager(ctx, case, storage="f32", schedule="fused")
+    mgr.fluidSimulate(5)
+    ctx.synchronize()
+    path = write_flow(mgr, str(tmp_path), 5, u_scale=2.0)
+    assert path.endswith("sphereFlow_5.000000.dat")
+    lines = open(path).read().splitlines()
+    head = dict(kv.split("=") for kv in lines[2].replace("ZONE, ", "").split(", ")[:2])
+    n, e = int(head["NODES"]), int(head["ELEMENTS"])
+    want = []
+    for l in range(mgr.L + 1):
+        _, tags = mgr.keys(l)
+        _, u = mgr.macros(l)
+        sel = np.concatenate([np.flatnonzero(tags & 1), np.flatnonzero(tags & 2)])
+        want.append(u[:, sel])
+    want = 2.0 * np.concatenate(want, axis=1)
+    assert want.shape[1] == e
+    got = np.array([float(v) for v in lines[3 + 3 * n:3 + 3 * n + 3 * e]]).reshape(3, e)
+    assert np.allclose(got, want, rtol=1e-5, atol=1e-9)
+    assert np.abs(want).max() > 1e-3      # the flow has started
+    mgr.close()

@@ -46,3 +46,34 @@ def test_request_case_on_template():
         for d in np.ndindex(3, 3, 3):
             cells = base + (np.array(d) - 1)[:, None]
             assert all(tuple(x) in band for x in cells.T[::37])
+
+
+def test_device_template_request_case():
+    """With device meshes a request's case is a spec fitted to its own radius
+    and amplitude (band slack 0) on the template's boxes."""
+    from mortontrie_amr_b200.mesh import SpecMesh
+    from mortontrie_amr_b200.serving import Request, TemplateCache, footprint_bytes, request_case
+    req = Request(rid=0, arrival=0.0, radius=3.4, levels=2, re=150.0, oscillating=True)
+    cache = TemplateCache()
+    tmpl = cache.get(req)
+    assert isinstance(tmpl, SpecMesh) and tmpl.spec.sphere.radius == 4.0
+    case = request_case(req, tmpl)
+    assert isinstance(case.mesh, SpecMesh)
+    sp = case.mesh.spec
+    assert sp.sphere.radius == 3.4 and sp.band_slack == 0.0 and sp.oscillation == (0.5 * 3.4, 2000)
+    assert sp.refine == tmpl.spec.refine
+    assert np.allclose(np.linalg.norm(case.mesh.markers.ref, axis=0), 3.4 * 4)
+    assert footprint_bytes(case, "f16") < footprint_bytes(case, "f64")
+
+
+def test_estimated_cells_bound_the_host_mesh():
+    from mortontrie_amr_b200.case import cavity_case, df_sphere_case, nested_sphere_case, sphere_case
+    from mortontrie_amr_b200.mesh import estimate_cells
+    for case in (sphere_case(), df_sphere_case(radius=3, max_level=2, oscillating=True),
+                 cavity_case(coarse=(24, 24, 24), max_level=2),
+                 nested_sphere_case(coarse=(48, 24, 24), max_level=2, center=(16, 12, 12), radius=2.0,
+                                    half_widths=(4.0, 2.5))):
+        est = estimate_cells(case.mesh.spec)
+        got = case.mesh.n_cells()
+        assert all(e >= g for e, g in zip(est, got)), (est, got)
+        assert sum(est) <= 1.3 * sum(got), (est, got)
