@@ -123,7 +123,8 @@ typedef struct mt_mesh_spec {
     int32_t has_refine[MT_MAX_LEVELS];   /* level l < max_level holds a refinement box */
     int64_t refine_lo[MT_MAX_LEVELS][3]; /* the box [lo, hi) in level-l cells */
     int64_t refine_hi[MT_MAX_LEVELS][3];
-    int32_t sphere;                      /* 0 none, 1 solid + wall distances, 2 forcing band (MT_IB_DF) */
+    int32_t sphere;                      /* 0 none, 1 solid + wall distances, 2 forcing band (MT_IB_DF),
+                                            3 the triangulated surface of mt_case_set_surface (solid + wall distances) */
     int32_t pad;
     double center[3];                    /* coarse-cell units from the box corner */
     double radius;                       /* coarse cells */
@@ -131,6 +132,16 @@ typedef struct mt_mesh_spec {
     double band_slack;                   /* extra inner band depth in coarse cells */
 } mt_mesh_spec;
 
+/* Closed triangulated solid surface for mt_case_generate with sphere = 3
+ * (an STL body, Shape::geofile_stl, Shape.cpp:341-470): tri[n][3][3] vertex
+ * coordinates in coarse-cell units.  A finest-level cell is solid when its
+ * centre lies inside (odd number of crossings of the +x line from the centre,
+ * edges shared by two triangles counted once); the wall distance of each
+ * link of a fluid cell is its nearest crossing with a triangle
+ * (Shape::intersect_line_with_triangle, Shape.cpp:809-843, edges included)
+ * normalised by the link length and kept in [0, 1]
+ * (Lat_Manager::compute_distance, Lat_Voxelize.cpp:1252-1285). */
+int mt_case_set_surface(mt_ctx *ctx, int32_t case_id, const double *tri, int64_t n);
 /* generate the case's sets from spec and build it (replaces mt_case_add_set,
  * mt_case_set_dis and mt_case_build); MT_ERR_MESH with the host mesher's
  * messages when the boxes or the sphere break the contract */

@@ -84,6 +84,28 @@ def sphere_case(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1, refine
     return Case(_mesh(spec, mesh), p)
 
 
+def surface_case(surface, q=19, collision="LBGK", coarse=(32, 16, 16), max_level=1, refine=None, ref_length=None,
+                 u=0.05, re=20.0, boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow", ib_method="FH",
+                 stream_convention="reference", mesh="host") -> Case:
+    """Flow past a closed triangulated body (an STL surface, (n, 3, 3) in
+    coarse-cell units), voxelised on the finest level; nu = u * ref_length /
+    Re with ref_length the body's largest extent across the flow (y, z) by
+    default."""
+    surface = np.asarray(surface, np.float64)
+    if refine is None:
+        lo, hi = surface.reshape(-1, 3).min(axis=0), surface.reshape(-1, 3).max(axis=0)
+        refine = [(tuple(int(np.floor(v)) - 3 for v in lo), tuple(int(np.ceil(v)) + 3 for v in hi))]
+    if ref_length is None:
+        ext = surface.reshape(-1, 3).max(axis=0) - surface.reshape(-1, 3).min(axis=0)
+        ref_length = float(max(ext[1], ext[2]))
+    nu = u * ref_length / re
+    spec = MeshSpec(q=q, max_level=max_level, coarse=tuple(coarse), refine=list(refine), boundary=tuple(boundary),
+                    surface=surface)
+    p = CaseParams(q=q, collision=collision, ib_method=ib_method, bc_mode=bc_mode, nu=nu, u_bc=(u, 0.0, 0.0),
+                   u_ref=u, stream_convention=stream_convention)
+    return Case(_mesh(spec, mesh), p)
+
+
 def nested_sphere_case(q=27, collision="Cumulant", coarse=(192, 96, 96), max_level=3, center=(64, 48, 48),
                        radius=6.0, half_widths=(4.0, 2.5, 1.75), u=0.04, re=200.0,
                        boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow", ib_method="FH",

@@ -303,6 +303,20 @@ int mt_case_build(mt_ctx *h, int32_t id)
     return MT_OK;
 }
 
+int mt_case_set_surface(mt_ctx *h, int32_t id, const double *tri, int64_t n)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || c->built) return set_err(ctx, MT_ERR_STATE, "the surface can only be set before the build");
+    if (n < 0 || (n > 0 && !tri) || n > INT32_MAX) return set_err(ctx, MT_ERR_ARG, "bad triangle array");
+    for (int64_t i = 0; i < 9 * n; ++i)
+        if (!std::isfinite(tri[i])) return set_err(ctx, MT_ERR_ARG, "non-finite triangle vertex");
+    c->h_tri.assign(tri, tri + 9 * n);
+    return MT_OK;
+}
+
 int mt_case_generate(mt_ctx *h, int32_t id, const mt_mesh_spec *sp)
 {
     Case *c;
@@ -322,10 +336,12 @@ int mt_case_generate(mt_ctx *h, int32_t id, const mt_mesh_spec *sp)
         if (sp->coarse[a] < 1 || (sp->coarse[a] << L) > (int64_t(1) << 21))
             return set_err(ctx, MT_ERR_ARG, "extent out of the 21-bit Morton range");
     }
-    if (sp->sphere < 0 || sp->sphere > 2) return set_err(ctx, MT_ERR_ARG, "sphere must be 0, 1 or 2");
+    if (sp->sphere < 0 || sp->sphere > 3) return set_err(ctx, MT_ERR_ARG, "sphere must be 0, 1, 2 or 3");
     if (sp->sphere == 2 && c->d.ib_method != MT_IB_DF)
         return set_err(ctx, MT_ERR_ARG, "a forcing band needs ib_method MT_IB_DF");
-    if (sp->sphere && !(sp->radius > 0.0)) return set_err(ctx, MT_ERR_ARG, "sphere radius must be positive");
+    if ((sp->sphere == 1 || sp->sphere == 2) && !(sp->radius > 0.0))
+        return set_err(ctx, MT_ERR_ARG, "sphere radius must be positive");
+    if (sp->sphere == 3 && c->h_tri.empty()) return set_err(ctx, MT_ERR_STATE, "no surface set (mt_case_set_surface)");
     {
         int64_t lo[3] = {0, 0, 0}, hi[3] = {sp->coarse[0], sp->coarse[1], sp->coarse[2]};
         for (int l = 0; l < L; ++l) {

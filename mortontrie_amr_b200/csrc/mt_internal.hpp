@@ -126,6 +126,7 @@ struct Case {
     std::vector<uint64_t> h_dis_key;
     std::vector<double> h_dis;
     bool dis_on_device = false;  // dis_key / dis generated on the device (ndis set)
+    std::vector<double> h_tri;   // solid surface triangles [n][3][3], coarse-cell units (mt_case_set_surface)
     double *ib_force = nullptr;  // [3 * nib] per-cell force of the last treat()
     double *force_acc = nullptr; // [4] fx, fy, fz, treat count
     int *dev_err = nullptr;

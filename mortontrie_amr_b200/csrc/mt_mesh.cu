@@ -39,9 +39,14 @@ struct LevelGen {
     Box dom;         // cells of this level
     int has_ref;     // refinement box of this level present
     Box ref;         // in this level's cells
-    int sphere;      // 0 none, 1 solid + links, 2 band (finest level only)
+    int sphere;      // 0 none, 1 solid + links, 2 band, 3 triangulated surface (finest level only)
     double cx, cy, cz, r, amp, slack;  // finest-level units
     int8_t side_bc[27];                // lat_bc index of a (-1, 0, 1)^3 side combination
+    // surface: crossings of the +x centre lines with the triangles, per
+    // finest (y, z) column over the finest box (CSR)
+    const int32_t *col_off;
+    const double *col_x;
+    int64_t col_lo[2], col_n[2];
 };
 
 MT_HD uint64_t level_key(int L, int l, int64_t x, int64_t y, int64_t z)
@@ -95,6 +100,15 @@ __global__ void k_classify(LevelGen g, uint64_t *key, uint32_t *pay, int *err)
         const double px = (double)x + 0.5 - g.cx, py = (double)y + 0.5 - g.cy, pz = (double)z + 0.5 - g.cz;
         if (g.sphere == 1) {
             if (px * px + py * py + pz * pz < g.r * g.r) p = P_SF;
+        } else if (g.sphere == 3) {
+            const int64_t cy = y - g.col_lo[0], cz = z - g.col_lo[1];
+            if (cy >= 0 && cy < g.col_n[0] && cz >= 0 && cz < g.col_n[1]) {
+                const int64_t col = cy * g.col_n[1] + cz;
+                const double xc = (double)x + 0.5;
+                int above = 0;
+                for (int32_t k = g.col_off[col]; k < g.col_off[col + 1]; ++k) above += g.col_x[k] > xc;
+                if (above & 1) p = P_SF;
+            }
         } else {
             const double qy = fmin(fmax(py, -g.amp), g.amp);
             const double dmin = sqrt(px * px + (py - qy) * (py - qy) + pz * pz);
@@ -216,6 +230,168 @@ __global__ void k_fill_u8(uint8_t *p, int64_t n, uint8_t v)
     if (t < n) p[t] = v;
 }
 
+// ---- triangulated surfaces (mesh.py column_crossings / link_hits, same
+// operation order) -------------------------------------------------------
+struct Tri {
+    double v[3][3];
+};
+
+MT_HD double edge_orient(double uy, double uz, double vy, double vz, double py, double pz)
+{
+    const bool swap = (uy > vy) || (uy == vy && uz > vz);
+    const double Py = swap ? vy : uy, Pz = swap ? vz : uz, Ry = swap ? uy : vy, Rz = swap ? uz : vz;
+    const double o = (Ry - Py) * (pz - Pz) - (Rz - Pz) * (py - Py);
+    return swap ? -o : o;
+}
+
+// crossing of the line {(t, py, pz)} with the triangle: x, or false
+MT_HD bool column_crossing(const Tri &t, double py, double pz, double *x)
+{
+    const double *a = t.v[0], *b = t.v[1], *c = t.v[2];
+    const double area = (b[1] - a[1]) * (c[2] - a[2]) - (b[2] - a[2]) * (c[1] - a[1]);
+    if (area == 0.0) return false;
+    const double *vs[3] = {a, area > 0.0 ? b : c, area > 0.0 ? c : b};
+    for (int i = 0; i < 3; ++i) {
+        const double *u = vs[i], *v = vs[(i + 1) % 3];
+        const double o = edge_orient(u[1], u[2], v[1], v[2], py, pz);
+        const double dy = v[1] - u[1], dz = v[2] - u[2];
+        const bool top_left = (dz < 0.0) || (dz == 0.0 && dy < 0.0);
+        if (!(o > 0.0 || (o == 0.0 && top_left))) return false;
+    }
+    const double ny = (b[2] - a[2]) * (c[0] - a[0]) - (b[0] - a[0]) * (c[2] - a[2]);
+    const double nz = (b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0]);
+    *x = a[0] - (ny * (py - a[1]) + nz * (pz - a[2])) / area;
+    return true;
+}
+
+struct ColRange {
+    int64_t y0, y1, z0, z1;  // inclusive, clipped to the columns
+};
+MT_HD ColRange tri_columns(const Tri &t, const int64_t lo[2], const int64_t n[2])
+{
+    double ylo = fmin(fmin(t.v[0][1], t.v[1][1]), t.v[2][1]), yhi = fmax(fmax(t.v[0][1], t.v[1][1]), t.v[2][1]);
+    double zlo = fmin(fmin(t.v[0][2], t.v[1][2]), t.v[2][2]), zhi = fmax(fmax(t.v[0][2], t.v[1][2]), t.v[2][2]);
+    ColRange r;
+    r.y0 = (int64_t)ceil(ylo - 0.5);
+    r.y1 = (int64_t)floor(yhi - 0.5);
+    r.z0 = (int64_t)ceil(zlo - 0.5);
+    r.z1 = (int64_t)floor(zhi - 0.5);
+    r.y0 = r.y0 > lo[0] ? r.y0 : lo[0];
+    r.z0 = r.z0 > lo[1] ? r.z0 : lo[1];
+    r.y1 = r.y1 < lo[0] + n[0] - 1 ? r.y1 : lo[0] + n[0] - 1;
+    r.z1 = r.z1 < lo[1] + n[1] - 1 ? r.z1 : lo[1] + n[1] - 1;
+    return r;
+}
+
+// pass 0: count the crossings per column; pass 1: write their x
+__global__ void k_tri_columns(const Tri *tri, int64_t ntri, LevelGen g, int pass, int32_t *cnt, int32_t *cursor,
+                              double *col_x)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= ntri) return;
+    const Tri t = tri[i];
+    const ColRange r = tri_columns(t, g.col_lo, g.col_n);
+    for (int64_t y = r.y0; y <= r.y1; ++y)
+        for (int64_t z = r.z0; z <= r.z1; ++z) {
+            double x;
+            if (!column_crossing(t, (double)y + 0.5, (double)z + 0.5, &x)) continue;
+            const int64_t col = (y - g.col_lo[0]) * g.col_n[1] + (z - g.col_lo[1]);
+            if (pass == 0)
+                atomicAdd(&cnt[col], 1);
+            else
+                col_x[atomicAdd(&cursor[col], 1)] = x;
+        }
+}
+
+struct BinBox {
+    int64_t lo[3], n[3];
+};
+// finest cells whose links can reach the triangle: [ceil(lo - 1.5), floor(hi + 0.5)] per axis, clipped
+MT_HD void tri_bins(const Tri &t, const BinBox &b, int64_t r0[3], int64_t r1[3])
+{
+    for (int a = 0; a < 3; ++a) {
+        const double lo = fmin(fmin(t.v[0][a], t.v[1][a]), t.v[2][a]);
+        const double hi = fmax(fmax(t.v[0][a], t.v[1][a]), t.v[2][a]);
+        int64_t u0 = (int64_t)ceil(lo - 1.5), u1 = (int64_t)floor(hi + 0.5);
+        r0[a] = u0 > b.lo[a] ? u0 : b.lo[a];
+        r1[a] = u1 < b.lo[a] + b.n[a] - 1 ? u1 : b.lo[a] + b.n[a] - 1;
+    }
+}
+
+__global__ void k_tri_bins(const Tri *tri, int64_t ntri, BinBox b, int pass, int32_t *cnt, int32_t *cursor,
+                           int32_t *bin_tri)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= ntri) return;
+    int64_t r0[3], r1[3];
+    tri_bins(tri[i], b, r0, r1);
+    for (int64_t x = r0[0]; x <= r1[0]; ++x)
+        for (int64_t y = r0[1]; y <= r1[1]; ++y)
+            for (int64_t z = r0[2]; z <= r1[2]; ++z) {
+                const int64_t cell = ((x - b.lo[0]) * b.n[1] + (y - b.lo[1])) * b.n[2] + (z - b.lo[2]);
+                if (pass == 0)
+                    atomicAdd(&cnt[cell], 1);
+                else
+                    bin_tri[atomicAdd(&cursor[cell], 1)] = (int32_t)i;
+            }
+}
+
+constexpr double kLinkEps = 1e-10;
+
+// wall distances of the finest fluid cells against the surface's triangles
+// (smallest normalised distance per link); hit[j] = 1 when any link crosses
+template <int Q>
+__global__ void k_links_surface(const uint64_t *keys, int64_t n, const Tri *tri, BinBox b, const int32_t *bin_off,
+                                const int32_t *bin_tri, double *rows, uint8_t *hit)
+{
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint64_t key = keys[j];
+    const int64_t c[3] = {(int64_t)compact3(key), (int64_t)compact3(key >> 1), (int64_t)compact3(key >> 2)};
+    double best[Q - 1];
+    for (int k = 0; k < Q - 1; ++k) best[k] = -1.0;
+    bool inbox = true;
+    for (int a = 0; a < 3; ++a) inbox &= c[a] >= b.lo[a] && c[a] < b.lo[a] + b.n[a];
+    if (inbox) {
+        const int64_t cell = ((c[0] - b.lo[0]) * b.n[1] + (c[1] - b.lo[1])) * b.n[2] + (c[2] - b.lo[2]);
+        const double px = (double)c[0] + 0.5, py = (double)c[1] + 0.5, pz = (double)c[2] + 0.5;
+        for (int32_t e = bin_off[cell]; e < bin_off[cell + 1]; ++e) {
+            const Tri t = tri[bin_tri[e]];
+            const double *v1 = t.v[0], *v2 = t.v[1], *v3 = t.v[2];
+            const double e1[3] = {v2[0] - v1[0], v2[1] - v1[1], v2[2] - v1[2]};
+            const double e2[3] = {v3[0] - v1[0], v3[1] - v1[1], v3[2] - v1[2]};
+            const double sx = px - v1[0], sy = py - v1[1], sz = pz - v1[2];
+            for (int k = 1; k < Q; ++k) {
+                const double gx = (double)ex(k), gy = (double)ey(k), gz = (double)ez(k);
+                const double mag = sqrt(gx * gx + gy * gy + gz * gz);
+                const double dx = gx / mag, dy = gy / mag, dz = gz / mag;
+                const double s1[3] = {dy * e2[2] - dz * e2[1], dz * e2[0] - dx * e2[2], dx * e2[1] - dy * e2[0]};
+                const double s2[3] = {sy * e1[2] - sz * e1[1], sz * e1[0] - sx * e1[2], sx * e1[1] - sy * e1[0]};
+                const double s1e1 = s1[0] * e1[0] + s1[1] * e1[1] + s1[2] * e1[2];
+                if (s1e1 == 0.0) continue;
+                const double tt = (s2[0] * e2[0] + s2[1] * e2[1] + s2[2] * e2[2]) / s1e1;
+                const double b1 = (s1[0] * sx + s1[1] * sy + s1[2] * sz) / s1e1;
+                const double b2 = (s2[0] * dx + s2[1] * dy + s2[2] * dz) / s1e1;
+                const double b0 = 1.0 - b1 - b2;
+                if (!(tt >= kLinkEps && b1 >= -kLinkEps && b2 >= -kLinkEps && b0 >= -kLinkEps)) continue;
+                const double ix = b0 * v1[0] + b1 * v2[0] + b2 * v3[0];
+                const double iy = b0 * v1[1] + b1 * v2[1] + b2 * v3[1];
+                const double iz = b0 * v1[2] + b1 * v2[2] + b2 * v3[2];
+                const double dist = sqrt((ix - px) * (ix - px) + (iy - py) * (iy - py) + (iz - pz) * (iz - pz));
+                const double nrm = dist / mag;
+                if (!(nrm >= 0.0 && nrm <= 1.0)) continue;
+                if (best[k - 1] == -1.0 || nrm < best[k - 1]) best[k - 1] = nrm;
+            }
+        }
+    }
+    bool any = false;
+    for (int k = 0; k < Q - 1; ++k) {
+        rows[j * (Q - 1) + k] = best[k];
+        any |= best[k] != -1.0;
+    }
+    hit[j] = any ? 1 : 0;
+}
+
 // device buffer with stream-ordered allocation and release
 template <class T> struct DBuf {
     T *p = nullptr;
@@ -318,6 +494,128 @@ int set_keys(Ctx &ctx, const uint64_t *skey, const uint32_t *spay, int64_t ns, i
     return select_flagged(ctx, skey, flag.p, ns, out);
 }
 
+// the surface's tables on the device: triangles in finest-cell units, the
+// column crossings (CSR over the finest box's (y, z) columns) and the link
+// bins (CSR of triangle indices per finest cell of the bin box)
+struct SurfaceTables {
+    DBuf<Tri> tri;
+    DBuf<int32_t> col_off, bin_off, bin_tri;
+    DBuf<double> col_x;
+    int64_t col_lo[2] = {0, 0}, col_n[2] = {0, 0};
+    BinBox box{};
+};
+
+int csr_offsets(Ctx &ctx, DBuf<int32_t> &cnt, int64_t n, DBuf<int32_t> &off, int64_t *total)
+{
+    if (int rc = off.alloc(ctx, n + 1)) return rc;
+    size_t tb = 0;
+    MT_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.p, off.p, (int)(n + 1), ctx.stream));
+    DBuf<char> tmp;
+    if (int rc = tmp.alloc(ctx, (int64_t)tb)) return rc;
+    MT_CUDA(ctx, cub::DeviceScan::ExclusiveSum(tmp.p, tb, cnt.p, off.p, (int)(n + 1), ctx.stream));
+    int32_t h = 0;
+    MT_CUDA(ctx, cudaMemcpyAsync(&h, off.p + n, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    *total = h;
+    return MT_OK;
+}
+
+int surface_tables(Ctx &ctx, const std::vector<double> &h_tri, int L, const Box &fdom, SurfaceTables &st)
+{
+    const int64_t nt = (int64_t)h_tri.size() / 9;
+    std::vector<Tri> tris((size_t)nt);
+    const double sc = (double)(1 << L);
+    for (int64_t i = 0; i < nt; ++i)
+        for (int v = 0; v < 3; ++v)
+            for (int a = 0; a < 3; ++a) tris[(size_t)i].v[v][a] = h_tri[(size_t)(9 * i + 3 * v + a)] * sc;
+    if (int rc = st.tri.alloc(ctx, nt)) return rc;
+    MT_CUDA(ctx, cudaMemcpyAsync(st.tri.p, tris.data(), sizeof(Tri) * nt, cudaMemcpyHostToDevice, ctx.stream));
+    // columns of the finest box; entries bounded on the host before the int32 offsets
+    st.col_lo[0] = fdom.lo[1];
+    st.col_lo[1] = fdom.lo[2];
+    st.col_n[0] = std::max<int64_t>(0, fdom.hi[1] - fdom.lo[1]);
+    st.col_n[1] = std::max<int64_t>(0, fdom.hi[2] - fdom.lo[2]);
+    int64_t col_bound = 0, bin_bound = 0;
+    int64_t blo[3] = {INT64_MAX, INT64_MAX, INT64_MAX}, bhi[3] = {INT64_MIN, INT64_MIN, INT64_MIN};
+    for (const Tri &t : tris) {
+        const ColRange r = tri_columns(t, st.col_lo, st.col_n);
+        if (r.y1 >= r.y0 && r.z1 >= r.z0) col_bound += (r.y1 - r.y0 + 1) * (r.z1 - r.z0 + 1);
+        for (int a = 0; a < 3; ++a) {
+            const double lo = std::fmin(std::fmin(t.v[0][a], t.v[1][a]), t.v[2][a]);
+            const double hi = std::fmax(std::fmax(t.v[0][a], t.v[1][a]), t.v[2][a]);
+            blo[a] = std::min<int64_t>(blo[a], (int64_t)std::ceil(lo - 1.5));
+            bhi[a] = std::max<int64_t>(bhi[a], (int64_t)std::floor(hi + 0.5));
+        }
+    }
+    bool empty = nt == 0;
+    for (int a = 0; a < 3; ++a) {
+        blo[a] = std::max(blo[a], fdom.lo[a]);
+        bhi[a] = std::min(bhi[a], fdom.hi[a] - 1);
+        empty |= bhi[a] < blo[a];
+    }
+    for (int a = 0; a < 3; ++a) {
+        st.box.lo[a] = empty ? 0 : blo[a];
+        st.box.n[a] = empty ? 0 : bhi[a] - blo[a] + 1;
+    }
+    if (!empty)
+        for (const Tri &t : tris) {
+            int64_t r0[3], r1[3];
+            tri_bins(t, st.box, r0, r1);
+            int64_t v = 1;
+            for (int a = 0; a < 3; ++a) v *= std::max<int64_t>(0, r1[a] - r0[a] + 1);
+            bin_bound += v;
+        }
+    const int64_t ncol = st.col_n[0] * st.col_n[1];
+    const int64_t nbin = st.box.n[0] * st.box.n[1] * st.box.n[2];
+    if (col_bound > INT32_MAX || bin_bound > INT32_MAX || ncol > INT32_MAX - 1 || nbin > INT32_MAX - 1)
+        return set_err(ctx, MT_ERR_ARG, "surface too large for the crossing and link tables");
+    LevelGen g{};
+    g.col_lo[0] = st.col_lo[0];
+    g.col_lo[1] = st.col_lo[1];
+    g.col_n[0] = st.col_n[0];
+    g.col_n[1] = st.col_n[1];
+    {
+        DBuf<int32_t> cnt, cur;
+        if (int rc = cnt.alloc(ctx, ncol + 1)) return rc;
+        MT_CUDA(ctx, cudaMemsetAsync(cnt.p, 0, sizeof(int32_t) * (ncol + 1), ctx.stream));
+        if (nt && ncol) {
+            k_tri_columns<<<grid_for(nt, 128), 128, 0, ctx.stream>>>(st.tri.p, nt, g, 0, cnt.p, nullptr, nullptr);
+            MT_LAUNCHED(ctx);
+        }
+        int64_t total = 0;
+        if (int rc = csr_offsets(ctx, cnt, ncol, st.col_off, &total)) return rc;
+        if (int rc = st.col_x.alloc(ctx, total)) return rc;
+        if (int rc = cur.alloc(ctx, ncol + 1)) return rc;
+        MT_CUDA(ctx, cudaMemcpyAsync(cur.p, st.col_off.p, sizeof(int32_t) * (ncol + 1), cudaMemcpyDeviceToDevice,
+                                     ctx.stream));
+        if (total) {
+            k_tri_columns<<<grid_for(nt, 128), 128, 0, ctx.stream>>>(st.tri.p, nt, g, 1, nullptr, cur.p, st.col_x.p);
+            MT_LAUNCHED(ctx);
+        }
+    }
+    {
+        DBuf<int32_t> cnt, cur;
+        if (int rc = cnt.alloc(ctx, nbin + 1)) return rc;
+        MT_CUDA(ctx, cudaMemsetAsync(cnt.p, 0, sizeof(int32_t) * (nbin + 1), ctx.stream));
+        if (nt && nbin) {
+            k_tri_bins<<<grid_for(nt, 128), 128, 0, ctx.stream>>>(st.tri.p, nt, st.box, 0, cnt.p, nullptr, nullptr);
+            MT_LAUNCHED(ctx);
+        }
+        int64_t total = 0;
+        if (int rc = csr_offsets(ctx, cnt, nbin, st.bin_off, &total)) return rc;
+        if (int rc = st.bin_tri.alloc(ctx, total)) return rc;
+        if (int rc = cur.alloc(ctx, nbin + 1)) return rc;
+        MT_CUDA(ctx, cudaMemcpyAsync(cur.p, st.bin_off.p, sizeof(int32_t) * (nbin + 1), cudaMemcpyDeviceToDevice,
+                                     ctx.stream));
+        if (total) {
+            k_tri_bins<<<grid_for(nt, 128), 128, 0, ctx.stream>>>(st.tri.p, nt, st.box, 1, nullptr, cur.p,
+                                                                 st.bin_tri.p);
+            MT_LAUNCHED(ctx);
+        }
+    }
+    return MT_OK;
+}
+
 }  // namespace
 
 // raw sets of every level, the dis table or the band, then the build
@@ -334,6 +632,21 @@ int amr_generate(Ctx &ctx, Case &c, const mt_mesh_spec &sp)
     if (int rc = derr.alloc(ctx, 1)) return rc;
     MT_CUDA(ctx, cudaMemsetAsync(derr.p, 0, sizeof(int), ctx.stream));
     Box dom{{0, 0, 0}, {sp.coarse[0], sp.coarse[1], sp.coarse[2]}};
+    SurfaceTables st;
+    if (sp.sphere == 3) {
+        if (L == 0) return set_err(ctx, MT_ERR_MESH, "the solid boundary is only applied on a refined finest level");
+        Box f = dom;
+        for (int l = 0; l < L; ++l) {
+            Box nx{{0, 0, 0}, {0, 0, 0}};
+            if (sp.has_refine[l] && f.n() > 0)
+                for (int a = 0; a < 3; ++a) {
+                    nx.lo[a] = 2 * sp.refine_lo[l][a];
+                    nx.hi[a] = 2 * sp.refine_hi[l][a];
+                }
+            f = nx;
+        }
+        if (int rc = surface_tables(ctx, c.h_tri, L, f, st)) return rc;
+    }
     for (int l = 0; l <= L; ++l) {
         LevelGen g{};
         g.level = l;
@@ -362,6 +675,12 @@ int amr_generate(Ctx &ctx, Case &c, const mt_mesh_spec &sp)
         g.r = sp.radius * s;
         g.amp = sp.osc_amplitude * s;
         g.slack = sp.band_slack * s;
+        g.col_off = st.col_off.p;
+        g.col_x = st.col_x.p;
+        for (int a = 0; a < 2; ++a) {
+            g.col_lo[a] = st.col_lo[a];
+            g.col_n[a] = st.col_n[a];
+        }
         if (g.sphere == 1 && L == 0)
             return set_err(ctx, MT_ERR_MESH, "the solid boundary is only applied on a refined finest level");
         Level &lv = c.lv[l];
@@ -441,20 +760,28 @@ int amr_generate(Ctx &ctx, Case &c, const mt_mesh_spec &sp)
             }
             if (int rc = select_flagged(ctx, uniq.p, flag.p, uniq.n, gf2c)) return rc;
         }
-        if (l == L && g.sphere == 1) {
+        if (l == L && (g.sphere == 1 || g.sphere == 3)) {
             // wall distances of the fluid cells; the solid must stay clear of C2F
             const int w = q - 1;
             DBuf<double> rows;
             DBuf<uint8_t> hit;
             if (int rc = rows.alloc(ctx, latf.n * w)) return rc;
             if (int rc = hit.alloc(ctx, latf.n)) return rc;
-            if (latf.n) {
+            if (latf.n && g.sphere == 1) {
                 if (q == 19)
                     k_links<19><<<grid_for(latf.n, 128), 128, 0, ctx.stream>>>(latf.p, latf.n, g.cx, g.cy, g.cz, g.r,
                                                                               rows.p, hit.p);
                 else
                     k_links<27><<<grid_for(latf.n, 128), 128, 0, ctx.stream>>>(latf.p, latf.n, g.cx, g.cy, g.cz, g.r,
                                                                               rows.p, hit.p);
+                MT_LAUNCHED(ctx);
+            } else if (latf.n) {
+                if (q == 19)
+                    k_links_surface<19><<<grid_for(latf.n, 128), 128, 0, ctx.stream>>>(
+                        latf.p, latf.n, st.tri.p, st.box, st.bin_off.p, st.bin_tri.p, rows.p, hit.p);
+                else
+                    k_links_surface<27><<<grid_for(latf.n, 128), 128, 0, ctx.stream>>>(
+                        latf.p, latf.n, st.tri.p, st.box, st.bin_off.p, st.bin_tri.p, rows.p, hit.p);
                 MT_LAUNCHED(ctx);
             }
             // indices of the hit cells, in key order

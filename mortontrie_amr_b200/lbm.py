@@ -34,7 +34,7 @@ EXPORTS = [
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
     "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
-    "mt_case_generate",
+    "mt_case_generate", "mt_case_set_surface",
 ]
 
 
@@ -78,7 +78,9 @@ def make_mesh_spec(spec) -> mt_mesh_spec:
         for a in range(3):
             m.refine_lo[l][a] = int(box[0][a])
             m.refine_hi[l][a] = int(box[1][a])
-    if spec.sphere is not None:
+    if getattr(spec, "surface", None) is not None:
+        m.sphere = 3
+    elif spec.sphere is not None:
         m.sphere = 2 if spec.ib == "markers" else 1
         for a in range(3):
             m.center[a] = float(spec.sphere.center[a])
@@ -114,7 +116,7 @@ def lib():
             "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
             "mt_batch_create": [vp, i32p], "mt_batch_destroy": [vp, i32], "mt_batch_add": [vp, i32, i32],
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
-            "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -217,6 +219,10 @@ class LBM_Manager:
         m = case.mesh
         if generate or isinstance(m, SpecMesh):
             ms = make_mesh_spec(m.spec)
+            if ms.sphere == 3:
+                t = np.ascontiguousarray(m.spec.surface, np.float64).reshape(-1, 9)
+                ctx.check(lib().mt_case_set_surface(ctx.h, self.id, _ptr(t, C.c_double), t.shape[0]),
+                          "mt_case_set_surface")
             ctx.check(lib().mt_case_generate(ctx.h, self.id, C.byref(ms)), "mt_case_generate")
             self._finish(m, schedule, scaling)
             return

@@ -1,6 +1,7 @@
 """Lattice classification on the device (mt_case_generate) against the host
 mesher: the same keys, set tags and neighbour tables on every level, and
-bit-identical populations and forces after stepping both builds."""
+bit-identical populations and forces after stepping both builds (analytic
+spheres, direct-forcing bands and triangulated STL surfaces)."""
 import numpy as np
 import pytest
 
@@ -17,7 +18,8 @@ def ctx():
 
 def _cases():
     from mortontrie_amr_b200.case import (cavity_case, df_sphere_case, nested_sphere_case, sphere_case,
-                                          uniform_box_case)
+                                          surface_case, uniform_box_case)
+    from mortontrie_amr_b200.stl import box_surface, icosphere
     return {
         "sphere_q19_fh": sphere_case(coarse=(32, 16, 16), refine=[((6, 4, 4), (18, 12, 12))], center=(12, 8, 8),
                                      radius=2.0),
@@ -30,6 +32,14 @@ def _cases():
         "df_osc_l2": df_sphere_case(radius=3, max_level=2, re=60.0, oscillating=True, period=100),
         "df_slack_l1": df_sphere_case(radius=4, max_level=1, re=80.0, band_slack=1.0),
         "box_periodic_empty": uniform_box_case(q=19, n=(16, 12, 8), empty_levels=1),
+        "surface_icosphere_q19_fh": surface_case(icosphere((12, 8, 8), 2.0, 3), coarse=(32, 16, 16),
+                                                 refine=[((6, 4, 4), (18, 12, 12))]),
+        "surface_box_q27_dw": surface_case(box_surface((10.3, 6.6, 6.1), (13.7, 9.4, 9.85)), q=27,
+                                           collision="Cumulant", ib_method="DW", coarse=(32, 16, 16),
+                                           refine=[((6, 4, 4), (18, 12, 12))]),
+        "surface_icosphere_l2": surface_case(icosphere((16, 12, 12), 2.0, 3), coarse=(48, 24, 24), max_level=2,
+                                             refine=[((8, 6, 6), (26, 18, 18)), ((22, 16, 16), (42, 32, 32))],
+                                             re=50.0),
     }
 
 
