@@ -528,8 +528,10 @@ def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=
         cd64 = solve_alone(ctx, cache, next(q for q in reqs if q.rid == r.rid), storage="f64")[0]
         if np.isfinite(cd64) and abs(cd64) > 1e-6:
             errs.append(abs(res[r.rid].cd - cd64) / abs(cd64))
+    from mortontrie_amr_b200.serving import U_INLET
     return {"workload": f"{len(reqs)} Poisson requests ({rate:g}/s over {duration:g} s, seed {seed}): DF sphere "
-                        "R 3-8, 1-3 levels, Re 20-300, half oscillating, 2000 finest steps each, FP16",
+                        f"R 3-8, 1-3 levels, Re 20-300, inlet u {U_INLET:g}, half oscillating, 2000 finest steps "
+                        "each, FP16",
             "template_build_s": round(prep, 1), "templates": len(cache.meshes), **served,
             "finite_results": len(finite),
             "one_at_a_time_cases_per_hour": round(alone_rate, 1),

@@ -205,7 +205,9 @@ int mt_case_status(mt_ctx *ctx, int32_t case_id);
 /* Autotuner of the dense path (no reference counterpart): times the fused
  * kernel at 128, 256, 512 and 1024 threads per block on the case's own state
  * (writing only the scratch array, so the state is unchanged) and keeps the
- * fastest; ms_per_candidate (nullable) receives the 4 mean launch times. */
+ * fastest; ms_per_candidate (nullable) receives the mean launch time of each
+ * candidate the kernel is built for (the paired 16-bit LBGK kernel: 128 and
+ * 256 only; the other slots are left unwritten). */
 int mt_case_tune(mt_ctx *ctx, int32_t case_id, int32_t *best_block, float *ms_per_candidate);
 /* Schedule of mt_step for a multi-level case (no reference counterpart):
  * MT_SCHED_PHASES (default) issues the reference's phases one pass each;

@@ -681,7 +681,10 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
 }
 
 template <int Q, class S, int COLL>
-__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? 6 : 1) k_brick_step(
+#ifndef MT_BRICK_MIN_BLOCKS
+#define MT_BRICK_MIN_BLOCKS 8  // resident 128-thread blocks per SM asked of the 16-bit brick passes (64 registers)
+#endif
+__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_MIN_BLOCKS : 1) k_brick_step(
     int64_t nb, const int32_t *__restrict__ halo, const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
     const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext, double tau,
     typename Store<S>::C *__restrict__ rho, typename Store<S>::C *__restrict__ u, int macros, int fall)
@@ -697,7 +700,7 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? 6 : 1) k_brick_ste
 // list belongs to the slot whose [off[s], off[s + 1]) range holds it; each
 // slot carries one case level's tables, buffers and relaxation time.
 template <int Q, class S, int COLL>
-__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? 6 : 1) k_brick_step_batch(const BrickBatch *__restrict__ bb)
+__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_MIN_BLOCKS : 1) k_brick_step_batch(const BrickBatch *__restrict__ bb)
 {
     __shared__ int32_t s_idx[4][216];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;

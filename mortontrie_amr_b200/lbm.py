@@ -508,9 +508,10 @@ class DenseCase:
         """Pick the fused kernel's block size (state unchanged); returns
         (block, {block: ms per launch})."""
         best = C.c_int32()
-        ms = (C.c_float * 4)()
+        ms = (C.c_float * 4)(*([-1.0] * 4))
         self.ctx.check(lib().mt_case_tune(self.ctx.h, self.id, C.byref(best), ms), "mt_case_tune")
-        return best.value, dict(zip((128, 256, 512, 1024), [round(float(v), 5) for v in ms]))
+        # candidates the kernel is not built for (paired 16-bit LBGK: at most 256 threads) are left out
+        return best.value, {b: round(float(v), 5) for b, v in zip((128, 256, 512, 1024), ms) if v >= 0.0}
 
     def close(self):
         if getattr(self, "id", None) is not None and self.ctx.h:

@@ -20,7 +20,8 @@ def test_poisson_stream_is_seeded_and_in_range():
 
 
 def test_request_case_on_template():
-    from mortontrie_amr_b200.serving import Request, build_template, footprint_bytes, request_case, template_key
+    from mortontrie_amr_b200.serving import (U_INLET, Request, build_template, footprint_bytes, request_case,
+                                             template_key)
     req = Request(rid=0, arrival=0.0, radius=3.4, levels=2, re=150.0, oscillating=True)
     assert template_key(req) == (4, 2, True)
     mesh = build_template(template_key(req))
@@ -32,7 +33,7 @@ def test_request_case_on_template():
     # the oscillation path: amplitude R/2 along y, one period of 2000 finest steps
     p = case.mesh.markers.path
     assert p.shape == (2000, 6) and abs(p[:, 1].max() - 0.5 * req.radius * s) < 1e-3
-    assert np.isclose(case.params.nu, 0.05 * 2 * req.radius / req.re)
+    assert np.isclose(case.params.nu, U_INLET * 2 * req.radius / req.re)
     assert case.mesh.levels[2]["lat_f"] is mesh.levels[2]["lat_f"]   # shared host mesh
     assert footprint_bytes(case, "f16") < footprint_bytes(case, "f64")
     # every stencil cell of every marker over the path lies in the forcing band
