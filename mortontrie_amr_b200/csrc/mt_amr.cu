@@ -962,6 +962,7 @@ int batch_bricks(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cs, int l, co
                 sl.textbook = c.d.stream_convention;
                 sl.fall = (l == 0 && c.d.bc_mode == MT_BC_NEQ) ? 1 : 0;
                 sl.macros = c.macros_now;
+                sl.acc = (l == c.d.max_level && lv.nband) ? c.acc : nullptr;
                 d.off[d.nslots + 1] = d.off[d.nslots] + lv.nbrick;
                 ++d.nslots;
             }

@@ -624,7 +624,8 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
                                            const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
                                            const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext,
                                            double tau, typename Store<S>::C *__restrict__ rho,
-                                           typename Store<S>::C *__restrict__ u, int macros, int fall)
+                                           typename Store<S>::C *__restrict__ u, int macros, int fall,
+                                           long long *__restrict__ acc)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -664,7 +665,28 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
             for (int k = 0; k < Q; ++k) fnext[(uint32_t)k * n + i] = v[k];
             continue;
         }
-        if (cls == 4) continue;  // direct-forcing band: collided after the forcing
+        if (cls == 4) {
+            // direct-forcing band: collided after the forcing; with acc the
+            // band's rho, unforced velocity and cleared accumulator are
+            // written here (what k_band_macros computes from the stored f)
+            if constexpr (COLL == MT_COLL_LBGK) {
+                if (acc) {
+                    C d[Q];
+#pragma unroll
+                    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::cv(v[k]), k);
+                    C r, x, y, z;
+                    macros_g<Q, C>(d, r, x, y, z);
+                    rho[i] = r;
+                    u[i] = x;
+                    u[n + i] = y;
+                    u[2 * n + i] = z;
+                    acc[i] = 0;
+                    acc[n + i] = 0;
+                    acc[2 * n + i] = 0;
+                }
+            }
+            continue;
+        }
         C d[Q];
 #pragma unroll
         for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::cv(v[k]), k);
@@ -687,13 +709,15 @@ template <int Q, class S, int COLL>
 __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_MIN_BLOCKS : 1) k_brick_step(
     int64_t nb, const int32_t *__restrict__ halo, const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
     const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext, double tau,
-    typename Store<S>::C *__restrict__ rho, typename Store<S>::C *__restrict__ u, int macros, int fall)
+    typename Store<S>::C *__restrict__ rho, typename Store<S>::C *__restrict__ u, int macros, int fall,
+    long long *__restrict__ acc)
 {
     __shared__ int32_t s_idx[4][216];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t b = 4 * (int64_t)blockIdx.x + w;
     if (b >= nb) return;
-    brick_warp<Q, S, COLL>(b, lane, s_idx[w], halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros, fall);
+    brick_warp<Q, S, COLL>(b, lane, s_idx[w], halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros, fall,
+                           acc);
 }
 
 // The same pass over the bricks of many cases (a batch): brick b of the work
@@ -717,7 +741,7 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_MIN_BLOCK
     const BrickSlot &sl = bb->slot[lo];
     using C = typename Store<S>::C;
     brick_warp<Q, S, COLL>(b - bb->off[lo], lane, s_idx[w], sl.halo, sl.cls, sl.n, sl.textbook, (const S *)sl.fcol,
-                           (S *)sl.f, (S *)sl.fnext, sl.tau, (C *)sl.rho, (C *)sl.u, sl.macros, sl.fall);
+                           (S *)sl.f, (S *)sl.fnext, sl.tau, (C *)sl.rho, (C *)sl.u, sl.macros, sl.fall, sl.acc);
 }
 
 // The streamed f of the class-1 cells, from the buffer the last fused pass
@@ -906,16 +930,36 @@ __global__ void k_df_markers(int64_t nm, const double *ref, const double *dv, do
 
 // the body force of one forcing step: a fixed-order sum of the markers'
 // forces into the accumulator (fx, fy, fz, count), then the substep count
-static __global__ void k_df_sum(const double *fk, int64_t nm, double *acc, long long *tstep)
+static __global__ void __launch_bounds__(256) k_df_sum(const double *fk, int64_t nm, double *part, unsigned *done,
+                                                        double *acc, long long *tstep)
 {
-    __shared__ double s[3][1024];
+    // body force: a fixed-order tree over each block of 256 markers, then the
+    // last block to finish sums the partials in block order (deterministic)
+    __shared__ double s[3][256];
+    __shared__ bool last;
     const int t = threadIdx.x;
+    const int64_t j = blockIdx.x * (int64_t)256 + t;
+    for (int c = 0; c < 3; ++c) s[c][t] = j < nm ? fk[c * nm + j] : 0.0;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (t < w)
+            for (int c = 0; c < 3; ++c) s[c][t] += s[c][t + w];
+        __syncthreads();
+    }
+    if (t == 0) {
+        for (int c = 0; c < 3; ++c) part[3 * blockIdx.x + c] = s[c][0];
+        __threadfence();
+        last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
     double a[3] = {0., 0., 0.};
-    for (int64_t j = t; j < nm; j += blockDim.x)
-        for (int c = 0; c < 3; ++c) a[c] += fk[c * nm + j];
+    for (int64_t b = t; b < gridDim.x; b += 256)
+        for (int c = 0; c < 3; ++c) a[c] += __ldcg(part + 3 * b + c);
     for (int c = 0; c < 3; ++c) s[c][t] = a[c];
     __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    for (int w = 128; w > 0; w >>= 1) {
         if (t < w)
             for (int c = 0; c < 3; ++c) s[c][t] += s[c][t + w];
         __syncthreads();
@@ -924,6 +968,7 @@ static __global__ void k_df_sum(const double *fk, int64_t nm, double *acc, long 
         for (int c = 0; c < 3; ++c) acc[c] += s[c][0];
         acc[3] += 1.0;
         *tstep += 1;
+        *done = 0u;
     }
 }
 
@@ -1131,17 +1176,20 @@ inline double f2c_scale(const Case &c, int coarse)
 
 // the direct-forcing step on level l (after its stream): band macros, the
 // markers' interpolation and spreading, the body force
+// (band_macros_done: the level's brick pass already wrote the band macros)
 template <class S, int Q>
-int df_force(Ctx &ctx, Case &c, int l)
+int df_force(Ctx &ctx, Case &c, int l, bool band_macros_done = false)
 {
     using A = AmrTyped<S>;
     using C = typename Store<S>::C;
     cudaStream_t s = ctx.stream;
     Level &lv = c.lv[l];
     if (!lv.nband) return MT_OK;
-    k_band_macros<Q, S><<<grid_for(lv.nband, 128), 128, 0, s>>>(lv.band, lv.nband, lv.n, A::f(lv), A::rho(lv),
-                                                                 A::u(lv), c.acc);
-    MT_LAUNCHED(ctx);
+    if (!band_macros_done) {
+        k_band_macros<Q, S><<<grid_for(lv.nband, 128), 128, 0, s>>>(lv.band, lv.nband, lv.n, A::f(lv), A::rho(lv),
+                                                                     A::u(lv), c.acc);
+        MT_LAUNCHED(ctx);
+    }
     if (!c.nm) {
         k_force_tick<<<1, 1, 0, s>>>(c.force_acc);
         MT_LAUNCHED(ctx);
@@ -1152,7 +1200,9 @@ int df_force(Ctx &ctx, Case &c, int l)
         c.mlo[1], c.mlo[2], c.mdim[0], c.mdim[1], c.mdim[2], lv.n, (const C *)A::rho(lv), (const C *)A::u(lv), c.acc,
         c.mforce);
     MT_LAUNCHED(ctx);
-    k_df_sum<<<1, 1024, 0, s>>>(c.mforce, c.nm, c.force_acc, c.tstep);
+    const int64_t nbf = (c.nm + 255) / 256;
+    k_df_sum<<<(unsigned)nbf, 256, 0, s>>>(c.mforce, c.nm, c.mforce + 3 * c.nm,
+                                           (unsigned *)(c.mforce + 3 * (c.nm + nbf)), c.force_acc, c.tstep);
     MT_LAUNCHED(ctx);
     return MT_OK;
 }
@@ -1355,7 +1405,8 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         return MT_OK;
     }
     case PH_DF: {
-        if (int rc = df_force<S, Q>(ctx, c, l)) return rc;
+        // after PH_PULL_COLLIDE: a brick level's pass (alone or batched) wrote the band macros
+        if (int rc = df_force<S, Q>(ctx, c, l, lv.bricks)) return rc;
         return band_collide<S, Q>(ctx, c, l, lv.fcol_alt);
     }
     case PH_BAND_GRID:
@@ -1454,16 +1505,18 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         } else if (lv.bricks) {
             const unsigned g = grid_for(lv.nbrick, 4);
             const uint32_t n32 = (uint32_t)n;
+            // the band's macros come out of the pass (the direct-forcing step skips k_band_macros)
+            long long *bacc = (l == L && lv.nband) ? c.acc : nullptr;
             if (c.d.collision == MT_COLL_LBGK) {
                 k_brick_step<Q, S, MT_COLL_LBGK><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb, A::fcol(lv),
                                                                    A::f(lv), (S *)lv.fcol_alt, c.d.tau[l],
-                                                                   A::rho(lv), A::u(lv), mac, fall);
+                                                                   A::rho(lv), A::u(lv), mac, fall, bacc);
             } else {
                 if constexpr (Q == 27)
                     k_brick_step<Q, S, MT_COLL_CUMULANT><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb,
                                                                            A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
                                                                            c.d.tau[l], A::rho(lv), A::u(lv), mac,
-                                                                           fall);
+                                                                           fall, nullptr);
             }
             MT_LAUNCHED(ctx);
         } else {

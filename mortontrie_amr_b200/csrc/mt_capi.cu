@@ -756,7 +756,11 @@ int mt_case_set_markers(mt_ctx *h, int32_t id, int64_t nm, const double *ref, co
     if (nm) {
         MT_CUDA(ctx, cudaMalloc(&c->mref, sizeof(double) * 3 * nm));
         MT_CUDA(ctx, cudaMalloc(&c->mdv, sizeof(double) * nm));
-        MT_CUDA(ctx, cudaMalloc(&c->mforce, sizeof(double) * 3 * (nm + (nm + 255) / 256)));
+        // per-marker forces [3][nm], the body-force partials of 256-marker
+        // blocks [3][ceil(nm / 256)], and the finished-block counter of the sum
+        const int64_t nbf = 3 * (nm + (nm + 255) / 256) + 1;
+        MT_CUDA(ctx, cudaMalloc(&c->mforce, sizeof(double) * nbf));
+        MT_CUDA(ctx, cudaMemset(c->mforce, 0, sizeof(double) * nbf));
         MT_CUDA(ctx, cudaMemcpy(c->mref, ref, sizeof(double) * 3 * nm, cudaMemcpyHostToDevice));
         MT_CUDA(ctx, cudaMemcpy(c->mdv, dv, sizeof(double) * nm, cudaMemcpyHostToDevice));
     }

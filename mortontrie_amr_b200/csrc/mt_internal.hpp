@@ -101,6 +101,7 @@ struct BrickSlot {
     const uint8_t *cls = nullptr;
     const void *fcol = nullptr;  // current post-collision buffer
     void *f = nullptr, *fnext = nullptr, *rho = nullptr, *u = nullptr;
+    long long *acc = nullptr;  // direct-forcing accumulator: band macros in the pass (finest level), else null
     double tau = 1.0;
     uint32_t n = 0;
     int32_t textbook = 0, fall = 0, macros = 0;
