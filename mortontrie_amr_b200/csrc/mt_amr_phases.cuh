@@ -893,19 +893,27 @@ __global__ void k_df_markers(int64_t nm, const double *ref, const double *dv, do
     const double X = cx + pp[0] + ref[m], Y = cy + pp[1] + ref[nm + m], Z = cz + pp[2] + ref[2 * nm + m];
     const double ubx = pp[3], uby = pp[4], ubz = pp[5];
     const int64_t ix = (int64_t)floor(X), iy = (int64_t)floor(Y), iz = (int64_t)floor(Z);
+    // the kernel's factors per axis (a stencil weight is wx wy wz, multiplied
+    // in that order as the per-point evaluation does)
+    double wx[3], wy[3], wz[3];
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+        wx[o] = roma3((double)(ix + o - 1) + 0.5 - X);
+        wy[o] = roma3((double)(iy + o - 1) + 0.5 - Y);
+        wz[o] = roma3((double)(iz + o - 1) + 0.5 - Z);
+    }
     int32_t idx[27];
-    double wgt[27];
     double r = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
+#pragma unroll
     for (int c = 0; c < 27; ++c) {
-        const int64_t x = ix + c % 3 - 1, y = iy + (c / 3) % 3 - 1, z = iz + c / 9 - 1;
-        const double wv = roma3((double)x + 0.5 - X) * roma3((double)y + 0.5 - Y) * roma3((double)z + 0.5 - Z);
+        const int ox = c % 3, oy = (c / 3) % 3, oz = c / 9;
+        const double wv = wx[ox] * wy[oy] * wz[oz];
         // only band cells take force; they all lie in the grid's box
-        const int64_t gx = x - lx, gy = y - ly, gz = z - lz;
+        const int64_t gx = ix + ox - 1 - lx, gy = iy + oy - 1 - ly, gz = iz + oz - 1 - lz;
         const int32_t i = (gx >= 0 && gy >= 0 && gz >= 0 && gx < dx && gy < dy && gz < dz)
                               ? __ldg(grid + gx + dx * (gy + dy * gz))
                               : -1;
         idx[c] = i;
-        wgt[c] = wv;
         if (i >= 0) {
             r += wv * (double)rho[i];
             vx += wv * (double)u[i];
@@ -915,10 +923,11 @@ __global__ void k_df_markers(int64_t nm, const double *ref, const double *dv, do
     }
     const double fx = 2.0 * r * (ubx - vx), fy = 2.0 * r * (uby - vy), fz = 2.0 * r * (ubz - vz);
     const double d = dv[m];
+#pragma unroll
     for (int c = 0; c < 27; ++c) {
         const int32_t i = idx[c];
         if (i < 0) continue;
-        const double s = wgt[c] * d;
+        const double s = wx[c % 3] * wy[(c / 3) % 3] * wz[c / 9] * d;
         atomicAdd((unsigned long long *)(acc + i), (unsigned long long)__double2ll_rn(fx * s * kForceScale));
         atomicAdd((unsigned long long *)(acc + n + i), (unsigned long long)__double2ll_rn(fy * s * kForceScale));
         atomicAdd((unsigned long long *)(acc + 2 * n + i), (unsigned long long)__double2ll_rn(fz * s * kForceScale));
