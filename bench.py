@@ -498,6 +498,40 @@ def _case_result(mgr, case):
     return {"u": np.concatenate(us, axis=1), "cd": cd}
 
 
+def served_case_section(ctx, torch, steps=10, warmup=2):
+    """The largest request of the served mix alone: a direct-forcing sphere
+    of radius 8 coarse cells (channel 128x64x64, 3 refinement levels, 51,472
+    markers), oscillating, D3Q19 LBGK, FP16 storage, fused schedule, lattice
+    classified on the device.  Also the profiling driver of the forcing
+    kernels (few launches: one case, `warmup` + `steps` coarse steps)."""
+    from mortontrie_amr_b200.case import df_sphere_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    from mortontrie_amr_b200.serving import AMPLITUDE, PERIOD, U_INLET
+    case = df_sphere_case(radius=8, max_level=3, re=150.0, oscillating=True, u=U_INLET, period=PERIOD,
+                          amplitude=AMPLITUDE, mesh="device")
+    stream = torch.cuda.current_stream()
+    mgr = LBM_Manager(ctx, case, "f16", schedule="fused", scaling="standard")
+    upd = _stepped_updates(mgr)
+    band = int(np.count_nonzero(mgr.keys(3)[1] & 256))
+    mgr.fluidSimulate(warmup)
+    torch.cuda.synchronize()
+    n0 = ctx.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    mgr.fluidSimulate(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    out = {"workload": "DF sphere R=8 (64 finest), 128x64x64 coarse, 3 refinement levels, oscillating, Re 150, FP16",
+           "cell_updates_per_coarse_step": upd, "band_cells": band, "markers": int(case.mesh.markers.dv.size),
+           "coarse_steps": steps, "ms_per_coarse_step": round(1e3 * secs / steps, 3),
+           "mlups": round(upd * steps / secs / 1e6, 1),
+           "launches_per_coarse_step": (ctx.launch_count() - n0) // steps}
+    mgr.close()
+    return out
+
+
 def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=16):
     """Served mix: a seeded Poisson stream (rate 20/s for `duration` s) of
     direct-forcing sphere flows (R in [3, 8], 16R x 8R x 8R, 1-3 refinement
@@ -692,6 +726,8 @@ def main():
     ap.add_argument("--served-only", type=float, default=0.0, metavar="SECONDS",
                     help="only the served mix, with SECONDS of Poisson arrivals")
     ap.add_argument("--batched-only", action="store_true", help="only the batched uneven instances section")
+    ap.add_argument("--served-case", action="store_true",
+                    help="only the largest served request alone (profiling driver of the forcing kernels)")
     ap.add_argument("--amr-variants", default=None,
                     help="comma list of multi-level runs to time (default all: "
                          "f64,f64_fused,f32,f16,bf16,f16_phases); profiling runs")
@@ -718,6 +754,16 @@ def main():
         ctx = Context(0)
         ctx.set_stream(stream.cuda_stream)
         print(json.dumps({"served_mix": served_section(ctx, torch, duration=args.served_only)}), flush=True)
+        ctx.close()
+    elif args.served_case:
+        import torch
+
+        from mortontrie_amr_b200.lbm import Context
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx = Context(0)
+        ctx.set_stream(stream.cuda_stream)
+        print(json.dumps({"served_case": served_case_section(ctx, torch, steps=args.steps, warmup=2)}), flush=True)
         ctx.close()
     elif args.batched_only:
         import torch

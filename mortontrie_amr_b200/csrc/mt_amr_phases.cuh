@@ -828,6 +828,7 @@ __global__ void k_ib_collide(const int32_t *list, int64_t nl, int64_t n, const i
 // The Eulerian force of a substep is spread into int64 fixed point (2^-32),
 // so the atomic sums are exact and independent of the order of arrival.
 constexpr double kForceScale = 4294967296.0;  // 2^32
+constexpr double kForceInv = 1.0 / 4294967296.0;
 
 __host__ __device__ __forceinline__ double roma3(double r)
 {
@@ -1003,8 +1004,9 @@ __global__ void k_band_collide(const int32_t *band, int64_t nb, int64_t n, doubl
         jy += d[k] * ey(k);
         jz += d[k] * ez(k);
     }
-    const C gx = (C)((double)acc[i] / kForceScale), gy = (C)((double)acc[n + i] / kForceScale),
-            gz = (C)((double)acc[2 * n + i] / kForceScale);
+    // times 2^-32: exactly the division by the power-of-two scale
+    const C gx = (C)((double)acc[i] * kForceInv), gy = (C)((double)acc[n + i] * kForceInv),
+            gz = (C)((double)acc[2 * n + i] * kForceInv);
     const C rs = (r > C(-1e-6) && r < C(1e-6)) ? ((r < C(0)) ? C(-1e-6) : C(1e-6)) : r;
     const C x = (jx + gx * C(0.5)) / rs, y = (jy + gy * C(0.5)) / rs, z = (jz + gz * C(0.5)) / rs;
     const C om = C(1) / C(tau);
