@@ -251,6 +251,8 @@ int mt_case_set_markers(mt_ctx *ctx, int32_t case_id, int64_t nm, const double *
  * level runs one batched brick pass per model family (Q, collision, storage)
  * over all members that have that level, driven from a work list of their
  * 4x4x4 bricks; the members' other phases run on parallel graph branches.
+ * A member level of 8192 bricks or more fills the GPU by itself and runs its
+ * own brick pass on a branch beside the batched one.
  * Each coarse step of the batch is one captured CUDA graph (re-captured when
  * the membership changes).  A member ends every step in the state it would
  * reach stepped alone with MT_SCHED_FUSED (bit-identical: the same kernels

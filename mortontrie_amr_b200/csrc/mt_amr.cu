@@ -929,7 +929,7 @@ int batch_bricks(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cs, int l, co
     // group by (q, collision, storage): one kernel instantiation each
     std::vector<std::vector<Case *>> groups;
     for (Case *c : cs) {
-        if (!c->lv[l].bricks) continue;
+        if (!c->lv[l].bricks || c->lv[l].nbrick >= kBatchOwnBricks) continue;
         bool placed = false;
         for (auto &g : groups)
             if (g[0]->d.q == c->d.q && g[0]->d.collision == c->d.collision &&
@@ -1000,13 +1000,15 @@ int batch_lbm_kernel(Ctx &ctx, BatchRec &R, const std::vector<Case *> &all, int 
                                  [&](Case &c) { return amr_phase(ctx, c, PH_EXPLOSION, l); })))
                 return rc;
         for (Case *c : cs) c->macros_now = last && !(l == 0 && c->d.bc_mode == MT_BC_NEQ);
-        // members' own pull work (IB cells; levels without bricks) beside the batched brick pass
+        // members' own pull work (IB cells; levels without bricks; levels
+        // large enough to fill the GPU alone) beside the batched brick pass
         {
             Batch &B = *R.b;
             cudaStream_t main = ctx.stream;
             std::vector<Case *> own;
+            auto batched = [&](const Case *c) { return c->lv[l].bricks && c->lv[l].nbrick < kBatchOwnBricks; };
             for (Case *c : cs)
-                if (!c->lv[l].bricks || (l == c->d.max_level && l > 0)) own.push_back(c);
+                if (!batched(c) || (l == c->d.max_level && l > 0)) own.push_back(c);
             const int P = (int)std::min<size_t>(B.pool.size(), own.size());
             if (P) {
                 MT_CUDA(ctx, cudaEventRecord(B.ev_fork, main));
@@ -1014,7 +1016,7 @@ int batch_lbm_kernel(Ctx &ctx, BatchRec &R, const std::vector<Case *> &all, int 
                 for (size_t i = 0; i < own.size(); ++i) {
                     Case &c = *own[i];
                     ctx.stream = B.pool[i % P];
-                    c.pull_mode = c.lv[l].bricks ? 1 : 0;
+                    c.pull_mode = batched(&c) ? 1 : 0;
                     rc = amr_phase(ctx, c, PH_PULL_COLLIDE, l);
                     c.pull_mode = 0;
                     if (rc) {

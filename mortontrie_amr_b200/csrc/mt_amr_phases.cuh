@@ -723,8 +723,11 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_MIN_BLOCK
 // The same pass over the bricks of many cases (a batch): brick b of the work
 // list belongs to the slot whose [off[s], off[s + 1]) range holds it; each
 // slot carries one case level's tables, buffers and relaxation time.
+#ifndef MT_BRICK_BATCH_MIN_BLOCKS
+#define MT_BRICK_BATCH_MIN_BLOCKS MT_BRICK_MIN_BLOCKS  // the same for the batched pass
+#endif
 template <int Q, class S, int COLL>
-__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_MIN_BLOCKS : 1) k_brick_step_batch(const BrickBatch *__restrict__ bb)
+__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_BATCH_MIN_BLOCKS : 1) k_brick_step_batch(const BrickBatch *__restrict__ bb)
 {
     __shared__ int32_t s_idx[4][216];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;

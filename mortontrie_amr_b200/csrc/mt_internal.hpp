@@ -107,6 +107,9 @@ struct BrickSlot {
     int32_t textbook = 0, fall = 0, macros = 0;
 };
 constexpr int kMaxBatchSlots = 128;
+// a member level with at least this many bricks fills the GPU by itself: it
+// runs its own brick pass (same kernel as alone) beside the batched one
+constexpr int64_t kBatchOwnBricks = 8192;
 // a batched brick pass: slots and the prefix offsets of their bricks
 struct BrickBatch {
     int32_t nslots = 0;

@@ -117,3 +117,27 @@ def test_batch_membership_and_parity(ctx):
     for a, x in zip(alone, m):
         _assert_same(_state(a), _state(x))
     batch.close()
+
+
+@pytest.mark.parametrize("storage", ["f64", "f16"])
+def test_large_member_runs_its_own_pass(ctx, storage):
+    """A member whose level holds 8192 bricks or more (here both levels of a
+    96^3 cavity: 706,536 and 1,729,792 cells) runs its own brick pass beside
+    the batched pass of the small members; every member still equals itself
+    stepped alone."""
+    from mortontrie_amr_b200.case import cavity_case
+    from mortontrie_amr_b200.lbm import Batch, LBM_Manager
+    cases = [cavity_case(q=19, coarse=(96, 96, 96), max_level=1, re=100.0, mesh="device")] + _mix()[:2]
+    alone = [LBM_Manager(ctx, c, storage, schedule="fused") for c in cases]
+    members = [LBM_Manager(ctx, c, storage) for c in cases]
+    assert members[0].size(0) >= 8192 * 64
+    batch = Batch(ctx, members)
+    for m in alone:
+        m.fluidSimulate(3)
+    batch.step(3)
+    ctx.synchronize()
+    for a, m in zip(alone, members):
+        _assert_same(_state(a), _state(m), exact=(storage == "f64"))
+    batch.close()
+    for m in alone + members:
+        m.close()
