@@ -540,10 +540,12 @@ def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=
     by continuous batching in FP16 under a 150 GB budget.  Cases/h and the
     p50/p99 time-to-solution come from the wall clock of the request loop;
     the one-at-a-time rate solves every request of the stream alone (FP16,
-    fused schedule, back to back); the drag error compares served results
+    fused schedule, back to back), and the plain one-at-a-time rate does so in
+    the plain form (FP64, phase order; set-up plus 1/8 of each request's
+    steps, scaled to all); the drag error compares served results
     with FP64 solves (phase schedule) of the lowest-Re requests whose served
     result is finite."""
-    from mortontrie_amr_b200.serving import Server, TemplateCache, poisson_requests, solve_alone
+    from mortontrie_amr_b200.serving import Server, TemplateCache, plain_solve_seconds, poisson_requests, solve_alone
     reqs = poisson_requests(seed=seed, rate=rate, duration=duration)
     cache = TemplateCache(workers=max(1, min(16, (os.cpu_count() or 2) - 1)))
     t0 = time.time()
@@ -555,6 +557,9 @@ def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=
     served = stats.summary()
     t_alone = [solve_alone(ctx, cache, r, storage="f16")[2] for r in reqs]
     alone_rate = 3600.0 * len(reqs) / float(np.sum(t_alone))
+    # the plain form one at a time (FP64, phase order), from 1/8 of each request's steps
+    t_plain = [plain_solve_seconds(ctx, cache, r) for r in reqs]
+    plain_rate = 3600.0 * len(reqs) / float(np.sum(t_plain))
     res = {r.rid: r for r in stats.results}
     finite = [r for r in stats.results if np.isfinite(r.cd)]
     errs = []
@@ -571,6 +576,8 @@ def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=
             "one_at_a_time_cases_per_hour": round(alone_rate, 1),
             "one_at_a_time_wall_s": round(float(np.sum(t_alone)), 2),
             "served_vs_one_at_a_time": round(served["cases_per_hour"] / alone_rate, 2),
+            "plain_f64_one_at_a_time_cases_per_hour": round(plain_rate, 1),
+            "served_vs_plain_f64_one_at_a_time": round(served["cases_per_hour"] / plain_rate, 2),
             "drag_rel_vs_fp64": {"median": float(np.median(errs)) if errs else None,
                                  "max": float(np.max(errs)) if errs else None, "sample": len(errs)}}
 

@@ -278,6 +278,21 @@ int mt_case_transfer(mt_ctx *src, int32_t case_id, mt_ctx *dst, int32_t *new_id)
 int mt_get_force(mt_ctx *ctx, int32_t case_id, double *out4);
 int mt_reset_force(mt_ctx *ctx, int32_t case_id);
 
+/* ---- asynchronous completion (no reference counterpart) ---------------
+ * For a request loop that keeps a bounded number of steps in flight and
+ * learns when a result is ready without synchronising the context.
+ * mt_marker_record records the current point of the context stream and
+ * returns its ticket (increasing from 0); mt_marker_done sets *done = 1 once
+ * the stream has passed that point (it never blocks; recording blocks only
+ * when 64 markers are outstanding).  mt_case_force_async enqueues a copy of
+ * the accumulated force (as mt_get_force returns it) into page-locked memory
+ * the case keeps; mt_case_force_copied returns that copy, which is complete
+ * once a marker recorded after mt_case_force_async is done. */
+int mt_marker_record(mt_ctx *ctx, int64_t *ticket);
+int mt_marker_done(mt_ctx *ctx, int64_t ticket, int32_t *done);
+int mt_case_force_async(mt_ctx *ctx, int32_t case_id);
+int mt_case_force_copied(mt_ctx *ctx, int32_t case_id, double *out4);
+
 #ifdef __cplusplus
 }
 #endif

@@ -535,6 +535,8 @@ void amr_free(Case &c)
             if (lv.bclist[b]) cudaFree(lv.bclist[b]);
         lv = Level();
     }
+    if (c.h_force) cudaFreeHost(c.h_force);
+    c.h_force = nullptr;
     void *ptrs[] = {c.dis_key, c.dis, c.ib_force, c.force_acc, c.dev_err, c.bc_tmp, c.bc_all, c.bc_setb, c.bc_tmp_all,
                     c.mref, c.mdv, c.path, c.mforce, c.tstep, c.acc, c.mgrid};
     for (void *p : ptrs)

@@ -135,8 +135,51 @@ int mt_destroy(mt_ctx *h)
             if (c->B) cudaFree(c->B);
             delete c;
         }
+    for (cudaEvent_t e : h->c.markers)
+        if (e) cudaEventDestroy(e);
     if (h->c.own_stream) cudaStreamDestroy(h->c.stream);
     delete h;
+    return MT_OK;
+}
+
+int mt_marker_record(mt_ctx *h, int64_t *ticket)
+{
+    if (!h || !ticket) return MT_ERR_ARG;
+    Ctx &ctx = h->c;
+    MT_CUDA(ctx, cudaSetDevice(ctx.device));
+    if (ctx.markers.empty()) {
+        ctx.markers.assign(kMarkerRing, nullptr);
+        for (auto &e : ctx.markers) MT_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    const int64_t t = ctx.next_marker;
+    cudaEvent_t e = ctx.markers[t % kMarkerRing];
+    // the slot's previous marker must have passed before the slot is reused,
+    // so that a ticket older than the ring is known to be done
+    if (t >= kMarkerRing) MT_CUDA(ctx, cudaEventSynchronize(e));
+    MT_CUDA(ctx, cudaEventRecord(e, ctx.stream));
+    ctx.next_marker = t + 1;
+    *ticket = t;
+    return MT_OK;
+}
+
+int mt_marker_done(mt_ctx *h, int64_t ticket, int32_t *done)
+{
+    if (!h || !done) return MT_ERR_ARG;
+    Ctx &ctx = h->c;
+    if (ticket < 0 || ticket >= ctx.next_marker) return set_err(ctx, MT_ERR_ARG, "unknown marker ticket");
+    if (ticket < ctx.next_marker - kMarkerRing) {
+        *done = 1;
+        return MT_OK;
+    }
+    const cudaError_t e = cudaEventQuery(ctx.markers[ticket % kMarkerRing]);
+    if (e == cudaSuccess) {
+        *done = 1;
+    } else if (e == cudaErrorNotReady) {
+        cudaGetLastError();
+        *done = 0;
+    } else {
+        return set_err(ctx, MT_ERR_CUDA, std::string("cudaEventQuery: ") + cudaGetErrorString(e));
+    }
     return MT_OK;
 }
 
@@ -994,6 +1037,33 @@ int mt_get_force(mt_ctx *h, int32_t id, double *out4)
     }
     MT_CUDA(ctx, cudaMemcpyAsync(out4, c->force_acc, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
     MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
+int mt_case_force_async(mt_ctx *h, int32_t id)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || !c->force_acc) return set_err(ctx, MT_ERR_STATE, "the case has no force accumulator");
+    if (!c->h_force) {
+        MT_CUDA(ctx, cudaHostAlloc((void **)&c->h_force, 4 * sizeof(double), cudaHostAllocDefault));
+        for (int i = 0; i < 4; ++i) c->h_force[i] = 0.0;
+    }
+    MT_CUDA(ctx, cudaMemcpyAsync(c->h_force, c->force_acc, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    return MT_OK;
+}
+
+int mt_case_force_copied(mt_ctx *h, int32_t id, double *out4)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!out4) return set_err(ctx, MT_ERR_ARG, "null output");
+    if (!c->h_force) return set_err(ctx, MT_ERR_STATE, "no force copy was requested (mt_case_force_async)");
+    for (int i = 0; i < 4; ++i) out4[i] = c->h_force[i];
     return MT_OK;
 }
 

@@ -133,6 +133,7 @@ struct Case {
     std::vector<double> h_tri;   // solid surface triangles [n][3][3], coarse-cell units (mt_case_set_surface)
     double *ib_force = nullptr;  // [3 * nib] per-cell force of the last treat()
     double *force_acc = nullptr; // [4] fx, fy, fz, treat count
+    double *h_force = nullptr;   // [4] page-locked copy of force_acc (mt_case_force_async)
     int *dev_err = nullptr;
     MortonGeom geom{};
     // dense uniform path
@@ -211,7 +212,11 @@ struct Ctx {
     std::vector<Batch *> batches;
     std::string last_error;
     int64_t launches = 0;  // kernels this library launched (graph nodes count per replay)
+    // stream markers (mt_marker_record): a ring of events, slot = ticket % size
+    std::vector<cudaEvent_t> markers;
+    int64_t next_marker = 0;
 };
+constexpr int kMarkerRing = 64;
 
 // kernel launchers implemented in the .cu files
 int amr_build(Ctx &ctx, Case &c);

@@ -34,7 +34,8 @@ EXPORTS = [
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
     "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
-    "mt_case_generate", "mt_case_set_surface",
+    "mt_case_generate", "mt_case_set_surface", "mt_marker_record", "mt_marker_done", "mt_case_force_async",
+    "mt_case_force_copied",
 ]
 
 
@@ -116,7 +117,9 @@ def lib():
             "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
             "mt_batch_create": [vp, i32p], "mt_batch_destroy": [vp, i32], "mt_batch_add": [vp, i32, i32],
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
-            "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64],
+            "mt_marker_record": [vp, i64p], "mt_marker_done": [vp, i64, i32p], "mt_case_force_async": [vp, i32],
+            "mt_case_force_copied": [vp, i32, dp], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -156,6 +159,18 @@ class Context:
 
     def synchronize(self):
         self.check(lib().mt_synchronize(self.h), "mt_synchronize")
+
+    def marker(self) -> int:
+        """Ticket of the current point of the context stream (mt_marker_record)."""
+        t = C.c_int64()
+        self.check(lib().mt_marker_record(self.h, C.byref(t)), "mt_marker_record")
+        return t.value
+
+    def marker_done(self, ticket: int) -> bool:
+        """Whether the stream has passed the marker (never blocks)."""
+        d = C.c_int32()
+        self.check(lib().mt_marker_done(self.h, int(ticket), C.byref(d)), "mt_marker_done")
+        return bool(d.value)
 
     def launch_count(self) -> int:
         v = C.c_int64()
@@ -398,6 +413,16 @@ class LBM_Manager:
     def force(self):
         out = np.zeros(4)
         self.ctx.check(lib().mt_get_force(self.ctx.h, self.id, _ptr(out, C.c_double)), "get_force")
+        return out
+
+    def force_async(self):
+        """Enqueue a copy of the accumulated force (read it with force_copied
+        once a marker recorded after this call is done)."""
+        self.ctx.check(lib().mt_case_force_async(self.ctx.h, self.id), "mt_case_force_async")
+
+    def force_copied(self):
+        out = np.zeros(4)
+        self.ctx.check(lib().mt_case_force_copied(self.ctx.h, self.id, _ptr(out, C.c_double)), "mt_case_force_copied")
         return out
 
     def reset_force(self):

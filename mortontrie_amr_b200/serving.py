@@ -162,7 +162,11 @@ def footprint_bytes(case, storage: str) -> int:
 
 
 def drag_lift(mgr, req: Request) -> tuple:
-    f = mgr.force()
+    return drag_lift_of(mgr.force(), req)
+
+
+def drag_lift_of(f, req: Request) -> tuple:
+    """Mean drag and lift coefficients from an accumulated force (fx, fy, fz, count)."""
     n = max(f[3], 1.0)
     u = U_INLET
     d = 2.0 * req.radius * (1 << req.levels)
@@ -211,7 +215,7 @@ class ServerStats:
     chunks: int = 0
     admit_s: float = 0.0    # host time creating and building admitted cases
     step_s: float = 0.0     # host time issuing batch steps (graph capture included)
-    drain_s: float = 0.0    # host time waiting for finished cases and reading results
+    drain_s: float = 0.0    # host time waiting for the device (queue full, no arrival) and releasing memory
 
     def summary(self) -> dict:
         lat = np.array([r.latency for r in self.results]) if self.results else np.zeros(1)
@@ -224,18 +228,29 @@ class ServerStats:
 
 
 class Server:
-    """Continuous-batching request loop on one device context."""
+    """Continuous-batching request loop on one device context.
+
+    The loop never synchronises the context while it runs: it keeps at most
+    `max_inflight` batch chunks queued on the device (stream markers tell it
+    when one has passed), admits arrivals while the device works, and learns
+    that a finished request's result is ready from a marker recorded after an
+    asynchronous copy of its force.  A finished case leaves the batch at once
+    but keeps its memory until the budget needs it (releasing device memory
+    waits for the whole device)."""
 
     def __init__(self, ctx, cache: TemplateCache, storage: str = "f16", budget_gb: float = 150.0,
-                 chunk: int = 16, scaling: str = "standard"):
+                 chunk: int = 16, scaling: str = "standard", max_inflight: int = 2):
         self.ctx = ctx
         self.cache = cache
         self.storage = storage
         self.budget = int(budget_gb * 1e9)
         self.chunk = chunk
         self.scaling = scaling
+        self.max_inflight = max_inflight
 
     def run(self, requests, realtime: bool = True, clock=None) -> ServerStats:
+        from collections import deque
+
         from .lbm import Batch, Context, LBM_Manager
         stats = ServerStats()
         # admitted cases are built on a context of their own, so that the
@@ -243,20 +258,42 @@ class Server:
         builder = Context(self.ctx.device)
         pending = sorted(requests, key=lambda r: r.arrival)
         batch = Batch(self.ctx)
-        live = {}    # rid -> [mgr, req, remaining, admitted, bytes]
+        live = {}        # rid -> [mgr, req, remaining, admitted, bytes]
+        finishing = []   # [marker, mgr, req, admitted, bytes]: force copy queued
+        closing = []     # [mgr, bytes]: results read, memory not yet released
+        inflight = deque()
         used = 0
         t0 = time.perf_counter() if clock is None else clock()
         now = (lambda: time.perf_counter() - t0) if clock is None else (lambda: clock() - t0)
         qi = 0
-        while qi < len(pending) or live:
+        while qi < len(pending) or live or finishing:
+            progressed = False
+            # results whose copies have landed
+            for ent in list(finishing):
+                if self.ctx.marker_done(ent[0]):
+                    _, mgr, req, adm, need = ent
+                    cd, cl = drag_lift_of(mgr.force_copied(), req)
+                    stats.results.append(Result(rid=req.rid, arrival=req.arrival, admitted=adm, finished=now(),
+                                                cd=cd, cl=cl, coarse_steps=req.coarse_steps(), storage=self.storage))
+                    finishing.remove(ent)
+                    closing.append([mgr, need])
+                    progressed = True
+            # admit arrivals as memory allows (oldest first)
             t = now() if realtime else float("inf")
-            # admit arrivals as memory frees up (oldest first)
             while qi < len(pending) and pending[qi].arrival <= t:
                 req = pending[qi]
                 case = request_case(req, self.cache.get(req))
                 need = footprint_bytes(case, self.storage)
-                if live and used + need > self.budget:
-                    break
+                if (live or finishing or closing) and used + need > self.budget:
+                    if not closing:
+                        break
+                    td = time.perf_counter()
+                    for mgr, nb in closing:
+                        mgr.close()
+                        used -= nb
+                    closing = []
+                    stats.drain_s += time.perf_counter() - td
+                    continue
                 ta = time.perf_counter()
                 mgr = LBM_Manager(builder, case, self.storage, schedule="fused", scaling=self.scaling)
                 mgr.prepare()
@@ -266,34 +303,36 @@ class Server:
                 live[req.rid] = [mgr, req, req.coarse_steps(), now(), need]
                 used += need
                 qi += 1
+                progressed = True
             stats.max_resident = max(stats.max_resident, len(live))
             stats.max_bytes = max(stats.max_bytes, used)
-            if not live:
-                if qi < len(pending) and realtime:
-                    time.sleep(max(0.0, min(pending[qi].arrival - now(), 0.05)))
-                continue
-            k = min(self.chunk, min(v[2] for v in live.values()))
-            ts = time.perf_counter()
-            batch.step(k)
-            stats.step_s += time.perf_counter() - ts
-            stats.chunks += 1
-            for v in live.values():
-                v[2] -= k
-            done = [rid for rid, v in live.items() if v[2] == 0]
-            if done:
-                td = time.perf_counter()
-                self.ctx.synchronize()
-                for rid in done:
+            # issue the next chunk while the device queue has room
+            while inflight and self.ctx.marker_done(inflight[0]):
+                inflight.popleft()
+            if live and len(inflight) < self.max_inflight:
+                k = min(self.chunk, min(v[2] for v in live.values()))
+                ts = time.perf_counter()
+                batch.step(k)
+                inflight.append(self.ctx.marker())
+                stats.step_s += time.perf_counter() - ts
+                stats.chunks += 1
+                for v in live.values():
+                    v[2] -= k
+                for rid in [rid for rid, v in live.items() if v[2] == 0]:
                     mgr, req, _, adm, need = live.pop(rid)
-                    cd, cl = drag_lift(mgr, req)
-                    stats.results.append(Result(rid=rid, arrival=req.arrival, admitted=adm, finished=now(), cd=cd,
-                                                cl=cl, coarse_steps=req.coarse_steps(), storage=self.storage))
+                    mgr.force_async()
+                    finishing.append([self.ctx.marker(), mgr, req, adm, need])
                     batch.remove(mgr)
-                    mgr.close()
-                    used -= need
+                continue
+            if not progressed:
+                # wait for the device or the next arrival
+                td = time.perf_counter()
+                time.sleep(0.0005)
                 stats.drain_s += time.perf_counter() - td
         self.ctx.synchronize()
         stats.wall_s = now()
+        for mgr, _ in closing:
+            mgr.close()
         batch.close()
         builder.close()
         return stats
@@ -313,3 +352,23 @@ def solve_alone(ctx, cache: TemplateCache, req: Request, storage: str = "f16", s
     dt = time.perf_counter() - t
     mgr.close()
     return cd, cl, dt
+
+
+def plain_solve_seconds(ctx, cache: TemplateCache, req: Request, sample: int = 8) -> float:
+    """Wall time of one request solved alone in the plain form (FP64, the
+    reference's phase order): set-up, then 1/`sample` of its coarse steps
+    (at least 2) timed and scaled to all of them (the per-step cost of a
+    case is constant)."""
+    from .lbm import LBM_Manager
+    case = request_case(req, cache.get(req))
+    t = time.perf_counter()
+    mgr = LBM_Manager(ctx, case, "f64", schedule="phases", scaling="standard")
+    ctx.synchronize()
+    t_build = time.perf_counter() - t
+    k = max(2, req.coarse_steps() // sample)
+    t = time.perf_counter()
+    mgr.fluidSimulate(k)
+    ctx.synchronize()
+    per = (time.perf_counter() - t) / k
+    mgr.close()
+    return t_build + per * req.coarse_steps()

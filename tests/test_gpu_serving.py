@@ -55,3 +55,30 @@ def test_budget_limits_residency(ctx):
     server = Server(ctx, cache, storage="f16", budget_gb=1.5 * small / 1e9, chunk=4)
     stats = server.run(reqs, realtime=False)
     assert len(stats.results) == 3 and stats.max_resident == 1
+
+
+def test_markers_and_async_force(ctx):
+    """A marker recorded after queued steps turns done once the stream passes
+    it, without synchronising; the force copied asynchronously before it
+    equals the synchronous read; tickets older than the marker ring read as
+    done."""
+    import time
+    from mortontrie_amr_b200.serving import Request, TemplateCache, request_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    req = Request(rid=0, arrival=0.0, radius=3.3, levels=2, re=80.0, oscillating=True, finest_steps=64)
+    mgr = LBM_Manager(ctx, request_case(req, TemplateCache().get(req)), "f16", schedule="fused")
+    first = ctx.marker()
+    mgr.fluidSimulate(16)
+    mgr.force_async()
+    tk = ctx.marker()
+    assert tk > first
+    t0 = time.time()
+    while not ctx.marker_done(tk):
+        assert time.time() - t0 < 60.0
+        time.sleep(0.001)
+    assert np.array_equal(mgr.force_copied(), mgr.force())
+    assert mgr.force()[3] > 0
+    for _ in range(70):
+        ctx.marker()
+    assert ctx.marker_done(first)
+    mgr.close()
