@@ -94,6 +94,11 @@ const char *mt_last_error(const mt_ctx *ctx);
 /* run all work of this context on a caller-owned cudaStream_t (NULL: own stream) */
 int mt_set_stream(mt_ctx *ctx, void *cuda_stream);
 int mt_synchronize(mt_ctx *ctx);
+/* Give the context's own stream the device's highest (high != 0) or lowest
+ * scheduling priority (no reference counterpart): a context that builds
+ * cases while another runs long batches gets its short kernels scheduled
+ * first.  Synchronises the context; MT_ERR_STATE on a caller's stream. */
+int mt_set_priority(mt_ctx *ctx, int32_t high);
 /* kernels launched by this context so far (graph replays count their nodes) */
 int mt_launch_count(const mt_ctx *ctx, int64_t *out);
 

@@ -142,6 +142,22 @@ int mt_destroy(mt_ctx *h)
     return MT_OK;
 }
 
+int mt_set_priority(mt_ctx *h, int32_t high)
+{
+    if (!h) return MT_ERR_ARG;
+    Ctx &ctx = h->c;
+    if (!ctx.own_stream) return set_err(ctx, MT_ERR_STATE, "the context runs on a caller's stream");
+    MT_CUDA(ctx, cudaSetDevice(ctx.device));
+    int lo = 0, hi = 0;
+    MT_CUDA(ctx, cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    cudaStream_t s = nullptr;
+    MT_CUDA(ctx, cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, high ? hi : lo));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    cudaStreamDestroy(ctx.stream);
+    ctx.stream = s;
+    return MT_OK;
+}
+
 int mt_marker_record(mt_ctx *h, int64_t *ticket)
 {
     if (!h || !ticket) return MT_ERR_ARG;

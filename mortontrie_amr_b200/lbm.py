@@ -35,7 +35,7 @@ EXPORTS = [
     "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
     "mt_case_generate", "mt_case_set_surface", "mt_marker_record", "mt_marker_done", "mt_case_force_async",
-    "mt_case_force_copied",
+    "mt_case_force_copied", "mt_set_priority",
 ]
 
 
@@ -119,7 +119,7 @@ def lib():
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
             "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64],
             "mt_marker_record": [vp, i64p], "mt_marker_done": [vp, i64, i32p], "mt_case_force_async": [vp, i32],
-            "mt_case_force_copied": [vp, i32, dp], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_case_force_copied": [vp, i32, dp], "mt_set_priority": [vp, i32], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -159,6 +159,10 @@ class Context:
 
     def synchronize(self):
         self.check(lib().mt_synchronize(self.h), "mt_synchronize")
+
+    def set_priority(self, high: bool = True):
+        """Highest (or lowest) scheduling priority for the context's own stream."""
+        self.check(lib().mt_set_priority(self.h, int(bool(high))), "mt_set_priority")
 
     def marker(self) -> int:
         """Ticket of the current point of the context stream (mt_marker_record)."""

@@ -239,8 +239,9 @@ class Server:
     waits for the whole device)."""
 
     def __init__(self, ctx, cache: TemplateCache, storage: str = "f16", budget_gb: float = 150.0,
-                 chunk: int = 16, scaling: str = "standard", max_inflight: int = 2):
+                 chunk: int = 16, scaling: str = "standard", max_inflight: int = 2, priority_builds: bool = True):
         self.ctx = ctx
+        self.priority_builds = priority_builds
         self.cache = cache
         self.storage = storage
         self.budget = int(budget_gb * 1e9)
@@ -256,6 +257,9 @@ class Server:
         # admitted cases are built on a context of their own, so that the
         # build's synchronisations do not wait for the batch's queued steps
         builder = Context(self.ctx.device)
+        if self.priority_builds:
+            # the builds' short kernels are scheduled ahead of the batch's
+            builder.set_priority(True)
         pending = sorted(requests, key=lambda r: r.arrival)
         batch = Batch(self.ctx)
         live = {}        # rid -> [mgr, req, remaining, admitted, bytes]
