@@ -151,6 +151,22 @@ int mt_case_set_surface(mt_ctx *ctx, int32_t case_id, const double *tri, int64_t
  * mt_case_set_dis and mt_case_build); MT_ERR_MESH with the host mesher's
  * messages when the boxes or the sphere break the contract */
 int mt_case_generate(mt_ctx *ctx, int32_t case_id, const mt_mesh_spec *spec);
+/* Carry the state of case src onto case dst, a lattice of the same model
+ * (Q, levels, level-0 extent) built from other refinement boxes: moving the
+ * refinement with a body (the reference's dynamic remeshing,
+ * Grid_Manager_dynamic.cpp, is not compiled in; no counterpart in its step).
+ * Each cell of dst takes f and fcol from src: the same key on the same level
+ * as they are (bit for bit); else from its ancestor on the nearest coarser
+ * level holding one, the non-equilibrium part rescaled as an explosion; else
+ * from the mean of its descendants on the nearest finer level holding any,
+ * rescaled as a coalescence; else the equilibrium
+ * (rho0, u_bc).  Solid cells of dst hold zeros; a fluid cell of dst that is
+ * solid in src takes the equilibrium at rest.  The interface factors are
+ * dst's.  dst's direct-forcing step
+ * counter follows src's (markers are dst's own).  counts (nullable) receives
+ * [4 * level + kind] cells of each kind 0..3 in that order.  Neither case may
+ * be in a batch. */
+int mt_case_remap(mt_ctx *ctx, int32_t dst_case, int32_t src_case, int64_t *counts);
 /* device build: radix sort + unique of the keys, set tags, neighbour table
  * by binary search of the Morton neighbour keys (Morton_Assist::find_neighbor
  * + D_map_define::find), explosion/coalescence child tables, IB list */

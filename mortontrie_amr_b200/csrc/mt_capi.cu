@@ -446,6 +446,24 @@ int mt_case_generate(mt_ctx *h, int32_t id, const mt_mesh_spec *sp)
     return MT_OK;
 }
 
+int mt_case_remap(mt_ctx *h, int32_t dst_id, int32_t src_id, int64_t *counts)
+{
+    Case *d, *s;
+    int rc = get_case(h, dst_id, &d);
+    if (rc) return rc;
+    if ((rc = get_case(h, src_id, &s))) return rc;
+    Ctx &ctx = h->c;
+    if (d == s) return set_err(ctx, MT_ERR_ARG, "remap needs two cases");
+    if (d->dense || s->dense || !d->built || !s->built) return set_err(ctx, MT_ERR_STATE, "remap needs two built multi-level cases");
+    if (d->d.q != s->d.q || d->d.max_level != s->d.max_level)
+        return set_err(ctx, MT_ERR_ARG, "remap needs the same lattice (Q) and level count");
+    for (int a = 0; a < 3; ++a)
+        if (d->d.extent0[a] != s->d.extent0[a]) return set_err(ctx, MT_ERR_ARG, "remap needs the same level-0 extent");
+    if (d->in_batch || s->in_batch) return set_err(ctx, MT_ERR_STATE, "remap of a batch member");
+    MT_CUDA(ctx, cudaSetDevice(ctx.device));
+    return amr_remap(ctx, *d, *s, counts);
+}
+
 int mt_case_level_size(mt_ctx *h, int32_t id, int32_t level, int64_t *n)
 {
     Case *c;

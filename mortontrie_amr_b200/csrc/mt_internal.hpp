@@ -222,6 +222,8 @@ constexpr int kMarkerRing = 64;
 int amr_build(Ctx &ctx, Case &c);
 // device lattice classification: raw sets of every level and the dis table
 int amr_generate(Ctx &ctx, Case &c, const mt_mesh_spec &spec);
+// the state of src carried onto dst's lattice (counts: [4 * level + kind] or null)
+int amr_remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts);
 int amr_init_equilibrium(Ctx &ctx, Case &c, double rho0, const double *u0);
 int amr_lbm_kernel(Ctx &ctx, Case &c, int level);
 int amr_step(Ctx &ctx, Case &c, int n);

@@ -35,7 +35,7 @@ EXPORTS = [
     "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
     "mt_case_generate", "mt_case_set_surface", "mt_marker_record", "mt_marker_done", "mt_case_force_async",
-    "mt_case_force_copied", "mt_set_priority",
+    "mt_case_force_copied", "mt_set_priority", "mt_case_remap",
 ]
 
 
@@ -119,7 +119,7 @@ def lib():
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
             "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64],
             "mt_marker_record": [vp, i64p], "mt_marker_done": [vp, i64, i32p], "mt_case_force_async": [vp, i32],
-            "mt_case_force_copied": [vp, i32, dp], "mt_set_priority": [vp, i32], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_case_force_copied": [vp, i32, dp], "mt_set_priority": [vp, i32], "mt_case_remap": [vp, i32, i32, i64p], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -231,6 +231,7 @@ class LBM_Manager:
         self.case = case
         self.q = case.params.q
         self.L = case.mesh.spec.max_level
+        self.storage = storage
         d = make_desc(case, storage)
         cid = C.c_int32()
         ctx.check(lib().mt_case_create(ctx.h, C.byref(d), C.byref(cid)), "mt_case_create")
@@ -418,6 +419,23 @@ class LBM_Manager:
         out = np.zeros(4)
         self.ctx.check(lib().mt_get_force(self.ctx.h, self.id, _ptr(out, C.c_double)), "get_force")
         return out
+
+    def remap_from(self, src: "LBM_Manager"):
+        """Carry src's state onto this case's lattice (mt_case_remap); returns
+        the cells per level that were copied, exploded from a parent,
+        coalesced from children, or set to equilibrium ((L+1, 4) array)."""
+        counts = np.zeros(4 * (self.L + 1), np.int64)
+        self.ctx.check(lib().mt_case_remap(self.ctx.h, self.id, src.id, _ptr(counts, C.c_int64)), "mt_case_remap")
+        return counts.reshape(self.L + 1, 4)
+
+    def remeshed(self, case: Case, storage: str = None, schedule: str = None) -> "LBM_Manager":
+        """A new case on `case`'s lattice (other refinement boxes, a moved
+        body's band or markers) carrying this case's state; this case is left
+        as it is (close it when done)."""
+        new = LBM_Manager(self.ctx, case, storage or self.storage, schedule=schedule or self.schedule,
+                          scaling=self.scaling)
+        new.remap_from(self)
+        return new
 
     def force_async(self):
         """Enqueue a copy of the accumulated force (read it with force_copied
