@@ -280,6 +280,12 @@ def run_ours(args):
             batched = batched_section(ctx, torch)
         except Exception as exc:
             batched = {"error": repr(exc)}
+    moving = None
+    if not args.no_moving and world == 1:
+        try:
+            moving = moving_section(ctx, torch)
+        except Exception as exc:
+            moving = {"error": repr(exc)}
 
     if rank == 0:
         cpu = cpu_baseline_sample() if (world == 1 and not args.no_cpu_baseline) else None
@@ -304,6 +310,7 @@ def run_ours(args):
             "amr_cumulant_sphere": amr,
             "batched_uneven": batched,
             "served_mix": served,
+            "moving_refinement": moving,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -534,6 +541,61 @@ def served_case_section(ctx, torch, steps=10, warmup=2):
     return out
 
 
+def moving_section(ctx, torch, steps=250, window=16, radius=8, max_level=3, re=100.0):
+    """An oscillating direct-forcing sphere (R = 8 coarse cells, 3
+    refinement levels, amplitude R/2, one period = 2000 finest = 250 coarse
+    steps, FP16) on the static mesh whose finest box and forcing band cover
+    the whole swept path, and with the refinement moving with the sphere
+    (re-meshed every `window` coarse steps on the device, state carried by
+    mt_case_remap).  Wall time per coarse step (re-meshing included), cells
+    of the finest level and of the band, and the mean drag and lift of both
+    runs."""
+    from mortontrie_amr_b200.case import df_sphere_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    from mortontrie_amr_b200.moving import MovingSphere
+    from mortontrie_amr_b200.serving import AMPLITUDE, PERIOD, U_INLET
+    kw = dict(radius=radius, max_level=max_level, re=re, u=U_INLET, amplitude=AMPLITUDE, period=PERIOD)
+    d = 2.0 * radius * (1 << max_level)
+    area = np.pi * d * d / 4.0
+
+    def coeffs(f):
+        n = max(f[3], 1.0)
+        return [float(2.0 * f[a] / n / (U_INLET ** 2 * area)) for a in (0, 1)]
+
+    out = {"workload": f"oscillating DF sphere R={radius}, {max_level} refinement levels, Re {re:g}, u {U_INLET:g}, "
+                       f"{steps} coarse steps (one period), FP16", "window_coarse_steps": window}
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    st = LBM_Manager(ctx, df_sphere_case(oscillating=True, mesh="device", **kw), "f16", schedule="fused",
+                     scaling="standard")
+    st.fluidSimulate(steps)
+    torch.cuda.synchronize()
+    ws = time.perf_counter() - t
+    fine_s = st.size(max_level)
+    band_s = int(np.count_nonzero(st.keys(max_level)[1] & 256))
+    cs = coeffs(st.force())
+    st.close()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    mv = MovingSphere(ctx, storage="f16", window=window, **kw)
+    mv.step(steps)
+    torch.cuda.synchronize()
+    wm = time.perf_counter() - t
+    fine_m = mv.mgr.size(max_level)
+    band_m = int(np.count_nonzero(mv.mgr.keys(max_level)[1] & 256))
+    cm = coeffs(mv.total_force())
+    out["static"] = {"ms_per_coarse_step": round(1e3 * ws / steps, 3), "finest_cells": fine_s, "band_cells": band_s,
+                     "cd": cs[0], "cl": cs[1]}
+    out["moving"] = {"ms_per_coarse_step": round(1e3 * wm / steps, 3), "finest_cells": fine_m, "band_cells": band_m,
+                     "cd": cm[0], "cl": cm[1], "windows": mv.windows, "remesh_s": round(mv.remesh_s, 2),
+                     "remesh_median_s": {k: round(float(np.median([t[i] for t in mv.remesh_times])), 4)
+                                         for i, k in enumerate(("build", "remap", "release"))}}
+    out["speedup"] = round(ws / wm, 3)
+    out["cd_rel_diff"] = float(abs(cm[0] - cs[0]) / max(abs(cs[0]), 1e-30))
+    mv.close()
+    return out
+
+
 def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=16):
     """Served mix: a seeded Poisson stream (rate 20/s for `duration` s) of
     direct-forcing sphere flows (R in [3, 8], 16R x 8R x 8R, 1-3 refinement
@@ -735,6 +797,8 @@ def main():
     ap.add_argument("--served-only", type=float, default=0.0, metavar="SECONDS",
                     help="only the served mix, with SECONDS of Poisson arrivals")
     ap.add_argument("--batched-only", action="store_true", help="only the batched uneven instances section")
+    ap.add_argument("--no-moving", action="store_true", help="skip the moving-refinement section")
+    ap.add_argument("--moving-only", action="store_true", help="only the moving-refinement section")
     ap.add_argument("--served-case", action="store_true",
                     help="only the largest served request alone (profiling driver of the forcing kernels)")
     ap.add_argument("--amr-variants", default=None,
@@ -763,6 +827,16 @@ def main():
         ctx = Context(0)
         ctx.set_stream(stream.cuda_stream)
         print(json.dumps({"served_mix": served_section(ctx, torch, duration=args.served_only)}), flush=True)
+        ctx.close()
+    elif args.moving_only:
+        import torch
+
+        from mortontrie_amr_b200.lbm import Context
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx = Context(0)
+        ctx.set_stream(stream.cuda_stream)
+        print(json.dumps({"moving_refinement": moving_section(ctx, torch)}), flush=True)
         ctx.close()
     elif args.served_case:
         import torch

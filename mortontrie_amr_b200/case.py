@@ -8,13 +8,14 @@ the reference hard-codes in LBM_Manager's constructor
 """
 from __future__ import annotations
 
+import dataclasses
 from dataclasses import dataclass, field
 from typing import Optional
 
 import numpy as np
 
 from .lattice import directions, reference_units, weights
-from .mesh import Mesh, MeshSpec, Sphere, build_mesh, spec_mesh
+from .mesh import Mesh, MeshSpec, Sphere, build_mesh, spec_mesh, sphere_markers
 
 COLLISIONS = {"LBGK": 0, "Cumulant": 1}
 IB_METHODS = {"DW": 0, "FH": 1, "DF": 2}
@@ -153,24 +154,34 @@ def cavity_case(q=19, collision="LBGK", coarse=(32, 32, 32), max_level=1, re=100
 
 
 def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q=19, period=2000,
-                   amplitude=0.5, band_slack=0.0, mesh="host") -> Case:
+                   amplitude=0.5, band_slack=0.0, mesh="host", window=None) -> Case:
     """Flow past a sphere represented by direct-forcing Lagrangian markers
     (one per finest cell^2 of surface, 3-point kernel): coarse channel
     16R x 8R x 8R, inlet on West, outflow on East, periodic sides, centre at
     (4R, 4R, 4R), nested refinement boxes around the sphere and its path
     (transverse oscillation of `amplitude` R along y with `period` finest
-    steps when oscillating), nu = u 2R / Re in coarse units, D3Q19 LBGK."""
+    steps when oscillating), nu = u 2R / Re in coarse units, D3Q19 LBGK.
+    window = (y_lo, y_hi): the boxes and the forcing band cover only the
+    centre displacements in [y_lo, y_hi] (coarse cells) of the path, for a
+    refinement that moves with the body (the markers still follow the whole
+    path)."""
     r = int(radius)
     nx, ny, nz = 16 * r, 8 * r, 8 * r
-    c = (4 * r, 4 * r, 4 * r)
+    c0 = (4 * r, 4 * r, 4 * r)
     amp = amplitude * r if oscillating else 0.0
+    if window is not None:
+        mid, half = 0.5 * (window[0] + window[1]), 0.5 * (window[1] - window[0])
+        c = (c0[0], c0[1] + mid, c0[2])
+    else:
+        c, half = c0, amp
     # finest box: the band (2.7 finest cells) plus the C2F shell and a margin
     mg = max(0.5 * r, 6.0 / (1 << max_level) + 0.5)
-    hw = [r + mg, r + amp + mg, r + mg]
+    hw = [r + mg, r + half + mg, r + mg]
     boxes = []
     for _ in range(max_level):
         boxes.append(list(hw))
-        hw = [hw[0] + max(2.0, 0.5 * r), min(hw[1] + max(2.0, 0.5 * r), 4 * r - 1.0), min(hw[2] + max(2.0, 0.5 * r), 4 * r - 1.0)]
+        hw = [hw[0] + max(2.0, 0.5 * r), min(hw[1] + max(2.0, 0.5 * r), min(c[1], ny - c[1]) - 1.0),
+              min(hw[2] + max(2.0, 0.5 * r), 4 * r - 1.0)]
     boxes = boxes[::-1]  # level 0 box first
     refine = []
     for l, b in enumerate(boxes):
@@ -178,11 +189,22 @@ def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q
         refine.append((tuple(int(np.floor((c[a] - b[a]) * s)) for a in range(3)),
                        tuple(int(np.ceil((c[a] + b[a]) * s)) for a in range(3))))
     nu = u * 2.0 * r / re
+    p = CaseParams(q=q, collision="LBGK", ib_method="DF", bc_mode="zouhe_outflow", nu=nu, u_bc=(u, 0.0, 0.0),
+                   u_ref=u)
+    if window is not None:
+        # the band of the window (its displacements as a symmetric sweep
+        # about its middle); the markers of the whole path about c0
+        spec = MeshSpec(q=q, max_level=max_level, coarse=(nx, ny, nz), refine=refine,
+                        boundary=("bc", "periodic", "periodic"), sphere=Sphere(c, float(r)), ib="markers",
+                        oscillation=(half, period), band_slack=band_slack)
+        path_spec = MeshSpec(q=q, max_level=max_level, coarse=(nx, ny, nz), refine=refine,
+                             boundary=spec.boundary, sphere=Sphere(c0, float(r)), ib="markers",
+                             oscillation=(amp, period) if oscillating else None)
+        m = _mesh(spec, mesh)
+        return Case(dataclasses.replace(m, markers=sphere_markers(path_spec)), p)
     spec = MeshSpec(q=q, max_level=max_level, coarse=(nx, ny, nz), refine=refine,
                     boundary=("bc", "periodic", "periodic"), sphere=Sphere(c, float(r)), ib="markers",
                     oscillation=(amp, period) if oscillating else None, band_slack=band_slack)
-    p = CaseParams(q=q, collision="LBGK", ib_method="DF", bc_mode="zouhe_outflow", nu=nu, u_bc=(u, 0.0, 0.0),
-                   u_ref=u)
     return Case(_mesh(spec, mesh), p)
 
 

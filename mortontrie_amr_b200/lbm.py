@@ -420,13 +420,17 @@ class LBM_Manager:
         self.ctx.check(lib().mt_get_force(self.ctx.h, self.id, _ptr(out, C.c_double)), "get_force")
         return out
 
-    def remap_from(self, src: "LBM_Manager"):
+    def remap_from(self, src: "LBM_Manager", counts: bool = True):
         """Carry src's state onto this case's lattice (mt_case_remap); returns
-        the cells per level that were copied, exploded from a parent,
-        coalesced from children, or set to equilibrium ((L+1, 4) array)."""
-        counts = np.zeros(4 * (self.L + 1), np.int64)
-        self.ctx.check(lib().mt_case_remap(self.ctx.h, self.id, src.id, _ptr(counts, C.c_int64)), "mt_case_remap")
-        return counts.reshape(self.L + 1, 4)
+        the cells per level that were copied, taken from an ancestor, taken
+        from descendants, or set to equilibrium ((L+1, 4) array), or None
+        when counts is False (no read-back)."""
+        if not counts:
+            self.ctx.check(lib().mt_case_remap(self.ctx.h, self.id, src.id, None), "mt_case_remap")
+            return None
+        out = np.zeros(4 * (self.L + 1), np.int64)
+        self.ctx.check(lib().mt_case_remap(self.ctx.h, self.id, src.id, _ptr(out, C.c_int64)), "mt_case_remap")
+        return out.reshape(self.L + 1, 4)
 
     def remeshed(self, case: Case, storage: str = None, schedule: str = None) -> "LBM_Manager":
         """A new case on `case`'s lattice (other refinement boxes, a moved
@@ -434,7 +438,7 @@ class LBM_Manager:
         as it is (close it when done)."""
         new = LBM_Manager(self.ctx, case, storage or self.storage, schedule=schedule or self.schedule,
                           scaling=self.scaling)
-        new.remap_from(self)
+        new.remap_from(self, counts=False)
         return new
 
     def force_async(self):
