@@ -38,3 +38,31 @@ def test_sphere_links_and_counts():
     # West/East faces only (y and z periodic)
     assert m.lat_bc[0].size == 32 * 32 and m.lat_bc[1].size == 32 * 32
     assert sum(b.size for b in m.lat_bc[2:]) == 0
+
+
+def test_window_case_covers_its_displacements():
+    """A moving-refinement window: its band covers every marker stencil of
+    the window's path positions, it is smaller than the static swept band,
+    and its markers follow the whole path like the static case's."""
+    from mortontrie_amr_b200.case import df_sphere_case
+    from mortontrie_amr_b200.lattice import cell_coords
+    from mortontrie_amr_b200.moving import path_window
+    L, period = 2, 400
+    static = df_sphere_case(radius=3, max_level=L, oscillating=True, period=period)
+    t0, t1 = 40, 72
+    lo, hi = path_window(t0, t1, 1.5, period)
+    assert lo < hi and hi <= 1.5
+    win = df_sphere_case(radius=3, max_level=L, oscillating=True, period=period, window=(lo, hi))
+    assert win.mesh.levels[L]["ib_band"].size < static.mesh.levels[L]["ib_band"].size
+    assert np.array_equal(win.mesh.markers.path, static.mesh.markers.path)
+    assert np.array_equal(win.mesh.markers.ref, static.mesh.markers.ref)
+    bx, by, bz = cell_coords(L, L, win.mesh.levels[L]["ib_band"])
+    band = set(zip(bx.tolist(), by.tolist(), bz.tolist()))
+    mk = win.mesh.markers
+    c = np.array(mk.center)
+    for t in (t0, (t0 + t1) // 2, t1):
+        pos = c[:, None] + mk.path[t % period, :3, None] + mk.ref
+        base = np.floor(pos).astype(int)
+        for d in np.ndindex(3, 3, 3):
+            cells = base + (np.array(d) - 1)[:, None]
+            assert all(tuple(x) in band for x in cells.T[::53])
