@@ -152,7 +152,7 @@ int mt_case_set_surface(mt_ctx *ctx, int32_t case_id, const double *tri, int64_t
  * messages when the boxes or the sphere break the contract */
 int mt_case_generate(mt_ctx *ctx, int32_t case_id, const mt_mesh_spec *spec);
 /* Carry the state of case src onto case dst, a lattice of the same model
- * (Q, levels, level-0 extent) built from other refinement boxes: moving the
+ * (Q, levels, level-0 extent, storage) built from other refinement boxes: moving the
  * refinement with a body (the reference's dynamic remeshing,
  * Grid_Manager_dynamic.cpp, is not compiled in; no counterpart in its step).
  * Each cell of dst takes f and fcol from src: the same key on the same level

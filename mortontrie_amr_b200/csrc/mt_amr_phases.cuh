@@ -1689,4 +1689,211 @@ int AmrOps<S>::guard(Ctx &ctx, Case &c)
     return MT_OK;
 }
 
+// ---- remap of a state onto another lattice (mt_case_remap) ---------------
+// one population set of Q values rescaled about its own equilibrium:
+// feq(rho, u) + s (in - feq(rho, u)), rho and u from the values themselves
+template <int Q> __device__ void remap_rescale(double *v, double s)
+{
+    double r = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
+    for (int k = 0; k < Q; ++k) {
+        r += v[k];
+        jx += v[k] * ex(k);
+        jy += v[k] * ey(k);
+        jz += v[k] * ez(k);
+    }
+    const double rs = (r > -1e-6 && r < 1e-6) ? ((r < 0.0) ? -1e-6 : 1e-6) : r;
+    const double ux = jx / rs, uy = jy / rs, uz = jz / rs;
+    const double uu = ux * ux + uy * uy + uz * uz;
+    for (int k = 0; k < Q; ++k) {
+        const double eu = ex(k) * ux + ey(k) * uy + ez(k) * uz;
+        const double feq = r * w<Q>(k) * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu);
+        v[k] = feq + s * (v[k] - feq);
+    }
+}
+
+__host__ __device__ __forceinline__ uint64_t cell_key_at(int L, int l, int64_t x, int64_t y, int64_t z)
+{
+    const int sh = L - l;
+    return dilate3((uint64_t)x << sh) | (dilate3((uint64_t)y << sh) << 1) | (dilate3((uint64_t)z << sh) << 2);
+}
+
+template <class S> struct RemapLevels {
+    struct Src {
+        const uint64_t *key = nullptr;
+        const uint32_t *tag = nullptr;
+        int64_t n = 0;
+        const S *f = nullptr, *fcol = nullptr;
+    } lv[kMaxLevels];
+    // explosion factors from coarser source level m, coalescence factors
+    // from finer source level m (products over the levels crossed)
+    double up_f[kMaxLevels], up_c[kMaxLevels], down_f[kMaxLevels], down_c[kMaxLevels];
+};
+
+// Each cell of a destination level takes f and fcol from the source: the same
+// key on the same level as they are (the stored values, bit for bit); else
+// the nearest coarser source level holding its ancestor, rescaled as an
+// explosion; else the mean of its descendants on the nearest finer source
+// level holding any, rescaled as a coalescence; else the equilibrium
+// (rho0, u0).  Solid cells hold zeros (the build's convention); a fluid cell
+// that is solid in the source takes the equilibrium at rest.  kind[i]: 0..3.
+template <int Q, class S>
+__global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, int L, int l, RemapLevels<S> src,
+                        double rho0, double ux0, double uy0, double uz0, S *fo, S *co, uint8_t *kind)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nd) return;
+    const uint64_t k = dkey[i];
+    double a[Q], b[Q];
+    auto put = [&](const double *pf, const double *pc, int kd) {
+        for (int q = 0; q < Q; ++q) {
+            T::st(fo, q * nd + i, stored_of<S, Q>((C)pf[q], q));
+            T::st(co, q * nd + i, stored_of<S, Q>((C)pc[q], q));
+        }
+        kind[i] = (uint8_t)kd;
+    };
+    if (dtag[i] & TAG_SF) {
+        for (int q = 0; q < Q; ++q) a[q] = 0.0;
+        put(a, a, 0);
+        return;
+    }
+    const auto &same = src.lv[l];
+    int64_t j = same.n ? find_key(same.key, same.n, k) : -1;
+    bool uncovered = false;
+    if (j >= 0 && (same.tag[j] & TAG_SF)) {
+        uncovered = true;
+        j = -1;
+    }
+    if (j >= 0) {
+        for (int q = 0; q < Q; ++q) {
+            fo[q * nd + i] = same.f[q * same.n + j];
+            co[q * nd + i] = same.fcol[q * same.n + j];
+        }
+        kind[i] = 0;
+        return;
+    }
+    const int sh = L - l;
+    const int64_t x = (int64_t)(compact3(k) >> sh), y = (int64_t)(compact3(k >> 1) >> sh),
+                  z = (int64_t)(compact3(k >> 2) >> sh);
+    for (int m = l - 1; m >= 0 && !uncovered; --m) {
+        const auto &cs = src.lv[m];
+        if (!cs.n) continue;
+        const int up = l - m;
+        const int64_t jm = find_key(cs.key, cs.n, cell_key_at(L, m, x >> up, y >> up, z >> up));
+        if (jm < 0) continue;
+        for (int q = 0; q < Q; ++q) {
+            a[q] = (double)full_of<S, Q>(T::ld(cs.f, q * cs.n + jm), q);
+            b[q] = (double)full_of<S, Q>(T::ld(cs.fcol, q * cs.n + jm), q);
+        }
+        remap_rescale<Q>(a, src.up_f[m]);
+        remap_rescale<Q>(b, src.up_c[m]);
+        put(a, b, 1);
+        return;
+    }
+    for (int d = 1; l + d <= L && !uncovered; ++d) {
+        const auto &fine = src.lv[l + d];
+        if (!fine.n) continue;
+        const int side = 1 << d;
+        int nch = 0;
+        for (int q = 0; q < Q; ++q) a[q] = b[q] = 0.0;
+        for (int c = 0; c < side * side * side; ++c) {
+            const int64_t cx = (x << d) + c % side, cy = (y << d) + (c / side) % side, cz = (z << d) + c / (side * side);
+            const int64_t jc = find_key(fine.key, fine.n, cell_key_at(L, l + d, cx, cy, cz));
+            if (jc < 0 || (fine.tag[jc] & TAG_SF)) continue;
+            for (int q = 0; q < Q; ++q) {
+                a[q] += (double)full_of<S, Q>(T::ld(fine.f, q * fine.n + jc), q);
+                b[q] += (double)full_of<S, Q>(T::ld(fine.fcol, q * fine.n + jc), q);
+            }
+            ++nch;
+        }
+        if (!nch) continue;
+        for (int q = 0; q < Q; ++q) {
+            a[q] /= nch;
+            b[q] /= nch;
+        }
+        remap_rescale<Q>(a, src.down_f[l + d]);
+        remap_rescale<Q>(b, src.down_c[l + d]);
+        put(a, b, 2);
+        return;
+    }
+    if (uncovered) ux0 = uy0 = uz0 = 0.0;
+    const double uu = ux0 * ux0 + uy0 * uy0 + uz0 * uz0;
+    for (int q = 0; q < Q; ++q) {
+        const double eu = ex(q) * ux0 + ey(q) * uy0 + ez(q) * uz0;
+        a[q] = rho0 * w<Q>(q) * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu);
+    }
+    put(a, a, 3);
+}
+
+template <class S>
+int AmrOps<S>::remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts)
+{
+    const int L = dst.d.max_level, Q = dst.d.q;
+    RemapLevels<S> rl;
+    for (int m = 0; m <= L && m <= src.d.max_level; ++m) {
+        if (!src.lv[m].n) continue;
+        rl.lv[m].key = src.lv[m].key;
+        rl.lv[m].tag = src.lv[m].tag;
+        rl.lv[m].n = src.lv[m].n;
+        rl.lv[m].f = (const S *)src.lv[m].f;
+        rl.lv[m].fcol = (const S *)src.lv[m].fcol;
+    }
+    // the interface factors of dst: the reference's (the same on f and
+    // fcol), or the stress-continuous ones (tau on f, tau - 1 on fcol)
+    const bool st = dst.scaling == MT_SCALE_STANDARD;
+    auto c2f = [&](int fine, bool col) {
+        const double tf = dst.d.tau[fine], tc = dst.d.tau[fine - 1];
+        if (!st) return (2.0 * tf) / tc;
+        return col ? (tf - 1.0) / (2.0 * (tc - 1.0)) : tf / (2.0 * tc);
+    };
+    uint8_t *kind = nullptr;
+    int64_t maxn = 0;
+    for (int l = 0; l <= L; ++l) maxn = std::max(maxn, dst.lv[l].n);
+    MT_CUDA(ctx, cudaMallocAsync(&kind, std::max<int64_t>(maxn, 1), ctx.stream));
+    int rc = MT_OK;
+    for (int l = 0; l <= L && !rc; ++l) {
+        Level &lv = dst.lv[l];
+        if (counts)
+            for (int k = 0; k < 4; ++k) counts[4 * l + k] = 0;
+        if (!lv.n) continue;
+        for (int m = 0; m < kMaxLevels; ++m) rl.up_f[m] = rl.up_c[m] = rl.down_f[m] = rl.down_c[m] = 1.0;
+        for (int m = l - 1; m >= 0; --m)
+            for (int j = m + 1; j <= l; ++j) {
+                rl.up_f[m] *= c2f(j, false);
+                rl.up_c[m] *= c2f(j, true);
+            }
+        for (int m = l + 1; m <= L; ++m)
+            for (int j = l + 1; j <= m; ++j) {
+                rl.down_f[m] /= c2f(j, false);
+                rl.down_c[m] /= c2f(j, true);
+            }
+        const double r0 = dst.d.rho0, u0 = dst.d.u_bc[0], u1 = dst.d.u_bc[1], u2 = dst.d.u_bc[2];
+        if (Q == 19)
+            k_remap<19, S><<<grid_for(lv.n, 128), 128, 0, ctx.stream>>>(lv.key, lv.tag, lv.n, L, l, rl, r0, u0, u1, u2,
+                                                                       (S *)lv.f, (S *)lv.fcol, kind);
+        else
+            k_remap<27, S><<<grid_for(lv.n, 128), 128, 0, ctx.stream>>>(lv.key, lv.tag, lv.n, L, l, rl, r0, u0, u1, u2,
+                                                                       (S *)lv.f, (S *)lv.fcol, kind);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            rc = set_err(ctx, MT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+            break;
+        }
+        ctx.launches++;
+        if (counts) {
+            std::vector<uint8_t> hk((size_t)lv.n);
+            e = cudaMemcpyAsync(hk.data(), kind, lv.n, cudaMemcpyDeviceToHost, ctx.stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx.stream);
+            if (e != cudaSuccess) {
+                rc = set_err(ctx, MT_ERR_CUDA, std::string("remap counts: ") + cudaGetErrorString(e));
+                break;
+            }
+            for (uint8_t v : hk) counts[4 * l + (v & 3)] += 1;
+        }
+    }
+    cudaFreeAsync(kind, ctx.stream);
+    return rc;
+}
+
 }  // namespace mt

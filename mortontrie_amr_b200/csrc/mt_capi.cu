@@ -114,6 +114,15 @@ int mt_create(int32_t device, mt_ctx **out)
         return MT_ERR_CUDA;
     }
     h->c.own_stream = true;
+    // stream-ordered allocations of case builds and re-meshes keep their
+    // memory in the device's pool between builds instead of returning it at
+    // every synchronisation (re-mapping it costs more than the build)
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     *out = h;
     return MT_OK;
 }
@@ -455,8 +464,8 @@ int mt_case_remap(mt_ctx *h, int32_t dst_id, int32_t src_id, int64_t *counts)
     Ctx &ctx = h->c;
     if (d == s) return set_err(ctx, MT_ERR_ARG, "remap needs two cases");
     if (d->dense || s->dense || !d->built || !s->built) return set_err(ctx, MT_ERR_STATE, "remap needs two built multi-level cases");
-    if (d->d.q != s->d.q || d->d.max_level != s->d.max_level)
-        return set_err(ctx, MT_ERR_ARG, "remap needs the same lattice (Q) and level count");
+    if (d->d.q != s->d.q || d->d.max_level != s->d.max_level || d->d.storage != s->d.storage)
+        return set_err(ctx, MT_ERR_ARG, "remap needs the same lattice (Q), level count and storage");
     for (int a = 0; a < 3; ++a)
         if (d->d.extent0[a] != s->d.extent0[a]) return set_err(ctx, MT_ERR_ARG, "remap needs the same level-0 extent");
     if (d->in_batch || s->in_batch) return set_err(ctx, MT_ERR_STATE, "remap of a batch member");

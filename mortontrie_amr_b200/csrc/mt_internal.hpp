@@ -253,6 +253,8 @@ template <class S> struct AmrOps {
     static int guard(Ctx &ctx, Case &c);
     // batched brick pass (descriptor in device memory, total bricks known on the host)
     static int batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total);
+    // src's state carried onto dst's lattice (same Q, levels, storage)
+    static int remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts);
 };
 void amr_free(Case &c);
 // forget the fused schedule's graphs and brick tables (rebuilt at the next fused step)

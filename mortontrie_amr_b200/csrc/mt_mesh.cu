@@ -616,227 +616,21 @@ int surface_tables(Ctx &ctx, const std::vector<double> &h_tri, int L, const Box 
     return MT_OK;
 }
 
-// ---- remap of a state onto another lattice (mt_case_remap) ---------------
-// one population set of Q values rescaled about its own equilibrium:
-// feq(rho, u) + s (in - feq(rho, u)), rho and u from the values themselves
-template <int Q> __device__ void eq_rescale(const double *in, double s, double *out)
-{
-    double r = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
-    for (int k = 0; k < Q; ++k) {
-        r += in[k];
-        jx += in[k] * ex(k);
-        jy += in[k] * ey(k);
-        jz += in[k] * ez(k);
-    }
-    const double rs = (r > -1e-6 && r < 1e-6) ? ((r < 0.0) ? -1e-6 : 1e-6) : r;
-    const double ux = jx / rs, uy = jy / rs, uz = jz / rs;
-    const double uu = ux * ux + uy * uy + uz * uz;
-    for (int k = 0; k < Q; ++k) {
-        const double eu = ex(k) * ux + ey(k) * uy + ez(k) * uz;
-        const double feq = r * w<Q>(k) * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu);
-        out[k] = feq + s * (in[k] - feq);
-    }
-}
-
-struct RemapSrc {
-    const uint64_t *key = nullptr;
-    const uint32_t *tag = nullptr;
-    int64_t n = 0;
-    const double *f = nullptr, *fcol = nullptr;  // FP64 [Q][n]
-};
-struct RemapLevels {
-    RemapSrc lv[kMaxLevels];
-    // explosion factors from source level m to the destination level (products over the levels crossed)
-    double up_f[kMaxLevels], up_c[kMaxLevels];
-    // coalescence factors from source level m (finer) to the destination level
-    double down_f[kMaxLevels], down_c[kMaxLevels];
-};
-
-// each cell of a destination level takes its populations (f and fcol) from
-// the source: the same key on the same level as they are; else the nearest
-// coarser source level holding its ancestor, rescaled as an explosion
-// (up_f on f, up_c on fcol); else the mean of its descendants on the nearest
-// finer source level holding any, rescaled as a coalescence (down_f,
-// down_c); else the equilibrium (rho0, u0).
-// kind[i] records which (0..3).  Solid cells hold zeros (the build's
-// convention); a fluid cell that was solid in the source (the body moved away)
-// takes the equilibrium (rho0, 0).
-template <int Q>
-__global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, int L, int l, RemapLevels src,
-                        double rho0, double ux0, double uy0, double uz0, double *fo, double *co, uint8_t *kind)
-{
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= nd) return;
-    const uint64_t k = dkey[i];
-    if (dtag[i] & TAG_SF) {
-        for (int q = 0; q < Q; ++q) fo[q * nd + i] = co[q * nd + i] = 0.0;
-        kind[i] = 0;
-        return;
-    }
-    const RemapSrc &same = src.lv[l];
-    int64_t j = same.n ? find_key(same.key, same.n, k) : -1;
-    if (j >= 0 && (same.tag[j] & TAG_SF)) {
-        ux0 = uy0 = uz0 = 0.0;
-        j = -2;
-    }
-    if (j >= 0) {
-        for (int q = 0; q < Q; ++q) {
-            fo[q * nd + i] = same.f[q * same.n + j];
-            co[q * nd + i] = same.fcol[q * same.n + j];
-        }
-        kind[i] = 0;
-        return;
-    }
-    const int sh = L - l;
-    const int64_t x = (int64_t)(compact3(k) >> sh), y = (int64_t)(compact3(k >> 1) >> sh),
-                  z = (int64_t)(compact3(k >> 2) >> sh);
-    double a[Q], b[Q];
-    for (int m = l - 1; m >= 0 && j != -2; --m) {
-        const RemapSrc &cs = src.lv[m];
-        if (!cs.n) continue;
-        const int up = l - m;
-        j = find_key(cs.key, cs.n, level_key(L, m, x >> up, y >> up, z >> up));
-        if (j < 0) continue;
-        for (int q = 0; q < Q; ++q) a[q] = cs.f[q * cs.n + j];
-        eq_rescale<Q>(a, src.up_f[m], b);
-        for (int q = 0; q < Q; ++q) fo[q * nd + i] = b[q];
-        for (int q = 0; q < Q; ++q) a[q] = cs.fcol[q * cs.n + j];
-        eq_rescale<Q>(a, src.up_c[m], b);
-        for (int q = 0; q < Q; ++q) co[q * nd + i] = b[q];
-        kind[i] = 1;
-        return;
-    }
-    // the nearest finer source level holding descendants: their mean
-    for (int d = 1; l + d <= L && j != -2; ++d) {
-        const RemapSrc &fine = src.lv[l + d];
-        if (!fine.n) continue;
-        const int side = 1 << d;
-        int nch = 0;
-        double sf[Q], sc[Q];
-        for (int q = 0; q < Q; ++q) sf[q] = sc[q] = 0.0;
-        for (int c = 0; c < side * side * side; ++c) {
-            const int64_t cx = (x << d) + c % side, cy = (y << d) + (c / side) % side, cz = (z << d) + c / (side * side);
-            const int64_t jc = find_key(fine.key, fine.n, level_key(L, l + d, cx, cy, cz));
-            if (jc < 0 || (fine.tag[jc] & TAG_SF)) continue;
-            for (int q = 0; q < Q; ++q) {
-                sf[q] += fine.f[q * fine.n + jc];
-                sc[q] += fine.fcol[q * fine.n + jc];
-            }
-            ++nch;
-        }
-        if (!nch) continue;
-        for (int q = 0; q < Q; ++q) a[q] = sf[q] / nch;
-        eq_rescale<Q>(a, src.down_f[l + d], b);
-        for (int q = 0; q < Q; ++q) fo[q * nd + i] = b[q];
-        for (int q = 0; q < Q; ++q) a[q] = sc[q] / nch;
-        eq_rescale<Q>(a, src.down_c[l + d], b);
-        for (int q = 0; q < Q; ++q) co[q * nd + i] = b[q];
-        kind[i] = 2;
-        return;
-    }
-    const double uu = ux0 * ux0 + uy0 * uy0 + uz0 * uz0;
-    for (int q = 0; q < Q; ++q) {
-        const double eu = ex(q) * ux0 + ey(q) * uy0 + ez(q) * uz0;
-        const double feq = rho0 * w<Q>(q) * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu);
-        fo[q * nd + i] = feq;
-        co[q * nd + i] = feq;
-    }
-    kind[i] = 3;
-}
-
 }  // namespace
 
 // the state of case src carried onto case dst (another lattice of the same
-// model): per level FP64 copies of src's populations, k_remap for each level
-// of dst, written back in dst's storage; dst's direct-forcing step counter
-// follows src's.  counts[4 * l + kind] receives the cells of each kind.
+// model and storage): AmrOps<S>::remap per level, then dst's direct-forcing
+// step counter follows src's.  counts[4 * l + kind] receives the cells of
+// each kind.
 int amr_remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts)
 {
-    const int L = dst.d.max_level, Q = dst.d.q;
     if (int rc = amr_sync_f(ctx, src)) return rc;
     if (int rc = amr_sync_f(ctx, dst)) return rc;
-    // FP64 copies of every source level
-    std::vector<DBuf<double>> sf(L + 1), sc(L + 1);
-    for (int l = 0; l <= L && l <= src.d.max_level; ++l) {
-        const int64_t n = src.lv[l].n;
-        if (!n) continue;
-        if (int rc = sf[l].alloc(ctx, Q * n)) return rc;
-        if (int rc = sc[l].alloc(ctx, Q * n)) return rc;
-        int rc = amr_dispatch(src, [&](auto *tag) {
-            using S = std::remove_pointer_t<decltype(tag)>;
-            int r = AmrOps<S>::get(ctx, src, l, 0, sf[l].p);
-            return r ? r : AmrOps<S>::get(ctx, src, l, 1, sc[l].p);
-        });
-        if (rc) return rc;
-    }
-    RemapLevels rl;
-    for (int m = 0; m <= L && m <= src.d.max_level; ++m) {
-        if (!src.lv[m].n) continue;
-        rl.lv[m].key = src.lv[m].key;
-        rl.lv[m].tag = src.lv[m].tag;
-        rl.lv[m].n = src.lv[m].n;
-        rl.lv[m].f = sf[m].p;
-        rl.lv[m].fcol = sc[m].p;
-    }
-    // the interface factors of dst: the reference's (the same on f and
-    // fcol), or the stress-continuous ones (tau on f, tau - 1 on fcol)
-    const bool st = dst.scaling == MT_SCALE_STANDARD;
-    auto c2f = [&](int fine, bool col) {
-        const double tf = dst.d.tau[fine], tc = dst.d.tau[fine - 1];
-        if (!st) return (2.0 * tf) / tc;
-        return col ? (tf - 1.0) / (2.0 * (tc - 1.0)) : tf / (2.0 * tc);
-    };
-    for (int l = 0; l <= L; ++l) {
-        Level &lv = dst.lv[l];
-        for (int k = 0; k < 4; ++k)
-            if (counts) counts[4 * l + k] = 0;
-        if (!lv.n) continue;
-        for (int m = 0; m < kMaxLevels; ++m) rl.up_f[m] = rl.up_c[m] = 1.0;
-        for (int m = l - 1; m >= 0; --m) {
-            double pf = 1.0, pc = 1.0;
-            for (int j = m + 1; j <= l; ++j) {
-                pf *= c2f(j, false);
-                pc *= c2f(j, true);
-            }
-            rl.up_f[m] = pf;
-            rl.up_c[m] = pc;
-        }
-        for (int m = 0; m < kMaxLevels; ++m) rl.down_f[m] = rl.down_c[m] = 1.0;
-        for (int m = l + 1; m <= L; ++m) {
-            double pf = 1.0, pc = 1.0;
-            for (int j = l + 1; j <= m; ++j) {
-                pf /= c2f(j, false);
-                pc /= c2f(j, true);
-            }
-            rl.down_f[m] = pf;
-            rl.down_c[m] = pc;
-        }
-        DBuf<double> fo, co;
-        DBuf<uint8_t> kind;
-        if (int rc = fo.alloc(ctx, Q * lv.n)) return rc;
-        if (int rc = co.alloc(ctx, Q * lv.n)) return rc;
-        if (int rc = kind.alloc(ctx, lv.n)) return rc;
-        const double r0 = dst.d.rho0, u0 = dst.d.u_bc[0], u1 = dst.d.u_bc[1], u2 = dst.d.u_bc[2];
-        if (Q == 19)
-            k_remap<19><<<grid_for(lv.n, 128), 128, 0, ctx.stream>>>(lv.key, lv.tag, lv.n, L, l, rl, r0, u0, u1, u2,
-                                                                    fo.p, co.p, kind.p);
-        else
-            k_remap<27><<<grid_for(lv.n, 128), 128, 0, ctx.stream>>>(lv.key, lv.tag, lv.n, L, l, rl, r0, u0, u1, u2,
-                                                                    fo.p, co.p, kind.p);
-        MT_LAUNCHED(ctx);
-        int rc = amr_dispatch(dst, [&](auto *tag) {
-            using S = std::remove_pointer_t<decltype(tag)>;
-            int r = AmrOps<S>::set(ctx, dst, l, 0, fo.p);
-            return r ? r : AmrOps<S>::set(ctx, dst, l, 1, co.p);
-        });
-        if (rc) return rc;
-        if (counts) {
-            std::vector<uint8_t> hk((size_t)lv.n);
-            MT_CUDA(ctx, cudaMemcpyAsync(hk.data(), kind.p, lv.n, cudaMemcpyDeviceToHost, ctx.stream));
-            MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
-            for (uint8_t v : hk) counts[4 * l + (v & 3)] += 1;
-        }
-    }
+    int rc = amr_dispatch(dst, [&](auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        return AmrOps<S>::remap(ctx, dst, src, counts);
+    });
+    if (rc) return rc;
     if (dst.tstep && src.tstep)
         MT_CUDA(ctx, cudaMemcpyAsync(dst.tstep, src.tstep, sizeof(long long), cudaMemcpyDeviceToDevice, ctx.stream));
     MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
