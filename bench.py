@@ -541,7 +541,7 @@ def served_case_section(ctx, torch, steps=10, warmup=2):
     return out
 
 
-def moving_section(ctx, torch, steps=250, window=16, radius=8, max_level=3, re=100.0):
+def moving_section(ctx, torch, steps=250, window=32, radius=8, max_level=3, re=100.0):
     """An oscillating direct-forcing sphere (R = 8 coarse cells, 3
     refinement levels, amplitude R/2, one period = 2000 finest = 250 coarse
     steps, FP16) on the static mesh whose finest box and forcing band cover
