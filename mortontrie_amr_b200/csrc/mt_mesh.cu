@@ -1,13 +1,15 @@
 // Lattice classification on the device: the per-level index sets of
 // Lat_Manager (Lat_Manager.hpp:245-316) for nested refinement boxes and an
-// analytic sphere, generated directly as raw (key, set) pairs for the build
-// (mt_case_generate).  It restates, set for set, what the host mesher
-// (mortontrie_amr_b200/mesh.py) produces -- boundary shell split into the 26
-// lat_bc sets, F2C = 1-cell shell of each refinement box, C2F = 2-cell shell
-// of each refined level, ghost layers from Q-neighbours, the voxelised solid
-// with its wall distances (Lat_Voxelize.cpp:1252-1285 semantics) or the
-// direct-forcing band -- and raises the same contract errors.  Compiled
-// without FMA contraction so the wall distances equal the host's.
+// analytic sphere or a triangulated surface, generated directly as raw
+// (key, set) pairs for the build (mt_case_generate).  It restates, set for
+// set, what the host mesher (mortontrie_amr_b200/mesh.py) produces --
+// boundary shell split into the 26 lat_bc sets, F2C = 1-cell shell of each
+// refinement box, C2F = 2-cell shell of each refined level, ghost layers
+// from Q-neighbours, the voxelised solid with its wall distances
+// (Lat_Voxelize.cpp:1252-1285 semantics) or the direct-forcing band -- and
+// raises the same contract errors.  Compiled without FMA contraction so the
+// wall distances equal the host's.  amr_remap (mt_case_remap) dispatches the
+// state remap onto such a lattice.
 #include <cub/cub.cuh>
 
 #include <algorithm>
