@@ -706,7 +706,13 @@ template <int Q, class S, int COLL>
 #ifndef MT_BRICK_MIN_BLOCKS
 #define MT_BRICK_MIN_BLOCKS 8  // resident 128-thread blocks per SM asked of the 16-bit brick passes (64 registers)
 #endif
-__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_MIN_BLOCKS : 1) k_brick_step(
+#ifndef MT_BRICK_MIN_BLOCKS_Q19_LBGK
+#define MT_BRICK_MIN_BLOCKS_Q19_LBGK 10  // 16-bit D3Q19 LBGK passes: 48 registers, no spills
+#endif
+__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? ((COLL == MT_COLL_LBGK && Q == 19)
+                                                                  ? MT_BRICK_MIN_BLOCKS_Q19_LBGK
+                                                                  : MT_BRICK_MIN_BLOCKS)
+                                                             : 1) k_brick_step(
     int64_t nb, const int32_t *__restrict__ halo, const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
     const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext, double tau,
     typename Store<S>::C *__restrict__ rho, typename Store<S>::C *__restrict__ u, int macros, int fall,
