@@ -88,6 +88,11 @@ typedef struct mt_case_desc {
 typedef struct mt_ctx mt_ctx;
 
 /* ---- context ---------------------------------------------------------- */
+/* A context on `device` with a stream of its own.  It also sets the release
+ * threshold of the device's default memory pool (cudaDeviceGetDefaultMemPool)
+ * to unlimited, so memory freed by stream-ordered frees stays in the pool for
+ * the next case build instead of being returned at every synchronisation;
+ * that pool is shared by every user of cudaMallocAsync in the process. */
 int mt_create(int32_t device, mt_ctx **out);
 int mt_destroy(mt_ctx *ctx);
 const char *mt_last_error(const mt_ctx *ctx);
