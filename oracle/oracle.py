@@ -263,3 +263,134 @@ def run_harness_morton(q, L, levels, keys, timeout=120):
             fh.write(struct.pack("<q", keys.size) + levels.tobytes() + keys.tobytes())
         subprocess.run([exe, "morton", fin, fout], check=True, timeout=timeout)
         return np.fromfile(fout, np.uint64).reshape(keys.size, q)
+
+
+def remap_restated(q, L, dst_levels, src_levels, taus, standard, rho0, u0):
+    """CPU restatement of the state remap onto another lattice (mt_case_remap),
+    FP64, in the device kernel's operation order, for the parity test.
+
+    dst_levels[l] = (keys, tags); src_levels[l] = (keys, tags, f, fcol) with
+    f, fcol [Q][n] FP64.  Returns per level (f, fcol, kind) of the
+    destination: kind 0 copied (same key and level), 1 from the nearest
+    coarser ancestor (non-equilibrium part scaled by the product of the
+    explosion factors crossed), 2 from the mean of the descendants on the
+    nearest finer level holding any (coalescence factors), 3 equilibrium.
+    Solid cells (tag 64) are zero; a cell solid in the source takes the
+    equilibrium at rest."""
+    from mortontrie_amr_b200.lattice import _compact3, _dilate3, directions, weights
+    ex, ey, ez, _ = directions(q)
+    w = weights(q)
+    T_SF = 64
+
+    def c2f(fine, col):
+        tf, tc = taus[fine], taus[fine - 1]
+        if not standard:
+            return (2.0 * tf) / tc
+        return (tf - 1.0) / (2.0 * (tc - 1.0)) if col else tf / (2.0 * tc)
+
+    def key_at(l, x, y, z):
+        sh = np.uint64(L - l)
+        return int(_dilate3(np.array([x], np.uint64) << sh)[0] | (_dilate3(np.array([y], np.uint64) << sh)[0] << np.uint64(1))
+                   | (_dilate3(np.array([z], np.uint64) << sh)[0] << np.uint64(2)))
+
+    def rescale(v, s):
+        r = jx = jy = jz = 0.0
+        for k in range(q):
+            r += v[k]
+            jx += v[k] * float(ex[k])
+            jy += v[k] * float(ey[k])
+            jz += v[k] * float(ez[k])
+        rs = (-1e-6 if r < 0.0 else 1e-6) if (-1e-6 < r < 1e-6) else r
+        ux, uy, uz = jx / rs, jy / rs, jz / rs
+        uu = ux * ux + uy * uy + uz * uz
+        out = np.empty(q)
+        for k in range(q):
+            eu = float(ex[k]) * ux + float(ey[k]) * uy + float(ez[k]) * uz
+            feq = r * w[k] * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu)
+            out[k] = feq + s * (v[k] - feq)
+        return out
+
+    def eq(rho, ua):
+        uu = ua[0] * ua[0] + ua[1] * ua[1] + ua[2] * ua[2]
+        out = np.empty(q)
+        for k in range(q):
+            eu = float(ex[k]) * ua[0] + float(ey[k]) * ua[1] + float(ez[k]) * ua[2]
+            out[k] = rho * w[k] * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uu)
+        return out
+
+    index = [dict(zip(k.tolist(), range(k.size))) for k, _, _, _ in src_levels]
+    result = []
+    for l, (dk, dt) in enumerate(dst_levels):
+        n = dk.size
+        fo, co, kind = np.zeros((q, n)), np.zeros((q, n)), np.zeros(n, np.int64)
+        up_f, up_c = [1.0] * (L + 1), [1.0] * (L + 1)
+        for m in range(l - 1, -1, -1):
+            for j in range(m + 1, l + 1):
+                up_f[m] *= c2f(j, False)
+                up_c[m] *= c2f(j, True)
+        dn_f, dn_c = [1.0] * (L + 1), [1.0] * (L + 1)
+        for m in range(l + 1, L + 1):
+            for j in range(l + 1, m + 1):
+                dn_f[m] /= c2f(j, False)
+                dn_c[m] /= c2f(j, True)
+        xs = (_compact3(dk) >> np.uint64(L - l)).astype(np.int64)
+        ys = (_compact3(dk >> np.uint64(1)) >> np.uint64(L - l)).astype(np.int64)
+        zs = (_compact3(dk >> np.uint64(2)) >> np.uint64(L - l)).astype(np.int64)
+        for i in range(n):
+            if dt[i] & T_SF:
+                continue
+            k = int(dk[i])
+            sk, stag, sf, sc = src_levels[l]
+            j = index[l].get(k, -1)
+            uncovered = j >= 0 and bool(stag[j] & T_SF)
+            if uncovered:
+                j = -1
+            if j >= 0:
+                fo[:, i], co[:, i] = sf[:, j], sc[:, j]
+                continue
+            x, y, z = int(xs[i]), int(ys[i]), int(zs[i])
+            done = False
+            for m in range(l - 1, -1, -1):
+                if uncovered or not index[m]:
+                    continue
+                up = l - m
+                jm = index[m].get(key_at(m, x >> up, y >> up, z >> up), -1)
+                if jm < 0:
+                    continue
+                fo[:, i] = rescale(src_levels[m][2][:, jm].copy(), up_f[m])
+                co[:, i] = rescale(src_levels[m][3][:, jm].copy(), up_c[m])
+                kind[i] = 1
+                done = True
+                break
+            if done:
+                continue
+            for d in range(1, L - l + 1):
+                if uncovered or not index[l + d]:
+                    continue
+                side = 1 << d
+                fk, ftag, ff, fc = src_levels[l + d]
+                a, b = np.zeros(q), np.zeros(q)
+                nch = 0
+                for c in range(side ** 3):
+                    cx, cy, cz = (x << d) + c % side, (y << d) + (c // side) % side, (z << d) + c // (side * side)
+                    jc = index[l + d].get(key_at(l + d, cx, cy, cz), -1)
+                    if jc < 0 or (ftag[jc] & T_SF):
+                        continue
+                    for qq in range(q):
+                        a[qq] += ff[qq, jc]
+                        b[qq] += fc[qq, jc]
+                    nch += 1
+                if not nch:
+                    continue
+                fo[:, i] = rescale(a / nch, dn_f[l + d])
+                co[:, i] = rescale(b / nch, dn_c[l + d])
+                kind[i] = 2
+                done = True
+                break
+            if done:
+                continue
+            e = eq(rho0, (0.0, 0.0, 0.0) if uncovered else u0)
+            fo[:, i], co[:, i] = e, e
+            kind[i] = 3
+        result.append((fo, co, kind))
+    return result
