@@ -63,7 +63,3 @@ def batched_uneven_cases(seed: int = 4, n: int = 64) -> list:
         out.append(CaseSpec(kind, coarse, levels, re, q, coll))
     return out
 
-
-def build_spec(spec: CaseSpec) -> Case:
-    """Host mesh of one case (a picklable entry point for worker processes)."""
-    return spec.build()
