@@ -1003,6 +1003,41 @@ __global__ void k_band_collide(const int32_t *band, int64_t nb, int64_t n, doubl
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j >= nb) return;
     const int64_t i = band[j];
+    if constexpr (T::shifted) {
+        // reduced precision: the stored deviations s = f - w throughout (the
+        // weights sum to 1 and have no first moment), the forcing term as
+        // 3 (e.g - u.g) + 9 (e.u)(e.g)
+        float sd[Q];
+        float rd = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            sd[k] = T::ld(f, k * n + i);
+            rd += sd[k];
+            jx += sd[k] * ex(k);
+            jy += sd[k] * ey(k);
+            jz += sd[k] * ez(k);
+        }
+        const float gx = (float)((double)acc[i] * kForceInv), gy = (float)((double)acc[n + i] * kForceInv),
+                    gz = (float)((double)acc[2 * n + i] * kForceInv);
+        const float r = 1.f + rd;
+        const float rs = (r > -1e-6f && r < 1e-6f) ? ((r < 0.f) ? -1e-6f : 1e-6f) : r;
+        const float ir = 1.f / rs;
+        const float x = (jx + 0.5f * gx) * ir, y = (jy + 0.5f * gy) * ir, z = (jz + 0.5f * gz) * ir;
+        const float om = (float)(1.0 / tau);
+        const float fpre = 1.f - 0.5f * om;
+        const float uu = 1.5f * (x * x + y * y + z * z);
+        const float ug = x * gx + y * gy + z * gz;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            const float eu = ex(k) * x + ey(k) * y + ez(k) * z;
+            const float eg = ex(k) * gx + ey(k) * gy + ez(k) * gz;
+            const float wk = (float)w<Q>(k);
+            const float dfeq = wk * ((r - 1.f) + r * (3.f * eu + 4.5f * eu * eu - uu));
+            const float ge = 3.f * (eg - ug) + 9.f * eu * eg;
+            T::st(fcol, k * n + i, fmaf(om, dfeq - sd[k], sd[k]) + fpre * wk * ge);
+        }
+        return;
+    }
     C d[Q];
     C r = 0, jx = 0, jy = 0, jz = 0;
 #pragma unroll
