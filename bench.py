@@ -344,12 +344,17 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
     res = {}
     # (label, storage, schedule): the plain form is FP64 in the reference's
     # phase order; the reduced storages run the fused schedule
+    # (*_inlet: reduced storage shifted by feq(1, u_bc) instead of w)
     runs = [("f64", "f64", "phases"), ("f64_fused", "f64", "fused"), ("f32", "f32", "fused"),
-            ("f16", "f16", "fused"), ("bf16", "bf16", "fused"), ("f16_phases", "f16", "phases")]
+            ("f16", "f16", "fused"), ("bf16", "bf16", "fused"), ("f16_phases", "f16", "phases"),
+            ("f16_inlet", "f16", "fused"), ("bf16_inlet", "bf16", "fused")]
     if only:
         runs = [r for r in runs if r[0] in only]
     for st, storage, schedule in runs:
-        mgr = LBM_Manager(ctx, case, storage, schedule=schedule)
+        mgr = LBM_Manager(ctx, case, storage, schedule=schedule,
+                          storage_shift="inlet" if st.endswith("_inlet") else None)
+        if st.endswith("_inlet"):
+            out[st] = {"storage_shift": "feq(1, u_bc)"}
         mgr.fluidSimulate(warmup)
         torch.cuda.synchronize()
         mgr.reset_force()
@@ -365,7 +370,7 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
         fluid = (tags & 1) != 0
         f = mgr.force()
         res[st] = dict(secs=secs, u=u[:, fluid], rho=rho[fluid], fx=f[0] / max(f[3], 1.0))
-        out[st] = {"storage": storage, "schedule": schedule,
+        out[st] = {**out.get(st, {}), "storage": storage, "schedule": schedule,
                    "fine_mlups": round(per_coarse_fine * steps / secs / 1e6, 1),
                    "total_mlups": round(per_coarse_total * steps / secs / 1e6, 1),
                    "ms_per_coarse_step": round(1e3 * secs / steps, 3)}
@@ -660,9 +665,10 @@ def _accuracy_case(name):
     return nested_sphere_case(re=20.0 if name == "cfg3_re20" else 200.0)
 
 
-def amr_accuracy(ctx, torch, steps=2500, case_name="cfg3", scaling="reference"):
-    """Long-run accuracy of the reduced storages (fused schedule) against the
-    FP64 phase schedule on a sphere case: after `steps` coarse steps, the
+def amr_accuracy(ctx, torch, steps=2500, case_name="cfg3", scaling="reference", only=None):
+    """Long-run accuracy of the reduced storages (fused schedule; shifted by
+    w or, *_inlet, by feq(1, u_bc)) against the FP64 phase schedule on a
+    sphere case: after `steps` coarse steps, the
     drag coefficient averaged over the last tenth of the run, the velocity
     field of every level's lat_f cells (relative L2), the total mass, and
     whether every population stayed finite."""
@@ -674,9 +680,13 @@ def amr_accuracy(ctx, torch, steps=2500, case_name="cfg3", scaling="reference"):
     u_in = float(case.params.u_bc[0])
     tail = max(steps // 10, 1)
     res = {}
-    for st, storage, schedule in [("f64", "f64", "phases"), ("f32", "f32", "fused"), ("f16", "f16", "fused"),
-                                  ("bf16", "bf16", "fused")]:
-        mgr = LBM_Manager(ctx, case, storage, schedule=schedule, scaling=scaling)
+    runs = [("f64", "f64", "phases"), ("f32", "f32", "fused"), ("f16", "f16", "fused"), ("bf16", "bf16", "fused"),
+            ("f16_inlet", "f16", "fused"), ("bf16_inlet", "bf16", "fused")]
+    if only:
+        runs = [r for r in runs if r[0] in only or r[0] == "f64"]
+    for st, storage, schedule in runs:
+        mgr = LBM_Manager(ctx, case, storage, schedule=schedule, scaling=scaling,
+                          storage_shift="inlet" if st.endswith("_inlet") else None)
         t0 = time.time()
         mgr.fluidSimulate(steps - tail)
         mgr.reset_force()
@@ -701,7 +711,7 @@ def amr_accuracy(ctx, torch, steps=2500, case_name="cfg3", scaling="reference"):
     out = {"case": ACCURACY_CASES[case_name], "interface_scaling": scaling, "coarse_steps": steps,
            "finest_steps": steps << L, "drag_window_coarse_steps": tail, "cd_f64": ref["cd"],
            "f64_finite": ref["finite"]}
-    for st in ("f32", "f16", "bf16"):
+    for st, _, _ in runs[1:]:
         r = res[st]
         out[st] = {"cd": r["cd"], "drag_rel_vs_f64": abs(r["cd"] - ref["cd"]) / abs(ref["cd"]),
                    "velocity_l2_vs_f64": float(np.linalg.norm(r["u"] - ref["u"]) / np.linalg.norm(ref["u"])),
@@ -803,7 +813,8 @@ def main():
                     help="only the largest served request alone (profiling driver of the forcing kernels)")
     ap.add_argument("--amr-variants", default=None,
                     help="comma list of multi-level runs to time (default all: "
-                         "f64,f64_fused,f32,f16,bf16,f16_phases); profiling runs")
+                         "f64,f64_fused,f32,f16,bf16,f16_phases,f16_inlet,bf16_inlet); profiling and "
+                         "accuracy runs")
     ap.add_argument("--amr-accuracy", type=int, default=0, metavar="N",
                     help="only the long-run accuracy of the reduced storages on the 4-level sphere (N coarse steps)")
     ap.add_argument("--accuracy-case", default="cfg3", choices=sorted(ACCURACY_CASES))
@@ -866,8 +877,9 @@ def main():
         torch.cuda.set_stream(stream)
         ctx = Context(0)
         ctx.set_stream(stream.cuda_stream)
+        only = set(args.amr_variants.split(",")) if args.amr_variants else None
         print(json.dumps({"amr_accuracy": amr_accuracy(ctx, torch, args.amr_accuracy, args.accuracy_case,
-                                                       args.scaling)}), flush=True)
+                                                       args.scaling, only)}), flush=True)
         ctx.close()
     elif args.amr_only:
         import torch

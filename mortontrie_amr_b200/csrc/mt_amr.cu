@@ -928,14 +928,20 @@ int storage_code(const Case &c) { return c.d.storage; }
 // batched brick passes of level l over the members in cs (brick levels only)
 int batch_bricks(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cs, int l, const BrickBatch **first_desc)
 {
-    // group by (q, collision, storage): one kernel instantiation each
+    // group by (q, collision, storage, storage shift): one kernel instantiation
+    // each, the shift a parameter of the pass
+    auto same_shift = [](const Case &a, const Case &b) {
+        for (int k = 0; k < 27; ++k)
+            if (a.shift.d[k] != b.shift.d[k]) return false;
+        return true;
+    };
     std::vector<std::vector<Case *>> groups;
     for (Case *c : cs) {
         if (!c->lv[l].bricks || c->lv[l].nbrick >= kBatchOwnBricks) continue;
         bool placed = false;
         for (auto &g : groups)
             if (g[0]->d.q == c->d.q && g[0]->d.collision == c->d.collision &&
-                storage_code(*g[0]) == storage_code(*c)) {
+                storage_code(*g[0]) == storage_code(*c) && same_shift(*g[0], *c)) {
                 g.push_back(c);
                 placed = true;
                 break;
@@ -974,7 +980,7 @@ int batch_bricks(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cs, int l, co
             Case &c = *g[0];
             int rc = amr_dispatch(c, [&](auto *tag) {
                 using S = std::remove_pointer_t<decltype(tag)>;
-                return AmrOps<S>::batch_pass(ctx, c.d.q, c.d.collision, dev, d.total);
+                return AmrOps<S>::batch_pass(ctx, c.d.q, c.d.collision, dev, d.total, c.shift);
             });
             if (rc) return rc;
         }

@@ -26,7 +26,7 @@ static __constant__ int8_t c_bdry27[26][18];
 
 template <int Q, class S>
 __global__ void k_init_eq(int64_t n, const uint32_t *tag, double rho0, double ux, double uy, double uz, S *f, S *fcol,
-                          typename Store<S>::C *rho, typename Store<S>::C *u)
+                          typename Store<S>::C *rho, typename Store<S>::C *u, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -37,7 +37,7 @@ __global__ void k_init_eq(int64_t n, const uint32_t *tag, double rho0, double ux
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const double v = solid ? 0. : feq_ref<Q>(k, rho0, ux, uy, uz);
-        const C s = (C)(T::shifted ? v - w<Q>(k) : v);
+        const C s = stored_f64<S>(sh, v, k);
         T::st(f, k * n + i, s);
         T::st(fcol, k * n + i, s);
     }
@@ -50,7 +50,7 @@ __global__ void k_init_eq(int64_t n, const uint32_t *tag, double rho0, double ux
 // LBM_Manager::calculateMacros(level), LBM_Manager.cpp:1003-1050
 template <int Q, class S>
 __global__ void k_macros(const int32_t *list, int64_t nl, int64_t n, const S *f, typename Store<S>::C *rho,
-                         typename Store<S>::C *u)
+                         typename Store<S>::C *u, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -59,7 +59,7 @@ __global__ void k_macros(const int32_t *list, int64_t nl, int64_t n, const S *f,
     const int64_t i = list[j];
     C d[Q];
 #pragma unroll
-    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::ld(f, k * n + i), k);
+    for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::ld(f, k * n + i), k);
     C r, x, y, z;
     macros_g<Q, C>(d, r, x, y, z);
     rho[i] = r;
@@ -76,7 +76,7 @@ __global__ void k_macros(const int32_t *list, int64_t nl, int64_t n, const S *f,
 template <int Q, class S, int COLL, class I = int64_t>
 __device__ __forceinline__ void collide_store(const typename Store<S>::C *d, typename Store<S>::C r,
                                               typename Store<S>::C x, typename Store<S>::C y,
-                                              typename Store<S>::C z, double tau, S *fcol, I n, I i)
+                                              typename Store<S>::C z, double tau, S *fcol, I n, I i, const Shift &sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -94,9 +94,10 @@ __device__ __forceinline__ void collide_store(const typename Store<S>::C *d, typ
             for (int k = 0; k < Q; ++k) {
                 const float eu = ex(k) * x + ey(k) * y + ez(k) * z;
                 const float wk = (float)w<Q>(k);
-                // deviations: feq - w = w ((rho - 1) + rho (3 eu + 4.5 eu^2 - 1.5 u^2))
-                const float dfeq = wk * ((r - 1.f) + r * (3.f * eu + 4.5f * eu * eu - uu));
-                const float s = d[k] - wk;
+                // deviations from the shift s_k = w_k + dw_k:
+                // feq - s = w ((rho - 1) + rho (3 eu + 4.5 eu^2 - 1.5 u^2)) - dw
+                const float dfeq = wk * ((r - 1.f) + r * (3.f * eu + 4.5f * eu * eu - uu)) - sh.dw[k];
+                const float s = d[k] - sh.v[k];
                 T::st(fcol, (I)k * n + i, fmaf(om, dfeq - s, s));
             }
         }
@@ -104,7 +105,7 @@ __device__ __forceinline__ void collide_store(const typename Store<S>::C *d, typ
         C o[27];
         cumulant_collide<C>(d, r, x, y, z, (C)(1. / tau), o);
 #pragma unroll
-        for (int k = 0; k < 27; ++k) T::st(fcol, (I)k * n + i, stored_of<S, 27>(o[k], k));
+        for (int k = 0; k < 27; ++k) T::st(fcol, (I)k * n + i, stored_sh<S>(sh, o[k], k));
     }
 }
 
@@ -112,7 +113,7 @@ __device__ __forceinline__ void collide_store(const typename Store<S>::C *d, typ
 // on lat_f then overlap_F2C (Collision_Manager.cpp:13-53, Collision_Cumulant.cpp:22-159)
 template <int Q, class S, int COLL>
 __global__ void k_collide(const int32_t *list, int64_t nl, int64_t n, double tau, const S *f,
-                          typename Store<S>::C *rho, typename Store<S>::C *u, S *fcol)
+                          typename Store<S>::C *rho, typename Store<S>::C *u, S *fcol, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -121,14 +122,14 @@ __global__ void k_collide(const int32_t *list, int64_t nl, int64_t n, double tau
     const int64_t i = list[j];
     C d[Q];
 #pragma unroll
-    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::ld(f, k * n + i), k);
+    for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::ld(f, k * n + i), k);
     C r, x, y, z;
     macros_g<Q, C>(d, r, x, y, z);
     rho[i] = r;
     u[i] = x;
     u[n + i] = y;
     u[2 * n + i] = z;
-    collide_store<Q, S, COLL>(d, r, x, y, z, tau, fcol, n, i);
+    collide_store<Q, S, COLL>(d, r, x, y, z, tau, fcol, n, i, sh);
 }
 
 // fcol = f on overlap_C2F (Collision_Manager.cpp:45-52)
@@ -169,7 +170,7 @@ __global__ void k_stream(const int32_t *list, int64_t nl, int64_t n, int textboo
 template <int Q, class S>
 __global__ void k_explosion(const int32_t *__restrict__ src, const int32_t *__restrict__ child, int64_t ns,
                             int64_t nc, const S *__restrict__ cfcol, int64_t nf, S *__restrict__ ffcol, double scale,
-                            S *__restrict__ ffcol2, int64_t nf2c)
+                            S *__restrict__ ffcol2, int64_t nf2c, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -182,14 +183,14 @@ __global__ void k_explosion(const int32_t *__restrict__ src, const int32_t *__re
     const int64_t i = src[j];
     C d[Q];
 #pragma unroll
-    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::ld(cfcol, k * nc + i), k);
+    for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::ld(cfcol, k * nc + i), k);
     C r, x, y, z;
     macros_g<Q, C>(d, r, x, y, z);
     const bool both = ffcol2 && j >= nf2c;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
-        const C v = stored_of<S, Q>(fe + (C)scale * (d[k] - fe), k);
+        const C v = stored_sh<S>(sh, fe + (C)scale * (d[k] - fe), k);
         T::st(ffcol, k * nf + ch, v);
         if (both) T::st(ffcol2, k * nf + ch, v);
     }
@@ -198,7 +199,7 @@ __global__ void k_explosion(const int32_t *__restrict__ src, const int32_t *__re
 // AMR_transDDF_coalescence (LBM_Manager.cpp:1131-1169)
 template <int Q, class S>
 __global__ void k_coalescence(const int32_t *list, const int32_t *child, int64_t nl, int64_t nc, S *cf, const S *ff,
-                              int64_t nf, double scale)
+                              int64_t nf, double scale, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -213,7 +214,7 @@ __global__ void k_coalescence(const int32_t *list, const int32_t *child, int64_t
     for (int k = 0; k < Q; ++k) {
         C s = 0;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) s += full_of<S, Q>(T::ld(ff, k * nf + ch[m]), k);
+        for (int m = 0; m < 8; ++m) s += full_sh<S>(sh, T::ld(ff, k * nf + ch[m]), k);
         a[k] = s / (C)8.0;
     }
     C r, x, y, z;
@@ -221,7 +222,7 @@ __global__ void k_coalescence(const int32_t *list, const int32_t *child, int64_t
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
-        T::st(cf, k * nc + i, stored_of<S, Q>(fe + (C)scale * (a[k] - fe), k));
+        T::st(cf, k * nc + i, stored_sh<S>(sh, fe + (C)scale * (a[k] - fe), k));
     }
 }
 
@@ -234,7 +235,7 @@ template <int Q, class S, int COLL>
 __global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *__restrict__ child, int64_t nl,
                                int64_t nc, S *__restrict__ cf, const S *__restrict__ ff, int64_t nf, double scale,
                                double tau, S *__restrict__ cfnext, typename Store<S>::C *__restrict__ rho,
-                               typename Store<S>::C *__restrict__ u, int macros)
+                               typename Store<S>::C *__restrict__ u, int macros, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -249,7 +250,7 @@ __global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *
     for (int k = 0; k < Q; ++k) {
         C s = 0;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) s += full_of<S, Q>(T::ld(ff, k * nf + ch[m]), k);
+        for (int m = 0; m < 8; ++m) s += full_sh<S>(sh, T::ld(ff, k * nf + ch[m]), k);
         a[k] = s / (C)8.0;
     }
     C r, x, y, z;
@@ -257,11 +258,11 @@ __global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
-        const C st = stored_of<S, Q>(fe + (C)scale * (a[k] - fe), k);
+        const C st = stored_sh<S>(sh, fe + (C)scale * (a[k] - fe), k);
         T::st(cf, k * nc + i, st);
         S sv;
         T::st(&sv, 0, st);
-        a[k] = full_of<S, Q>(T::cv(sv), k);
+        a[k] = full_sh<S>(sh, T::cv(sv), k);
     }
     macros_g<Q, C>(a, r, x, y, z);
     if (macros) {
@@ -270,7 +271,7 @@ __global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *
         u[nc + i] = y;
         u[2 * nc + i] = z;
     }
-    collide_store<Q, S, COLL>(a, r, x, y, z, tau, cfnext, nc, i);
+    collide_store<Q, S, COLL>(a, r, x, y, z, tau, cfnext, nc, i, sh);
 }
 
 // Non-equilibrium extrapolation ("eflow stable" form) on one boundary set:
@@ -281,7 +282,7 @@ __global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *
 template <int Q, class S>
 __global__ void k_bc_neq(const int32_t *list, int64_t nl, int b, int64_t n, const int32_t *nbr,
                          const typename Store<S>::C *rho, const typename Store<S>::C *u, S *f, double ubx,
-                         double uby, double ubz, double *tmp, int phase, int *err)
+                         double uby, double ubz, double *tmp, int phase, int *err, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -296,14 +297,14 @@ __global__ void k_bc_neq(const int32_t *list, int64_t nl, int b, int64_t n, cons
             const int32_t nb = k == 0 ? (int32_t)i : nbr[(int64_t)(k - 1) * n + i];
             if (nb < 0) {
                 atomicOr(err, DEVERR_MISSING_BC_NBR);
-                tmp[t * nl + j] = (double)full_of<S, Q>(T::ld(f, k * n + i), k);
+                tmp[t * nl + j] = (double)full_sh<S>(sh, T::ld(f, k * n + i), k);
                 continue;
             }
             const C fw = feq_g<Q, C>(k, rho[i], (C)ubx, (C)uby, (C)ubz);
             const C fn = feq_g<Q, C>(k, rho[nb], u[nb], u[n + nb], u[2 * n + nb]);
-            tmp[t * nl + j] = (double)(fw + full_of<S, Q>(T::ld(f, k * n + nb), k) - fn);
+            tmp[t * nl + j] = (double)(fw + full_sh<S>(sh, T::ld(f, k * n + nb), k) - fn);
         } else {
-            T::st(f, k * n + i, stored_of<S, Q>((C)tmp[t * nl + j], k));
+            T::st(f, k * n + i, stored_sh<S>(sh, (C)tmp[t * nl + j], k));
         }
     }
 }
@@ -316,7 +317,7 @@ struct BcVel {
 template <int Q, class S>
 __global__ void k_bc_neq_all(const int32_t *list, const int8_t *setb, int64_t nl, int64_t n, const int32_t *nbr,
                              const typename Store<S>::C *rho, const typename Store<S>::C *u, S *f, BcVel ub,
-                             double *tmp, int phase, int *err)
+                             double *tmp, int phase, int *err, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -332,14 +333,14 @@ __global__ void k_bc_neq_all(const int32_t *list, const int8_t *setb, int64_t nl
             const int32_t nb = k == 0 ? (int32_t)i : nbr[(int64_t)(k - 1) * n + i];
             if (nb < 0) {
                 atomicOr(err, DEVERR_MISSING_BC_NBR);
-                tmp[t * nl + j] = (double)full_of<S, Q>(T::ld(f, k * n + i), k);
+                tmp[t * nl + j] = (double)full_sh<S>(sh, T::ld(f, k * n + i), k);
                 continue;
             }
             const C fw = feq_g<Q, C>(k, rho[i], (C)ub.u[b][0], (C)ub.u[b][1], (C)ub.u[b][2]);
             const C fn = feq_g<Q, C>(k, rho[nb], u[nb], u[n + nb], u[2 * n + nb]);
-            tmp[t * nl + j] = (double)(fw + full_of<S, Q>(T::ld(f, k * n + nb), k) - fn);
+            tmp[t * nl + j] = (double)(fw + full_sh<S>(sh, T::ld(f, k * n + nb), k) - fn);
         } else {
-            T::st(f, k * n + i, stored_of<S, Q>((C)tmp[t * nl + j], k));
+            T::st(f, k * n + i, stored_sh<S>(sh, (C)tmp[t * nl + j], k));
         }
     }
 }
@@ -350,7 +351,7 @@ __global__ void k_bc_neq_all(const int32_t *list, const int8_t *setb, int64_t nl
 // cells copy the inner cell's fcol (BC/Outflow.cpp:39-52).
 template <int Q, class S>
 __global__ void k_bc_inout(const int32_t *list, int64_t nl, int east, int64_t n, const int32_t *nbr, double rho0,
-                           S *f, S *fcol, double ubx, double uby, double ubz, int *err)
+                           S *f, S *fcol, double ubx, double uby, double ubz, int *err, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -369,7 +370,7 @@ __global__ void k_bc_inout(const int32_t *list, int64_t nl, int east, int64_t n,
             fcol[k * n + i] = v;
             f[k * n + i] = v;
         } else {
-            const C v = stored_of<S, Q>(feq_g<Q, C>(k, (C)rho0, (C)ubx, (C)uby, (C)ubz), k);
+            const C v = stored_sh<S>(sh, feq_g<Q, C>(k, (C)rho0, (C)ubx, (C)uby, (C)ubz), k);
             T::st(fcol, k * n + i, v);
             T::st(f, k * n + i, v);
         }
@@ -380,7 +381,7 @@ __global__ void k_bc_inout(const int32_t *list, int64_t nl, int east, int64_t n,
 // boundary set: f = fcol = feq(rho0, u) with the face's velocity
 template <int Q, class S>
 __global__ void k_bc_set_eq(const int32_t *list, int64_t nl, int64_t n, double rho0, double ux, double uy, double uz,
-                            S *f, S *fcol)
+                            S *f, S *fcol, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -390,7 +391,7 @@ __global__ void k_bc_set_eq(const int32_t *list, int64_t nl, int64_t n, double r
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const double v = feq_ref<Q>(k, rho0, ux, uy, uz);
-        const C st = (C)(T::shifted ? v - w<Q>(k) : v);
+        const C st = stored_f64<S>(sh, v, k);
         T::st(f, k * n + i, st);
         T::st(fcol, k * n + i, st);
     }
@@ -406,11 +407,11 @@ template <int Q, int FH, class S>
 __device__ __forceinline__ void ib_cell(int64_t i, int64_t n, const double *dr, const int32_t *nbr, const S *fcol,
                                         typename Store<S>::C rho_b, typename Store<S>::C *g,
                                         typename Store<S>::C &fx, typename Store<S>::C &fy,
-                                        typename Store<S>::C &fz)
+                                        typename Store<S>::C &fz, const Shift &sh)
 {
     using T = Store<S>;
     using C = typename T::C;
-    auto FC = [&](int k, int64_t idx) { return full_of<S, Q>(T::ld(fcol, k * n + idx), k); };
+    auto FC = [&](int k, int64_t idx) { return full_sh<S>(sh, T::ld(fcol, k * n + idx), k); };
     g[0] = FC(0, i);
     fx = 0;
     fy = 0;
@@ -485,7 +486,7 @@ __device__ __forceinline__ void ib_cell(int64_t i, int64_t n, const double *dr, 
 
 template <int Q, int FH, class S>
 __global__ void k_ib_treat(const int32_t *list, int64_t nl, int64_t n, const int32_t *disrow, const double *dis,
-                           const int32_t *nbr, const S *fcol, const typename Store<S>::C *rho, S *f, double *force)
+                           const int32_t *nbr, const S *fcol, const typename Store<S>::C *rho, S *f, double *force, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -494,9 +495,9 @@ __global__ void k_ib_treat(const int32_t *list, int64_t nl, int64_t n, const int
     const int64_t i = list[j];
     const double *dr = dis + (int64_t)disrow[i] * (Q - 1);
     C g[Q], fx, fy, fz;
-    ib_cell<Q, FH, S>(i, n, dr, nbr, fcol, rho[i], g, fx, fy, fz);
+    ib_cell<Q, FH, S>(i, n, dr, nbr, fcol, rho[i], g, fx, fy, fz, sh);
 #pragma unroll
-    for (int k = 0; k < Q; ++k) T::st(f, k * n + i, stored_of<S, Q>(g[k], k));
+    for (int k = 0; k < Q; ++k) T::st(f, k * n + i, stored_sh<S>(sh, g[k], k));
     force[j] = (double)fx;
     force[nl + j] = (double)fy;
     force[2 * nl + j] = (double)fz;
@@ -559,7 +560,7 @@ template <int Q, class S, int COLL>
 __global__ void k_pull_collide(const int32_t *__restrict__ list, int64_t nl, int64_t n, int textbook,
                                const int32_t *__restrict__ nbr, const S *__restrict__ fcol, S *__restrict__ f,
                                S *__restrict__ fnext, double tau, typename Store<S>::C *__restrict__ rho,
-                               typename Store<S>::C *__restrict__ u, int macros)
+                               typename Store<S>::C *__restrict__ u, int macros, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -571,7 +572,7 @@ __global__ void k_pull_collide(const int32_t *__restrict__ list, int64_t nl, int
         S v[Q];
         pull_cell<Q, S>(i, n, textbook, nbr, fcol, f, v);
 #pragma unroll
-        for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::cv(v[k]), k);
+        for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::cv(v[k]), k);
     }
     C r, x, y, z;
     macros_g<Q, C>(d, r, x, y, z);
@@ -581,7 +582,7 @@ __global__ void k_pull_collide(const int32_t *__restrict__ list, int64_t nl, int
         u[n + i] = y;
         u[2 * n + i] = z;
     }
-    collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i);
+    collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i, sh);
 }
 
 // stream on overlap_C2F cells and their next collision, fcol = f
@@ -625,7 +626,7 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
                                            const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext,
                                            double tau, typename Store<S>::C *__restrict__ rho,
                                            typename Store<S>::C *__restrict__ u, int macros, int fall,
-                                           long long *__restrict__ acc)
+                                           long long *__restrict__ acc, const Shift &sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -673,7 +674,7 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
                 if (acc) {
                     C d[Q];
 #pragma unroll
-                    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::cv(v[k]), k);
+                    for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::cv(v[k]), k);
                     C r, x, y, z;
                     macros_g<Q, C>(d, r, x, y, z);
                     rho[i] = r;
@@ -689,7 +690,7 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
         }
         C d[Q];
 #pragma unroll
-        for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::cv(v[k]), k);
+        for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::cv(v[k]), k);
         C r, x, y, z;
         macros_g<Q, C>(d, r, x, y, z);
         if (macros) {
@@ -698,7 +699,7 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
             u[n + i] = y;
             u[2 * n + i] = z;
         }
-        collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i);
+        collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i, sh);
     }
 }
 
@@ -716,14 +717,14 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? ((COLL == MT_COLL_
     int64_t nb, const int32_t *__restrict__ halo, const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
     const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext, double tau,
     typename Store<S>::C *__restrict__ rho, typename Store<S>::C *__restrict__ u, int macros, int fall,
-    long long *__restrict__ acc)
+    long long *__restrict__ acc, const Shift sh)
 {
     __shared__ int32_t s_idx[4][216];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t b = 4 * (int64_t)blockIdx.x + w;
     if (b >= nb) return;
     brick_warp<Q, S, COLL>(b, lane, s_idx[w], halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros, fall,
-                           acc);
+                           acc, sh);
 }
 
 // The same pass over the bricks of many cases (a batch): brick b of the work
@@ -733,7 +734,8 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? ((COLL == MT_COLL_
 #define MT_BRICK_BATCH_MIN_BLOCKS MT_BRICK_MIN_BLOCKS  // the same for the batched pass
 #endif
 template <int Q, class S, int COLL>
-__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_BATCH_MIN_BLOCKS : 1) k_brick_step_batch(const BrickBatch *__restrict__ bb)
+__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_BATCH_MIN_BLOCKS : 1) k_brick_step_batch(const BrickBatch *__restrict__ bb,
+                                                                                                   const Shift sh)
 {
     __shared__ int32_t s_idx[4][216];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -750,7 +752,7 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_BATCH_MIN
     const BrickSlot &sl = bb->slot[lo];
     using C = typename Store<S>::C;
     brick_warp<Q, S, COLL>(b - bb->off[lo], lane, s_idx[w], sl.halo, sl.cls, sl.n, sl.textbook, (const S *)sl.fcol,
-                           (S *)sl.f, (S *)sl.fnext, sl.tau, (C *)sl.rho, (C *)sl.u, sl.macros, sl.fall, sl.acc);
+                           (S *)sl.f, (S *)sl.fnext, sl.tau, (C *)sl.rho, (C *)sl.u, sl.macros, sl.fall, sl.acc, sh);
 }
 
 // The streamed f of the class-1 cells, from the buffer the last fused pass
@@ -791,7 +793,7 @@ __global__ void __launch_bounds__(128) k_brick_pull(int64_t nb, const int32_t *_
 template <int Q, int FH, class S, int COLL>
 __global__ void k_ib_collide(const int32_t *list, int64_t nl, int64_t n, const int32_t *disrow, const double *dis,
                              const int32_t *nbr, const S *fcol, S *f, S *fnext, double tau, double *force,
-                             typename Store<S>::C *rho, typename Store<S>::C *u, int macros)
+                             typename Store<S>::C *rho, typename Store<S>::C *u, int macros, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -802,19 +804,19 @@ __global__ void k_ib_collide(const int32_t *list, int64_t nl, int64_t n, const i
     C g[Q], fx, fy, fz;
     {
 #pragma unroll
-        for (int k = 0; k < Q; ++k) g[k] = full_of<S, Q>(T::ld(f, k * n + i), k);
+        for (int k = 0; k < Q; ++k) g[k] = full_sh<S>(sh, T::ld(f, k * n + i), k);
         C r, x, y, z;
         macros_g<Q, C>(g, r, x, y, z);
-        ib_cell<Q, FH, S>(i, n, dr, nbr, fcol, r, g, fx, fy, fz);
+        ib_cell<Q, FH, S>(i, n, dr, nbr, fcol, r, g, fx, fy, fz, sh);
     }
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-        const C st = stored_of<S, Q>(g[k], k);
+        const C st = stored_sh<S>(sh, g[k], k);
         T::st(f, k * n + i, st);
         // the next collision reads the stored value
         S sv;
         T::st(&sv, 0, st);
-        g[k] = full_of<S, Q>(T::cv(sv), k);
+        g[k] = full_sh<S>(sh, T::cv(sv), k);
     }
     force[j] = (double)fx;
     force[nl + j] = (double)fy;
@@ -827,7 +829,7 @@ __global__ void k_ib_collide(const int32_t *list, int64_t nl, int64_t n, const i
         u[n + i] = y;
         u[2 * n + i] = z;
     }
-    collide_store<Q, S, COLL>(g, r, x, y, z, tau, fnext, n, i);
+    collide_store<Q, S, COLL>(g, r, x, y, z, tau, fnext, n, i, sh);
 }
 
 // ---- direct-forcing immersed boundary (Lagrangian markers) --------------------
@@ -854,7 +856,7 @@ __host__ __device__ __forceinline__ double roma3(double r)
 // band's force accumulator restarts from zero
 template <int Q, class S>
 __global__ void k_band_macros(const int32_t *band, int64_t nb, int64_t n, const S *f, typename Store<S>::C *rho,
-                              typename Store<S>::C *u, long long *acc)
+                              typename Store<S>::C *u, long long *acc, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -863,7 +865,7 @@ __global__ void k_band_macros(const int32_t *band, int64_t nb, int64_t n, const 
     const int64_t i = band[j];
     C d[Q];
 #pragma unroll
-    for (int k = 0; k < Q; ++k) d[k] = full_of<S, Q>(T::ld(f, k * n + i), k);
+    for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::ld(f, k * n + i), k);
     C r, x, y, z;
     macros_g<Q, C>(d, r, x, y, z);
     rho[i] = r;
@@ -996,7 +998,7 @@ static __global__ void __launch_bounds__(256) k_df_sum(const double *fk, int64_t
 // (the band's rho and unforced velocity are written by k_band_macros)
 template <int Q, class S>
 __global__ void k_band_collide(const int32_t *band, int64_t nb, int64_t n, double tau, const S *f,
-                               const long long *acc, S *fcol)
+                               const long long *acc, S *fcol, const Shift sh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -1004,9 +1006,9 @@ __global__ void k_band_collide(const int32_t *band, int64_t nb, int64_t n, doubl
     if (j >= nb) return;
     const int64_t i = band[j];
     if constexpr (T::shifted) {
-        // reduced precision: the stored deviations s = f - w throughout (the
-        // weights sum to 1 and have no first moment), the forcing term as
-        // 3 (e.g - u.g) + 9 (e.u)(e.g)
+        // reduced precision: the stored deviations s = f - s_k throughout
+        // (the shift sums to 1 and its first moment is u_s), the forcing term
+        // as 3 (e.g - u.g) + 9 (e.u)(e.g)
         float sd[Q];
         float rd = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
 #pragma unroll
@@ -1020,6 +1022,9 @@ __global__ void k_band_collide(const int32_t *band, int64_t nb, int64_t n, doubl
         const float gx = (float)((double)acc[i] * kForceInv), gy = (float)((double)acc[n + i] * kForceInv),
                     gz = (float)((double)acc[2 * n + i] * kForceInv);
         const float r = 1.f + rd;
+        jx += sh.u[0];
+        jy += sh.u[1];
+        jz += sh.u[2];
         const float rs = (r > -1e-6f && r < 1e-6f) ? ((r < 0.f) ? -1e-6f : 1e-6f) : r;
         const float ir = 1.f / rs;
         const float x = (jx + 0.5f * gx) * ir, y = (jy + 0.5f * gy) * ir, z = (jz + 0.5f * gz) * ir;
@@ -1032,7 +1037,7 @@ __global__ void k_band_collide(const int32_t *band, int64_t nb, int64_t n, doubl
             const float eu = ex(k) * x + ey(k) * y + ez(k) * z;
             const float eg = ex(k) * gx + ey(k) * gy + ez(k) * gz;
             const float wk = (float)w<Q>(k);
-            const float dfeq = wk * ((r - 1.f) + r * (3.f * eu + 4.5f * eu * eu - uu));
+            const float dfeq = wk * ((r - 1.f) + r * (3.f * eu + 4.5f * eu * eu - uu)) - sh.dw[k];
             const float ge = 3.f * (eg - ug) + 9.f * eu * eg;
             T::st(fcol, k * n + i, fmaf(om, dfeq - sd[k], sd[k]) + fpre * wk * ge);
         }
@@ -1042,7 +1047,7 @@ __global__ void k_band_collide(const int32_t *band, int64_t nb, int64_t n, doubl
     C r = 0, jx = 0, jy = 0, jz = 0;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-        d[k] = full_of<S, Q>(T::ld(f, k * n + i), k);
+        d[k] = full_sh<S>(sh, T::ld(f, k * n + i), k);
         r += d[k];
         jx += d[k] * ex(k);
         jy += d[k] * ey(k);
@@ -1063,7 +1068,7 @@ __global__ void k_band_collide(const int32_t *band, int64_t nb, int64_t n, doubl
         const C ge = (C(3) * (ex(k) - x) + C(9) * eu * ex(k)) * gx + (C(3) * (ey(k) - y) + C(9) * eu * ey(k)) * gy +
                      (C(3) * (ez(k) - z) + C(9) * eu * ez(k)) * gz;
         const C out = d[k] - (d[k] - feq) * om + fpre * (C)w<Q>(k) * ge;
-        T::st(fcol, k * n + i, stored_of<S, Q>(out, k));
+        T::st(fcol, k * n + i, stored_sh<S>(sh, out, k));
     }
 }
 
@@ -1109,15 +1114,15 @@ static __global__ void k_force_reduce(const double *force, int64_t nl, double *a
 static __global__ void k_force_tick(double *acc) { acc[3] += 1.0; }
 
 template <int Q, class S>
-__global__ void k_to_f64(const S *src, double *dst, int64_t n)
+__global__ void k_to_f64(const S *src, double *dst, int64_t n, const Shift sh)
 {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
 #pragma unroll
-    for (int k = 0; k < Q; ++k) dst[k * n + i] = (double)full_of<S, Q>(Store<S>::ld(src, k * n + i), k);
+    for (int k = 0; k < Q; ++k) dst[k * n + i] = (double)full_sh<S>(sh, Store<S>::ld(src, k * n + i), k);
 }
 template <int Q, class S>
-__global__ void k_from_f64(const double *src, S *dst, int64_t n)
+__global__ void k_from_f64(const double *src, S *dst, int64_t n, const Shift sh)
 {
     using C = typename Store<S>::C;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -1125,7 +1130,7 @@ __global__ void k_from_f64(const double *src, S *dst, int64_t n)
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const double v = src[k * n + i];
-        Store<S>::st(dst, k * n + i, (C)(Store<S>::shifted ? v - w<Q>(k) : v));
+        Store<S>::st(dst, k * n + i, stored_f64<S>(sh, v, k));
     }
 }
 template <class C>
@@ -1242,7 +1247,7 @@ int df_force(Ctx &ctx, Case &c, int l, bool band_macros_done = false)
     if (!lv.nband) return MT_OK;
     if (!band_macros_done) {
         k_band_macros<Q, S><<<grid_for(lv.nband, 128), 128, 0, s>>>(lv.band, lv.nband, lv.n, A::f(lv), A::rho(lv),
-                                                                     A::u(lv), c.acc);
+                                                                     A::u(lv), c.acc, c.shift);
         MT_LAUNCHED(ctx);
     }
     if (!c.nm) {
@@ -1269,7 +1274,7 @@ int band_collide(Ctx &ctx, Case &c, int l, void *out)
     Level &lv = c.lv[l];
     if (!lv.nband) return MT_OK;
     k_band_collide<Q, S><<<grid_for(lv.nband, 64), 64, 0, ctx.stream>>>(lv.band, lv.nband, lv.n, c.d.tau[l],
-                                                                         A::f(lv), c.acc, (S *)out);
+                                                                         A::f(lv), c.acc, (S *)out, c.shift);
     MT_LAUNCHED(ctx);
     return MT_OK;
 }
@@ -1286,7 +1291,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
     case PH_MACROS:
         if (lv.ncollide) {
             k_macros<Q, S><<<grid_for(lv.ncollide, B), B, 0, s>>>(lv.collide_list, lv.ncollide, n, A::f(lv),
-                                                                   A::rho(lv), A::u(lv));
+                                                                   A::rho(lv), A::u(lv), c.shift);
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
@@ -1297,12 +1302,12 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         if (ncl) {
             if (c.d.collision == MT_COLL_LBGK) {
                 k_collide<Q, S, MT_COLL_LBGK><<<grid_for(ncl, B), B, 0, s>>>(cl, ncl, n, c.d.tau[l], A::f(lv),
-                                                                             A::rho(lv), A::u(lv), A::fcol(lv));
+                                                                             A::rho(lv), A::u(lv), A::fcol(lv), c.shift);
             } else {
                 // the cumulant model exists for D3Q27 only (checked at case creation)
                 if constexpr (Q == 27)
                     k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(ncl, 64), 64, 0, s>>>(
-                        cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv));
+                        cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv), c.shift);
             }
             MT_LAUNCHED(ctx);
         }
@@ -1327,7 +1332,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         const double scale = c2f_scale(c, l);
         k_explosion<Q, S><<<grid_for(8 * lv.nexpl, B), B, 0, s>>>(lv.expl_src, lv.expl_child, lv.nexpl, cl.n, A::fcol(cl),
                                                                n, A::fcol(lv), scale, (S *)lv.fcol_alt,
-                                                               lv.nexpl_f2c);
+                                                               lv.nexpl_f2c, c.shift);
         MT_LAUNCHED(ctx);
         return MT_OK;
     }
@@ -1336,7 +1341,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         Level &fl = c.lv[l + 1];
         const double scale = f2c_scale(c, l);
         k_coalescence<Q, S><<<grid_for(lv.nlist[1], B), B, 0, s>>>(lv.list[1], lv.coal_child, lv.nlist[1], n,
-                                                                    A::f(lv), A::f(fl), fl.n, scale);
+                                                                    A::f(lv), A::f(fl), fl.n, scale, c.shift);
         MT_LAUNCHED(ctx);
         return MT_OK;
     }
@@ -1357,7 +1362,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             for (int ph = 0; ph < 2; ++ph) {
                 k_bc_neq_all<Q, S><<<grid_for(c.nbc_all, B), B, 0, s>>>(c.bc_all, c.bc_setb, c.nbc_all, l0.n, l0.nbr,
                                                                          A::rho(l0), A::u(l0), A::f(l0), ub,
-                                                                         c.bc_tmp_all, ph, c.dev_err);
+                                                                         c.bc_tmp_all, ph, c.dev_err, c.shift);
                 MT_LAUNCHED(ctx);
             }
             return MT_OK;
@@ -1372,7 +1377,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
                 for (int ph = 0; ph < 2; ++ph) {
                     k_bc_neq<Q, S><<<grid_for(l0.nbc[b], B), B, 0, s>>>(
                         l0.bclist[b], l0.nbc[b], b, l0.n, l0.nbr, A::rho(l0), A::u(l0), A::f(l0), c.face_u[face][0],
-                        c.face_u[face][1], c.face_u[face][2], tmp, ph, c.dev_err);
+                        c.face_u[face][1], c.face_u[face][2], tmp, ph, c.dev_err, c.shift);
                     MT_LAUNCHED(ctx);
                 }
             }
@@ -1384,7 +1389,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             if (!l0.nbc[face]) continue;
             k_bc_inout<Q, S><<<grid_for(l0.nbc[face], B), B, 0, s>>>(l0.bclist[face], l0.nbc[face], face, l0.n, l0.nbr,
                                                                       c.d.rho0, A::f(l0), A::fcol(l0), c.face_u[0][0],
-                                                                      c.face_u[0][1], c.face_u[0][2], c.dev_err);
+                                                                      c.face_u[0][1], c.face_u[0][2], c.dev_err, c.shift);
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
@@ -1399,10 +1404,10 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         }
         if (c.d.ib_method == MT_IB_FH)
             k_ib_treat<Q, 1, S><<<grid_for(fl.nib, 64), 64, 0, s>>>(fl.iblist, fl.nib, fl.n, fl.disrow, c.dis, fl.nbr,
-                                                                     A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force);
+                                                                     A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force, c.shift);
         else
             k_ib_treat<Q, 0, S><<<grid_for(fl.nib, 64), 64, 0, s>>>(fl.iblist, fl.nib, fl.n, fl.disrow, c.dis, fl.nbr,
-                                                                     A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force);
+                                                                     A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force, c.shift);
         MT_LAUNCHED(ctx);
         // ib_force holds 3 * nib per-cell values followed by room for the partials
         const unsigned nb = grid_for(fl.nib, 256);
@@ -1418,11 +1423,11 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         if (lv.nlist[1]) {
             if (c.d.collision == MT_COLL_LBGK) {
                 k_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nlist[1], B), B, 0, s>>>(
-                    lv.list[1], lv.nlist[1], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv));
+                    lv.list[1], lv.nlist[1], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv), c.shift);
             } else {
                 if constexpr (Q == 27)
                     k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nlist[1], 64), 64, 0, s>>>(
-                        lv.list[1], lv.nlist[1], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv));
+                        lv.list[1], lv.nlist[1], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv), c.shift);
             }
             MT_LAUNCHED(ctx);
         }
@@ -1434,12 +1439,12 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         if (c.d.collision == MT_COLL_LBGK) {
             k_coal_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nlist[1], 64), 64, 0, s>>>(
                 lv.list[1], lv.coal_child, lv.nlist[1], n, A::f(lv), A::f(fl), fl.n, scale, c.d.tau[l],
-                (S *)lv.fcol_alt, A::rho(lv), A::u(lv), c.macros_now);
+                (S *)lv.fcol_alt, A::rho(lv), A::u(lv), c.macros_now, c.shift);
         } else {
             if constexpr (Q == 27)
                 k_coal_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nlist[1], 64), 64, 0, s>>>(
                     lv.list[1], lv.coal_child, lv.nlist[1], n, A::f(lv), A::f(fl), fl.n, scale, c.d.tau[l],
-                    (S *)lv.fcol_alt, A::rho(lv), A::u(lv), c.macros_now);
+                    (S *)lv.fcol_alt, A::rho(lv), A::u(lv), c.macros_now, c.shift);
         }
         MT_LAUNCHED(ctx);
         return MT_OK;
@@ -1454,7 +1459,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             if (!l0.nbc[b]) continue;
             k_bc_set_eq<Q, S><<<grid_for(l0.nbc[b], B), B, 0, s>>>(l0.bclist[b], l0.nbc[b], l0.n, c.d.rho0,
                                                                     c.face_u[face][0], c.face_u[face][1],
-                                                                    c.face_u[face][2], A::f(l0), A::fcol(l0));
+                                                                    c.face_u[face][2], A::f(l0), A::fcol(l0), c.shift);
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
@@ -1490,11 +1495,11 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             if (ncl) {
                 if (c.d.collision == MT_COLL_LBGK) {
                     k_collide<Q, S, MT_COLL_LBGK><<<grid_for(ncl, B), B, 0, s>>>(
-                        cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt);
+                        cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt, c.shift);
                 } else {
                     if constexpr (Q == 27)
                         k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(ncl, 64), 64, 0, s>>>(
-                            cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt);
+                            cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt, c.shift);
                 }
                 MT_LAUNCHED(ctx);
             }
@@ -1533,7 +1538,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
                     constexpr int FH = decltype(fh)::value, COLL = decltype(coll)::value;
                     k_ib_collide<Q, FH, S, COLL><<<grid_for(lv.nib, 64), 64, 0, is>>>(
                         lv.iblist, lv.nib, n, lv.disrow, c.dis, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt, tau,
-                        c.ib_force, A::rho(lv), A::u(lv), mac);
+                        c.ib_force, A::rho(lv), A::u(lv), mac, c.shift);
                 };
                 using I0 = std::integral_constant<int, 0>;
                 using I1 = std::integral_constant<int, 1>;
@@ -1565,13 +1570,13 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             if (c.d.collision == MT_COLL_LBGK) {
                 k_brick_step<Q, S, MT_COLL_LBGK><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb, A::fcol(lv),
                                                                    A::f(lv), (S *)lv.fcol_alt, c.d.tau[l],
-                                                                   A::rho(lv), A::u(lv), mac, fall, bacc);
+                                                                   A::rho(lv), A::u(lv), mac, fall, bacc, c.shift);
             } else {
                 if constexpr (Q == 27)
                     k_brick_step<Q, S, MT_COLL_CUMULANT><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb,
                                                                            A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
                                                                            c.d.tau[l], A::rho(lv), A::u(lv), mac,
-                                                                           fall, nullptr);
+                                                                           fall, nullptr, c.shift);
             }
             MT_LAUNCHED(ctx);
         } else {
@@ -1579,12 +1584,12 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
                 if (c.d.collision == MT_COLL_LBGK) {
                     k_pull_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nfused, B), B, 0, s>>>(
                         lv.fused_list, lv.nfused, n, tb, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
-                        c.d.tau[l], A::rho(lv), A::u(lv), mac);
+                        c.d.tau[l], A::rho(lv), A::u(lv), mac, c.shift);
                 } else {
                     if constexpr (Q == 27)
                         k_pull_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nfused, 64), 64, 0, s>>>(
                             lv.fused_list, lv.nfused, n, tb, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
-                            c.d.tau[l], A::rho(lv), A::u(lv), mac);
+                            c.d.tau[l], A::rho(lv), A::u(lv), mac, c.shift);
                 }
                 MT_LAUNCHED(ctx);
             }
@@ -1651,10 +1656,10 @@ int AmrOps<S>::init_eq(Ctx &ctx, Case &c, double rho0, const double *u0)
         if (!lv.n) continue;
         if (c.d.q == 19)
             k_init_eq<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(lv.n, lv.tag, rho0, u0[0], u0[1], u0[2],
-                                                                           A::f(lv), A::fcol(lv), A::rho(lv), A::u(lv));
+                                                                           A::f(lv), A::fcol(lv), A::rho(lv), A::u(lv), c.shift);
         else
             k_init_eq<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(lv.n, lv.tag, rho0, u0[0], u0[1], u0[2],
-                                                                           A::f(lv), A::fcol(lv), A::rho(lv), A::u(lv));
+                                                                           A::f(lv), A::fcol(lv), A::rho(lv), A::u(lv), c.shift);
         MT_LAUNCHED(ctx);
     }
     return MT_OK;
@@ -1667,9 +1672,9 @@ int AmrOps<S>::get(Ctx &ctx, Case &c, int l, int which, double *d_out)
     const S *src = (const S *)(which == 0 ? lv.f : lv.fcol);
     if (!lv.n) return MT_OK;
     if (c.d.q == 19)
-        k_to_f64<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(src, d_out, lv.n);
+        k_to_f64<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(src, d_out, lv.n, c.shift);
     else
-        k_to_f64<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(src, d_out, lv.n);
+        k_to_f64<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(src, d_out, lv.n, c.shift);
     MT_LAUNCHED(ctx);
     return MT_OK;
 }
@@ -1681,9 +1686,9 @@ int AmrOps<S>::set(Ctx &ctx, Case &c, int l, int which, const double *d_in)
     S *dst = (S *)(which == 0 ? lv.f : lv.fcol);
     if (!lv.n) return MT_OK;
     if (c.d.q == 19)
-        k_from_f64<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(d_in, dst, lv.n);
+        k_from_f64<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(d_in, dst, lv.n, c.shift);
     else
-        k_from_f64<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(d_in, dst, lv.n);
+        k_from_f64<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(d_in, dst, lv.n, c.shift);
     MT_LAUNCHED(ctx);
     return MT_OK;
 }
@@ -1702,16 +1707,16 @@ int AmrOps<S>::macros_out(Ctx &ctx, Case &c, int l, double *d_rho, double *d_u)
 }
 
 template <class S>
-int AmrOps<S>::batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total)
+int AmrOps<S>::batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total, const Shift &sh)
 {
     const unsigned g = grid_for(total, 4);
     if (!g) return MT_OK;
     if (q == 19)
-        k_brick_step_batch<19, S, MT_COLL_LBGK><<<g, 128, 0, ctx.stream>>>(d_desc);
+        k_brick_step_batch<19, S, MT_COLL_LBGK><<<g, 128, 0, ctx.stream>>>(d_desc, sh);
     else if (coll == MT_COLL_LBGK)
-        k_brick_step_batch<27, S, MT_COLL_LBGK><<<g, 128, 0, ctx.stream>>>(d_desc);
+        k_brick_step_batch<27, S, MT_COLL_LBGK><<<g, 128, 0, ctx.stream>>>(d_desc, sh);
     else
-        k_brick_step_batch<27, S, MT_COLL_CUMULANT><<<g, 128, 0, ctx.stream>>>(d_desc);
+        k_brick_step_batch<27, S, MT_COLL_CUMULANT><<<g, 128, 0, ctx.stream>>>(d_desc, sh);
     MT_LAUNCHED(ctx);
     return MT_OK;
 }
@@ -1779,7 +1784,8 @@ template <class S> struct RemapLevels {
 // that is solid in the source takes the equilibrium at rest.  kind[i]: 0..3.
 template <int Q, class S>
 __global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, int L, int l, RemapLevels<S> src,
-                        double rho0, double ux0, double uy0, double uz0, S *fo, S *co, uint8_t *kind)
+                        double rho0, double ux0, double uy0, double uz0, S *fo, S *co, uint8_t *kind, const Shift dsh,
+                        const Shift ssh, int same_shift)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -1789,8 +1795,8 @@ __global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, 
     double a[Q], b[Q];
     auto put = [&](const double *pf, const double *pc, int kd) {
         for (int q = 0; q < Q; ++q) {
-            T::st(fo, q * nd + i, stored_of<S, Q>((C)pf[q], q));
-            T::st(co, q * nd + i, stored_of<S, Q>((C)pc[q], q));
+            T::st(fo, q * nd + i, stored_sh<S>(dsh, (C)pf[q], q));
+            T::st(co, q * nd + i, stored_sh<S>(dsh, (C)pc[q], q));
         }
         kind[i] = (uint8_t)kd;
     };
@@ -1807,9 +1813,16 @@ __global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, 
         j = -1;
     }
     if (j >= 0) {
-        for (int q = 0; q < Q; ++q) {
-            fo[q * nd + i] = same.f[q * same.n + j];
-            co[q * nd + i] = same.fcol[q * same.n + j];
+        if (same_shift) {
+            for (int q = 0; q < Q; ++q) {
+                fo[q * nd + i] = same.f[q * same.n + j];
+                co[q * nd + i] = same.fcol[q * same.n + j];
+            }
+        } else {
+            for (int q = 0; q < Q; ++q) {
+                T::st(fo, q * nd + i, stored_sh<S>(dsh, full_sh<S>(ssh, T::ld(same.f, q * same.n + j), q), q));
+                T::st(co, q * nd + i, stored_sh<S>(dsh, full_sh<S>(ssh, T::ld(same.fcol, q * same.n + j), q), q));
+            }
         }
         kind[i] = 0;
         return;
@@ -1824,8 +1837,8 @@ __global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, 
         const int64_t jm = find_key(cs.key, cs.n, cell_key_at(L, m, x >> up, y >> up, z >> up));
         if (jm < 0) continue;
         for (int q = 0; q < Q; ++q) {
-            a[q] = (double)full_of<S, Q>(T::ld(cs.f, q * cs.n + jm), q);
-            b[q] = (double)full_of<S, Q>(T::ld(cs.fcol, q * cs.n + jm), q);
+            a[q] = (double)full_sh<S>(ssh, T::ld(cs.f, q * cs.n + jm), q);
+            b[q] = (double)full_sh<S>(ssh, T::ld(cs.fcol, q * cs.n + jm), q);
         }
         remap_rescale<Q>(a, src.up_f[m]);
         remap_rescale<Q>(b, src.up_c[m]);
@@ -1843,8 +1856,8 @@ __global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, 
             const int64_t jc = find_key(fine.key, fine.n, cell_key_at(L, l + d, cx, cy, cz));
             if (jc < 0 || (fine.tag[jc] & TAG_SF)) continue;
             for (int q = 0; q < Q; ++q) {
-                a[q] += (double)full_of<S, Q>(T::ld(fine.f, q * fine.n + jc), q);
-                b[q] += (double)full_of<S, Q>(T::ld(fine.fcol, q * fine.n + jc), q);
+                a[q] += (double)full_sh<S>(ssh, T::ld(fine.f, q * fine.n + jc), q);
+                b[q] += (double)full_sh<S>(ssh, T::ld(fine.fcol, q * fine.n + jc), q);
             }
             ++nch;
         }
@@ -1872,6 +1885,9 @@ int AmrOps<S>::remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts)
 {
     const int L = dst.d.max_level, Q = dst.d.q;
     RemapLevels<S> rl;
+    // equal storage shifts: cells present on both lattices copy their stored values
+    int same_shift = 1;
+    for (int k = 0; k < 27; ++k) same_shift &= dst.shift.d[k] == src.shift.d[k];
     for (int m = 0; m <= L && m <= src.d.max_level; ++m) {
         if (!src.lv[m].n) continue;
         rl.lv[m].key = src.lv[m].key;
@@ -1912,10 +1928,12 @@ int AmrOps<S>::remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts)
         const double r0 = dst.d.rho0, u0 = dst.d.u_bc[0], u1 = dst.d.u_bc[1], u2 = dst.d.u_bc[2];
         if (Q == 19)
             k_remap<19, S><<<grid_for(lv.n, 128), 128, 0, ctx.stream>>>(lv.key, lv.tag, lv.n, L, l, rl, r0, u0, u1, u2,
-                                                                       (S *)lv.f, (S *)lv.fcol, kind);
+                                                                       (S *)lv.f, (S *)lv.fcol, kind, dst.shift, src.shift,
+                                                                       same_shift);
         else
             k_remap<27, S><<<grid_for(lv.n, 128), 128, 0, ctx.stream>>>(lv.key, lv.tag, lv.n, L, l, rl, r0, u0, u1, u2,
-                                                                       (S *)lv.f, (S *)lv.fcol, kind);
+                                                                       (S *)lv.f, (S *)lv.fcol, kind, dst.shift, src.shift,
+                                                                       same_shift);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) {
             rc = set_err(ctx, MT_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));

@@ -119,6 +119,8 @@ struct BrickBatch {
     BrickSlot slot[kMaxBatchSlots];
 };
 
+inline constexpr double kZeroU[3] = {0.0, 0.0, 0.0};
+
 struct Case {
     mt_case_desc d{};
     bool dense = false;
@@ -158,6 +160,7 @@ struct Case {
     // lookahead buffers hold the collision of the current f
     int schedule = MT_SCHED_PHASES;
     int scaling = MT_SCALE_REFERENCE;  // interface rescaling of the non-equilibrium part
+    Shift shift = make_shift(19, kZeroU);  // storage shift of the reduced storages (from d.u_shift)
     double face_u[6][3] = {};          // bc_velocity of each face's strategy (u_bc unless set)
     // direct-forcing markers (MT_IB_DF)
     int64_t nm = 0;
@@ -252,7 +255,7 @@ template <class S> struct AmrOps {
     static int macros_out(Ctx &ctx, Case &c, int level, double *d_rho, double *d_u);
     static int guard(Ctx &ctx, Case &c);
     // batched brick pass (descriptor in device memory, total bricks known on the host)
-    static int batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total);
+    static int batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total, const Shift &sh);
     // src's state carried onto dst's lattice (same Q, levels, storage)
     static int remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts);
 };

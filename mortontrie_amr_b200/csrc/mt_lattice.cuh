@@ -43,6 +43,35 @@ template <int Q> MT_HD constexpr double w(int k)
     return Q == 19 ? (k == 0 ? 1. / 3. : (k <= 6 ? 1. / 18. : 1. / 36.))
                    : (k == 0 ? 8. / 27. : (k <= 6 ? 2. / 27. : (k <= 18 ? 1. / 54. : 1. / 216.)));
 }
+// Storage shift of the reduced storages (FP32, FP16, BF16): they keep
+// f_k - s_k with s_k = feq_k(1, u_s) = w_k (1 + 3 e.u_s + 4.5 (e.u_s)^2 -
+// 1.5 u_s^2), so the stored deviations are small where the flow is near u_s
+// (u_s = 0: s_k = w_k).  v: s_k rounded to FP32 (the compute type), dw: s_k -
+// w_k rounded to FP32, d: s_k in FP64 (conversions from FP64 values), u: u_s.
+// Kernels take it by value: with the direction loops unrolled its entries are
+// constant-bank operands, as the literal weights were.
+struct Shift {
+    float v[27];
+    float dw[27];
+    float u[3];
+    double d[27];
+};
+inline Shift make_shift(int q, const double *us)
+{
+    Shift s{};
+    const double uu = us[0] * us[0] + us[1] * us[1] + us[2] * us[2];
+    for (int k = 0; k < q; ++k) {
+        const double wk = q == 19 ? w<19>(k) : w<27>(k);
+        const double eu = ex(k) * us[0] + ey(k) * us[1] + ez(k) * us[2];
+        const double dw = wk * (3.0 * eu + 4.5 * eu * eu - 1.5 * uu);
+        s.d[k] = wk + dw;
+        s.v[k] = (float)s.d[k];
+        s.dw[k] = (float)dw;
+    }
+    for (int a = 0; a < 3; ++a) s.u[a] = (float)us[a];
+    return s;
+}
+
 // D3Q19 weights used by the solid-boundary treatment for every Q; entries
 // 19..26 are zero (ComplexBoundary_Manager.cpp:102-107,184-189).
 MT_HD constexpr double w19z(int k) { return k >= 19 ? 0.0 : w<19>(k); }

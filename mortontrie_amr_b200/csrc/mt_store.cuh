@@ -57,16 +57,34 @@ template <> struct Store<__nv_bfloat16> {
     }
 };
 
-// full population value of direction k from a stored value, and back
-template <class S, int Q> __device__ __forceinline__ typename Store<S>::C full_of(typename Store<S>::C v, int k)
+// full population value of direction k from a stored value, and back, under
+// the case's storage shift (u_s = 0: the weights)
+template <class S>
+__device__ __forceinline__ typename Store<S>::C full_sh(const Shift &sh, typename Store<S>::C v, int k)
 {
     using C = typename Store<S>::C;
-    return Store<S>::shifted ? v + (C)w<Q>(k) : v;
+    if constexpr (Store<S>::shifted)
+        return v + (C)sh.v[k];
+    else
+        return v;
 }
-template <class S, int Q> __device__ __forceinline__ typename Store<S>::C stored_of(typename Store<S>::C v, int k)
+template <class S>
+__device__ __forceinline__ typename Store<S>::C stored_sh(const Shift &sh, typename Store<S>::C v, int k)
 {
     using C = typename Store<S>::C;
-    return Store<S>::shifted ? v - (C)w<Q>(k) : v;
+    if constexpr (Store<S>::shifted)
+        return v - (C)sh.v[k];
+    else
+        return v;
+}
+// the stored value of an FP64 population (subtraction in FP64, one rounding)
+template <class S> __device__ __forceinline__ typename Store<S>::C stored_f64(const Shift &sh, double v, int k)
+{
+    using C = typename Store<S>::C;
+    if constexpr (Store<S>::shifted)
+        return (C)(v - sh.d[k]);
+    else
+        return (C)v;
 }
 
 }  // namespace mt

@@ -51,7 +51,7 @@ class mt_case_desc(C.Structure):
     _fields_ = [("q", C.c_int32), ("max_level", C.c_int32), ("collision", C.c_int32), ("ib_method", C.c_int32),
                 ("bc_mode", C.c_int32), ("stream_convention", C.c_int32), ("storage", C.c_int32),
                 ("periodic", C.c_int32 * 3), ("extent0", C.c_int64 * 3), ("tau", C.c_double * MAX_LEVELS),
-                ("rho0", C.c_double), ("u_bc", C.c_double * 3)]
+                ("rho0", C.c_double), ("u_bc", C.c_double * 3), ("u_shift", C.c_double * 3)]
 
 
 class mt_mesh_spec(C.Structure):
@@ -193,7 +193,22 @@ class Context:
             pass
 
 
-def make_desc(case: Case, storage: str = None) -> mt_case_desc:
+def storage_shift_of(case: Case, storage_shift) -> tuple:
+    """The shift velocity u_s of the reduced storages: None (f - w_q),
+    "inlet" (the case's boundary velocity u_bc) or three numbers."""
+    if storage_shift is None:
+        return (0.0, 0.0, 0.0)
+    if isinstance(storage_shift, str):
+        if storage_shift != "inlet":
+            raise ValueError(f"storage_shift: None, 'inlet' or a velocity, not {storage_shift!r}")
+        return tuple(float(v) for v in case.params.u_bc)
+    u = tuple(float(v) for v in storage_shift)
+    if len(u) != 3:
+        raise ValueError("storage_shift needs three components")
+    return u
+
+
+def make_desc(case: Case, storage: str = None, storage_shift=None) -> mt_case_desc:
     p = case.params
     m = case.mesh
     d = mt_case_desc()
@@ -208,6 +223,8 @@ def make_desc(case: Case, storage: str = None) -> mt_case_desc:
         d.periodic[a] = int(m.spec.boundary[a] == "periodic")
         d.extent0[a] = int(m.spec.coarse[a])
         d.u_bc[a] = float(p.u_bc[a])
+    for a, v in enumerate(storage_shift_of(case, storage_shift)):
+        d.u_shift[a] = v
     for l, t in enumerate(p.taus(m.spec.max_level)):
         d.tau[l] = float(t)
     d.rho0 = float(p.rho0)
@@ -219,9 +236,11 @@ class LBM_Manager:
     strategy objects (collide / stream / treat / boundary) as methods."""
 
     def __init__(self, ctx: Context, case: Case, storage: str = "f64", schedule: str = "phases",
-                 scaling: str = "reference", generate: bool = False):
+                 scaling: str = "reference", generate: bool = False, storage_shift=None):
         """storage: "f64" (the reference's precision, bit-exact) or "f32" /
-        "f16" / "bf16" (FP32 arithmetic on stored deviations f - w_q).
+        "f16" / "bf16" (FP32 arithmetic on stored deviations f - s_q).
+        storage_shift: s_q = feq_q(1, u_s) of the reduced storages; None
+        (u_s = 0, s_q = w_q), "inlet" (u_s = the case's u_bc) or a velocity.
         schedule: "phases" (the reference's passes) or "fused" (stream fused
         with the next collision; same state after every coarse step).
         generate: classify the lattice on the device from the mesh spec
@@ -232,7 +251,8 @@ class LBM_Manager:
         self.q = case.params.q
         self.L = case.mesh.spec.max_level
         self.storage = storage
-        d = make_desc(case, storage)
+        self.storage_shift = storage_shift_of(case, storage_shift)
+        d = make_desc(case, storage, storage_shift)
         cid = C.c_int32()
         ctx.check(lib().mt_case_create(ctx.h, C.byref(d), C.byref(cid)), "mt_case_create")
         self.id = cid.value
@@ -437,7 +457,7 @@ class LBM_Manager:
         body's band or markers) carrying this case's state; this case is left
         as it is (close it when done)."""
         new = LBM_Manager(self.ctx, case, storage or self.storage, schedule=schedule or self.schedule,
-                          scaling=self.scaling)
+                          scaling=self.scaling, storage_shift=self.storage_shift)
         new.remap_from(self, counts=False)
         return new
 
