@@ -319,6 +319,18 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+SHIFT_NOTE = {"inlet": "feq(1, u_bc) on every level", "far_field": "feq(1, u_bc) below the finest level, w on it"}
+
+
+def _shift_of_label(label):
+    """storage_shift of a run label: *_inlet, *_far or none (w)."""
+    if label.endswith("_inlet"):
+        return "inlet"
+    if label.endswith("_far"):
+        return "far_field"
+    return None
+
+
 def amr_section(ctx, torch, steps=10, warmup=2, only=None):
     """4-level D3Q27 cumulant sphere (192x96x96 coarse, R = 6 coarse = 48
     finest cells, Re 200, u 0.04, nested boxes 4R / 2.5R / 1.75R): coarse
@@ -344,17 +356,18 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
     res = {}
     # (label, storage, schedule): the plain form is FP64 in the reference's
     # phase order; the reduced storages run the fused schedule
-    # (*_inlet: reduced storage shifted by feq(1, u_bc) instead of w)
+    # (*_inlet: reduced storage shifted by feq(1, u_bc) instead of w on every
+    # level; *_far: on the levels below the finest)
     runs = [("f64", "f64", "phases"), ("f64_fused", "f64", "fused"), ("f32", "f32", "fused"),
             ("f16", "f16", "fused"), ("bf16", "bf16", "fused"), ("f16_phases", "f16", "phases"),
-            ("f16_inlet", "f16", "fused"), ("bf16_inlet", "bf16", "fused")]
+            ("f16_inlet", "f16", "fused"), ("f16_far", "f16", "fused"), ("bf16_far", "bf16", "fused")]
     if only:
         runs = [r for r in runs if r[0] in only]
     for st, storage, schedule in runs:
         mgr = LBM_Manager(ctx, case, storage, schedule=schedule,
-                          storage_shift="inlet" if st.endswith("_inlet") else None)
-        if st.endswith("_inlet"):
-            out[st] = {"storage_shift": "feq(1, u_bc)"}
+                          storage_shift=_shift_of_label(st))
+        if _shift_of_label(st):
+            out[st] = {"storage_shift": SHIFT_NOTE[_shift_of_label(st)]}
         mgr.fluidSimulate(warmup)
         torch.cuda.synchronize()
         mgr.reset_force()
@@ -667,7 +680,8 @@ def _accuracy_case(name):
 
 def amr_accuracy(ctx, torch, steps=2500, case_name="cfg3", scaling="reference", only=None):
     """Long-run accuracy of the reduced storages (fused schedule; shifted by
-    w or, *_inlet, by feq(1, u_bc)) against the FP64 phase schedule on a
+    w, or by feq(1, u_bc) on every level (*_inlet) or below the finest
+    (*_far)) against the FP64 phase schedule on a
     sphere case: after `steps` coarse steps, the
     drag coefficient averaged over the last tenth of the run, the velocity
     field of every level's lat_f cells (relative L2), the total mass, and
@@ -681,12 +695,12 @@ def amr_accuracy(ctx, torch, steps=2500, case_name="cfg3", scaling="reference", 
     tail = max(steps // 10, 1)
     res = {}
     runs = [("f64", "f64", "phases"), ("f32", "f32", "fused"), ("f16", "f16", "fused"), ("bf16", "bf16", "fused"),
-            ("f16_inlet", "f16", "fused"), ("bf16_inlet", "bf16", "fused")]
+            ("f16_inlet", "f16", "fused"), ("f16_far", "f16", "fused"), ("bf16_far", "bf16", "fused")]
     if only:
         runs = [r for r in runs if r[0] in only or r[0] == "f64"]
     for st, storage, schedule in runs:
         mgr = LBM_Manager(ctx, case, storage, schedule=schedule, scaling=scaling,
-                          storage_shift="inlet" if st.endswith("_inlet") else None)
+                          storage_shift=_shift_of_label(st))
         t0 = time.time()
         mgr.fluidSimulate(steps - tail)
         mgr.reset_force()
@@ -704,8 +718,9 @@ def amr_accuracy(ctx, torch, steps=2500, case_name="cfg3", scaling="reference", 
             fl = (tags & 1) != 0
             u_all.append(u[:, fl])
             mass += float(rho[fl].sum())
-        res[st] = dict(u=np.concatenate(u_all, axis=1), mass=mass, cd=drag_coefficient(mgr.force(), u_in, d_fine),
-                       wall_s=round(time.time() - t0, 2), finite=finite)
+        res[st] = dict(u=np.concatenate(u_all, axis=1), u_lv=u_all, mass=mass,
+                       cd=drag_coefficient(mgr.force(), u_in, d_fine), wall_s=round(time.time() - t0, 2),
+                       finite=finite)
         mgr.close()
     ref = res["f64"]
     out = {"case": ACCURACY_CASES[case_name], "interface_scaling": scaling, "coarse_steps": steps,
@@ -715,6 +730,8 @@ def amr_accuracy(ctx, torch, steps=2500, case_name="cfg3", scaling="reference", 
         r = res[st]
         out[st] = {"cd": r["cd"], "drag_rel_vs_f64": abs(r["cd"] - ref["cd"]) / abs(ref["cd"]),
                    "velocity_l2_vs_f64": float(np.linalg.norm(r["u"] - ref["u"]) / np.linalg.norm(ref["u"])),
+                   "velocity_l2_per_level": [float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+                                             for a, b in zip(r["u_lv"], ref["u_lv"])],
                    "mass_drift_vs_f64": abs(r["mass"] - ref["mass"]) / ref["mass"], "wall_s": r["wall_s"],
                    "finite": r["finite"]}
     return out
@@ -813,7 +830,7 @@ def main():
                     help="only the largest served request alone (profiling driver of the forcing kernels)")
     ap.add_argument("--amr-variants", default=None,
                     help="comma list of multi-level runs to time (default all: "
-                         "f64,f64_fused,f32,f16,bf16,f16_phases,f16_inlet,bf16_inlet); profiling and "
+                         "f64,f64_fused,f32,f16,bf16,f16_phases,f16_inlet,f16_far,bf16_far); profiling and "
                          "accuracy runs")
     ap.add_argument("--amr-accuracy", type=int, default=0, metavar="N",
                     help="only the long-run accuracy of the reduced storages on the 4-level sphere (N coarse steps)")

@@ -83,11 +83,13 @@ typedef struct mt_case_desc {
     double tau[MT_MAX_LEVELS]; /* LBM_Manager::tau */
     double rho0;               /* U_rho0 / CF_Rho */
     double u_bc[3];            /* boundary velocity in lattice units (input_v / CF_U) */
-    /* Storage shift velocity u_s of the reduced storages (no reference
-     * counterpart): FP32/FP16/BF16 keep f_k - feq_k(1, u_s) instead of f_k, so
-     * the stored deviations stay small where the flow is near u_s (the inlet
-     * velocity for a channel flow).  All zero: f_k - w_k.  FP64 stores f. */
-    double u_shift[3];
+    /* Storage shift velocity u_s of the reduced storages, per level (no
+     * reference counterpart): FP32/FP16/BF16 keep f_k - feq_k(1, u_s) instead
+     * of f_k, so the stored deviations stay small where the flow is near u_s
+     * (the inlet velocity on the far-field levels of a channel flow; the
+     * level holding a wall is better kept at zero, since the wall
+     * populations are near w).  All zero: f_k - w_k.  FP64 stores f. */
+    double u_shift[MT_MAX_LEVELS][3];
 } mt_case_desc;
 
 typedef struct mt_ctx mt_ctx;

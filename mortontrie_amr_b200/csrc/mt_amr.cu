@@ -930,9 +930,9 @@ int batch_bricks(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cs, int l, co
 {
     // group by (q, collision, storage, storage shift): one kernel instantiation
     // each, the shift a parameter of the pass
-    auto same_shift = [](const Case &a, const Case &b) {
+    auto same_shift = [l](const Case &a, const Case &b) {
         for (int k = 0; k < 27; ++k)
-            if (a.shift.d[k] != b.shift.d[k]) return false;
+            if (a.shift[l].d[k] != b.shift[l].d[k]) return false;
         return true;
     };
     std::vector<std::vector<Case *>> groups;
@@ -980,7 +980,7 @@ int batch_bricks(Ctx &ctx, BatchRec &R, const std::vector<Case *> &cs, int l, co
             Case &c = *g[0];
             int rc = amr_dispatch(c, [&](auto *tag) {
                 using S = std::remove_pointer_t<decltype(tag)>;
-                return AmrOps<S>::batch_pass(ctx, c.d.q, c.d.collision, dev, d.total, c.shift);
+                return AmrOps<S>::batch_pass(ctx, c.d.q, c.d.collision, dev, d.total, c.shift[l]);
             });
             if (rc) return rc;
         }

@@ -170,7 +170,7 @@ __global__ void k_stream(const int32_t *list, int64_t nl, int64_t n, int textboo
 template <int Q, class S>
 __global__ void k_explosion(const int32_t *__restrict__ src, const int32_t *__restrict__ child, int64_t ns,
                             int64_t nc, const S *__restrict__ cfcol, int64_t nf, S *__restrict__ ffcol, double scale,
-                            S *__restrict__ ffcol2, int64_t nf2c, const Shift sh)
+                            S *__restrict__ ffcol2, int64_t nf2c, const Shift csh, const Shift fsh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -183,14 +183,14 @@ __global__ void k_explosion(const int32_t *__restrict__ src, const int32_t *__re
     const int64_t i = src[j];
     C d[Q];
 #pragma unroll
-    for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::ld(cfcol, k * nc + i), k);
+    for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(csh, T::ld(cfcol, k * nc + i), k);
     C r, x, y, z;
     macros_g<Q, C>(d, r, x, y, z);
     const bool both = ffcol2 && j >= nf2c;
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
-        const C v = stored_sh<S>(sh, fe + (C)scale * (d[k] - fe), k);
+        const C v = stored_sh<S>(fsh, fe + (C)scale * (d[k] - fe), k);
         T::st(ffcol, k * nf + ch, v);
         if (both) T::st(ffcol2, k * nf + ch, v);
     }
@@ -199,7 +199,7 @@ __global__ void k_explosion(const int32_t *__restrict__ src, const int32_t *__re
 // AMR_transDDF_coalescence (LBM_Manager.cpp:1131-1169)
 template <int Q, class S>
 __global__ void k_coalescence(const int32_t *list, const int32_t *child, int64_t nl, int64_t nc, S *cf, const S *ff,
-                              int64_t nf, double scale, const Shift sh)
+                              int64_t nf, double scale, const Shift csh, const Shift fsh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -214,7 +214,7 @@ __global__ void k_coalescence(const int32_t *list, const int32_t *child, int64_t
     for (int k = 0; k < Q; ++k) {
         C s = 0;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) s += full_sh<S>(sh, T::ld(ff, k * nf + ch[m]), k);
+        for (int m = 0; m < 8; ++m) s += full_sh<S>(fsh, T::ld(ff, k * nf + ch[m]), k);
         a[k] = s / (C)8.0;
     }
     C r, x, y, z;
@@ -222,7 +222,7 @@ __global__ void k_coalescence(const int32_t *list, const int32_t *child, int64_t
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
-        T::st(cf, k * nc + i, stored_sh<S>(sh, fe + (C)scale * (a[k] - fe), k));
+        T::st(cf, k * nc + i, stored_sh<S>(csh, fe + (C)scale * (a[k] - fe), k));
     }
 }
 
@@ -235,7 +235,8 @@ template <int Q, class S, int COLL>
 __global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *__restrict__ child, int64_t nl,
                                int64_t nc, S *__restrict__ cf, const S *__restrict__ ff, int64_t nf, double scale,
                                double tau, S *__restrict__ cfnext, typename Store<S>::C *__restrict__ rho,
-                               typename Store<S>::C *__restrict__ u, int macros, const Shift sh)
+                               typename Store<S>::C *__restrict__ u, int macros, const Shift csh,
+                               const Shift fsh)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -250,7 +251,7 @@ __global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *
     for (int k = 0; k < Q; ++k) {
         C s = 0;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) s += full_sh<S>(sh, T::ld(ff, k * nf + ch[m]), k);
+        for (int m = 0; m < 8; ++m) s += full_sh<S>(fsh, T::ld(ff, k * nf + ch[m]), k);
         a[k] = s / (C)8.0;
     }
     C r, x, y, z;
@@ -258,11 +259,11 @@ __global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
         const C fe = feq_heluo_g<Q, C>(k, r, x, y, z);
-        const C st = stored_sh<S>(sh, fe + (C)scale * (a[k] - fe), k);
+        const C st = stored_sh<S>(csh, fe + (C)scale * (a[k] - fe), k);
         T::st(cf, k * nc + i, st);
         S sv;
         T::st(&sv, 0, st);
-        a[k] = full_sh<S>(sh, T::cv(sv), k);
+        a[k] = full_sh<S>(csh, T::cv(sv), k);
     }
     macros_g<Q, C>(a, r, x, y, z);
     if (macros) {
@@ -271,7 +272,7 @@ __global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *
         u[nc + i] = y;
         u[2 * nc + i] = z;
     }
-    collide_store<Q, S, COLL>(a, r, x, y, z, tau, cfnext, nc, i, sh);
+    collide_store<Q, S, COLL>(a, r, x, y, z, tau, cfnext, nc, i, csh);
 }
 
 // Non-equilibrium extrapolation ("eflow stable" form) on one boundary set:
@@ -1247,7 +1248,7 @@ int df_force(Ctx &ctx, Case &c, int l, bool band_macros_done = false)
     if (!lv.nband) return MT_OK;
     if (!band_macros_done) {
         k_band_macros<Q, S><<<grid_for(lv.nband, 128), 128, 0, s>>>(lv.band, lv.nband, lv.n, A::f(lv), A::rho(lv),
-                                                                     A::u(lv), c.acc, c.shift);
+                                                                     A::u(lv), c.acc, c.shift[l]);
         MT_LAUNCHED(ctx);
     }
     if (!c.nm) {
@@ -1274,7 +1275,7 @@ int band_collide(Ctx &ctx, Case &c, int l, void *out)
     Level &lv = c.lv[l];
     if (!lv.nband) return MT_OK;
     k_band_collide<Q, S><<<grid_for(lv.nband, 64), 64, 0, ctx.stream>>>(lv.band, lv.nband, lv.n, c.d.tau[l],
-                                                                         A::f(lv), c.acc, (S *)out, c.shift);
+                                                                         A::f(lv), c.acc, (S *)out, c.shift[l]);
     MT_LAUNCHED(ctx);
     return MT_OK;
 }
@@ -1291,7 +1292,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
     case PH_MACROS:
         if (lv.ncollide) {
             k_macros<Q, S><<<grid_for(lv.ncollide, B), B, 0, s>>>(lv.collide_list, lv.ncollide, n, A::f(lv),
-                                                                   A::rho(lv), A::u(lv), c.shift);
+                                                                   A::rho(lv), A::u(lv), c.shift[l]);
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
@@ -1302,12 +1303,12 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         if (ncl) {
             if (c.d.collision == MT_COLL_LBGK) {
                 k_collide<Q, S, MT_COLL_LBGK><<<grid_for(ncl, B), B, 0, s>>>(cl, ncl, n, c.d.tau[l], A::f(lv),
-                                                                             A::rho(lv), A::u(lv), A::fcol(lv), c.shift);
+                                                                             A::rho(lv), A::u(lv), A::fcol(lv), c.shift[l]);
             } else {
                 // the cumulant model exists for D3Q27 only (checked at case creation)
                 if constexpr (Q == 27)
                     k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(ncl, 64), 64, 0, s>>>(
-                        cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv), c.shift);
+                        cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv), c.shift[l]);
             }
             MT_LAUNCHED(ctx);
         }
@@ -1332,7 +1333,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         const double scale = c2f_scale(c, l);
         k_explosion<Q, S><<<grid_for(8 * lv.nexpl, B), B, 0, s>>>(lv.expl_src, lv.expl_child, lv.nexpl, cl.n, A::fcol(cl),
                                                                n, A::fcol(lv), scale, (S *)lv.fcol_alt,
-                                                               lv.nexpl_f2c, c.shift);
+                                                               lv.nexpl_f2c, c.shift[l - 1], c.shift[l]);
         MT_LAUNCHED(ctx);
         return MT_OK;
     }
@@ -1341,7 +1342,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         Level &fl = c.lv[l + 1];
         const double scale = f2c_scale(c, l);
         k_coalescence<Q, S><<<grid_for(lv.nlist[1], B), B, 0, s>>>(lv.list[1], lv.coal_child, lv.nlist[1], n,
-                                                                    A::f(lv), A::f(fl), fl.n, scale, c.shift);
+                                                                    A::f(lv), A::f(fl), fl.n, scale, c.shift[l], c.shift[l + 1]);
         MT_LAUNCHED(ctx);
         return MT_OK;
     }
@@ -1362,7 +1363,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             for (int ph = 0; ph < 2; ++ph) {
                 k_bc_neq_all<Q, S><<<grid_for(c.nbc_all, B), B, 0, s>>>(c.bc_all, c.bc_setb, c.nbc_all, l0.n, l0.nbr,
                                                                          A::rho(l0), A::u(l0), A::f(l0), ub,
-                                                                         c.bc_tmp_all, ph, c.dev_err, c.shift);
+                                                                         c.bc_tmp_all, ph, c.dev_err, c.shift[0]);
                 MT_LAUNCHED(ctx);
             }
             return MT_OK;
@@ -1377,7 +1378,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
                 for (int ph = 0; ph < 2; ++ph) {
                     k_bc_neq<Q, S><<<grid_for(l0.nbc[b], B), B, 0, s>>>(
                         l0.bclist[b], l0.nbc[b], b, l0.n, l0.nbr, A::rho(l0), A::u(l0), A::f(l0), c.face_u[face][0],
-                        c.face_u[face][1], c.face_u[face][2], tmp, ph, c.dev_err, c.shift);
+                        c.face_u[face][1], c.face_u[face][2], tmp, ph, c.dev_err, c.shift[0]);
                     MT_LAUNCHED(ctx);
                 }
             }
@@ -1389,7 +1390,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             if (!l0.nbc[face]) continue;
             k_bc_inout<Q, S><<<grid_for(l0.nbc[face], B), B, 0, s>>>(l0.bclist[face], l0.nbc[face], face, l0.n, l0.nbr,
                                                                       c.d.rho0, A::f(l0), A::fcol(l0), c.face_u[0][0],
-                                                                      c.face_u[0][1], c.face_u[0][2], c.dev_err, c.shift);
+                                                                      c.face_u[0][1], c.face_u[0][2], c.dev_err, c.shift[0]);
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
@@ -1404,10 +1405,10 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         }
         if (c.d.ib_method == MT_IB_FH)
             k_ib_treat<Q, 1, S><<<grid_for(fl.nib, 64), 64, 0, s>>>(fl.iblist, fl.nib, fl.n, fl.disrow, c.dis, fl.nbr,
-                                                                     A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force, c.shift);
+                                                                     A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force, c.shift[c.d.max_level]);
         else
             k_ib_treat<Q, 0, S><<<grid_for(fl.nib, 64), 64, 0, s>>>(fl.iblist, fl.nib, fl.n, fl.disrow, c.dis, fl.nbr,
-                                                                     A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force, c.shift);
+                                                                     A::fcol(fl), A::rho(fl), A::f(fl), c.ib_force, c.shift[c.d.max_level]);
         MT_LAUNCHED(ctx);
         // ib_force holds 3 * nib per-cell values followed by room for the partials
         const unsigned nb = grid_for(fl.nib, 256);
@@ -1423,11 +1424,11 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         if (lv.nlist[1]) {
             if (c.d.collision == MT_COLL_LBGK) {
                 k_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nlist[1], B), B, 0, s>>>(
-                    lv.list[1], lv.nlist[1], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv), c.shift);
+                    lv.list[1], lv.nlist[1], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv), c.shift[l]);
             } else {
                 if constexpr (Q == 27)
                     k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nlist[1], 64), 64, 0, s>>>(
-                        lv.list[1], lv.nlist[1], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv), c.shift);
+                        lv.list[1], lv.nlist[1], n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), A::fcol(lv), c.shift[l]);
             }
             MT_LAUNCHED(ctx);
         }
@@ -1439,12 +1440,12 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         if (c.d.collision == MT_COLL_LBGK) {
             k_coal_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nlist[1], 64), 64, 0, s>>>(
                 lv.list[1], lv.coal_child, lv.nlist[1], n, A::f(lv), A::f(fl), fl.n, scale, c.d.tau[l],
-                (S *)lv.fcol_alt, A::rho(lv), A::u(lv), c.macros_now, c.shift);
+                (S *)lv.fcol_alt, A::rho(lv), A::u(lv), c.macros_now, c.shift[l], c.shift[l + 1]);
         } else {
             if constexpr (Q == 27)
                 k_coal_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nlist[1], 64), 64, 0, s>>>(
                     lv.list[1], lv.coal_child, lv.nlist[1], n, A::f(lv), A::f(fl), fl.n, scale, c.d.tau[l],
-                    (S *)lv.fcol_alt, A::rho(lv), A::u(lv), c.macros_now, c.shift);
+                    (S *)lv.fcol_alt, A::rho(lv), A::u(lv), c.macros_now, c.shift[l], c.shift[l + 1]);
         }
         MT_LAUNCHED(ctx);
         return MT_OK;
@@ -1459,7 +1460,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             if (!l0.nbc[b]) continue;
             k_bc_set_eq<Q, S><<<grid_for(l0.nbc[b], B), B, 0, s>>>(l0.bclist[b], l0.nbc[b], l0.n, c.d.rho0,
                                                                     c.face_u[face][0], c.face_u[face][1],
-                                                                    c.face_u[face][2], A::f(l0), A::fcol(l0), c.shift);
+                                                                    c.face_u[face][2], A::f(l0), A::fcol(l0), c.shift[0]);
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
@@ -1495,11 +1496,11 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             if (ncl) {
                 if (c.d.collision == MT_COLL_LBGK) {
                     k_collide<Q, S, MT_COLL_LBGK><<<grid_for(ncl, B), B, 0, s>>>(
-                        cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt, c.shift);
+                        cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt, c.shift[l]);
                 } else {
                     if constexpr (Q == 27)
                         k_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(ncl, 64), 64, 0, s>>>(
-                            cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt, c.shift);
+                            cl, ncl, n, c.d.tau[l], A::f(lv), A::rho(lv), A::u(lv), (S *)lv.fcol_alt, c.shift[l]);
                 }
                 MT_LAUNCHED(ctx);
             }
@@ -1538,7 +1539,7 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
                     constexpr int FH = decltype(fh)::value, COLL = decltype(coll)::value;
                     k_ib_collide<Q, FH, S, COLL><<<grid_for(lv.nib, 64), 64, 0, is>>>(
                         lv.iblist, lv.nib, n, lv.disrow, c.dis, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt, tau,
-                        c.ib_force, A::rho(lv), A::u(lv), mac, c.shift);
+                        c.ib_force, A::rho(lv), A::u(lv), mac, c.shift[l]);
                 };
                 using I0 = std::integral_constant<int, 0>;
                 using I1 = std::integral_constant<int, 1>;
@@ -1570,13 +1571,13 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             if (c.d.collision == MT_COLL_LBGK) {
                 k_brick_step<Q, S, MT_COLL_LBGK><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb, A::fcol(lv),
                                                                    A::f(lv), (S *)lv.fcol_alt, c.d.tau[l],
-                                                                   A::rho(lv), A::u(lv), mac, fall, bacc, c.shift);
+                                                                   A::rho(lv), A::u(lv), mac, fall, bacc, c.shift[l]);
             } else {
                 if constexpr (Q == 27)
                     k_brick_step<Q, S, MT_COLL_CUMULANT><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb,
                                                                            A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
                                                                            c.d.tau[l], A::rho(lv), A::u(lv), mac,
-                                                                           fall, nullptr, c.shift);
+                                                                           fall, nullptr, c.shift[l]);
             }
             MT_LAUNCHED(ctx);
         } else {
@@ -1584,12 +1585,12 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
                 if (c.d.collision == MT_COLL_LBGK) {
                     k_pull_collide<Q, S, MT_COLL_LBGK><<<grid_for(lv.nfused, B), B, 0, s>>>(
                         lv.fused_list, lv.nfused, n, tb, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
-                        c.d.tau[l], A::rho(lv), A::u(lv), mac, c.shift);
+                        c.d.tau[l], A::rho(lv), A::u(lv), mac, c.shift[l]);
                 } else {
                     if constexpr (Q == 27)
                         k_pull_collide<Q, S, MT_COLL_CUMULANT><<<grid_for(lv.nfused, 64), 64, 0, s>>>(
                             lv.fused_list, lv.nfused, n, tb, lv.nbr, A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
-                            c.d.tau[l], A::rho(lv), A::u(lv), mac, c.shift);
+                            c.d.tau[l], A::rho(lv), A::u(lv), mac, c.shift[l]);
                 }
                 MT_LAUNCHED(ctx);
             }
@@ -1656,10 +1657,10 @@ int AmrOps<S>::init_eq(Ctx &ctx, Case &c, double rho0, const double *u0)
         if (!lv.n) continue;
         if (c.d.q == 19)
             k_init_eq<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(lv.n, lv.tag, rho0, u0[0], u0[1], u0[2],
-                                                                           A::f(lv), A::fcol(lv), A::rho(lv), A::u(lv), c.shift);
+                                                                           A::f(lv), A::fcol(lv), A::rho(lv), A::u(lv), c.shift[l]);
         else
             k_init_eq<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(lv.n, lv.tag, rho0, u0[0], u0[1], u0[2],
-                                                                           A::f(lv), A::fcol(lv), A::rho(lv), A::u(lv), c.shift);
+                                                                           A::f(lv), A::fcol(lv), A::rho(lv), A::u(lv), c.shift[l]);
         MT_LAUNCHED(ctx);
     }
     return MT_OK;
@@ -1672,9 +1673,9 @@ int AmrOps<S>::get(Ctx &ctx, Case &c, int l, int which, double *d_out)
     const S *src = (const S *)(which == 0 ? lv.f : lv.fcol);
     if (!lv.n) return MT_OK;
     if (c.d.q == 19)
-        k_to_f64<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(src, d_out, lv.n, c.shift);
+        k_to_f64<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(src, d_out, lv.n, c.shift[l]);
     else
-        k_to_f64<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(src, d_out, lv.n, c.shift);
+        k_to_f64<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(src, d_out, lv.n, c.shift[l]);
     MT_LAUNCHED(ctx);
     return MT_OK;
 }
@@ -1686,9 +1687,9 @@ int AmrOps<S>::set(Ctx &ctx, Case &c, int l, int which, const double *d_in)
     S *dst = (S *)(which == 0 ? lv.f : lv.fcol);
     if (!lv.n) return MT_OK;
     if (c.d.q == 19)
-        k_from_f64<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(d_in, dst, lv.n, c.shift);
+        k_from_f64<19, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(d_in, dst, lv.n, c.shift[l]);
     else
-        k_from_f64<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(d_in, dst, lv.n, c.shift);
+        k_from_f64<27, S><<<grid_for(lv.n, 256), 256, 0, ctx.stream>>>(d_in, dst, lv.n, c.shift[l]);
     MT_LAUNCHED(ctx);
     return MT_OK;
 }
@@ -1769,6 +1770,7 @@ template <class S> struct RemapLevels {
         const uint32_t *tag = nullptr;
         int64_t n = 0;
         const S *f = nullptr, *fcol = nullptr;
+        float shift[27] = {};  // the level's storage shift (reduced storages)
     } lv[kMaxLevels];
     // explosion factors from coarser source level m, coalescence factors
     // from finer source level m (products over the levels crossed)
@@ -1785,7 +1787,7 @@ template <class S> struct RemapLevels {
 template <int Q, class S>
 __global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, int L, int l, RemapLevels<S> src,
                         double rho0, double ux0, double uy0, double uz0, S *fo, S *co, uint8_t *kind, const Shift dsh,
-                        const Shift ssh, int same_shift)
+                        int same_shift)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -1820,8 +1822,8 @@ __global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, 
             }
         } else {
             for (int q = 0; q < Q; ++q) {
-                T::st(fo, q * nd + i, stored_sh<S>(dsh, full_sh<S>(ssh, T::ld(same.f, q * same.n + j), q), q));
-                T::st(co, q * nd + i, stored_sh<S>(dsh, full_sh<S>(ssh, T::ld(same.fcol, q * same.n + j), q), q));
+                T::st(fo, q * nd + i, stored_sh<S>(dsh, full_v<S>(same.shift, T::ld(same.f, q * same.n + j), q), q));
+                T::st(co, q * nd + i, stored_sh<S>(dsh, full_v<S>(same.shift, T::ld(same.fcol, q * same.n + j), q), q));
             }
         }
         kind[i] = 0;
@@ -1837,8 +1839,8 @@ __global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, 
         const int64_t jm = find_key(cs.key, cs.n, cell_key_at(L, m, x >> up, y >> up, z >> up));
         if (jm < 0) continue;
         for (int q = 0; q < Q; ++q) {
-            a[q] = (double)full_sh<S>(ssh, T::ld(cs.f, q * cs.n + jm), q);
-            b[q] = (double)full_sh<S>(ssh, T::ld(cs.fcol, q * cs.n + jm), q);
+            a[q] = (double)full_v<S>(cs.shift, T::ld(cs.f, q * cs.n + jm), q);
+            b[q] = (double)full_v<S>(cs.shift, T::ld(cs.fcol, q * cs.n + jm), q);
         }
         remap_rescale<Q>(a, src.up_f[m]);
         remap_rescale<Q>(b, src.up_c[m]);
@@ -1856,8 +1858,8 @@ __global__ void k_remap(const uint64_t *dkey, const uint32_t *dtag, int64_t nd, 
             const int64_t jc = find_key(fine.key, fine.n, cell_key_at(L, l + d, cx, cy, cz));
             if (jc < 0 || (fine.tag[jc] & TAG_SF)) continue;
             for (int q = 0; q < Q; ++q) {
-                a[q] += (double)full_sh<S>(ssh, T::ld(fine.f, q * fine.n + jc), q);
-                b[q] += (double)full_sh<S>(ssh, T::ld(fine.fcol, q * fine.n + jc), q);
+                a[q] += (double)full_v<S>(fine.shift, T::ld(fine.f, q * fine.n + jc), q);
+                b[q] += (double)full_v<S>(fine.shift, T::ld(fine.fcol, q * fine.n + jc), q);
             }
             ++nch;
         }
@@ -1885,9 +1887,6 @@ int AmrOps<S>::remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts)
 {
     const int L = dst.d.max_level, Q = dst.d.q;
     RemapLevels<S> rl;
-    // equal storage shifts: cells present on both lattices copy their stored values
-    int same_shift = 1;
-    for (int k = 0; k < 27; ++k) same_shift &= dst.shift.d[k] == src.shift.d[k];
     for (int m = 0; m <= L && m <= src.d.max_level; ++m) {
         if (!src.lv[m].n) continue;
         rl.lv[m].key = src.lv[m].key;
@@ -1895,6 +1894,7 @@ int AmrOps<S>::remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts)
         rl.lv[m].n = src.lv[m].n;
         rl.lv[m].f = (const S *)src.lv[m].f;
         rl.lv[m].fcol = (const S *)src.lv[m].fcol;
+        for (int k = 0; k < 27; ++k) rl.lv[m].shift[k] = src.shift[m].v[k];
     }
     // the interface factors of dst: the reference's (the same on f and
     // fcol), or the stress-continuous ones (tau on f, tau - 1 on fcol)
@@ -1926,13 +1926,16 @@ int AmrOps<S>::remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts)
                 rl.down_c[m] /= c2f(j, true);
             }
         const double r0 = dst.d.rho0, u0 = dst.d.u_bc[0], u1 = dst.d.u_bc[1], u2 = dst.d.u_bc[2];
+        // equal storage shifts on level l: cells present on both lattices copy their stored values
+        int same_shift = l <= src.d.max_level;
+        for (int k = 0; k < 27; ++k) same_shift &= dst.shift[l].d[k] == src.shift[l].d[k];
         if (Q == 19)
             k_remap<19, S><<<grid_for(lv.n, 128), 128, 0, ctx.stream>>>(lv.key, lv.tag, lv.n, L, l, rl, r0, u0, u1, u2,
-                                                                       (S *)lv.f, (S *)lv.fcol, kind, dst.shift, src.shift,
+                                                                       (S *)lv.f, (S *)lv.fcol, kind, dst.shift[l],
                                                                        same_shift);
         else
             k_remap<27, S><<<grid_for(lv.n, 128), 128, 0, ctx.stream>>>(lv.key, lv.tag, lv.n, L, l, rl, r0, u0, u1, u2,
-                                                                       (S *)lv.f, (S *)lv.fcol, kind, dst.shift, src.shift,
+                                                                       (S *)lv.f, (S *)lv.fcol, kind, dst.shift[l],
                                                                        same_shift);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) {

@@ -59,9 +59,10 @@ int check_desc(Ctx &ctx, const mt_case_desc *d)
     for (int a = 0; a < 3; ++a)
         if (d->extent0[a] <= 0 || d->extent0[a] > ((int64_t)1 << (21 - d->max_level)))
             return set_err(ctx, MT_ERR_ARG, "extent does not fit the 21-bit Morton coordinate");
-    for (int a = 0; a < 3; ++a)
-        if (!(std::fabs(d->u_shift[a]) <= 0.5))
-            return set_err(ctx, MT_ERR_ARG, "u_shift must be finite with |u_s| <= 0.5 per axis");
+    for (int l = 0; l < MT_MAX_LEVELS; ++l)
+        for (int a = 0; a < 3; ++a)
+            if (!(std::fabs(d->u_shift[l][a]) <= 0.5))
+                return set_err(ctx, MT_ERR_ARG, "u_shift must be finite with |u_s| <= 0.5 per axis");
     return MT_OK;
 }
 
@@ -252,7 +253,7 @@ int mt_case_create(mt_ctx *h, const mt_case_desc *d, int32_t *id)
     if (rc) return rc;
     Case *c = new Case();
     c->d = *d;
-    c->shift = make_shift(d->q, d->u_shift);
+    for (int l = 0; l < MT_MAX_LEVELS; ++l) c->shift[l] = make_shift(d->q, d->u_shift[l]);
     return add_case(ctx, c, id);
 }
 
@@ -268,8 +269,9 @@ int mt_case_create_dense(mt_ctx *h, const mt_case_desc *d, int32_t *id)
     const int64_t e = d->extent0[0];
     if (e != d->extent0[1] || e != d->extent0[2] || (e & (e - 1)) != 0 || e < 2 || e > 1024)
         return set_err(ctx, MT_ERR_ARG, "the dense path needs a cube of 2^b cells per edge, 2 <= 2^b <= 1024");
-    if (d->u_shift[0] != 0.0 || d->u_shift[1] != 0.0 || d->u_shift[2] != 0.0)
-        return set_err(ctx, MT_ERR_ARG, "the dense path stores f - w (u_shift must be zero)");
+    for (int a = 0; a < 3; ++a)
+        if (d->u_shift[0][a] != 0.0)
+            return set_err(ctx, MT_ERR_ARG, "the dense path stores f - w (u_shift must be zero)");
     Case *c = new Case();
     c->d = *d;
     c->dense = true;

@@ -119,8 +119,6 @@ struct BrickBatch {
     BrickSlot slot[kMaxBatchSlots];
 };
 
-inline constexpr double kZeroU[3] = {0.0, 0.0, 0.0};
-
 struct Case {
     mt_case_desc d{};
     bool dense = false;
@@ -160,7 +158,7 @@ struct Case {
     // lookahead buffers hold the collision of the current f
     int schedule = MT_SCHED_PHASES;
     int scaling = MT_SCALE_REFERENCE;  // interface rescaling of the non-equilibrium part
-    Shift shift = make_shift(19, kZeroU);  // storage shift of the reduced storages (from d.u_shift)
+    Shift shift[kMaxLevels];  // per level: storage shift of the reduced storages (from d.u_shift)
     double face_u[6][3] = {};          // bc_velocity of each face's strategy (u_bc unless set)
     // direct-forcing markers (MT_IB_DF)
     int64_t nm = 0;

@@ -77,6 +77,16 @@ __device__ __forceinline__ typename Store<S>::C stored_sh(const Shift &sh, typen
     else
         return v;
 }
+// full value from a stored one under a shift given as its FP32 table
+template <class S>
+__device__ __forceinline__ typename Store<S>::C full_v(const float *shv, typename Store<S>::C v, int k)
+{
+    using C = typename Store<S>::C;
+    if constexpr (Store<S>::shifted)
+        return v + (C)shv[k];
+    else
+        return v;
+}
 // the stored value of an FP64 population (subtraction in FP64, one rounding)
 template <class S> __device__ __forceinline__ typename Store<S>::C stored_f64(const Shift &sh, double v, int k)
 {

@@ -51,7 +51,8 @@ class mt_case_desc(C.Structure):
     _fields_ = [("q", C.c_int32), ("max_level", C.c_int32), ("collision", C.c_int32), ("ib_method", C.c_int32),
                 ("bc_mode", C.c_int32), ("stream_convention", C.c_int32), ("storage", C.c_int32),
                 ("periodic", C.c_int32 * 3), ("extent0", C.c_int64 * 3), ("tau", C.c_double * MAX_LEVELS),
-                ("rho0", C.c_double), ("u_bc", C.c_double * 3), ("u_shift", C.c_double * 3)]
+                ("rho0", C.c_double), ("u_bc", C.c_double * 3),
+                ("u_shift", (C.c_double * 3) * MAX_LEVELS)]
 
 
 class mt_mesh_spec(C.Structure):
@@ -193,19 +194,29 @@ class Context:
             pass
 
 
-def storage_shift_of(case: Case, storage_shift) -> tuple:
-    """The shift velocity u_s of the reduced storages: None (f - w_q),
-    "inlet" (the case's boundary velocity u_bc) or three numbers."""
+def storage_shift_of(case: Case, storage_shift) -> list:
+    """The shift velocity u_s of the reduced storages per level (a list of
+    max_level + 1 triples): None (f - w_q on every level), "inlet" (the
+    case's boundary velocity u_bc on every level), "far_field" (u_bc on the
+    levels below the finest, zero on the finest, which holds the body), one
+    velocity for every level, or one velocity per level."""
+    nl = case.mesh.spec.max_level + 1
+    ubc = tuple(float(v) for v in case.params.u_bc)
+    zero = (0.0, 0.0, 0.0)
     if storage_shift is None:
-        return (0.0, 0.0, 0.0)
+        return [zero] * nl
     if isinstance(storage_shift, str):
-        if storage_shift != "inlet":
-            raise ValueError(f"storage_shift: None, 'inlet' or a velocity, not {storage_shift!r}")
-        return tuple(float(v) for v in case.params.u_bc)
-    u = tuple(float(v) for v in storage_shift)
-    if len(u) != 3:
-        raise ValueError("storage_shift needs three components")
-    return u
+        if storage_shift == "inlet":
+            return [ubc] * nl
+        if storage_shift == "far_field":
+            return [ubc] * (nl - 1) + [zero]
+        raise ValueError(f"storage_shift: None, 'inlet', 'far_field' or velocities, not {storage_shift!r}")
+    a = np.asarray(storage_shift, np.float64)
+    if a.shape == (3,):
+        return [tuple(a.tolist())] * nl
+    if a.shape == (nl, 3):
+        return [tuple(r) for r in a.tolist()]
+    raise ValueError(f"storage_shift needs 3 or ({nl}, 3) components, not {a.shape}")
 
 
 def make_desc(case: Case, storage: str = None, storage_shift=None) -> mt_case_desc:
@@ -223,8 +234,9 @@ def make_desc(case: Case, storage: str = None, storage_shift=None) -> mt_case_de
         d.periodic[a] = int(m.spec.boundary[a] == "periodic")
         d.extent0[a] = int(m.spec.coarse[a])
         d.u_bc[a] = float(p.u_bc[a])
-    for a, v in enumerate(storage_shift_of(case, storage_shift)):
-        d.u_shift[a] = v
+    for l, u in enumerate(storage_shift_of(case, storage_shift)):
+        for a in range(3):
+            d.u_shift[l][a] = u[a]
     for l, t in enumerate(p.taus(m.spec.max_level)):
         d.tau[l] = float(t)
     d.rho0 = float(p.rho0)
@@ -239,8 +251,10 @@ class LBM_Manager:
                  scaling: str = "reference", generate: bool = False, storage_shift=None):
         """storage: "f64" (the reference's precision, bit-exact) or "f32" /
         "f16" / "bf16" (FP32 arithmetic on stored deviations f - s_q).
-        storage_shift: s_q = feq_q(1, u_s) of the reduced storages; None
-        (u_s = 0, s_q = w_q), "inlet" (u_s = the case's u_bc) or a velocity.
+        storage_shift: s_q = feq_q(1, u_s) of the reduced storages, per
+        level; None (u_s = 0, s_q = w_q), "inlet" (u_s = the case's u_bc),
+        "far_field" (u_bc below the finest level, 0 on it) or velocities
+        (see storage_shift_of).
         schedule: "phases" (the reference's passes) or "fused" (stream fused
         with the next collision; same state after every coarse step).
         generate: classify the lattice on the device from the mesh spec
