@@ -50,3 +50,30 @@ def test_ctypes_structs_match_header_layout(tmp_path):
         got = _c_layout(name, fields, tmp_path)
         want = [ctypes.sizeof(cls)] + [getattr(cls, f).offset for f in fields]
         assert got == want, (name, got, want)
+
+
+def test_storage_shift_levels():
+    """storage_shift options map to one velocity per level in mt_case_desc."""
+    import numpy as np
+    import pytest
+    from mortontrie_amr_b200.case import nested_sphere_case
+    from mortontrie_amr_b200.lbm import MAX_LEVELS, make_desc, storage_shift_of
+    case = nested_sphere_case(coarse=(48, 24, 24), max_level=2, center=(16, 12, 12), radius=2.0,
+                              half_widths=(4.0, 2.5), re=50.0, mesh="device")
+    ubc = tuple(float(v) for v in case.params.u_bc)
+    z = (0.0, 0.0, 0.0)
+    assert storage_shift_of(case, None) == [z] * 3
+    assert storage_shift_of(case, "inlet") == [ubc] * 3
+    assert storage_shift_of(case, "far_field") == [ubc, ubc, z]
+    assert storage_shift_of(case, (0.01, 0.02, 0.03)) == [(0.01, 0.02, 0.03)] * 3
+    per = [(0.01, 0, 0), (0, 0.02, 0), (0, 0, 0.03)]
+    assert storage_shift_of(case, per) == [tuple(float(v) for v in r) for r in per]
+    with pytest.raises(ValueError):
+        storage_shift_of(case, "outlet")
+    with pytest.raises(ValueError):
+        storage_shift_of(case, [(0, 0, 0)] * 2)
+    d = make_desc(case, "f16", "far_field")
+    got = np.array([[d.u_shift[l][a] for a in range(3)] for l in range(MAX_LEVELS)])
+    want = np.zeros((MAX_LEVELS, 3))
+    want[:2] = ubc
+    assert np.array_equal(got, want)
