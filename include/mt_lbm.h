@@ -58,9 +58,9 @@ extern "C" {
 #define MT_PULL_REFERENCE 0   /* f_q(x) = fcol_q(x + e_q), Stream_Manager.cpp:43-76 */
 #define MT_PULL_TEXTBOOK 1    /* f_q(x) = fcol_q(x - e_q) */
 #define MT_STORE_F64 0
-#define MT_STORE_F32 1  /* FP32 storage of f - w_q, FP32 arithmetic */
-#define MT_STORE_F16 2  /* FP16 storage of f - w_q, FP32 arithmetic */
-#define MT_STORE_BF16 3 /* BF16 storage of f - w_q, FP32 arithmetic */
+#define MT_STORE_F32 1  /* FP32 storage of f - s_q (u_shift below), FP32 arithmetic */
+#define MT_STORE_F16 2  /* FP16 storage of f - s_q, FP32 arithmetic */
+#define MT_STORE_BF16 3 /* BF16 storage of f - s_q, FP32 arithmetic */
 #define MT_SCHED_PHASES 0 /* the reference's phase order: collide, stream, ... as separate passes */
 #define MT_SCHED_FUSED 1  /* stream of one substep fused with the collision of the next (same results) */
 #define MT_SCHED_FUSED_LISTS 2 /* MT_SCHED_FUSED over cell lists and the neighbour table, no 4x4x4 bricks */

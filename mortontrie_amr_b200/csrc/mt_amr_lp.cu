@@ -1,5 +1,6 @@
 // Reduced-precision instantiations of the multi-level phases: FP32
-// arithmetic on populations stored as f - w_q in FP32, FP16 or BF16.
+// arithmetic on populations stored as f - s_q (the level's storage shift) in
+// FP32, FP16 or BF16.
 #include "mt_amr_phases.cuh"
 
 namespace mt {

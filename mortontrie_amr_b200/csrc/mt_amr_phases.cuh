@@ -2,8 +2,8 @@
 // population storage type S (mt_store.cuh).  With S = double every
 // expression keeps the reference's operation order and, compiled without
 // FMA contraction (mt_amr_f64.cu), reproduces its results bit-for-bit; the
-// float / half / bfloat16 instantiations (mt_amr_lp.cu) store f - w_q and
-// compute in FP32.
+// float / half / bfloat16 instantiations (mt_amr_lp.cu) store f - s_q, s_q
+// the level's storage shift (the weights unless set), and compute in FP32.
 //
 // Macros are computed inside the collision kernel from the same f the
 // reference's calculateMacros(level) reads just before collide(level)

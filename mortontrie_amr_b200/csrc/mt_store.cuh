@@ -1,7 +1,9 @@
 // Population storage types shared by the dense and multi-level kernels.
 //
 // double: unshifted populations, FP64 arithmetic (the reference's precision).
-// float / half / bfloat16: the deviation f - w_q is stored, arithmetic is FP32.
+// float / half / bfloat16: the deviation f - s_q from a storage shift is
+// stored (s_q = w_q on the dense path; per level on the multi-level path),
+// arithmetic is FP32.
 // cv converts one stored value to the compute type.
 // Index type I of ld/st: uint32_t while an array fits 2^32 elements (one wide
 // multiply-add per address), int64_t beyond.
