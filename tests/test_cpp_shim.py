@@ -28,6 +28,13 @@ def test_map_semantics(tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
 
 
+def test_storage_shift_table(tmp_path):
+    """The per-level storage shift table built on the host (make_shift)."""
+    exe = _compile("shift_test.cpp", str(tmp_path / "shift_test"))
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
 def test_demo_links(tmp_path):
     _compile("shim_demo.cpp", str(tmp_path / "shim_demo"), link=True)
 
