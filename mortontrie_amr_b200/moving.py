@@ -33,7 +33,7 @@ class MovingSphere:
     """An oscillating direct-forcing sphere whose refinement follows it."""
 
     def __init__(self, ctx, radius=8, max_level=3, re=150.0, u=0.1, storage="f16", window=16,
-                 amplitude=AMPLITUDE, period=PERIOD, scaling="standard"):
+                 amplitude=AMPLITUDE, period=PERIOD, scaling="standard", storage_shift=None):
         self.ctx = ctx
         self.kw = dict(radius=radius, max_level=max_level, re=re, u=u, oscillating=True, period=period,
                        amplitude=amplitude, mesh="device")
@@ -43,6 +43,7 @@ class MovingSphere:
         self.storage = storage
         self.window = window
         self.scaling = scaling
+        self.storage_shift = storage_shift
         self.mgr = None
         self.coarse = 0          # coarse steps done
         self.force = np.zeros(4)  # accumulated over the finished windows
@@ -64,7 +65,8 @@ class MovingSphere:
                 # the previous window's steps finish first (not re-meshing time)
                 self.ctx.synchronize()
                 t = time.perf_counter()
-                new = LBM_Manager(self.ctx, self._case(), self.storage, schedule="fused", scaling=self.scaling)
+                new = LBM_Manager(self.ctx, self._case(), self.storage, schedule="fused", scaling=self.scaling,
+                                  storage_shift=self.storage_shift)
                 self.ctx.synchronize()
                 t1 = time.perf_counter()
                 if self.mgr is not None:

@@ -239,8 +239,10 @@ class Server:
     waits for the whole device)."""
 
     def __init__(self, ctx, cache: TemplateCache, storage: str = "f16", budget_gb: float = 150.0,
-                 chunk: int = 16, scaling: str = "standard", max_inflight: int = 2, priority_builds: bool = True):
+                 chunk: int = 16, scaling: str = "standard", max_inflight: int = 2, priority_builds: bool = True,
+                 storage_shift=None):
         self.ctx = ctx
+        self.storage_shift = storage_shift  # per-level storage shift of every case (LBM_Manager)
         self.priority_builds = priority_builds
         self.cache = cache
         self.storage = storage
@@ -299,7 +301,8 @@ class Server:
                     stats.drain_s += time.perf_counter() - td
                     continue
                 ta = time.perf_counter()
-                mgr = LBM_Manager(builder, case, self.storage, schedule="fused", scaling=self.scaling)
+                mgr = LBM_Manager(builder, case, self.storage, schedule="fused", scaling=self.scaling,
+                                  storage_shift=self.storage_shift)
                 mgr.prepare()
                 mgr.transfer(self.ctx)
                 batch.add(mgr)
@@ -343,13 +346,13 @@ class Server:
 
 
 def solve_alone(ctx, cache: TemplateCache, req: Request, storage: str = "f16", scaling: str = "standard",
-                schedule: Optional[str] = None) -> tuple:
+                schedule: Optional[str] = None, storage_shift=None) -> tuple:
     """One request by itself (no batch); returns (cd, cl, seconds)."""
     from .lbm import LBM_Manager
     case = request_case(req, cache.get(req))
     t = time.perf_counter()
     mgr = LBM_Manager(ctx, case, storage, schedule=schedule or ("phases" if storage == "f64" else "fused"),
-                      scaling=scaling)
+                      scaling=scaling, storage_shift=storage_shift)
     mgr.fluidSimulate(req.coarse_steps())
     ctx.synchronize()
     cd, cl = drag_lift(mgr, req)
