@@ -350,8 +350,9 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
     per_coarse_fine = stepped[L] << L
     out = {"workload": "4-level D3Q27 cumulant sphere 192x96x96, R=6 (48 finest), Re=200, u=0.04",
            "stepped_cells_per_level": stepped, "coarse_steps": steps,
-           "accuracy_note": "errors vs FP64 after the first warm-up + timed coarse steps from rest (a small "
-                            "transient drag); the long-run comparison is bench.py --amr-accuracy"}
+           "accuracy_note": "errors vs FP64 after the first warm-up + timed coarse steps from the uniform "
+                            "inflow state (an impulsively started sphere: a transient drag); the long-run "
+                            "comparison is bench.py --amr-accuracy"}
     stream = torch.cuda.current_stream()
     res = {}
     # (label, storage, schedule): the plain form is FP64 in the reference's
