@@ -18,9 +18,24 @@ TEST INFRASTRUCTURE ONLY.
        run_col_times{0,0,0}`` get an empty initialiser, because three
        initialisers do not compile unless C_max_level == 2.
 
+  The periodic variants (``_ref/refharness_q{Q}_l{L}_periodic``) add a third:
+  ``_ref/shim_q{Q}_l{L}_periodic/Morton_Assist.h``, written from
+  ``header/Morton_Assist.h`` with the result of ``find_neighbor``
+  (``Morton_Assist.h:254-280``) passed through a wrap of the level-0 box on
+  the axes the harness input marks periodic.  The reference has no periodic
+  path that builds (``BC/Periodic.cpp`` needs the ghost layers that
+  ``BC_NO_GHOST`` removes), and every neighbour lookup of the step (stream,
+  boundary, IB) goes through ``find_neighbor``; the explosion and coalescence
+  children (``find_x1``/``find_y1``/``find_z1`` inside one parent) never
+  cross the box.  With no axis marked the wrap returns the reference's key.
+
   Nothing else in the reference is changed.  The reference's own Makefile is
   not used (it links HDF5, which this image lacks); the flags are its
   ``-std=c++17 -O3`` (Makefile:15-17).  Outputs go to ``oracle/_ref`` only.
+
+The reference checkout is read from ``$MT_REFERENCE_DIR`` (default
+``/root/reference``); without it the prebuilt harnesses under ``_ref`` are
+used as they are.
 """
 from __future__ import annotations
 
@@ -30,7 +45,7 @@ import sys
 from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference"
+REF = os.environ.get("MT_REFERENCE_DIR", "/root/reference")
 REF_TUS = [
     "LBM_Manager.cpp",
     "LBM_Simulator.cpp",
@@ -42,7 +57,9 @@ REF_TUS = [
     "ComplexBoundary_Manager.cpp",
     "Morton_Assist.cpp",
 ]
-HARNESS_VARIANTS = [(19, 0), (19, 1), (19, 2), (27, 0), (27, 1), (27, 2)]
+HARNESS_VARIANTS = [(19, 0), (19, 1), (19, 2), (19, 3), (27, 0), (27, 1), (27, 2), (27, 3)]
+# (Q, L) of the harnesses built with the periodic find_neighbor wrap
+PERIODIC_VARIANTS = [(19, 1)]
 
 
 def oracle_lib_path() -> str:
@@ -59,13 +76,80 @@ def build_oracle_lib(force: bool = False) -> str:
     return out
 
 
-def harness_path(q: int, L: int) -> str:
-    return os.path.join(HERE, "_ref", f"refharness_q{q}_l{L}")
+def harness_path(q: int, L: int, periodic: bool = False) -> str:
+    return os.path.join(HERE, "_ref", f"refharness_q{q}_l{L}" + ("_periodic" if periodic else ""))
 
 
-def _shim_header(q: int, L: int) -> str:
-    d = os.path.join(HERE, "_ref", f"shim_q{q}_l{L}")
+_WRAP = r"""
+/* ---- inserted by oracle/build.py: periodic wrap of the level-0 box ---- */
+inline int hc_periodic[3] = {0, 0, 0};
+inline long long hc_extent0[3] = {0, 0, 0};
+inline unsigned long long hc_dilate(unsigned long long v)
+{
+    v &= 0x1FFFFFULL;
+    v = (v | (v << 32)) & 0x1F00000000FFFFULL;
+    v = (v | (v << 16)) & 0x1F0000FF0000FFULL;
+    v = (v | (v << 8)) & 0x100F00F00F00F00FULL;
+    v = (v | (v << 4)) & 0x10C30C30C30C30C3ULL;
+    v = (v | (v << 2)) & 0x1249249249249249ULL;
+    return v;
+}
+inline unsigned long long hc_compact(unsigned long long v)
+{
+    v &= 0x1249249249249249ULL;
+    v = (v ^ (v >> 2)) & 0x10C30C30C30C30C3ULL;
+    v = (v ^ (v >> 4)) & 0x100F00F00F00F00FULL;
+    v = (v ^ (v >> 8)) & 0x1F0000FF0000FFULL;
+    v = (v ^ (v >> 16)) & 0x1F00000000FFFFULL;
+    v = (v ^ (v >> 32)) & 0x1FFFFFULL;
+    return v;
+}
+/* key: the cell; rst: find_neighbor's result for the shift (sx, sy, sz) at
+ * `level`.  On a periodic axis whose shifted coordinate leaves [0, n_l)
+ * (n_l = level-0 extent << level) the axis bits of rst are replaced by the
+ * wrapped coordinate. */
+inline D_morton hc_periodic_wrap(const D_morton &key, const D_morton &rst, unsigned level, int sx, int sy, int sz)
+{
+    const int s[3] = {sx, sy, sz};
+    unsigned long long k = key.to_ullong(), r = rst.to_ullong();
+    const unsigned sh = C_max_level - level;
+    for (int a = 0; a < 3; ++a) {
+        if (!hc_periodic[a] || s[a] == 0) continue;
+        long long n = hc_extent0[a] << level;
+        long long t = (long long)(hc_compact(k >> a) >> sh) + s[a];
+        if (t >= 0 && t < n) continue;
+        t = ((t % n) + n) % n;
+        unsigned long long m = 0x1249249249249249ULL << a;
+        r = (r & ~m) | (hc_dilate((unsigned long long)t << sh) << a);
+    }
+    return D_morton(r);
+}
+/* ---- end of insertion ---- */
+"""
+
+
+def _morton_shim(d: str) -> None:
+    src = open(os.path.join(REF, "header", "Morton_Assist.h")).read()
+    head = "inline D_morton Morton_Assist::find_neighbor(const D_morton& key, const uint level, const int x_shift, " \
+           "const int y_shift, const int z_shift)"
+    i = src.find(head)
+    if i < 0 or src.count(head) != 1:
+        raise RuntimeError("Morton_Assist.h no longer has the expected find_neighbor definition")
+    j = src.find("return rst_code;", i)
+    k = src.find("\n}", i)
+    if j < 0 or j > k:
+        raise RuntimeError("Morton_Assist.h find_neighbor no longer ends in 'return rst_code;'")
+    src = (src[:i] + _WRAP + src[i:j]
+           + "return hc_periodic_wrap(key, rst_code, level, x_shift, y_shift, z_shift);" + src[j + len("return rst_code;"):])
+    with open(os.path.join(d, "Morton_Assist.h"), "w") as fh:
+        fh.write(src)
+
+
+def _shim_header(q: int, L: int, periodic: bool = False) -> str:
+    d = os.path.join(HERE, "_ref", f"shim_q{q}_l{L}" + ("_periodic" if periodic else ""))
     os.makedirs(d, exist_ok=True)
+    if periodic:
+        _morton_shim(d)
     src = open(os.path.join(REF, "header", "LBM_Manager.hpp")).read()
     old_col = "run_col_times{0,0,0};"
     old_stm = "run_stm_times{0,0,0};"
@@ -77,8 +161,8 @@ def _shim_header(q: int, L: int) -> str:
     return d
 
 
-def build_refharness(q: int, L: int, force: bool = False) -> str:
-    out = harness_path(q, L)
+def build_refharness(q: int, L: int, force: bool = False, periodic: bool = False) -> str:
+    out = harness_path(q, L, periodic)
     if not os.path.isdir(REF):
         if os.path.exists(out):
             return out
@@ -87,8 +171,8 @@ def build_refharness(q: int, L: int, force: bool = False) -> str:
             os.path.abspath(__file__)]
     if not force and os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(p) for p in deps):
         return out
-    shim = _shim_header(q, L)
-    objdir = os.path.join(HERE, "_ref", f"obj_q{q}_l{L}")
+    shim = _shim_header(q, L, periodic)
+    objdir = os.path.join(HERE, "_ref", f"obj_q{q}_l{L}" + ("_periodic" if periodic else ""))
     os.makedirs(objdir, exist_ok=True)
     # with -I- every directory reached by a quoted include must be listed,
     # including the one libstdc++'s parallel-algorithm headers use
@@ -96,7 +180,7 @@ def build_refharness(q: int, L: int, force: bool = False) -> str:
     inc = ["-I", shim, "-I", os.path.join(HERE, "refharness"), "-I", os.path.join(REF, "header"),
            "-I", os.path.join(REF, "header", "lbm_kernel"), "-I", os.path.join(REF, "header", "BC"), "-I", REF,
            "-I", f"/usr/include/c++/{gxx}/pstl", "-I-"]
-    flags = ["g++", "-std=c++17", "-O3", "-w", f"-DHC_Q={q}", f"-DHC_L={L}"] + inc
+    flags = ["g++", "-std=c++17", "-O3", "-w", f"-DHC_Q={q}", f"-DHC_L={L}"] + (["-DHC_PERIODIC"] if periodic else []) + inc
     srcs = [os.path.join(REF, t) for t in REF_TUS] + [os.path.join(HERE, "refharness", "harness.cpp")]
 
     def comp(src):
@@ -117,6 +201,8 @@ def build_all(harness: bool = True) -> None:
     if harness and os.path.isdir(REF):
         for q, L in HARNESS_VARIANTS:
             build_refharness(q, L)
+        for q, L in PERIODIC_VARIANTS:
+            build_refharness(q, L, periodic=True)
 
 
 if __name__ == "__main__":

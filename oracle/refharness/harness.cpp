@@ -14,7 +14,15 @@
  * (LBM_Simulator.cpp:8-18) without the diagnostics print and Tecplot output.
  *
  * usage: harness step  <in.bin> <out.bin>
+ *        harness pstep <in.bin> <out.bin>      (step with periodic axes)
+ *        harness trace <in.bin> <out.bin>      (state dumps after chosen steps)
  *        harness morton <in.bin> <out.bin>     (neighbour-key known answers)
+ *
+ * Built with -DHC_PERIODIC the harness includes a generated copy of
+ * Morton_Assist.h whose find_neighbor wraps the level-0 box on the axes the
+ * trace input marks periodic (the reference has no periodic path that
+ * builds, BC/Periodic.cpp needs the ghost layers that BC_NO_GHOST removes);
+ * with no axis marked it is the reference's arithmetic unchanged.
  */
 #include <algorithm>
 #include <array>
@@ -111,10 +119,15 @@ int run_morton(Reader &in, FILE *out)
     return 0;
 }
 
-int run_step(Reader &in, FILE *out)
+struct Loaded {
+    LBM_Manager *mgr = nullptr;
+    int32_t L = 0, nsteps = 0, nwarm = 0;
+};
+
+/* reads the case (index sets, parameters, optional initial populations) and
+ * constructs the reference's LBM_Manager on it */
+int load_case(Reader &in, Loaded &c)
 {
-    Morton_Assist ma;
-    setup_morton(ma);
     int32_t q = in.get<int32_t>(), L = in.get<int32_t>();
     if (q != C_Q || L != (int32_t)C_max_level) {
         fprintf(stderr, "harness built for Q=%d L=%d, input has Q=%d L=%d\n", C_Q, (int)C_max_level, q, L);
@@ -130,10 +143,10 @@ int run_step(Reader &in, FILE *out)
     sphere::U_dynaViscosity = sphere::U_kineViscosity * U_rho0;
     sphere::R_Re = sphere::R_velocity * R_length / sphere::U_kineViscosity;
 
-    Lat_Manager lm;
-    Lat_Manager::pointer_me = &lm;
-    std::array<D_mapLat, C_max_level + 1> *maps[5] = {&lm.lat_f, &lm.lat_overlap_F2C, &lm.lat_overlap_C2F,
-                                                     &lm.ghost_overlap_C2F, &lm.ghost_overlap_F2C};
+    Lat_Manager *lm = new Lat_Manager();
+    Lat_Manager::pointer_me = lm;
+    std::array<D_mapLat, C_max_level + 1> *maps[5] = {&lm->lat_f, &lm->lat_overlap_F2C, &lm->lat_overlap_C2F,
+                                                     &lm->ghost_overlap_C2F, &lm->ghost_overlap_F2C};
     const int flags[5] = {FLUID, OVERLAP_F2C, OVERLAP_C2F, OVERLAP_GHOST, OVERLAP_GHOST};
     for (int l = 0; l <= L; ++l) {
         for (int s = 0; s < 6; ++s) {
@@ -143,15 +156,15 @@ int run_step(Reader &in, FILE *out)
                 if (s < 5)
                     (*maps[s])[l].insert(std::make_pair(K(k), Cell(flags[s])));
                 else
-                    lm.lat_sf.insert(std::make_pair(K(k), Cell(SOLID)));
+                    lm->lat_sf.insert(std::make_pair(K(k), Cell(SOLID)));
             }
         }
-        lm.dx[l] = C_dx / (double)two_power_n(l);
+        lm->dx[l] = C_dx / (double)two_power_n(l);
     }
     for (int b = 0; b < 26; ++b) {
         int64_t n = in.get<int64_t>();
         auto keys = in.vec<uint64_t>(n);
-        for (auto k : keys) lm.lat_bc[b].insert(K(k));
+        for (auto k : keys) lm->lat_bc[b].insert(K(k));
     }
     {
         int64_t n = in.get<int64_t>();
@@ -160,7 +173,7 @@ int run_step(Reader &in, FILE *out)
             auto row = in.vec<double>(C_Q - 1);
             std::array<D_real, C_Q - 1> a;
             for (int j = 0; j < C_Q - 1; ++j) a[j] = row[j];
-            lm.dis.insert(std::make_pair(K(k), a));
+            lm->dis.insert(std::make_pair(K(k), a));
         }
     }
 
@@ -183,28 +196,30 @@ int run_step(Reader &in, FILE *out)
             }
         }
     }
+    c.mgr = mgr;
+    c.L = L;
+    c.nsteps = nsteps;
+    c.nwarm = nwarm;
+    return 0;
+}
 
-    std::vector<double> force;
-    for (int s = 0; s < nwarm; ++s) {
-        mgr->LBMkernel(0);
-        mgr->calculateMacros();
-    }
+/* one coarse step as LBM_Manager::fluidSimulate takes it (LBM_Simulator.cpp:8-18),
+ * then the step's IB force sum is appended and the accumulator cleared */
+void coarse_step(LBM_Manager *mgr, std::vector<double> &force)
+{
+    mgr->LBMkernel(0);
+    mgr->calculateMacros();
+    force.push_back(mgr->m_ibFx_sum);
+    force.push_back(mgr->m_ibFy_sum);
+    force.push_back(mgr->m_ibFz_sum);
+    force.push_back((double)mgr->m_ibForce_count);
     mgr->m_ibFx_sum = mgr->m_ibFy_sum = mgr->m_ibFz_sum = 0.0;
     mgr->m_ibForce_count = 0;
-    auto t0 = std::chrono::steady_clock::now();
-    for (int s = 0; s < nsteps; ++s) {
-        mgr->LBMkernel(0);
-        mgr->calculateMacros();
-        force.push_back(mgr->m_ibFx_sum);
-        force.push_back(mgr->m_ibFy_sum);
-        force.push_back(mgr->m_ibFz_sum);
-        force.push_back((double)mgr->m_ibForce_count);
-        mgr->m_ibFx_sum = mgr->m_ibFy_sum = mgr->m_ibFz_sum = 0.0;
-        mgr->m_ibForce_count = 0;
-    }
-    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
 
-    fwrite(&secs, 8, 1, out);
+/* every stored cell of every level, ascending key: f[Q], fcol[Q], rho, u */
+void write_levels(LBM_Manager *mgr, int L, FILE *out)
+{
     for (int l = 0; l <= L; ++l) {
         std::vector<uint64_t> keys;
         for (auto &kv : mgr->user[l].df.f[0]) keys.push_back(kv.first.to_ullong());
@@ -227,12 +242,92 @@ int run_step(Reader &in, FILE *out)
             fwrite(rec, 8, 2 * C_Q + 4, out);
         }
     }
+}
+
+void write_tail(LBM_Manager *mgr, const std::vector<double> &force, FILE *out)
+{
     int64_t nf = (int64_t)force.size();
     fwrite(&nf, 8, 1, out);
     fwrite(force.data(), 8, force.size(), out);
     double tau[C_max_level + 1];
     for (unsigned l = 0; l <= C_max_level; ++l) tau[l] = mgr->tau[l];
     fwrite(tau, 8, C_max_level + 1, out);
+}
+
+/* reads int32 periodic[3], int32 extent0[3] and turns the find_neighbor
+ * wrap on (harness built with HC_PERIODIC) */
+int read_periodic(Reader &in)
+{
+    int32_t per[3], ext[3];
+    for (auto &p : per) p = in.get<int32_t>();
+    for (auto &e : ext) e = in.get<int32_t>();
+#ifdef HC_PERIODIC
+    for (int a = 0; a < 3; ++a) {
+        hc_periodic[a] = per[a];
+        hc_extent0[a] = ext[a];
+    }
+#else
+    if (per[0] || per[1] || per[2]) {
+        fprintf(stderr, "periodic axes need the harness built with HC_PERIODIC\n");
+        return 2;
+    }
+#endif
+    return 0;
+}
+
+/* step (pstep: followed by the periodic section of read_periodic) */
+int run_step(Reader &in, FILE *out, bool periodic = false)
+{
+    Morton_Assist ma;
+    setup_morton(ma);
+    Loaded c;
+    if (int rc = load_case(in, c)) return rc;
+    if (periodic)
+        if (int rc = read_periodic(in)) return rc;
+    LBM_Manager *mgr = c.mgr;
+    std::vector<double> force;
+    for (int s = 0; s < c.nwarm; ++s) {
+        mgr->LBMkernel(0);
+        mgr->calculateMacros();
+    }
+    mgr->m_ibFx_sum = mgr->m_ibFy_sum = mgr->m_ibFz_sum = 0.0;
+    mgr->m_ibForce_count = 0;
+    auto t0 = std::chrono::steady_clock::now();
+    for (int s = 0; s < c.nsteps; ++s) coarse_step(mgr, force);
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+
+    fwrite(&secs, 8, 1, out);
+    write_levels(mgr, c.L, out);
+    write_tail(mgr, force, out);
+    return 0;
+}
+
+/* trace: the step input followed by int32 ndump, int32 dump_after[ndump]
+ * (ascending coarse-step counts), int32 periodic[3], int32 extent0[3]
+ * (level-0 box).  Output: seconds, then the levels after each listed step,
+ * then the per-step force series and tau. */
+int run_trace(Reader &in, FILE *out)
+{
+    Morton_Assist ma;
+    setup_morton(ma);
+    Loaded c;
+    if (int rc = load_case(in, c)) return rc;
+    int32_t ndump = in.get<int32_t>();
+    auto dumps = in.vec<int32_t>(ndump);
+    if (int rc = read_periodic(in)) return rc;
+    LBM_Manager *mgr = c.mgr;
+    std::vector<double> force;
+    double secs = 0;
+    int32_t done = 0;
+    for (int32_t d = 0; d < ndump; ++d) {
+        auto t0 = std::chrono::steady_clock::now();
+        for (; done < dumps[d]; ++done) coarse_step(mgr, force);
+        secs += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        write_levels(mgr, c.L, out);
+        fflush(out);
+    }
+    fwrite(&secs, 8, 1, out);
+    write_tail(mgr, force, out);
     return 0;
 }
 
@@ -241,7 +336,7 @@ int run_step(Reader &in, FILE *out)
 int main(int argc, char **argv)
 {
     if (argc != 4) {
-        fprintf(stderr, "usage: %s step|morton <in.bin> <out.bin>\n", argv[0]);
+        fprintf(stderr, "usage: %s step|pstep|trace|morton <in.bin> <out.bin>\n", argv[0]);
         return 2;
     }
     std::ofstream devnull("/dev/null");
@@ -253,7 +348,10 @@ int main(int argc, char **argv)
     Reader rd{fin};
     int rc;
     try {
-        rc = std::string(argv[1]) == "morton" ? run_morton(rd, fout) : run_step(rd, fout);
+        const std::string mode = argv[1];
+        rc = mode == "morton"  ? run_morton(rd, fout)
+             : mode == "trace" ? run_trace(rd, fout)
+             : run_step(rd, fout, mode == "pstep");
     } catch (const std::exception &e) {
         fprintf(stderr, "harness: %s\n", e.what());
         rc = 4;

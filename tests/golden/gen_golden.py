@@ -3,8 +3,11 @@ own LBM translation units (oracle/refharness, built by oracle/build.py from
 the reference checkout) on seeded synthetic cases.
 
 Run here, where the reference checkout exists:
-    python tests/golden/gen_golden.py
-The outputs are small .npz files; the GPU box only reads them.
+    python tests/golden/gen_golden.py            # short cases + Morton answers
+    python tests/golden/gen_golden.py --trace [name ...]   # TRACE_CASES
+The outputs are small .npz files; the GPU box only reads them.  The trace
+cases run one harness process each, in parallel; cfg1's 1000 coarse steps
+take about half an hour of one core.
 """
 from __future__ import annotations
 
@@ -21,7 +24,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 from mortontrie_amr_b200.case import perturbed_populations  # noqa: E402
-from golden_cases import GOLDEN_CASES, build_case  # noqa: E402
+from golden_cases import GOLDEN_CASES, TRACE_CASES, build_case  # noqa: E402
 
 
 def set_digest(case):
@@ -79,5 +82,66 @@ def main():
         print("morton kat", os.path.getsize(path), "bytes")
 
 
+SAMPLE = 64
+
+
+def trace_arrays(case, out, seed=1):
+    """What a trace golden keeps: per dump and level the SHA-256 of f on the
+    non-boundary cells (boundary-cell f depends on the reference's hash-set
+    order, and no fluid cell reads it), of fcol, of rho and u on the lat_f
+    cells, and SAMPLE cells in full; the per-step force series; tau."""
+    m = case.mesh
+    L = m.spec.max_level
+    arrays = {"tau": out["tau"], "force": out["force"]}
+    bc = np.sort(np.concatenate([np.asarray(b, np.uint64) for b in m.lat_bc]))
+    rng = np.random.default_rng(seed)
+    for l in range(L + 1):
+        keys = out["states"][0][l]["keys"]
+        arrays[f"keysha{l}"] = _sha(keys.astype(np.uint64))
+        n = keys.size
+        arrays[f"sidx{l}"] = np.sort(rng.choice(n, size=min(SAMPLE, n), replace=False)).astype(np.int64)
+    for d, st in enumerate(out["states"]):
+        for l in range(L + 1):
+            lv = st[l]
+            keys = lv["keys"]
+            keep = ~np.isin(keys, bc) if l == 0 else np.ones(keys.size, bool)
+            fl = np.isin(keys, m.levels[l]["lat_f"])
+            arrays[f"fsha_{d}_{l}"] = _sha(lv["f"][:, keep])
+            arrays[f"fcolsha_{d}_{l}"] = _sha(lv["fcol"])
+            arrays[f"rhosha_{d}_{l}"] = _sha(lv["rho"][fl])
+            arrays[f"usha_{d}_{l}"] = _sha(lv["u"][:, fl])
+            si = arrays[f"sidx{l}"]
+            arrays[f"sf_{d}_{l}"] = lv["f"][:, si]
+            arrays[f"sfcol_{d}_{l}"] = lv["fcol"][:, si]
+            arrays[f"finite_{d}_{l}"] = np.array([np.isfinite(lv["f"]).all()])
+    return arrays
+
+
+def _sha(a):
+    return np.frombuffer(hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest(), np.uint8)
+
+
+def gen_trace(name):
+    import oracle as O
+    spec = TRACE_CASES[name]
+    case = build_case(spec)
+    init = perturbed_populations(case, seed=spec["seed"]) if spec["init"] == "perturbed" else None
+    out = O.run_harness_trace(case, spec["dumps"], init, timeout=4 * 3600)
+    arrays = trace_arrays(case, out)
+    meta = dict(spec=spec, set_digest=set_digest(case), seconds=out["seconds"])
+    arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), np.uint8)
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **arrays)
+    return name, os.path.getsize(path), out["seconds"]
+
+
 if __name__ == "__main__":
-    main()
+    if "--trace" in sys.argv:
+        from concurrent.futures import ProcessPoolExecutor
+        import multiprocessing as mp
+        names = [a for a in sys.argv[1:] if not a.startswith("--")] or sorted(TRACE_CASES)
+        with ProcessPoolExecutor(max_workers=len(names), mp_context=mp.get_context("spawn")) as ex:
+            for r in ex.map(gen_trace, names):
+                print(*r, flush=True)
+    else:
+        main()

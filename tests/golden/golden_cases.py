@@ -30,6 +30,40 @@ GOLDEN_CASES = {
                              steps=2, seed=3, init="perturbed"),
 }
 
+# Runs whose reference state is recorded after several coarse-step counts
+# ("dumps"): SHA-256 of every level's arrays, a sample of cells in full, and
+# the per-step IB force series (gen_golden.py --trace).
+TRACE_CASES = {
+    # cfg1 geometry (64x32x32 coarse, 2 levels, refined box (4,8,8)-(28,24,24),
+    # sphere R = 4 at (16,16,16), Re 20: nu = 0.05 * 8 / 20), closed by the
+    # reference's live non-equilibrium boundary on every face, from the
+    # reference's own initial state, 1000 coarse steps
+    "cfg1_neq_1000": dict(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1, refine=[((4, 8, 8), (28, 24, 24))],
+                          sphere=((16.0, 16.0, 16.0), 4.0), boundary=("bc", "bc", "bc"), nu=0.02, u=0.05, ib="FH",
+                          seed=0, init="reference", dumps=[10, 100, 1000]),
+    # the same with periodic y and z (the cfg1 lateral sides), non-equilibrium
+    # boundary on the West and East faces
+    "cfg1_periodic_1000": dict(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1,
+                               refine=[((4, 8, 8), (28, 24, 24))], sphere=((16.0, 16.0, 16.0), 4.0),
+                               boundary=("bc", "periodic", "periodic"), nu=0.02, u=0.05, ib="FH", seed=0,
+                               init="reference", dumps=[10, 100, 1000]),
+    # the 4-level D3Q27 cumulant sphere scaled by 1/4 (48x24x24 coarse, R = 1.5
+    # coarse = 12 finest cells, nested half-widths 4R, 2.5R, 1.75R, Re 200,
+    # u 0.04), 12 coarse steps = 96 finest steps (the reference itself turns
+    # non-finite between coarse steps 14 and 15 of this case)
+    "cfg3_small_q27_l3": dict(q=27, collision="Cumulant", coarse=(48, 24, 24), max_level=3,
+                              refine=[((10, 6, 6), (22, 18, 18)), ((24, 16, 16), (40, 32, 32)),
+                                      ((54, 38, 38), (74, 58, 58))],
+                              sphere=((16.0, 12.0, 12.0), 1.5), boundary=("bc", "bc", "bc"), nu=0.0006, u=0.04,
+                              ib="FH", seed=0, init="reference", dumps=[2, 12]),
+    # four levels of D3Q19 LBGK with distance-weighted links from a perturbed state
+    "nested_q19_dw_l3": dict(q=19, collision="LBGK", coarse=(28, 16, 16), max_level=3,
+                             refine=[((4, 2, 2), (16, 14, 14)), ((13, 9, 9), (27, 23, 23)),
+                                     ((32, 24, 24), (48, 40, 40))],
+                             sphere=((10.0, 8.0, 8.0), 1.0), boundary=("bc", "bc", "bc"), nu=0.002, u=0.05, ib="DW",
+                             seed=21, init="perturbed", dumps=[1, 6]),
+}
+
 
 def build_case(spec) -> Case:
     sphere = Sphere(tuple(spec["sphere"][0]), spec["sphere"][1]) if spec["sphere"] else None

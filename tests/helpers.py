@@ -24,6 +24,46 @@ def sha(a) -> bytes:
     return hashlib.sha256(np.ascontiguousarray(a, np.float64).tobytes()).digest()
 
 
+def load_trace(name):
+    from golden_cases import build_case
+    z = np.load(os.path.join(GOLDEN_DIR, f"{name}.npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    return meta["spec"], build_case(meta["spec"]), z, meta
+
+
+def trace_mismatches(case, z, d, level_state):
+    """Compare one dump of a trace golden with a state: level_state(l) gives
+    dict(keys, tags, f (Q, n), fcol (Q, n), rho (n,), u (3, n)) of level l.
+    Returns the list of differences (empty when everything is bit-exact)."""
+    bad = []
+    for l in range(case.max_level + 1):
+        s = level_state(l)
+        keys = np.asarray(s["keys"], np.uint64)
+        if hashlib.sha256(np.ascontiguousarray(keys).tobytes()).digest() != bytes(z[f"keysha{l}"]):
+            bad.append(f"level {l}: keys")
+            continue
+        keep = (np.asarray(s["tags"]) & TAG_BC) == 0
+        fl = np.isin(keys, case.mesh.levels[l]["lat_f"])
+        si = z[f"sidx{l}"]
+        for what, arr, ref in (("f", s["f"][:, keep], "fsha"), ("fcol", s["fcol"], "fcolsha"),
+                               ("rho", np.asarray(s["rho"])[fl], "rhosha"), ("u", np.asarray(s["u"])[:, fl], "usha")):
+            if sha(arr) != bytes(z[f"{ref}_{d}_{l}"]):
+                msg = f"dump {d} level {l}: {what}"
+                if what in ("f", "fcol"):
+                    full = s["f"] if what == "f" else s["fcol"]
+                    msg += f" (sampled cells max |diff| {float(np.abs(full[:, si] - z[f's{what}_{d}_{l}']).max()):.3g})"
+                bad.append(msg)
+    return bad
+
+
+def oracle_state(oc):
+    def get(l):
+        g = oc.get(l)
+        g["u"] = np.ascontiguousarray(g["u"].T)
+        return g
+    return get
+
+
 def init_of(case, spec):
     from mortontrie_amr_b200.case import perturbed_populations
     return perturbed_populations(case, seed=spec["seed"]) if spec["init"] == "perturbed" else None
