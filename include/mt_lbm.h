@@ -55,6 +55,10 @@ extern "C" {
 #define MT_IB_DF 2         /* direct forcing on Lagrangian markers (no reference counterpart) */
 #define MT_BC_NEQ 0        /* nonEquilibrumExtrapolation_* (BC/NonEquilibrumExtrapolation.cpp) */
 #define MT_BC_ZOUHE_OUTFLOW 1 /* velocity inlet on West, zero-gradient outflow on East */
+/* Zou-He velocity inlet with Hecht-Harting corrections on West (formula family of
+   BC/ZouHe_Velocity.cpp:81-93,170-199), five-population outflow on East
+   (BC/Outflow.cpp:39-52); wet nodes on the boundary shell, D3Q19 LBGK, phase schedule */
+#define MT_BC_ZOUHE_HH 2
 #define MT_PULL_REFERENCE 0   /* f_q(x) = fcol_q(x + e_q), Stream_Manager.cpp:43-76 */
 #define MT_PULL_TEXTBOOK 1    /* f_q(x) = fcol_q(x - e_q) */
 #define MT_STORE_F64 0
@@ -66,6 +70,8 @@ extern "C" {
 #define MT_SCHED_FUSED_LISTS 2 /* MT_SCHED_FUSED over cell lists and the neighbour table, no 4x4x4 bricks */
 #define MT_SCALE_REFERENCE 0 /* explosion x 2 tau_f / tau_c, coalescence x tau_c / (2 tau_f): LBM_Manager.cpp:1065, 1137 */
 #define MT_SCALE_STANDARD 1  /* stress-continuous rescaling: fneq_f = tau_f / (2 tau_c) fneq_c and its inverse */
+#define MT_ITIME_REFERENCE 0 /* fine level explodes in its first substep only: LBM_Simulator.cpp:47-51 */
+#define MT_ITIME_HOLD 1      /* in both substeps, from the parent's post-collision state of the coarse step */
 
 /* Case description: the switches the reference hard-codes in
  * LBM_Manager::LBM_Manager (LBM_Manager.cpp:32-95) and its per-level
@@ -201,17 +207,29 @@ int mt_case_set_populations(mt_ctx *ctx, int32_t case_id, int32_t level, const d
 int mt_case_get_populations(mt_ctx *ctx, int32_t case_id, int32_t level, double *f, double *fcol);
 /* density [n] and velocity [3][n] of a level (density/velocity maps of User) */
 int mt_case_get_macros(mt_ctx *ctx, int32_t case_id, int32_t level, double *rho, double *u);
-/* FP64 reductions over the stepped cells (dense path): out[5] = mass, x/y/z momentum,
-   kinetic energy sum of |j|^2 / (2 rho) */
+/* FP64 reductions over the stepped cells: out[5] = mass, x/y/z momentum,
+   kinetic energy sum of |j|^2 / (2 rho).  Dense path: every cell.  Multi-level
+   cases: the volume-weighted total of mt_case_reduce_levels (last row). */
 int mt_case_reduce(mt_ctx *ctx, int32_t case_id, double *out5);
+/* Per-level FP64 reductions of a multi-level case, the device counterpart of
+   the per-level scans of LBM_Manager::infoPrint (LBM_Manager.cpp:914-981):
+   out[(max_level + 2) * 5]; row l (l = 0 .. max_level) sums mass sum_q f_q,
+   momentum sum_q f_q e_q and |j|^2 / (2 rho) over level l's lat_f and
+   overlap_F2C cells (the cells calculateMacros visits), from the streamed f
+   widened to FP64 (storage shift added in FP64); row max_level + 1 is
+   sum_l 8^-l row_l (a level-l cell is 8^-l coarse cells; the F2C cells stand
+   for the region their C2F children cover).  Dense cases: two equal rows.
+   Each row is summed in a fixed order (run to run identical). */
+int mt_case_reduce_levels(mt_ctx *ctx, int32_t case_id, double *out);
 /* Allocation-free variant of mt_case_reduce; no reference counterpart (the
    reference has no device-side reduction).  For callers that must not allocate
    device memory during the call (a host that budgets the GPU's memory up front
    for its cases).  Same outputs and kernels; the scratch is a static device
    array of 640 KiB, so cases above 4,194,304 cells return MT_ERR_ARG.  Calls
    that overlap in time on one device race on that array: serialise them.  The
-   first call on a device does a one-time set-up (looks up the array's address);
-   make it before any stream capture.  Synchronises the stream. */
+   first call on a device does a one-time set-up (looks up the array's address
+   with that device current, then makes the caller's current device current
+   again); make it before any stream capture.  Synchronises the stream. */
 int mt_case_reduce_noalloc(mt_ctx *ctx, int32_t case_id, double *out5);
 
 /* ---- the reference call surface --------------------------------------- */
@@ -258,6 +276,14 @@ int mt_case_set_schedule(mt_ctx *ctx, int32_t case_id, int32_t schedule);
  * level interface; with the reference's factors the non-equilibrium part is
  * amplified 4x from coarse to fine and flows near tau = 0.5 go unstable. */
 int mt_case_set_interface_scaling(mt_ctx *ctx, int32_t case_id, int32_t scaling);
+/* When a fine level takes its interface cells from its parent (no reference
+ * counterpart; the reference explodes in the first substep only,
+ * LBM_Simulator.cpp:47-51,122-125, MT_ITIME_REFERENCE, the default).
+ * MT_ITIME_HOLD explodes in the second substep as well, from the same parent
+ * values (the parent has not streamed yet), so the C2F cells of the second
+ * substep hold the parent's state instead of populations streamed through
+ * the shell without a collision. */
+int mt_case_set_interface_time(mt_ctx *ctx, int32_t case_id, int32_t mode);
 /* Velocity of one face strategy (face 0..5 = West East South North Bot Top),
  * the input_v each nonEquilibrumExtrapolation_<face> / inlet strategy is
  * constructed with (NonEquilibrumExtrapolation.hpp:37-100; LBM_Manager.cpp:53-61
@@ -325,6 +351,12 @@ int mt_marker_record(mt_ctx *ctx, int64_t *ticket);
 int mt_marker_done(mt_ctx *ctx, int64_t ticket, int32_t *done);
 int mt_case_force_async(mt_ctx *ctx, int32_t case_id);
 int mt_case_force_copied(mt_ctx *ctx, int32_t case_id, double *out4);
+/* The non-finite check of the state (mt_case_status's guard, over the
+ * post-collision buffers every schedule steps from) that mt_case_force_async
+ * also enqueues: MT_OK, or MT_ERR_NONFINITE when the copied flags show a NaN
+ * or Inf population.  Valid under the same marker as the force copy.  The
+ * reference stops on NaN by scanning on the host (LBM_Simulator.cpp:33-41). */
+int mt_case_status_copied(mt_ctx *ctx, int32_t case_id);
 
 #ifdef __cplusplus
 }

@@ -19,7 +19,7 @@ from .mesh import Mesh, MeshSpec, Sphere, build_mesh, spec_mesh, sphere_markers
 
 COLLISIONS = {"LBGK": 0, "Cumulant": 1}
 IB_METHODS = {"DW": 0, "FH": 1, "DF": 2}
-BC_MODES = {"neq": 0, "zouhe_outflow": 1}
+BC_MODES = {"neq": 0, "zouhe_outflow": 1, "zouhe_hh": 2}
 STREAM_CONVENTIONS = {"reference": 0, "textbook": 1}
 STORAGE = {"f64": 0, "f32": 1, "f16": 2, "bf16": 3}
 

@@ -610,10 +610,11 @@ int amr_lbm_kernel(Ctx &ctx, Case &c, int l)
         if (l == 0 && c.d.bc_mode == MT_BC_ZOUHE_OUTFLOW) RUN(PH_BC_INOUT, 0);
         if (l < L)
             if ((rc = amr_lbm_kernel(ctx, c, l + 1))) return rc;
-        if (sub == 0 && l > 0) RUN(PH_EXPLOSION, l);
+        if ((sub == 0 || c.itime == MT_ITIME_HOLD) && l > 0) RUN(PH_EXPLOSION, l);
         RUN(PH_STREAM, l);
         if (l == 0) {
             if (c.d.bc_mode == MT_BC_NEQ) RUN(PH_BC, 0);
+            if (c.d.bc_mode == MT_BC_ZOUHE_HH) RUN(PH_BC_HH, 0);
         } else if (l == L) {
             RUN(PH_IB, L);
         }
@@ -688,7 +689,7 @@ static int fused_lbm_kernel(Ctx &ctx, Case &c, int l, bool last_parent)
         if (l == 0 && c.d.bc_mode == MT_BC_ZOUHE_OUTFLOW) RUN(PH_BC_INOUT, 0);
         if (l < L)
             if ((rc = fused_lbm_kernel(ctx, c, l + 1, last))) return rc;
-        if (sub == 0 && l > 0) RUN(PH_EXPLOSION, l);
+        if ((sub == 0 || c.itime == MT_ITIME_HOLD) && l > 0) RUN(PH_EXPLOSION, l);
         c.macros_now = last && !(l == 0 && c.d.bc_mode == MT_BC_NEQ);
         RUN(PH_PULL_COLLIDE, l);
         if (l == L && c.lv[l].nband) RUN(PH_DF, l);
@@ -1003,8 +1004,8 @@ int batch_lbm_kernel(Ctx &ctx, BatchRec &R, const std::vector<Case *> &all, int 
                                  [&](Case &c) { return amr_phase(ctx, c, PH_BC_INOUT, 0); })))
                 return rc;
         if ((rc = batch_lbm_kernel(ctx, R, cs, l + 1, last))) return rc;
-        if (sub == 0 && l > 0)
-            if ((rc = fork_cases(ctx, R, cs, [](Case &) { return true; },
+        if (l > 0)
+            if ((rc = fork_cases(ctx, R, cs, [sub](Case &c) { return sub == 0 || c.itime == MT_ITIME_HOLD; },
                                  [&](Case &c) { return amr_phase(ctx, c, PH_EXPLOSION, l); })))
                 return rc;
         for (Case *c : cs) c->macros_now = last && !(l == 0 && c->d.bc_mode == MT_BC_NEQ);
@@ -1188,6 +1189,25 @@ int amr_guard(Ctx &ctx, Case &c, int *flags)
     MT_CUDA(ctx, cudaMemcpyAsync(flags, c.dev_err, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
     MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
     return MT_OK;
+}
+
+// FP64 per-level and volume-weighted sums of mass, momentum and kinetic
+// energy (host out[(max_level + 2) * 5]); the streamed f is rebuilt first
+// where the fused schedule does not store it
+int amr_reduce(Ctx &ctx, Case &c, double *h_out)
+{
+    if (int rc = amr_sync_f(ctx, c)) return rc;
+    const size_t nb = sizeof(double) * 5 * (size_t)(c.d.max_level + 2);
+    double *d = nullptr;
+    MT_CUDA(ctx, cudaMallocAsync(&d, nb, ctx.stream));
+    int rc = amr_dispatch(c, [&](auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        return AmrOps<S>::reduce(ctx, c, d);
+    });
+    if (!rc) MT_CUDA(ctx, cudaMemcpyAsync(h_out, d, nb, cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    cudaFreeAsync(d, ctx.stream);
+    return rc;
 }
 
 // populations of one level as FP64 [Q][n] (host buffers), in either direction

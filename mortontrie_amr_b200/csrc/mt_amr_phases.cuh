@@ -14,6 +14,7 @@
 #include <algorithm>
 
 #include "mt_internal.hpp"
+#include "mt_pack2.cuh"
 #include "mt_store.cuh"
 
 namespace mt {
@@ -378,6 +379,82 @@ __global__ void k_bc_inout(const int32_t *list, int64_t nl, int east, int64_t n,
     }
 }
 
+// Restated wet-node boundaries on the x faces (MT_BC_ZOUHE_HH, D3Q19):
+// after the level-0 stream the West / East shell cells pull from their
+// neighbours like fluid cells (a missing source keeps f) and complete the
+// populations that come from outside the box -- West: the Zou-He velocity
+// inlet with the Hecht-Harting transverse corrections (the formula family of
+// BC/ZouHe_Velocity.cpp:81-93,170-199); East: the five incoming populations
+// copied from the inner neighbour's streamed ones (BC/Outflow.cpp:39-52).
+// The formulas are those of a textbook stream; under the reference's
+// reversed pull they act on g_k = f_inv(k) with the velocity -u_bc.
+// k_bc_wall_collide then collides the completed cells (LBGK, level-0 tau).
+template <class S>
+__global__ void k_bc_hh(const int32_t *list, int64_t nl, int east, int64_t n, int textbook,
+                        const int32_t *__restrict__ nbr, const S *__restrict__ fcol, S *__restrict__ f, double ux,
+                        double uy, double uz, int *err, const Shift sh)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    C g[19];
+#pragma unroll
+    for (int k = 0; k < 19; ++k) {
+        const int m = textbook ? k : inv(k);
+        const int32_t src = m == 0 ? (int32_t)i : nbr[(int64_t)((textbook ? inv(m) : m) - 1) * n + i];
+        g[k] = full_sh<S>(sh, src >= 0 ? T::ld(fcol, (int64_t)m * n + src) : T::ld(f, (int64_t)m * n + i), m);
+    }
+    const C sgn = textbook ? C(1) : C(-1);
+    if (!east) {
+        const C Ux = sgn * (C)ux, Uy = sgn * (C)uy, Uz = sgn * (C)uz;
+        const C rho = (g[0] + g[3] + g[4] + g[5] + g[6] + g[15] + g[16] + g[17] + g[18] +
+                       C(2) * (g[2] + g[8] + g[10] + g[12] + g[14])) / (C(1) - Ux);
+        const C ny = C(0.5) * (g[3] + g[15] + g[17] - g[4] - g[16] - g[18]) - rho * Uy / C(3);
+        const C nz = C(0.5) * (g[5] + g[15] + g[18] - g[6] - g[16] - g[17]) - rho * Uz / C(3);
+        g[1] = g[2] + rho * Ux / C(3);
+        g[7] = g[8] + rho * (Ux + Uy) / C(6) - ny;
+        g[9] = g[10] + rho * (Ux - Uy) / C(6) + ny;
+        g[11] = g[12] + rho * (Ux + Uz) / C(6) - nz;
+        g[13] = g[14] + rho * (Ux - Uz) / C(6) + nz;
+    } else {
+        const int32_t nb = nbr[(int64_t)(2 - 1) * n + i];  // the cell at -x
+        if (nb < 0) {
+            atomicOr(err, DEVERR_MISSING_BC_NBR);
+            return;
+        }
+        const int in_e[5] = {2, 8, 10, 12, 14};
+#pragma unroll
+        for (int t = 0; t < 5; ++t) {
+            const int k = in_e[t], m = textbook ? k : inv(k);
+            g[k] = full_sh<S>(sh, T::ld(f, (int64_t)m * n + nb), m);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 19; ++k) {
+        const int m = textbook ? k : inv(k);
+        T::st(f, (int64_t)m * n + i, stored_sh<S>(sh, g[k], m));
+    }
+}
+
+template <class S>
+__global__ void k_bc_wall_collide(const int32_t *list, int64_t nl, int64_t n, double tau, const S *__restrict__ f,
+                                  S *__restrict__ fcol, const Shift sh)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= nl) return;
+    const int64_t i = list[j];
+    C d[19];
+#pragma unroll
+    for (int k = 0; k < 19; ++k) d[k] = full_sh<S>(sh, T::ld(f, (int64_t)k * n + i), k);
+    C r, x, y, z;
+    macros_g<19, C>(d, r, x, y, z);
+    collide_store<19, S, MT_COLL_LBGK>(d, r, x, y, z, tau, fcol, n, i, sh);
+}
+
 // D3Q19_BC_Strategy::initial_Feq (D3Q19_BC_Manager.hpp:157-167) on one
 // boundary set: f = fcol = feq(rho0, u) with the face's velocity
 template <int Q, class S>
@@ -704,17 +781,156 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
     }
 }
 
+// The reduced-precision form of brick_warp: both cells of a lane are
+// gathered first, then collided together with packed FP32 pairs (mt_pack2.cuh).
+// Cells that stream without colliding (class 2), band cells (class 4) and
+// absent cells take their own scalar paths; when only one cell of the pair
+// collides, the other lane of the pair repeats its values and is not stored.
 template <int Q, class S, int COLL>
+__device__ __forceinline__ void brick_warp_pair(int64_t b, int lane, int32_t *s_idx, const int32_t *__restrict__ halo,
+                                                const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
+                                                const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext,
+                                                double tau, float *__restrict__ rho, float *__restrict__ u, int macros,
+                                                int fall, long long *__restrict__ acc, const Shift &sh)
+{
+    using T = Store<S>;
+    const int32_t *hb = halo + 216 * b;
+    for (int h = lane; h < 216; h += 32) s_idx[h] = __ldg(hb + h);
+    __syncwarp();
+    int base[2], cls[2];
+    uint32_t idx[2];
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+        const int m = lane + 32 * p;
+        const int lx = (m & 1) | ((m >> 2) & 2), ly = ((m >> 1) & 1) | ((m >> 3) & 2),
+                  lz = ((m >> 2) & 1) | ((m >> 4) & 2);
+        base[p] = (lx + 1) + 6 * (ly + 1) + 36 * (lz + 1);
+        const int32_t ii = s_idx[base[p]];
+        cls[p] = ii >= 0 ? (int)__ldg(bcls + 64 * b + m) : 0;
+        idx[p] = ii >= 0 ? (uint32_t)ii : 0u;
+    }
+    if (!cls[0] && !cls[1]) return;
+    bool coll[2];
+    float2 d[Q];
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+        coll[p] = cls[p] == 1 || cls[p] == 3;
+        if (!cls[p]) continue;
+        const uint32_t i = idx[p];
+        const bool keep_f = cls[p] != 1 || fall;
+        // gather, store what this cell's class stores, keep the full FP32 value
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            const int off = ex(k) + 6 * ey(k) + 36 * ez(k);
+            const int32_t src = k ? s_idx[base[p] + (textbook ? -off : off)] : (int32_t)i;
+            const S val = src >= 0 ? fcol[(uint32_t)k * n + (uint32_t)src] : f[(uint32_t)k * n + i];
+            if (keep_f && src >= 0) f[(uint32_t)k * n + i] = val;
+            if (cls[p] == 2) fnext[(uint32_t)k * n + i] = val;
+            const float fv = full_sh<S>(sh, T::cv(val), k);
+            if (p == 0)
+                d[k].x = fv;
+            else
+                d[k].y = fv;
+        }
+        if constexpr (COLL == MT_COLL_LBGK) {
+            if (cls[p] == 4 && acc) {
+                // direct-forcing band: macros of the streamed f, accumulator cleared
+                float dd[Q];
+#pragma unroll
+                for (int k = 0; k < Q; ++k) dd[k] = p == 0 ? d[k].x : d[k].y;
+                float r, x, y, z;
+                macros_g<Q, float>(dd, r, x, y, z);
+                rho[i] = r;
+                u[i] = x;
+                u[n + i] = y;
+                u[2 * n + i] = z;
+                acc[i] = 0;
+                acc[n + i] = 0;
+                acc[2 * n + i] = 0;
+            }
+        }
+    }
+    if (!coll[0] && !coll[1]) return;
+    // a pair with one colliding cell: the other lane repeats its values
+    if (!coll[1]) {
+#pragma unroll
+        for (int k = 0; k < Q; ++k) d[k].y = d[k].x;
+    } else if (!coll[0]) {
+#pragma unroll
+        for (int k = 0; k < Q; ++k) d[k].x = d[k].y;
+    }
+    float2 r, x, y, z;
+    p2::macros<Q>(d, r, x, y, z);
+    if (macros) {
+        if (coll[0]) {
+            rho[idx[0]] = r.x;
+            u[idx[0]] = x.x;
+            u[n + idx[0]] = y.x;
+            u[2 * n + idx[0]] = z.x;
+        }
+        if (coll[1]) {
+            rho[idx[1]] = r.y;
+            u[idx[1]] = x.y;
+            u[n + idx[1]] = y.y;
+            u[2 * n + idx[1]] = z.y;
+        }
+    }
+    float2 o[Q];
+    if constexpr (COLL == MT_COLL_LBGK) {
+        p2::lbgk<Q>(d, r, x, y, z, (float)(1.0 / tau), sh, o);  // stored deviations already
+    } else {
+        p2::cumulant(d, r, x, y, z, (float)(1.0 / tau), o);
+#pragma unroll
+        for (int k = 0; k < Q; ++k) o[k] = p2::sub(o[k], p2::bc(sh.v[k]));
+    }
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        if (coll[0]) T::st(fnext, (uint32_t)k * n + idx[0], o[k].x);
+        if (coll[1]) T::st(fnext, (uint32_t)k * n + idx[1], o[k].y);
+    }
+}
+
+// brick_warp for every storage: the pair form for the reduced storages
+// (MT_BRICK_SCALAR keeps the one-cell-at-a-time form for them too)
+template <int Q, class S, int COLL>
+__device__ __forceinline__ void brick_warp_any(int64_t b, int lane, int32_t *s_idx, const int32_t *__restrict__ halo,
+                                               const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
+                                               const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext,
+                                               double tau, typename Store<S>::C *__restrict__ rho,
+                                               typename Store<S>::C *__restrict__ u, int macros, int fall,
+                                               long long *__restrict__ acc, const Shift &sh)
+{
+#ifndef MT_BRICK_SCALAR
+    if constexpr (Store<S>::shifted && (COLL == MT_COLL_LBGK || Q == 27))
+        brick_warp_pair<Q, S, COLL>(b, lane, s_idx, halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros,
+                                    fall, acc, sh);
+    else
+#endif
+        brick_warp<Q, S, COLL>(b, lane, s_idx, halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros, fall,
+                               acc, sh);
+}
+
 #ifndef MT_BRICK_MIN_BLOCKS
-#define MT_BRICK_MIN_BLOCKS 8  // resident 128-thread blocks per SM asked of the 16-bit brick passes (64 registers)
+#define MT_BRICK_MIN_BLOCKS 8  // resident 128-thread blocks per SM asked of the 16-bit one-cell passes (64 registers)
 #endif
 #ifndef MT_BRICK_MIN_BLOCKS_Q19_LBGK
-#define MT_BRICK_MIN_BLOCKS_Q19_LBGK 10  // 16-bit D3Q19 LBGK passes: 48 registers, no spills
+#define MT_BRICK_MIN_BLOCKS_Q19_LBGK 10  // 16-bit D3Q19 LBGK one-cell passes: 48 registers, no spills
 #endif
-__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? ((COLL == MT_COLL_LBGK && Q == 19)
-                                                                  ? MT_BRICK_MIN_BLOCKS_Q19_LBGK
-                                                                  : MT_BRICK_MIN_BLOCKS)
-                                                             : 1) k_brick_step(
+#ifndef MT_BRICK_PAIR_MIN_BLOCKS
+#define MT_BRICK_PAIR_MIN_BLOCKS 4  // the pair passes of every reduced storage (128 registers)
+#endif
+// resident blocks per SM asked of a brick pass
+template <int Q, class S, int COLL> constexpr int brick_min_blocks()
+{
+#ifndef MT_BRICK_SCALAR
+    if (Store<S>::shifted) return MT_BRICK_PAIR_MIN_BLOCKS;
+#endif
+    if (Store<S>::bytes == 2) return (COLL == MT_COLL_LBGK && Q == 19) ? MT_BRICK_MIN_BLOCKS_Q19_LBGK : MT_BRICK_MIN_BLOCKS;
+    return 1;
+}
+
+template <int Q, class S, int COLL>
+__global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL>()) k_brick_step(
     int64_t nb, const int32_t *__restrict__ halo, const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
     const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext, double tau,
     typename Store<S>::C *__restrict__ rho, typename Store<S>::C *__restrict__ u, int macros, int fall,
@@ -724,19 +940,16 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? ((COLL == MT_COLL_
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t b = 4 * (int64_t)blockIdx.x + w;
     if (b >= nb) return;
-    brick_warp<Q, S, COLL>(b, lane, s_idx[w], halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros, fall,
-                           acc, sh);
+    brick_warp_any<Q, S, COLL>(b, lane, s_idx[w], halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros, fall,
+                               acc, sh);
 }
 
 // The same pass over the bricks of many cases (a batch): brick b of the work
 // list belongs to the slot whose [off[s], off[s + 1]) range holds it; each
 // slot carries one case level's tables, buffers and relaxation time.
-#ifndef MT_BRICK_BATCH_MIN_BLOCKS
-#define MT_BRICK_BATCH_MIN_BLOCKS MT_BRICK_MIN_BLOCKS  // the same for the batched pass
-#endif
 template <int Q, class S, int COLL>
-__global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_BATCH_MIN_BLOCKS : 1) k_brick_step_batch(const BrickBatch *__restrict__ bb,
-                                                                                                   const Shift sh)
+__global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL>()) k_brick_step_batch(const BrickBatch *__restrict__ bb,
+                                                                                          const Shift sh)
 {
     __shared__ int32_t s_idx[4][216];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -752,8 +965,9 @@ __global__ void __launch_bounds__(128, Store<S>::bytes == 2 ? MT_BRICK_BATCH_MIN
     }
     const BrickSlot &sl = bb->slot[lo];
     using C = typename Store<S>::C;
-    brick_warp<Q, S, COLL>(b - bb->off[lo], lane, s_idx[w], sl.halo, sl.cls, sl.n, sl.textbook, (const S *)sl.fcol,
-                           (S *)sl.f, (S *)sl.fnext, sl.tau, (C *)sl.rho, (C *)sl.u, sl.macros, sl.fall, sl.acc, sh);
+    brick_warp_any<Q, S, COLL>(b - bb->off[lo], lane, s_idx[w], sl.halo, sl.cls, sl.n, sl.textbook,
+                               (const S *)sl.fcol, (S *)sl.f, (S *)sl.fnext, sl.tau, (C *)sl.rho, (C *)sl.u, sl.macros,
+                               sl.fall, sl.acc, sh);
 }
 
 // The streamed f of the class-1 cells, from the buffer the last fused pass
@@ -1384,6 +1598,29 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             }
         return MT_OK;
     }
+    case PH_BC_HH: {
+        if constexpr (Q == 19) {
+            Level &l0 = c.lv[0];
+            for (int face = 0; face < 2; ++face) {
+                if (!l0.nbc[face]) continue;
+                k_bc_hh<S><<<grid_for(l0.nbc[face], B), B, 0, s>>>(l0.bclist[face], l0.nbc[face], face, l0.n,
+                                                                    c.d.stream_convention, l0.nbr, A::fcol(l0),
+                                                                    A::f(l0), c.face_u[0][0], c.face_u[0][1],
+                                                                    c.face_u[0][2], c.dev_err, c.shift[0]);
+                MT_LAUNCHED(ctx);
+            }
+            for (int face = 0; face < 2; ++face) {
+                if (!l0.nbc[face]) continue;
+                k_bc_wall_collide<S><<<grid_for(l0.nbc[face], B), B, 0, s>>>(l0.bclist[face], l0.nbc[face], l0.n,
+                                                                              c.d.tau[0], A::f(l0), A::fcol(l0),
+                                                                              c.shift[0]);
+                MT_LAUNCHED(ctx);
+            }
+            return MT_OK;
+        } else {
+            return set_err(ctx, MT_ERR_ARG, "the Zou-He / Hecht-Harting boundary is D3Q19");
+        }
+    }
     case PH_BC_INOUT: {
         Level &l0 = c.lv[0];
         for (int face = 0; face < 2; ++face) {
@@ -1722,15 +1959,135 @@ int AmrOps<S>::batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, i
     return MT_OK;
 }
 
+// ---- FP64 reductions of a multi-level case (mt_case_reduce_levels) -------
+// Per-block partial sums over a level's stepped cells (the collide list,
+// lat_f then overlap_F2C: the cells LBM_Manager::calculateMacros visits,
+// LBM_Manager.cpp:1003-1050) of mass sum_q f_q, momentum sum_q f_q e_q and
+// kinetic energy |j|^2 / (2 rho), every value widened to FP64 before the
+// storage shift (FP64) is added back.  partial: [5][gridDim.x].
+template <int Q, class S>
+__global__ void k_level_reduce(const S *f, int64_t n, const int32_t *list, int64_t m, const Shift sh,
+                               double *partial)
+{
+    __shared__ double red[5][256];
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double a[5] = {0, 0, 0, 0, 0};
+    if (j < m) {
+        const int64_t i = list[j];
+        double r = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            double v = (double)Store<S>::ld(f, (int64_t)k * n + i);
+            if (Store<S>::shifted) v += sh.d[k];
+            r += v;
+            jx += v * ex(k);
+            jy += v * ey(k);
+            jz += v * ez(k);
+        }
+        a[0] = r;
+        a[1] = jx;
+        a[2] = jy;
+        a[3] = jz;
+        a[4] = 0.5 * (jx * jx + jy * jy + jz * jz) / r;
+    }
+    for (int c = 0; c < 5; ++c) red[c][threadIdx.x] = a[c];
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st)
+            for (int c = 0; c < 5; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 5; ++c) partial[(int64_t)c * gridDim.x + blockIdx.x] = red[c][0];
+}
+
+// where each level's partials start in the scratch and how many blocks it has
+struct LevelPartials {
+    int64_t off[kMaxLevels];
+    int64_t nb[kMaxLevels];
+    int nlev;
+};
+
+// one block: level rows in a fixed order (strided sums, then a tree), then
+// the global row sum_l 8^-l row_l (a level-l cell is 8^-l coarse cells).
+// out: [(nlev + 1) * 5]
+static __global__ void k_level_totals(const double *partial, const LevelPartials P, double *out)
+{
+    __shared__ double red[256];
+    for (int l = 0; l < P.nlev; ++l)
+        for (int c = 0; c < 5; ++c) {
+            const double *p = partial + P.off[l] + (int64_t)c * P.nb[l];
+            double a = 0;
+            for (int64_t j = threadIdx.x; j < P.nb[l]; j += blockDim.x) a += p[j];
+            red[threadIdx.x] = a;
+            __syncthreads();
+            for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+                if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) out[l * 5 + c] = red[0];
+            __syncthreads();
+        }
+    if (threadIdx.x < 5) {
+        double g = 0, wl = 1.0;
+        for (int l = 0; l < P.nlev; ++l) {
+            g += wl * out[l * 5 + threadIdx.x];
+            wl *= 0.125;
+        }
+        out[P.nlev * 5 + threadIdx.x] = g;
+    }
+}
+
 template <class S>
-int AmrOps<S>::guard(Ctx &ctx, Case &c)
+int AmrOps<S>::reduce(Ctx &ctx, Case &c, double *d_out)
+{
+    LevelPartials P{};
+    P.nlev = c.d.max_level + 1;
+    int64_t total = 0;
+    for (int l = 0; l < P.nlev; ++l) {
+        P.off[l] = total;
+        P.nb[l] = (c.lv[l].ncollide + 255) / 256;
+        total += 5 * P.nb[l];
+    }
+    double *partial = nullptr;
+    MT_CUDA(ctx, cudaMallocAsync(&partial, sizeof(double) * std::max<int64_t>(total, 1), ctx.stream));
+    cudaError_t err = cudaSuccess;
+    auto launched = [&]() {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) err = e;
+        else ctx.launches++;
+        return e == cudaSuccess;
+    };
+    bool ok = true;
+    for (int l = 0; l < P.nlev && ok; ++l) {
+        Level &lv = c.lv[l];
+        if (!P.nb[l]) continue;
+        if (c.d.q == 19)
+            k_level_reduce<19, S><<<(unsigned)P.nb[l], 256, 0, ctx.stream>>>(
+                (const S *)lv.f, lv.n, lv.collide_list, lv.ncollide, c.shift[l], partial + P.off[l]);
+        else
+            k_level_reduce<27, S><<<(unsigned)P.nb[l], 256, 0, ctx.stream>>>(
+                (const S *)lv.f, lv.n, lv.collide_list, lv.ncollide, c.shift[l], partial + P.off[l]);
+        ok = launched();
+    }
+    if (ok) {
+        k_level_totals<<<1, 256, 0, ctx.stream>>>(partial, P, d_out);
+        ok = launched();
+    }
+    cudaFreeAsync(partial, ctx.stream);
+    if (!ok) return set_err(ctx, MT_ERR_CUDA, std::string("reduction launch: ") + cudaGetErrorString(err));
+    return MT_OK;
+}
+
+template <class S>
+int AmrOps<S>::guard(Ctx &ctx, Case &c, bool current_only)
 {
     for (int l = 0; l <= c.d.max_level; ++l) {
         Level &lv = c.lv[l];
         if (!lv.n) continue;
         const int64_t total = lv.n * c.d.q;
         k_guard<S><<<(unsigned)std::min<int64_t>(grid_for(total, 256), 148 * 16), 256, 0, ctx.stream>>>(
-            (const S *)lv.f, (const S *)lv.fcol, total, c.dev_err);
+            (const S *)(current_only ? lv.fcol : lv.f), (const S *)lv.fcol, total, c.dev_err);
         MT_LAUNCHED(ctx);
     }
     return MT_OK;

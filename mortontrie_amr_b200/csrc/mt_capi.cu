@@ -52,6 +52,10 @@ int check_desc(Ctx &ctx, const mt_case_desc *d)
     if (d->storage < MT_STORE_F64 || d->storage > MT_STORE_BF16) return set_err(ctx, MT_ERR_ARG, "unknown storage");
     if (d->ib_method != MT_IB_DW && d->ib_method != MT_IB_FH && d->ib_method != MT_IB_DF)
         return set_err(ctx, MT_ERR_ARG, "unknown immersed-boundary method");
+    if (d->bc_mode != MT_BC_NEQ && d->bc_mode != MT_BC_ZOUHE_OUTFLOW && d->bc_mode != MT_BC_ZOUHE_HH)
+        return set_err(ctx, MT_ERR_ARG, "unknown boundary mode");
+    if (d->bc_mode == MT_BC_ZOUHE_HH && (d->q != 19 || d->collision != MT_COLL_LBGK))
+        return set_err(ctx, MT_ERR_ARG, "the Zou-He / Hecht-Harting boundary is D3Q19 LBGK");
     if (d->ib_method == MT_IB_DF && d->collision != MT_COLL_LBGK)
         return set_err(ctx, MT_ERR_ARG, "direct forcing is implemented with the LBGK collision");
     for (int l = 0; l <= d->max_level; ++l)
@@ -269,9 +273,12 @@ int mt_case_create_dense(mt_ctx *h, const mt_case_desc *d, int32_t *id)
     const int64_t e = d->extent0[0];
     if (e != d->extent0[1] || e != d->extent0[2] || (e & (e - 1)) != 0 || e < 2 || e > 1024)
         return set_err(ctx, MT_ERR_ARG, "the dense path needs a cube of 2^b cells per edge, 2 <= 2^b <= 1024");
-    for (int a = 0; a < 3; ++a)
-        if (d->u_shift[0][a] != 0.0)
-            return set_err(ctx, MT_ERR_ARG, "the dense path stores f - w (u_shift must be zero)");
+    // every level's shift is checked, not only level 0's: a shift requested
+    // for any level would otherwise be dropped without a word
+    for (int l = 0; l < MT_MAX_LEVELS; ++l)
+        for (int a = 0; a < 3; ++a)
+            if (d->u_shift[l][a] != 0.0)
+                return set_err(ctx, MT_ERR_ARG, "the dense path stores f - w (u_shift must be zero on every level)");
     Case *c = new Case();
     c->d = *d;
     c->dense = true;
@@ -673,6 +680,24 @@ int mt_case_get_macros(mt_ctx *h, int32_t id, int32_t level, double *rho, double
     return amr_macros(ctx, *c, level, rho, u);
 }
 
+int mt_case_reduce_levels(mt_ctx *h, int32_t id, double *out)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!out) return set_err(ctx, MT_ERR_ARG, "null output");
+    if (c->dense) {
+        // one level: its row and the total are the same sums
+        rc = mt_case_reduce(h, id, out);
+        if (!rc)
+            for (int k = 0; k < 5; ++k) out[5 + k] = out[k];
+        return rc;
+    }
+    if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+    return amr_reduce(ctx, *c, out);
+}
+
 int mt_case_reduce(mt_ctx *h, int32_t id, double *out)
 {
     Case *c;
@@ -680,7 +705,15 @@ int mt_case_reduce(mt_ctx *h, int32_t id, double *out)
     if (rc) return rc;
     Ctx &ctx = h->c;
     if (!out) return set_err(ctx, MT_ERR_ARG, "null output");
-    if (!c->dense) return set_err(ctx, MT_ERR_STATE, "device reductions are implemented for the dense path");
+    if (!c->dense) {
+        // the volume-weighted total row of the per-level reduction
+        if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+        std::vector<double> rows(5 * (size_t)(c->d.max_level + 2));
+        rc = amr_reduce(ctx, *c, rows.data());
+        if (!rc)
+            for (int k = 0; k < 5; ++k) out[k] = rows[5 * (size_t)(c->d.max_level + 1) + k];
+        return rc;
+    }
     double *d = nullptr;
     MT_CUDA(ctx, cudaMallocAsync(&d, sizeof(double) * 5, ctx.stream));
     rc = dense_dispatch(*c, [&](auto *tag) {
@@ -703,7 +736,8 @@ int mt_apply_bc(mt_ctx *h, int32_t id)
     Case *c;
     int rc = get_case(h, id, &c);
     if (rc) return rc;
-    return phase_call(h, id, c->d.bc_mode == MT_BC_NEQ ? PH_BC : PH_BC_INOUT, 0);
+    return phase_call(h, id, c->d.bc_mode == MT_BC_NEQ ? PH_BC : (c->d.bc_mode == MT_BC_ZOUHE_HH ? PH_BC_HH : PH_BC_INOUT),
+                      0);
 }
 int mt_apply_bc_face(mt_ctx *h, int32_t id, int32_t face)
 {
@@ -774,6 +808,8 @@ int mt_case_set_schedule(mt_ctx *h, int32_t id, int32_t schedule)
     if (c->dense) return set_err(ctx, MT_ERR_STATE, "the dense path has a single (fused) schedule");
     if (schedule != MT_SCHED_PHASES && schedule != MT_SCHED_FUSED && schedule != MT_SCHED_FUSED_LISTS)
         return set_err(ctx, MT_ERR_ARG, "schedule must be MT_SCHED_PHASES, MT_SCHED_FUSED or MT_SCHED_FUSED_LISTS");
+    if (schedule != MT_SCHED_PHASES && c->d.bc_mode == MT_BC_ZOUHE_HH)
+        return set_err(ctx, MT_ERR_ARG, "the Zou-He / Hecht-Harting boundary runs under the phase schedule");
     const bool bricks = schedule == MT_SCHED_FUSED;
     if (!c->dense && c->built && (rc = amr_sync_f(ctx, *c))) return rc;
     if (schedule == MT_SCHED_PHASES) {
@@ -810,6 +846,28 @@ int mt_case_set_interface_scaling(mt_ctx *h, int32_t id, int32_t scaling)
         }
     }
     c->scaling = scaling;
+    return MT_OK;
+}
+
+int mt_case_set_interface_time(mt_ctx *h, int32_t id, int32_t mode)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense) return set_err(ctx, MT_ERR_STATE, "the dense path has no level interface");
+    if (mode != MT_ITIME_REFERENCE && mode != MT_ITIME_HOLD)
+        return set_err(ctx, MT_ERR_ARG, "mode must be MT_ITIME_REFERENCE or MT_ITIME_HOLD");
+    if (mode != c->itime) {
+        // the captured steps bake the explosion launches in
+        if (c->graph) cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+        for (int p = 0; p < 2; ++p) {
+            if (c->fgraph[p]) cudaGraphExecDestroy(c->fgraph[p]);
+            c->fgraph[p] = nullptr;
+        }
+    }
+    c->itime = mode;
     return MT_OK;
 }
 
@@ -906,6 +964,8 @@ int mt_case_prepare(mt_ctx *h, int32_t id)
     if (rc) return rc;
     Ctx &ctx = h->c;
     if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "prepare needs a built multi-level case");
+    if (c->d.bc_mode == MT_BC_ZOUHE_HH)
+        return set_err(ctx, MT_ERR_ARG, "the Zou-He / Hecht-Harting boundary runs under the phase schedule");
     if ((rc = amr_sync_f(ctx, *c))) return rc;
     if (c->schedule != MT_SCHED_FUSED) {
         c->schedule = MT_SCHED_FUSED;
@@ -976,6 +1036,8 @@ int mt_batch_add(mt_ctx *h, int32_t id, int32_t case_id)
     if ((rc = get_case(h, case_id, &c))) return rc;
     Ctx &ctx = h->c;
     if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "batches hold built multi-level cases");
+    if (c->d.bc_mode == MT_BC_ZOUHE_HH)
+        return set_err(ctx, MT_ERR_ARG, "the Zou-He / Hecht-Harting boundary runs under the phase schedule");
     for (int32_t x : b->ids)
         if (x == case_id) return set_err(ctx, MT_ERR_ARG, "the case is already in the batch");
     if ((rc = amr_sync_f(ctx, *c))) return rc;
@@ -1099,10 +1161,31 @@ int mt_case_force_async(mt_ctx *h, int32_t id)
     Ctx &ctx = h->c;
     if (c->dense || !c->force_acc) return set_err(ctx, MT_ERR_STATE, "the case has no force accumulator");
     if (!c->h_force) {
-        MT_CUDA(ctx, cudaHostAlloc((void **)&c->h_force, 4 * sizeof(double), cudaHostAllocDefault));
-        for (int i = 0; i < 4; ++i) c->h_force[i] = 0.0;
+        MT_CUDA(ctx, cudaHostAlloc((void **)&c->h_force, 6 * sizeof(double), cudaHostAllocDefault));
+        for (int i = 0; i < 6; ++i) c->h_force[i] = 0.0;
     }
     MT_CUDA(ctx, cudaMemcpyAsync(c->h_force, c->force_acc, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    // the state's guard, stream-ordered behind the same steps: flags land
+    // beside the force copy
+    MT_CUDA(ctx, cudaMemsetAsync(c->dev_err, 0, sizeof(int), ctx.stream));
+    rc = amr_dispatch(*c, [&](auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        return AmrOps<S>::guard(ctx, *c, true);
+    });
+    if (rc) return rc;
+    MT_CUDA(ctx, cudaMemcpyAsync((int *)(c->h_force + 4), c->dev_err, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    return MT_OK;
+}
+
+int mt_case_status_copied(mt_ctx *h, int32_t id)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!c->h_force) return set_err(ctx, MT_ERR_STATE, "no status copy was requested (mt_case_force_async)");
+    const int flags = *(const int *)(c->h_force + 4);
+    if (flags & DEVERR_NONFINITE) return set_err(ctx, MT_ERR_NONFINITE, "non-finite population found by the guard");
     return MT_OK;
 }
 
@@ -1169,13 +1252,21 @@ int noalloc_scratch(mt::Ctx &ctx, double **out)
         return mt::set_err(ctx, MT_ERR_ARG, "device index out of range for the static reduction scratch");
     std::lock_guard<std::mutex> lock(g_scratch_mu);
     if (!g_scratch_ptr[ctx.device]) {
-        cudaError_t e = cudaSetDevice(ctx.device);
+        // the lookup needs ctx.device current; the caller's current device is
+        // put back afterwards, so the set-up leaves no trace on the thread
+        int prev = -1;
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) return mt::set_err(ctx, MT_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+        e = cudaSetDevice(ctx.device);
         if (e != cudaSuccess) return mt::set_err(ctx, MT_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
         double *p = nullptr;
         e = cudaGetSymbolAddress((void **)&p, g_reduce_scratch);
+        cudaError_t r = cudaSetDevice(prev);
         if (e != cudaSuccess || !p)
             return mt::set_err(ctx, MT_ERR_CUDA,
                                std::string("cudaGetSymbolAddress(reduction scratch): ") + cudaGetErrorString(e));
+        if (r != cudaSuccess)
+            return mt::set_err(ctx, MT_ERR_CUDA, std::string("cudaSetDevice (restore): ") + cudaGetErrorString(r));
         g_scratch_ptr[ctx.device] = p;
     }
     *out = g_scratch_ptr[ctx.device];

@@ -22,7 +22,7 @@ constexpr int kNumSets = 6;  // lat_f, F2C, C2F, ghost C2F, ghost F2C, solid
 // then the fused schedule's own passes
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
        PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
-       PH_SYNC_F, PH_DF, PH_BAND_GRID, PH_FACE_EQ0 = 24 };
+       PH_SYNC_F, PH_DF, PH_BAND_GRID, PH_FACE_EQ0 = 24, PH_BC_HH = 32 };
 
 // per-cell tag bits (which reference index sets the cell belongs to)
 enum : uint32_t {
@@ -133,7 +133,7 @@ struct Case {
     std::vector<double> h_tri;   // solid surface triangles [n][3][3], coarse-cell units (mt_case_set_surface)
     double *ib_force = nullptr;  // [3 * nib] per-cell force of the last treat()
     double *force_acc = nullptr; // [4] fx, fy, fz, treat count
-    double *h_force = nullptr;   // [4] page-locked copy of force_acc (mt_case_force_async)
+    double *h_force = nullptr;   // [6] page-locked: force_acc copy [4], then the guard flags (int) (mt_case_force_async)
     int *dev_err = nullptr;
     MortonGeom geom{};
     // dense uniform path
@@ -158,6 +158,7 @@ struct Case {
     // lookahead buffers hold the collision of the current f
     int schedule = MT_SCHED_PHASES;
     int scaling = MT_SCALE_REFERENCE;  // interface rescaling of the non-equilibrium part
+    int itime = MT_ITIME_REFERENCE;    // substeps in which a fine level explodes from its parent
     Shift shift[kMaxLevels];  // per level: storage shift of the reduced storages (from d.u_shift)
     double face_u[6][3] = {};          // bc_velocity of each face's strategy (u_bc unless set)
     // direct-forcing markers (MT_IB_DF)
@@ -234,6 +235,7 @@ int amr_guard(Ctx &ctx, Case &c, int *flags);
 int amr_get(Ctx &ctx, Case &c, int level, double *h_f, double *h_fcol);
 int amr_set(Ctx &ctx, Case &c, int level, const double *h_f, const double *h_fcol);
 int amr_macros(Ctx &ctx, Case &c, int level, double *h_rho, double *h_u);
+int amr_reduce(Ctx &ctx, Case &c, double *h_out);
 int amr_sync_f(Ctx &ctx, Case &c);
 int amr_set_face(Ctx &ctx, Case &c, int face, const double *u);
 int amr_prime(Ctx &ctx, Case &c);
@@ -251,7 +253,12 @@ template <class S> struct AmrOps {
     static int get(Ctx &ctx, Case &c, int level, int which, double *d_out);      // which: 0 f, 1 fcol
     static int set(Ctx &ctx, Case &c, int level, int which, const double *d_in);
     static int macros_out(Ctx &ctx, Case &c, int level, double *d_rho, double *d_u);
-    static int guard(Ctx &ctx, Case &c);
+    // non-finite populations into c.dev_err; current_only: the post-collision
+    // buffers alone (the state every schedule steps from), no f rebuild needed
+    static int guard(Ctx &ctx, Case &c, bool current_only = false);
+    // FP64 mass, momentum, kinetic energy per level over the collide list and
+    // the volume-weighted total: d_out[(max_level + 2) * 5]
+    static int reduce(Ctx &ctx, Case &c, double *d_out);
     // batched brick pass (descriptor in device memory, total bricks known on the host)
     static int batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total, const Shift &sh);
     // src's state carried onto dst's lattice (same Q, levels, storage)

@@ -32,15 +32,16 @@ EXPORTS = [
     "mt_case_init_equilibrium", "mt_case_init_fields", "mt_case_set_populations", "mt_case_get_populations",
     "mt_case_get_macros", "mt_case_reduce", "mt_calculate_macros", "mt_collide", "mt_stream", "mt_explosion",
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
-    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_face_velocity", "mt_case_set_markers",
+    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_reduce_levels", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_interface_time", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
     "mt_case_generate", "mt_case_set_surface", "mt_marker_record", "mt_marker_done", "mt_case_force_async",
-    "mt_case_force_copied", "mt_set_priority", "mt_case_remap",
+    "mt_case_force_copied", "mt_set_priority", "mt_case_remap", "mt_case_status_copied",
 ]
 
 
 SCHEDULES = {"phases": 0, "fused": 1, "fused_lists": 2}
 SCALINGS = {"reference": 0, "standard": 1}
+ITIMES = {"reference": 0, "hold": 1}
 
 
 class MTError(RuntimeError):
@@ -115,12 +116,12 @@ def lib():
             "mt_find": [vp, i32, i32, u64p, i64, i64p], "mt_case_init_equilibrium": [vp, i32, C.c_double, dp],
             "mt_case_init_fields": [vp, i32, dp, dp, dp, dp], "mt_case_set_populations": [vp, i32, i32, dp, dp],
             "mt_case_get_populations": [vp, i32, i32, dp, dp], "mt_case_get_macros": [vp, i32, i32, dp, dp],
-            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
+            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_reduce_levels": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_interface_time": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
             "mt_batch_create": [vp, i32p], "mt_batch_destroy": [vp, i32], "mt_batch_add": [vp, i32, i32],
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
             "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64],
             "mt_marker_record": [vp, i64p], "mt_marker_done": [vp, i64, i32p], "mt_case_force_async": [vp, i32],
-            "mt_case_force_copied": [vp, i32, dp], "mt_set_priority": [vp, i32], "mt_case_remap": [vp, i32, i32, i64p], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_case_force_copied": [vp, i32, dp], "mt_case_status_copied": [vp, i32], "mt_set_priority": [vp, i32], "mt_case_remap": [vp, i32, i32, i64p], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -248,7 +249,8 @@ class LBM_Manager:
     strategy objects (collide / stream / treat / boundary) as methods."""
 
     def __init__(self, ctx: Context, case: Case, storage: str = "f64", schedule: str = "phases",
-                 scaling: str = "reference", generate: bool = False, storage_shift=None):
+                 scaling: str = "reference", generate: bool = False, storage_shift=None,
+                 interface_time: str = "reference"):
         """storage: "f64" (the reference's precision, bit-exact) or "f32" /
         "f16" / "bf16" (FP32 arithmetic on stored deviations f - s_q).
         storage_shift: s_q = feq_q(1, u_s) of the reduced storages, per
@@ -257,6 +259,8 @@ class LBM_Manager:
         (see storage_shift_of).
         schedule: "phases" (the reference's passes) or "fused" (stream fused
         with the next collision; same state after every coarse step).
+        interface_time: "reference" (a fine level explodes in its first
+        substep) or "hold" (in both, from the parent's state of the step).
         generate: classify the lattice on the device from the mesh spec
         (mt_case_generate) instead of uploading the host mesher's sets; a
         SpecMesh (no host sets) is always generated."""
@@ -264,6 +268,7 @@ class LBM_Manager:
         self.case = case
         self.q = case.params.q
         self.L = case.mesh.spec.max_level
+        self.interface_time = interface_time
         self.storage = storage
         self.storage_shift = storage_shift_of(case, storage_shift)
         d = make_desc(case, storage, storage_shift)
@@ -302,6 +307,7 @@ class LBM_Manager:
             self.set_markers(m.markers)
         self.set_schedule(schedule)
         self.set_interface_scaling(scaling)
+        self.set_interface_time(self.interface_time)
         for face, u in sorted(getattr(self.case.params, "face_u", {}).items()):
             self.set_face_velocity(face, u)
 
@@ -338,6 +344,12 @@ class LBM_Manager:
         """"reference" (the reference's factors) or "standard" (stress-continuous)."""
         self.ctx.check(lib().mt_case_set_interface_scaling(self.ctx.h, self.id, SCALINGS[scaling]), "set_scaling")
         self.scaling = scaling
+
+    def set_interface_time(self, mode: str):
+        """"reference" (explosion in the first substep only) or "hold"
+        (both substeps, from the parent's post-collision state)."""
+        self.ctx.check(lib().mt_case_set_interface_time(self.ctx.h, self.id, ITIMES[mode]), "set_interface_time")
+        self.interface_time = mode
 
     def set_schedule(self, schedule: str):
         self.ctx.check(lib().mt_case_set_schedule(self.ctx.h, self.id, SCHEDULES[schedule]), "set_schedule")
@@ -454,6 +466,13 @@ class LBM_Manager:
         self.ctx.check(lib().mt_get_force(self.ctx.h, self.id, _ptr(out, C.c_double)), "get_force")
         return out
 
+    def reduce_levels(self):
+        """FP64 device sums per level (rows 0..L) and volume-weighted over all
+        levels (row L+1): columns mass, x/y/z momentum, kinetic energy."""
+        out = np.zeros((self.L + 2, 5))
+        self.ctx.check(lib().mt_case_reduce_levels(self.ctx.h, self.id, _ptr(out, C.c_double)), "reduce_levels")
+        return out
+
     def remap_from(self, src: "LBM_Manager", counts: bool = True):
         """Carry src's state onto this case's lattice (mt_case_remap); returns
         the cells per level that were copied, taken from an ancestor, taken
@@ -484,6 +503,15 @@ class LBM_Manager:
         out = np.zeros(4)
         self.ctx.check(lib().mt_case_force_copied(self.ctx.h, self.id, _ptr(out, C.c_double)), "mt_case_force_copied")
         return out
+
+    def finite_copied(self) -> bool:
+        """Whether the state was finite when force_async was enqueued (its
+        guard flags arrive with the force copy)."""
+        rc = lib().mt_case_status_copied(self.ctx.h, self.id)
+        if rc == -5:
+            return False
+        self.ctx.check(rc, "mt_case_status_copied")
+        return True
 
     def reset_force(self):
         self.ctx.check(lib().mt_reset_force(self.ctx.h, self.id), "reset_force")

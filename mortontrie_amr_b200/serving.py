@@ -71,6 +71,7 @@ class Result:
     cl: float
     coarse_steps: int
     storage: str
+    finite: bool = True    # the device guard found no NaN / Inf population when it finished
 
     @property
     def latency(self) -> float:
@@ -218,9 +219,14 @@ class ServerStats:
     drain_s: float = 0.0    # host time waiting for the device (queue full, no arrival) and releasing memory
 
     def summary(self) -> dict:
-        lat = np.array([r.latency for r in self.results]) if self.results else np.zeros(1)
-        return {"completed": len(self.results), "wall_s": round(self.wall_s, 2),
-                "cases_per_hour": round(3600.0 * len(self.results) / max(self.wall_s, 1e-9), 1),
+        """cases/h, p50 and p99 count the requests whose result is finite
+        (the guard of their state and their drag); diverged ones are counted
+        apart as failed."""
+        good = [r for r in self.results if r.finite and np.isfinite(r.cd)]
+        lat = np.array([r.latency for r in good]) if good else np.zeros(1)
+        return {"completed": len(self.results), "finite": len(good), "failed": len(self.results) - len(good),
+                "wall_s": round(self.wall_s, 2),
+                "cases_per_hour": round(3600.0 * len(good) / max(self.wall_s, 1e-9), 1),
                 "p50_s": round(float(np.percentile(lat, 50)), 3), "p99_s": round(float(np.percentile(lat, 99)), 3),
                 "max_resident_cases": self.max_resident, "max_resident_gb": round(self.max_bytes / 1e9, 2),
                 "chunks": self.chunks, "admit_s": round(self.admit_s, 2), "step_s": round(self.step_s, 2),
@@ -280,7 +286,8 @@ class Server:
                     _, mgr, req, adm, need = ent
                     cd, cl = drag_lift_of(mgr.force_copied(), req)
                     stats.results.append(Result(rid=req.rid, arrival=req.arrival, admitted=adm, finished=now(),
-                                                cd=cd, cl=cl, coarse_steps=req.coarse_steps(), storage=self.storage))
+                                                cd=cd, cl=cl, coarse_steps=req.coarse_steps(), storage=self.storage,
+                                                finite=mgr.finite_copied()))
                     finishing.remove(ent)
                     closing.append([mgr, need])
                     progressed = True
@@ -346,9 +353,10 @@ class Server:
 
 
 def solve_alone(ctx, cache: TemplateCache, req: Request, storage: str = "f16", scaling: str = "standard",
-                schedule: Optional[str] = None, storage_shift=None) -> tuple:
-    """One request by itself (no batch); returns (cd, cl, seconds)."""
-    from .lbm import LBM_Manager
+                schedule: Optional[str] = None, storage_shift=None, with_status: bool = False) -> tuple:
+    """One request by itself (no batch); returns (cd, cl, seconds), and
+    whether the state stayed finite (the device guard) with with_status."""
+    from .lbm import LBM_Manager, MTError
     case = request_case(req, cache.get(req))
     t = time.perf_counter()
     mgr = LBM_Manager(ctx, case, storage, schedule=schedule or ("phases" if storage == "f64" else "fused"),
@@ -357,8 +365,14 @@ def solve_alone(ctx, cache: TemplateCache, req: Request, storage: str = "f16", s
     ctx.synchronize()
     cd, cl = drag_lift(mgr, req)
     dt = time.perf_counter() - t
+    finite = True
+    if with_status:
+        try:
+            mgr.status()
+        except MTError:
+            finite = False
     mgr.close()
-    return cd, cl, dt
+    return (cd, cl, dt, finite) if with_status else (cd, cl, dt)
 
 
 def plain_solve_seconds(ctx, cache: TemplateCache, req: Request, sample: int = 8) -> float:

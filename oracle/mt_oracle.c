@@ -33,7 +33,7 @@ enum { COLL_LBGK = 0, COLL_CUMULANT = 1 };
 enum { IB_DW = 0, IB_FH = 1, IB_DF = 2 };
 /* domain boundary treatment on the x faces (the y/z faces follow the same
  * rule when they are not periodic) */
-enum { BC_NEQ = 0, BC_ZOUHE_OUTFLOW = 1 };
+enum { BC_NEQ = 0, BC_ZOUHE_OUTFLOW = 1, BC_ZOUHE_HH = 2 };
 
 /* Lattice tables in the reference ordering (header/Constants.h:492-538). */
 static const int EX[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0,
@@ -122,6 +122,7 @@ typedef struct {
 
 typedef struct {
     int q, L, collision, ib_method, bc_mode, stream_conv;
+    int itime_hold; /* explosion in both substeps (MT_ITIME_HOLD) */
     int periodic[3];
     int64_t extent0[3];
     double tau[OC_MAXL];
@@ -477,6 +478,7 @@ void *oc_case_new(int q, int max_level, int collision, int ib_method, int bc_mod
 {
     if ((q != 19 && q != 27) || max_level < 0 || max_level >= OC_MAXL) return NULL;
     if (collision == COLL_CUMULANT && q != 27) return NULL;
+    if (bc_mode == BC_ZOUHE_HH && (q != 19 || collision != COLL_LBGK)) return NULL;
     oc_case *c = (oc_case *)calloc(1, sizeof(oc_case));
     c->q = q;
     c->L = max_level;
@@ -1140,6 +1142,91 @@ static int phase_bc_inout(oc_case *c)
     return 0;
 }
 
+/* Restated wet-node boundaries on the x faces (MT_BC_ZOUHE_HH, D3Q19 LBGK;
+ * no runnable reference code: BC/ZouHe_Velocity.cpp and BC/Outflow.cpp need
+ * the ghost layers that BC_NO_GHOST removes).  After the level-0 stream the
+ * boundary-shell cells of the West and East faces pull what their
+ * neighbours hold, as fluid cells do (a missing source keeps f), and
+ * complete the populations that would come from outside the box:
+ *   West: the velocity inlet of BC/ZouHe_Velocity.cpp:170-199 (Zou-He with
+ *   the Hecht-Harting transverse corrections; the East formulas there, the
+ *   West ones at :81-93): rho from the known populations, the normal one
+ *   from its opposite plus rho U_x / 3, the four diagonal ones with the
+ *   transverse corrections N_y, N_z;
+ *   East: the outflow of BC/Outflow.cpp:39-52, the five incoming populations
+ *   copied from the inner neighbour's streamed ones.
+ * The formulas are written for a textbook (push-along-e) stream; with the
+ * reference's reversed pull they act on g_k = f_inv(k) and the velocity
+ * -u_bc (the same scheme mirrored), which keeps the inflow mass balance
+ * consistent with the stream direction.  The completed cells then collide
+ * (LBGK, level-0 tau) so that the fluid pulls post-collision populations
+ * from them as from any other cell. */
+static const int HH_IN_E[5] = {2, 8, 10, 12, 14};
+
+static int phase_bc_hh(oc_case *c)
+{
+    oc_level *lv = &c->lv[0];
+    const int64_t n = lv->n;
+    const int tb = c->stream_conv != 0;
+    const double sgn = tb ? 1.0 : -1.0;
+    const double Ux = sgn * c->face_u[0][0], Uy = sgn * c->face_u[0][1], Uz = sgn * c->face_u[0][2];
+    for (int face = 0; face < 2; ++face) {
+        for (int64_t j = 0; j < lv->nbc[face]; ++j) {
+            int64_t i = lv->bclist[face][j];
+            double g[19];
+            for (int k = 0; k < 19; ++k) {
+                int m = tb ? k : INV[k];
+                int64_t src = m == 0 ? i : pull_src(c, lv, 0, i, m);
+                g[k] = src >= 0 ? lv->fcol[m * n + src] : lv->f[m * n + i];
+            }
+            if (face == 0) {
+                double rho = (g[0] + g[3] + g[4] + g[5] + g[6] + g[15] + g[16] + g[17] + g[18] +
+                              2.0 * (g[2] + g[8] + g[10] + g[12] + g[14])) / (1.0 - Ux);
+                double ny = 0.5 * (g[3] + g[15] + g[17] - g[4] - g[16] - g[18]) - rho * Uy / 3.0;
+                double nz = 0.5 * (g[5] + g[15] + g[18] - g[6] - g[16] - g[17]) - rho * Uz / 3.0;
+                g[1] = g[2] + rho * Ux / 3.0;
+                g[7] = g[8] + rho * (Ux + Uy) / 6.0 - ny;
+                g[9] = g[10] + rho * (Ux - Uy) / 6.0 + ny;
+                g[11] = g[12] + rho * (Ux + Uz) / 6.0 - nz;
+                g[13] = g[14] + rho * (Ux - Uz) / 6.0 + nz;
+            } else {
+                int64_t nb = find_idx(lv, find_neighbor(c, lv->key[i], 0, -1, 0, 0));
+                if (nb < 0) return -6;
+                for (int t = 0; t < 5; ++t) {
+                    int k = HH_IN_E[t];
+                    int m = tb ? k : INV[k];
+                    g[k] = lv->f[m * n + nb];
+                }
+            }
+            for (int k = 0; k < 19; ++k) lv->f[(tb ? k : INV[k]) * n + i] = g[k];
+        }
+    }
+    double feq[27], rho, u[3];
+    const double tau0 = c->tau[0];
+    for (int face = 0; face < 2; ++face)
+        for (int64_t j = 0; j < lv->nbc[face]; ++j) {
+            int64_t i = lv->bclist[face][j];
+            double d[27];
+            for (int k = 0; k < 19; ++k) d[k] = lv->f[k * n + i];
+            macros_of(19, d, &rho, u);
+            feq_bgk(19, rho, u, feq);
+            for (int k = 0; k < 19; ++k) {
+                double fk = d[k];
+                lv->fcol[k * n + i] = fk - (fk - feq[k]) / tau0;
+            }
+        }
+    return 0;
+}
+
+/* MT_ITIME_HOLD of the device path (no reference counterpart): a fine level
+ * explodes from its parent in both substeps, not only in the first
+ * (LBM_Simulator.cpp:47-51,122-125). */
+int oc_set_interface_time(void *h, int hold)
+{
+    ((oc_case *)h)->itime_hold = hold ? 1 : 0;
+    return 0;
+}
+
 /* Velocity of one face strategy (the input_v of
  * nonEquilibrumExtrapolation_<face>, NonEquilibrumExtrapolation.hpp:37-100)
  * and the face's boundary cells reset to f = fcol = feq(rho0, u) as
@@ -1178,12 +1265,14 @@ static int lbm_kernel(oc_case *c, int l)
             if ((rc = phase_bc_inout(c))) return rc;
         if (l < L)
             if ((rc = lbm_kernel(c, l + 1))) return rc;
-        if (sub == 0 && l > 0)
+        if ((sub == 0 || c->itime_hold) && l > 0)
             if ((rc = phase_explosion(c, l))) return rc;
         phase_stream(c, l);
         if (l == 0) {
             if (c->bc_mode == BC_NEQ)
                 if ((rc = phase_bc_neq(c))) return rc;
+            if (c->bc_mode == BC_ZOUHE_HH)
+                if ((rc = phase_bc_hh(c))) return rc;
         } else if (l == L) {
             phase_ib(c);
         }

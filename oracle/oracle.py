@@ -45,6 +45,7 @@ def lib():
         L.oc_neighbor_keys.argtypes = [vp, i32, u64p, i64, u64p]
         L.oc_collide_cell.argtypes = [i32, i32, dp, C.c_double, dp, C.c_double, dp]
         L.oc_set_face_velocity.argtypes = [vp, i32, dp]
+        L.oc_set_interface_time.argtypes = [vp, i32]
         L.oc_set_markers.argtypes = [vp, i64, dp, dp, dp, i64, dp]
         _lib = L
     return _lib
@@ -111,6 +112,10 @@ class OracleCase:
         if getattr(self, "h", None):
             lib().oc_case_free(self.h)
             self.h = None
+
+    def set_interface_time(self, mode):
+        """"reference" (explosion in the first substep) or "hold" (both substeps)."""
+        lib().oc_set_interface_time(self.h, {"reference": 0, "hold": 1}[mode])
 
     def size(self, l):
         return int(lib().oc_level_size(self.h, l))
@@ -238,18 +243,69 @@ def run_harness(case, nsteps, init=None, timeout=600, nwarm=0):
             return parse_harness_output(fh.read(), q, L, nsteps)
 
 
-def start_harness(case, nsteps, workdir, tag, nwarm=0):
-    """Launch one harness process without waiting (CPU baseline runs several
-    in parallel, one per core); returns (Popen, output path)."""
+def run_harness_trace(case, dumps, init=None, timeout=7200):
+    """Run the reference's step on `case` and return its full state after
+    each coarse-step count in `dumps` (ascending), plus the per-step force
+    series and tau.  Periodic axes of the mesh use the harness built with
+    the find_neighbor wrap (oracle/build.py)."""
     import build
     q, L = case.params.q, case.mesh.spec.max_level
-    exe = build.harness_path(q, L)
+    per = [int(b == "periodic") for b in case.mesh.spec.boundary]
+    exe = build.build_refharness(q, L, periodic=any(per))
+    dumps = [int(d) for d in dumps]
+    if dumps != sorted(dumps) or not dumps or dumps[0] < 0:
+        raise ValueError("dump steps must be ascending and non-negative")
+    tail = struct.pack("<i", len(dumps)) + struct.pack(f"<{len(dumps)}i", *dumps)
+    tail += struct.pack("<3i", *per) + struct.pack("<3i", *[int(n) for n in case.mesh.spec.coarse])
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as fh:
+            fh.write(harness_input(case, dumps[-1], init) + tail)
+        subprocess.run([exe, "trace", fin, fout], check=True, timeout=timeout)
+        with open(fout, "rb") as fh:
+            data = fh.read()
+    off = 0
+    states = []
+    dt = np.dtype([("k", "<u8"), ("v", "<f8", (2 * q + 4,))])
+    for _ in dumps:
+        levels = []
+        for _ in range(L + 1):
+            n = struct.unpack_from("<q", data, off)[0]
+            off += 8
+            rec = np.frombuffer(data, dt, n, off)
+            off += n * dt.itemsize
+            v = rec["v"]
+            levels.append(dict(keys=rec["k"].copy(), f=np.ascontiguousarray(v[:, :q].T),
+                               fcol=np.ascontiguousarray(v[:, q:2 * q].T), rho=v[:, 2 * q].copy(),
+                               u=np.ascontiguousarray(v[:, 2 * q + 1:2 * q + 4].T)))
+        states.append(levels)
+    secs = struct.unpack_from("<d", data, off)[0]
+    off += 8
+    nf = struct.unpack_from("<q", data, off)[0]
+    off += 8
+    force = np.frombuffer(data, "<f8", nf, off).reshape(-1, 4).copy()
+    off += nf * 8
+    tau = np.frombuffer(data, "<f8", L + 1, off).copy()
+    return dict(seconds=secs, states=states, force=force, tau=tau, dumps=dumps)
+
+
+def start_harness(case, nsteps, workdir, tag, nwarm=0, init=None):
+    """Launch one harness process without waiting (CPU baseline runs several
+    in parallel, one per core); returns (Popen, output path).  A mesh with
+    periodic axes runs the harness built with the find_neighbor wrap."""
+    import build
+    q, L = case.params.q, case.mesh.spec.max_level
+    per = [int(b == "periodic") for b in case.mesh.spec.boundary]
+    exe = build.harness_path(q, L, any(per))
     if not os.path.exists(exe):
-        exe = build.build_refharness(q, L)
+        exe = build.build_refharness(q, L, periodic=any(per))
     fin, fout = os.path.join(workdir, f"in{tag}.bin"), os.path.join(workdir, f"out{tag}.bin")
+    data = harness_input(case, nsteps, init, nwarm)
+    if any(per):
+        data += struct.pack("<3i", *per) + struct.pack("<3i", *[int(n) for n in case.mesh.spec.coarse])
     with open(fin, "wb") as fh:
-        fh.write(harness_input(case, nsteps, None, nwarm))
-    return subprocess.Popen([exe, "step", fin, fout]), fout
+        fh.write(data)
+    return subprocess.Popen([exe, "pstep" if any(per) else "step", fin, fout]), fout
 
 
 def run_harness_morton(q, L, levels, keys, timeout=120):

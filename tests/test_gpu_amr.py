@@ -379,3 +379,60 @@ def test_direct_forcing_reduced_storage(ctx, storage):
     assert err < TOL_AMR[storage], err
     fa, fb = a.force(), b.force()
     assert abs(fb[0] - fa[0]) / abs(fa[0]) < 10 * TOL_AMR[storage], (fa, fb)
+
+
+@pytest.mark.parametrize("conv", ["reference", "textbook"])
+@pytest.mark.parametrize("steps", [1, 7])
+def test_zouhe_hh_matches_oracle(ctx, conv, steps):
+    """Zou-He / Hecht-Harting inlet and five-population outflow (restated,
+    unpinned): GPU vs oracle bit-exact, wall cells included."""
+    case = _cfg1_small(bc_mode="zouhe_hh", stream_convention=conv)
+    mgr = _device_case(ctx, case, None)
+    mgr.fluidSimulate(steps)
+    ctx.synchronize()
+    oc = run_oracle(case, steps)
+    for l in range(2):
+        f, fcol = mgr.populations(l)
+        g = oc.get(l)
+        assert np.array_equal(f, g["f"]) and np.array_equal(fcol, g["fcol"]), (l, float(np.abs(f - g["f"]).max()))
+    assert rel_err(mgr.force()[:3], oc.force()[:3]) < 1e-12
+
+
+def test_zouhe_hh_runs_under_the_phase_schedule_only(ctx):
+    from mortontrie_amr_b200.lbm import LBM_Manager, MTError
+    mgr = LBM_Manager(ctx, _cfg1_small(bc_mode="zouhe_hh"))
+    with pytest.raises(MTError, match="MT_ERR_ARG"):
+        mgr.set_schedule("fused")
+    mgr.close()
+
+
+@pytest.mark.parametrize("schedule", ["phases", "fused"])
+def test_interface_hold_matches_oracle(ctx, schedule):
+    """Explosion in both substeps (interface_time "hold", no reference
+    counterpart): GPU FP64 under both schedules vs the oracle, bit-exact."""
+    from golden_cases import TRACE_CASES, build_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    import oracle as O
+    spec = TRACE_CASES["nested_q19_dw_l3"]
+    case = build_case(spec)
+    init = init_of(case, spec)
+    mgr = LBM_Manager(ctx, case, schedule=schedule, interface_time="hold")
+    for l, (_, f) in enumerate(init):
+        mgr.set_populations(l, f)
+    oc = O.OracleCase(case)
+    oc.set_interface_time("hold")
+    for l, (_, f) in enumerate(init):
+        oc.set_populations(l, f)
+    mgr.fluidSimulate(3)
+    oc.step(3)
+    ctx.synchronize()
+    for l in range(case.max_level + 1):
+        f, fcol = mgr.populations(l)
+        g = oc.get(l)
+        keep = (g["tags"] & TAG_BC) == 0
+        assert np.array_equal(f[:, keep], g["f"][:, keep]), l
+        assert np.array_equal(fcol, g["fcol"]), l
+    ref = oc.get(1)["f"]
+    oc2 = run_oracle(case, 3, init)
+    assert not np.array_equal(oc2.get(1)["f"], ref)   # the option changes the run
+    mgr.close()

@@ -82,3 +82,32 @@ def test_markers_and_async_force(ctx):
         ctx.marker()
     assert ctx.marker_done(first)
     mgr.close()
+
+
+def test_async_guard_flags_nonfinite_state(ctx):
+    """The guard enqueued with the force copy: a healthy state reads finite;
+    a state given a NaN population on the host (the failure is made on the
+    host, no kernel is driven into a fault) reads non-finite under the next
+    marker."""
+    import time
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    from mortontrie_amr_b200.serving import Request, TemplateCache, request_case
+    req = Request(rid=0, arrival=0.0, radius=3.3, levels=1, re=80.0, oscillating=False, finest_steps=32)
+    mgr = LBM_Manager(ctx, request_case(req, TemplateCache().get(req)), "f16", schedule="fused")
+
+    def guard_after_marker():
+        mgr.force_async()
+        tk = ctx.marker()
+        t0 = time.time()
+        while not ctx.marker_done(tk):
+            assert time.time() - t0 < 60.0
+            time.sleep(0.001)
+        return mgr.finite_copied()
+
+    mgr.fluidSimulate(4)
+    assert guard_after_marker()
+    f, fcol = mgr.populations(1)
+    fcol[5, fcol.shape[1] // 2] = np.nan
+    mgr.set_populations(1, f, fcol)
+    assert not guard_after_marker()
+    mgr.close()

@@ -78,3 +78,16 @@ def test_estimated_cells_bound_the_host_mesh():
         got = case.mesh.n_cells()
         assert all(e >= g for e, g in zip(est, got)), (est, got)
         assert sum(est) <= 1.3 * sum(got), (est, got)
+
+
+def test_summary_counts_finite_results_only():
+    """cases/h, p50 and p99 of the request loop count finite results; a
+    request whose state diverged (guard) or whose drag is NaN is failed."""
+    from mortontrie_amr_b200.serving import Result, ServerStats
+    rs = [Result(rid=0, arrival=0, admitted=0, finished=1, cd=1.0, cl=0, coarse_steps=1, storage="f16"),
+          Result(rid=1, arrival=0, admitted=0, finished=2, cd=1.0, cl=0, coarse_steps=1, storage="f16",
+                 finite=False),
+          Result(rid=2, arrival=0, admitted=0, finished=9, cd=float("nan"), cl=0, coarse_steps=1, storage="f16")]
+    s = ServerStats(results=rs, wall_s=3600.0).summary()
+    assert s["completed"] == 3 and s["finite"] == 1 and s["failed"] == 2
+    assert s["cases_per_hour"] == 1.0 and s["p99_s"] == 1.0

@@ -46,6 +46,32 @@ def _reduce(ctx, d):
     return np.array([r["mass"], *r["momentum"], r["kinetic_energy"]])
 
 
+class _PoolWatch:
+    """High-water mark of the device's default memory pool, which every
+    stream-ordered allocation of the library draws from: reset before a
+    stretch of calls, read after it."""
+
+    def __init__(self, device=0):
+        from cuda.bindings import runtime as rt
+        self.rt = rt
+        err, self.pool = rt.cudaDeviceGetDefaultMemPool(device)
+        assert err == rt.cudaError_t.cudaSuccess, err
+
+    def _get(self, attr):
+        err, v = self.rt.cudaMemPoolGetAttribute(self.pool, attr)
+        assert err == self.rt.cudaError_t.cudaSuccess, err
+        return int(v)
+
+    def reset(self):
+        A = self.rt.cudaMemPoolAttr
+        err, = self.rt.cudaMemPoolSetAttribute(self.pool, A.cudaMemPoolAttrUsedMemHigh, self.rt.cuuint64_t(0))
+        assert err == self.rt.cudaError_t.cudaSuccess, err
+        return self._get(A.cudaMemPoolAttrUsedMemCurrent)
+
+    def high(self):
+        return self._get(self.rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh)
+
+
 @pytest.mark.parametrize("n,q,collision,storage", [
     (32, 19, "LBGK", "f64"),
     (64, 19, "LBGK", "f16"),
@@ -54,25 +80,28 @@ def _reduce(ctx, d):
 ])
 def test_noalloc_matches_reduce_twice(ctx, n, q, collision, storage):
     """Two calls in a row after some steps equal the allocating entry point
-    (same kernels, same summation order: identical up to rounding, tested at
-    1e-12 relative on the mass and 1e-12 of the mass on the other sums)."""
+    bit for bit (same kernels, same grid, same summation order), and the
+    pair of calls takes nothing from the device's memory pool."""
     d = _dense_tgv(ctx, n, q, collision, storage)
     d.step(7)
     ref = _reduce(ctx, d)
+    ctx.synchronize()
+    pool = _PoolWatch(0)
+    used = pool.reset()
     launches0 = ctx.launch_count()
     a = _reduce_noalloc(ctx, d)
     b = _reduce_noalloc(ctx, d)
     assert ctx.launch_count() - launches0 == 4
-    scale = abs(ref[0])
+    assert pool.high() == used, "the allocation-free reduction drew memory from the pool"
     for got in (a, b):
         assert np.all(np.isfinite(got))
-        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * scale)
+        np.testing.assert_array_equal(got, ref)
     # the state moves on; the next pair of calls follows it
     d.step(3)
     ref2 = _reduce(ctx, d)
     assert not np.array_equal(ref2[4], ref[4])
-    np.testing.assert_allclose(_reduce_noalloc(ctx, d), ref2, rtol=1e-12, atol=1e-12 * scale)
-    np.testing.assert_allclose(_reduce_noalloc(ctx, d), ref2, rtol=1e-12, atol=1e-12 * scale)
+    np.testing.assert_array_equal(_reduce_noalloc(ctx, d), ref2)
+    np.testing.assert_array_equal(_reduce_noalloc(ctx, d), ref2)
     d.close()
 
 
@@ -90,6 +119,5 @@ def test_noalloc_rejects_cases_beyond_scratch(ctx):
     big.close()
     small = _dense_tgv(ctx, 128, 19, "LBGK", "f16")
     assert small.n == 2 * 1024 * 1024
-    np.testing.assert_allclose(_reduce_noalloc(ctx, small), _reduce(ctx, small), rtol=1e-12,
-                               atol=1e-12 * small.n)
+    np.testing.assert_array_equal(_reduce_noalloc(ctx, small), _reduce(ctx, small))
     small.close()
