@@ -747,32 +747,42 @@ def amr_accuracy(ctx, torch, steps=2500, case_name="cfg3", scaling="reference", 
     return out
 
 
+REF_EDGE = 64
+
+
 def _reference_sample_case():
-    """Bounded CPU sample of the workload for the reference's own code: a
-    48^3 single populated level (the reference needs a second, empty level
-    and has no periodic wrap, so the box is closed by its non-equilibrium
-    extrapolation boundary), D3Q19 LBGK, tau 0.6."""
-    from mortontrie_amr_b200.case import uniform_box_case
-    return uniform_box_case(q=Q, n=(48, 48, 48), nu=NU, boundary=("bc", "bc", "bc"), empty_levels=1,
-                            u_bc=(U0, 0.0, 0.0), u_ref=U0)
+    """Bounded CPU sample of the workload for the reference's own code: the
+    same periodic Taylor-Green D3Q19 LBGK step (tau 0.6, u0 0.02, wavenumber
+    2 pi / edge) on a 64^3 box instead of 256^3 (the reference's hash maps
+    hold about 2 KB per cell); the reference needs a second, empty level, and
+    its periodic wrap is the harness's find_neighbor wrap."""
+    from mortontrie_amr_b200.case import equilibrium, taylor_green_fields, uniform_box_case
+    from mortontrie_amr_b200.lbm import morton_order_fields
+    n = REF_EDGE
+    case = uniform_box_case(q=Q, n=(n, n, n), nu=NU, boundary=("periodic",) * 3, empty_levels=1, u_ref=U0)
+    fields = morton_order_fields(n, *taylor_green_fields((n, n, n), U0))
+    f0 = equilibrium(Q, *fields)
+    keys0 = case.mesh.all_keys(0)
+    init = [(keys0, f0), (case.mesh.all_keys(1), np.zeros((Q, 0)))]
+    return case, init
 
 
 def cpu_reference_run(nprocs, steps, warmup):
     """Run `nprocs` single-threaded reference harness processes at once (one
-    per core, the reference has no threading); returns (MLUPS, kind, cores,
-    sample)."""
+    per core, the reference has no threading); returns (MLUPS of all
+    processes, kind, cores, sample)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    case = _reference_sample_case()
+    case, init = _reference_sample_case()
     n_fluid = int(case.mesh.levels[0]["lat_f"].size)
     try:
         import oracle as O
         import build as B
-        have_ref = os.path.exists(B.harness_path(Q, 1)) or os.path.isdir(B.REF)
+        have_ref = os.path.exists(B.harness_path(Q, 1, True)) or os.path.isdir(B.REF)
     except Exception:
         have_ref = False
     if have_ref:
         with tempfile.TemporaryDirectory() as td:
-            procs = [O.start_harness(case, steps, td, i, nwarm=warmup) for i in range(nprocs)]
+            procs = [O.start_harness(case, steps, td, i, nwarm=warmup, init=init) for i in range(nprocs)]
             secs = []
             for p, out in procs:
                 p.wait(timeout=3600)
@@ -785,19 +795,21 @@ def cpu_reference_run(nprocs, steps, warmup):
     else:
         import oracle as O
         oc = O.OracleCase(case)
+        oc.set_populations(0, init[0][1])
         oc.step(warmup)
         t = time.perf_counter()
         oc.step(steps)
         mlups = n_fluid * steps / (time.perf_counter() - t) / 1e6
         kind, nprocs = "port", 1
-    sample = (f"{nprocs} process(es) x {steps} steps of a 48^3 D3Q19 LBGK box ({n_fluid} stepped cells each), "
-              f"hash-map backend, 1 thread per process")
+    sample = (f"{nprocs} process(es) x {steps} timed steps of a {REF_EDGE}^3 periodic Taylor-Green D3Q19 LBGK box "
+              f"({n_fluid} cells each, tau 0.6), hash-map backend, 1 thread per process")
     return mlups, kind, nprocs, sample
 
 
 def cpu_baseline_sample():
-    mlups, kind, cores, sample = cpu_reference_run(1, 12, 1)
-    return {"value": round(mlups, 4), "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample}
+    mlups, kind, cores, sample = cpu_reference_run(1, 10, 1)
+    return {"value": round(mlups, 4), "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample,
+            "per_core": round(mlups / cores, 4)}
 
 
 def run_reference(args):
@@ -806,14 +818,15 @@ def run_reference(args):
     if rank != 0:
         return
     nprocs = max(1, min(os.cpu_count() or 1, 32))
-    # each bench step is one time step of every sample process
-    mlups, kind, cores, sample = cpu_reference_run(nprocs, max(1, args.steps // 25), max(0, min(args.warmup, 2)))
+    # each process times at least 10 steps (at most 20) of its box
+    mlups, kind, cores, sample = cpu_reference_run(nprocs, max(10, min(args.steps, 20)), max(0, min(args.warmup, 2)))
     line = {
         "impl": "reference", "metric": "fine-level MLUPS (uniform case), %HBM roofline", "value": round(mlups, 4),
         "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "sample": sample},
-        "cpu_baseline": {"value": round(mlups, 4), "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample},
+        "cpu_baseline": {"value": round(mlups, 4), "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample,
+                         "per_core": round(mlups / cores, 4)},
         "e2e": {"value": round(mlups, 4), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -260,6 +260,16 @@ int mt_case_status(mt_ctx *ctx, int32_t case_id);
  * candidate the kernel is built for (the paired 16-bit LBGK kernel: 128 and
  * 256 only; the other slots are left unwritten). */
 int mt_case_tune(mt_ctx *ctx, int32_t case_id, int32_t *best_block, float *ms_per_candidate);
+/* Project autotuner of the multi-level fused brick pass (no reference
+ * counterpart): times each brick level's pass in both of its forms (one cell
+ * per lane step, or two cells per lane with packed FP32 pair arithmetic;
+ * FP64 has only the first) on the case's own bricks, without changing the
+ * state, and keeps the faster per level for the fused steps that follow.
+ * variant[max_level + 1]: the form kept (0 / 1, -1 for a level without
+ * bricks); ms[2 * (max_level + 1)]: ms per launch of each form (-1 if not
+ * timed).  Either may be NULL.  Synchronises the stream; the case keeps its
+ * schedule. */
+int mt_case_tune_bricks(mt_ctx *ctx, int32_t case_id, int32_t *variant, float *ms);
 /* Schedule of mt_step for a multi-level case (no reference counterpart):
  * MT_SCHED_PHASES (default) issues the reference's phases one pass each;
  * MT_SCHED_FUSED keeps a second post-collision buffer per level and streams

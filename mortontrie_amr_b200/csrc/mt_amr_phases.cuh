@@ -890,9 +890,9 @@ __device__ __forceinline__ void brick_warp_pair(int64_t b, int lane, int32_t *s_
     }
 }
 
-// brick_warp for every storage: the pair form for the reduced storages
-// (MT_BRICK_SCALAR keeps the one-cell-at-a-time form for them too)
-template <int Q, class S, int COLL>
+// brick_warp for every storage: V = 1 the pair form (reduced storages), V = 0
+// the one-cell-at-a-time form
+template <int Q, class S, int COLL, int V>
 __device__ __forceinline__ void brick_warp_any(int64_t b, int lane, int32_t *s_idx, const int32_t *__restrict__ halo,
                                                const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
                                                const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext,
@@ -900,12 +900,10 @@ __device__ __forceinline__ void brick_warp_any(int64_t b, int lane, int32_t *s_i
                                                typename Store<S>::C *__restrict__ u, int macros, int fall,
                                                long long *__restrict__ acc, const Shift &sh)
 {
-#ifndef MT_BRICK_SCALAR
-    if constexpr (Store<S>::shifted && (COLL == MT_COLL_LBGK || Q == 27))
+    if constexpr (V == 1 && Store<S>::shifted && (COLL == MT_COLL_LBGK || Q == 27))
         brick_warp_pair<Q, S, COLL>(b, lane, s_idx, halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros,
                                     fall, acc, sh);
     else
-#endif
         brick_warp<Q, S, COLL>(b, lane, s_idx, halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros, fall,
                                acc, sh);
 }
@@ -919,18 +917,19 @@ __device__ __forceinline__ void brick_warp_any(int64_t b, int lane, int32_t *s_i
 #ifndef MT_BRICK_PAIR_MIN_BLOCKS
 #define MT_BRICK_PAIR_MIN_BLOCKS 4  // the pair passes of every reduced storage (128 registers)
 #endif
-// resident blocks per SM asked of a brick pass
-template <int Q, class S, int COLL> constexpr int brick_min_blocks()
+// resident blocks per SM asked of a brick pass (V: one cell or a pair per step)
+template <int Q, class S, int COLL, int V> constexpr int brick_min_blocks()
 {
-#ifndef MT_BRICK_SCALAR
-    if (Store<S>::shifted) return MT_BRICK_PAIR_MIN_BLOCKS;
-#endif
+    if (V == 1 && Store<S>::shifted) return MT_BRICK_PAIR_MIN_BLOCKS;
     if (Store<S>::bytes == 2) return (COLL == MT_COLL_LBGK && Q == 19) ? MT_BRICK_MIN_BLOCKS_Q19_LBGK : MT_BRICK_MIN_BLOCKS;
     return 1;
 }
+// the form a level runs until mt_case_tune_bricks times both: pairs for every
+// reduced storage (FP64 has only the one-cell form)
+template <class S> constexpr int brick_default_variant() { return Store<S>::shifted ? 1 : 0; }
 
-template <int Q, class S, int COLL>
-__global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL>()) k_brick_step(
+template <int Q, class S, int COLL, int V>
+__global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL, V>()) k_brick_step(
     int64_t nb, const int32_t *__restrict__ halo, const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
     const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext, double tau,
     typename Store<S>::C *__restrict__ rho, typename Store<S>::C *__restrict__ u, int macros, int fall,
@@ -940,16 +939,16 @@ __global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL>()) k_brick_s
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t b = 4 * (int64_t)blockIdx.x + w;
     if (b >= nb) return;
-    brick_warp_any<Q, S, COLL>(b, lane, s_idx[w], halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros, fall,
-                               acc, sh);
+    brick_warp_any<Q, S, COLL, V>(b, lane, s_idx[w], halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros,
+                                  fall, acc, sh);
 }
 
 // The same pass over the bricks of many cases (a batch): brick b of the work
 // list belongs to the slot whose [off[s], off[s + 1]) range holds it; each
 // slot carries one case level's tables, buffers and relaxation time.
-template <int Q, class S, int COLL>
-__global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL>()) k_brick_step_batch(const BrickBatch *__restrict__ bb,
-                                                                                          const Shift sh)
+template <int Q, class S, int COLL, int V>
+__global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL, V>()) k_brick_step_batch(const BrickBatch *__restrict__ bb,
+                                                                                             const Shift sh)
 {
     __shared__ int32_t s_idx[4][216];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -965,7 +964,7 @@ __global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL>()) k_brick_s
     }
     const BrickSlot &sl = bb->slot[lo];
     using C = typename Store<S>::C;
-    brick_warp_any<Q, S, COLL>(b - bb->off[lo], lane, s_idx[w], sl.halo, sl.cls, sl.n, sl.textbook,
+    brick_warp_any<Q, S, COLL, V>(b - bb->off[lo], lane, s_idx[w], sl.halo, sl.cls, sl.n, sl.textbook,
                                (const S *)sl.fcol, (S *)sl.f, (S *)sl.fnext, sl.tau, (C *)sl.rho, (C *)sl.u, sl.macros,
                                sl.fall, sl.acc, sh);
 }
@@ -1494,6 +1493,37 @@ int band_collide(Ctx &ctx, Case &c, int l, void *out)
     return MT_OK;
 }
 
+// One fused brick pass of level l in the form `variant` (0 one cell, 1 a
+// pair per lane step; reduced storages only have a pair form) on stream s,
+// writing the next collision into fnext.
+template <int Q, class S>
+void brick_launch(Case &c, int l, int variant, cudaStream_t s, S *fnext, int mac, int fall, long long *bacc)
+{
+    using A = AmrTyped<S>;
+    Level &lv = c.lv[l];
+    const unsigned g = grid_for(lv.nbrick, 4);
+    const uint32_t n32 = (uint32_t)lv.n;
+    const int tb = c.d.stream_convention;
+    auto go = [&](auto coll, auto v) {
+        constexpr int COLL = decltype(coll)::value, V = decltype(v)::value;
+        k_brick_step<Q, S, COLL, V><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb, A::fcol(lv), A::f(lv),
+                                                      fnext, c.d.tau[l], A::rho(lv), A::u(lv), mac, fall,
+                                                      COLL == MT_COLL_LBGK ? bacc : nullptr, c.shift[l]);
+    };
+    using LB = std::integral_constant<int, MT_COLL_LBGK>;
+    using CU = std::integral_constant<int, MT_COLL_CUMULANT>;
+    using V0 = std::integral_constant<int, 0>;
+    using V1 = std::integral_constant<int, 1>;
+    const bool pair = Store<S>::shifted && variant == 1;
+    if (c.d.collision == MT_COLL_LBGK) {
+        if (pair) go(LB{}, V1{}); else go(LB{}, V0{});
+    } else {
+        if constexpr (Q == 27) {
+            if (pair) go(CU{}, V1{}); else go(CU{}, V0{});
+        }
+    }
+}
+
 template <class S, int Q>
 int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
 {
@@ -1801,21 +1831,9 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
         if (c.pull_mode == 1) {
             // the batch runs this level's bricks
         } else if (lv.bricks) {
-            const unsigned g = grid_for(lv.nbrick, 4);
-            const uint32_t n32 = (uint32_t)n;
             // the band's macros come out of the pass (the direct-forcing step skips k_band_macros)
             long long *bacc = (l == L && lv.nband) ? c.acc : nullptr;
-            if (c.d.collision == MT_COLL_LBGK) {
-                k_brick_step<Q, S, MT_COLL_LBGK><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb, A::fcol(lv),
-                                                                   A::f(lv), (S *)lv.fcol_alt, c.d.tau[l],
-                                                                   A::rho(lv), A::u(lv), mac, fall, bacc, c.shift[l]);
-            } else {
-                if constexpr (Q == 27)
-                    k_brick_step<Q, S, MT_COLL_CUMULANT><<<g, 128, 0, s>>>(lv.nbrick, lv.bhalo, lv.bcls, n32, tb,
-                                                                           A::fcol(lv), A::f(lv), (S *)lv.fcol_alt,
-                                                                           c.d.tau[l], A::rho(lv), A::u(lv), mac,
-                                                                           fall, nullptr, c.shift[l]);
-            }
+            brick_launch<Q, S>(c, l, lv.brick_variant, s, (S *)lv.fcol_alt, mac, fall, bacc);
             MT_LAUNCHED(ctx);
         } else {
             if (lv.nfused) {
@@ -1874,6 +1892,7 @@ int AmrOps<S>::alloc(Ctx &ctx, Case &c, int l)
         int rc = upload_bdry_tables(ctx);
         if (rc) return rc;
     }
+    lv.brick_variant = brick_default_variant<S>();
     MT_CUDA(ctx, cudaMallocAsync(&lv.f, sizeof(S) * n * Q, ctx.stream));
     MT_CUDA(ctx, cudaMallocAsync(&lv.fcol, sizeof(S) * n * Q, ctx.stream));
     MT_CUDA(ctx, cudaMallocAsync(&lv.rho, sizeof(C) * n, ctx.stream));
@@ -1949,14 +1968,82 @@ int AmrOps<S>::batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, i
 {
     const unsigned g = grid_for(total, 4);
     if (!g) return MT_OK;
+    constexpr int V = brick_default_variant<S>();
     if (q == 19)
-        k_brick_step_batch<19, S, MT_COLL_LBGK><<<g, 128, 0, ctx.stream>>>(d_desc, sh);
+        k_brick_step_batch<19, S, MT_COLL_LBGK, V><<<g, 128, 0, ctx.stream>>>(d_desc, sh);
     else if (coll == MT_COLL_LBGK)
-        k_brick_step_batch<27, S, MT_COLL_LBGK><<<g, 128, 0, ctx.stream>>>(d_desc, sh);
+        k_brick_step_batch<27, S, MT_COLL_LBGK, V><<<g, 128, 0, ctx.stream>>>(d_desc, sh);
     else
-        k_brick_step_batch<27, S, MT_COLL_CUMULANT><<<g, 128, 0, ctx.stream>>>(d_desc, sh);
+        k_brick_step_batch<27, S, MT_COLL_CUMULANT, V><<<g, 128, 0, ctx.stream>>>(d_desc, sh);
     MT_LAUNCHED(ctx);
     return MT_OK;
+}
+
+// ---- the brick pass autotuner (mt_case_tune_bricks) ----------------------
+// Each brick level's fused pass is timed in both forms (one cell per lane
+// step, or two cells with packed FP32 pairs; FP64 has only the first) on the
+// case's own bricks: one warm-up and three timed launches per form, CUDA
+// events on the case's stream.  The passes read the current post-collision
+// buffer and write the next collision into a scratch buffer; the f they
+// store is what the last real pass stored, and no macros are written, so the
+// state is untouched.  The faster form is kept for the level.
+template <class S>
+int AmrOps<S>::tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms)
+{
+    int64_t nmax = 0;
+    for (int l = 0; l <= c.d.max_level; ++l)
+        if (c.lv[l].bricks) nmax = std::max(nmax, c.lv[l].n);
+    for (int l = 0; l <= c.d.max_level; ++l) {
+        if (variant) variant[l] = -1;
+        if (ms) ms[2 * l] = ms[2 * l + 1] = -1.f;
+    }
+    if (!nmax) return MT_OK;
+    S *scratch = nullptr;
+    MT_CUDA(ctx, cudaMallocAsync(&scratch, sizeof(S) * (size_t)c.d.q * (size_t)nmax, ctx.stream));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = MT_OK;
+    for (int l = 0; l <= c.d.max_level && !rc; ++l) {
+        Level &lv = c.lv[l];
+        if (!lv.bricks || !lv.nbrick) continue;
+        const int nform = Store<S>::shifted ? 2 : 1;
+        float best = 0.f;
+        int pick = lv.brick_variant;
+        for (int v = 0; v < nform && !rc; ++v) {
+            auto launch = [&]() {
+                if (c.d.q == 19)
+                    brick_launch<19, S>(c, l, v, ctx.stream, scratch, 0, 0, nullptr);
+                else
+                    brick_launch<27, S>(c, l, v, ctx.stream, scratch, 0, 0, nullptr);
+            };
+            launch();
+            cudaEventRecord(e0, ctx.stream);
+            for (int r = 0; r < 3; ++r) launch();
+            cudaEventRecord(e1, ctx.stream);
+            cudaError_t e = cudaEventSynchronize(e1);
+            if (e == cudaSuccess) e = cudaGetLastError();
+            if (e != cudaSuccess) {
+                rc = set_err(ctx, MT_ERR_CUDA, std::string("brick tuner: ") + cudaGetErrorString(e));
+                break;
+            }
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            t /= 3.f;
+            ctx.launches += 4;
+            if (ms) ms[2 * l + v] = t;
+            if (v == 0 || t < best) {
+                best = t;
+                pick = v;
+            }
+        }
+        lv.brick_variant = pick;
+        if (variant) variant[l] = pick;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeAsync(scratch, ctx.stream);
+    return rc;
 }
 
 // ---- FP64 reductions of a multi-level case (mt_case_reduce_levels) -------

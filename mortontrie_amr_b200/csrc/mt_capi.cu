@@ -1137,6 +1137,35 @@ int mt_case_tune(mt_ctx *h, int32_t id, int32_t *best_block, float *ms_per_candi
     return MT_OK;
 }
 
+int mt_case_tune_bricks(mt_ctx *h, int32_t id, int32_t *variant, float *ms)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || !c->built) return set_err(ctx, MT_ERR_STATE, "the brick tuner needs a built multi-level case");
+    if (c->d.bc_mode == MT_BC_ZOUHE_HH)
+        return set_err(ctx, MT_ERR_ARG, "the Zou-He / Hecht-Harting boundary runs under the phase schedule");
+    const int prev = c->schedule;
+    if (c->schedule != MT_SCHED_FUSED) {
+        // the brick tables are built with the fused schedule
+        if ((rc = mt_case_set_schedule(h, id, MT_SCHED_FUSED))) return rc;
+    }
+    if ((rc = amr_prime(ctx, *c))) return rc;
+    rc = amr_dispatch(*c, [&](auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        return AmrOps<S>::tune_bricks(ctx, *c, variant, ms);
+    });
+    if (rc) return rc;
+    // the captured steps bake the kernel choice in
+    for (int p = 0; p < 2; ++p) {
+        if (c->fgraph[p]) cudaGraphExecDestroy(c->fgraph[p]);
+        c->fgraph[p] = nullptr;
+    }
+    if (prev != MT_SCHED_FUSED) return mt_case_set_schedule(h, id, prev);
+    return MT_OK;
+}
+
 int mt_get_force(mt_ctx *h, int32_t id, double *out4)
 {
     Case *c;

@@ -35,7 +35,7 @@ EXPORTS = [
     "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_reduce_levels", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_interface_time", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
     "mt_case_generate", "mt_case_set_surface", "mt_marker_record", "mt_marker_done", "mt_case_force_async",
-    "mt_case_force_copied", "mt_set_priority", "mt_case_remap", "mt_case_status_copied",
+    "mt_case_force_copied", "mt_set_priority", "mt_case_remap", "mt_case_status_copied", "mt_case_tune_bricks",
 ]
 
 
@@ -121,7 +121,7 @@ def lib():
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
             "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64],
             "mt_marker_record": [vp, i64p], "mt_marker_done": [vp, i64, i32p], "mt_case_force_async": [vp, i32],
-            "mt_case_force_copied": [vp, i32, dp], "mt_case_status_copied": [vp, i32], "mt_set_priority": [vp, i32], "mt_case_remap": [vp, i32, i32, i64p], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_case_force_copied": [vp, i32, dp], "mt_case_status_copied": [vp, i32], "mt_case_tune_bricks": [vp, i32, i32p, C.POINTER(C.c_float)], "mt_set_priority": [vp, i32], "mt_case_remap": [vp, i32, i32, i64p], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -465,6 +465,16 @@ class LBM_Manager:
         out = np.zeros(4)
         self.ctx.check(lib().mt_get_force(self.ctx.h, self.id, _ptr(out, C.c_double)), "get_force")
         return out
+
+    def tune_bricks(self):
+        """Time both forms of every brick level's fused pass (one cell, or a
+        packed pair, per lane step) and keep the faster per level; returns
+        (form per level, -1 without bricks; ms per launch [level][form])."""
+        v = np.zeros(self.L + 1, np.int32)
+        ms = np.zeros((self.L + 1, 2), np.float32)
+        self.ctx.check(lib().mt_case_tune_bricks(self.ctx.h, self.id, _ptr(v, C.c_int32), _ptr(ms, C.c_float)),
+                       "mt_case_tune_bricks")
+        return v, ms
 
     def reduce_levels(self):
         """FP64 device sums per level (rows 0..L) and volume-weighted over all

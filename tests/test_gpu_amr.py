@@ -436,3 +436,33 @@ def test_interface_hold_matches_oracle(ctx, schedule):
     oc2 = run_oracle(case, 3, init)
     assert not np.array_equal(oc2.get(1)["f"], ref)   # the option changes the run
     mgr.close()
+
+
+@pytest.mark.parametrize("storage", ["f16", "f64"])
+def test_brick_tuner_keeps_the_trajectory(ctx, storage):
+    """mt_case_tune_bricks times the brick pass forms on the case itself and
+    leaves the state as it was: a tuned case and an untuned one stay equal
+    (FP64 bit for bit; FP16 within the two forms' rounding)."""
+    from mortontrie_amr_b200.case import nested_sphere_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    case = nested_sphere_case(coarse=(48, 24, 24), center=(16, 12, 12), radius=1.5)
+    a = LBM_Manager(ctx, case, storage, schedule="fused")
+    b = LBM_Manager(ctx, case, storage, schedule="fused")
+    a.fluidSimulate(2)
+    b.fluidSimulate(2)
+    v, ms = a.tune_bricks()
+    assert (v >= 0).any() and (ms.max() > 0)
+    if storage == "f64":
+        assert set(v[v >= 0]) == {0}
+    a.fluidSimulate(3)
+    b.fluidSimulate(3)
+    ctx.synchronize()
+    for l in range(case.max_level + 1):
+        fa, ca = a.populations(l)
+        fb, cb = b.populations(l)
+        if storage == "f64":
+            assert np.array_equal(fa, fb) and np.array_equal(ca, cb), l
+        else:
+            assert rel_err(ca, cb) < 1e-2, l
+    a.close()
+    b.close()
