@@ -72,6 +72,7 @@ extern "C" {
 #define MT_SCALE_STANDARD 1  /* stress-continuous rescaling: fneq_f = tau_f / (2 tau_c) fneq_c and its inverse */
 #define MT_ITIME_REFERENCE 0 /* fine level explodes in its first substep only: LBM_Simulator.cpp:47-51 */
 #define MT_ITIME_HOLD 1      /* in both substeps, from the parent's post-collision state of the coarse step */
+#define MT_ITIME_EXTRAP 2    /* second substep from that state extrapolated to the half step */
 
 /* Case description: the switches the reference hard-codes in
  * LBM_Manager::LBM_Manager (LBM_Manager.cpp:32-95) and its per-level
@@ -292,7 +293,10 @@ int mt_case_set_interface_scaling(mt_ctx *ctx, int32_t case_id, int32_t scaling)
  * MT_ITIME_HOLD explodes in the second substep as well, from the same parent
  * values (the parent has not streamed yet), so the C2F cells of the second
  * substep hold the parent's state instead of populations streamed through
- * the shell without a collision. */
+ * the shell without a collision.  MT_ITIME_EXTRAP explodes the second
+ * substep from 1.5 fcol(t) - 0.5 fcol(t - 1) of the parent cells (t - 1:
+ * the parent's previous step; the current values right after the state or
+ * the option was set), the parent state at the half step to second order. */
 int mt_case_set_interface_time(mt_ctx *ctx, int32_t case_id, int32_t mode);
 /* Velocity of one face strategy (face 0..5 = West East South North Bot Top),
  * the input_v each nonEquilibrumExtrapolation_<face> / inlet strategy is

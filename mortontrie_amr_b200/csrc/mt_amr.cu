@@ -526,7 +526,7 @@ void amr_free(Case &c)
         void *ptrs[] = {lv.key, lv.tag, lv.bcidx, lv.disrow, lv.nbr, lv.f, lv.fcol, lv.rho, lv.u,
                         lv.collide_list, lv.stream_list, lv.iblist, lv.expl_src, lv.expl_child, lv.coal_child,
                         lv.fcol_alt, lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls, lv.bhalo,
-                        lv.band, lv.collide_nb, lv.draw_keys, lv.draw_set};
+                        lv.band, lv.collide_nb, lv.draw_keys, lv.draw_set, lv.expl_prev};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         for (int s = 0; s < kNumSets; ++s)
@@ -586,6 +586,7 @@ int amr_phase(Ctx &ctx, Case &c, int phase, int level)
 
 int amr_init_equilibrium(Ctx &ctx, Case &c, double rho0, const double *u0)
 {
+    c.prev_stale = true;
     return amr_dispatch(c, [&](auto *tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         return AmrOps<S>::init_eq(ctx, c, rho0, u0);
@@ -610,7 +611,8 @@ int amr_lbm_kernel(Ctx &ctx, Case &c, int l)
         if (l == 0 && c.d.bc_mode == MT_BC_ZOUHE_OUTFLOW) RUN(PH_BC_INOUT, 0);
         if (l < L)
             if ((rc = amr_lbm_kernel(ctx, c, l + 1))) return rc;
-        if ((sub == 0 || c.itime == MT_ITIME_HOLD) && l > 0) RUN(PH_EXPLOSION, l);
+        if (l > 0 && sub == 0) RUN(PH_EXPLOSION, l);
+        if (l > 0 && sub == 1 && c.itime != MT_ITIME_REFERENCE) RUN(PH_EXPLOSION_B, l);
         RUN(PH_STREAM, l);
         if (l == 0) {
             if (c.d.bc_mode == MT_BC_NEQ) RUN(PH_BC, 0);
@@ -689,7 +691,8 @@ static int fused_lbm_kernel(Ctx &ctx, Case &c, int l, bool last_parent)
         if (l == 0 && c.d.bc_mode == MT_BC_ZOUHE_OUTFLOW) RUN(PH_BC_INOUT, 0);
         if (l < L)
             if ((rc = fused_lbm_kernel(ctx, c, l + 1, last))) return rc;
-        if ((sub == 0 || c.itime == MT_ITIME_HOLD) && l > 0) RUN(PH_EXPLOSION, l);
+        if (l > 0 && sub == 0) RUN(PH_EXPLOSION, l);
+        if (l > 0 && sub == 1 && c.itime != MT_ITIME_REFERENCE) RUN(PH_EXPLOSION_B, l);
         c.macros_now = last && !(l == 0 && c.d.bc_mode == MT_BC_NEQ);
         RUN(PH_PULL_COLLIDE, l);
         if (l == L && c.lv[l].nband) RUN(PH_DF, l);
@@ -836,9 +839,27 @@ int amr_set_face(Ctx &ctx, Case &c, int face, const double *u)
 }
 
 // n coarse steps replayed from one captured graph (fluidSimulate loop body)
+int amr_prev_sync(Ctx &ctx, Case &c)
+{
+    if (c.itime != MT_ITIME_EXTRAP) return MT_OK;
+    const size_t sb = c.d.storage == MT_STORE_F64 ? 8 : c.d.storage == MT_STORE_F32 ? 4 : 2;
+    for (int l = 1; l <= c.d.max_level; ++l) {
+        Level &lv = c.lv[l];
+        if (!lv.nexpl || lv.expl_prev) continue;
+        MT_CUDA(ctx, cudaMallocAsync(&lv.expl_prev, sb * (size_t)c.d.q * (size_t)lv.nexpl, ctx.stream));
+        c.prev_stale = true;
+    }
+    if (!c.prev_stale) return MT_OK;
+    for (int l = 1; l <= c.d.max_level; ++l)
+        if (int rc = amr_phase(ctx, c, PH_EXPL_SAVE, l)) return rc;
+    c.prev_stale = false;
+    return MT_OK;
+}
+
 int amr_step(Ctx &ctx, Case &c, int n)
 {
     int rc;
+    if ((rc = amr_prev_sync(ctx, c))) return rc;
     if (c.schedule == MT_SCHED_FUSED) {
         if (!c.primed && (rc = prime_fused(ctx, c))) return rc;
         for (int s = 0; s < n; ++s) {
@@ -1005,8 +1026,8 @@ int batch_lbm_kernel(Ctx &ctx, BatchRec &R, const std::vector<Case *> &all, int 
                 return rc;
         if ((rc = batch_lbm_kernel(ctx, R, cs, l + 1, last))) return rc;
         if (l > 0)
-            if ((rc = fork_cases(ctx, R, cs, [sub](Case &c) { return sub == 0 || c.itime == MT_ITIME_HOLD; },
-                                 [&](Case &c) { return amr_phase(ctx, c, PH_EXPLOSION, l); })))
+            if ((rc = fork_cases(ctx, R, cs, [sub](Case &c) { return sub == 0 || c.itime != MT_ITIME_REFERENCE; },
+                                 [&](Case &c) { return amr_phase(ctx, c, sub == 0 ? PH_EXPLOSION : PH_EXPLOSION_B, l); })))
                 return rc;
         for (Case *c : cs) c->macros_now = last && !(l == 0 && c->d.bc_mode == MT_BC_NEQ);
         // members' own pull work (IB cells; levels without bricks; levels
@@ -1098,6 +1119,7 @@ int batch_step(Ctx &ctx, Batch &B, const std::vector<Case *> &cases, int n)
     if (cases.empty() || n <= 0) return MT_OK;
     int rc;
     for (Case *c : cases) {
+        if ((rc = amr_prev_sync(ctx, *c))) return rc;
         if ((rc = amr_sync_f(ctx, *c))) return rc;
         if (!c->primed && (rc = prime_fused(ctx, *c))) return rc;
     }
@@ -1237,6 +1259,7 @@ int amr_get(Ctx &ctx, Case &c, int level, double *h_f, double *h_fcol)
 int amr_set(Ctx &ctx, Case &c, int level, const double *h_f, const double *h_fcol)
 {
     if (int rc = amr_sync_f(ctx, c)) return rc;
+    c.prev_stale = true;
     Level &lv = c.lv[level];
     if (!lv.n) return MT_OK;
     const size_t nb = sizeof(double) * (size_t)c.d.q * (size_t)lv.n;

@@ -168,10 +168,14 @@ __global__ void k_stream(const int32_t *list, int64_t nl, int64_t n, int textboo
 // With a second post-collision buffer (fused schedule) the children of ghost
 // F2C cells (sources from nf2c on) are written to both: nothing else writes
 // them, and the reference keeps them over the second substep.
+// cprev (MT_ITIME_EXTRAP, second substep): the sources' parent values at the
+// parent's previous step, [Q][ns]; the explosion then starts from
+// 1.5 fcol - 0.5 prev, the parent state extrapolated to the half step.
 template <int Q, class S>
 __global__ void k_explosion(const int32_t *__restrict__ src, const int32_t *__restrict__ child, int64_t ns,
                             int64_t nc, const S *__restrict__ cfcol, int64_t nf, S *__restrict__ ffcol, double scale,
-                            S *__restrict__ ffcol2, int64_t nf2c, const Shift csh, const Shift fsh)
+                            S *__restrict__ ffcol2, int64_t nf2c, const Shift csh, const Shift fsh,
+                            const S *__restrict__ cprev = nullptr)
 {
     using T = Store<S>;
     using C = typename T::C;
@@ -185,6 +189,10 @@ __global__ void k_explosion(const int32_t *__restrict__ src, const int32_t *__re
     C d[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(csh, T::ld(cfcol, k * nc + i), k);
+    if (cprev) {
+#pragma unroll
+        for (int k = 0; k < Q; ++k) d[k] = C(1.5) * d[k] - C(0.5) * full_sh<S>(csh, T::ld(cprev, k * ns + j), k);
+    }
     C r, x, y, z;
     macros_g<Q, C>(d, r, x, y, z);
     const bool both = ffcol2 && j >= nf2c;
@@ -195,6 +203,18 @@ __global__ void k_explosion(const int32_t *__restrict__ src, const int32_t *__re
         T::st(ffcol, k * nf + ch, v);
         if (both) T::st(ffcol2, k * nf + ch, v);
     }
+}
+
+// the explosion sources' parent values into prev [Q][ns] (MT_ITIME_EXTRAP)
+template <int Q, class S>
+__global__ void k_expl_save(const int32_t *__restrict__ src, int64_t ns, const S *__restrict__ cfcol, int64_t nc,
+                            S *__restrict__ prev)
+{
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    const int64_t i = src[j];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) prev[k * ns + j] = cfcol[k * nc + i];
 }
 
 // AMR_transDDF_coalescence (LBM_Manager.cpp:1131-1169)
@@ -1571,13 +1591,34 @@ int amr_phase_q(Ctx &ctx, Case &c, int phase, int l)
             MT_LAUNCHED(ctx);
         }
         return MT_OK;
-    case PH_EXPLOSION: {
+    case PH_EXPLOSION:
+    case PH_EXPLOSION_B: {
+        // PH_EXPLOSION_B: the second substep's explosion of MT_ITIME_HOLD /
+        // MT_ITIME_EXTRAP (the latter from the extrapolated parent state, then
+        // the sources' values are kept for the next one)
         if (l < 1 || !lv.nexpl) return MT_OK;
         Level &cl = c.lv[l - 1];
         const double scale = c2f_scale(c, l);
+        const bool ex = phase == PH_EXPLOSION_B && c.itime == MT_ITIME_EXTRAP;
+        if (ex && !lv.expl_prev) return set_err(ctx, MT_ERR_STATE, "extrapolated explosion without saved sources");
         k_explosion<Q, S><<<grid_for(8 * lv.nexpl, B), B, 0, s>>>(lv.expl_src, lv.expl_child, lv.nexpl, cl.n, A::fcol(cl),
                                                                n, A::fcol(lv), scale, (S *)lv.fcol_alt,
-                                                               lv.nexpl_f2c, c.shift[l - 1], c.shift[l]);
+                                                               lv.nexpl_f2c, c.shift[l - 1], c.shift[l],
+                                                               ex ? (const S *)lv.expl_prev : nullptr);
+        MT_LAUNCHED(ctx);
+        if (ex) {
+            k_expl_save<Q, S><<<grid_for(lv.nexpl, B), B, 0, s>>>(lv.expl_src, lv.nexpl, A::fcol(cl), cl.n,
+                                                                (S *)lv.expl_prev);
+            MT_LAUNCHED(ctx);
+        }
+        return MT_OK;
+    }
+    case PH_EXPL_SAVE: {
+        // the sources' current parent values (the state was set or the option turned on)
+        if (l < 1 || !lv.nexpl || !lv.expl_prev) return MT_OK;
+        Level &cl = c.lv[l - 1];
+        k_expl_save<Q, S><<<grid_for(lv.nexpl, B), B, 0, s>>>(lv.expl_src, lv.nexpl, A::fcol(cl), cl.n,
+                                                            (S *)lv.expl_prev);
         MT_LAUNCHED(ctx);
         return MT_OK;
     }

@@ -96,6 +96,7 @@ int phase_call(mt_ctx *h, int32_t id, int phase, int level)
     if (rc) return rc;
     if (c->dense) return set_err(h->c, MT_ERR_STATE, "per-phase calls need a multi-level case (use mt_step)");
     if (!c->built) return set_err(h->c, MT_ERR_STATE, "case not built");
+    if ((rc = amr_prev_sync(h->c, *c))) return rc;
     if ((rc = amr_sync_f(h->c, *c))) return rc;
     c->primed = false;  // the fused schedule's lookahead no longer matches f
     return amr_phase(h->c, *c, phase, level);
@@ -856,8 +857,9 @@ int mt_case_set_interface_time(mt_ctx *h, int32_t id, int32_t mode)
     if (rc) return rc;
     Ctx &ctx = h->c;
     if (c->dense) return set_err(ctx, MT_ERR_STATE, "the dense path has no level interface");
-    if (mode != MT_ITIME_REFERENCE && mode != MT_ITIME_HOLD)
-        return set_err(ctx, MT_ERR_ARG, "mode must be MT_ITIME_REFERENCE or MT_ITIME_HOLD");
+    if (mode != MT_ITIME_REFERENCE && mode != MT_ITIME_HOLD && mode != MT_ITIME_EXTRAP)
+        return set_err(ctx, MT_ERR_ARG, "mode must be MT_ITIME_REFERENCE, MT_ITIME_HOLD or MT_ITIME_EXTRAP");
+    c->prev_stale = true;
     if (mode != c->itime) {
         // the captured steps bake the explosion launches in
         if (c->graph) cudaGraphExecDestroy(c->graph);

@@ -22,7 +22,7 @@ constexpr int kNumSets = 6;  // lat_f, F2C, C2F, ghost C2F, ghost F2C, solid
 // then the fused schedule's own passes
 enum { PH_MACROS = 0, PH_COLLIDE, PH_STREAM, PH_EXPLOSION, PH_COALESCENCE, PH_BC, PH_IB, PH_BC_INOUT,
        PH_BC_FACE0 = 8, PH_F2C_COLLIDE = 16, PH_PULL_COLLIDE, PH_PRIME, PH_COAL_COLLIDE,
-       PH_SYNC_F, PH_DF, PH_BAND_GRID, PH_FACE_EQ0 = 24, PH_BC_HH = 32 };
+       PH_SYNC_F, PH_DF, PH_BAND_GRID, PH_FACE_EQ0 = 24, PH_BC_HH = 32, PH_EXPLOSION_B, PH_EXPL_SAVE };
 
 // per-cell tag bits (which reference index sets the cell belongs to)
 enum : uint32_t {
@@ -85,6 +85,7 @@ struct Level {
     int32_t *collide_nb = nullptr; int64_t ncollide_nb = 0; // lat_f (not band) then F2C
     // explosion sources on the parent level (F2C then ghost F2C) and their children on this level
     int32_t *expl_src = nullptr; int32_t *expl_child = nullptr; int64_t nexpl = 0, nexpl_f2c = 0;
+    void *expl_prev = nullptr;  // MT_ITIME_EXTRAP: [Q * nexpl] the sources' parent values at the parent's previous step
     // coalescence: F2C cells of this level and their children on the next level
     int32_t *coal_child = nullptr;
     // raw uploads, consumed by the build
@@ -160,6 +161,7 @@ struct Case {
     int schedule = MT_SCHED_PHASES;
     int scaling = MT_SCALE_REFERENCE;  // interface rescaling of the non-equilibrium part
     int itime = MT_ITIME_REFERENCE;    // substeps in which a fine level explodes from its parent
+    bool prev_stale = true;            // expl_prev no longer belongs to the state (MT_ITIME_EXTRAP)
     Shift shift[kMaxLevels];  // per level: storage shift of the reduced storages (from d.u_shift)
     double face_u[6][3] = {};          // bc_velocity of each face's strategy (u_bc unless set)
     // direct-forcing markers (MT_IB_DF)
@@ -238,6 +240,8 @@ int amr_set(Ctx &ctx, Case &c, int level, const double *h_f, const double *h_fco
 int amr_macros(Ctx &ctx, Case &c, int level, double *h_rho, double *h_u);
 int amr_reduce(Ctx &ctx, Case &c, double *h_out);
 int amr_sync_f(Ctx &ctx, Case &c);
+// MT_ITIME_EXTRAP: saved explosion sources allocated and, when stale, taken from the state
+int amr_prev_sync(Ctx &ctx, Case &c);
 int amr_set_face(Ctx &ctx, Case &c, int face, const double *u);
 int amr_prime(Ctx &ctx, Case &c);
 int batch_step(Ctx &ctx, Batch &b, const std::vector<Case *> &cases, int n);

@@ -626,6 +626,7 @@ int surface_tables(Ctx &ctx, const std::vector<double> &h_tri, int L, const Box 
 // each kind.
 int amr_remap(Ctx &ctx, Case &dst, Case &src, int64_t *counts)
 {
+    dst.prev_stale = true;
     if (int rc = amr_sync_f(ctx, src)) return rc;
     if (int rc = amr_sync_f(ctx, dst)) return rc;
     int rc = amr_dispatch(dst, [&](auto *tag) {

@@ -41,7 +41,7 @@ EXPORTS = [
 
 SCHEDULES = {"phases": 0, "fused": 1, "fused_lists": 2}
 SCALINGS = {"reference": 0, "standard": 1}
-ITIMES = {"reference": 0, "hold": 1}
+ITIMES = {"reference": 0, "hold": 1, "extrap": 2}
 
 
 class MTError(RuntimeError):
@@ -260,7 +260,8 @@ class LBM_Manager:
         schedule: "phases" (the reference's passes) or "fused" (stream fused
         with the next collision; same state after every coarse step).
         interface_time: "reference" (a fine level explodes in its first
-        substep) or "hold" (in both, from the parent's state of the step).
+        substep), "hold" (in both, from the parent's state of the step) or
+        "extrap" (the second from that state extrapolated to the half step).
         generate: classify the lattice on the device from the mesh spec
         (mt_case_generate) instead of uploading the host mesher's sets; a
         SpecMesh (no host sets) is always generated."""
@@ -346,8 +347,9 @@ class LBM_Manager:
         self.scaling = scaling
 
     def set_interface_time(self, mode: str):
-        """"reference" (explosion in the first substep only) or "hold"
-        (both substeps, from the parent's post-collision state)."""
+        """"reference" (explosion in the first substep only), "hold" (both
+        substeps, from the parent's post-collision state) or "extrap" (the
+        second from the parent state extrapolated to the half step)."""
         self.ctx.check(lib().mt_case_set_interface_time(self.ctx.h, self.id, ITIMES[mode]), "set_interface_time")
         self.interface_time = mode
 

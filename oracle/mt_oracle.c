@@ -118,11 +118,13 @@ typedef struct {
     keyvec rawband;
     int64_t nband;
     int64_t *band;
+    double *prev; /* MT_ITIME_EXTRAP: explosion sources' parent values at the previous parent step */
 } oc_level;
 
 typedef struct {
     int q, L, collision, ib_method, bc_mode, stream_conv;
-    int itime_hold; /* explosion in both substeps (MT_ITIME_HOLD) */
+    int itime; /* 0 explosion in the first substep, 1 hold, 2 extrapolated second substep */
+    int prev_stale; /* the saved sources no longer belong to the state */
     int periodic[3];
     int64_t extent0[3];
     double tau[OC_MAXL];
@@ -507,7 +509,7 @@ void oc_case_free(void *h)
         free(lv->f); free(lv->fcol); free(lv->rho); free(lv->u);
         for (int s = 0; s < OC_NSETS; ++s) { free(lv->list[s]); free(lv->raw[s].keys); }
         for (int b = 0; b < 26; ++b) { free(lv->bclist[b]); free(lv->rawbc[b].keys); }
-        free(lv->band); free(lv->rawband.keys);
+        free(lv->band); free(lv->rawband.keys); free(lv->prev);
     }
     free(c->dis_key); free(c->dis);
     free(c->mref); free(c->mdv); free(c->path); free(c->acc);
@@ -610,6 +612,7 @@ int oc_build(void *h)
 int oc_init_equilibrium(void *h, double rho0, const double *u0)
 {
     oc_case *c = (oc_case *)h;
+    c->prev_stale = 1;
     int q = c->q;
     double feq[27];
     feq_bgk(q, rho0, u0, feq);
@@ -654,6 +657,7 @@ int oc_set_level(void *h, int level, const double *f, const double *fcol, const 
     if (fcol) memcpy(lv->fcol, fcol, n * (size_t)c->q * 8);
     if (rho) memcpy(lv->rho, rho, n * 8);
     if (u) memcpy(lv->u, u, n * 24);
+    c->prev_stale = 1;
     return 0;
 }
 
@@ -778,19 +782,42 @@ static void children_of(const oc_case *c, uint64_t code, int fine, uint64_t *ch)
 }
 
 /* LBM_Manager::AMR_transDDF_explosion (LBM_Manager.cpp:1059-1129) */
-static int phase_explosion(oc_case *c, int fine)
+/* the explosion sources of level `fine` (F2C then ghost F2C of its parent)
+ * as one list: source s -> parent cell index */
+static int64_t expl_source(const oc_level *cl, int64_t s)
+{
+    return s < cl->nlist[S_F2C] ? cl->list[S_F2C][s] : cl->list[S_GF2C][s - cl->nlist[S_F2C]];
+}
+
+/* parent values of every source into fl->prev [q][nsources] */
+static void save_sources(oc_case *c, int fine)
+{
+    oc_level *cl = &c->lv[fine - 1], *fl = &c->lv[fine];
+    int64_t ns = cl->nlist[S_F2C] + cl->nlist[S_GF2C];
+    if (!fl->prev) fl->prev = (double *)calloc((size_t)(c->q * ns + 1), sizeof(double));
+    for (int64_t s = 0; s < ns; ++s) {
+        int64_t i = expl_source(cl, s);
+        for (int k = 0; k < c->q; ++k) fl->prev[k * ns + s] = cl->fcol[k * cl->n + i];
+    }
+}
+
+static int phase_explosion(oc_case *c, int fine, int extrap)
 {
     int coarse = fine - 1, q = c->q;
     oc_level *cl = &c->lv[coarse], *fl = &c->lv[fine];
     double scale = (2.0 * c->tau[fine]) / c->tau[coarse];
     double dc[27], feq[27], rho, u[3];
     uint64_t ch[8];
+    const int64_t ns = cl->nlist[S_F2C] + cl->nlist[S_GF2C];
     for (int pass = 0; pass < 2; ++pass) {
         int64_t nl = cl->nlist[pass == 0 ? S_F2C : S_GF2C];
         int64_t *li = cl->list[pass == 0 ? S_F2C : S_GF2C];
         for (int64_t j = 0; j < nl; ++j) {
             int64_t i = li[j];
+            const int64_t sidx = pass == 0 ? j : cl->nlist[S_F2C] + j;
             for (int k = 0; k < q; ++k) dc[k] = cl->fcol[k * cl->n + i];
+            if (extrap)
+                for (int k = 0; k < q; ++k) dc[k] = 1.5 * dc[k] - 0.5 * fl->prev[k * ns + sidx];
             macros_of(q, dc, &rho, u);
             feq_heluo(q, rho, u, feq);
             children_of(c, cl->key[i], fine, ch);
@@ -805,6 +832,7 @@ static int phase_explosion(oc_case *c, int fine)
             }
         }
     }
+    if (extrap) save_sources(c, fine);
     return 0;
 }
 
@@ -1218,12 +1246,19 @@ static int phase_bc_hh(oc_case *c)
     return 0;
 }
 
-/* MT_ITIME_HOLD of the device path (no reference counterpart): a fine level
- * explodes from its parent in both substeps, not only in the first
- * (LBM_Simulator.cpp:47-51,122-125). */
-int oc_set_interface_time(void *h, int hold)
+/* Interface time options of the device path (no reference counterpart; the
+ * reference explodes in the first substep only, LBM_Simulator.cpp:47-51,
+ * 122-125): 1 (MT_ITIME_HOLD) explodes in the second substep too from the
+ * same parent values; 2 (MT_ITIME_EXTRAP) explodes the second substep from
+ * the parent's values extrapolated to the half step, 1.5 fcol(t) - 0.5
+ * fcol(t - 1), fcol(t - 1) being the sources' values at the parent's
+ * previous step (the current values when the state was just set). */
+int oc_set_interface_time(void *h, int mode)
 {
-    ((oc_case *)h)->itime_hold = hold ? 1 : 0;
+    oc_case *c = (oc_case *)h;
+    if (mode < 0 || mode > 2) return -1;
+    c->itime = mode;
+    c->prev_stale = 1;
     return 0;
 }
 
@@ -1265,8 +1300,8 @@ static int lbm_kernel(oc_case *c, int l)
             if ((rc = phase_bc_inout(c))) return rc;
         if (l < L)
             if ((rc = lbm_kernel(c, l + 1))) return rc;
-        if ((sub == 0 || c->itime_hold) && l > 0)
-            if ((rc = phase_explosion(c, l))) return rc;
+        if ((sub == 0 || c->itime) && l > 0)
+            if ((rc = phase_explosion(c, l, sub == 1 && c->itime == 2))) return rc;
         phase_stream(c, l);
         if (l == 0) {
             if (c->bc_mode == BC_NEQ)
@@ -1288,6 +1323,10 @@ static int lbm_kernel(oc_case *c, int l)
 int oc_step(void *h, int n_coarse)
 {
     oc_case *c = (oc_case *)h;
+    if (c->itime == 2 && c->prev_stale) {
+        for (int l = 1; l <= c->L; ++l) save_sources(c, l);
+        c->prev_stale = 0;
+    }
     for (int s = 0; s < n_coarse; ++s) {
         int rc = lbm_kernel(c, 0);
         if (rc) return rc;

@@ -114,8 +114,9 @@ class OracleCase:
             self.h = None
 
     def set_interface_time(self, mode):
-        """"reference" (explosion in the first substep) or "hold" (both substeps)."""
-        lib().oc_set_interface_time(self.h, {"reference": 0, "hold": 1}[mode])
+        """"reference" (explosion in the first substep), "hold" (both substeps) or
+        "extrap" (the second from the parent state extrapolated to the half step)."""
+        lib().oc_set_interface_time(self.h, {"reference": 0, "hold": 1, "extrap": 2}[mode])
 
     def size(self, l):
         return int(lib().oc_level_size(self.h, l))

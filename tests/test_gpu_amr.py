@@ -406,21 +406,23 @@ def test_zouhe_hh_runs_under_the_phase_schedule_only(ctx):
     mgr.close()
 
 
+@pytest.mark.parametrize("mode", ["hold", "extrap"])
 @pytest.mark.parametrize("schedule", ["phases", "fused"])
-def test_interface_hold_matches_oracle(ctx, schedule):
-    """Explosion in both substeps (interface_time "hold", no reference
-    counterpart): GPU FP64 under both schedules vs the oracle, bit-exact."""
+def test_interface_hold_matches_oracle(ctx, schedule, mode):
+    """Explosion in both substeps (interface_time "hold", or "extrap" from the
+    parent state extrapolated to the half step; no reference counterpart):
+    GPU FP64 under both schedules vs the oracle, bit-exact."""
     from golden_cases import TRACE_CASES, build_case
     from mortontrie_amr_b200.lbm import LBM_Manager
     import oracle as O
     spec = TRACE_CASES["nested_q19_dw_l3"]
     case = build_case(spec)
     init = init_of(case, spec)
-    mgr = LBM_Manager(ctx, case, schedule=schedule, interface_time="hold")
+    mgr = LBM_Manager(ctx, case, schedule=schedule, interface_time=mode)
     for l, (_, f) in enumerate(init):
         mgr.set_populations(l, f)
     oc = O.OracleCase(case)
-    oc.set_interface_time("hold")
+    oc.set_interface_time(mode)
     for l, (_, f) in enumerate(init):
         oc.set_populations(l, f)
     mgr.fluidSimulate(3)
