@@ -944,9 +944,11 @@ template <int Q, class S, int COLL, int V> constexpr int brick_min_blocks()
     if (Store<S>::bytes == 2) return (COLL == MT_COLL_LBGK && Q == 19) ? MT_BRICK_MIN_BLOCKS_Q19_LBGK : MT_BRICK_MIN_BLOCKS;
     return 1;
 }
-// the form a level runs until mt_case_tune_bricks times both: pairs for every
-// reduced storage (FP64 has only the one-cell form)
-template <class S> constexpr int brick_default_variant() { return Store<S>::shifted ? 1 : 0; }
+// the form a level runs until mt_case_tune_bricks times both: one cell per
+// lane step (measured on the 4-level cumulant sphere and the direct-forcing
+// sphere, FP16 / BF16 / FP32: the pair form runs 2-4x longer per launch, at
+// half the resident warps)
+template <class S> constexpr int brick_default_variant() { return 0; }
 
 template <int Q, class S, int COLL, int V>
 __global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL, V>()) k_brick_step(

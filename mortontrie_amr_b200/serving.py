@@ -41,6 +41,11 @@ AMPLITUDE = 0.5        # oscillation amplitude in sphere radii
 # unstable; 0.1 (Mach 0.17) doubles the finite share of the seeded stream
 # over 0.05
 U_INLET = 0.1
+# the fine interface cells of every request are re-exploded in the second
+# substep too (MT_ITIME_HOLD): with the reference's first-substep-only
+# explosion 18 of the 60 requests of the seeded 20/s stream stay finite, with
+# this 59 (FP16, solved alone)
+INTERFACE_TIME = "hold"
 
 
 @dataclass
@@ -246,7 +251,8 @@ class Server:
 
     def __init__(self, ctx, cache: TemplateCache, storage: str = "f16", budget_gb: float = 150.0,
                  chunk: int = 16, scaling: str = "standard", max_inflight: int = 2, priority_builds: bool = True,
-                 storage_shift=None):
+                 storage_shift=None, interface_time: str = INTERFACE_TIME):
+        self.interface_time = interface_time
         self.ctx = ctx
         self.storage_shift = storage_shift  # per-level storage shift of every case (LBM_Manager)
         self.priority_builds = priority_builds
@@ -309,7 +315,7 @@ class Server:
                     continue
                 ta = time.perf_counter()
                 mgr = LBM_Manager(builder, case, self.storage, schedule="fused", scaling=self.scaling,
-                                  storage_shift=self.storage_shift)
+                                  storage_shift=self.storage_shift, interface_time=self.interface_time)
                 mgr.prepare()
                 mgr.transfer(self.ctx)
                 batch.add(mgr)
@@ -353,14 +359,15 @@ class Server:
 
 
 def solve_alone(ctx, cache: TemplateCache, req: Request, storage: str = "f16", scaling: str = "standard",
-                schedule: Optional[str] = None, storage_shift=None, with_status: bool = False) -> tuple:
+                schedule: Optional[str] = None, storage_shift=None, with_status: bool = False,
+                interface_time: str = INTERFACE_TIME) -> tuple:
     """One request by itself (no batch); returns (cd, cl, seconds), and
     whether the state stayed finite (the device guard) with with_status."""
     from .lbm import LBM_Manager, MTError
     case = request_case(req, cache.get(req))
     t = time.perf_counter()
     mgr = LBM_Manager(ctx, case, storage, schedule=schedule or ("phases" if storage == "f64" else "fused"),
-                      scaling=scaling, storage_shift=storage_shift)
+                      scaling=scaling, storage_shift=storage_shift, interface_time=interface_time)
     mgr.fluidSimulate(req.coarse_steps())
     ctx.synchronize()
     cd, cl = drag_lift(mgr, req)
@@ -383,7 +390,7 @@ def plain_solve_seconds(ctx, cache: TemplateCache, req: Request, sample: int = 8
     from .lbm import LBM_Manager
     case = request_case(req, cache.get(req))
     t = time.perf_counter()
-    mgr = LBM_Manager(ctx, case, "f64", schedule="phases", scaling="standard")
+    mgr = LBM_Manager(ctx, case, "f64", schedule="phases", scaling="standard", interface_time=INTERFACE_TIME)
     ctx.synchronize()
     t_build = time.perf_counter() - t
     k = max(2, req.coarse_steps() // sample)

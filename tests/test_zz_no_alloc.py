@@ -64,7 +64,8 @@ class _PoolWatch:
 
     def reset(self):
         A = self.rt.cudaMemPoolAttr
-        err, = self.rt.cudaMemPoolSetAttribute(self.pool, A.cudaMemPoolAttrUsedMemHigh, self.rt.cuuint64_t(0))
+        from cuda.bindings import driver
+        err, = self.rt.cudaMemPoolSetAttribute(self.pool, A.cudaMemPoolAttrUsedMemHigh, driver.cuuint64_t(0))
         assert err == self.rt.cudaError_t.cudaSuccess, err
         return self._get(A.cudaMemPoolAttrUsedMemCurrent)
 
