@@ -193,9 +193,10 @@ def run_ours(args):
     n_cells = N_EDGE ** 3
     peak, peak_kind = measured_hbm_peak()
 
-    # headline: FP16 shifted storage
-    case = make_case("f16")
-    dense = DenseCase(ctx, case, "f16")
+    # headline: FP16 shifted storage (profiling runs: --quick --quick-storage picks another)
+    hs = args.quick_storage if args.quick else "f16"
+    case = make_case(hs)
+    dense = DenseCase(ctx, case, hs)
     dense.init_fields(*fields)
     block, tune_ms = dense.tune()  # outside the timed region; leaves the state unchanged
     sampler = ClockSampler(local)
@@ -205,7 +206,7 @@ def run_ours(args):
     clocks = sampler.stop() if rank == 0 else None
     mlups = world * n_cells * args.steps / secs / 1e6
     per_launch = secs / args.steps
-    achieved = BYTES_PER_CELL["f16"] * n_cells / per_launch / 1e9
+    achieved = BYTES_PER_CELL[hs] * n_cells / per_launch / 1e9
     red = dense.reduce()
     dense.close()
 
@@ -226,7 +227,7 @@ def run_ours(args):
     # steps, density + velocity back to pinned host memory
     if args.quick:
         if rank == 0:
-            print(json.dumps({"quick": True, "edge": N_EDGE, "mlups": round(mlups, 1), "block": block,
+            print(json.dumps({"quick": True, "storage": hs, "edge": N_EDGE, "mlups": round(mlups, 1), "block": block,
                               "tune_ms": tune_ms, "achieved_gbs": round(achieved, 1),
                               "launches": int(launches)}), flush=True)
         ctx.close()
@@ -358,7 +359,7 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
     per_coarse_fine = stepped[L] << L
     out = {"workload": "4-level D3Q27 cumulant sphere 192x96x96, R=6 (48 finest), Re=200, u=0.04",
            "stepped_cells_per_level": stepped, "coarse_steps": steps,
-           "accuracy_note": "errors vs FP64 after the first warm-up + timed coarse steps from the uniform "
+           "accuracy_note": "errors vs FP64 after the warm-up, one more and the timed coarse steps from the uniform "
                             "inflow state (an impulsively started sphere: a transient drag); the long-run "
                             "comparison is bench.py --amr-accuracy"}
     stream = torch.cuda.current_stream()
@@ -378,6 +379,11 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
         if _shift_of_label(st):
             out[st] = {"storage_shift": SHIFT_NOTE[_shift_of_label(st)]}
         mgr.fluidSimulate(warmup)
+        forms = None
+        if schedule == "fused":
+            # the project autotuner picks each brick level's pass form (outside the timed region)
+            forms, _ = mgr.tune_bricks()
+        mgr.fluidSimulate(1)  # every run: captures the tuned step's graph before the timing
         torch.cuda.synchronize()
         mgr.reset_force()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -396,6 +402,8 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
                    "fine_mlups": round(per_coarse_fine * steps / secs / 1e6, 1),
                    "total_mlups": round(per_coarse_total * steps / secs / 1e6, 1),
                    "ms_per_coarse_step": round(1e3 * secs / steps, 3)}
+        if forms is not None:
+            out[st]["brick_forms_per_level"] = [int(v) for v in forms]
         mgr.close()
     ref = res.get("f64")
     for st, _, _ in runs:
@@ -875,6 +883,8 @@ def main():
                     help="interface rescaling of the accuracy run")
     ap.add_argument("--edge", type=int, default=256, help="cube edge (power of two); 256 is the configuration")
     ap.add_argument("--quick", action="store_true", help="headline kernel only (profiling runs)")
+    ap.add_argument("--quick-storage", default="f16", choices=sorted(BYTES_PER_CELL),
+                    help="storage of the --quick run's kernel")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -262,13 +262,15 @@ int mt_case_status(mt_ctx *ctx, int32_t case_id);
  * 256 only; the other slots are left unwritten). */
 int mt_case_tune(mt_ctx *ctx, int32_t case_id, int32_t *best_block, float *ms_per_candidate);
 /* Project autotuner of the multi-level fused brick pass (no reference
- * counterpart): times each brick level's pass in both of its forms (one cell
- * per lane step, or two cells per lane with packed FP32 pair arithmetic;
- * FP64 has only the first) on the case's own bricks, without changing the
- * state, and keeps the faster per level for the fused steps that follow.
- * variant[max_level + 1]: the form kept (0 / 1, -1 for a level without
- * bricks); ms[2 * (max_level + 1)]: ms per launch of each form (-1 if not
- * timed).  Either may be NULL.  Synchronises the stream; the case keeps its
+ * counterpart): times each brick level's pass in each of its forms (0: one
+ * cell per lane step at 8 resident 128-thread blocks per SM; for FP32 / FP16 /
+ * BF16 storage also 1: the lane's two cells together in packed FP32 pair
+ * arithmetic at 4 blocks, and 2: form 0 at 6 blocks with more registers per
+ * thread; FP64 has form 0 only) on the case's own bricks, without changing
+ * the state, and keeps the fastest per level for the fused steps that follow.
+ * variant[max_level + 1]: the form kept (-1 for a level without bricks);
+ * ms[3 * (max_level + 1)]: ms per launch of each form (-1 if not timed).
+ * Either may be NULL.  Synchronises the stream; the case keeps its
  * schedule. */
 int mt_case_tune_bricks(mt_ctx *ctx, int32_t case_id, int32_t *variant, float *ms);
 /* Schedule of mt_step for a multi-level case (no reference counterpart):

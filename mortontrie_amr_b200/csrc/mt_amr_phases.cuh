@@ -110,6 +110,28 @@ __device__ __forceinline__ void collide_store(const typename Store<S>::C *d, typ
     }
 }
 
+// The macros of d (rho, u into r, x, y, z) and its collision stored into
+// out: the reduced-precision D3Q27 cumulant takes the macros from the
+// collision's own first chimera pass (cumulant_macros_collide); every other
+// form computes them with macros_g and then collides (collide_store).
+template <int Q, class S, int COLL, class I>
+__device__ __forceinline__ void macros_collide_store(const typename Store<S>::C *d, typename Store<S>::C &r,
+                                                     typename Store<S>::C &x, typename Store<S>::C &y,
+                                                     typename Store<S>::C &z, double tau, S *out, I n, I i,
+                                                     const Shift &sh)
+{
+    using T = Store<S>;
+    if constexpr (COLL == MT_COLL_CUMULANT && Q == 27 && T::shifted) {
+        float o[27];
+        cumulant_macros_collide(d, r, x, y, z, (float)(1. / tau), o);
+#pragma unroll
+        for (int k = 0; k < 27; ++k) T::st(out, (I)k * n + i, stored_sh<S>(sh, o[k], k));
+    } else {
+        macros_g<Q, typename T::C>(d, r, x, y, z);
+        collide_store<Q, S, COLL>(d, r, x, y, z, tau, out, n, i, sh);
+    }
+}
+
 // calculateMacros(level) + Collision_LBGK::collide / Collision_Cumulant::collide
 // on lat_f then overlap_F2C (Collision_Manager.cpp:13-53, Collision_Cumulant.cpp:22-159)
 template <int Q, class S, int COLL>
@@ -125,12 +147,12 @@ __global__ void k_collide(const int32_t *list, int64_t nl, int64_t n, double tau
 #pragma unroll
     for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::ld(f, k * n + i), k);
     C r, x, y, z;
-    macros_g<Q, C>(d, r, x, y, z);
+    macros_collide_store<Q, S, COLL>(d, r, x, y, z, tau, fcol, n, i, sh);
     rho[i] = r;
     u[i] = x;
     u[n + i] = y;
     u[2 * n + i] = z;
-    collide_store<Q, S, COLL>(d, r, x, y, z, tau, fcol, n, i, sh);
+    
 }
 
 // fcol = f on overlap_C2F (Collision_Manager.cpp:45-52)
@@ -286,14 +308,13 @@ __global__ void k_coal_collide(const int32_t *__restrict__ list, const int32_t *
         T::st(&sv, 0, st);
         a[k] = full_sh<S>(csh, T::cv(sv), k);
     }
-    macros_g<Q, C>(a, r, x, y, z);
+    macros_collide_store<Q, S, COLL>(a, r, x, y, z, tau, cfnext, nc, i, csh);
     if (macros) {
         rho[i] = r;
         u[i] = x;
         u[nc + i] = y;
         u[2 * nc + i] = z;
     }
-    collide_store<Q, S, COLL>(a, r, x, y, z, tau, cfnext, nc, i, csh);
 }
 
 // Non-equilibrium extrapolation ("eflow stable" form) on one boundary set:
@@ -673,14 +694,13 @@ __global__ void k_pull_collide(const int32_t *__restrict__ list, int64_t nl, int
         for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::cv(v[k]), k);
     }
     C r, x, y, z;
-    macros_g<Q, C>(d, r, x, y, z);
+    macros_collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i, sh);
     if (macros) {
         rho[i] = r;
         u[i] = x;
         u[n + i] = y;
         u[2 * n + i] = z;
     }
-    collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i, sh);
 }
 
 // stream on overlap_C2F cells and their next collision, fcol = f
@@ -729,7 +749,14 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
     using T = Store<S>;
     using C = typename T::C;
     const int32_t *hb = halo + 216 * b;
-    for (int h = lane; h < 216; h += 32) s_idx[h] = __ldg(hb + h);
+    bool ok = true;
+    for (int h = lane; h < 216; h += 32) {
+        const int32_t e = __ldg(hb + h);
+        s_idx[h] = e;
+        ok &= e >= 0;
+    }
+    // every position of the neighbourhood holds a cell: no missing-link test per gather
+    const bool full = __all_sync(0xffffffffu, ok);
     __syncwarp();
 #pragma unroll 1
     for (int part = 0; part < 2; ++part) {
@@ -750,14 +777,19 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
         }
         S v[Q];
         v[0] = fcol[i];
+        if (full) {
 #pragma unroll
-        for (int k = 1; k < Q; ++k)
-            v[k] = src[k] >= 0 ? fcol[(uint32_t)k * n + (uint32_t)src[k]] : f[(uint32_t)k * n + i];
+            for (int k = 1; k < Q; ++k) v[k] = fcol[(uint32_t)k * n + (uint32_t)src[k]];
+        } else {
+#pragma unroll
+            for (int k = 1; k < Q; ++k)
+                v[k] = src[k] >= 0 ? fcol[(uint32_t)k * n + (uint32_t)src[k]] : f[(uint32_t)k * n + i];
+        }
         if (cls != 1 || fall) {
             f[i] = v[0];
 #pragma unroll
             for (int k = 1; k < Q; ++k)
-                if (src[k] >= 0) f[(uint32_t)k * n + i] = v[k];
+                if (full || src[k] >= 0) f[(uint32_t)k * n + i] = v[k];
         }
         if (cls == 2) {
 #pragma unroll
@@ -790,14 +822,13 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
 #pragma unroll
         for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::cv(v[k]), k);
         C r, x, y, z;
-        macros_g<Q, C>(d, r, x, y, z);
+        macros_collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i, sh);
         if (macros) {
             rho[i] = r;
             u[i] = x;
             u[n + i] = y;
             u[2 * n + i] = z;
         }
-        collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i, sh);
     }
 }
 
@@ -938,17 +969,22 @@ __device__ __forceinline__ void brick_warp_any(int64_t b, int lane, int32_t *s_i
 #define MT_BRICK_PAIR_MIN_BLOCKS 4  // the pair passes of every reduced storage (128 registers)
 #endif
 // resident blocks per SM asked of a brick pass (V: one cell or a pair per step)
+#ifndef MT_BRICK_WIDE_MIN_BLOCKS
+#define MT_BRICK_WIDE_MIN_BLOCKS 6  // the one-cell form with more registers (85), reduced storages
+#endif
 template <int Q, class S, int COLL, int V> constexpr int brick_min_blocks()
 {
     if (V == 1 && Store<S>::shifted) return MT_BRICK_PAIR_MIN_BLOCKS;
+    if (V == 2 && Store<S>::shifted) return MT_BRICK_WIDE_MIN_BLOCKS;
     if (Store<S>::bytes == 2) return (COLL == MT_COLL_LBGK && Q == 19) ? MT_BRICK_MIN_BLOCKS_Q19_LBGK : MT_BRICK_MIN_BLOCKS;
     return 1;
 }
-// the form a level runs until mt_case_tune_bricks times both: one cell per
-// lane step (measured on the 4-level cumulant sphere and the direct-forcing
-// sphere, FP16 / BF16 / FP32: the pair form runs 2-4x longer per launch, at
-// half the resident warps)
-template <class S> constexpr int brick_default_variant() { return 0; }
+// the form a level runs until mt_case_tune_bricks times them (measured on
+// the 4-level cumulant sphere and the direct-forcing sphere: the pair form
+// runs 2-4x longer per launch at half the resident warps; 16-bit storage is
+// fastest in form 0, FP32 storage in form 2, whose 6-block bound keeps more
+// warps resident than form 0's unbounded registers)
+template <class S> constexpr int brick_default_variant() { return std::is_same<S, float>::value ? 2 : 0; }
 
 template <int Q, class S, int COLL, int V>
 __global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL, V>()) k_brick_step(
@@ -1058,14 +1094,13 @@ __global__ void k_ib_collide(const int32_t *list, int64_t nl, int64_t n, const i
     force[nl + j] = (double)fy;
     force[2 * nl + j] = (double)fz;
     C r, x, y, z;
-    macros_g<Q, C>(g, r, x, y, z);
+    macros_collide_store<Q, S, COLL>(g, r, x, y, z, tau, fnext, n, i, sh);
     if (macros) {
         rho[i] = r;
         u[i] = x;
         u[n + i] = y;
         u[2 * n + i] = z;
     }
-    collide_store<Q, S, COLL>(g, r, x, y, z, tau, fnext, n, i, sh);
 }
 
 // ---- direct-forcing immersed boundary (Lagrangian markers) --------------------
@@ -1515,9 +1550,10 @@ int band_collide(Ctx &ctx, Case &c, int l, void *out)
     return MT_OK;
 }
 
-// One fused brick pass of level l in the form `variant` (0 one cell, 1 a
-// pair per lane step; reduced storages only have a pair form) on stream s,
-// writing the next collision into fnext.
+// One fused brick pass of level l in the form `variant` (0 one cell per lane
+// step; for the reduced storages also 1, a packed pair, and 2, one cell with
+// more registers per thread) on stream s, writing the next collision into
+// fnext.
 template <int Q, class S>
 void brick_launch(Case &c, int l, int variant, cudaStream_t s, S *fnext, int mac, int fall, long long *bacc)
 {
@@ -1536,12 +1572,13 @@ void brick_launch(Case &c, int l, int variant, cudaStream_t s, S *fnext, int mac
     using CU = std::integral_constant<int, MT_COLL_CUMULANT>;
     using V0 = std::integral_constant<int, 0>;
     using V1 = std::integral_constant<int, 1>;
-    const bool pair = Store<S>::shifted && variant == 1;
+    using V2 = std::integral_constant<int, 2>;
+    const int v = Store<S>::shifted ? variant : 0;
     if (c.d.collision == MT_COLL_LBGK) {
-        if (pair) go(LB{}, V1{}); else go(LB{}, V0{});
+        if (v == 1) go(LB{}, V1{}); else if (v == 2) go(LB{}, V2{}); else go(LB{}, V0{});
     } else {
         if constexpr (Q == 27) {
-            if (pair) go(CU{}, V1{}); else go(CU{}, V0{});
+            if (v == 1) go(CU{}, V1{}); else if (v == 2) go(CU{}, V2{}); else go(CU{}, V0{});
         }
     }
 }
@@ -2023,8 +2060,9 @@ int AmrOps<S>::batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, i
 }
 
 // ---- the brick pass autotuner (mt_case_tune_bricks) ----------------------
-// Each brick level's fused pass is timed in both forms (one cell per lane
-// step, or two cells with packed FP32 pairs; FP64 has only the first) on the
+// Each brick level's fused pass is timed in each of its forms (one cell per
+// lane step at 8 resident blocks per SM; two cells with packed FP32 pairs;
+// one cell at 6 blocks with more registers; FP64 has only the first) on the
 // case's own bricks: one warm-up and three timed launches per form, CUDA
 // events on the case's stream.  The passes read the current post-collision
 // buffer and write the next collision into a scratch buffer; the f they
@@ -2038,7 +2076,7 @@ int AmrOps<S>::tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms)
         if (c.lv[l].bricks) nmax = std::max(nmax, c.lv[l].n);
     for (int l = 0; l <= c.d.max_level; ++l) {
         if (variant) variant[l] = -1;
-        if (ms) ms[2 * l] = ms[2 * l + 1] = -1.f;
+        if (ms) ms[3 * l] = ms[3 * l + 1] = ms[3 * l + 2] = -1.f;
     }
     if (!nmax) return MT_OK;
     S *scratch = nullptr;
@@ -2050,7 +2088,7 @@ int AmrOps<S>::tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms)
     for (int l = 0; l <= c.d.max_level && !rc; ++l) {
         Level &lv = c.lv[l];
         if (!lv.bricks || !lv.nbrick) continue;
-        const int nform = Store<S>::shifted ? 2 : 1;
+        const int nform = Store<S>::shifted ? 3 : 1;
         float best = 0.f;
         int pick = lv.brick_variant;
         for (int v = 0; v < nform && !rc; ++v) {
@@ -2074,7 +2112,7 @@ int AmrOps<S>::tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms)
             cudaEventElapsedTime(&t, e0, e1);
             t /= 3.f;
             ctx.launches += 4;
-            if (ms) ms[2 * l + v] = t;
+            if (ms) ms[3 * l + v] = t;
             if (v == 0 || t < best) {
                 best = t;
                 pick = v;

@@ -270,71 +270,14 @@ MT_HD void chim_back(R a0, R a1, R a2, R v, R v2, R &pn, R &pz, R &pp)
 // backward pass, as in the reference (Collision_Cumulant.cpp:451-454).
 // R = double reproduces the reference bit-for-bit without FMA contraction;
 // R = float is the reduced-precision variant.
+// The part of cumulant_collide after the forward central moments: cumulant
+// relaxation and the backward transforms (Collision_Cumulant.cpp:374-652);
+// m holds the 27 central moments about u, slot (a,b,c) = a + 3b + 9c, and is
+// overwritten.
 template <class R>
-MT_HD void cumulant_collide(const R *f, R rho, R ux, R uy, R uz, R omega1, R *out)
+MT_HD void cumulant_from_moments(R *m, R rho, R ux, R uy, R uz, R omega1, R *out)
 {
-    R m[27];
 #define MM(a, b, c) m[(a) + 3 * (b) + 9 * (c)]
-    if constexpr (!std::is_same<R, double>::value) {
-        // reduced precision: the same central moments by three chimera passes
-        // (x, then y, then z lines of three), a quarter of the operations
-        R g[27];
-#pragma unroll
-        for (int i = 0; i < 27; ++i) g[(ex(i) + 1) + 3 * (ey(i) + 1) + 9 * (ez(i) + 1)] = f[i];
-        const R v[3] = {ux, uy, uz};
-#pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
-            const int st = ax == 0 ? 1 : (ax == 1 ? 3 : 9);
-            const R u = v[ax], u2 = u * u;
-#pragma unroll
-            for (int line = 0; line < 9; ++line) {
-                // base index of the line: the two other axes' positions
-                const int o1 = line % 3, o2 = line / 3;
-                const int bidx = ax == 0 ? 3 * o1 + 9 * o2 : (ax == 1 ? o1 + 9 * o2 : o1 + 3 * o2);
-                const R fm = g[bidx], f0 = g[bidx + st], fp = g[bidx + 2 * st];
-                const R k0 = fm + f0 + fp, d1 = fp - fm, s1 = fp + fm;
-                g[bidx] = k0;
-                g[bidx + st] = d1 - u * k0;
-                g[bidx + 2 * st] = s1 - 2 * u * d1 + u2 * k0;
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < 27; ++i) m[i] = g[i];
-    } else {
-#pragma unroll
-    for (int i = 0; i < 27; ++i) m[i] = 0;
-#pragma unroll
-    for (int i = 0; i < 27; ++i) {
-        const R cx = ex(i) - ux, cy = ey(i) - uy, cz = ez(i) - uz, fi = f[i];
-        MM(0, 0, 0) += fi;
-        MM(1, 0, 0) += cx * fi;
-        MM(0, 1, 0) += cy * fi;
-        MM(0, 0, 1) += cz * fi;
-        MM(2, 0, 0) += cx * cx * fi;
-        MM(0, 2, 0) += cy * cy * fi;
-        MM(0, 0, 2) += cz * cz * fi;
-        MM(1, 1, 0) += cx * cy * fi;
-        MM(1, 0, 1) += cx * cz * fi;
-        MM(0, 1, 1) += cy * cz * fi;
-        MM(2, 1, 0) += cx * cx * cy * fi;
-        MM(2, 0, 1) += cx * cx * cz * fi;
-        MM(0, 2, 1) += cy * cy * cz * fi;
-        MM(1, 2, 0) += cx * cy * cy * fi;
-        MM(1, 0, 2) += cx * cz * cz * fi;
-        MM(0, 1, 2) += cy * cz * cz * fi;
-        MM(1, 1, 1) += cx * cy * cz * fi;
-        MM(2, 2, 0) += cx * cx * cy * cy * fi;
-        MM(2, 0, 2) += cx * cx * cz * cz * fi;
-        MM(0, 2, 2) += cy * cy * cz * cz * fi;
-        MM(2, 1, 1) += cx * cx * cy * cz * fi;
-        MM(1, 2, 1) += cx * cy * cy * cz * fi;
-        MM(1, 1, 2) += cx * cy * cz * cz * fi;
-        MM(2, 2, 1) += cx * cx * cy * cy * cz * fi;
-        MM(2, 1, 2) += cx * cx * cy * cz * cz * fi;
-        MM(1, 2, 2) += cx * cy * cy * cz * cz * fi;
-        MM(2, 2, 2) += cx * cx * cy * cy * cz * cz * fi;
-    }
-    }
     R c200 = MM(2, 0, 0), c020 = MM(0, 2, 0), c002 = MM(0, 0, 2);
     R c110 = MM(1, 1, 0), c101 = MM(1, 0, 1), c011 = MM(0, 1, 1);
     const R k000 = MM(0, 0, 0);
@@ -405,6 +348,142 @@ MT_HD void cumulant_collide(const R *f, R rho, R ux, R uy, R uz, R omega1, R *ou
 #pragma unroll
     for (int i = 0; i < 27; ++i) out[i] = m[(ex(i) + 1) + 3 * (ey(i) + 1) + 9 * (ez(i) + 1)];
 #undef MM
+}
+
+template <class R>
+MT_HD void cumulant_collide(const R *f, R rho, R ux, R uy, R uz, R omega1, R *out)
+{
+    R m[27];
+#define MM(a, b, c) m[(a) + 3 * (b) + 9 * (c)]
+    if constexpr (!std::is_same<R, double>::value) {
+        // reduced precision: the same central moments by three chimera passes
+        // (x, then y, then z lines of three), a quarter of the operations
+        R g[27];
+#pragma unroll
+        for (int i = 0; i < 27; ++i) g[(ex(i) + 1) + 3 * (ey(i) + 1) + 9 * (ez(i) + 1)] = f[i];
+        const R v[3] = {ux, uy, uz};
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            const int st = ax == 0 ? 1 : (ax == 1 ? 3 : 9);
+            const R u = v[ax], u2 = u * u;
+#pragma unroll
+            for (int line = 0; line < 9; ++line) {
+                // base index of the line: the two other axes' positions
+                const int o1 = line % 3, o2 = line / 3;
+                const int bidx = ax == 0 ? 3 * o1 + 9 * o2 : (ax == 1 ? o1 + 9 * o2 : o1 + 3 * o2);
+                const R fm = g[bidx], f0 = g[bidx + st], fp = g[bidx + 2 * st];
+                const R k0 = fm + f0 + fp, d1 = fp - fm, s1 = fp + fm;
+                g[bidx] = k0;
+                g[bidx + st] = d1 - u * k0;
+                g[bidx + 2 * st] = s1 - 2 * u * d1 + u2 * k0;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 27; ++i) m[i] = g[i];
+    } else {
+#pragma unroll
+    for (int i = 0; i < 27; ++i) m[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 27; ++i) {
+        const R cx = ex(i) - ux, cy = ey(i) - uy, cz = ez(i) - uz, fi = f[i];
+        MM(0, 0, 0) += fi;
+        MM(1, 0, 0) += cx * fi;
+        MM(0, 1, 0) += cy * fi;
+        MM(0, 0, 1) += cz * fi;
+        MM(2, 0, 0) += cx * cx * fi;
+        MM(0, 2, 0) += cy * cy * fi;
+        MM(0, 0, 2) += cz * cz * fi;
+        MM(1, 1, 0) += cx * cy * fi;
+        MM(1, 0, 1) += cx * cz * fi;
+        MM(0, 1, 1) += cy * cz * fi;
+        MM(2, 1, 0) += cx * cx * cy * fi;
+        MM(2, 0, 1) += cx * cx * cz * fi;
+        MM(0, 2, 1) += cy * cy * cz * fi;
+        MM(1, 2, 0) += cx * cy * cy * fi;
+        MM(1, 0, 2) += cx * cz * cz * fi;
+        MM(0, 1, 2) += cy * cz * cz * fi;
+        MM(1, 1, 1) += cx * cy * cz * fi;
+        MM(2, 2, 0) += cx * cx * cy * cy * fi;
+        MM(2, 0, 2) += cx * cx * cz * cz * fi;
+        MM(0, 2, 2) += cy * cy * cz * cz * fi;
+        MM(2, 1, 1) += cx * cx * cy * cz * fi;
+        MM(1, 2, 1) += cx * cy * cy * cz * fi;
+        MM(1, 1, 2) += cx * cy * cz * cz * fi;
+        MM(2, 2, 1) += cx * cx * cy * cy * cz * fi;
+        MM(2, 1, 2) += cx * cx * cy * cz * cz * fi;
+        MM(1, 2, 2) += cx * cy * cy * cz * cz * fi;
+        MM(2, 2, 2) += cx * cx * cy * cy * cz * cz * fi;
+    }
+    }
+    cumulant_from_moments<R>(m, rho, ux, uy, uz, omega1, out);
+#undef MM
+}
+
+// Reduced precision D3Q27 cumulant with the macroscopic moments taken from
+// the collision's own first chimera pass: the populations are grouped into
+// the nine x lines of three (e_x = -1, 0, +1) and summed along each line
+// once; the line sums give rho and the momentum directly (rho = sum of the
+// line totals k0, j_x = sum of the line differences d1, j_y / j_z = the line
+// totals of the e_y / e_z = +1 lines minus those of the -1 lines), and the
+// same sums are the x pass of the forward transform once u is known.  The
+// rest is cumulant_collide's FP32 path.  Saves the separate macros pass over
+// the 27 populations and the x pass's own line sums.
+MT_HD void cumulant_macros_collide(const float *f, float &rho, float &ux, float &uy, float &uz, float omega1,
+                                    float *out)
+{
+    float g[27];
+#pragma unroll
+    for (int i = 0; i < 27; ++i) g[(ex(i) + 1) + 3 * (ey(i) + 1) + 9 * (ez(i) + 1)] = f[i];
+    // x lines: slot 0 line total k0, slot 1 difference d1, slot 2 sum of the ends s1
+    float r = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int line = 0; line < 9; ++line) {
+        const int b = 3 * line;
+        const float fm = g[b], f0 = g[b + 1], fp = g[b + 2];
+        const float s1 = fp + fm, d1 = fp - fm, k0 = s1 + f0;
+        g[b] = k0;
+        g[b + 1] = d1;
+        g[b + 2] = s1;
+        r += k0;
+        jx += d1;
+        const int ly = line % 3, lz = line / 3;  // y, z positions 0 1 2 = -1 0 +1
+        if (ly == 2) jy += k0;
+        if (ly == 0) jy -= k0;
+        if (lz == 2) jz += k0;
+        if (lz == 0) jz -= k0;
+    }
+    const float is = 1.f / ((r > -1e-6f && r < 1e-6f) ? ((r < 0.f) ? -1e-6f : 1e-6f) : r);
+    rho = r;
+    ux = jx * is;
+    uy = jy * is;
+    uz = jz * is;
+    {
+        const float u = ux, u2 = u * u;
+#pragma unroll
+        for (int line = 0; line < 9; ++line) {
+            const int b = 3 * line;
+            const float k0 = g[b], d1 = g[b + 1], s1 = g[b + 2];
+            g[b + 1] = d1 - u * k0;
+            g[b + 2] = s1 - 2 * u * d1 + u2 * k0;
+        }
+    }
+    const float v[3] = {ux, uy, uz};
+#pragma unroll
+    for (int ax = 1; ax < 3; ++ax) {
+        const int st = ax == 1 ? 3 : 9;
+        const float u = v[ax], u2 = u * u;
+#pragma unroll
+        for (int line = 0; line < 9; ++line) {
+            const int o1 = line % 3, o2 = line / 3;
+            const int bidx = ax == 1 ? o1 + 9 * o2 : o1 + 3 * o2;
+            const float fm = g[bidx], f0 = g[bidx + st], fp = g[bidx + 2 * st];
+            const float k0 = fm + f0 + fp, d1 = fp - fm, s1 = fp + fm;
+            g[bidx] = k0;
+            g[bidx + st] = d1 - u * k0;
+            g[bidx + 2 * st] = s1 - 2 * u * d1 + u2 * k0;
+        }
+    }
+    cumulant_from_moments<float>(g, rho, ux, uy, uz, omega1, out);
 }
 
 }  // namespace mt
