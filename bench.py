@@ -340,7 +340,7 @@ def _shift_of_label(label):
     return None
 
 
-def amr_section(ctx, torch, steps=10, warmup=2, only=None):
+def amr_section(ctx, torch, steps=10, warmup=2, only=None, tune=True):
     """4-level D3Q27 cumulant sphere (192x96x96 coarse, R = 6 coarse = 48
     finest cells, Re 200, u 0.04, nested boxes 4R / 2.5R / 1.75R): coarse
     steps of the multi-level path in the reference's FP64 and with FP32 / FP16
@@ -380,7 +380,7 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None):
             out[st] = {"storage_shift": SHIFT_NOTE[_shift_of_label(st)]}
         mgr.fluidSimulate(warmup)
         forms = None
-        if schedule == "fused":
+        if schedule == "fused" and tune:
             # the project autotuner picks each brick level's pass form (outside the timed region)
             forms, _ = mgr.tune_bricks()
         mgr.fluidSimulate(1)  # every run: captures the tuned step's graph before the timing
@@ -885,6 +885,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="headline kernel only (profiling runs)")
     ap.add_argument("--quick-storage", default="f16", choices=sorted(BYTES_PER_CELL),
                     help="storage of the --quick run's kernel")
+    ap.add_argument("--no-brick-tune", action="store_true",
+                    help="4-level section: keep each storage's default brick form (launch-list captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -953,7 +955,8 @@ def main():
         ctx = Context(0)
         ctx.set_stream(stream.cuda_stream)
         only = args.amr_variants.split(",") if args.amr_variants else None
-        print(json.dumps({"amr_cumulant_sphere": amr_section(ctx, torch, steps=args.steps, warmup=1, only=only)}),
+        print(json.dumps({"amr_cumulant_sphere": amr_section(ctx, torch, steps=args.steps, warmup=1, only=only,
+                                                                       tune=not args.no_brick_tune)}),
               flush=True)
         ctx.close()
     else:
