@@ -5,6 +5,7 @@ the reference checkout) on seeded synthetic cases.
 Run here, where the reference checkout exists:
     python tests/golden/gen_golden.py            # short cases + Morton answers
     python tests/golden/gen_golden.py --trace [name ...]   # TRACE_CASES
+    python tests/golden/gen_golden.py --morton             # neighbour blocks
 The outputs are small .npz files; the GPU box only reads them.  The trace
 cases run one harness process each, in parallel; cfg1's 1000 coarse steps
 take about half an hour of one core.
@@ -82,6 +83,30 @@ def main():
         print("morton kat", os.path.getsize(path), "bytes")
 
 
+def morton_blocks():
+    """Known answers of Morton_Assist::find_neighbor for every cell of two
+    8^3 blocks per level -- at the origin (every -1 step underflows a
+    coordinate field) and straddling 32 * 2^l on every axis (the +1 / -1
+    steps carry across five bits) -- for D3Q19 with 2 levels and D3Q19 /
+    D3Q27 with 4 levels."""
+    import oracle as O
+    from mortontrie_amr_b200.lattice import cell_key
+    for (q, L) in [(19, 1), (19, 3), (27, 3)]:
+        levels, keys = [], []
+        for l in range(L + 1):
+            for lo in (0, (32 << l) - 4):
+                r = np.arange(lo, lo + 8)
+                X, Y, Z = np.meshgrid(r, r, r, indexing="ij")
+                keys.append(cell_key(L, l, X.ravel(), Y.ravel(), Z.ravel()))
+                levels.append(np.full(X.size, l, np.int32))
+        levels = np.concatenate(levels)
+        keys = np.concatenate(keys)
+        nb = O.run_harness_morton(q, L, levels, keys)
+        path = os.path.join(HERE, f"morton_blocks_q{q}_l{L}.npz")
+        np.savez_compressed(path, levels=levels, keys=keys, neighbors=nb)
+        print("morton blocks", q, L, keys.size, os.path.getsize(path), "bytes")
+
+
 SAMPLE = 64
 
 
@@ -136,7 +161,9 @@ def gen_trace(name):
 
 
 if __name__ == "__main__":
-    if "--trace" in sys.argv:
+    if "--morton" in sys.argv:
+        morton_blocks()
+    elif "--trace" in sys.argv:
         from concurrent.futures import ProcessPoolExecutor
         import multiprocessing as mp
         names = [a for a in sys.argv[1:] if not a.startswith("--")] or sorted(TRACE_CASES)

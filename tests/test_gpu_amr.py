@@ -468,3 +468,24 @@ def test_brick_tuner_keeps_the_trajectory(ctx, storage):
             assert rel_err(ca, cb) < 1e-2, l
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("q,L", [(19, 1), (19, 3), (27, 3)])
+def test_device_neighbor_table_matches_reference_blocks(ctx, q, L):
+    """The device-built neighbour table of the KAT blocks (every cell of two
+    8^3 blocks per level, with every neighbour the reference gives them
+    stored): each link is the index of the key Morton_Assist::find_neighbor
+    returns (the reference's pull direction, +e_q)."""
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    from test_morton import blocks_case
+    case, z = blocks_case(q, L)
+    mgr = LBM_Manager(ctx, case)
+    for lev in range(L + 1):
+        keys, _ = mgr.keys(lev)
+        nb = mgr.neighbors(lev)
+        m = z["levels"] == lev
+        idx = np.searchsorted(keys, z["keys"][m])
+        assert np.array_equal(keys[idx], z["keys"][m])
+        want = np.searchsorted(keys, z["neighbors"][m][:, 1:])          # (cells, Q-1)
+        assert np.array_equal(nb[:, idx].T, want), lev
+    mgr.close()
