@@ -263,15 +263,16 @@ int mt_case_status(mt_ctx *ctx, int32_t case_id);
 int mt_case_tune(mt_ctx *ctx, int32_t case_id, int32_t *best_block, float *ms_per_candidate);
 /* Project autotuner of the multi-level fused brick pass (no reference
  * counterpart): times each brick level's pass in each of its forms (0: one
- * cell per lane step at 8 resident 128-thread blocks per SM; for FP32 / FP16 /
- * BF16 storage also 1: the lane's two cells together in packed FP32 pair
- * arithmetic at 4 blocks, and 2: form 0 at 6 blocks with more registers per
- * thread; FP64 has form 0 only) on the case's own bricks, without changing
- * the state, and keeps the fastest per level for the fused steps that follow.
- * variant[max_level + 1]: the form kept (-1 for a level without bricks);
- * ms[3 * (max_level + 1)]: ms per launch of each form (-1 if not timed).
- * Either may be NULL.  Synchronises the stream; the case keeps its
- * schedule. */
+ * cell per lane step at 8 resident 128-thread blocks per SM; 3: the lane's two
+ * cells in one unrolled sequence, so that the second cell's gathers overlap
+ * the first cell's collision, at 6 blocks; for FP32 / FP16 / BF16 storage
+ * also 1: the two cells together in packed FP32 pair arithmetic at 4 blocks,
+ * and 2: form 0 at 6 blocks with more registers per thread) on the case's
+ * own bricks, without changing the state, and keeps the fastest per level
+ * for the fused steps that follow.  variant[max_level + 1]: the form kept
+ * (-1 for a level without bricks); ms[4 * (max_level + 1)]: ms per launch of
+ * each form (-1 if not timed).  Either may be NULL.  Synchronises the
+ * stream; the case keeps its schedule. */
 int mt_case_tune_bricks(mt_ctx *ctx, int32_t case_id, int32_t *variant, float *ms);
 /* Schedule of mt_step for a multi-level case (no reference counterpart):
  * MT_SCHED_PHASES (default) issues the reference's phases one pass each;

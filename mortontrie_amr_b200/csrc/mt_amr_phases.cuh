@@ -737,8 +737,90 @@ __global__ void k_pull_copy(const int32_t *__restrict__ list, int64_t nl, int64_
 // When `macros` is set (the level's last substep of the coarse step) the
 // macros of the streamed f are written too: they are what the all-level
 // calculateMacros at the end of the coarse step computes.
-// one warp's brick b (see above); s_idx is the warp's 216-entry shared table
+// one cell (local Morton index m) of brick b in the fused brick pass
 template <int Q, class S, int COLL>
+__device__ __forceinline__ void brick_cell(int64_t b, int m, const int32_t *s_idx, const uint8_t *__restrict__ bcls,
+                                           uint32_t n, int textbook, bool full, const S *__restrict__ fcol,
+                                           S *__restrict__ f, S *__restrict__ fnext, double tau,
+                                           typename Store<S>::C *__restrict__ rho,
+                                           typename Store<S>::C *__restrict__ u, int macros, int fall,
+                                           long long *__restrict__ acc, const Shift &sh)
+{
+    using T = Store<S>;
+    using C = typename T::C;
+    const int lx = (m & 1) | ((m >> 2) & 2), ly = ((m >> 1) & 1) | ((m >> 3) & 2),
+              lz = ((m >> 2) & 1) | ((m >> 4) & 2);
+    const int base = (lx + 1) + 6 * (ly + 1) + 36 * (lz + 1);
+    const int32_t ii = s_idx[base];
+    if (ii < 0) return;
+    const int cls = __ldg(bcls + 64 * b + m);
+    if (!cls) return;
+    const uint32_t i = (uint32_t)ii;
+    int32_t src[Q];
+#pragma unroll
+    for (int k = 1; k < Q; ++k) {
+        const int off = ex(k) + 6 * ey(k) + 36 * ez(k);
+        src[k] = s_idx[base + (textbook ? -off : off)];
+    }
+    S v[Q];
+    v[0] = fcol[i];
+    if (full) {
+#pragma unroll
+        for (int k = 1; k < Q; ++k) v[k] = fcol[(uint32_t)k * n + (uint32_t)src[k]];
+    } else {
+#pragma unroll
+        for (int k = 1; k < Q; ++k)
+            v[k] = src[k] >= 0 ? fcol[(uint32_t)k * n + (uint32_t)src[k]] : f[(uint32_t)k * n + i];
+    }
+    if (cls != 1 || fall) {
+        f[i] = v[0];
+#pragma unroll
+        for (int k = 1; k < Q; ++k)
+            if (full || src[k] >= 0) f[(uint32_t)k * n + i] = v[k];
+    }
+    if (cls == 2) {
+#pragma unroll
+        for (int k = 0; k < Q; ++k) fnext[(uint32_t)k * n + i] = v[k];
+        return;
+    }
+    if (cls == 4) {
+        // direct-forcing band: collided after the forcing; with acc the
+        // band's rho, unforced velocity and cleared accumulator are
+        // written here (what k_band_macros computes from the stored f)
+        if constexpr (COLL == MT_COLL_LBGK) {
+            if (acc) {
+                C d[Q];
+#pragma unroll
+                for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::cv(v[k]), k);
+                C r, x, y, z;
+                macros_g<Q, C>(d, r, x, y, z);
+                rho[i] = r;
+                u[i] = x;
+                u[n + i] = y;
+                u[2 * n + i] = z;
+                acc[i] = 0;
+                acc[n + i] = 0;
+                acc[2 * n + i] = 0;
+            }
+        }
+        return;
+    }
+    C d[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::cv(v[k]), k);
+    C r, x, y, z;
+    macros_collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i, sh);
+    if (macros) {
+        rho[i] = r;
+        u[i] = x;
+        u[n + i] = y;
+        u[2 * n + i] = z;
+    }
+}
+
+// one warp's brick b (see above); s_idx is the warp's 216-entry shared table;
+// UNROLL (form 3): the lane's two cells in one unrolled sequence
+template <int Q, class S, int COLL, bool UNROLL = false>
 __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, const int32_t *__restrict__ halo,
                                            const uint8_t *__restrict__ bcls, uint32_t n, int textbook,
                                            const S *__restrict__ fcol, S *__restrict__ f, S *__restrict__ fnext,
@@ -758,77 +840,18 @@ __device__ __forceinline__ void brick_warp(int64_t b, int lane, int32_t *s_idx, 
     // every position of the neighbourhood holds a cell: no missing-link test per gather
     const bool full = __all_sync(0xffffffffu, ok);
     __syncwarp();
+    if constexpr (UNROLL) {
+        // both cells in one sequence: the second cell's gathers can be issued
+        // before the first cell's collision
+#pragma unroll
+        for (int part = 0; part < 2; ++part)
+            brick_cell<Q, S, COLL>(b, lane + 32 * part, s_idx, bcls, n, textbook, full, fcol, f, fnext, tau, rho, u,
+                                   macros, fall, acc, sh);
+    } else {
 #pragma unroll 1
-    for (int part = 0; part < 2; ++part) {
-        const int m = lane + 32 * part;
-        const int lx = (m & 1) | ((m >> 2) & 2), ly = ((m >> 1) & 1) | ((m >> 3) & 2),
-                  lz = ((m >> 2) & 1) | ((m >> 4) & 2);
-        const int base = (lx + 1) + 6 * (ly + 1) + 36 * (lz + 1);
-        const int32_t ii = s_idx[base];
-        if (ii < 0) continue;
-        const int cls = __ldg(bcls + 64 * b + m);
-        if (!cls) continue;
-        const uint32_t i = (uint32_t)ii;
-        int32_t src[Q];
-#pragma unroll
-        for (int k = 1; k < Q; ++k) {
-            const int off = ex(k) + 6 * ey(k) + 36 * ez(k);
-            src[k] = s_idx[base + (textbook ? -off : off)];
-        }
-        S v[Q];
-        v[0] = fcol[i];
-        if (full) {
-#pragma unroll
-            for (int k = 1; k < Q; ++k) v[k] = fcol[(uint32_t)k * n + (uint32_t)src[k]];
-        } else {
-#pragma unroll
-            for (int k = 1; k < Q; ++k)
-                v[k] = src[k] >= 0 ? fcol[(uint32_t)k * n + (uint32_t)src[k]] : f[(uint32_t)k * n + i];
-        }
-        if (cls != 1 || fall) {
-            f[i] = v[0];
-#pragma unroll
-            for (int k = 1; k < Q; ++k)
-                if (full || src[k] >= 0) f[(uint32_t)k * n + i] = v[k];
-        }
-        if (cls == 2) {
-#pragma unroll
-            for (int k = 0; k < Q; ++k) fnext[(uint32_t)k * n + i] = v[k];
-            continue;
-        }
-        if (cls == 4) {
-            // direct-forcing band: collided after the forcing; with acc the
-            // band's rho, unforced velocity and cleared accumulator are
-            // written here (what k_band_macros computes from the stored f)
-            if constexpr (COLL == MT_COLL_LBGK) {
-                if (acc) {
-                    C d[Q];
-#pragma unroll
-                    for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::cv(v[k]), k);
-                    C r, x, y, z;
-                    macros_g<Q, C>(d, r, x, y, z);
-                    rho[i] = r;
-                    u[i] = x;
-                    u[n + i] = y;
-                    u[2 * n + i] = z;
-                    acc[i] = 0;
-                    acc[n + i] = 0;
-                    acc[2 * n + i] = 0;
-                }
-            }
-            continue;
-        }
-        C d[Q];
-#pragma unroll
-        for (int k = 0; k < Q; ++k) d[k] = full_sh<S>(sh, T::cv(v[k]), k);
-        C r, x, y, z;
-        macros_collide_store<Q, S, COLL>(d, r, x, y, z, tau, fnext, n, i, sh);
-        if (macros) {
-            rho[i] = r;
-            u[i] = x;
-            u[n + i] = y;
-            u[2 * n + i] = z;
-        }
+        for (int part = 0; part < 2; ++part)
+            brick_cell<Q, S, COLL>(b, lane + 32 * part, s_idx, bcls, n, textbook, full, fcol, f, fnext, tau, rho, u,
+                                   macros, fall, acc, sh);
     }
 }
 
@@ -955,8 +978,8 @@ __device__ __forceinline__ void brick_warp_any(int64_t b, int lane, int32_t *s_i
         brick_warp_pair<Q, S, COLL>(b, lane, s_idx, halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros,
                                     fall, acc, sh);
     else
-        brick_warp<Q, S, COLL>(b, lane, s_idx, halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros, fall,
-                               acc, sh);
+        brick_warp<Q, S, COLL, V == 3>(b, lane, s_idx, halo, bcls, n, textbook, fcol, f, fnext, tau, rho, u, macros,
+                                       fall, acc, sh);
 }
 
 #ifndef MT_BRICK_MIN_BLOCKS
@@ -972,10 +995,14 @@ __device__ __forceinline__ void brick_warp_any(int64_t b, int lane, int32_t *s_i
 #ifndef MT_BRICK_WIDE_MIN_BLOCKS
 #define MT_BRICK_WIDE_MIN_BLOCKS 6  // the one-cell form with more registers (85), reduced storages
 #endif
+#ifndef MT_BRICK_UNROLL_MIN_BLOCKS
+#define MT_BRICK_UNROLL_MIN_BLOCKS 6  // the two cells of a lane in one unrolled sequence (form 3)
+#endif
 template <int Q, class S, int COLL, int V> constexpr int brick_min_blocks()
 {
     if (V == 1 && Store<S>::shifted) return MT_BRICK_PAIR_MIN_BLOCKS;
     if (V == 2 && Store<S>::shifted) return MT_BRICK_WIDE_MIN_BLOCKS;
+    if (V == 3) return Store<S>::shifted ? MT_BRICK_UNROLL_MIN_BLOCKS : 1;
     if (Store<S>::bytes == 2) return (COLL == MT_COLL_LBGK && Q == 19) ? MT_BRICK_MIN_BLOCKS_Q19_LBGK : MT_BRICK_MIN_BLOCKS;
     return 1;
 }
@@ -1551,9 +1578,9 @@ int band_collide(Ctx &ctx, Case &c, int l, void *out)
 }
 
 // One fused brick pass of level l in the form `variant` (0 one cell per lane
-// step; for the reduced storages also 1, a packed pair, and 2, one cell with
-// more registers per thread) on stream s, writing the next collision into
-// fnext.
+// step; 3 the lane's two cells in one unrolled sequence; for the reduced
+// storages also 1, a packed pair, and 2, one cell with more registers per
+// thread) on stream s, writing the next collision into fnext.
 template <int Q, class S>
 void brick_launch(Case &c, int l, int variant, cudaStream_t s, S *fnext, int mac, int fall, long long *bacc)
 {
@@ -1573,12 +1600,13 @@ void brick_launch(Case &c, int l, int variant, cudaStream_t s, S *fnext, int mac
     using V0 = std::integral_constant<int, 0>;
     using V1 = std::integral_constant<int, 1>;
     using V2 = std::integral_constant<int, 2>;
-    const int v = Store<S>::shifted ? variant : 0;
+    using V3 = std::integral_constant<int, 3>;
+    const int v = (Store<S>::shifted || variant == 3) ? variant : 0;
     if (c.d.collision == MT_COLL_LBGK) {
-        if (v == 1) go(LB{}, V1{}); else if (v == 2) go(LB{}, V2{}); else go(LB{}, V0{});
+        if (v == 1) go(LB{}, V1{}); else if (v == 2) go(LB{}, V2{}); else if (v == 3) go(LB{}, V3{}); else go(LB{}, V0{});
     } else {
         if constexpr (Q == 27) {
-            if (v == 1) go(CU{}, V1{}); else if (v == 2) go(CU{}, V2{}); else go(CU{}, V0{});
+            if (v == 1) go(CU{}, V1{}); else if (v == 2) go(CU{}, V2{}); else if (v == 3) go(CU{}, V3{}); else go(CU{}, V0{});
         }
     }
 }
@@ -2062,7 +2090,8 @@ int AmrOps<S>::batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, i
 // ---- the brick pass autotuner (mt_case_tune_bricks) ----------------------
 // Each brick level's fused pass is timed in each of its forms (one cell per
 // lane step at 8 resident blocks per SM; two cells with packed FP32 pairs;
-// one cell at 6 blocks with more registers; FP64 has only the first) on the
+// one cell at 6 blocks with more registers; the lane's two cells in one
+// unrolled sequence at 6 blocks; FP64 has the first and the last) on the
 // case's own bricks: one warm-up and three timed launches per form, CUDA
 // events on the case's stream.  The passes read the current post-collision
 // buffer and write the next collision into a scratch buffer; the f they
@@ -2076,7 +2105,7 @@ int AmrOps<S>::tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms)
         if (c.lv[l].bricks) nmax = std::max(nmax, c.lv[l].n);
     for (int l = 0; l <= c.d.max_level; ++l) {
         if (variant) variant[l] = -1;
-        if (ms) ms[3 * l] = ms[3 * l + 1] = ms[3 * l + 2] = -1.f;
+        if (ms) ms[4 * l] = ms[4 * l + 1] = ms[4 * l + 2] = ms[4 * l + 3] = -1.f;
     }
     if (!nmax) return MT_OK;
     S *scratch = nullptr;
@@ -2088,10 +2117,11 @@ int AmrOps<S>::tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms)
     for (int l = 0; l <= c.d.max_level && !rc; ++l) {
         Level &lv = c.lv[l];
         if (!lv.bricks || !lv.nbrick) continue;
-        const int nform = Store<S>::shifted ? 3 : 1;
+        const int nform = 4;
         float best = 0.f;
         int pick = lv.brick_variant;
         for (int v = 0; v < nform && !rc; ++v) {
+            if (!Store<S>::shifted && (v == 1 || v == 2)) continue;  // FP64: forms 0 and 3
             auto launch = [&]() {
                 if (c.d.q == 19)
                     brick_launch<19, S>(c, l, v, ctx.stream, scratch, 0, 0, nullptr);
@@ -2112,8 +2142,8 @@ int AmrOps<S>::tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms)
             cudaEventElapsedTime(&t, e0, e1);
             t /= 3.f;
             ctx.launches += 4;
-            if (ms) ms[3 * l + v] = t;
-            if (v == 0 || t < best) {
+            if (ms) ms[4 * l + v] = t;
+            if (v == 0 || t < best) {  // form 0 is always timed first
                 best = t;
                 pick = v;
             }

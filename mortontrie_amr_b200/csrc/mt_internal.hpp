@@ -66,7 +66,7 @@ struct Level {
     // position of the 6x6x6 neighbourhood; bcls[64 * b + m] is
     // the cell's work in the fused pass (0 none, 1 stream + collide, 2 stream + copy).
     bool bricks = false;
-    int brick_variant = 0;  // fused brick pass: 0 one cell per lane step, 1 two cells with packed FP32 pairs, 2 one cell with more registers
+    int brick_variant = 0;  // fused brick pass: 0 one cell per lane step, 1 two cells with packed FP32 pairs, 2 one cell with more registers, 3 both cells unrolled
     int64_t nbrick = 0;
     int32_t *bstart = nullptr;
     uint64_t *bmask = nullptr;
@@ -266,7 +266,7 @@ template <class S> struct AmrOps {
     static int reduce(Ctx &ctx, Case &c, double *d_out);
     // time every form of every brick level's fused pass (into scratch, state
     // untouched) and keep the fastest in Level::brick_variant;
-    // ms[3 * level + form], variant[level] (-1: no brick pass on the level)
+    // ms[4 * level + form], variant[level] (-1: no brick pass on the level)
     static int tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms);
     // batched brick pass (descriptor in device memory, total bricks known on the host)
     static int batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total, const Shift &sh);

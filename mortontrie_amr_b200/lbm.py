@@ -470,11 +470,12 @@ class LBM_Manager:
 
     def tune_bricks(self):
         """Time every form of every brick level's fused pass (0 one cell per
-        lane step, 1 a packed pair, 2 one cell with more registers) and keep
+        lane step, 1 a packed pair, 2 one cell with more registers, 3 the
+        lane's two cells unrolled together) and keep
         the fastest per level; returns (form per level, -1 without bricks;
         ms per launch [level][form], -1 where not timed)."""
         v = np.zeros(self.L + 1, np.int32)
-        ms = np.zeros((self.L + 1, 3), np.float32)
+        ms = np.zeros((self.L + 1, 4), np.float32)
         self.ctx.check(lib().mt_case_tune_bricks(self.ctx.h, self.id, _ptr(v, C.c_int32), _ptr(ms, C.c_float)),
                        "mt_case_tune_bricks")
         return v, ms
