@@ -455,7 +455,7 @@ def test_brick_tuner_keeps_the_trajectory(ctx, storage):
     v, ms = a.tune_bricks()
     assert (v >= 0).any() and (ms.max() > 0)
     if storage == "f64":
-        assert set(v[v >= 0]) == {0}
+        assert set(v[v >= 0]) <= {0, 3}  # FP64 has the one-cell forms only
     a.fluidSimulate(3)
     b.fluidSimulate(3)
     ctx.synchronize()
