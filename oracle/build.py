@@ -56,6 +56,7 @@ REF_TUS = [
     "BC/NonEquilibrumExtrapolation.cpp",
     "ComplexBoundary_Manager.cpp",
     "Morton_Assist.cpp",
+    "tecplot.cpp",
 ]
 HARNESS_VARIANTS = [(19, 0), (19, 1), (19, 2), (19, 3), (27, 0), (27, 1), (27, 2), (27, 3)]
 # (Q, L) of the harnesses built with the periodic find_neighbor wrap

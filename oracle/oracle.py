@@ -290,6 +290,25 @@ def run_harness_trace(case, dumps, init=None, timeout=7200):
     return dict(seconds=secs, states=states, force=force, tau=tau, dumps=dumps)
 
 
+def run_harness_tecplot(case, nsteps, iteration, init=None, timeout=600):
+    """Run the reference's step on `case` for nsteps coarse steps, then its
+    IO_TECPLOTH::write(iteration); returns (file name, file text)."""
+    import build
+    q, L = case.params.q, case.mesh.spec.max_level
+    exe = build.build_refharness(q, L)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as fh:
+            fh.write(harness_input(case, nsteps, init) + struct.pack("<i", int(iteration)))
+        subprocess.run([exe, "tecplot", fin, fout], check=True, timeout=timeout, cwd=td)
+        outdir = os.path.join(td, "output")
+        names = sorted(os.listdir(outdir))
+        if len(names) != 1:
+            raise RuntimeError(f"expected one flow file, found {names}")
+        with open(os.path.join(outdir, names[0])) as fh:
+            return names[0], fh.read()
+
+
 def start_harness(case, nsteps, workdir, tag, nwarm=0, init=None):
     """Launch one harness process without waiting (CPU baseline runs several
     in parallel, one per core); returns (Popen, output path).  A mesh with

@@ -16,6 +16,7 @@
  * usage: harness step  <in.bin> <out.bin>
  *        harness pstep <in.bin> <out.bin>      (step with periodic axes)
  *        harness trace <in.bin> <out.bin>      (state dumps after chosen steps)
+ *        harness tecplot <in.bin> <out.bin>    (the reference's flow file after the steps)
  *        harness morton <in.bin> <out.bin>     (neighbour-key known answers)
  *
  * Built with -DHC_PERIODIC the harness includes a generated copy of
@@ -24,6 +25,8 @@
  * builds, BC/Periodic.cpp needs the ghost layers that BC_NO_GHOST removes);
  * with no axis marked it is the reference's arithmetic unchanged.
  */
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <array>
 #include <bitset>
@@ -58,6 +61,8 @@
 #include "BC/D3Q19_BC_Manager.hpp"
 #undef private
 #undef protected
+#include "Grid_Manager.h"
+#include "Solid_Manager.h"
 
 /* static members whose definitions live in translation units the harness
  * does not build (Grid_Manager.cpp, Lat_Manager.cpp, Obj_Manager.cpp ...) */
@@ -74,6 +79,9 @@ D_morton Morton_Assist::mortonz_min, Morton_Assist::mortonz_max;
 Lat_Manager *Lat_Manager::pointer_me;
 LBM_Manager *LBM_Manager::pointer_me;
 IO_Manager *IO_Manager::pointer_me;
+/* tecplot.cpp's mesh writers name these; the flow writer used here does not */
+Grid_Manager *Grid_Manager::pointer_me;
+Solid_Manager *Solid_Manager::pointer_me;
 std::ofstream *Log_function::logfile;
 void IO_Manager::writeFlow(const D_int) {}
 
@@ -302,6 +310,26 @@ int run_step(Reader &in, FILE *out, bool periodic = false)
     return 0;
 }
 
+/* tecplot: the step input followed by int32 iter; after the steps the
+ * reference's IO_TECPLOTH::write(iter) (tecplot.cpp:16-176) writes
+ * output/sphereFlow_<iter * CF_T[0]>.dat under the working directory. */
+int run_tecplot(Reader &in, FILE *out)
+{
+    Morton_Assist ma;
+    setup_morton(ma);
+    Loaded c;
+    if (int rc = load_case(in, c)) return rc;
+    const int32_t iter = in.get<int32_t>();
+    std::vector<double> force;
+    for (int s = 0; s < c.nsteps; ++s) coarse_step(c.mgr, force);
+    mkdir(C_OUTPUT_DIR, 0777);
+    IO_TECPLOTH tp;
+    tp.write(iter);
+    const int32_t done = 1;
+    fwrite(&done, 4, 1, out);
+    return 0;
+}
+
 /* trace: the step input followed by int32 ndump, int32 dump_after[ndump]
  * (ascending coarse-step counts), int32 periodic[3], int32 extent0[3]
  * (level-0 box).  Output: seconds, then the levels after each listed step,
@@ -336,7 +364,7 @@ int run_trace(Reader &in, FILE *out)
 int main(int argc, char **argv)
 {
     if (argc != 4) {
-        fprintf(stderr, "usage: %s step|pstep|trace|morton <in.bin> <out.bin>\n", argv[0]);
+        fprintf(stderr, "usage: %s step|pstep|trace|tecplot|morton <in.bin> <out.bin>\n", argv[0]);
         return 2;
     }
     std::ofstream devnull("/dev/null");
@@ -349,8 +377,9 @@ int main(int argc, char **argv)
     int rc;
     try {
         const std::string mode = argv[1];
-        rc = mode == "morton"  ? run_morton(rd, fout)
-             : mode == "trace" ? run_trace(rd, fout)
+        rc = mode == "morton"    ? run_morton(rd, fout)
+             : mode == "trace"   ? run_trace(rd, fout)
+             : mode == "tecplot" ? run_tecplot(rd, fout)
              : run_step(rd, fout, mode == "pstep");
     } catch (const std::exception &e) {
         fprintf(stderr, "harness: %s\n", e.what());

@@ -6,6 +6,7 @@ Run here, where the reference checkout exists:
     python tests/golden/gen_golden.py            # short cases + Morton answers
     python tests/golden/gen_golden.py --trace [name ...]   # TRACE_CASES
     python tests/golden/gen_golden.py --morton             # neighbour blocks
+    python tests/golden/gen_golden.py --tecplot            # the reference's flow file
 The outputs are small .npz files; the GPU box only reads them.  The trace
 cases run one harness process each, in parallel; cfg1's 1000 coarse steps
 take about half an hour of one core.
@@ -107,6 +108,21 @@ def morton_blocks():
         print("morton blocks", q, L, keys.size, os.path.getsize(path), "bytes")
 
 
+def tecplot_golden():
+    """The reference's own flow file (IO_TECPLOTH::write, tecplot.cpp:16-176)
+    after 3 coarse steps of the sphere_q19_fh_refinit case, written at
+    iteration 7."""
+    import oracle as O
+    spec = GOLDEN_CASES["sphere_q19_fh_refinit"]
+    case = build_case(spec)
+    name, text = O.run_harness_tecplot(case, 3, 7)
+    meta = dict(case="sphere_q19_fh_refinit", steps=3, iteration=7, file=name, set_digest=set_digest(case))
+    path = os.path.join(HERE, "tecplot_sphere_q19_fh_refinit.npz")
+    np.savez_compressed(path, text=np.frombuffer(text.encode(), np.uint8),
+                        meta=np.frombuffer(json.dumps(meta).encode(), np.uint8))
+    print("tecplot", name, os.path.getsize(path), "bytes")
+
+
 SAMPLE = 64
 
 
@@ -163,6 +179,8 @@ def gen_trace(name):
 if __name__ == "__main__":
     if "--morton" in sys.argv:
         morton_blocks()
+    elif "--tecplot" in sys.argv:
+        tecplot_golden()
     elif "--trace" in sys.argv:
         from concurrent.futures import ProcessPoolExecutor
         import multiprocessing as mp

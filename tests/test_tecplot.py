@@ -1,6 +1,9 @@
 """Flow output in the reference's Tecplot format: the vectorised writer
 against a loop-by-loop restatement of IO_TECPLOTH::write (tecplot.cpp:16-176)
-on small multi-level meshes, and the file's structure."""
+on small multi-level meshes, the file's structure, and the file the
+reference's own IO_TECPLOTH::write produced (golden)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -100,3 +103,71 @@ def test_file_structure(tmp_path):
     assert np.allclose(d, want[:, None, :] * size[None, :, None])
     # no two nodes at the same point
     assert np.unique(xyz.T, axis=0).shape[0] == n
+
+
+def _parse_flow(text):
+    """(nodes, elements) of a FEBRICK flow file: elements keyed by the
+    coordinate strings of their 8 corners in connectivity order, with their
+    U, V, W strings."""
+    lines = text.splitlines()
+    head = lines[2]
+    nn = int(head.split("NODES=")[1].split(",")[0])
+    ne = int(head.split("ELEMENTS=")[1].split(",")[0])
+    body = lines[3:]
+    x, y, z = body[:nn], body[nn:2 * nn], body[2 * nn:3 * nn]
+    u = body[3 * nn:3 * nn + ne]
+    v = body[3 * nn + ne:3 * nn + 2 * ne]
+    w = body[3 * nn + 2 * ne:3 * nn + 3 * ne]
+    conn = body[3 * nn + 3 * ne:]
+    assert len(conn) == ne
+    nodes = [(x[i], y[i], z[i]) for i in range(nn)]
+    elems = {}
+    for j, row in enumerate(conn):
+        corners = tuple(nodes[int(t) - 1] for t in row.split())
+        assert corners not in elems
+        elems[corners] = (u[j], v[j], w[j])
+    return lines[:3], nodes, elems
+
+
+def test_flow_file_matches_reference_output():
+    """write_flow against the file the reference's own IO_TECPLOTH::write
+    produced (tests/golden/tecplot_sphere_q19_fh_refinit.npz, 3 coarse steps
+    of the 2-level FH sphere, iteration 7): same header and counts, the same
+    set of node coordinates, and every element -- its 8 corner coordinates in
+    connectivity order -- with the same velocity text.  The reference built
+    with hash maps visits cells in hash order, so nodes and elements are
+    compared as sets, not by position."""
+    import json
+
+    from golden_cases import build_case
+    from helpers import GOLDEN_DIR, run_oracle
+    from mortontrie_amr_b200.tecplot import write_flow
+    z = np.load(os.path.join(GOLDEN_DIR, "tecplot_sphere_q19_fh_refinit.npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    ref_text = bytes(z["text"]).decode()
+    from golden_cases import GOLDEN_CASES
+    case = build_case(GOLDEN_CASES[meta["case"]])
+    oc = run_oracle(case, meta["steps"])
+
+    class View:
+        L = case.max_level
+
+        def keys(self, l):
+            g = oc.get(l)
+            return g["keys"], g["tags"]
+
+        def macros(self, l):
+            g = oc.get(l)
+            return g["rho"], np.ascontiguousarray(g["u"].T)
+
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        path = write_flow(View(), td, meta["iteration"])
+        assert os.path.basename(path) == meta["file"]
+        with open(path) as fh:
+            ours = fh.read()
+    h1, n1, e1 = _parse_flow(ours)
+    h0, n0, e0 = _parse_flow(ref_text)
+    assert h1 == h0
+    assert sorted(n1) == sorted(n0)
+    assert e1 == e0
