@@ -57,6 +57,8 @@ REF_TUS = [
     "ComplexBoundary_Manager.cpp",
     "Morton_Assist.cpp",
     "tecplot.cpp",
+    "Lat_Voxelize.cpp",
+    "Shape.cpp",
 ]
 HARNESS_VARIANTS = [(19, 0), (19, 1), (19, 2), (19, 3), (27, 0), (27, 1), (27, 2), (27, 3)]
 # (Q, L) of the harnesses built with the periodic find_neighbor wrap

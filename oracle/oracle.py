@@ -309,6 +309,26 @@ def run_harness_tecplot(case, nsteps, iteration, init=None, timeout=600):
             return names[0], fh.read()
 
 
+def run_harness_dis(q, L, tris, keys, centers, timeout=600):
+    """Wall distances of the finest-level cells `keys` (centres [n][3], coarse
+    units) over the triangles [m][3][3] (coarse units) by the reference's own
+    Lat_Manager::compute_distance; returns [n][q - 1], -1 where free."""
+    import build
+    exe = build.build_refharness(q, L)
+    tris = np.ascontiguousarray(tris, np.float64).reshape(-1, 9)
+    keys = np.ascontiguousarray(keys, np.uint64)
+    centers = np.ascontiguousarray(centers, np.float64).reshape(-1, 3)
+    rec = np.zeros(keys.size, dtype=[("k", "<u8"), ("c", "<f8", (3,))])
+    rec["k"] = keys
+    rec["c"] = centers
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as fh:
+            fh.write(struct.pack("<q", tris.shape[0]) + tris.tobytes() + struct.pack("<q", keys.size) + rec.tobytes())
+        subprocess.run([exe, "dis", fin, fout], check=True, timeout=timeout)
+        return np.fromfile(fout, np.float64).reshape(keys.size, q - 1)
+
+
 def start_harness(case, nsteps, workdir, tag, nwarm=0, init=None):
     """Launch one harness process without waiting (CPU baseline runs several
     in parallel, one per core); returns (Popen, output path).  A mesh with

@@ -17,6 +17,7 @@
  *        harness pstep <in.bin> <out.bin>      (step with periodic axes)
  *        harness trace <in.bin> <out.bin>      (state dumps after chosen steps)
  *        harness tecplot <in.bin> <out.bin>    (the reference's flow file after the steps)
+ *        harness dis <in.bin> <out.bin>        (wall distances by compute_distance)
  *        harness morton <in.bin> <out.bin>     (neighbour-key known answers)
  *
  * Built with -DHC_PERIODIC the harness includes a generated copy of
@@ -63,6 +64,7 @@
 #undef protected
 #include "Grid_Manager.h"
 #include "Solid_Manager.h"
+#include "Shape.h"
 
 /* static members whose definitions live in translation units the harness
  * does not build (Grid_Manager.cpp, Lat_Manager.cpp, Obj_Manager.cpp ...) */
@@ -310,6 +312,41 @@ int run_step(Reader &in, FILE *out, bool periodic = false)
     return 0;
 }
 
+/* dis: wall distances of chosen finest-level cells by the reference's own
+ * Lat_Manager::compute_distance (Lat_Voxelize.cpp:1252-1285, through
+ * Shape::intersect_line_with_triangle, Shape.cpp:809-843) over every given
+ * triangle, the call Lat_Voxelize.cpp:848 makes for each triangle near an
+ * immersed-boundary cell.  Input: int64 ntri, ntri x 9 doubles (coarse-cell
+ * units), int64 ncell, per cell uint64 key + 3 doubles (its centre).
+ * Output: per cell Q - 1 doubles, -1 where no link crosses. */
+int run_dis(Reader &in, FILE *out)
+{
+    Morton_Assist ma;
+    setup_morton(ma);
+    Lat_Manager *lm = new Lat_Manager();
+    Lat_Manager::pointer_me = lm;
+    for (unsigned l = 0; l <= C_max_level; ++l) lm->dx[l] = C_dx / (double)two_power_n(l);
+    const int64_t nt = in.get<int64_t>();
+    std::vector<Solid_Face> tris((size_t)nt);
+    for (auto &t : tris) {
+        auto v = in.vec<double>(9);
+        t.vertex1.x = v[0]; t.vertex1.y = v[1]; t.vertex1.z = v[2];
+        t.vertex2.x = v[3]; t.vertex2.y = v[4]; t.vertex2.z = v[5];
+        t.vertex3.x = v[6]; t.vertex3.y = v[7]; t.vertex3.z = v[8];
+    }
+    const int64_t nc = in.get<int64_t>();
+    for (int64_t i = 0; i < nc; ++i) {
+        const uint64_t k = in.get<uint64_t>();
+        auto c = in.vec<double>(3);
+        for (const auto &t : tris) lm->compute_distance(t, K(k), D_vec(c[0], c[1], c[2]));
+        double row[C_Q - 1];
+        auto it = lm->dis.find(K(k));
+        for (int j = 0; j < C_Q - 1; ++j) row[j] = it == lm->dis.end() ? -1.0 : it->second[j];
+        fwrite(row, 8, C_Q - 1, out);
+    }
+    return 0;
+}
+
 /* tecplot: the step input followed by int32 iter; after the steps the
  * reference's IO_TECPLOTH::write(iter) (tecplot.cpp:16-176) writes
  * output/sphereFlow_<iter * CF_T[0]>.dat under the working directory. */
@@ -364,7 +401,7 @@ int run_trace(Reader &in, FILE *out)
 int main(int argc, char **argv)
 {
     if (argc != 4) {
-        fprintf(stderr, "usage: %s step|pstep|trace|tecplot|morton <in.bin> <out.bin>\n", argv[0]);
+        fprintf(stderr, "usage: %s step|pstep|trace|tecplot|dis|morton <in.bin> <out.bin>\n", argv[0]);
         return 2;
     }
     std::ofstream devnull("/dev/null");
@@ -380,6 +417,7 @@ int main(int argc, char **argv)
         rc = mode == "morton"    ? run_morton(rd, fout)
              : mode == "trace"   ? run_trace(rd, fout)
              : mode == "tecplot" ? run_tecplot(rd, fout)
+             : mode == "dis"     ? run_dis(rd, fout)
              : run_step(rd, fout, mode == "pstep");
     } catch (const std::exception &e) {
         fprintf(stderr, "harness: %s\n", e.what());

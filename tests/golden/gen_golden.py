@@ -7,6 +7,7 @@ Run here, where the reference checkout exists:
     python tests/golden/gen_golden.py --trace [name ...]   # TRACE_CASES
     python tests/golden/gen_golden.py --morton             # neighbour blocks
     python tests/golden/gen_golden.py --tecplot            # the reference's flow file
+    python tests/golden/gen_golden.py --dis                # STL link wall distances
 The outputs are small .npz files; the GPU box only reads them.  The trace
 cases run one harness process each, in parallel; cfg1's 1000 coarse steps
 take about half an hour of one core.
@@ -123,6 +124,43 @@ def tecplot_golden():
     print("tecplot", name, os.path.getsize(path), "bytes")
 
 
+DIS_CASES = {
+    # off-centre icospheres: links cross faces, edges and vertices at generic angles
+    "dis_icosphere_q19": dict(q=19, center=(12.3, 8.1, 7.9), radius=2.2, sub=3),
+    "dis_icosphere_q27": dict(q=27, center=(12.3, 8.1, 7.9), radius=2.2, sub=3),
+}
+
+
+def dis_cells(spec, mesh):
+    """The finest fluid cells within 1.2 coarse cells of the sphere's surface:
+    every cell with a link across it and a shell of cells without one."""
+    from mortontrie_amr_b200.lattice import cell_coords
+    L = mesh.spec.max_level
+    keys = mesh.levels[L]["lat_f"]
+    x, y, z = cell_coords(L, L, keys)
+    c = (np.stack([x, y, z], 1) + 0.5) / 2 ** L
+    r = np.linalg.norm(c - np.asarray(spec["center"]), axis=1)
+    sel = np.abs(r - spec["radius"]) < 1.2
+    return keys[sel], c[sel]
+
+
+def dis_golden():
+    """Per link wall distances of the cells near an STL sphere by the
+    reference's own Lat_Manager::compute_distance (Lat_Voxelize.cpp
+    :1252-1285) over every triangle, in coarse units as the reference stores
+    the surface."""
+    import oracle as O
+    from golden_cases import dis_mesh
+    for name, spec in DIS_CASES.items():
+        mesh, tris = dis_mesh(spec)
+        keys, centers = dis_cells(spec, mesh)
+        ref = O.run_harness_dis(spec["q"], mesh.spec.max_level, tris, keys, centers)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, keys=keys, dis=ref,
+                            meta=np.frombuffer(json.dumps(spec).encode(), np.uint8))
+        print("dis", name, keys.size, int((ref != -1).sum()), os.path.getsize(path), "bytes")
+
+
 SAMPLE = 64
 
 
@@ -181,6 +219,8 @@ if __name__ == "__main__":
         morton_blocks()
     elif "--tecplot" in sys.argv:
         tecplot_golden()
+    elif "--dis" in sys.argv:
+        dis_golden()
     elif "--trace" in sys.argv:
         from concurrent.futures import ProcessPoolExecutor
         import multiprocessing as mp

@@ -73,3 +73,13 @@ def build_case(spec) -> Case:
     p = CaseParams(q=spec["q"], collision=spec["collision"], ib_method=spec["ib"], bc_mode="neq", nu=spec["nu"],
                    u_bc=(spec["u"], 0.0, 0.0), u_ref=spec["u"])
     return Case(build_mesh(ms), p)
+
+
+def dis_mesh(spec):
+    """The two-level STL sphere mesh of a wall-distance golden and its
+    triangles (coarse units)."""
+    from mortontrie_amr_b200.stl import icosphere
+    tris = icosphere(spec["center"], spec["radius"], spec["sub"])
+    mesh = build_mesh(MeshSpec(q=spec["q"], max_level=1, coarse=(32, 16, 16), refine=[((6, 4, 4), (18, 12, 12))],
+                               boundary=("bc", "periodic", "periodic"), surface=tris))
+    return mesh, tris
