@@ -379,10 +379,10 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None, tune=True):
         if _shift_of_label(st):
             out[st] = {"storage_shift": SHIFT_NOTE[_shift_of_label(st)]}
         mgr.fluidSimulate(warmup)
-        forms = None
+        forms = form_ms = None
         if schedule == "fused" and tune:
             # the project autotuner picks each brick level's pass form (outside the timed region)
-            forms, _ = mgr.tune_bricks()
+            forms, form_ms = mgr.tune_bricks()
         mgr.fluidSimulate(1)  # every run: captures the tuned step's graph before the timing
         torch.cuda.synchronize()
         mgr.reset_force()
@@ -404,6 +404,8 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None, tune=True):
                    "ms_per_coarse_step": round(1e3 * secs / steps, 3)}
         if forms is not None:
             out[st]["brick_forms_per_level"] = [int(v) for v in forms]
+            # ms per launch of each form (rows: levels; -1: not timed)
+            out[st]["brick_form_ms"] = [[round(float(t), 4) for t in row] for row in form_ms]
         mgr.close()
     ref = res.get("f64")
     for st, _, _ in runs:

@@ -261,19 +261,28 @@ int mt_case_status(mt_ctx *ctx, int32_t case_id);
  * candidate the kernel is built for (the paired 16-bit LBGK kernel: 128 and
  * 256 only; the other slots are left unwritten). */
 int mt_case_tune(mt_ctx *ctx, int32_t case_id, int32_t *best_block, float *ms_per_candidate);
-/* Project autotuner of the multi-level fused brick pass (no reference
- * counterpart): times each brick level's pass in each of its forms (0: one
- * cell per lane step at 8 resident 128-thread blocks per SM; 3: the lane's two
- * cells in one unrolled sequence, so that the second cell's gathers overlap
- * the first cell's collision, at 6 blocks; for FP32 / FP16 / BF16 storage
- * also 1: the two cells together in packed FP32 pair arithmetic at 4 blocks,
- * and 2: form 0 at 6 blocks with more registers per thread) on the case's
- * own bricks, without changing the state, and keeps the fastest per level
- * for the fused steps that follow.  variant[max_level + 1]: the form kept
- * (-1 for a level without bricks); ms[4 * (max_level + 1)]: ms per launch of
- * each form (-1 if not timed).  Either may be NULL.  Synchronises the
- * stream; the case keeps its schedule. */
+/* Forms of the multi-level fused brick pass (no reference counterpart):
+ * 0: one cell per lane step at 8 resident 128-thread blocks per SM;
+ * 3: the lane's two cells in one unrolled sequence, so that the second
+ *    cell's gathers overlap the first cell's collision, at 6 blocks;
+ * for FP32 / FP16 / BF16 storage also
+ * 1: the two cells together in packed FP32 pair arithmetic at 4 blocks,
+ * 2: form 0 at 6 blocks with more registers per thread.
+ * Forms 0, 2 and 3 compute the same values bit for bit. */
+#define MT_BRICK_FORMS 4
+/* Project autotuner of the multi-level fused brick pass: times each brick
+ * level's pass in each of its forms on the case's own bricks, without
+ * changing the state, and keeps the fastest per level for the fused steps
+ * that follow.  variant[max_level + 1]: the form kept (-1 for a level without
+ * bricks); ms[MT_BRICK_FORMS * (max_level + 1)]: ms per launch of each form
+ * (-1 if not timed).  Either may be NULL.  Synchronises the stream; the case
+ * keeps its schedule. */
 int mt_case_tune_bricks(mt_ctx *ctx, int32_t case_id, int32_t *variant, float *ms);
+/* Sets the brick pass form of each level (form[max_level + 1]; a negative
+ * entry keeps the level's form), e.g. one a previous mt_case_tune_bricks
+ * picked.  MT_ERR_ARG for a form outside 0..MT_BRICK_FORMS-1 or one the
+ * storage does not have (FP64: 0 and 3). */
+int mt_case_set_brick_forms(mt_ctx *ctx, int32_t case_id, const int32_t *form);
 /* Schedule of mt_step for a multi-level case (no reference counterpart):
  * MT_SCHED_PHASES (default) issues the reference's phases one pass each;
  * MT_SCHED_FUSED keeps a second post-collision buffer per level and streams

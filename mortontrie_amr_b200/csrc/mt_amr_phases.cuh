@@ -737,46 +737,23 @@ __global__ void k_pull_copy(const int32_t *__restrict__ list, int64_t nl, int64_
 // When `macros` is set (the level's last substep of the coarse step) the
 // macros of the streamed f are written too: they are what the all-level
 // calculateMacros at the end of the coarse step computes.
-// one cell (local Morton index m) of brick b in the fused brick pass
-template <int Q, class S, int COLL>
-__device__ __forceinline__ void brick_cell(int64_t b, int m, const int32_t *s_idx, const uint8_t *__restrict__ bcls,
-                                           uint32_t n, int textbook, bool full, const S *__restrict__ fcol,
-                                           S *__restrict__ f, S *__restrict__ fnext, double tau,
-                                           typename Store<S>::C *__restrict__ rho,
-                                           typename Store<S>::C *__restrict__ u, int macros, int fall,
-                                           long long *__restrict__ acc, const Shift &sh)
+// The part of a brick cell's pass after its gather: v holds the streamed f
+// of cell i (class cls), present(k) says whether link k had a source cell
+// (a missing one keeps f, which is then not stored again).
+template <int Q, class S, int COLL, class P>
+__device__ __forceinline__ void brick_finish(uint32_t i, int cls, const S *v, P present, uint32_t n,
+                                             S *__restrict__ f, S *__restrict__ fnext, double tau,
+                                             typename Store<S>::C *__restrict__ rho,
+                                             typename Store<S>::C *__restrict__ u, int macros, int fall,
+                                             long long *__restrict__ acc, const Shift &sh)
 {
     using T = Store<S>;
     using C = typename T::C;
-    const int lx = (m & 1) | ((m >> 2) & 2), ly = ((m >> 1) & 1) | ((m >> 3) & 2),
-              lz = ((m >> 2) & 1) | ((m >> 4) & 2);
-    const int base = (lx + 1) + 6 * (ly + 1) + 36 * (lz + 1);
-    const int32_t ii = s_idx[base];
-    if (ii < 0) return;
-    const int cls = __ldg(bcls + 64 * b + m);
-    if (!cls) return;
-    const uint32_t i = (uint32_t)ii;
-    int32_t src[Q];
-#pragma unroll
-    for (int k = 1; k < Q; ++k) {
-        const int off = ex(k) + 6 * ey(k) + 36 * ez(k);
-        src[k] = s_idx[base + (textbook ? -off : off)];
-    }
-    S v[Q];
-    v[0] = fcol[i];
-    if (full) {
-#pragma unroll
-        for (int k = 1; k < Q; ++k) v[k] = fcol[(uint32_t)k * n + (uint32_t)src[k]];
-    } else {
-#pragma unroll
-        for (int k = 1; k < Q; ++k)
-            v[k] = src[k] >= 0 ? fcol[(uint32_t)k * n + (uint32_t)src[k]] : f[(uint32_t)k * n + i];
-    }
     if (cls != 1 || fall) {
         f[i] = v[0];
 #pragma unroll
         for (int k = 1; k < Q; ++k)
-            if (full || src[k] >= 0) f[(uint32_t)k * n + i] = v[k];
+            if (present(k)) f[(uint32_t)k * n + i] = v[k];
     }
     if (cls == 2) {
 #pragma unroll
@@ -816,6 +793,43 @@ __device__ __forceinline__ void brick_cell(int64_t b, int m, const int32_t *s_id
         u[n + i] = y;
         u[2 * n + i] = z;
     }
+}
+
+// one cell (local Morton index m) of brick b in the fused brick pass
+template <int Q, class S, int COLL>
+__device__ __forceinline__ void brick_cell(int64_t b, int m, const int32_t *s_idx, const uint8_t *__restrict__ bcls,
+                                           uint32_t n, int textbook, bool full, const S *__restrict__ fcol,
+                                           S *__restrict__ f, S *__restrict__ fnext, double tau,
+                                           typename Store<S>::C *__restrict__ rho,
+                                           typename Store<S>::C *__restrict__ u, int macros, int fall,
+                                           long long *__restrict__ acc, const Shift &sh)
+{
+    const int lx = (m & 1) | ((m >> 2) & 2), ly = ((m >> 1) & 1) | ((m >> 3) & 2),
+              lz = ((m >> 2) & 1) | ((m >> 4) & 2);
+    const int base = (lx + 1) + 6 * (ly + 1) + 36 * (lz + 1);
+    const int32_t ii = s_idx[base];
+    if (ii < 0) return;
+    const int cls = __ldg(bcls + 64 * b + m);
+    if (!cls) return;
+    const uint32_t i = (uint32_t)ii;
+    int32_t src[Q];
+#pragma unroll
+    for (int k = 1; k < Q; ++k) {
+        const int off = ex(k) + 6 * ey(k) + 36 * ez(k);
+        src[k] = s_idx[base + (textbook ? -off : off)];
+    }
+    S v[Q];
+    v[0] = fcol[i];
+    if (full) {
+#pragma unroll
+        for (int k = 1; k < Q; ++k) v[k] = fcol[(uint32_t)k * n + (uint32_t)src[k]];
+    } else {
+#pragma unroll
+        for (int k = 1; k < Q; ++k)
+            v[k] = src[k] >= 0 ? fcol[(uint32_t)k * n + (uint32_t)src[k]] : f[(uint32_t)k * n + i];
+    }
+    brick_finish<Q, S, COLL>(i, cls, v, [&](int k) { return full || src[k] >= 0; }, n, f, fnext, tau, rho, u,
+                             macros, fall, acc, sh);
 }
 
 // one warp's brick b (see above); s_idx is the warp's 216-entry shared table;
@@ -2088,11 +2102,11 @@ int AmrOps<S>::batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, i
 }
 
 // ---- the brick pass autotuner (mt_case_tune_bricks) ----------------------
-// Each brick level's fused pass is timed in each of its forms (one cell per
-// lane step at 8 resident blocks per SM; two cells with packed FP32 pairs;
-// one cell at 6 blocks with more registers; the lane's two cells in one
-// unrolled sequence at 6 blocks; FP64 has the first and the last) on the
-// case's own bricks: one warm-up and three timed launches per form, CUDA
+// Each brick level's fused pass is timed in each of its forms (0 one cell per
+// lane step at 8 resident blocks per SM; 1 two cells with packed FP32 pairs;
+// 2 one cell at 6 blocks with more registers; 3 the lane's two cells in one
+// unrolled sequence at 6 blocks; FP64 has forms 0 and 3) on the case's own
+// bricks: one warm-up and three timed launches per form, CUDA
 // events on the case's stream.  The passes read the current post-collision
 // buffer and write the next collision into a scratch buffer; the f they
 // store is what the last real pass stored, and no macros are written, so the
@@ -2105,7 +2119,8 @@ int AmrOps<S>::tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms)
         if (c.lv[l].bricks) nmax = std::max(nmax, c.lv[l].n);
     for (int l = 0; l <= c.d.max_level; ++l) {
         if (variant) variant[l] = -1;
-        if (ms) ms[4 * l] = ms[4 * l + 1] = ms[4 * l + 2] = ms[4 * l + 3] = -1.f;
+        if (ms)
+            for (int v = 0; v < MT_BRICK_FORMS; ++v) ms[MT_BRICK_FORMS * l + v] = -1.f;
     }
     if (!nmax) return MT_OK;
     S *scratch = nullptr;
@@ -2117,11 +2132,10 @@ int AmrOps<S>::tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms)
     for (int l = 0; l <= c.d.max_level && !rc; ++l) {
         Level &lv = c.lv[l];
         if (!lv.bricks || !lv.nbrick) continue;
-        const int nform = 4;
         float best = 0.f;
         int pick = lv.brick_variant;
-        for (int v = 0; v < nform && !rc; ++v) {
-            if (!Store<S>::shifted && (v == 1 || v == 2)) continue;  // FP64: forms 0 and 3
+        for (int v = 0; v < MT_BRICK_FORMS && !rc; ++v) {
+            if (!Store<S>::shifted && v != 0 && v != 3) continue;  // FP64: forms 0 and 3
             auto launch = [&]() {
                 if (c.d.q == 19)
                     brick_launch<19, S>(c, l, v, ctx.stream, scratch, 0, 0, nullptr);
@@ -2142,7 +2156,7 @@ int AmrOps<S>::tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms)
             cudaEventElapsedTime(&t, e0, e1);
             t /= 3.f;
             ctx.launches += 4;
-            if (ms) ms[4 * l + v] = t;
+            if (ms) ms[MT_BRICK_FORMS * l + v] = t;
             if (v == 0 || t < best) {  // form 0 is always timed first
                 best = t;
                 pick = v;

@@ -1168,6 +1168,30 @@ int mt_case_tune_bricks(mt_ctx *h, int32_t id, int32_t *variant, float *ms)
     return MT_OK;
 }
 
+int mt_case_set_brick_forms(mt_ctx *h, int32_t id, const int32_t *form)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense) return set_err(ctx, MT_ERR_STATE, "brick forms belong to multi-level cases");
+    if (!form) return set_err(ctx, MT_ERR_ARG, "form is NULL");
+    const bool f64 = c->d.storage == MT_STORE_F64;
+    for (int l = 0; l <= c->d.max_level; ++l) {
+        const int v = form[l];
+        if (v >= MT_BRICK_FORMS || (v >= 0 && f64 && v != 0 && v != 3))
+            return set_err(ctx, MT_ERR_ARG, "brick form " + std::to_string(v) + " is not available for this storage");
+    }
+    for (int l = 0; l <= c->d.max_level; ++l)
+        if (form[l] >= 0) c->lv[l].brick_variant = form[l];
+    // the captured steps bake the kernel choice in
+    for (int p = 0; p < 2; ++p) {
+        if (c->fgraph[p]) cudaGraphExecDestroy(c->fgraph[p]);
+        c->fgraph[p] = nullptr;
+    }
+    return MT_OK;
+}
+
 int mt_get_force(mt_ctx *h, int32_t id, double *out4)
 {
     Case *c;

@@ -266,7 +266,7 @@ template <class S> struct AmrOps {
     static int reduce(Ctx &ctx, Case &c, double *d_out);
     // time every form of every brick level's fused pass (into scratch, state
     // untouched) and keep the fastest in Level::brick_variant;
-    // ms[4 * level + form], variant[level] (-1: no brick pass on the level)
+    // ms[MT_BRICK_FORMS * level + form], variant[level] (-1: no brick pass on the level)
     static int tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms);
     // batched brick pass (descriptor in device memory, total bricks known on the host)
     static int batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total, const Shift &sh);

@@ -36,12 +36,14 @@ EXPORTS = [
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
     "mt_case_generate", "mt_case_set_surface", "mt_marker_record", "mt_marker_done", "mt_case_force_async",
     "mt_case_force_copied", "mt_set_priority", "mt_case_remap", "mt_case_status_copied", "mt_case_tune_bricks",
+    "mt_case_set_brick_forms",
 ]
 
 
 SCHEDULES = {"phases": 0, "fused": 1, "fused_lists": 2}
 SCALINGS = {"reference": 0, "standard": 1}
 ITIMES = {"reference": 0, "hold": 1, "extrap": 2}
+BRICK_FORMS = 4  # MT_BRICK_FORMS
 
 
 class MTError(RuntimeError):
@@ -121,7 +123,7 @@ def lib():
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
             "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64],
             "mt_marker_record": [vp, i64p], "mt_marker_done": [vp, i64, i32p], "mt_case_force_async": [vp, i32],
-            "mt_case_force_copied": [vp, i32, dp], "mt_case_status_copied": [vp, i32], "mt_case_tune_bricks": [vp, i32, i32p, C.POINTER(C.c_float)], "mt_set_priority": [vp, i32], "mt_case_remap": [vp, i32, i32, i64p], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
+            "mt_case_force_copied": [vp, i32, dp], "mt_case_status_copied": [vp, i32], "mt_case_tune_bricks": [vp, i32, i32p, C.POINTER(C.c_float)], "mt_case_set_brick_forms": [vp, i32, i32p], "mt_set_priority": [vp, i32], "mt_case_remap": [vp, i32, i32, i64p], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
             "mt_apply_bc": [vp, i32], "mt_apply_bc_face": [vp, i32, i32], "mt_ib_treat": [vp, i32], "mt_lbm_kernel": [vp, i32, i32],
             "mt_step": [vp, i32, i32], "mt_get_force": [vp, i32, dp], "mt_reset_force": [vp, i32],
@@ -471,14 +473,22 @@ class LBM_Manager:
     def tune_bricks(self):
         """Time every form of every brick level's fused pass (0 one cell per
         lane step, 1 a packed pair, 2 one cell with more registers, 3 the
-        lane's two cells unrolled together) and keep
-        the fastest per level; returns (form per level, -1 without bricks;
-        ms per launch [level][form], -1 where not timed)."""
+        lane's two cells unrolled together) and keep the fastest per level; returns (form per level, -1
+        without bricks; ms per launch [level][form], -1 where not timed)."""
         v = np.zeros(self.L + 1, np.int32)
-        ms = np.zeros((self.L + 1, 4), np.float32)
+        ms = np.zeros((self.L + 1, BRICK_FORMS), np.float32)
         self.ctx.check(lib().mt_case_tune_bricks(self.ctx.h, self.id, _ptr(v, C.c_int32), _ptr(ms, C.c_float)),
                        "mt_case_tune_bricks")
         return v, ms
+
+    def set_brick_forms(self, forms):
+        """Run each level's brick pass in the given form (a negative entry
+        keeps the level's form); FP64 storage has forms 0 and 3."""
+        v = np.ascontiguousarray(forms, np.int32)
+        if v.shape != (self.L + 1,):
+            raise ValueError(f"one form per level: {self.L + 1} entries")
+        self.ctx.check(lib().mt_case_set_brick_forms(self.ctx.h, self.id, _ptr(v, C.c_int32)),
+                       "mt_case_set_brick_forms")
 
     def reduce_levels(self):
         """FP64 device sums per level (rows 0..L) and volume-weighted over all

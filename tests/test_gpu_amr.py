@@ -455,7 +455,8 @@ def test_brick_tuner_keeps_the_trajectory(ctx, storage):
     v, ms = a.tune_bricks()
     assert (v >= 0).any() and (ms.max() > 0)
     if storage == "f64":
-        assert set(v[v >= 0]) <= {0, 3}  # FP64 has the one-cell forms only
+        assert set(v[v >= 0]) <= {0, 3}  # FP64 has forms 0 and 3 only
+        assert (ms[:, [1, 2]] == -1).all()
     a.fluidSimulate(3)
     b.fluidSimulate(3)
     ctx.synchronize()
@@ -468,6 +469,65 @@ def test_brick_tuner_keeps_the_trajectory(ctx, storage):
             assert rel_err(ca, cb) < 1e-2, l
     a.close()
     b.close()
+
+
+def _forms_case(family):
+    from mortontrie_amr_b200.case import df_sphere_case, nested_sphere_case, sphere_case
+    if family == "cumulant":
+        return nested_sphere_case(coarse=(128, 64, 64), max_level=2, center=(40, 32, 32), radius=2.0,
+                                  half_widths=(4.0, 2.5), re=50.0)
+    if family == "df":
+        return df_sphere_case(radius=3, max_level=2, re=50.0, oscillating=True, period=200)
+    return sphere_case(coarse=(128, 64, 64), refine=[((36, 24, 24), (60, 40, 40))], center=(48, 32, 32), radius=3.0)
+
+
+@pytest.mark.parametrize("family,storage", [("cumulant", "f16"), ("cumulant", "f32"), ("cumulant", "bf16"),
+                                            ("df", "f16"), ("df", "f32"), ("lbgk", "f16"), ("lbgk", "bf16")])
+def test_brick_forms_compute_the_same_values(ctx, family, storage):
+    """The one-cell forms of the fused brick pass (0; 2 with more registers;
+    3 with the lane's two cells unrolled) share the per-cell arithmetic: a
+    case run in each form stays equal to form 0 bit for bit (populations,
+    macros, force), boundary cells, partial bricks, the IB level and the
+    direct-forcing band included."""
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    case = _forms_case(family)
+    L = case.max_level
+    runs = {}
+    for form in (0, 2, 3):
+        m = LBM_Manager(ctx, case, storage, schedule="fused")
+        m.set_brick_forms([form] * (L + 1))
+        m.fluidSimulate(5)
+        runs[form] = m
+    ctx.synchronize()
+    for form in (2, 3):
+        _same_state(runs[0], runs[form], L)
+        assert np.array_equal(runs[0].force(), runs[form].force()), form
+    for m in runs.values():
+        m.close()
+
+
+def test_brick_forms_fp64_and_arguments(ctx):
+    """FP64 runs forms 0 and 3 (equal bit for bit); the others, and forms out
+    of range, are refused with MT_ERR_ARG."""
+    from mortontrie_amr_b200.lbm import LBM_Manager, MTError
+    case = _nested_small()
+    L = case.max_level
+    a = LBM_Manager(ctx, case, "f64", schedule="fused")
+    b = LBM_Manager(ctx, case, "f64", schedule="fused")
+    b.set_brick_forms([3] * (L + 1))
+    for bad in (1, 2, 4):
+        with pytest.raises(MTError, match="MT_ERR_ARG"):
+            b.set_brick_forms([bad] * (L + 1))
+    a.fluidSimulate(3)
+    b.fluidSimulate(3)
+    ctx.synchronize()
+    _same_state(a, b, L)
+    c = LBM_Manager(ctx, case, "f16", schedule="fused")
+    with pytest.raises(MTError, match="MT_ERR_ARG"):
+        c.set_brick_forms([4] * (L + 1))
+    c.set_brick_forms([-1] * (L + 1))  # keeps every level's form
+    for m in (a, b, c):
+        m.close()
 
 
 @pytest.mark.parametrize("q,L", [(19, 1), (19, 3), (27, 3)])
