@@ -294,7 +294,10 @@ MT_HD void cumulant_from_moments(R *m, R rho, R ux, R uy, R uz, R omega1, R *out
     const R x2 = (1 - om1) * (c200 - c002) - 3 * rho * (1 - om1 * R(0.5)) * (ux2 * dxu - uz2 * dzw);
     const R x3 = k000 * om2 + (1 - om2) * (c200 + c020 + c002) -
                  3 * rho * (1 - om2 * R(0.5)) * (ux2 * dxu + uy2 * dyv + uz2 * dzw);
-    c200 = (x1 + x2 + x3) / 3;
+    if constexpr (std::is_same<R, double>::value)
+        c200 = (x1 + x2 + x3) / 3;  // the reference's expression
+    else
+        c200 = (x1 + x2 + x3) * R(1.0 / 3.0);
     c020 = c200 - x1;
     c002 = c200 - x2;
 
