@@ -829,10 +829,63 @@ def cpu_reference_run(nprocs, steps, warmup):
     return mlups, kind, nprocs, sample
 
 
+def _stepped_updates(case):
+    """Cell updates of one coarse step: every level's collide set (lat_f and
+    overlap_F2C) times its 2^l substeps."""
+    m = case.mesh
+    return sum((m.levels[l]["lat_f"].size + m.levels[l]["overlap_F2C"].size) << l
+               for l in range(m.spec.max_level + 1))
+
+
+def cpu_reference_extras():
+    """The reference's own multi-level step on the host cores for the
+    multi-level configurations, one single-threaded harness process per case,
+    side by side: the cfg1 geometry (64x32x32 coarse, 2 levels, sphere R 4,
+    Re 20, periodic lateral sides, non-equilibrium West / East) for 3 coarse
+    steps, and the 4-level D3Q27 cumulant sphere scaled by 1/4 (48x24x24
+    coarse, R 1.5, Re 200, every face closed: the reference's live
+    boundary) for 1 coarse step.  Each reports its seconds per coarse step,
+    the 1000-step cfg1 run extrapolated from it, and MLUPS over all levels."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        import oracle as O
+        import build as B
+    except Exception as e:  # noqa: BLE001
+        return {"unavailable": f"oracle harness not importable: {e}"}
+    from mortontrie_amr_b200.case import nested_sphere_case, sphere_case
+    runs = {
+        "cfg1_periodic": (sphere_case(bc_mode="neq"), 3),
+        "cfg3_scaled_quarter": (nested_sphere_case(coarse=(48, 24, 24), center=(16, 12, 12), radius=1.5,
+                                                   bc_mode="neq", boundary=("bc", "bc", "bc")), 1),
+    }
+    for case, _ in runs.values():
+        per = any(b == "periodic" for b in case.mesh.spec.boundary)
+        if not (os.path.exists(B.harness_path(case.params.q, case.mesh.spec.max_level, per)) or os.path.isdir(B.REF)):
+            return {"unavailable": "the reference harness is not built"}
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        procs = {name: (O.start_harness(case, steps, td, name), case, steps) for name, (case, steps) in runs.items()}
+        for name, ((p, path), case, steps) in procs.items():
+            p.wait(timeout=1800)
+            if p.returncode != 0:
+                out[name] = {"unavailable": f"harness exit {p.returncode}"}
+                continue
+            with open(path, "rb") as fh:
+                secs = O.parse_harness_output(fh.read(), case.params.q, case.mesh.spec.max_level, steps)["seconds"]
+            upd = _stepped_updates(case)
+            out[name] = {"coarse_steps": steps, "seconds_per_coarse_step": round(secs / steps, 4),
+                         "total_mlups": round(upd * steps / secs / 1e6, 4), "cell_updates_per_coarse_step": upd,
+                         "cores": 1}
+    if "seconds_per_coarse_step" in out.get("cfg1_periodic", {}):
+        out["cfg1_periodic"]["run_1000_coarse_steps_s_extrapolated"] = round(
+            1000 * out["cfg1_periodic"]["seconds_per_coarse_step"], 1)
+    return out
+
+
 def cpu_baseline_sample():
     mlups, kind, cores, sample = cpu_reference_run(1, 10, 1)
     return {"value": round(mlups, 4), "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample,
-            "per_core": round(mlups / cores, 4)}
+            "per_core": round(mlups / cores, 4), "extras": cpu_reference_extras()}
 
 
 def run_reference(args):

@@ -15,7 +15,7 @@ from typing import Optional
 import numpy as np
 
 from .lattice import directions, reference_units, weights
-from .mesh import Mesh, MeshSpec, Sphere, build_mesh, spec_mesh, sphere_markers
+from .mesh import Mesh, MeshSpec, Octree, Sphere, build_mesh, spec_mesh, sphere_markers
 
 COLLISIONS = {"LBGK": 0, "Cumulant": 1}
 IB_METHODS = {"DW": 0, "FH": 1, "DF": 2}
@@ -73,13 +73,16 @@ def _mesh(spec: MeshSpec, where: str):
 
 def sphere_case(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1, refine=None, center=(16, 16, 16),
                 radius=4.0, u=0.05, re=20.0, boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow",
-                ib_method="FH", stream_convention="reference", mesh="host") -> Case:
-    """Flow past a sphere; nu = u * 2R / Re in coarse units."""
-    if refine is None:
+                ib_method="FH", stream_convention="reference", mesh="host", octree=None) -> Case:
+    """Flow past a sphere; nu = u * 2R / Re in coarse units.  octree (an
+    mesh.Octree) refines around the sphere itself instead of in boxes."""
+    if octree is not None:
+        refine = []
+    elif refine is None:
         refine = [((4, 8, 8), (28, 24, 24))]
     nu = u * 2.0 * radius / re
     spec = MeshSpec(q=q, max_level=max_level, coarse=tuple(coarse), refine=list(refine), boundary=tuple(boundary),
-                    sphere=Sphere(tuple(center), radius))
+                    sphere=Sphere(tuple(center), radius), octree=octree)
     p = CaseParams(q=q, collision=collision, ib_method=ib_method, bc_mode=bc_mode, nu=nu, u_bc=(u, 0.0, 0.0),
                    u_ref=u, stream_convention=stream_convention)
     return Case(_mesh(spec, mesh), p)
@@ -87,13 +90,16 @@ def sphere_case(q=19, collision="LBGK", coarse=(64, 32, 32), max_level=1, refine
 
 def surface_case(surface, q=19, collision="LBGK", coarse=(32, 16, 16), max_level=1, refine=None, ref_length=None,
                  u=0.05, re=20.0, boundary=("bc", "periodic", "periodic"), bc_mode="zouhe_outflow", ib_method="FH",
-                 stream_convention="reference", mesh="host") -> Case:
+                 stream_convention="reference", mesh="host", octree=None) -> Case:
     """Flow past a closed triangulated body (an STL surface, (n, 3, 3) in
     coarse-cell units), voxelised on the finest level; nu = u * ref_length /
     Re with ref_length the body's largest extent across the flow (y, z) by
-    default."""
+    default.  octree (an mesh.Octree) refines around the body itself
+    instead of in boxes."""
     surface = np.asarray(surface, np.float64)
-    if refine is None:
+    if octree is not None:
+        refine = []
+    elif refine is None:
         lo, hi = surface.reshape(-1, 3).min(axis=0), surface.reshape(-1, 3).max(axis=0)
         refine = [(tuple(int(np.floor(v)) - 3 for v in lo), tuple(int(np.ceil(v)) + 3 for v in hi))]
     if ref_length is None:
@@ -101,7 +107,7 @@ def surface_case(surface, q=19, collision="LBGK", coarse=(32, 16, 16), max_level
         ref_length = float(max(ext[1], ext[2]))
     nu = u * ref_length / re
     spec = MeshSpec(q=q, max_level=max_level, coarse=tuple(coarse), refine=list(refine), boundary=tuple(boundary),
-                    surface=surface)
+                    surface=surface, octree=octree)
     p = CaseParams(q=q, collision=collision, ib_method=ib_method, bc_mode=bc_mode, nu=nu, u_bc=(u, 0.0, 0.0),
                    u_ref=u, stream_convention=stream_convention)
     return Case(_mesh(spec, mesh), p)

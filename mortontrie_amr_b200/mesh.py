@@ -79,6 +79,23 @@ class MeshSpec:
     # closed triangulated solid surface (n, 3, 3) in coarse-cell units,
     # voxelised on the finest level instead of a sphere (links mode)
     surface: Optional[np.ndarray] = None
+    # refinement driven by the body instead of boxes (refine then lists no
+    # boxes): see Octree
+    octree: Optional["Octree"] = None
+
+
+@dataclass
+class Octree:
+    """Refinement regions made from the body (sphere or surface) instead of
+    boxes: the finest level covers every level-(L-1) cell within `band` of
+    those cells of the body's surface and inside it (the near-solid cells
+    Grid_Manager::generate_inner refines, Grid_Manager.cpp:136-454), and
+    every coarser level covers the next finer region grown by `margin` of
+    its own cells, rounded out to whole parent cells (the intermediate
+    levels the reference's generate_intermediate would make and leaves
+    empty, Grid_Manager.cpp:99-102).  The levels nest 2:1 by construction."""
+    band: float = 3.0   # level-(L-1) cells around the surface
+    margin: int = 4     # level-l cells between level l+1's region and level l's edge
 
 
 @dataclass
@@ -146,6 +163,8 @@ class SpecMesh:
 
 
 def spec_mesh(spec: MeshSpec) -> SpecMesh:
+    if spec.octree is not None:
+        raise ValueError("the device classifies box refinements; an octree is built by the host mesher")
     if len(spec.refine) != spec.max_level:
         raise ValueError("need one refinement box per level below the maximum level")
     mk = sphere_markers(spec) if (spec.sphere is not None and spec.ib == "markers") else None
@@ -156,9 +175,17 @@ def estimate_cells(spec: MeshSpec) -> list:
     """Upper bound of the stored cells per level from the boxes alone (no
     classification): the level's box minus the interior under the next
     refinement box, plus a one-cell layer outside the box (ghost C2F) and
-    outside the refinement box (ghost F2C)."""
+    outside the refinement box (ghost F2C); for an octree, each level's
+    domain and its one-cell layer."""
     def vol(lo, hi, g=0):
         return int(np.prod([max(0, h - l + 2 * g) for l, h in zip(lo, hi)]))
+    if spec.octree is not None:
+        # each level's domain (the children of its region) with its ghost layer
+        regions = octree_regions(spec)
+        out = [vol((0, 0, 0), tuple(spec.coarse))]
+        for l in range(1, spec.max_level + 1):
+            out.append(int(regions[l].children().dilate(1).mask.sum()))
+        return out
     out = []
     lo, hi = (0, 0, 0), tuple(spec.coarse)
     for l in range(spec.max_level + 1):
@@ -175,6 +202,154 @@ def estimate_cells(spec: MeshSpec) -> list:
             lo, hi = (0, 0, 0), (0, 0, 0)
         out.append(n)
     return out
+
+
+class Region:
+    """A set of cells of one level as a dense mask over its bounding box:
+    cell (x, y, z) is in the set iff mask[x - lo[0], y - lo[1], z - lo[2]]."""
+
+    def __init__(self, lo, mask):
+        self.lo = np.asarray(lo, np.int64)
+        self.mask = np.ascontiguousarray(mask, bool)
+
+    @property
+    def hi(self):
+        return self.lo + np.array(self.mask.shape, np.int64)
+
+    def padded(self, p):
+        return Region(self.lo - p, np.pad(self.mask, p))
+
+    def dilate(self, m):
+        """Every cell within Chebyshev distance m of the set (a cube of
+        half-width m, one axis at a time)."""
+        r = self.padded(m)
+        mk = r.mask
+        for axis in range(3):
+            acc = mk.copy()
+            for d in range(1, m + 1):
+                acc |= _shifted(mk, d, axis)
+                acc |= _shifted(mk, -d, axis)
+            mk = acc
+        return Region(r.lo, mk)
+
+    def shell(self):
+        """Cells of the set with one of their 26 neighbours outside it (the
+        set minus its erosion by the 3x3x3 cube, one axis at a time)."""
+        r = self.padded(1)
+        er = r.mask
+        for axis in range(3):
+            er = er & _shifted(er, 1, axis) & _shifted(er, -1, axis)
+        return Region(r.lo, r.mask & ~er)
+
+    def parents(self):
+        """The level-(l-1) cells with at least one child in the set."""
+        lo = self.lo - (self.lo & 1)
+        pre = self.lo - lo
+        shape = np.array(self.mask.shape) + pre
+        post = shape & 1
+        m = np.pad(self.mask, [(int(a), int(b)) for a, b in zip(pre, post)])
+        nx, ny, nz = (np.array(m.shape) // 2).tolist()
+        return Region(lo // 2, m.reshape(nx, 2, ny, 2, nz, 2).any(axis=(1, 3, 5)))
+
+    def children(self):
+        """The level-(l+1) cells whose parent is in the set."""
+        m = self.mask.repeat(2, axis=0).repeat(2, axis=1).repeat(2, axis=2)
+        return Region(2 * self.lo, m)
+
+    def contains(self, x, y, z):
+        x, y, z = (np.asarray(v, np.int64) for v in (x, y, z))
+        ix, iy, iz = x - self.lo[0], y - self.lo[1], z - self.lo[2]
+        sh = self.mask.shape
+        ok = (ix >= 0) & (ix < sh[0]) & (iy >= 0) & (iy < sh[1]) & (iz >= 0) & (iz < sh[2])
+        out = np.zeros(x.size, bool)
+        out[ok] = self.mask[ix[ok], iy[ok], iz[ok]]
+        return out
+
+    def cells(self):
+        ix, iy, iz = np.nonzero(self.mask)
+        return ix + self.lo[0], iy + self.lo[1], iz + self.lo[2]
+
+
+def _shifted(m, d, axis):
+    """m moved by d cells along axis: out[c] = m[c - d], False where c - d
+    falls outside."""
+    out = np.zeros_like(m)
+    src = [slice(None)] * 3
+    dst = [slice(None)] * 3
+    if d > 0:
+        src[axis], dst[axis] = slice(0, -d), slice(d, None)
+    else:
+        src[axis], dst[axis] = slice(-d, None), slice(0, d)
+    out[tuple(dst)] = m[tuple(src)]
+    return out
+
+
+def box_region(lo, hi):
+    return Region(lo, np.ones(tuple(int(h - l) for l, h in zip(lo, hi)), bool))
+
+
+def surface_points(tris, spacing):
+    """Points on every triangle no further apart than `spacing` (a
+    barycentric lattice per triangle, vertices included)."""
+    tris = np.asarray(tris, np.float64)
+    out = []
+    for t in tris:
+        e = max(np.linalg.norm(t[1] - t[0]), np.linalg.norm(t[2] - t[0]), np.linalg.norm(t[2] - t[1]))
+        n = max(1, int(np.ceil(e / spacing)))
+        i, j = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+        keep = (i + j) <= n
+        a, b = i[keep] / n, j[keep] / n
+        out.append(t[0] + a[:, None] * (t[1] - t[0]) + b[:, None] * (t[2] - t[0]))
+    return np.concatenate(out) if out else np.zeros((0, 3))
+
+
+def octree_regions(spec: "MeshSpec") -> list:
+    """regions[l] for l = 1..L: the level-(l-1) cells refined to level l
+    (regions[0] is None), made from the body as Octree describes."""
+    L = spec.max_level
+    oc = spec.octree
+    if L < 1:
+        raise ValueError("an octree needs a refined level")
+    lv = L - 1
+    s = float(1 << lv)
+    band = float(oc.band)
+    if spec.surface is not None:
+        tris = np.asarray(spec.surface, np.float64) * s
+        pts = surface_points(tris, 0.5)
+        lo = np.floor(pts.min(axis=0)).astype(np.int64) - int(np.ceil(band)) - 1
+        hi = np.floor(pts.max(axis=0)).astype(np.int64) + int(np.ceil(band)) + 2
+        mask = np.zeros(tuple((hi - lo).tolist()), bool)
+        c = np.floor(pts).astype(np.int64) - lo
+        mask[c[:, 0], c[:, 1], c[:, 2]] = True
+        near = Region(lo, mask).dilate(int(np.ceil(band)))
+        gx, gy, gz = _grid(near.lo, near.hi)
+        inside = surface_inside(tris, gx, gy, gz).reshape(near.mask.shape)
+        fine = Region(near.lo, near.mask | inside)
+    elif spec.sphere is not None:
+        c = np.asarray(spec.sphere.center, np.float64) * s
+        r = spec.sphere.radius * s
+        ext = r + band + 1.0
+        lo = np.floor(c - ext).astype(np.int64) - 1
+        hi = np.ceil(c + ext).astype(np.int64) + 1
+        gx, gy, gz = _grid(lo, hi)
+        d = np.sqrt((gx + 0.5 - c[0]) ** 2 + (gy + 0.5 - c[1]) ** 2 + (gz + 0.5 - c[2]) ** 2)
+        # every cell that reaches within `band` of the surface, and the inside
+        fine = Region(lo, (d <= r + band + np.sqrt(3.0) / 2.0).reshape(tuple((hi - lo).tolist())))
+    else:
+        raise ValueError("an octree is made from a body: a sphere or a surface")
+    regions = [None] * (L + 1)
+    regions[L] = fine
+    for l in range(L - 1, 0, -1):
+        regions[l] = regions[l + 1].dilate(int(oc.margin)).parents()
+    for l in range(1, L + 1):
+        ext = np.array(spec.coarse, np.int64) << (l - 1)
+        x, y, z = regions[l].cells()
+        if x.size == 0:
+            raise ValueError(f"level {l}: empty octree region")
+        if (x.min() < 0 or y.min() < 0 or z.min() < 0 or x.max() >= ext[0] or y.max() >= ext[1]
+                or z.max() >= ext[2]):
+            raise ValueError(f"level {l}: the octree region leaves the domain (a larger box or a smaller margin)")
+    return regions
 
 
 def _grid(lo, hi):
@@ -233,7 +408,13 @@ def _in_sorted(a, sorted_b):
 def build_mesh(spec: MeshSpec) -> Mesh:
     L = spec.max_level
     q = spec.q
-    if len(spec.refine) != L:
+    octree = spec.octree is not None
+    if octree:
+        if spec.refine:
+            raise ValueError("refinement boxes and an octree are exclusive")
+        if spec.ib == "markers":
+            raise ValueError("the octree is made for the links body (sphere or surface)")
+    elif len(spec.refine) != L:
         raise ValueError("need one refinement box per level below the maximum level")
     periodic = tuple(b == "periodic" for b in spec.boundary)
     nx, ny, nz = spec.coarse
@@ -241,22 +422,28 @@ def build_mesh(spec: MeshSpec) -> Mesh:
     extents = []
     lat_bc = [np.zeros(0, np.uint64) for _ in range(26)]
 
-    # domain of each level in its own cell units
+    # domain of each level in its own cell units: a box, or for an octree
+    # the children of the level's region
     dom_lo = [(0, 0, 0)]
     dom_hi = [(nx, ny, nz)]
-    for l in range(L):
-        if spec.refine[l] is None or dom_hi[-1] == (0, 0, 0):
-            dom_lo.append((0, 0, 0))
-            dom_hi.append((0, 0, 0))
-            continue
-        lo, hi = spec.refine[l]
-        dom_lo.append(tuple(2 * v for v in lo))
-        dom_hi.append(tuple(2 * v for v in hi))
+    regions = octree_regions(spec) if octree else None
+    if not octree:
+        for l in range(L):
+            if spec.refine[l] is None or dom_hi[-1] == (0, 0, 0):
+                dom_lo.append((0, 0, 0))
+                dom_hi.append((0, 0, 0))
+                continue
+            lo, hi = spec.refine[l]
+            dom_lo.append(tuple(2 * v for v in lo))
+            dom_hi.append(tuple(2 * v for v in hi))
     for l in range(L + 1):
         extents.append(tuple((n << l) for n in (nx, ny, nz)))
 
     for l in range(L + 1):
-        x, y, z = _grid(dom_lo[l], dom_hi[l])
+        if octree and l > 0:
+            x, y, z = regions[l].children().cells()
+        else:
+            x, y, z = _grid(dom_lo[l], dom_hi[l])
         sets = {}
         stored = np.ones(x.size, bool)
         is_bc = np.zeros(x.size, bool)
@@ -271,7 +458,15 @@ def build_mesh(spec: MeshSpec) -> Mesh:
                 m = is_bc & (side[:, 0] == s[0]) & (side[:, 1] == s[1]) & (side[:, 2] == s[2])
                 lat_bc[i] = _sorted_unique(cell_key(L, 0, x[m], y[m], z[m]))
         f2c = np.zeros(x.size, bool)
-        if l < L and dom_hi[l + 1] != (0, 0, 0):
+        if octree and l < L:
+            # the region's outer layer of level-l cells; the rest of it is
+            # stored on the finer level only
+            inside = regions[l + 1].contains(x, y, z)
+            f2c = regions[l + 1].shell().contains(x, y, z)
+            stored &= ~(inside & ~f2c)
+            if np.any(inside & is_bc):
+                raise ValueError("the octree region touches the boundary shell")
+        elif l < L and dom_hi[l + 1] != (0, 0, 0):
             lo, hi = spec.refine[l]
             inside = _inside(x, y, z, lo, hi)
             f2c = inside & _shell_mask(x, y, z, lo, hi, 1)
@@ -280,9 +475,13 @@ def build_mesh(spec: MeshSpec) -> Mesh:
                 raise ValueError("refinement box touches the boundary shell")
         c2f = np.zeros(x.size, bool)
         if l > 0:
-            c2f = _shell_mask(x, y, z, dom_lo[l], dom_hi[l], 2)
+            # the children of the coarser level's F2C cells: for a box, the
+            # two-cell shell of the level's domain
+            c2f = (regions[l].shell().children().contains(x, y, z) if octree
+                   else _shell_mask(x, y, z, dom_lo[l], dom_hi[l], 2))
             if np.any(c2f & f2c):
-                raise ValueError(f"level {l}: refinement box too close to the coarse/fine interface")
+                raise ValueError(f"level {l}: refinement {'region' if octree else 'box'} too close to the "
+                                 "coarse/fine interface")
         fluid = stored & ~is_bc & ~f2c & ~c2f
         sets["overlap_F2C"] = _sorted_unique(cell_key(L, l, x[f2c], y[f2c], z[f2c]))
         sets["overlap_C2F"] = _sorted_unique(cell_key(L, l, x[c2f], y[c2f], z[c2f]))

@@ -530,6 +530,49 @@ def test_brick_forms_fp64_and_arguments(ctx):
         m.close()
 
 
+@pytest.mark.parametrize("schedule", ["phases", "fused"])
+@pytest.mark.parametrize("which", ["sphere_q19_l2", "stl_q27_l2"])
+def test_octree_case_matches_oracle(ctx, which, schedule):
+    """Refinement made from the body (an octree of 2:1-nested regions around
+    an analytic sphere, FH links, or an STL icosphere, D3Q27 cumulant): GPU
+    FP64 vs the oracle, bit-exact populations and the drag to 1e-12."""
+    from test_octree import _octree_cases
+    case = _octree_cases()[which]()
+    mgr = _device_case(ctx, case, None, schedule=schedule)
+    mgr.fluidSimulate(4)
+    ctx.synchronize()
+    oc = run_oracle(case, 4)
+    for l in range(case.max_level + 1):
+        f, fcol = mgr.populations(l)
+        _, tags = mgr.keys(l)
+        g = oc.get(l)
+        keep = (tags & TAG_BC) == 0
+        assert np.array_equal(f[:, keep], g["f"][:, keep]), l
+        assert np.array_equal(fcol, g["fcol"]), l
+    assert rel_err(mgr.force()[:3], oc.force()[:3]) < 1e-12
+    mgr.close()
+
+
+def test_octree_case_reduced_storage(ctx):
+    """The octree sphere in FP16 under the fused schedule against FP64."""
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    from test_octree import _octree_cases
+    case = _octree_cases()["sphere_q19_l2"]()
+    a = LBM_Manager(ctx, case, "f64")
+    b = LBM_Manager(ctx, case, "f16", schedule="fused")
+    a.fluidSimulate(20)
+    b.fluidSimulate(20)
+    ctx.synchronize()
+    L = case.max_level
+    _, ua = a.macros(L)
+    _, ub = b.macros(L)
+    _, tags = a.keys(L)
+    fl = (tags & 1) != 0
+    assert np.linalg.norm(ub[:, fl] - ua[:, fl]) / np.linalg.norm(ua[:, fl]) < TOL_AMR["f16"]
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("q,L", [(19, 1), (19, 3), (27, 3)])
 def test_device_neighbor_table_matches_reference_blocks(ctx, q, L):
     """The device-built neighbour table of the KAT blocks (every cell of two
