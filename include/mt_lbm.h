@@ -144,7 +144,9 @@ int mt_case_set_dis(mt_ctx *ctx, int32_t case_id, const uint64_t *keys, const do
 typedef struct mt_mesh_spec {
     int64_t coarse[3];                   /* level-0 cells per axis (the case's extent0) */
     int32_t boundary_bc[3];              /* 1: boundary shell on this axis, 0: periodic (the case's periodic[] inverted) */
-    int32_t has_refine[MT_MAX_LEVELS];   /* level l < max_level holds a refinement box */
+    int32_t has_refine[MT_MAX_LEVELS];   /* level l < max_level is refined: 1 in the box refine_lo/hi[l],
+                                            2 in the region of level l + 1 set by mt_case_set_region (an
+                                            octree: every refined level then takes a region) */
     int64_t refine_lo[MT_MAX_LEVELS][3]; /* the box [lo, hi) in level-l cells */
     int64_t refine_hi[MT_MAX_LEVELS][3];
     int32_t sphere;                      /* 0 none, 1 solid + wall distances, 2 forcing band (MT_IB_DF),
@@ -166,6 +168,21 @@ typedef struct mt_mesh_spec {
  * normalised by the link length and kept in [0, 1]
  * (Lat_Manager::compute_distance, Lat_Voxelize.cpp:1252-1285). */
 int mt_case_set_surface(mt_ctx *ctx, int32_t case_id, const double *tri, int64_t n);
+/* Refinement region of `level` (1..max_level) for mt_case_generate with
+ * has_refine[level - 1] = 2 (refinement made from the body instead of boxes,
+ * the octree of Grid_Manager::generate_inner, Grid_Manager.cpp:136-454, with
+ * the intermediate levels its generate_intermediate leaves empty,
+ * :99-102): the level-(level - 1) cells refined to `level`, a dense mask
+ * mask[(i * shape[1] + j) * shape[2] + k] != 0 for cell lo + (i, j, k).  The
+ * level's cells are the children of the region; its overlap_C2F cells are
+ * the children of the region's cells with one of their 26 neighbours outside
+ * it, which are the coarser level's overlap_F2C cells; the rest of the
+ * region is stored on the finer level only.  The box [lo, lo + shape) must
+ * lie inside level (level - 1)'s extent; regions must nest 2:1 (each inside
+ * the coarser one with room for the interface layers), which
+ * mt_case_generate checks as it does for boxes. */
+int mt_case_set_region(mt_ctx *ctx, int32_t case_id, int32_t level, const int64_t *lo, const int64_t *shape,
+                       const uint8_t *mask);
 /* generate the case's sets from spec and build it (replaces mt_case_add_set,
  * mt_case_set_dis and mt_case_build); MT_ERR_MESH with the host mesher's
  * messages when the boxes or the sphere break the contract */

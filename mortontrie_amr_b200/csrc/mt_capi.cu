@@ -401,6 +401,31 @@ int mt_case_set_surface(mt_ctx *h, int32_t id, const double *tri, int64_t n)
     return MT_OK;
 }
 
+int mt_case_set_region(mt_ctx *h, int32_t id, int32_t level, const int64_t *lo, const int64_t *shape,
+                       const uint8_t *mask)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (c->dense || c->built) return set_err(ctx, MT_ERR_STATE, "a region can only be set before the build");
+    if (level < 1 || level > c->d.max_level) return set_err(ctx, MT_ERR_ARG, "region level out of range");
+    if (!lo || !shape || !mask) return set_err(ctx, MT_ERR_ARG, "null region argument");
+    int64_t n = 1;
+    for (int a = 0; a < 3; ++a) {
+        const int64_t ext = c->d.extent0[a] << (level - 1);
+        if (shape[a] < 1 || lo[a] < 0 || lo[a] + shape[a] > ext)
+            return set_err(ctx, MT_ERR_ARG, "region box outside the coarser level's extent");
+        n *= shape[a];
+    }
+    c->h_reg[level].assign(mask, mask + n);
+    for (int a = 0; a < 3; ++a) {
+        c->reg_lo[level][a] = lo[a];
+        c->reg_n[level][a] = shape[a];
+    }
+    return MT_OK;
+}
+
 int mt_case_generate(mt_ctx *h, int32_t id, const mt_mesh_spec *sp)
 {
     Case *c;
@@ -426,16 +451,30 @@ int mt_case_generate(mt_ctx *h, int32_t id, const mt_mesh_spec *sp)
     if ((sp->sphere == 1 || sp->sphere == 2) && !(sp->radius > 0.0))
         return set_err(ctx, MT_ERR_ARG, "sphere radius must be positive");
     if (sp->sphere == 3 && c->h_tri.empty()) return set_err(ctx, MT_ERR_STATE, "no surface set (mt_case_set_surface)");
+    bool regions = false;
+    for (int l = 0; l < L; ++l) {
+        if (sp->has_refine[l] < 0 || sp->has_refine[l] > 2) return set_err(ctx, MT_ERR_ARG, "has_refine must be 0, 1 or 2");
+        regions |= sp->has_refine[l] == 2;
+    }
+    if (regions)
+        for (int l = 0; l < L; ++l) {
+            if (sp->has_refine[l] != 2)
+                return set_err(ctx, MT_ERR_ARG, "regions refine every level or none (no boxes beside them)");
+            if (c->h_reg[l + 1].empty()) return set_err(ctx, MT_ERR_STATE, "no region set for a refined level");
+        }
     {
         int64_t lo[3] = {0, 0, 0}, hi[3] = {sp->coarse[0], sp->coarse[1], sp->coarse[2]};
         for (int l = 0; l < L; ++l) {
             if (!sp->has_refine[l]) break;
             for (int a = 0; a < 3; ++a) {
-                if (sp->refine_lo[l][a] < lo[a] || sp->refine_hi[l][a] > hi[a] ||
-                    sp->refine_hi[l][a] - sp->refine_lo[l][a] < 1)
-                    return set_err(ctx, MT_ERR_ARG, "refinement box outside its level's domain");
-                lo[a] = 2 * sp->refine_lo[l][a];
-                hi[a] = 2 * sp->refine_hi[l][a];
+                // the refined cells in level-l cells: the box, or the region's box
+                const int64_t rl = regions ? c->reg_lo[l + 1][a] : sp->refine_lo[l][a];
+                const int64_t rh = regions ? c->reg_lo[l + 1][a] + c->reg_n[l + 1][a] : sp->refine_hi[l][a];
+                if (rl < lo[a] || rh > hi[a] || rh - rl < 1)
+                    return set_err(ctx, MT_ERR_ARG, regions ? "refinement region outside its level's domain"
+                                                            : "refinement box outside its level's domain");
+                lo[a] = 2 * rl;
+                hi[a] = 2 * rh;
             }
             if ((hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]) > INT32_MAX)
                 return set_err(ctx, MT_ERR_ARG, "a level box above 2^31 cells");

@@ -133,6 +133,11 @@ struct Case {
     std::vector<double> h_dis;
     bool dis_on_device = false;  // dis_key / dis generated on the device (ndis set)
     std::vector<double> h_tri;   // solid surface triangles [n][3][3], coarse-cell units (mt_case_set_surface)
+    // refinement regions (mt_case_set_region): h_reg[l] the level-(l-1)
+    // cells refined to level l, a dense mask over [reg_lo[l], reg_lo[l] + reg_n[l])
+    std::vector<uint8_t> h_reg[MT_MAX_LEVELS + 1];
+    int64_t reg_lo[MT_MAX_LEVELS + 1][3] = {};
+    int64_t reg_n[MT_MAX_LEVELS + 1][3] = {};
     double *ib_force = nullptr;  // [3 * nib] per-cell force of the last treat()
     double *force_acc = nullptr; // [4] fx, fy, fz, treat count
     double *h_force = nullptr;   // [6] page-locked: force_acc copy [4], then the guard flags (int) (mt_case_force_async)

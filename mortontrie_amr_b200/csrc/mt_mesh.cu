@@ -33,14 +33,38 @@ struct Box {
     MT_HD int64_t n() const { return (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]); }
 };
 
+// a set of cells of one level as a dense mask over a box (mt_case_set_region)
+struct RegionMask {
+    const uint8_t *m;
+    int64_t lo[3], n[3];
+    MT_HD bool has(int64_t x, int64_t y, int64_t z) const
+    {
+        const int64_t a = x - lo[0], b = y - lo[1], c = z - lo[2];
+        if (a < 0 || b < 0 || c < 0 || a >= n[0] || b >= n[1] || c >= n[2]) return false;
+        return m[(a * n[1] + b) * n[2] + c] != 0;
+    }
+    // in the set with one of its 26 neighbours outside it
+    MT_HD bool edge(int64_t x, int64_t y, int64_t z) const
+    {
+        if (!has(x, y, z)) return false;
+        for (int d = 0; d < 27; ++d)
+            if (d != 13 && !has(x + d % 3 - 1, y + (d / 3) % 3 - 1, z + d / 9 - 1)) return true;
+        return false;
+    }
+};
+
 struct LevelGen {
     int level, L, q;
     int64_t ext[3];  // level extent in its own cells
     int bc[3];       // boundary shell on this axis (level 0)
     int per[3];      // periodic axis
-    Box dom;         // cells of this level
+    Box dom;         // cells of this level (for a region: the box of its children)
+    int dom_region;  // the level's cells are the children of dreg's cells
+    RegionMask dreg; // in level-(l-1) cells
     int has_ref;     // refinement box of this level present
     Box ref;         // in this level's cells
+    int ref_region;  // the refined cells are rreg's (instead of the box ref)
+    RegionMask rreg; // in this level's cells
     int sphere;      // 0 none, 1 solid + links, 2 band, 3 triangulated surface (finest level only)
     double cx, cy, cz, r, amp, slack;  // finest-level units
     int8_t side_bc[27];                // lat_bc index of a (-1, 0, 1)^3 side combination
@@ -65,6 +89,13 @@ __global__ void k_classify(LevelGen g, uint64_t *key, uint32_t *pay, int *err)
     if (t >= g.dom.n()) return;
     const int64_t x = g.dom.lo[0] + t % nx, y = g.dom.lo[1] + (t / nx) % ny, z = g.dom.lo[2] + t / (nx * ny);
     const int64_t c[3] = {x, y, z};
+    if (g.dom_region && !g.dreg.has(x >> 1, y >> 1, z >> 1)) {
+        // inside the box of the region's children but not one of them
+        if (g.ref_region && g.rreg.has(x, y, z)) atomicOr(err, MERR_BOX_C2F);
+        key[t] = ~0ull;
+        pay[t] = P_NONE;
+        return;
+    }
     int bcb = -1;
     if (g.level == 0) {
         int side[3] = {0, 0, 0};
@@ -75,16 +106,23 @@ __global__ void k_classify(LevelGen g, uint64_t *key, uint32_t *pay, int *err)
     bool f2c = false, removed = false;
     if (g.has_ref) {
         bool inside = true, shell = false;
-        for (int a = 0; a < 3; ++a) {
-            inside &= c[a] >= g.ref.lo[a] && c[a] < g.ref.hi[a];
-            shell |= c[a] < g.ref.lo[a] + 1 || c[a] >= g.ref.hi[a] - 1;
+        if (g.ref_region) {
+            inside = g.rreg.has(x, y, z);
+            shell = inside && g.rreg.edge(x, y, z);
+        } else {
+            for (int a = 0; a < 3; ++a) {
+                inside &= c[a] >= g.ref.lo[a] && c[a] < g.ref.hi[a];
+                shell |= c[a] < g.ref.lo[a] + 1 || c[a] >= g.ref.hi[a] - 1;
+            }
         }
         f2c = inside && shell;
         removed = inside && !shell;
         if (inside && bcb >= 0) atomicOr(err, MERR_BOX_BC);
     }
     bool c2f = false;
-    if (g.level > 0)
+    if (g.dom_region)
+        c2f = g.dreg.edge(x >> 1, y >> 1, z >> 1);  // a child of a coarser F2C cell
+    else if (g.level > 0)
         for (int a = 0; a < 3; ++a) c2f |= c[a] < g.dom.lo[a] + 2 || c[a] >= g.dom.hi[a] - 2;
     if (c2f && f2c) atomicOr(err, MERR_BOX_C2F);
     uint32_t p;
@@ -655,6 +693,34 @@ int amr_generate(Ctx &ctx, Case &c, const mt_mesh_spec &sp)
     if (int rc = derr.alloc(ctx, 1)) return rc;
     MT_CUDA(ctx, cudaMemsetAsync(derr.p, 0, sizeof(int), ctx.stream));
     Box dom{{0, 0, 0}, {sp.coarse[0], sp.coarse[1], sp.coarse[2]}};
+    // refinement regions (has_refine == 2) on the device; rbox[l]: the box of
+    // level l's cells refined to l + 1, in level-l cells
+    DBuf<uint8_t> dreg[MT_MAX_LEVELS + 1];
+    Box rbox[MT_MAX_LEVELS];
+    for (int l = 0; l < L; ++l) {
+        if (sp.has_refine[l] == 2) {
+            const std::vector<uint8_t> &h = c.h_reg[l + 1];
+            if (int rc = dreg[l + 1].alloc(ctx, (int64_t)h.size())) return rc;
+            MT_CUDA(ctx, cudaMemcpyAsync(dreg[l + 1].p, h.data(), h.size(), cudaMemcpyHostToDevice, ctx.stream));
+            for (int a = 0; a < 3; ++a) {
+                rbox[l].lo[a] = c.reg_lo[l + 1][a];
+                rbox[l].hi[a] = c.reg_lo[l + 1][a] + c.reg_n[l + 1][a];
+            }
+        } else {
+            for (int a = 0; a < 3; ++a) {
+                rbox[l].lo[a] = sp.refine_lo[l][a];
+                rbox[l].hi[a] = sp.refine_hi[l][a];
+            }
+        }
+    }
+    auto region = [&](int l) {  // the mask of level l's refined cells (l + 1's region)
+        RegionMask r{dreg[l + 1].p, {0, 0, 0}, {0, 0, 0}};
+        for (int a = 0; a < 3; ++a) {
+            r.lo[a] = c.reg_lo[l + 1][a];
+            r.n[a] = c.reg_n[l + 1][a];
+        }
+        return r;
+    };
     SurfaceTables st;
     if (sp.sphere == 3) {
         if (L == 0) return set_err(ctx, MT_ERR_MESH, "the solid boundary is only applied on a refined finest level");
@@ -663,8 +729,8 @@ int amr_generate(Ctx &ctx, Case &c, const mt_mesh_spec &sp)
             Box nx{{0, 0, 0}, {0, 0, 0}};
             if (sp.has_refine[l] && f.n() > 0)
                 for (int a = 0; a < 3; ++a) {
-                    nx.lo[a] = 2 * sp.refine_lo[l][a];
-                    nx.hi[a] = 2 * sp.refine_hi[l][a];
+                    nx.lo[a] = 2 * rbox[l].lo[a];
+                    nx.hi[a] = 2 * rbox[l].hi[a];
                 }
             f = nx;
         }
@@ -684,11 +750,15 @@ int amr_generate(Ctx &ctx, Case &c, const mt_mesh_spec &sp)
         for (int b = 0; b < 26; ++b)
             g.side_bc[(sides[b][0] + 1) + 3 * (sides[b][1] + 1) + 9 * (sides[b][2] + 1)] = (int8_t)b;
         g.dom = dom;
+        g.dom_region = l > 0 && sp.has_refine[l - 1] == 2;
+        if (g.dom_region) g.dreg = region(l - 1);
         g.has_ref = l < L && sp.has_refine[l] && dom.n() > 0;
+        g.ref_region = g.has_ref && sp.has_refine[l] == 2;
+        if (g.ref_region) g.rreg = region(l);
         if (g.has_ref)
             for (int a = 0; a < 3; ++a) {
-                g.ref.lo[a] = sp.refine_lo[l][a];
-                g.ref.hi[a] = sp.refine_hi[l][a];
+                g.ref.lo[a] = rbox[l].lo[a];
+                g.ref.hi[a] = rbox[l].hi[a];
             }
         g.sphere = (l == L) ? sp.sphere : 0;
         const double s = (double)(1 << L);

@@ -34,7 +34,7 @@ EXPORTS = [
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
     "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_reduce_levels", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_interface_time", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
-    "mt_case_generate", "mt_case_set_surface", "mt_marker_record", "mt_marker_done", "mt_case_force_async",
+    "mt_case_generate", "mt_case_set_surface", "mt_case_set_region", "mt_marker_record", "mt_marker_done", "mt_case_force_async",
     "mt_case_force_copied", "mt_set_priority", "mt_case_remap", "mt_case_status_copied", "mt_case_tune_bricks",
     "mt_case_set_brick_forms",
 ]
@@ -67,8 +67,10 @@ class mt_mesh_spec(C.Structure):
 
 def make_mesh_spec(spec) -> mt_mesh_spec:
     """mt_mesh_spec of a MeshSpec (mesh.py): the device classification
-    produces the sets build_mesh(spec) would."""
-    if len(spec.refine) != spec.max_level:
+    produces the sets build_mesh(spec) would.  An octree's levels are marked
+    as regions (has_refine 2), uploaded by upload_regions."""
+    octree = getattr(spec, "octree", None) is not None
+    if not octree and len(spec.refine) != spec.max_level:
         raise ValueError("need one refinement box per level below the maximum level")
     if spec.max_level >= MAX_LEVELS:
         raise ValueError("too many levels")
@@ -76,7 +78,10 @@ def make_mesh_spec(spec) -> mt_mesh_spec:
     for a in range(3):
         m.coarse[a] = int(spec.coarse[a])
         m.boundary_bc[a] = int(spec.boundary[a] == "bc")
-    for l, box in enumerate(spec.refine):
+    if octree:
+        for l in range(spec.max_level):
+            m.has_refine[l] = 2
+    for l, box in enumerate([] if octree else spec.refine):
         if box is None:
             break
         m.has_refine[l] = 1
@@ -93,6 +98,23 @@ def make_mesh_spec(spec) -> mt_mesh_spec:
         m.osc_amplitude = float(spec.oscillation[0]) if (spec.ib == "markers" and spec.oscillation) else 0.0
         m.band_slack = float(spec.band_slack)
     return m
+
+
+def upload_regions(ctx, case_id, spec):
+    """The octree's refinement regions (mesh.octree_regions, made on the
+    host) for mt_case_generate, each cropped to the box of its cells."""
+    from .mesh import octree_regions
+    regions = octree_regions(spec)
+    for l in range(1, spec.max_level + 1):
+        r = regions[l]
+        ix, iy, iz = np.nonzero(r.mask)
+        lo = np.array([ix.min(), iy.min(), iz.min()], np.int64)
+        hi = np.array([ix.max(), iy.max(), iz.max()], np.int64) + 1
+        mask = np.ascontiguousarray(r.mask[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]], np.uint8)
+        blo = np.ascontiguousarray(lo + r.lo, np.int64)
+        shape = np.ascontiguousarray(hi - lo, np.int64)
+        ctx.check(lib().mt_case_set_region(ctx.h, case_id, l, _ptr(blo, C.c_int64), _ptr(shape, C.c_int64),
+                                           _ptr(mask, C.c_uint8)), "mt_case_set_region")
 
 
 _lib = None
@@ -122,6 +144,7 @@ def lib():
             "mt_batch_create": [vp, i32p], "mt_batch_destroy": [vp, i32], "mt_batch_add": [vp, i32, i32],
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
             "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64],
+            "mt_case_set_region": [vp, i32, i32, i64p, i64p, C.POINTER(C.c_uint8)],
             "mt_marker_record": [vp, i64p], "mt_marker_done": [vp, i64, i32p], "mt_case_force_async": [vp, i32],
             "mt_case_force_copied": [vp, i32, dp], "mt_case_status_copied": [vp, i32], "mt_case_tune_bricks": [vp, i32, i32p, C.POINTER(C.c_float)], "mt_case_set_brick_forms": [vp, i32, i32p], "mt_set_priority": [vp, i32], "mt_case_remap": [vp, i32, i32, i64p], "mt_calculate_macros": [vp, i32, i32], "mt_collide": [vp, i32, i32],
             "mt_stream": [vp, i32, i32], "mt_explosion": [vp, i32, i32], "mt_coalescence": [vp, i32, i32],
@@ -281,6 +304,8 @@ class LBM_Manager:
         m = case.mesh
         if generate or isinstance(m, SpecMesh):
             ms = make_mesh_spec(m.spec)
+            if getattr(m.spec, "octree", None) is not None:
+                upload_regions(ctx, self.id, m.spec)
             if ms.sphere == 3:
                 t = np.ascontiguousarray(m.spec.surface, np.float64).reshape(-1, 9)
                 ctx.check(lib().mt_case_set_surface(ctx.h, self.id, _ptr(t, C.c_double), t.shape[0]),

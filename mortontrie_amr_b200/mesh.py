@@ -164,7 +164,12 @@ class SpecMesh:
 
 def spec_mesh(spec: MeshSpec) -> SpecMesh:
     if spec.octree is not None:
-        raise ValueError("the device classifies box refinements; an octree is built by the host mesher")
+        if spec.refine:
+            raise ValueError("refinement boxes and an octree are exclusive")
+        if spec.ib == "markers":
+            raise ValueError("the octree is made for the links body (sphere or surface)")
+        octree_regions(spec)  # the regions' own checks, before the device build
+        return SpecMesh(spec=spec, markers=None)
     if len(spec.refine) != spec.max_level:
         raise ValueError("need one refinement box per level below the maximum level")
     mk = sphere_markers(spec) if (spec.sphere is not None and spec.ib == "markers") else None

@@ -17,7 +17,7 @@ def ctx():
 
 
 def _cases():
-    from mortontrie_amr_b200.case import (cavity_case, df_sphere_case, nested_sphere_case, sphere_case,
+    from mortontrie_amr_b200.case import (Octree, cavity_case, df_sphere_case, nested_sphere_case, sphere_case,
                                           surface_case, uniform_box_case)
     from mortontrie_amr_b200.stl import box_surface, icosphere
     return {
@@ -40,6 +40,11 @@ def _cases():
         "surface_icosphere_l2": surface_case(icosphere((16, 12, 12), 2.0, 3), coarse=(48, 24, 24), max_level=2,
                                              refine=[((8, 6, 6), (26, 18, 18)), ((22, 16, 16), (42, 32, 32))],
                                              re=50.0),
+        # refinement made from the body (regions uploaded with mt_case_set_region)
+        "octree_sphere_q19_l3": sphere_case(coarse=(48, 24, 24), max_level=3, center=(16, 12, 12), radius=2.5,
+                                            octree=Octree()),
+        "octree_surface_q27_l2": surface_case(icosphere((16.3, 12.1, 11.8), 2.5, 3), q=27, collision="Cumulant",
+                                              coarse=(48, 24, 24), max_level=2, octree=Octree(band=2.0, margin=5)),
     }
 
 

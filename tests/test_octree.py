@@ -151,8 +151,10 @@ def test_octree_errors():
         build_mesh(MeshSpec(sphere=Sphere((3.0, 8.0, 8.0), 1.5), octree=Octree(), **base))
     with pytest.raises(ValueError, match="made from a body"):
         build_mesh(MeshSpec(octree=Octree(), **base))
-    with pytest.raises(ValueError, match="host mesher"):
-        spec_mesh(MeshSpec(sphere=Sphere((16.0, 8.0, 8.0), 1.5), octree=Octree(), **base))
+    with pytest.raises(ValueError, match="leaves the domain"):
+        spec_mesh(MeshSpec(sphere=Sphere((3.0, 8.0, 8.0), 1.5), octree=Octree(), **base))
+    ok = spec_mesh(MeshSpec(sphere=Sphere((16.0, 8.0, 8.0), 1.5), octree=Octree(), **base))
+    assert ok.spec.octree is not None
 
 
 def _octree_cases():
