@@ -829,9 +829,9 @@ def cpu_reference_run(nprocs, steps, warmup):
     return mlups, kind, nprocs, sample
 
 
-def _stepped_updates(case):
-    """Cell updates of one coarse step: every level's collide set (lat_f and
-    overlap_F2C) times its 2^l substeps."""
+def _case_updates(case):
+    """Cell updates of one coarse step of a host-meshed case: every level's
+    collide set (lat_f and overlap_F2C) times its 2^l substeps."""
     m = case.mesh
     return sum((m.levels[l]["lat_f"].size + m.levels[l]["overlap_F2C"].size) << l
                for l in range(m.spec.max_level + 1))
@@ -872,7 +872,7 @@ def cpu_reference_extras():
                 continue
             with open(path, "rb") as fh:
                 secs = O.parse_harness_output(fh.read(), case.params.q, case.mesh.spec.max_level, steps)["seconds"]
-            upd = _stepped_updates(case)
+            upd = _case_updates(case)
             out[name] = {"coarse_steps": steps, "seconds_per_coarse_step": round(secs / steps, 4),
                          "total_mlups": round(upd * steps / secs / 1e6, 4), "cell_updates_per_coarse_step": upd,
                          "cores": 1}
