@@ -277,6 +277,12 @@ def run_ours(args):
             amr = amr_section(ctx, torch)
         except Exception as exc:  # reported, not hidden: the line says why the section is missing
             amr = {"error": repr(exc)}
+    octree = None
+    if not args.no_amr and not args.no_octree:
+        try:
+            octree = octree_section(ctx, torch)
+        except Exception as exc:
+            octree = {"error": repr(exc)}
     served = None
     if not args.no_served and world == 1:
         try:
@@ -317,6 +323,7 @@ def run_ours(args):
             "diagnostics": {"mass": red["mass"], "kinetic_energy": red["kinetic_energy"]},
             "cpu_baseline": cpu,
             "amr_cumulant_sphere": amr,
+            "amr_octree_sphere": octree,
             "batched_uneven": batched,
             "served_mix": served,
             "moving_refinement": moving,
@@ -429,6 +436,55 @@ def amr_section(ctx, torch, steps=10, warmup=2, only=None, tune=True):
     mgr.close()
     out["case_setup_s"] = {"host_mesher": round(host_mesh_s, 2), "device_classification_and_build": round(dev_s, 3),
                            "same_keys": bool(same)}
+    return out
+
+
+def octree_section(ctx, torch, steps=10, warmup=2, band=6.0, margin=6):
+    """The 4-level D3Q27 cumulant sphere of amr_section (192x96x96 coarse,
+    R = 6, Re 200) refined from the body instead of nested boxes: octree
+    regions (every level-2 cell within `band` of the surface on the finest
+    level, `margin` cells of each level around the next), classified on the
+    device.  Cells per level, setup time, FP64 (phase order) and FP16 (fused,
+    tuned brick forms) ms per coarse step."""
+    from mortontrie_amr_b200.case import Octree, sphere_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    oc = Octree(band=band, margin=margin)
+    case = sphere_case(q=27, collision="Cumulant", coarse=(192, 96, 96), max_level=3, center=(64, 48, 48),
+                       radius=6.0, u=0.04, re=200.0, octree=oc, mesh="device")
+    out = {"workload": f"4-level D3Q27 cumulant sphere 192x96x96, R=6, Re=200, octree band {band} level-2 cells, "
+                       f"margin {margin}, classified on the device"}
+    stream = torch.cuda.current_stream()
+    for st, storage, schedule in (("f64", "f64", "phases"), ("f16", "f16", "fused")):
+        torch.cuda.synchronize()
+        t0 = time.time()
+        mgr = LBM_Manager(ctx, case, storage, schedule=schedule)
+        torch.cuda.synchronize()
+        setup = time.time() - t0
+        if "stored_cells_per_level" not in out:
+            out["stored_cells_per_level"] = [int(mgr.keys(l)[0].size) for l in range(mgr.L + 1)]
+            out["cell_updates_per_coarse_step"] = _stepped_updates(mgr)
+        mgr.fluidSimulate(warmup)
+        if schedule == "fused":
+            mgr.tune_bricks()
+        mgr.fluidSimulate(1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        mgr.fluidSimulate(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        secs = e0.elapsed_time(e1) / 1e3
+        from mortontrie_amr_b200.lbm import MTError
+        try:
+            mgr.status()
+            finite = True
+        except MTError:
+            finite = False
+        out[st] = {"schedule": schedule, "setup_s": round(setup, 3), "ms_per_coarse_step": round(1e3 * secs / steps, 3),
+                   "total_mlups": round(out["cell_updates_per_coarse_step"] * steps / secs / 1e6, 1),
+                   "finite": finite}
+        mgr.close()
     return out
 
 
@@ -918,6 +974,8 @@ def main():
     ap.add_argument("--no-amr", action="store_true", help="skip the 4-level cumulant sphere section")
     ap.add_argument("--amr-only", action="store_true",
                     help="only the 4-level cumulant sphere section (K coarse steps per storage; profiling runs)")
+    ap.add_argument("--no-octree", action="store_true", help="skip the octree-refined sphere section")
+    ap.add_argument("--octree-only", action="store_true", help="only the octree-refined sphere section")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven instances section")
     ap.add_argument("--no-served", action="store_true", help="skip the served mix section")
     ap.add_argument("--served-only", type=float, default=0.0, metavar="SECONDS",
@@ -1013,6 +1071,16 @@ def main():
         print(json.dumps({"amr_cumulant_sphere": amr_section(ctx, torch, steps=args.steps, warmup=1, only=only,
                                                                        tune=not args.no_brick_tune)}),
               flush=True)
+        ctx.close()
+    elif args.octree_only:
+        import torch
+
+        from mortontrie_amr_b200.lbm import Context
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx = Context(0)
+        ctx.set_stream(stream.cuda_stream)
+        print(json.dumps({"amr_octree_sphere": octree_section(ctx, torch, steps=min(args.steps, 20))}), flush=True)
         ctx.close()
     else:
         run_ours(args)
