@@ -691,7 +691,7 @@ def moving_section(ctx, torch, steps=250, window=32, radius=8, max_level=3, re=1
     return out
 
 
-def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=16):
+def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=16, refine="boxes"):
     """Served mix: a seeded Poisson stream (rate 20/s for `duration` s) of
     direct-forcing sphere flows (R in [3, 8], 16R x 8R x 8R, 1-3 refinement
     levels, Re in [20, 300], D3Q19 LBGK, half oscillating with amplitude R/2
@@ -705,10 +705,11 @@ def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=
     the plain form (FP64, phase order; set-up plus 1/8 of each request's
     steps, scaled to all); the drag error compares served results
     with FP64 solves (phase schedule) of the lowest-Re requests whose served
-    result is finite."""
+    result is finite.  refine: nested boxes around each sphere and its path,
+    or an octree made from its forcing band ("octree")."""
     from mortontrie_amr_b200.serving import Server, TemplateCache, plain_solve_seconds, poisson_requests, solve_alone
     reqs = poisson_requests(seed=seed, rate=rate, duration=duration)
-    cache = TemplateCache(workers=max(1, min(16, (os.cpu_count() or 2) - 1)))
+    cache = TemplateCache(workers=max(1, min(16, (os.cpu_count() or 2) - 1)), refine=refine)
     t0 = time.time()
     cache.prepare(reqs)
     prep = time.time() - t0
@@ -738,7 +739,7 @@ def served_section(ctx, torch, duration=3.0, rate=20.0, seed=5, n_fp64=4, chunk=
     from mortontrie_amr_b200.serving import U_INLET
     return {"workload": f"{len(reqs)} Poisson requests ({rate:g}/s over {duration:g} s, seed {seed}): DF sphere "
                         f"R 3-8, 1-3 levels, Re 20-300, inlet u {U_INLET:g}, half oscillating, 2000 finest steps "
-                        "each, FP16",
+                        f"each, FP16, refinement: {refine}",
             "template_build_s": round(prep, 1), "templates": len(cache.meshes), **served,
             "finite_results": len(finite),
             "finite_alone": len(ok_alone),
@@ -975,6 +976,8 @@ def main():
     ap.add_argument("--amr-only", action="store_true",
                     help="only the 4-level cumulant sphere section (K coarse steps per storage; profiling runs)")
     ap.add_argument("--no-octree", action="store_true", help="skip the octree-refined sphere section")
+    ap.add_argument("--served-refine", default="boxes", choices=["boxes", "octree"],
+                    help="refinement of the served requests (--served-only runs)")
     ap.add_argument("--octree-only", action="store_true", help="only the octree-refined sphere section")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven instances section")
     ap.add_argument("--no-served", action="store_true", help="skip the served mix section")
@@ -1015,7 +1018,8 @@ def main():
         torch.cuda.set_stream(stream)
         ctx = Context(0)
         ctx.set_stream(stream.cuda_stream)
-        print(json.dumps({"served_mix": served_section(ctx, torch, duration=args.served_only)}), flush=True)
+        print(json.dumps({"served_mix": served_section(ctx, torch, duration=args.served_only,
+                                                       refine=args.served_refine)}), flush=True)
         ctx.close()
     elif args.moving_only:
         import torch

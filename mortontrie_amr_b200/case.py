@@ -160,7 +160,7 @@ def cavity_case(q=19, collision="LBGK", coarse=(32, 32, 32), max_level=1, re=100
 
 
 def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q=19, period=2000,
-                   amplitude=0.5, band_slack=0.0, mesh="host", window=None) -> Case:
+                   amplitude=0.5, band_slack=0.0, mesh="host", window=None, octree=None) -> Case:
     """Flow past a sphere represented by direct-forcing Lagrangian markers
     (one per finest cell^2 of surface, 3-point kernel): coarse channel
     16R x 8R x 8R, inlet on West, outflow on East, periodic sides, centre at
@@ -170,7 +170,8 @@ def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q
     window = (y_lo, y_hi): the boxes and the forcing band cover only the
     centre displacements in [y_lo, y_hi] (coarse cells) of the path, for a
     refinement that moves with the body (the markers still follow the whole
-    path)."""
+    path).  octree (an mesh.Octree): refine around the forcing band and its
+    path instead of boxes (the fluid inside the sphere on coarser levels)."""
     r = int(radius)
     nx, ny, nz = 16 * r, 8 * r, 8 * r
     c0 = (4 * r, 4 * r, 4 * r)
@@ -194,6 +195,11 @@ def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q
         s = 1 << l
         refine.append((tuple(int(np.floor((c[a] - b[a]) * s)) for a in range(3)),
                        tuple(int(np.ceil((c[a] + b[a]) * s)) for a in range(3))))
+    if octree is not None:
+        # refinement made from the forcing band over the path instead of boxes
+        if window is not None:
+            raise ValueError("a moving window takes refinement boxes")
+        refine = []
     nu = u * 2.0 * r / re
     p = CaseParams(q=q, collision="LBGK", ib_method="DF", bc_mode="zouhe_outflow", nu=nu, u_bc=(u, 0.0, 0.0),
                    u_ref=u)
@@ -210,7 +216,7 @@ def df_sphere_case(radius=4, max_level=2, re=100.0, oscillating=False, u=0.05, q
         return Case(dataclasses.replace(m, markers=sphere_markers(path_spec)), p)
     spec = MeshSpec(q=q, max_level=max_level, coarse=(nx, ny, nz), refine=refine,
                     boundary=("bc", "periodic", "periodic"), sphere=Sphere(c, float(r)), ib="markers",
-                    oscillation=(amp, period) if oscillating else None, band_slack=band_slack)
+                    oscillation=(amp, period) if oscillating else None, band_slack=band_slack, octree=octree)
     return Case(_mesh(spec, mesh), p)
 
 

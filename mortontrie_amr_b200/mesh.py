@@ -89,7 +89,9 @@ class Octree:
     """Refinement regions made from the body (sphere or surface) instead of
     boxes: the finest level covers every level-(L-1) cell within `band` of
     those cells of the body's surface and inside it (the near-solid cells
-    Grid_Manager::generate_inner refines, Grid_Manager.cpp:136-454), and
+    Grid_Manager::generate_inner refines, Grid_Manager.cpp:136-454; for a
+    direct-forcing sphere the cells within `band` of its forcing band over
+    the whole path, the fluid inside left to coarser levels), and
     every coarser level covers the next finer region grown by `margin` of
     its own cells, rounded out to whole parent cells (the intermediate
     levels the reference's generate_intermediate would make and leaves
@@ -166,10 +168,9 @@ def spec_mesh(spec: MeshSpec) -> SpecMesh:
     if spec.octree is not None:
         if spec.refine:
             raise ValueError("refinement boxes and an octree are exclusive")
-        if spec.ib == "markers":
-            raise ValueError("the octree is made for the links body (sphere or surface)")
         octree_regions(spec)  # the regions' own checks, before the device build
-        return SpecMesh(spec=spec, markers=None)
+        mk = sphere_markers(spec) if (spec.sphere is not None and spec.ib == "markers") else None
+        return SpecMesh(spec=spec, markers=mk)
     if len(spec.refine) != spec.max_level:
         raise ValueError("need one refinement box per level below the maximum level")
     mk = sphere_markers(spec) if (spec.sphere is not None and spec.ib == "markers") else None
@@ -330,6 +331,26 @@ def octree_regions(spec: "MeshSpec") -> list:
         gx, gy, gz = _grid(near.lo, near.hi)
         inside = surface_inside(tris, gx, gy, gz).reshape(near.mask.shape)
         fine = Region(near.lo, near.mask | inside)
+    elif spec.sphere is not None and spec.ib == "markers":
+        # a direct-forcing sphere: only the forcing band over the whole path
+        # (finest cells within 2.7 of the surface at some position, and
+        # band_slack deeper; 1.35 level-(L-1) cells) and `band` around it; the
+        # fluid inside stays on coarser levels
+        c = np.asarray(spec.sphere.center, np.float64) * s
+        r = spec.sphere.radius * s
+        amp = spec.oscillation[0] * s if spec.oscillation else 0.0
+        slack = spec.band_slack * s
+        reach = band + np.sqrt(3.0) / 2.0
+        ext = np.array([r, r + amp, r]) + 1.35 + reach + 1.0
+        lo = np.floor(c - ext).astype(np.int64) - 1
+        hi = np.ceil(c + ext).astype(np.int64) + 1
+        gx, gy, gz = _grid(lo, hi)
+        px, py, pz = gx + 0.5 - c[0], gy + 0.5 - c[1], gz + 0.5 - c[2]
+        qy = np.clip(py, -amp, amp)
+        dmin = np.sqrt(px * px + (py - qy) ** 2 + pz * pz)
+        dmax = np.sqrt(px * px + (np.abs(py) + amp) ** 2 + pz * pz)
+        keep = (dmin <= r + 1.35 + reach) & (dmax >= r - 1.35 - slack - reach)
+        fine = Region(lo, keep.reshape(tuple((hi - lo).tolist())))
     elif spec.sphere is not None:
         c = np.asarray(spec.sphere.center, np.float64) * s
         r = spec.sphere.radius * s
@@ -417,8 +438,6 @@ def build_mesh(spec: MeshSpec) -> Mesh:
     if octree:
         if spec.refine:
             raise ValueError("refinement boxes and an octree are exclusive")
-        if spec.ib == "markers":
-            raise ValueError("the octree is made for the links body (sphere or surface)")
     elif len(spec.refine) != L:
         raise ValueError("need one refinement box per level below the maximum level")
     periodic = tuple(b == "periodic" for b in spec.boundary)

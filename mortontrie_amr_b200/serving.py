@@ -105,16 +105,29 @@ def template_key(req: Request) -> tuple:
     return (req.grid_radius, req.levels, req.oscillating)
 
 
-def build_template(key: tuple, mesh: str = "host"):
+# refinement of a request when made from its body: the finest level covers
+# the forcing band over the path and 2 level-(L-1) cells around it, each
+# coarser level the next with 4 cells of margin
+SERVE_OCTREE = dict(band=2.0, margin=4)
+
+
+def build_template(key: tuple, mesh: str = "host", refine: str = "boxes"):
     """Mesh of a template: the host mesher's sets ("host", picklable for
-    worker processes) or the spec alone ("device")."""
+    worker processes) or the spec alone ("device"); refinement in nested
+    boxes around the sphere and its path, or an octree made from its forcing
+    band ("octree")."""
+    from .mesh import Octree
     r, levels, osc = key
+    if refine not in ("boxes", "octree"):
+        raise ValueError(f"refine must be 'boxes' or 'octree', not {refine!r}")
     return df_sphere_case(radius=r, max_level=levels, re=100.0, oscillating=osc, period=PERIOD,
-                          amplitude=AMPLITUDE, band_slack=1.0, mesh=mesh).mesh
+                          amplitude=AMPLITUDE, band_slack=1.0, mesh=mesh,
+                          octree=Octree(**SERVE_OCTREE) if refine == "octree" else None).mesh
 
 
-def _build_host_template(key: tuple):
-    return build_template(key, "host")
+def _build_host_template(key_refine: tuple):
+    key, refine = key_refine
+    return build_template(key, "host", refine)
 
 
 def request_case(req: Request, mesh):
@@ -184,10 +197,11 @@ class TemplateCache:
     """Templates by key; mesh "device" keeps specs only (the lattice is
     classified on the device per request), "host" the host mesher's sets."""
 
-    def __init__(self, workers: int = 0, mesh: str = "device"):
+    def __init__(self, workers: int = 0, mesh: str = "device", refine: str = "boxes"):
         self.meshes = {}
         self.workers = workers
         self.mesh = mesh
+        self.refine = refine
 
     def prepare(self, requests):
         """Build every template the requests need (host sets in worker processes)."""
@@ -199,16 +213,16 @@ class TemplateCache:
             from concurrent.futures import ProcessPoolExecutor
             with ProcessPoolExecutor(max_workers=min(self.workers, len(keys)),
                                      mp_context=mp.get_context("spawn")) as ex:
-                for k, m in zip(keys, ex.map(_build_host_template, keys)):
+                for k, m in zip(keys, ex.map(_build_host_template, [(k, self.refine) for k in keys])):
                     self.meshes[k] = m
         else:
             for k in keys:
-                self.meshes[k] = build_template(k, self.mesh)
+                self.meshes[k] = build_template(k, self.mesh, self.refine)
 
     def get(self, req: Request):
         k = template_key(req)
         if k not in self.meshes:
-            self.meshes[k] = build_template(k, self.mesh)
+            self.meshes[k] = build_template(k, self.mesh, self.refine)
         return self.meshes[k]
 
 

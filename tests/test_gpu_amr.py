@@ -553,6 +553,29 @@ def test_octree_case_matches_oracle(ctx, which, schedule):
     mgr.close()
 
 
+@pytest.mark.parametrize("schedule", ["phases", "fused"])
+def test_octree_direct_forcing_matches_oracle(ctx, schedule):
+    """A direct-forcing oscillating sphere refined around its forcing band
+    (octree, fluid inside on coarser levels): GPU FP64 vs the oracle,
+    bit-exact populations and the force to 1e-12."""
+    from mortontrie_amr_b200.case import Octree, df_sphere_case
+    case = df_sphere_case(radius=3, max_level=2, re=50.0, oscillating=True, period=60,
+                          octree=Octree(band=2.0, margin=4))
+    mgr = _device_case(ctx, case, None, schedule=schedule)
+    mgr.fluidSimulate(4)
+    ctx.synchronize()
+    oc = run_oracle(case, 4)
+    for l in range(case.max_level + 1):
+        f, fcol = mgr.populations(l)
+        _, tags = mgr.keys(l)
+        g = oc.get(l)
+        keep = (tags & TAG_BC) == 0
+        assert np.array_equal(f[:, keep], g["f"][:, keep]), l
+        assert np.array_equal(fcol, g["fcol"]), l
+    assert rel_err(mgr.force()[:3], oc.force()[:3]) < 1e-12
+    mgr.close()
+
+
 def test_octree_case_reduced_storage(ctx):
     """The octree sphere in FP16 under the fused schedule against FP64."""
     from mortontrie_amr_b200.lbm import LBM_Manager

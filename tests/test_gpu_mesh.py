@@ -43,6 +43,8 @@ def _cases():
         # refinement made from the body (regions uploaded with mt_case_set_region)
         "octree_sphere_q19_l3": sphere_case(coarse=(48, 24, 24), max_level=3, center=(16, 12, 12), radius=2.5,
                                             octree=Octree()),
+        "octree_df_osc_l2": df_sphere_case(radius=3, max_level=2, re=60.0, oscillating=True, period=100,
+                                           octree=Octree(band=2.0, margin=4)),
         "octree_surface_q27_l2": surface_case(icosphere((16.3, 12.1, 11.8), 2.5, 3), q=27, collision="Cumulant",
                                               coarse=(48, 24, 24), max_level=2, octree=Octree(band=2.0, margin=5)),
     }

@@ -127,6 +127,48 @@ def test_octree_mesh_contract(name, spec):
     assert m.levels[L]["lat_sf"].size > 0 and m.dis_keys.size > 0
 
 
+def _tiles_once(m):
+    L = m.spec.max_level
+    ext = np.array(m.spec.coarse) << L
+    count = np.zeros(tuple(ext.tolist()), np.int32)
+    bc = np.concatenate(m.lat_bc)
+    for l in range(L + 1):
+        s = m.levels[l]
+        leaves = np.concatenate([s["lat_f"], s["overlap_C2F"], s["lat_sf"]] + ([bc] if l == 0 else []))
+        x, y, z = cell_coords(L, l, leaves)
+        w = 1 << (L - l)
+        for d in np.ndindex(w, w, w):
+            np.add.at(count, (w * x + d[0], w * y + d[1], w * z + d[2]), 1)
+    return count.min() == 1 and count.max() == 1
+
+
+@pytest.mark.parametrize("osc", [False, True])
+def test_octree_direct_forcing_sphere(osc):
+    """A direct-forcing sphere refined around its forcing band and path: the
+    same band as the boxes give, the fluid inside on coarser levels, every
+    C2F cell a child of an F2C cell, the leaves tiling the domain once."""
+    from mortontrie_amr_b200.case import df_sphere_case
+    oc = df_sphere_case(radius=3, max_level=2, oscillating=osc, octree=Octree(band=2.0, margin=4)).mesh
+    box = df_sphere_case(radius=3, max_level=2, oscillating=osc).mesh
+    L = 2
+    assert np.array_equal(oc.levels[L]["ib_band"], box.levels[L]["ib_band"])
+    assert oc.n_cells()[L] < box.n_cells()[L]
+    for l in range(1, L + 1):
+        x, y, z = cell_coords(L, l - 1, oc.levels[l - 1]["overlap_F2C"])
+        kids = np.unique(np.concatenate([cell_key(L, l, 2 * x + d[0], 2 * y + d[1], 2 * z + d[2])
+                                         for d in np.ndindex(2, 2, 2)]))
+        assert np.array_equal(kids, oc.levels[l]["overlap_C2F"]), l
+    assert _tiles_once(oc)
+    if not osc:
+        # the sphere's centre is not on the finest level (hollow region; a
+        # path of amplitude R/2 sweeps the band over the centre of so small a sphere)
+        s = 1 << L
+        c = [int(v * s) for v in oc.spec.sphere.center]
+        fine = set(zip(*[v.tolist() for v in cell_coords(L, L, oc.all_keys(L))]))
+        assert tuple(c) not in fine
+    assert np.array_equal(oc.markers.ref, box.markers.ref) and np.array_equal(oc.markers.path, box.markers.path)
+
+
 def test_octree_smaller_than_boxes():
     """The 4-level sphere: the octree's finest level covers the body and its
     band, far fewer cells than the nested box of the same sphere."""

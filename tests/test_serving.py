@@ -91,3 +91,22 @@ def test_summary_counts_finite_results_only():
     s = ServerStats(results=rs, wall_s=3600.0).summary()
     assert s["completed"] == 3 and s["finite"] == 1 and s["failed"] == 2
     assert s["cases_per_hour"] == 1.0 and s["p99_s"] == 1.0
+
+
+def test_octree_templates():
+    """Templates refined from the forcing band (refine="octree"): the host
+    template's band equals the box template's, with fewer cells; a request
+    on a device template keeps the octree and takes its own radius and path."""
+    from mortontrie_amr_b200.mesh import SpecMesh, estimate_cells
+    from mortontrie_amr_b200.serving import Request, TemplateCache, build_template, request_case
+    key = (3, 2, True)
+    box = build_template(key, "host")
+    oc = build_template(key, "host", refine="octree")
+    assert np.array_equal(oc.levels[2]["ib_band"], box.levels[2]["ib_band"])
+    assert sum(oc.n_cells()) < sum(box.n_cells())
+    req = Request(rid=0, arrival=0.0, radius=2.6, levels=2, re=80.0, oscillating=True, finest_steps=2000)
+    case = request_case(req, TemplateCache(refine="octree").get(req))
+    assert isinstance(case.mesh, SpecMesh) and case.mesh.spec.octree is not None
+    assert case.mesh.spec.sphere.radius == 2.6
+    est = estimate_cells(case.mesh.spec)
+    assert est[2] < estimate_cells(request_case(req, TemplateCache().get(req)).mesh.spec)[2]
