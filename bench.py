@@ -642,9 +642,9 @@ def moving_section(ctx, torch, steps=250, window=32, radius=8, max_level=3, re=1
     steps, FP16) on the static mesh whose finest box and forcing band cover
     the whole swept path, and with the refinement moving with the sphere
     (re-meshed every `window` coarse steps on the device, state carried by
-    mt_case_remap).  Wall time per coarse step (re-meshing included), cells
-    of the finest level and of the band, and the mean drag and lift of both
-    runs."""
+    mt_case_remap), and on a static octree made from the forcing band over
+    the path.  Wall time per coarse step (re-meshing included), cells of the
+    finest level and of the band, and the mean drag and lift of the runs."""
     from mortontrie_amr_b200.case import df_sphere_case
     from mortontrie_amr_b200.lbm import LBM_Manager
     from mortontrie_amr_b200.moving import MovingSphere
@@ -688,6 +688,25 @@ def moving_section(ctx, torch, steps=250, window=32, radius=8, max_level=3, re=1
     out["speedup"] = round(ws / wm, 3)
     out["cd_rel_diff"] = float(abs(cm[0] - cs[0]) / max(abs(cs[0]), 1e-30))
     mv.close()
+    # the static mesh refined from the forcing band over the path (octree;
+    # the fluid inside the sphere on coarser levels) instead of boxes
+    from mortontrie_amr_b200.case import Octree
+    from mortontrie_amr_b200.serving import SERVE_OCTREE
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    so = LBM_Manager(ctx, df_sphere_case(oscillating=True, mesh="device", octree=Octree(**SERVE_OCTREE), **kw), "f16",
+                     schedule="fused", scaling="standard")
+    so.fluidSimulate(steps)
+    torch.cuda.synchronize()
+    wo = time.perf_counter() - t
+    co = coeffs(so.force())
+    out["static_octree"] = {"ms_per_coarse_step": round(1e3 * wo / steps, 3), "finest_cells": so.size(max_level),
+                            "band_cells": int(np.count_nonzero(so.keys(max_level)[1] & 256)),
+                            "cells_all_levels": int(sum(so.size(l) for l in range(max_level + 1))),
+                            "cd": co[0], "cl": co[1], "speedup_vs_static": round(ws / wo, 3),
+                            "cd_rel_diff_vs_static": float(abs(co[0] - cs[0]) / max(abs(cs[0]), 1e-30)),
+                            "cl_abs_diff_vs_static": float(abs(co[1] - cs[1]))}
+    so.close()
     return out
 
 
