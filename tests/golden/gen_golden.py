@@ -8,6 +8,7 @@ Run here, where the reference checkout exists:
     python tests/golden/gen_golden.py --morton             # neighbour blocks
     python tests/golden/gen_golden.py --tecplot            # the reference's flow file
     python tests/golden/gen_golden.py --dis                # STL link wall distances
+    python tests/golden/gen_golden.py --collide            # single-cell collision answers
 The outputs are small .npz files; the GPU box only reads them.  The trace
 cases run one harness process each, in parallel; cfg1's 1000 coarse steps
 take about half an hour of one core.
@@ -161,6 +162,26 @@ def dis_golden():
         print("dis", name, keys.size, int((ref != -1).sum()), os.path.getsize(path), "bytes")
 
 
+def collide_golden():
+    """Single-cell collision known answers from the reference's own
+    Collision_LBGK / Collision_Cumulant (one coarse step of a closed box):
+    the sampled interior cells' populations before and after collision."""
+    import oracle as O
+    from golden_cases import COLLIDE_CASES, COLLIDE_SEED, collide_case, collide_sample, collide_state
+    for name, spec in COLLIDE_CASES.items():
+        case = collide_case(spec)
+        init = collide_state(case)
+        out = O.run_harness(case, 1, init)
+        keys = case.mesh.all_keys(0)
+        assert np.array_equal(out["levels"][0]["keys"], keys)
+        idx = collide_sample(case)
+        meta = dict(spec=spec, seed=COLLIDE_SEED)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, keys=keys[idx], f_in=init[0][1][:, idx], fcol=out["levels"][0]["fcol"][:, idx],
+                            meta=np.frombuffer(json.dumps(meta).encode(), np.uint8))
+        print("collide", name, os.path.getsize(path), "bytes")
+
+
 SAMPLE = 64
 
 
@@ -221,6 +242,8 @@ if __name__ == "__main__":
         tecplot_golden()
     elif "--dis" in sys.argv:
         dis_golden()
+    elif "--collide" in sys.argv:
+        collide_golden()
     elif "--trace" in sys.argv:
         from concurrent.futures import ProcessPoolExecutor
         import multiprocessing as mp

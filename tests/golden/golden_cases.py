@@ -3,6 +3,8 @@ vectors.  Shared by gen_golden.py and the tests, so both rebuild the same
 index sets with the mesher."""
 from __future__ import annotations
 
+import numpy as np
+
 from mortontrie_amr_b200.case import Case, CaseParams
 from mortontrie_amr_b200.mesh import MeshSpec, Sphere, build_mesh
 
@@ -83,3 +85,49 @@ def dis_mesh(spec):
     mesh = build_mesh(MeshSpec(q=spec["q"], max_level=1, coarse=(32, 16, 16), refine=[((6, 4, 4), (18, 12, 12))],
                                boundary=("bc", "periodic", "periodic"), surface=tris))
     return mesh, tris
+
+
+# single-cell collision known answers: a closed 10^3 box (its 8^3 interior
+# collides), one coarse step of the reference's own code from seeded random
+# cell states; the fixture keeps SAMPLE_CELLS interior cells' inputs and
+# post-collision outputs
+COLLIDE_CASES = {
+    "collide_q19_lbgk": dict(q=19, collision="LBGK", nu=0.02),
+    "collide_q27_cumulant": dict(q=27, collision="Cumulant", nu=0.005),
+}
+COLLIDE_SEED = 1234
+SAMPLE_CELLS = 64
+
+
+def collide_case(spec):
+    from mortontrie_amr_b200.case import uniform_box_case
+    return uniform_box_case(q=spec["q"], n=(10, 10, 10), nu=spec["nu"], boundary=("bc", "bc", "bc"),
+                            collision=spec["collision"], empty_levels=1)
+
+
+def collide_state(case, seed=COLLIDE_SEED):
+    """Seeded per-cell states of every level-0 cell: rho in U[0.9, 1.1), u of
+    uniform direction and |u| in U[0, 0.1), the BGK equilibrium of those
+    plus a non-equilibrium part 0.01 w_q N(0, 1).  Returns the harness's
+    init list (level 0 keys and f; the empty level 1)."""
+    from mortontrie_amr_b200.case import equilibrium
+    from mortontrie_amr_b200.lattice import weights
+    q = case.params.q
+    keys = case.mesh.all_keys(0)
+    rng = np.random.default_rng(seed)
+    n = keys.size
+    rho = rng.uniform(0.9, 1.1, n)
+    d = rng.standard_normal((3, n))
+    d /= np.linalg.norm(d, axis=0)
+    u = d * rng.uniform(0.0, 0.1, n)
+    f = equilibrium(q, rho, u[0], u[1], u[2]) + 0.01 * weights(q)[:, None] * rng.standard_normal((q, n))
+    return [(keys, f), (case.mesh.all_keys(1), np.zeros((q, 0)))]
+
+
+def collide_sample(case, seed=COLLIDE_SEED):
+    """Indices (into the level-0 keys) of the sampled interior cells."""
+    lat_f = case.mesh.levels[0]["lat_f"]
+    keys = case.mesh.all_keys(0)
+    idx = np.searchsorted(keys, lat_f)
+    rng = np.random.default_rng(seed + 1)
+    return np.sort(rng.choice(idx, size=SAMPLE_CELLS, replace=False))

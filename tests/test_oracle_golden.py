@@ -31,3 +31,29 @@ def test_taus_match_reference_unit_conversion():
     for name in GOLDEN_CASES:
         spec, case, z, _ = load_golden(name)
         assert np.array_equal(np.array(case.params.taus(case.max_level)), z["tau"]), name
+
+
+def _collide_kat(name):
+    import json
+    import os
+    from golden_cases import COLLIDE_CASES, collide_case, collide_sample, collide_state
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    case = collide_case(COLLIDE_CASES[name])
+    init = collide_state(case, meta["seed"])
+    idx = collide_sample(case, meta["seed"])
+    assert np.array_equal(case.mesh.all_keys(0)[idx], z["keys"])
+    assert np.array_equal(init[0][1][:, idx], z["f_in"])  # the same seeded inputs
+    return z, case, init, idx
+
+
+@pytest.mark.parametrize("name", ["collide_q19_lbgk", "collide_q27_cumulant"])
+def test_oracle_single_cell_collision(name):
+    """Single-cell collision known answers (seeded cell states, rho in
+    [0.9, 1.1), |u| < 0.1, a non-equilibrium part; the reference's own
+    Collision_LBGK / Collision_Cumulant, Collision_Manager.cpp:13-53 and
+    Collision_Cumulant.cpp:22-652): the oracle's post-collision populations
+    of the 64 sampled cells, bit for bit."""
+    z, case, init, idx = _collide_kat(name)
+    oc = run_oracle(case, 1, init[:1] + [init[1]])
+    assert np.array_equal(oc.get(0)["fcol"][:, idx], z["fcol"])
