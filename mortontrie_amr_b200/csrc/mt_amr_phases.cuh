@@ -727,16 +727,17 @@ __global__ void k_pull_copy(const int32_t *__restrict__ list, int64_t nl, int64_
 // memory, so a cell's Q - 1 source indices are shared-memory reads at fixed
 // offsets.  The brick neighbours come from Morton_Assist::find_neighbor on a
 // corner cell, so each source is the cell the reference's find() returns.
-// 16-bit storage runs six blocks per SM (85 registers, a few spilled); the
-// wider types keep their registers.
+// Resident blocks per SM of each form and storage: brick_min_blocks.
 // bcls: 1 stream + collide, 3 the same with the streamed f stored, 2 stream
-// (f stored) + copy.  The streamed f of class-1 cells is read by nothing in
+// (f stored) + copy, 4 a direct-forcing band cell (stream; collided after
+// the forcing).  The streamed f of class-1 cells is read by nothing in
 // the coarse step (their next collision is computed here, a missing link's
 // f never changes), so it is stored only when `fall` is set or when the
 // state leaves the fused schedule (k_brick_pull).
 // When `macros` is set (the level's last substep of the coarse step) the
 // macros of the streamed f are written too: they are what the all-level
 // calculateMacros at the end of the coarse step computes.
+
 // The part of a brick cell's pass after its gather: v holds the streamed f
 // of cell i (class cls), present(k) says whether link k had a source cell
 // (a missing one keeps f, which is then not stored again).
