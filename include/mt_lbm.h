@@ -239,6 +239,18 @@ int mt_case_reduce(mt_ctx *ctx, int32_t case_id, double *out5);
    for the region their C2F children cover).  Dense cases: two equal rows.
    Each row is summed in a fixed order (run to run identical). */
 int mt_case_reduce_levels(mt_ctx *ctx, int32_t case_id, double *out);
+/* The diagnostics LBM_Manager::infoPrint prints each coarse step
+   (LBM_Manager.cpp:914-979), from the end-of-step macros on the device:
+   out[4 * (max_level + 1)], per level l: out[4l] the largest |u| and
+   out[4l + 1] the number of cells with |u| > 1 over lat_f and overlap_F2C
+   (a NaN velocity counts in neither, as in the reference's comparisons);
+   over lat_f, out[4l + 2] = sum |u - u_prev|^2 and out[4l + 3] = sum |u|^2,
+   the reference's velocity error being sqrt(sum_l out[4l + 2] /
+   sum_l out[4l + 3]).  u_prev is the velocity the previous mt_case_info call
+   of the case saw (the reference keeps the one of the level's last
+   substep); the first call reports 0.  The drag part of the line is
+   mt_get_force.  Multi-level cases; synchronises the stream. */
+int mt_case_info(mt_ctx *ctx, int32_t case_id, double *out);
 /* Allocation-free variant of mt_case_reduce; no reference counterpart (the
    reference has no device-side reduction).  For callers that must not allocate
    device memory during the call (a host that budgets the GPU's memory up front

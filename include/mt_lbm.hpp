@@ -34,6 +34,8 @@
 
 #include <algorithm>
 #include <array>
+#include <cmath>
+#include <cstdio>
 #include <bitset>
 #include <cstdint>
 #include <memory>
@@ -602,6 +604,41 @@ public:
         device([&] { ctx_.check(mt_case_reduce_levels(ctx_.get(), id_, out.data()), "reduce_levels"); });
         return out;
     }
+    // infoPrint's diagnostics per level: [(max_level + 1) * 4] = max |u|,
+    // cells with |u| > 1, sum |u - u_prev|^2, sum |u|^2 (mt_case_info)
+    std::vector<double> info()
+    {
+        std::vector<double> out(4 * (size_t)(desc_.max_level + 1));
+        device([&] { ctx_.check(mt_case_info(ctx_.get(), id_, out.data()), "info"); });
+        return out;
+    }
+    // LBM_Manager::infoPrint (LBM_Manager.cpp:914-979): the velocity change
+    // since the previous call, per level max |u| / cells above 1, and with a
+    // drag scale (u_lb = the boundary velocity in level-0 lattice units,
+    // d_lb = the body's diameter in finest cells, both > 0) Cd of the mean
+    // force per treat() call since the previous call, whose sums are then
+    // reset as the reference resets them
+    void infoPrint(long iter_no, double u_lb = 0.0, double d_lb = 0.0, std::FILE *out = stdout)
+    {
+        const std::vector<double> d = info();
+        double e2 = 0.0, v2 = 0.0;
+        for (int l = 0; l <= desc_.max_level; ++l) {
+            e2 += d[4 * l + 2];
+            v2 += d[4 * l + 3];
+        }
+        std::fprintf(out, "[Iter] %ld Velocity error = %g | max|v|/nbig:", iter_no, std::sqrt(e2) / std::sqrt(v2 + 1e-16));
+        for (int l = 0; l <= desc_.max_level; ++l) std::fprintf(out, " L%d=%g/%ld", l, d[4 * l], (long)d[4 * l + 1]);
+        const std::array<double, 4> f = force();
+        if (u_lb > 0.0 && d_lb > 0.0 && f[3] > 0.0) {
+            const double fx = f[0] / f[3];
+            const double cd = 2.0 * fx / (u_lb * u_lb * 3.14159265358979323846 * d_lb * d_lb / 4.0);
+            cd_sum_ += cd;
+            ++cd_count_;
+            std::fprintf(out, "  Cd = %g  (Cd_avg = %g, Fx_lb = %g, n = %ld)", cd, cd_sum_ / cd_count_, fx, (long)f[3]);
+            ctx_.check(mt_reset_force(ctx_.get(), id_), "reset_force");
+        }
+        std::fprintf(out, "\n");
+    }
     int32_t id() const { return id_; }
     const mt_case_desc &desc() const { return desc_; }
 
@@ -613,6 +650,8 @@ public:
     User *user = nullptr;
 
 private:
+    double cd_sum_ = 0.0;
+    long cd_count_ = 0;
     static Lat_Manager &lat_or_throw()
     {
         if (!Lat_Manager::pointer_me) throw std::runtime_error("LBM_Manager(): no Lat_Manager constructed");

@@ -526,7 +526,7 @@ void amr_free(Case &c)
         void *ptrs[] = {lv.key, lv.tag, lv.bcidx, lv.disrow, lv.nbr, lv.f, lv.fcol, lv.rho, lv.u,
                         lv.collide_list, lv.stream_list, lv.iblist, lv.expl_src, lv.expl_child, lv.coal_child,
                         lv.fcol_alt, lv.fused_list, lv.bstart, lv.bmask, lv.bnbr, lv.bcls, lv.bhalo,
-                        lv.band, lv.collide_nb, lv.draw_keys, lv.draw_set, lv.expl_prev};
+                        lv.band, lv.collide_nb, lv.draw_keys, lv.draw_set, lv.expl_prev, lv.info_prev};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         for (int s = 0; s < kNumSets; ++s)
@@ -1225,6 +1225,24 @@ int amr_reduce(Ctx &ctx, Case &c, double *h_out)
     int rc = amr_dispatch(c, [&](auto *tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         return AmrOps<S>::reduce(ctx, c, d);
+    });
+    if (!rc) MT_CUDA(ctx, cudaMemcpyAsync(h_out, d, nb, cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    cudaFreeAsync(d, ctx.stream);
+    return rc;
+}
+
+// LBM_Manager::infoPrint's per-level diagnostics (mt_case_info): the
+// end-of-step macros are current after every coarse step under both
+// schedules, so no population sync is needed
+int amr_info(Ctx &ctx, Case &c, double *h_out)
+{
+    const size_t nb = sizeof(double) * 4 * (size_t)(c.d.max_level + 1);
+    double *d = nullptr;
+    MT_CUDA(ctx, cudaMallocAsync(&d, nb, ctx.stream));
+    int rc = amr_dispatch(c, [&](auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        return AmrOps<S>::info(ctx, c, d);
     });
     if (!rc) MT_CUDA(ctx, cudaMemcpyAsync(h_out, d, nb, cudaMemcpyDeviceToHost, ctx.stream));
     MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));

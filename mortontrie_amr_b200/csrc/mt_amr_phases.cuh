@@ -2292,6 +2292,125 @@ int AmrOps<S>::reduce(Ctx &ctx, Case &c, double *d_out)
     return MT_OK;
 }
 
+// ---- LBM_Manager::infoPrint's diagnostics (mt_case_info) ----------------
+// Per block over a level's collide list (lat_f then overlap_F2C, the cells
+// infoPrint visits, LBM_Manager.cpp:914-955): the largest |u| and the number
+// of cells with |u| > 1 over both sets, and over the lat_f cells (the first
+// nlatf entries) sum |u - u_prev|^2 and sum |u|^2, u_prev the velocity the
+// previous call saw (prev [3][nlatf], FP64, rewritten here).  A NaN velocity
+// never wins the maximum, as in the reference's comparisons.
+// partial: [4][gridDim.x]
+template <class C>
+__global__ void k_level_info(const int32_t *__restrict__ list, int64_t m, int64_t nlatf, const C *__restrict__ u,
+                             int64_t n, double *__restrict__ prev, int have_prev, double *__restrict__ partial)
+{
+    __shared__ double red[4][256];
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double a[4] = {0, 0, 0, 0};
+    if (j < m) {
+        const int64_t i = list[j];
+        const double ux = (double)u[i], uy = (double)u[n + i], uz = (double)u[2 * n + i];
+        const double v2 = ux * ux + uy * uy + uz * uz;
+        const double vmag = sqrt(v2);
+        a[0] = vmag > 0.0 ? vmag : 0.0;
+        a[1] = vmag > 1.0 ? 1.0 : 0.0;
+        if (j < nlatf) {
+            if (have_prev) {
+                const double dx = ux - prev[j], dy = uy - prev[nlatf + j], dz = uz - prev[2 * nlatf + j];
+                a[2] = dx * dx + dy * dy + dz * dz;
+            }
+            a[3] = v2;
+            prev[j] = ux;
+            prev[nlatf + j] = uy;
+            prev[2 * nlatf + j] = uz;
+        }
+    }
+    for (int c = 0; c < 4; ++c) red[c][threadIdx.x] = a[c];
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) {
+            red[0][threadIdx.x] = fmax(red[0][threadIdx.x], red[0][threadIdx.x + st]);
+            for (int c = 1; c < 4; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + st];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) partial[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = red[threadIdx.x][0];
+}
+
+// one block: each level's row (column 0 the maximum, the others sums) in a
+// fixed order.  out: [nlev * 4]
+static __global__ void k_info_totals(const double *partial, const LevelPartials P, double *out)
+{
+    __shared__ double red[256];
+    for (int l = 0; l < P.nlev; ++l)
+        for (int c = 0; c < 4; ++c) {
+            const double *p = partial + P.off[l] + (int64_t)c * P.nb[l];
+            double a = 0;
+            for (int64_t j = threadIdx.x; j < P.nb[l]; j += blockDim.x) a = c == 0 ? fmax(a, p[j]) : a + p[j];
+            red[threadIdx.x] = a;
+            __syncthreads();
+            for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+                if (threadIdx.x < st)
+                    red[threadIdx.x] = c == 0 ? fmax(red[threadIdx.x], red[threadIdx.x + st])
+                                              : red[threadIdx.x] + red[threadIdx.x + st];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) out[l * 4 + c] = red[0];
+            __syncthreads();
+        }
+}
+
+template <class S>
+int AmrOps<S>::info(Ctx &ctx, Case &c, double *d_out)
+{
+    using C = typename Store<S>::C;
+    LevelPartials P{};
+    P.nlev = c.d.max_level + 1;
+    int64_t total = 0;
+    for (int l = 0; l < P.nlev; ++l) {
+        P.off[l] = total;
+        P.nb[l] = (c.lv[l].ncollide + 255) / 256;
+        total += 4 * P.nb[l];
+        Level &lv = c.lv[l];
+        if (!lv.info_prev && lv.nlist[0])
+            MT_CUDA(ctx, cudaMallocAsync(&lv.info_prev, sizeof(double) * 3 * (size_t)lv.nlist[0], ctx.stream));
+    }
+    double *partial = nullptr;
+    MT_CUDA(ctx, cudaMallocAsync(&partial, sizeof(double) * std::max<int64_t>(total, 1), ctx.stream));
+    MT_CUDA(ctx, cudaMemsetAsync(d_out, 0, sizeof(double) * 4 * (size_t)P.nlev, ctx.stream));
+    cudaError_t err = cudaSuccess;
+    bool ok = true;
+    for (int l = 0; l < P.nlev && ok; ++l) {
+        Level &lv = c.lv[l];
+        if (!P.nb[l]) continue;
+        k_level_info<C><<<(unsigned)P.nb[l], 256, 0, ctx.stream>>>(lv.collide_list, lv.ncollide, lv.nlist[0],
+                                                                 AmrTyped<S>::u(lv), lv.n, lv.info_prev,
+                                                                 lv.info_have ? 1 : 0, partial + P.off[l]);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            err = e;
+            ok = false;
+        } else {
+            ctx.launches++;
+            lv.info_have = true;
+        }
+    }
+    if (ok) {
+        k_info_totals<<<1, 256, 0, ctx.stream>>>(partial, P, d_out);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            err = e;
+            ok = false;
+        } else {
+            ctx.launches++;
+        }
+    }
+    cudaFreeAsync(partial, ctx.stream);
+    if (!ok) return set_err(ctx, MT_ERR_CUDA, std::string("info launch: ") + cudaGetErrorString(err));
+    return MT_OK;
+}
+
+
 template <class S>
 int AmrOps<S>::guard(Ctx &ctx, Case &c, bool current_only)
 {

@@ -738,6 +738,18 @@ int mt_case_reduce_levels(mt_ctx *h, int32_t id, double *out)
     return amr_reduce(ctx, *c, out);
 }
 
+int mt_case_info(mt_ctx *h, int32_t id, double *out)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!out) return set_err(ctx, MT_ERR_ARG, "null output");
+    if (c->dense) return set_err(ctx, MT_ERR_STATE, "the info diagnostics belong to multi-level cases");
+    if (!c->built) return set_err(ctx, MT_ERR_STATE, "case not built");
+    return amr_info(ctx, *c, out);
+}
+
 int mt_case_reduce(mt_ctx *h, int32_t id, double *out)
 {
     Case *c;

@@ -86,6 +86,8 @@ struct Level {
     // explosion sources on the parent level (F2C then ghost F2C) and their children on this level
     int32_t *expl_src = nullptr; int32_t *expl_child = nullptr; int64_t nexpl = 0, nexpl_f2c = 0;
     void *expl_prev = nullptr;  // MT_ITIME_EXTRAP: [Q * nexpl] the sources' parent values at the parent's previous step
+    double *info_prev = nullptr;  // mt_case_info: [3][nlist[0]] the lat_f velocities the last call saw
+    bool info_have = false;
     // coalescence: F2C cells of this level and their children on the next level
     int32_t *coal_child = nullptr;
     // raw uploads, consumed by the build
@@ -245,6 +247,7 @@ int amr_set(Ctx &ctx, Case &c, int level, const double *h_f, const double *h_fco
 int amr_macros(Ctx &ctx, Case &c, int level, double *h_rho, double *h_u);
 int amr_reduce(Ctx &ctx, Case &c, double *h_out);
 int amr_sync_f(Ctx &ctx, Case &c);
+int amr_info(Ctx &ctx, Case &c, double *h_out);
 // MT_ITIME_EXTRAP: saved explosion sources allocated and, when stale, taken from the state
 int amr_prev_sync(Ctx &ctx, Case &c);
 int amr_set_face(Ctx &ctx, Case &c, int face, const double *u);
@@ -273,6 +276,9 @@ template <class S> struct AmrOps {
     // untouched) and keep the fastest in Level::brick_variant;
     // ms[MT_BRICK_FORMS * level + form], variant[level] (-1: no brick pass on the level)
     static int tune_bricks(Ctx &ctx, Case &c, int32_t *variant, float *ms);
+    // infoPrint's diagnostics per level into d_out [(max_level + 1) * 4]
+    // (mt_case_info)
+    static int info(Ctx &ctx, Case &c, double *d_out);
     // batched brick pass (descriptor in device memory, total bricks known on the host)
     static int batch_pass(Ctx &ctx, int q, int coll, const BrickBatch *d_desc, int64_t total, const Shift &sh);
     // src's state carried onto dst's lattice (same Q, levels, storage)

@@ -32,7 +32,7 @@ EXPORTS = [
     "mt_case_init_equilibrium", "mt_case_init_fields", "mt_case_set_populations", "mt_case_get_populations",
     "mt_case_get_macros", "mt_case_reduce", "mt_calculate_macros", "mt_collide", "mt_stream", "mt_explosion",
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
-    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_reduce_levels", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_interface_time", "mt_case_set_face_velocity", "mt_case_set_markers",
+    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_reduce_levels", "mt_case_info", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_interface_time", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
     "mt_case_generate", "mt_case_set_surface", "mt_case_set_region", "mt_marker_record", "mt_marker_done", "mt_case_force_async",
     "mt_case_force_copied", "mt_set_priority", "mt_case_remap", "mt_case_status_copied", "mt_case_tune_bricks",
@@ -140,7 +140,7 @@ def lib():
             "mt_find": [vp, i32, i32, u64p, i64, i64p], "mt_case_init_equilibrium": [vp, i32, C.c_double, dp],
             "mt_case_init_fields": [vp, i32, dp, dp, dp, dp], "mt_case_set_populations": [vp, i32, i32, dp, dp],
             "mt_case_get_populations": [vp, i32, i32, dp, dp], "mt_case_get_macros": [vp, i32, i32, dp, dp],
-            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_reduce_levels": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_interface_time": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
+            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_reduce_levels": [vp, i32, dp], "mt_case_info": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_interface_time": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
             "mt_batch_create": [vp, i32p], "mt_batch_destroy": [vp, i32], "mt_batch_add": [vp, i32, i32],
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
             "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64],
@@ -521,6 +521,38 @@ class LBM_Manager:
         out = np.zeros((self.L + 2, 5))
         self.ctx.check(lib().mt_case_reduce_levels(self.ctx.h, self.id, _ptr(out, C.c_double)), "reduce_levels")
         return out
+
+    def info(self):
+        """infoPrint's diagnostics per level (mt_case_info): rows 0..L,
+        columns max |u| and cells with |u| > 1 (lat_f and overlap_F2C), sum
+        |u - u_prev|^2 and sum |u|^2 (lat_f; u_prev = the previous call's)."""
+        out = np.zeros((self.L + 1, 4))
+        self.ctx.check(lib().mt_case_info(self.ctx.h, self.id, _ptr(out, C.c_double)), "mt_case_info")
+        return out
+
+    def infoPrint(self, iter_no, file=None):
+        """The line LBM_Manager::infoPrint prints (LBM_Manager.cpp:914-979):
+        the velocity change since the previous call relative to the velocity,
+        per level max |u| / cells above 1, and for a sphere the drag
+        coefficient of the mean force per treat() call since the previous
+        call (the accumulated force is then reset, as the reference resets its
+        sums) with its running average.  Returns the line."""
+        import sys
+        d = self.info()
+        err = float(np.sqrt(d[:, 2].sum()) / np.sqrt(d[:, 3].sum() + 1e-16))
+        line = f"[Iter] {iter_no} Velocity error = {err:.6g} | max|v|/nbig:"
+        line += "".join(f" L{l}={d[l, 0]:.6g}/{int(d[l, 1])}" for l in range(self.L + 1))
+        sphere = getattr(self.case.mesh.spec, "sphere", None)
+        f = self.force()
+        if sphere is not None and f[3] > 0:
+            dia = 2.0 * sphere.radius * (1 << self.L)
+            cd = drag_coefficient(f, self.case.params.u_ref, dia)
+            self._cd = getattr(self, "_cd", []) + [cd]
+            line += (f"  Cd = {cd:.6g}  (Cd_avg = {np.mean(self._cd):.6g}, Fx_lb = {f[0] / f[3]:.6g}, "
+                     f"n = {int(f[3])})")
+            self.reset_force()
+        print(line, file=file or sys.stdout)
+        return line
 
     def remap_from(self, src: "LBM_Manager", counts: bool = True):
         """Carry src's state onto this case's lattice (mt_case_remap); returns

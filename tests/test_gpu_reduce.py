@@ -79,3 +79,50 @@ def test_reduce_levels_reduced_storage(ctx, storage):
     want = host_rows(case, lambda l: mgr.populations(l)[0])
     _close(got, want, 1e-6)
     mgr.close()
+
+
+def _host_info(mgr, prev):
+    """infoPrint's quantities from the read-back macros: per level max |u|
+    and cells with |u| > 1 over lat_f and F2C, sum |u - prev|^2 and sum |u|^2
+    over lat_f (prev: the lat_f velocities of the previous call, or None)."""
+    rows, snap = [], []
+    for l in range(mgr.L + 1):
+        _, u = mgr.macros(l)
+        _, tags = mgr.keys(l)
+        both = (tags & 3) != 0
+        latf = (tags & 1) != 0
+        v = np.sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2])
+        ul = u[:, latf]
+        e2 = 0.0 if prev is None else float(((ul - prev[l]) ** 2).sum())
+        rows.append([float(v[both].max()) if both.any() else 0.0, int((v[both] > 1.0).sum()), e2,
+                     float((ul * ul).sum())])
+        snap.append(ul)
+    return np.array(rows), snap
+
+
+@pytest.mark.parametrize("schedule", ["phases", "fused"])
+def test_info_matches_host_diagnostics(ctx, schedule):
+    """mt_case_info (the diagnostics LBM_Manager::infoPrint prints) against
+    the same quantities from the read-back FP64 macros: the maximum and the
+    count exactly, the sums to 1e-12; the velocity change is measured from
+    the previous call (zero on the first)."""
+    from mortontrie_amr_b200.case import nested_sphere_case
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    case = nested_sphere_case(coarse=(48, 24, 24), max_level=2, center=(16, 12, 12), radius=2.0,
+                              half_widths=(4.0, 2.5), re=50.0)
+    mgr = LBM_Manager(ctx, case, schedule=schedule)
+    mgr.fluidSimulate(2)
+    d0 = mgr.info()
+    h0, snap = _host_info(mgr, None)
+    assert np.all(d0[:, 2] == 0)
+    mgr.fluidSimulate(1)
+    d1 = mgr.info()
+    h1, _ = _host_info(mgr, snap)
+    for d, h in ((d0, h0), (d1, h1)):
+        assert np.array_equal(d[:, 0], h[:, 0]) and np.array_equal(d[:, 1], h[:, 1])
+        for c in (2, 3):
+            assert np.allclose(d[:, c], h[:, c], rtol=1e-12, atol=0), (c, d[:, c], h[:, c])
+    assert d1[:, 2].sum() > 0
+    line = mgr.infoPrint(3)
+    assert line.startswith("[Iter] 3 Velocity error = ") and "Cd = " in line and " L2=" in line
+    mgr.close()
