@@ -417,6 +417,7 @@ int mt_case_set_region(mt_ctx *h, int32_t id, int32_t level, const int64_t *lo, 
         if (shape[a] < 1 || lo[a] < 0 || lo[a] + shape[a] > ext)
             return set_err(ctx, MT_ERR_ARG, "region box outside the coarser level's extent");
         n *= shape[a];
+        if (n > INT32_MAX) return set_err(ctx, MT_ERR_ARG, "a region box above 2^31 cells");
     }
     c->h_reg[level].assign(mask, mask + n);
     for (int a = 0; a < 3; ++a) {
