@@ -157,3 +157,31 @@ def test_flow_output_of_a_stepped_case(ctx, tmp_path):
     assert np.allclose(got, want, rtol=1e-5, atol=1e-9)
     assert np.abs(want).max() > 1e-3      # the flow has started
     mgr.close()
+
+
+def test_region_arguments(ctx):
+    """mt_case_set_region / mt_case_generate with regions: levels out of
+    range, boxes outside the coarser level's extent, regions beside boxes
+    and a refined level without its region are refused."""
+    import ctypes as C
+    from mortontrie_amr_b200.case import Octree, sphere_case
+    from mortontrie_amr_b200.lbm import _ptr, lib, make_desc, make_mesh_spec
+    case = sphere_case(coarse=(48, 24, 24), max_level=2, center=(16, 12, 12), radius=2.5, octree=Octree(),
+                       mesh="device")
+    d = make_desc(case, "f64", None)
+    cid = C.c_int32()
+    assert lib().mt_case_create(ctx.h, C.byref(d), C.byref(cid)) == 0
+    lo = np.zeros(3, np.int64)
+    shape = np.array([4, 4, 4], np.int64)
+    mask = np.ones(64, np.uint8)
+    args = lambda l, lo_, sh_: (ctx.h, cid.value, l, _ptr(lo_, C.c_int64), _ptr(sh_, C.c_int64), _ptr(mask, C.c_uint8))
+    assert lib().mt_case_set_region(*args(0, lo, shape)) == -1           # level 0 has no region
+    assert lib().mt_case_set_region(*args(3, lo, shape)) == -1           # above max_level
+    far = np.array([46, 0, 0], np.int64)
+    assert lib().mt_case_set_region(*args(1, far, shape)) == -1          # leaves level 0's extent
+    assert lib().mt_case_set_region(*args(1, np.array([20, 10, 10], np.int64), shape)) == 0
+    ms = make_mesh_spec(case.mesh.spec)
+    assert lib().mt_case_generate(ctx.h, cid.value, C.byref(ms)) == -3   # level 2's region missing
+    ms.has_refine[1] = 1                                                  # a box beside a region
+    assert lib().mt_case_generate(ctx.h, cid.value, C.byref(ms)) == -1
+    lib().mt_case_destroy(ctx.h, cid.value)
