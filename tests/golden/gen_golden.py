@@ -9,6 +9,7 @@ Run here, where the reference checkout exists:
     python tests/golden/gen_golden.py --tecplot            # the reference's flow file
     python tests/golden/gen_golden.py --dis                # STL link wall distances
     python tests/golden/gen_golden.py --collide            # single-cell collision answers
+    python tests/golden/gen_golden.py --tgv                # periodic Taylor-Green box
 The outputs are small .npz files; the GPU box only reads them.  The trace
 cases run one harness process each, in parallel; cfg1's 1000 coarse steps
 take about half an hour of one core.
@@ -182,6 +183,31 @@ def collide_golden():
         print("collide", name, os.path.getsize(path), "bytes")
 
 
+def tgv_golden():
+    """The uniform periodic Taylor-Green configuration at 32^3 (D3Q19 LBGK,
+    tau 0.6, u0 0.02, Morton order) after TGV_STEPS steps of the reference's
+    own code (the periodic harness, an empty second level): SHA-256 of f and
+    fcol over every cell and 64 sampled cells in full."""
+    import tempfile
+    import oracle as O
+    from golden_cases import TGV, tgv_reference_case
+    case, init = tgv_reference_case()
+    with tempfile.TemporaryDirectory() as td:
+        p, path = O.start_harness(case, TGV["steps"], td, 0, init=init)
+        p.wait(timeout=3600)
+        assert p.returncode == 0
+        with open(path, "rb") as fh:
+            out = O.parse_harness_output(fh.read(), 19, 1, TGV["steps"])
+    lv = out["levels"][0]
+    assert np.array_equal(lv["keys"], init[0][0])
+    rng = np.random.default_rng(7)
+    idx = np.sort(rng.choice(lv["keys"].size, size=64, replace=False))
+    path = os.path.join(HERE, "tgv_q19_32_periodic.npz")
+    np.savez_compressed(path, fsha=_sha(lv["f"]), fcolsha=_sha(lv["fcol"]), idx=idx, f=lv["f"][:, idx],
+                        fcol=lv["fcol"][:, idx], meta=np.frombuffer(json.dumps(TGV).encode(), np.uint8))
+    print("tgv", os.path.getsize(path), "bytes", round(out["seconds"], 1), "s")
+
+
 SAMPLE = 64
 
 
@@ -244,6 +270,8 @@ if __name__ == "__main__":
         dis_golden()
     elif "--collide" in sys.argv:
         collide_golden()
+    elif "--tgv" in sys.argv:
+        tgv_golden()
     elif "--trace" in sys.argv:
         from concurrent.futures import ProcessPoolExecutor
         import multiprocessing as mp

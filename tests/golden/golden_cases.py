@@ -131,3 +131,25 @@ def collide_sample(case, seed=COLLIDE_SEED):
     idx = np.searchsorted(keys, lat_f)
     rng = np.random.default_rng(seed + 1)
     return np.sort(rng.choice(idx, size=SAMPLE_CELLS, replace=False))
+
+
+# the uniform periodic Taylor-Green configuration (the dense path's
+# workload), small enough for the reference's own code
+TGV = dict(n=32, steps=10, nu=1.0 / 30.0, u0=0.02)
+
+
+def tgv_fields(n=TGV["n"], u0=TGV["u0"]):
+    from mortontrie_amr_b200.case import taylor_green_fields
+    from mortontrie_amr_b200.lbm import morton_order_fields
+    return morton_order_fields(n, *taylor_green_fields((n, n, n), u0))
+
+
+def tgv_reference_case():
+    """The case as the reference harness runs it (an empty second level, the
+    periodic wrap) and its initial state: the BGK equilibrium of the fields."""
+    from mortontrie_amr_b200.case import equilibrium, uniform_box_case
+    n = TGV["n"]
+    case = uniform_box_case(q=19, n=(n, n, n), nu=TGV["nu"], boundary=("periodic",) * 3, empty_levels=1,
+                            u_ref=TGV["u0"])
+    f0 = equilibrium(19, *tgv_fields())
+    return case, [(case.mesh.all_keys(0), f0), (case.mesh.all_keys(1), np.zeros((19, 0)))]
