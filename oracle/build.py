@@ -62,7 +62,7 @@ REF_TUS = [
 ]
 HARNESS_VARIANTS = [(19, 0), (19, 1), (19, 2), (19, 3), (27, 0), (27, 1), (27, 2), (27, 3)]
 # (Q, L) of the harnesses built with the periodic find_neighbor wrap
-PERIODIC_VARIANTS = [(19, 1)]
+PERIODIC_VARIANTS = [(19, 1), (27, 1)]
 
 
 def oracle_lib_path() -> str:

@@ -184,28 +184,30 @@ def collide_golden():
 
 
 def tgv_golden():
-    """The uniform periodic Taylor-Green configuration at 32^3 (D3Q19 LBGK,
-    tau 0.6, u0 0.02, Morton order) after TGV_STEPS steps of the reference's
-    own code (the periodic harness, an empty second level): SHA-256 of f and
-    fcol over every cell and 64 sampled cells in full."""
+    """The uniform periodic Taylor-Green configuration (Morton order; D3Q19
+    LBGK at 32^3 and D3Q27 cumulant at 16^3, tau 0.6, u0 0.02) after 10
+    steps of the reference's own code (the periodic harness, an empty second
+    level): SHA-256 of f and fcol over every cell and 64 sampled cells in
+    full."""
     import tempfile
     import oracle as O
-    from golden_cases import TGV, tgv_reference_case
-    case, init = tgv_reference_case()
-    with tempfile.TemporaryDirectory() as td:
-        p, path = O.start_harness(case, TGV["steps"], td, 0, init=init)
-        p.wait(timeout=3600)
-        assert p.returncode == 0
-        with open(path, "rb") as fh:
-            out = O.parse_harness_output(fh.read(), 19, 1, TGV["steps"])
-    lv = out["levels"][0]
-    assert np.array_equal(lv["keys"], init[0][0])
-    rng = np.random.default_rng(7)
-    idx = np.sort(rng.choice(lv["keys"].size, size=64, replace=False))
-    path = os.path.join(HERE, "tgv_q19_32_periodic.npz")
-    np.savez_compressed(path, fsha=_sha(lv["f"]), fcolsha=_sha(lv["fcol"]), idx=idx, f=lv["f"][:, idx],
-                        fcol=lv["fcol"][:, idx], meta=np.frombuffer(json.dumps(TGV).encode(), np.uint8))
-    print("tgv", os.path.getsize(path), "bytes", round(out["seconds"], 1), "s")
+    from golden_cases import TGV_CASES, tgv_reference_case
+    for name, spec in TGV_CASES.items():
+        case, init = tgv_reference_case(spec)
+        with tempfile.TemporaryDirectory() as td:
+            p, path = O.start_harness(case, spec["steps"], td, 0, init=init)
+            p.wait(timeout=3600)
+            assert p.returncode == 0
+            with open(path, "rb") as fh:
+                out = O.parse_harness_output(fh.read(), spec["q"], 1, spec["steps"])
+        lv = out["levels"][0]
+        assert np.array_equal(lv["keys"], init[0][0])
+        rng = np.random.default_rng(7)
+        idx = np.sort(rng.choice(lv["keys"].size, size=64, replace=False))
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, fsha=_sha(lv["f"]), fcolsha=_sha(lv["fcol"]), idx=idx, f=lv["f"][:, idx],
+                            fcol=lv["fcol"][:, idx], meta=np.frombuffer(json.dumps(spec).encode(), np.uint8))
+        print("tgv", name, os.path.getsize(path), "bytes", round(out["seconds"], 1), "s")
 
 
 SAMPLE = 64

@@ -135,21 +135,25 @@ def collide_sample(case, seed=COLLIDE_SEED):
 
 # the uniform periodic Taylor-Green configuration (the dense path's
 # workload), small enough for the reference's own code
-TGV = dict(n=32, steps=10, nu=1.0 / 30.0, u0=0.02)
+TGV_CASES = {
+    "tgv_q19_32_periodic": dict(q=19, collision="LBGK", n=32, steps=10, nu=1.0 / 30.0, u0=0.02),
+    "tgv_q27_cumulant_16_periodic": dict(q=27, collision="Cumulant", n=16, steps=10, nu=1.0 / 30.0, u0=0.02),
+}
 
 
-def tgv_fields(n=TGV["n"], u0=TGV["u0"]):
+def tgv_fields(spec):
     from mortontrie_amr_b200.case import taylor_green_fields
     from mortontrie_amr_b200.lbm import morton_order_fields
-    return morton_order_fields(n, *taylor_green_fields((n, n, n), u0))
+    n = spec["n"]
+    return morton_order_fields(n, *taylor_green_fields((n, n, n), spec["u0"]))
 
 
-def tgv_reference_case():
+def tgv_reference_case(spec):
     """The case as the reference harness runs it (an empty second level, the
     periodic wrap) and its initial state: the BGK equilibrium of the fields."""
     from mortontrie_amr_b200.case import equilibrium, uniform_box_case
-    n = TGV["n"]
-    case = uniform_box_case(q=19, n=(n, n, n), nu=TGV["nu"], boundary=("periodic",) * 3, empty_levels=1,
-                            u_ref=TGV["u0"])
-    f0 = equilibrium(19, *tgv_fields())
-    return case, [(case.mesh.all_keys(0), f0), (case.mesh.all_keys(1), np.zeros((19, 0)))]
+    n, q = spec["n"], spec["q"]
+    case = uniform_box_case(q=q, n=(n, n, n), nu=spec["nu"], boundary=("periodic",) * 3, empty_levels=1,
+                            u_ref=spec["u0"], collision=spec["collision"])
+    f0 = equilibrium(q, *tgv_fields(spec))
+    return case, [(case.mesh.all_keys(0), f0), (case.mesh.all_keys(1), np.zeros((q, 0)))]

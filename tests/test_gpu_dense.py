@@ -161,20 +161,22 @@ def test_taylor_green_decay(ctx):
     assert abs(ratios["f16", "reference"] - ratios["f64", "reference"]) / ratios["f64", "reference"] < 1e-3
 
 
-def test_dense_f64_matches_reference_periodic_tgv(ctx):
+@pytest.mark.parametrize("name", ["tgv_q19_32_periodic", "tgv_q27_cumulant_16_periodic"])
+def test_dense_f64_matches_reference_periodic_tgv(ctx, name):
     """The dense kernel in FP64 on the uniform periodic Taylor-Green box
-    (32^3, tau 0.6, u0 0.02) against the reference's own code after 10 steps
-    (golden from the periodic reference harness): f and fcol of every cell
-    bit for bit."""
+    (D3Q19 LBGK at 32^3, D3Q27 cumulant at 16^3; tau 0.6, u0 0.02) against
+    the reference's own code after 10 steps (golden from the periodic
+    reference harness): f and fcol of every cell bit for bit."""
     import os
-    from golden_cases import TGV, tgv_fields
+    from golden_cases import TGV_CASES, tgv_fields
     from helpers import sha
     from mortontrie_amr_b200.case import uniform_box_case
-    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "tgv_q19_32_periodic.npz"))
-    n = TGV["n"]
-    case = uniform_box_case(q=19, n=(n, n, n), nu=TGV["nu"], u_ref=TGV["u0"])
-    d = _dense(ctx, case, tgv_fields(), "f64")
-    d.step(TGV["steps"])
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    spec = TGV_CASES[name]
+    n = spec["n"]
+    case = uniform_box_case(q=spec["q"], n=(n, n, n), nu=spec["nu"], u_ref=spec["u0"], collision=spec["collision"])
+    d = _dense(ctx, case, tgv_fields(spec), "f64")
+    d.step(spec["steps"])
     ctx.synchronize()
     f, fcol = d.populations()
     assert np.array_equal(f[:, z["idx"]], z["f"]) and np.array_equal(fcol[:, z["idx"]], z["fcol"])

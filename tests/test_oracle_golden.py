@@ -59,14 +59,16 @@ def test_oracle_single_cell_collision(name):
     assert np.array_equal(oc.get(0)["fcol"][:, idx], z["fcol"])
 
 
-def test_oracle_matches_reference_periodic_tgv():
-    """The uniform periodic Taylor-Green box (the dense path's workload at
-    32^3) after 10 steps of the reference's own code (the periodic harness):
-    the oracle's f and fcol over every cell, bit for bit."""
+@pytest.mark.parametrize("name", ["tgv_q19_32_periodic", "tgv_q27_cumulant_16_periodic"])
+def test_oracle_matches_reference_periodic_tgv(name):
+    """The uniform periodic Taylor-Green box (the dense path's workload)
+    after 10 steps of the reference's own code (the periodic harness): the
+    oracle's f and fcol over every cell, bit for bit."""
     import os
-    from golden_cases import TGV, tgv_reference_case
-    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "tgv_q19_32_periodic.npz"))
-    case, init = tgv_reference_case()
-    oc = run_oracle(case, TGV["steps"], init)
+    from golden_cases import TGV_CASES, tgv_reference_case
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    spec = TGV_CASES[name]
+    case, init = tgv_reference_case(spec)
+    oc = run_oracle(case, spec["steps"], init)
     g = oc.get(0)
     assert sha(g["f"]) == bytes(z["fsha"]) and sha(g["fcol"]) == bytes(z["fcolsha"])
