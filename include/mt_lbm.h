@@ -278,6 +278,21 @@ int mt_lbm_kernel(mt_ctx *ctx, int32_t case_id, int32_t level);       /* LBM_Man
  * LBMkernel(0) then calculateMacros() on every level, replayed from a CUDA
  * graph; asynchronous on the context stream */
 int mt_step(mt_ctx *ctx, int32_t case_id, int32_t n_coarse_steps);
+/* Coarse steps the case has taken through mt_step / mt_batch_step (no
+ * reference counterpart; with mt_case_get/set_populations the state of a
+ * checkpoint).  mt_case_set_step restores the count, and for a
+ * direct-forcing case the markers' position on their path, which follows
+ * the finest substeps taken; the other cases' steps do not depend on it. */
+int mt_case_get_step(mt_ctx *ctx, int32_t case_id, int64_t *coarse_steps);
+int mt_case_set_step(mt_ctx *ctx, int32_t case_id, int64_t coarse_steps);
+/* The direct-forcing body-force density of the finest level's cells
+ * (MT_IB_DF; fixed point, units of 2^-32), [3][n] in the level's key order
+ * (no reference counterpart).  Between coarse steps it holds the force the
+ * forcing band's next collision takes, so a checkpoint of a direct-forcing
+ * case saves and restores it beside the populations and the step count.
+ * MT_ERR_STATE for other cases. */
+int mt_case_get_df_force_field(mt_ctx *ctx, int32_t case_id, int64_t *out);
+int mt_case_set_df_force_field(mt_ctx *ctx, int32_t case_id, const int64_t *in);
 /* Health check after a run of steps: scans every population for NaN/Inf
  * (the reference prints NaN diagnostics each substep, LBM_Simulator.cpp:33-86)
  * and reports errors the step kernels raised.  MT_OK, MT_ERR_NONFINITE or

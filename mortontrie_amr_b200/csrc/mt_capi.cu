@@ -833,7 +833,7 @@ int mt_step(mt_ctx *h, int32_t id, int32_t n)
     if (n < 0) return set_err(ctx, MT_ERR_ARG, "negative step count");
     if (n == 0) return MT_OK;
     if (c->dense) {
-        return dense_dispatch(*c, [&](auto *tag) {
+        rc = dense_dispatch(*c, [&](auto *tag) {
             using S = std::remove_pointer_t<decltype(tag)>;
             int r = MT_OK, left = n;
             if (!c->a_is_fcol) {
@@ -845,10 +845,77 @@ int mt_step(mt_ctx *h, int32_t id, int32_t n)
             for (int s = 0; s < left && !r; ++s) r = DenseOps<S>::step(ctx, *c, 0);
             return r;
         });
+        if (!rc) c->coarse_steps += n;
+        return rc;
     }
     if (c->in_batch) return set_err(ctx, MT_ERR_STATE, "the case belongs to a batch: step it with mt_batch_step");
     rc = amr_step(ctx, *c, n);
     if (rc) return rc;
+    c->coarse_steps += n;
+    return MT_OK;
+}
+
+int mt_case_get_step(mt_ctx *h, int32_t id, int64_t *coarse_steps)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    if (!coarse_steps) return set_err(h->c, MT_ERR_ARG, "null output");
+    *coarse_steps = c->coarse_steps;
+    return MT_OK;
+}
+
+// the direct-forcing force field of the finest level (fixed point, 2^-32)
+static int df_field(mt_ctx *h, int32_t id, Case **out)
+{
+    int rc = get_case(h, id, out);
+    if (rc) return rc;
+    if (!(*out)->built) return set_err(h->c, MT_ERR_STATE, "case not built");
+    if (!(*out)->acc) return set_err(h->c, MT_ERR_STATE, "not a direct-forcing case");
+    return MT_OK;
+}
+
+int mt_case_get_df_force_field(mt_ctx *h, int32_t id, int64_t *out)
+{
+    Case *c;
+    int rc = df_field(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!out) return set_err(ctx, MT_ERR_ARG, "null output");
+    const size_t nb = sizeof(long long) * 3 * (size_t)c->lv[c->d.max_level].n;
+    MT_CUDA(ctx, cudaMemcpyAsync(out, c->acc, nb, cudaMemcpyDeviceToHost, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    return MT_OK;
+}
+
+int mt_case_set_df_force_field(mt_ctx *h, int32_t id, const int64_t *in)
+{
+    Case *c;
+    int rc = df_field(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (!in) return set_err(ctx, MT_ERR_ARG, "null input");
+    const size_t nb = sizeof(long long) * 3 * (size_t)c->lv[c->d.max_level].n;
+    MT_CUDA(ctx, cudaMemcpyAsync(c->acc, in, nb, cudaMemcpyHostToDevice, ctx.stream));
+    MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    c->primed = false;  // the band's next collision takes this force
+    return MT_OK;
+}
+
+int mt_case_set_step(mt_ctx *h, int32_t id, int64_t coarse_steps)
+{
+    Case *c;
+    int rc = get_case(h, id, &c);
+    if (rc) return rc;
+    Ctx &ctx = h->c;
+    if (coarse_steps < 0) return set_err(ctx, MT_ERR_ARG, "negative step count");
+    if (c->tstep) {
+        // the markers' path is indexed by the finest substeps taken
+        const long long t = (long long)(coarse_steps << c->d.max_level);
+        MT_CUDA(ctx, cudaMemcpyAsync(c->tstep, &t, sizeof(t), cudaMemcpyHostToDevice, ctx.stream));
+        MT_CUDA(ctx, cudaStreamSynchronize(ctx.stream));
+    }
+    c->coarse_steps = coarse_steps;
     return MT_OK;
 }
 
@@ -1144,7 +1211,10 @@ int mt_batch_step(mt_ctx *h, int32_t id, int32_t n)
         if ((rc = get_case(h, cid, &c))) return rc;
         cs.push_back(c);
     }
-    return batch_step(h->c, *b, cs, n);
+    rc = batch_step(h->c, *b, cs, n);
+    if (!rc)
+        for (Case *c : cs) c->coarse_steps += n;
+    return rc;
 }
 
 int mt_case_status(mt_ctx *h, int32_t id)

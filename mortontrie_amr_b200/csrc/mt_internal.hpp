@@ -177,6 +177,7 @@ struct Case {
     double center[3] = {0, 0, 0};
     int64_t period = 1;
     long long *tstep = nullptr;
+    int64_t coarse_steps = 0;  // coarse steps taken through mt_step / mt_batch_step (mt_case_get_step)
     long long *acc = nullptr;  // [3][n_L] Eulerian force, fixed point
     // dense index of the band cells over the box the markers' stencils can reach
     int32_t *mgrid = nullptr;

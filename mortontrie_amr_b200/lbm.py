@@ -32,7 +32,8 @@ EXPORTS = [
     "mt_case_init_equilibrium", "mt_case_init_fields", "mt_case_set_populations", "mt_case_get_populations",
     "mt_case_get_macros", "mt_case_reduce", "mt_calculate_macros", "mt_collide", "mt_stream", "mt_explosion",
     "mt_coalescence", "mt_apply_bc", "mt_apply_bc_face", "mt_ib_treat", "mt_lbm_kernel", "mt_step", "mt_get_force",
-    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_reduce_levels", "mt_case_info", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_interface_time", "mt_case_set_face_velocity", "mt_case_set_markers",
+    "mt_reset_force", "mt_case_tune", "mt_case_status", "mt_case_reduce_noalloc", "mt_case_reduce_levels", "mt_case_info", "mt_case_get_step", "mt_case_set_step",
+    "mt_case_get_df_force_field", "mt_case_set_df_force_field", "mt_case_set_schedule", "mt_case_set_interface_scaling", "mt_case_set_interface_time", "mt_case_set_face_velocity", "mt_case_set_markers",
     "mt_batch_create", "mt_batch_destroy", "mt_batch_add", "mt_batch_remove", "mt_batch_size", "mt_batch_step", "mt_case_prepare", "mt_case_transfer",
     "mt_case_generate", "mt_case_set_surface", "mt_case_set_region", "mt_marker_record", "mt_marker_done", "mt_case_force_async",
     "mt_case_force_copied", "mt_set_priority", "mt_case_remap", "mt_case_status_copied", "mt_case_tune_bricks",
@@ -100,6 +101,11 @@ def make_mesh_spec(spec) -> mt_mesh_spec:
     return m
 
 
+def _storage_code(storage) -> int:
+    from .case import STORAGE
+    return STORAGE[storage]
+
+
 def upload_regions(ctx, case_id, spec):
     """The octree's refinement regions (mesh.octree_regions, made on the
     host) for mt_case_generate, each cropped to the box of its cells."""
@@ -140,7 +146,8 @@ def lib():
             "mt_find": [vp, i32, i32, u64p, i64, i64p], "mt_case_init_equilibrium": [vp, i32, C.c_double, dp],
             "mt_case_init_fields": [vp, i32, dp, dp, dp, dp], "mt_case_set_populations": [vp, i32, i32, dp, dp],
             "mt_case_get_populations": [vp, i32, i32, dp, dp], "mt_case_get_macros": [vp, i32, i32, dp, dp],
-            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_reduce_levels": [vp, i32, dp], "mt_case_info": [vp, i32, dp], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_interface_time": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
+            "mt_case_reduce": [vp, i32, dp], "mt_case_reduce_noalloc": [vp, i32, dp], "mt_case_reduce_levels": [vp, i32, dp], "mt_case_info": [vp, i32, dp], "mt_case_get_step": [vp, i32, i64p], "mt_case_set_step": [vp, i32, i64],
+            "mt_case_get_df_force_field": [vp, i32, i64p], "mt_case_set_df_force_field": [vp, i32, i64p], "mt_case_set_schedule": [vp, i32, i32], "mt_case_set_interface_scaling": [vp, i32, i32], "mt_case_set_interface_time": [vp, i32, i32], "mt_case_set_face_velocity": [vp, i32, i32, dp], "mt_case_set_markers": [vp, i32, i64, dp, dp, dp, i64, dp],
             "mt_batch_create": [vp, i32p], "mt_batch_destroy": [vp, i32], "mt_batch_add": [vp, i32, i32],
             "mt_batch_remove": [vp, i32, i32], "mt_batch_size": [vp, i32, i32p], "mt_batch_step": [vp, i32, i32], "mt_case_prepare": [vp, i32], "mt_case_transfer": [vp, i32, vp, i32p],
             "mt_case_generate": [vp, i32, C.POINTER(mt_mesh_spec)], "mt_case_set_surface": [vp, i32, dp, i64],
@@ -521,6 +528,50 @@ class LBM_Manager:
         out = np.zeros((self.L + 2, 5))
         self.ctx.check(lib().mt_case_reduce_levels(self.ctx.h, self.id, _ptr(out, C.c_double)), "reduce_levels")
         return out
+
+    def steps(self) -> int:
+        """Coarse steps taken (mt_case_get_step)."""
+        out = np.zeros(1, np.int64)
+        self.ctx.check(lib().mt_case_get_step(self.ctx.h, self.id, _ptr(out, C.c_int64)), "mt_case_get_step")
+        return int(out[0])
+
+    def save_checkpoint(self, path):
+        """The case's state to `path` (.npz): per level its sorted keys and
+        FP64 populations f and fcol, the coarse steps taken and, for a
+        direct-forcing case, the force field of its band.  Loading it
+        into a case of the same lattice and storage (load_checkpoint) and
+        stepping on gives what stepping on here gives, bit for bit in FP64
+        (the reference and hold interface times; the extrapolated one keeps
+        parent values of the previous step that are not saved)."""
+        arrays = {"meta": np.array([self.q, self.L, _storage_code(self.storage or self.case.params.storage), self.steps()], np.int64)}
+        for l in range(self.L + 1):
+            keys, _ = self.keys(l)
+            f, fcol = self.populations(l)
+            arrays[f"keys{l}"], arrays[f"f{l}"], arrays[f"fcol{l}"] = keys, f, fcol
+        if self.case.params.ib_method == "DF":
+            # the force the band's next collision takes
+            acc = np.zeros((3, self.size(self.L)), np.int64)
+            self.ctx.check(lib().mt_case_get_df_force_field(self.ctx.h, self.id, _ptr(acc, C.c_int64)),
+                           "mt_case_get_df_force_field")
+            arrays["df_force"] = acc
+        np.savez(path, **arrays)
+
+    def load_checkpoint(self, path):
+        """Restore a state saved by save_checkpoint (same lattice and storage)."""
+        z = np.load(path)
+        q, L, st, steps = (int(v) for v in z["meta"])
+        if (q, L, st) != (self.q, self.L, _storage_code(self.storage or self.case.params.storage)):
+            raise ValueError("checkpoint of another model, level count or storage")
+        for l in range(L + 1):
+            if not np.array_equal(self.keys(l)[0], z[f"keys{l}"]):
+                raise ValueError(f"checkpoint of another lattice (level {l})")
+        for l in range(L + 1):
+            self.set_populations(l, z[f"f{l}"], z[f"fcol{l}"])
+        if "df_force" in z.files:
+            acc = np.ascontiguousarray(z["df_force"], np.int64)
+            self.ctx.check(lib().mt_case_set_df_force_field(self.ctx.h, self.id, _ptr(acc, C.c_int64)),
+                           "mt_case_set_df_force_field")
+        self.ctx.check(lib().mt_case_set_step(self.ctx.h, self.id, steps), "mt_case_set_step")
 
     def info(self):
         """infoPrint's diagnostics per level (mt_case_info): rows 0..L,

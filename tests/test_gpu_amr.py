@@ -641,3 +641,33 @@ def test_single_cell_collision_matches_reference(ctx, name, schedule):
     _, fcol = mgr.populations(0)
     assert np.array_equal(fcol[:, idx], z["fcol"])
     mgr.close()
+
+
+@pytest.mark.parametrize("which,storage", [("cumulant", "f64"), ("df", "f64"), ("cumulant", "f16")])
+def test_checkpoint_resume_equals_continuous(ctx, tmp_path, which, storage):
+    """save_checkpoint after 3 coarse steps, load into a fresh case of the
+    same lattice, 3 more steps: the same populations and force as 6 steps
+    without a break (bit for bit, the direct-forcing markers' path phase
+    included); a checkpoint of another lattice is refused."""
+    from mortontrie_amr_b200.lbm import LBM_Manager
+    case = _forms_case(which) if which == "df" else _nested_small()
+    a = LBM_Manager(ctx, case, storage, schedule="fused")
+    a.fluidSimulate(3)
+    path = str(tmp_path / "state.npz")
+    a.save_checkpoint(path)
+    assert a.steps() == 3
+    a.reset_force()
+    a.fluidSimulate(3)
+    b = LBM_Manager(ctx, case, storage, schedule="fused")
+    b.load_checkpoint(path)
+    assert b.steps() == 3
+    b.fluidSimulate(3)
+    ctx.synchronize()
+    _same_state(a, b, case.max_level)
+    assert np.array_equal(a.force(), b.force())
+    from mortontrie_amr_b200.case import cavity_case
+    other = LBM_Manager(ctx, cavity_case(coarse=(16, 16, 16), max_level=1), storage, schedule="fused")
+    with pytest.raises(ValueError):
+        other.load_checkpoint(path)
+    for m in (a, b, other):
+        m.close()
