@@ -306,7 +306,8 @@ int mt_case_status(mt_ctx *ctx, int32_t case_id);
  * 256 only; the other slots are left unwritten). */
 int mt_case_tune(mt_ctx *ctx, int32_t case_id, int32_t *best_block, float *ms_per_candidate);
 /* Forms of the multi-level fused brick pass (no reference counterpart):
- * 0: one cell per lane step at 8 resident 128-thread blocks per SM;
+ * 0: one cell per lane step at 8 resident 128-thread blocks per SM (FP32: 7),
+ *    the default;
  * 3: the lane's two cells in one unrolled sequence, so that the second
  *    cell's gathers overlap the first cell's collision, at 6 blocks;
  * for FP32 / FP16 / BF16 storage also

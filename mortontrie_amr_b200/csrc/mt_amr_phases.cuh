@@ -1000,6 +1000,9 @@ __device__ __forceinline__ void brick_warp_any(int64_t b, int lane, int32_t *s_i
 #ifndef MT_BRICK_MIN_BLOCKS
 #define MT_BRICK_MIN_BLOCKS 8  // resident 128-thread blocks per SM asked of the 16-bit one-cell passes (64 registers)
 #endif
+#ifndef MT_BRICK_MIN_BLOCKS_F32
+#define MT_BRICK_MIN_BLOCKS_F32 7  // resident blocks asked of the FP32 one-cell passes (72 registers)
+#endif
 #ifndef MT_BRICK_MIN_BLOCKS_Q19_LBGK
 #define MT_BRICK_MIN_BLOCKS_Q19_LBGK 10  // 16-bit D3Q19 LBGK one-cell passes: 48 registers, no spills
 #endif
@@ -1019,14 +1022,15 @@ template <int Q, class S, int COLL, int V> constexpr int brick_min_blocks()
     if (V == 2 && Store<S>::shifted) return MT_BRICK_WIDE_MIN_BLOCKS;
     if (V == 3) return Store<S>::shifted ? MT_BRICK_UNROLL_MIN_BLOCKS : 1;
     if (Store<S>::bytes == 2) return (COLL == MT_COLL_LBGK && Q == 19) ? MT_BRICK_MIN_BLOCKS_Q19_LBGK : MT_BRICK_MIN_BLOCKS;
+    if (Store<S>::bytes == 4) return MT_BRICK_MIN_BLOCKS_F32;
     return 1;
 }
-// the form a level runs until mt_case_tune_bricks times them (measured on
-// the 4-level cumulant sphere and the direct-forcing sphere: the pair form
-// runs 2-4x longer per launch at half the resident warps; 16-bit storage is
-// fastest in form 0, FP32 storage in form 2, whose 6-block bound keeps more
-// warps resident than form 0's unbounded registers)
-template <class S> constexpr int brick_default_variant() { return std::is_same<S, float>::value ? 2 : 0; }
+// the form a level runs until mt_case_tune_bricks times them: form 0 for
+// every storage (measured on the 4-level cumulant sphere and the
+// direct-forcing sphere: the pair form runs 2-4x longer per launch at half
+// the resident warps; FP32 form 0 at 7 resident blocks is as fast as or
+// faster than forms 2 and 3 at 6)
+template <class S> constexpr int brick_default_variant() { return 0; }
 
 template <int Q, class S, int COLL, int V>
 __global__ void __launch_bounds__(128, brick_min_blocks<Q, S, COLL, V>()) k_brick_step(
