@@ -94,6 +94,7 @@ def dis_mesh(spec):
 COLLIDE_CASES = {
     "collide_q19_lbgk": dict(q=19, collision="LBGK", nu=0.02),
     "collide_q27_cumulant": dict(q=27, collision="Cumulant", nu=0.005),
+    "collide_q27_lbgk": dict(q=27, collision="LBGK", nu=0.01),
 }
 COLLIDE_SEED = 1234
 SAMPLE_CELLS = 64
@@ -138,6 +139,7 @@ def collide_sample(case, seed=COLLIDE_SEED):
 TGV_CASES = {
     "tgv_q19_32_periodic": dict(q=19, collision="LBGK", n=32, steps=10, nu=1.0 / 30.0, u0=0.02),
     "tgv_q27_cumulant_16_periodic": dict(q=27, collision="Cumulant", n=16, steps=10, nu=1.0 / 30.0, u0=0.02),
+    "tgv_q27_lbgk_16_periodic": dict(q=27, collision="LBGK", n=16, steps=10, nu=1.0 / 30.0, u0=0.02),
 }
 
 

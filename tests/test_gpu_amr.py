@@ -623,7 +623,7 @@ def test_device_neighbor_table_matches_reference_blocks(ctx, q, L):
 
 
 @pytest.mark.parametrize("schedule", ["phases", "fused"])
-@pytest.mark.parametrize("name", ["collide_q19_lbgk", "collide_q27_cumulant"])
+@pytest.mark.parametrize("name", ["collide_q19_lbgk", "collide_q27_cumulant", "collide_q27_lbgk"])
 def test_single_cell_collision_matches_reference(ctx, name, schedule):
     """Single-cell collision known answers from the reference's own
     Collision_LBGK / Collision_Cumulant (seeded cell states, one coarse

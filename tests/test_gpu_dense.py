@@ -161,7 +161,7 @@ def test_taylor_green_decay(ctx):
     assert abs(ratios["f16", "reference"] - ratios["f64", "reference"]) / ratios["f64", "reference"] < 1e-3
 
 
-@pytest.mark.parametrize("name", ["tgv_q19_32_periodic", "tgv_q27_cumulant_16_periodic"])
+@pytest.mark.parametrize("name", ["tgv_q19_32_periodic", "tgv_q27_cumulant_16_periodic", "tgv_q27_lbgk_16_periodic"])
 def test_dense_f64_matches_reference_periodic_tgv(ctx, name):
     """The dense kernel in FP64 on the uniform periodic Taylor-Green box
     (D3Q19 LBGK at 32^3, D3Q27 cumulant at 16^3; tau 0.6, u0 0.02) against

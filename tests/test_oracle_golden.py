@@ -47,7 +47,7 @@ def _collide_kat(name):
     return z, case, init, idx
 
 
-@pytest.mark.parametrize("name", ["collide_q19_lbgk", "collide_q27_cumulant"])
+@pytest.mark.parametrize("name", ["collide_q19_lbgk", "collide_q27_cumulant", "collide_q27_lbgk"])
 def test_oracle_single_cell_collision(name):
     """Single-cell collision known answers (seeded cell states, rho in
     [0.9, 1.1), |u| < 0.1, a non-equilibrium part; the reference's own
@@ -59,7 +59,7 @@ def test_oracle_single_cell_collision(name):
     assert np.array_equal(oc.get(0)["fcol"][:, idx], z["fcol"])
 
 
-@pytest.mark.parametrize("name", ["tgv_q19_32_periodic", "tgv_q27_cumulant_16_periodic"])
+@pytest.mark.parametrize("name", ["tgv_q19_32_periodic", "tgv_q27_cumulant_16_periodic", "tgv_q27_lbgk_16_periodic"])
 def test_oracle_matches_reference_periodic_tgv(name):
     """The uniform periodic Taylor-Green box (the dense path's workload)
     after 10 steps of the reference's own code (the periodic harness): the
