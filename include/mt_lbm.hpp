@@ -597,6 +597,97 @@ public:
         ctx_.check(mt_get_force(ctx_.get(), id_, out.data()), "get_force");
         return out;
     }
+    // A checkpoint of the state between coarse steps (no reference
+    // counterpart), one binary file: a header (Q, levels, storage, coarse
+    // steps), per level n, its sorted keys and FP64 f and fcol [Q][n], and
+    // for direct forcing the band's force field [3][n of the finest level].
+    // loadCheckpoint restores it into a case of the same lattice and storage
+    // (std::runtime_error otherwise); stepping on then gives what stepping
+    // on from the saved case gives.
+    // coarse steps taken (mt_case_get_step)
+    int64_t coarseSteps()
+    {
+        int64_t st = 0;
+        ctx_.check(mt_case_get_step(ctx_.get(), id_, &st), "get_step");
+        return st;
+    }
+    void saveCheckpoint(const std::string &path)
+    {
+        device([&] {
+            std::FILE *fp = std::fopen(path.c_str(), "wb");
+            if (!fp) throw std::runtime_error("saveCheckpoint: cannot open " + path);
+            int64_t steps = 0;
+            ctx_.check(mt_case_get_step(ctx_.get(), id_, &steps), "get_step");
+            const int64_t head[5] = {0x4d54434b50540001LL, desc_.q, desc_.max_level, desc_.storage, steps};
+            bool ok = std::fwrite(head, sizeof(head), 1, fp) == 1;
+            int64_t nfine = 0;
+            for (int l = 0; l <= desc_.max_level && ok; ++l) {
+                int64_t n = 0;
+                ctx_.check(mt_case_level_size(ctx_.get(), id_, l, &n), "level_size");
+                std::vector<uint64_t> k((size_t)n);
+                std::vector<uint32_t> tags((size_t)n);
+                std::vector<double> f((size_t)(n * desc_.q)), fc((size_t)(n * desc_.q));
+                ctx_.check(mt_case_get_keys(ctx_.get(), id_, l, k.data(), tags.data()), "get_keys");
+                ctx_.check(mt_case_get_populations(ctx_.get(), id_, l, f.data(), fc.data()), "get_populations");
+                ok = std::fwrite(&n, sizeof(n), 1, fp) == 1 && (!n || (std::fwrite(k.data(), 8, k.size(), fp) == k.size() &&
+                     std::fwrite(f.data(), 8, f.size(), fp) == f.size() && std::fwrite(fc.data(), 8, fc.size(), fp) == fc.size()));
+                nfine = n;
+            }
+            const int64_t has_df = desc_.ib_method == MT_IB_DF ? 1 : 0;
+            ok = ok && std::fwrite(&has_df, sizeof(has_df), 1, fp) == 1;
+            if (ok && has_df) {
+                std::vector<int64_t> acc((size_t)(3 * nfine));
+                ctx_.check(mt_case_get_df_force_field(ctx_.get(), id_, acc.data()), "get_df_force_field");
+                ok = std::fwrite(acc.data(), 8, acc.size(), fp) == acc.size();
+            }
+            if (std::fclose(fp) != 0 || !ok) throw std::runtime_error("saveCheckpoint: write failed: " + path);
+        });
+    }
+    void loadCheckpoint(const std::string &path)
+    {
+        device([&] {
+            std::FILE *fp = std::fopen(path.c_str(), "rb");
+            if (!fp) throw std::runtime_error("loadCheckpoint: cannot open " + path);
+            auto fail = [&](const std::string &why) {
+                std::fclose(fp);
+                throw std::runtime_error("loadCheckpoint: " + why);
+            };
+            int64_t head[5];
+            if (std::fread(head, sizeof(head), 1, fp) != 1 || head[0] != 0x4d54434b50540001LL) fail("not a checkpoint");
+            if (head[1] != desc_.q || head[2] != desc_.max_level || head[3] != desc_.storage)
+                fail("checkpoint of another model, level count or storage");
+            std::vector<std::vector<double>> f(desc_.max_level + 1), fc(desc_.max_level + 1);
+            int64_t nfine = 0;
+            for (int l = 0; l <= desc_.max_level; ++l) {
+                int64_t n = 0, m = 0;
+                ctx_.check(mt_case_level_size(ctx_.get(), id_, l, &m), "level_size");
+                if (std::fread(&n, sizeof(n), 1, fp) != 1 || n != m) fail("checkpoint of another lattice");
+                std::vector<uint64_t> k((size_t)n), mine((size_t)n);
+                std::vector<uint32_t> tags((size_t)n);
+                f[l].resize((size_t)(n * desc_.q));
+                fc[l].resize((size_t)(n * desc_.q));
+                if (n && (std::fread(k.data(), 8, k.size(), fp) != k.size() ||
+                          std::fread(f[l].data(), 8, f[l].size(), fp) != f[l].size() ||
+                          std::fread(fc[l].data(), 8, fc[l].size(), fp) != fc[l].size()))
+                    fail("truncated file");
+                ctx_.check(mt_case_get_keys(ctx_.get(), id_, l, mine.data(), tags.data()), "get_keys");
+                if (k != mine) fail("checkpoint of another lattice");
+                nfine = n;
+            }
+            int64_t has_df = 0;
+            if (std::fread(&has_df, sizeof(has_df), 1, fp) != 1) fail("truncated file");
+            std::vector<int64_t> acc;
+            if (has_df) {
+                acc.resize((size_t)(3 * nfine));
+                if (std::fread(acc.data(), 8, acc.size(), fp) != acc.size()) fail("truncated file");
+            }
+            std::fclose(fp);
+            for (int l = 0; l <= desc_.max_level; ++l)
+                ctx_.check(mt_case_set_populations(ctx_.get(), id_, l, f[l].data(), fc[l].data()), "set_populations");
+            if (has_df) ctx_.check(mt_case_set_df_force_field(ctx_.get(), id_, acc.data()), "set_df_force_field");
+            ctx_.check(mt_case_set_step(ctx_.get(), id_, head[4]), "set_step");
+        });
+    }
     // FP64 device sums per level and volume-weighted: [(max_level + 2) * 5]
     std::vector<double> reduce_levels()
     {

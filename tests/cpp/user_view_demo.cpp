@@ -4,7 +4,8 @@
 // like LBM_Manager::infoPrint (LBM_Manager.cpp:914-981) reads
 // user[l].velocity.at(code) and user[l].density.at(code) over every level's
 // lat_f; then one population is changed through user[0].df.f[q].at(code)
-// and one more coarse step is taken.
+// and one more coarse step is taken; then a checkpoint is saved and loaded
+// back, and the steps after it must repeat bit for bit.
 // usage: user_view_demo <sets.bin> <out.bin> <steps> <tau0> [tau1 ...]
 // sets.bin uses the reference-harness input layout (oracle/oracle.py).
 // out.bin: per level n, rho[n], ux[n], uy[n], uz[n] on lat_f (ascending key),
@@ -13,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "mt_lbm.hpp"
@@ -126,6 +128,29 @@ int main(int argc, char **argv)
             std::fprintf(stderr, "missing key did not throw\n");
             return 1;
         }
+        // checkpoint: save, two more steps; load it back, the same two
+        // steps: the same populations, bit for bit
+        const std::string ck_path = std::string(argv[2]) + ".ckpt";
+        mgr.saveCheckpoint(ck_path);
+        mgr.fluidSimulate(2);
+        std::vector<std::vector<double>> fa(d.max_level + 1), fca(d.max_level + 1);
+        for (int l = 0; l <= d.max_level; ++l) mgr.populations(l, fa[l], fca[l]);
+        mgr.loadCheckpoint(ck_path);
+        mgr.fluidSimulate(2);
+        for (int l = 0; l <= d.max_level; ++l) {
+            std::vector<double> f, fcol;
+            mgr.populations(l, f, fcol);
+            if (f != fa[l] || fcol != fca[l]) {
+                std::fprintf(stderr, "resumed level %d differs\n", l);
+                return 1;
+            }
+        }
+        const int64_t st = mgr.coarseSteps();
+        if (st != steps + 1 + 2) {
+            std::fprintf(stderr, "step count %lld after resume\n", (long long)st);
+            return 1;
+        }
+        std::remove(ck_path.c_str());
     } catch (const std::exception &e) {
         std::fprintf(stderr, "user_view_demo: %s\n", e.what());
         return 1;
